@@ -1,0 +1,314 @@
+"""B200-native IMPACT-Z space-charge kick and element push: Python bindings.
+
+The product is the C-ABI library ``libimpz_b200.so`` (include/impz_b200.h);
+this module binds it with ctypes, mirroring the reference's call surface
+(BeamBunch / CompDom / FieldQuant, src/Appl/BeamBunch.f90, CompDom.f90,
+Field.f90) so that tests and the benchmark read like the reference's own
+step loop.  There is no CPU fallback: every compute entry point runs the CUDA
+kernels and raises ImpzError if the library or a GPU is missing.
+
+The package directory is named ``impact-z_b200``; load it under the import
+name ``impz_b200`` with :func:`load_package` helpers in the callers.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libimpz_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "impz_b200.h")
+
+OK = 0
+ERR_ARG, ERR_NOMEM, ERR_CUDA, ERR_UNSUPPORTED = -1, -2, -3, -4
+ERR_NONUNIFORM, ERR_STATE, ERR_NONFINITE, ERR_NODEVICE, ERR_BUDGET = -5, -6, -7, -8, -9
+FORM_FP64 = 0
+FORM_FP32CONV = 1
+FLAG_TRACK_IDS = 1
+RAW_LEN = 44
+DIAG_LEN = 45
+MOMREC = 48
+
+
+class ImpzError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        msg = "%s failed: %s (%d)" % (what, error_string(code), code)
+        if code == ERR_CUDA:
+            msg += ": " + last_cuda_error()
+        super().__init__(msg)
+
+
+class ElemStruct(ctypes.Structure):
+    """impz_elem_t: one ImpactZ.in lattice line (src/Contrl/Input.f90:300-315)."""
+
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("nseg", ctypes.c_int),
+        ("mapstp", ctypes.c_int),
+        ("ndata", ctypes.c_int),
+        ("length", ctypes.c_double),
+        ("val", ctypes.c_double * 24),
+        ("zdat", ctypes.POINTER(ctypes.c_double)),
+        ("edat", ctypes.POINTER(ctypes.c_double)),
+        ("epdat", ctypes.POINTER(ctypes.c_double)),
+        ("eppdat", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_LL = ctypes.POINTER(ctypes.c_longlong)
+_E = ctypes.POINTER(ElemStruct)
+_B = ctypes.c_void_p
+
+_SIGS = {
+    "impz_version": (ctypes.c_char_p, []),
+    "impz_error_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "impz_last_cuda_error": (ctypes.c_char_p, []),
+    "impz_set_device": (ctypes.c_int, [ctypes.c_int]),
+    "impz_bunch_create": (ctypes.c_int, [_D, ctypes.c_longlong, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_double, _D, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(_B)]),
+    "impz_bunch_download": (ctypes.c_int, [_B, _D, ctypes.c_longlong, _LL]),
+    "impz_bunch_destroy": (ctypes.c_int, [_B]),
+    "impz_bunch_info": (ctypes.c_int, [_B, _D]),
+    "impz_bunch_stream": (ctypes.c_void_p, [_B]),
+    "impz_map_half": (ctypes.c_int, [_B, _E, ctypes.c_double, _D, ctypes.c_double, ctypes.c_int,
+                                     _I]),
+    "impz_bend_entry": (ctypes.c_int, [_B, _E]),
+    "impz_bend_sector": (ctypes.c_int, [_B, _D, ctypes.c_double]),
+    "impz_bend_exit": (ctypes.c_int, [_B]),
+    "impz_sc_prepare": (ctypes.c_int, [_B, ctypes.c_double, ctypes.c_double, _LL, _D, _D, _D]),
+    "impz_deposit": (ctypes.c_int, [_B, _D, _I]),
+    "impz_poisson_open": (ctypes.c_int, [_B, _D]),
+    "impz_kick": (ctypes.c_int, [_B, ctypes.c_double, _D]),
+    "impz_moments": (ctypes.c_int, [_B, _D]),
+    "impz_diag_row": (ctypes.c_int, [ctypes.c_double, _D, _D, ctypes.c_double, ctypes.c_double,
+                                     _D]),
+    "impz_run": (ctypes.c_int, [_B, _E, ctypes.c_int, _D, _D, ctypes.c_int, _I]),
+    "impz_run_async": (ctypes.c_int, [_B, _E, ctypes.c_int]),
+    "impz_run_fetch": (ctypes.c_int, [_B, _D, _D, ctypes.c_int, _I]),
+    "impz_count_steps": (ctypes.c_int, [_E, ctypes.c_int]),
+    "impz_maplinear": (ctypes.c_int, [_E, ctypes.c_double, ctypes.c_double, ctypes.c_double, _D,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]),
+}
+
+
+def lib():
+    """The loaded C-ABI library (raises ImpzError/OSError if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libimpz_b200.so is not built; run impact-z_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def declared_symbols():
+    """Entry points declared in include/impz_b200.h."""
+    import re
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(impz_[a-z0-9_]+)\s*\(", txt)))
+
+
+def error_string(code):
+    return lib().impz_error_string(code).decode()
+
+
+def last_cuda_error():
+    return lib().impz_last_cuda_error().decode()
+
+
+def _check(rc, what):
+    if rc != OK:
+        raise ImpzError(rc, what)
+
+
+def _dp(a):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+# ---------------------------------------------------------------------------
+def elem(etype, length, nseg, mapstp=1, vals=(), rf=None):
+    """Build an impz_elem_t.  vals are the deck values v1..v24; rf is an
+    optional (z, Ez, Ez', Ez'') on-axis table for linear RF maps."""
+    e = ElemStruct()
+    e.type = int(etype)
+    e.nseg = int(nseg)
+    e.mapstp = int(mapstp)
+    e.length = float(length)
+    for i, v in enumerate(vals):
+        e.val[i] = float(v)
+    e._keep = None
+    if rf is not None:
+        cols = [np.ascontiguousarray(c, dtype=np.float64) for c in rf]
+        e.ndata = len(cols[0])
+        e.zdat, e.edat, e.epdat, e.eppdat = [c.ctypes.data_as(_D) for c in cols]
+        e._keep = cols
+    return e
+
+
+def elem_array(elems):
+    arr = (ElemStruct * len(elems))()
+    keep = []
+    for i, e in enumerate(elems):
+        arr[i] = e
+        keep.append(getattr(e, "_keep", None))
+    arr._keep = keep
+    return arr
+
+
+def count_steps(elems):
+    arr = elem_array(elems)
+    return lib().impz_count_steps(arr, len(elems))
+
+
+def maplinear(e, zedge, t, tau, refpt, charge, mass, freq):
+    ref = np.array(refpt, dtype=np.float64)
+    xm = np.zeros(36)
+    _check(lib().impz_maplinear(ctypes.byref(e), zedge, t, tau, _dp(ref), charge, mass, freq,
+                                _dp(xm)), "impz_maplinear")
+    return xm.reshape(6, 6, order="F"), ref
+
+
+def diag_row(z, rec, refptcl, mass, freq):
+    rec = np.ascontiguousarray(rec, dtype=np.float64)
+    ref = np.ascontiguousarray(refptcl, dtype=np.float64)
+    row = np.zeros(DIAG_LEN)
+    _check(lib().impz_diag_row(z, _dp(rec), _dp(ref), mass, freq, _dp(row)), "impz_diag_row")
+    return row
+
+
+class Bunch:
+    """A bunch resident on the GPU (BeamBunch + CompDom + FieldQuant of one rank)."""
+
+    def __init__(self, pts, current, mass, charge, freq, refptcl, grid, form=FORM_FP64,
+                 track_ids=True):
+        pts = np.ascontiguousarray(pts, dtype=np.float64)
+        if pts.ndim != 2 or pts.shape[1] != 9:
+            raise ValueError("pts must be (n, 9): Pts1 transposed")
+        ref = np.ascontiguousarray(refptcl, dtype=np.float64)
+        h = _B()
+        nx, ny, nz = grid
+        flags = FLAG_TRACK_IDS if track_ids else 0
+        _check(lib().impz_bunch_create(_dp(pts), pts.shape[0], current, mass, charge, freq,
+                                       _dp(ref), nx, ny, nz, form, flags, ctypes.byref(h)),
+               "impz_bunch_create")
+        self.h = h
+        self.n0 = pts.shape[0]
+        self.grid = (nx, ny, nz)
+        self.mass, self.charge, self.freq, self.form = mass, charge, freq, form
+
+    def close(self):
+        if self.h:
+            lib().impz_bunch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self):
+        out = np.zeros(11)
+        _check(lib().impz_bunch_info(self.h, _dp(out)), "impz_bunch_info")
+        return {"current": out[0], "npt": int(out[1]), "nlocal": int(out[2]),
+                "refptcl": out[3:9].copy(), "z": out[9], "bytes": int(out[10])}
+
+    def download(self):
+        pts = np.zeros((self.n0, 9))
+        n = ctypes.c_longlong()
+        _check(lib().impz_bunch_download(self.h, _dp(pts), self.n0, ctypes.byref(n)),
+               "impz_bunch_download")
+        return pts[: n.value].copy()
+
+    # --- the per-step surface -------------------------------------------
+    def map_half(self, e, zedge, z, tau, nst, ihlf):
+        zc = ctypes.c_double(z)
+        ih = ctypes.c_int(ihlf)
+        _check(lib().impz_map_half(self.h, ctypes.byref(e), zedge, ctypes.byref(zc), tau, nst,
+                                   ctypes.byref(ih)), "impz_map_half")
+        return zc.value, ih.value
+
+    def bend_entry(self, e):
+        _check(lib().impz_bend_entry(self.h, ctypes.byref(e)), "impz_bend_entry")
+
+    def bend_sector(self, z, tau):
+        zc = ctypes.c_double(z)
+        _check(lib().impz_bend_sector(self.h, ctypes.byref(zc), tau), "impz_bend_sector")
+        return zc.value
+
+    def bend_exit(self):
+        _check(lib().impz_bend_exit(self.h), "impz_bend_exit")
+
+    def sc_prepare(self, piperad, piperad2):
+        nptot = ctypes.c_longlong()
+        ptrange, rng, msize = np.zeros(6), np.zeros(6), np.zeros(3)
+        _check(lib().impz_sc_prepare(self.h, piperad, piperad2, ctypes.byref(nptot), _dp(ptrange),
+                                     _dp(rng), _dp(msize)), "impz_sc_prepare")
+        return nptot.value, ptrange, rng, msize
+
+    def deposit(self, want_rho=True, want_counts=True):
+        G = int(np.prod(self.grid))
+        rho = np.zeros(G) if want_rho else None
+        cnt = np.zeros(G, dtype=np.int32) if want_counts else None
+        _check(lib().impz_deposit(self.h, _dp(rho),
+                                  cnt.ctypes.data_as(_I) if cnt is not None else None),
+               "impz_deposit")
+        return rho, cnt
+
+    def poisson(self, want_phi=True):
+        phi = np.zeros(int(np.prod(self.grid))) if want_phi else None
+        _check(lib().impz_poisson_open(self.h, _dp(phi)), "impz_poisson_open")
+        return phi
+
+    def kick(self, tau, want_e=False):
+        eg = np.zeros(3 * int(np.prod(self.grid))) if want_e else None
+        _check(lib().impz_kick(self.h, tau, _dp(eg)), "impz_kick")
+        return eg
+
+    def moments(self):
+        rec = np.zeros(MOMREC)
+        _check(lib().impz_moments(self.h, _dp(rec)), "impz_moments")
+        return rec
+
+    # --- whole lattice ------------------------------------------------------
+    def run(self, elems):
+        arr = elem_array(elems)
+        nrec_cap = count_steps(elems) + 1
+        recs = np.zeros((nrec_cap, MOMREC))
+        zs = np.zeros(nrec_cap)
+        nrec = ctypes.c_int()
+        _check(lib().impz_run(self.h, arr, len(elems), _dp(recs), _dp(zs), nrec_cap,
+                              ctypes.byref(nrec)), "impz_run")
+        return recs[: nrec.value], zs[: nrec.value]
+
+    def run_async(self, elems):
+        arr = elem_array(elems)
+        self._pending = (arr, count_steps(elems) + 1)
+        _check(lib().impz_run_async(self.h, arr, len(elems)), "impz_run_async")
+
+    def run_fetch(self):
+        arr, cap = self._pending
+        recs = np.zeros((cap, MOMREC))
+        zs = np.zeros(cap)
+        nrec = ctypes.c_int()
+        _check(lib().impz_run_fetch(self.h, _dp(recs), _dp(zs), cap, ctypes.byref(nrec)),
+               "impz_run_fetch")
+        self._pending = None
+        return recs[: nrec.value], zs[: nrec.value]

@@ -1,0 +1,144 @@
+"""Seeded synthetic bunches and lattices of the benchmark configurations.
+
+Bunches are written in the reference's particle.in / Pts1 layout
+(readin_Dist, src/Appl/Distribution.f90:1666-1714): 9 columns per particle
+x/Scxl, gamma*beta_x, y/Scxl, gamma*beta_y, phase[rad], gamma0-gamma, q/m,
+charge weight, id, with the charge weight Current/Scfreq/Npt*sign(q)
+(Distribution.f90:245).  Random numbers come from numpy's Philox counter-based
+generator (4x64, 10 rounds) keyed by the seed, so every run of a
+configuration sees the same particles.
+"""
+import math
+
+import numpy as np
+
+CLIGHT = 299792458.0
+PROTON_MASS_EV = 938.27208816e6
+ELECTRON_MASS_EV = 0.51099895000e6
+SEED0 = 20261203
+
+
+def scxl(freq):
+    """PhysConst Scxl = c/(2 pi f) (src/DataStruct/PhysConst.f90:30)."""
+    return CLIGHT / (2 * (2 * math.asin(1.0)) * freq)
+
+
+def _truncated_normal(rng, shape, trunc):
+    z = rng.standard_normal(shape)
+    if trunc is not None:
+        bad = np.abs(z) > trunc
+        while bad.any():
+            z[bad] = rng.standard_normal(int(bad.sum()))
+            bad = np.abs(z) > trunc
+    return z
+
+
+def refptcl_for(ekin, mass, phase=0.0):
+    """construct_BeamBunch's refptcl (BeamBunch.f90:56-58)."""
+    r = np.zeros(6)
+    r[4] = phase
+    r[5] = -(ekin / mass + 1.0)
+    return r
+
+
+def gaussian_bunch(n, seed=SEED0, mass=PROTON_MASS_EV, charge=1.0, ekin=2.5e6, current=0.030,
+                   freq=402.5e6, sig_x=1e-3, sig_y=1e-3, sig_xp=1e-3, sig_yp=1e-3,
+                   sig_phase_deg=5.0, sig_e=50e3, trunc=4.0):
+    """Uncorrelated 6D Gaussian truncated at `trunc` sigma per coordinate.
+
+    sig_x/y in m, sig_xp/yp in rad, phase in degrees, energy spread in eV."""
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    z = _truncated_normal(rng, (6, n), trunc)
+    gam0 = 1.0 + ekin / mass
+    gb0 = math.sqrt(gam0 * gam0 - 1.0)
+    xl = scxl(freq)
+    pts = np.empty((n, 9))
+    pts[:, 0] = z[0] * (sig_x / xl)
+    pts[:, 1] = z[1] * (sig_xp * gb0)
+    pts[:, 2] = z[2] * (sig_y / xl)
+    pts[:, 3] = z[3] * (sig_yp * gb0)
+    pts[:, 4] = z[4] * math.radians(sig_phase_deg)
+    pts[:, 5] = z[5] * (sig_e / mass)
+    pts[:, 6] = charge / mass
+    pts[:, 7] = current / freq / n * charge / abs(charge)
+    pts[:, 8] = np.arange(1, n + 1, dtype=np.float64)
+    return pts, refptcl_for(ekin, mass)
+
+
+def flat_top_bunch(n, seed=SEED0, mass=ELECTRON_MASS_EV, charge=-1.0, ekin=250e6 - ELECTRON_MASS_EV,
+                   current=100.0, freq=1.3e9, length=1e-3, mod_amp=0.01, mod_lambda=10e-6,
+                   sig_x=0.2e-3, sig_xp=0.02e-3, sig_e=5e3, trunc=4.0):
+    """Flat-top longitudinal profile with a sinusoidal density modulation
+    (rejection sampled), Gaussian transverse, uncorrelated energy spread."""
+    rng = np.random.Generator(np.random.Philox(key=seed))
+    gam0 = 1.0 + ekin / mass
+    gb0 = math.sqrt(gam0 * gam0 - 1.0)
+    beta0 = gb0 / gam0
+    xl = scxl(freq)
+    zpos = np.empty(0)
+    while zpos.size < n:
+        m = int((n - zpos.size) * 1.1) + 1024
+        cand = rng.uniform(-length / 2, length / 2, m)
+        keep = rng.uniform(0, 1 + mod_amp, m) < 1 + mod_amp * np.cos(2 * np.pi * cand / mod_lambda)
+        zpos = np.concatenate([zpos, cand[keep]])
+    zpos = zpos[:n]
+    t = _truncated_normal(rng, (5, n), trunc)
+    pts = np.empty((n, 9))
+    pts[:, 0] = t[0] * (sig_x / xl)
+    pts[:, 1] = t[1] * (sig_xp * gb0)
+    pts[:, 2] = t[2] * (sig_x / xl)
+    pts[:, 3] = t[3] * (sig_xp * gb0)
+    # phase = -omega*z/(beta c) in the reference's units (z>0 is the head)
+    pts[:, 4] = -zpos / (beta0 * xl)
+    pts[:, 5] = t[4] * (sig_e / mass)
+    pts[:, 6] = charge / mass
+    pts[:, 7] = current / freq / n * charge / abs(charge)
+    pts[:, 8] = np.arange(1, n + 1, dtype=np.float64)
+    return pts, refptcl_for(ekin, mass)
+
+
+def fodo(periods=10, gradient=20.0, ldrift=0.1, lquad=0.1, nseg=4, mapstp=1, radius=1.0):
+    """[drift, quad(+G), drift, quad(-G)] x periods; quads in gradient mode
+    (file ID 0, Quadrupole.f90:19-28)."""
+    from . import elem
+    out = []
+    for _ in range(periods):
+        out.append(elem(0, ldrift, nseg, mapstp, [radius]))
+        out.append(elem(1, lquad, nseg, mapstp, [gradient, 0.0, radius]))
+        out.append(elem(0, ldrift, nseg, mapstp, [radius]))
+        out.append(elem(1, lquad, nseg, mapstp, [-gradient, 0.0, radius]))
+    return out
+
+
+def chicane(angle_deg=3.0, lbend=0.2, ldrift_in=20.0, ldrift_mid=1.0, ldrift_c=0.5, nseg_bend=8,
+            nseg_drift=4, drift_steps_in=400, half_gap=0.01):
+    """20 m of drift then a 4-dipole chicane (+a, -a, -a, +a sector bends).
+    Dipole deck values: v1 angle[rad], v2 k1, v3 file ID (150: z map + SC,
+    no CSR), v4 half gap (Dipole.f90:19-31, AccSimulator.f90:1060-1074)."""
+    from . import elem
+    a = math.radians(angle_deg)
+
+    def bend(sgn):
+        return elem(4, lbend, nseg_bend, 1, [sgn * a, 0.0, 150.0, half_gap, 0.0, 0.0, 0.0, 0.0, 0.0])
+
+    out = [elem(0, ldrift_in, drift_steps_in, 1, [1.0])]
+    out += [bend(+1), elem(0, ldrift_mid, nseg_drift, 1, [1.0]), bend(-1),
+            elem(0, ldrift_c, nseg_drift, 1, [1.0]), bend(-1),
+            elem(0, ldrift_mid, nseg_drift, 1, [1.0]), bend(+1)]
+    return out
+
+
+# benchmark configurations -------------------------------------------------
+def config0(n=100_000, seed=SEED0):
+    """Proton FODO, 1e5 particles, 32x32x64, 160 steps (plain FP64)."""
+    pts, ref = gaussian_bunch(n, seed)
+    return dict(pts=pts, refptcl=ref, current=0.030, mass=PROTON_MASS_EV, charge=1.0,
+                freq=402.5e6, grid=(32, 32, 64), lattice=fodo(10))
+
+
+def config1(n=4_000_000, seed=SEED0, periods=25, nseg=10):
+    """The same beam with 4e6 particles on 64x64x128; 25 FODO periods with
+    10 steps per element = 1000 steps."""
+    pts, ref = gaussian_bunch(n, seed)
+    return dict(pts=pts, refptcl=ref, current=0.030, mass=PROTON_MASS_EV, charge=1.0,
+                freq=402.5e6, grid=(64, 64, 128), lattice=fodo(periods, nseg=nseg))

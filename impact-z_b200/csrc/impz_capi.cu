@@ -1,0 +1,801 @@
+// impz_capi.cu -- the C ABI (include/impz_b200.h): bunch lifetime, the
+// reference's per-step call surface, and the whole-lattice runner.
+//
+// A bunch owns its device state: two buffers of six FP64 SoA columns (the
+// fused particle pass writes the sorted state into the other buffer), the
+// int64 charge grid with per-cell counts and sort cursors, the Poisson work
+// arrays of its numerical form, a device step table, and reduction scratch.
+// All launches go to the bunch's own stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/impz_b200.h"
+#include "impz_common.h"
+#include "impz_host.h"
+#include "impz_launch.h"
+
+using namespace impz;
+
+namespace {
+
+thread_local char g_cuda_err[256] = "";
+
+int cuda_fail(cudaError_t e, const char* where) {
+  std::snprintf(g_cuda_err, sizeof(g_cuda_err), "%s: %s", where, cudaGetErrorString(e));
+  return IMPZ_ERR_CUDA;
+}
+
+#define CK(call)                                  \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+// device buffers -------------------------------------------------------
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+__global__ void k_aos_to_soa(const double* __restrict__ aos, long long n, double* x, double* px,
+                             double* y, double* py, double* ph, double* pt, long long* ids,
+                             double qm_ref, double w_ref, unsigned int* bad) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double* r = aos + 9 * i;
+    x[i] = r[0]; px[i] = r[1]; y[i] = r[2]; py[i] = r[3]; ph[i] = r[4]; pt[i] = r[5];
+    if (ids) ids[i] = (long long)r[8];
+    if (r[6] != qm_ref || r[7] != w_ref) atomicOr(bad, 1u);
+  }
+}
+
+__global__ void k_soa_to_aos(double* __restrict__ aos, long long n, const double* x,
+                             const double* px, const double* y, const double* py,
+                             const double* ph, const double* pt, const long long* ids,
+                             double qm, double w) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double* r = aos + 9 * i;
+    r[0] = x[i]; r[1] = px[i]; r[2] = y[i]; r[3] = py[i]; r[4] = ph[i]; r[5] = pt[i];
+    r[6] = qm; r[7] = w;
+    r[8] = ids ? (double)ids[i] : (double)(i + 1);
+  }
+}
+
+__global__ void k_e4_to_grids(const void* e4, int f32, long long G, double* out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < G;
+       i += (long long)gridDim.x * blockDim.x) {
+    for (int c = 0; c < 3; c++)
+      out[c * G + i] = f32 ? (double)((const float*)e4)[4 * i + c] : ((const double*)e4)[4 * i + c];
+  }
+}
+
+__global__ void k_to_double(const float* in, long long n, double scale, double* out) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = (double)in[i] * scale;
+}
+
+bool is_pow2(int n) { return n >= 4 && (n & (n - 1)) == 0; }
+
+int ilog2i(long long n) {
+  int l = 0;
+  while ((1ll << l) < n) l++;
+  return l;
+}
+
+enum Stage { ST_IDLE = 0, ST_PREPARED = 1, ST_DEPOSITED = 2, ST_SOLVED = 3 };
+
+}  // namespace
+
+struct impz_bunch_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int form = 0, flags = 0;
+  long long cap = 0;
+  int nx = 0, ny = 0, nz = 0;
+  long long G = 0;
+  Phys P;
+  Species sp;
+  double current0 = 0, weight = 0, freq = 0;
+  double refptcl[6] = {0};
+  double z = 0;
+  Consts k;
+  int fixbits = 40;
+  double* pbuf[2][6] = {{nullptr}};
+  long long* ids[2] = {nullptr, nullptr};
+  int parity = 0;
+  unsigned long long* rho = nullptr;
+  int* counts = nullptr;
+  int* cursor = nullptr;
+  int* bsum = nullptr;
+  int nscan = 0;
+  void* spec = nullptr;
+  double* F = nullptr;
+  double* Gt = nullptr;
+  void* ghat = nullptr;
+  void* phi = nullptr;
+  void* efield = nullptr;
+  void* tw[3] = {nullptr, nullptr, nullptr};
+  double2* tw64[3] = {nullptr, nullptr, nullptr};
+  DevState* st = nullptr;
+  StepParams* dsteps = nullptr;
+  int dsteps_cap = 0;
+  StepParams* dfine = nullptr;  // 2-entry table of the per-call surface
+  double* mom_part = nullptr;
+  double* rng_part = nullptr;
+  double* mom_out = nullptr;
+  int mom_cap = 0;
+  double* mom_fine = nullptr;
+  int grid_adv = 0, grid_dep = 0;
+  BendState bend;
+  int stage = ST_IDLE;
+  double sc_gam = 0, sc_rad = 0;
+  // last impz_run_async
+  CompiledLattice lat;
+  bool run_pending = false;
+  size_t bytes = 0;
+
+  double* cur(int c) { return pbuf[parity][c]; }
+  bool f32() const { return form == IMPZ_FORM_FP32CONV; }
+};
+
+namespace {
+
+PoissonBuffers poisson_of(impz_bunch_t b) {
+  PoissonBuffers pb;
+  pb.nx = b->nx; pb.ny = b->ny; pb.nz = b->nz;
+  pb.rho = b->rho;
+  pb.qscale = b->f32() ? std::ldexp(1.0, -b->fixbits) : b->weight * std::ldexp(1.0, -b->fixbits);
+  pb.spec = b->spec; pb.F = b->F; pb.Gt = b->Gt; pb.ghat = b->ghat;
+  pb.phi = b->phi; pb.efield = b->efield;
+  pb.twx = b->tw[0]; pb.twy = b->tw[1]; pb.twz = b->tw[2];
+  pb.tw64x = b->tw64[0]; pb.tw64y = b->tw64[1]; pb.tw64z = b->tw64[2];
+  pb.st = b->st;
+  return pb;
+}
+
+AdvanceArgs advance_args(impz_bunch_t b, const StepParams* table, int fixed, int kick, int post,
+                         int pre, double* mom_out, int mom_index) {
+  AdvanceArgs a;
+  std::memset(&a, 0, sizeof(a));
+  const int in = b->parity, out = kick ? b->parity ^ 1 : b->parity;
+  for (int c = 0; c < 6; c++) {
+    a.in[c] = b->pbuf[in][c];
+    a.out[c] = b->pbuf[out][c];
+  }
+  if (b->ids[0]) {
+    a.id_in = b->ids[in];
+    a.id_out = kick ? b->ids[out] : nullptr;
+  }
+  a.steps = table;
+  a.st = b->st;
+  a.nx = b->nx; a.ny = b->ny; a.nz = b->nz;
+  a.cap = b->cap;
+  a.efield = b->efield;
+  a.efield_scale = b->f32() ? b->weight : 1.0;
+  a.cursor = b->cursor;
+  a.bsum = b->bsum;
+  a.mom_part = b->mom_part;
+  a.rng_part = b->rng_part;
+  a.mom_out = mom_out;
+  a.k = b->k;
+  a.fixed_step = fixed;
+  a.kick = kick;
+  a.do_post = post;
+  a.do_pre = pre;
+  a.mom_index = mom_index;
+  return a;
+}
+
+cudaError_t launch_adv(impz_bunch_t b, const AdvanceArgs& a) {
+  if (b->f32()) return fast::launch_advance(a, true, b->grid_adv, b->stream);
+  return exact::launch_advance(a, false, b->grid_adv, b->stream);
+}
+
+DepositArgs deposit_args(impz_bunch_t b, const StepParams* table, int fixed) {
+  DepositArgs d;
+  std::memset(&d, 0, sizeof(d));
+  for (int c = 0; c < 6; c++) d.in[c] = b->pbuf[b->parity][c];
+  d.steps = table;
+  d.st = b->st;
+  d.fixed_step = fixed;
+  d.nx = b->nx; d.ny = b->ny; d.nz = b->nz;
+  d.fixbits = b->fixbits;
+  d.rho = b->rho;
+  d.counts = b->counts;
+  d.xl = b->P.Scxl;
+  return d;
+}
+
+// deposit + scan + field solve + E for step `fixed` of `table`
+int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
+  DepositArgs d = deposit_args(b, table, fixed);
+  CK(exact::launch_deposit(d, b->grid_dep, b->stream));
+  CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
+  PoissonBuffers pb = poisson_of(b);
+  if (b->f32()) {
+    CK(launch_green<float>(pb, b->stream));
+    CK(launch_convolve<float>(pb, b->stream));
+    CK(launch_efield<float>(pb, b->stream));
+  } else {
+    CK(launch_green<double>(pb, b->stream));
+    CK(launch_convolve<double>(pb, b->stream));
+    CK(launch_efield<double>(pb, b->stream));
+  }
+  return IMPZ_OK;
+}
+
+int upload_fine(impz_bunch_t b, const StepParams* host2) {
+  CK(cudaMemcpyAsync(b->dfine, host2, 2 * sizeof(StepParams), cudaMemcpyHostToDevice,
+                     b->stream));
+  return IMPZ_OK;
+}
+
+void blank_steps(StepParams s[2]) {
+  std::memset(s, 0, 2 * sizeof(StepParams));
+  s[0].gam = 2.0; s[1].gam = 2.0;
+  s[0].rad = 1e300; s[1].rad = 1e300;
+}
+
+int check_err(impz_bunch_t b) {
+  unsigned int err = 0;
+  CK(cudaMemcpyAsync(&err, &b->st->err, sizeof(err), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  if (err & DERR_NONFINITE) return IMPZ_ERR_NONFINITE;
+  if (err & DERR_SLOT) return IMPZ_ERR_STATE;
+  return IMPZ_OK;
+}
+
+int ensure_steps(impz_bunch_t b, int n) {
+  if (n <= b->dsteps_cap) return IMPZ_OK;
+  if (b->dsteps) cudaFree(b->dsteps);
+  b->dsteps = nullptr;
+  CK(dalloc(&b->dsteps, (size_t)n));
+  b->dsteps_cap = n;
+  return IMPZ_OK;
+}
+
+int ensure_mom(impz_bunch_t b, int rows) {
+  if (rows <= b->mom_cap) return IMPZ_OK;
+  if (b->mom_out) cudaFree(b->mom_out);
+  b->mom_out = nullptr;
+  CK(dalloc(&b->mom_out, (size_t)rows * IMPZ_MOMREC));
+  b->mom_cap = rows;
+  return IMPZ_OK;
+}
+
+template <typename C>
+void fill_tw(std::vector<C>& v, int n) {
+  v.resize(n / 2 > 0 ? n / 2 : 1);
+  for (int k = 0; k < n / 2; k++) {
+    const double a = -2.0 * M_PI * (double)k / (double)n;
+    v[k].x = (decltype(v[k].x))std::cos(a);
+    v[k].y = (decltype(v[k].y))std::sin(a);
+  }
+}
+
+void free_bunch(impz_bunch_t b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (int p = 0; p < 2; p++) {
+    for (int c = 0; c < 6; c++) cudaFree(b->pbuf[p][c]);
+    cudaFree(b->ids[p]);
+  }
+  void* ptrs[] = {b->rho, b->counts, b->cursor, b->bsum, b->spec, b->F, b->Gt, b->ghat,
+                  b->phi, b->efield, b->tw[0], b->tw[1], b->tw[2], b->tw64[0], b->tw64[1],
+                  b->tw64[2], b->st, b->dsteps, b->dfine, b->mom_part, b->rng_part,
+                  b->mom_out, b->mom_fine};
+  for (void* p : ptrs) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+}  // namespace
+
+// =====================================================================
+extern "C" {
+
+const char* impz_version(void) { return "impz_b200 0.1 (sm_100a)"; }
+
+const char* impz_error_string(int code) {
+  switch (code) {
+    case IMPZ_OK: return "ok";
+    case IMPZ_ERR_ARG: return "invalid argument";
+    case IMPZ_ERR_NOMEM: return "out of memory";
+    case IMPZ_ERR_CUDA: return "CUDA error";
+    case IMPZ_ERR_UNSUPPORTED: return "unsupported element or option";
+    case IMPZ_ERR_NONUNIFORM: return "particles differ in q/m or charge weight";
+    case IMPZ_ERR_STATE: return "call out of order";
+    case IMPZ_ERR_NONFINITE: return "non-finite particle coordinate";
+    case IMPZ_ERR_NODEVICE: return "no CUDA device";
+    case IMPZ_ERR_BUDGET: return "footprint above budget";
+    default: return "unknown error";
+  }
+}
+
+const char* impz_last_cuda_error(void) { return g_cuda_err; }
+
+int impz_set_device(int device) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return IMPZ_ERR_NODEVICE;
+  if (device < 0 || device >= n) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(device));
+  return IMPZ_OK;
+}
+
+int impz_bunch_create(const double* pts, long long n, double current, double mass,
+                      double charge, double freq, const double refptcl[6], int nx, int ny,
+                      int nz, int form, int flags, impz_bunch_t* out) {
+  if (!out || !refptcl || n < 1 || !pts) return IMPZ_ERR_ARG;
+  *out = nullptr;
+  if (!is_pow2(nx) || !is_pow2(ny) || !is_pow2(nz)) return IMPZ_ERR_UNSUPPORTED;
+  if (nx > 64 || ny > 64) return IMPZ_ERR_UNSUPPORTED;  // xy plane must fit one block
+  if (nz > 4096) return IMPZ_ERR_UNSUPPORTED;
+  if (form != IMPZ_FORM_FP64 && form != IMPZ_FORM_FP32CONV) return IMPZ_ERR_ARG;
+  if (!(mass > 0) || !(freq > 0) || charge == 0.0) return IMPZ_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return IMPZ_ERR_NODEVICE;
+  impz_bunch_t b = new impz_bunch_s();
+  cudaGetDevice(&b->device);
+  b->form = form;
+  b->flags = flags;
+  b->cap = n;
+  b->nx = nx; b->ny = ny; b->nz = nz;
+  b->G = (long long)nx * ny * nz;
+  b->P = make_phys(freq);
+  b->freq = freq;
+  b->current0 = current;
+  std::memcpy(b->refptcl, refptcl, sizeof(b->refptcl));
+  b->sp.charge = charge;
+  b->sp.mass = mass;
+  b->sp.qmi = pts[6];
+  b->weight = pts[7];
+  b->k.Scxl = b->P.Scxl;
+  b->k.xk = 1 / b->P.Scxl;
+  b->k.Clight = b->P.Clight;
+  b->k.Pi = b->P.Pi;
+  b->k.Scfreq = b->P.Scfreq;
+  b->k.mass = mass;
+  b->k.charge = charge;
+  b->k.qm0 = charge / mass;
+  b->k.qmi = b->sp.qmi;
+  // fixed point: no cell can exceed n units, so n * 2^fixbits < 2^62
+  b->fixbits = std::min(40, 62 - ilog2i(n + 1));
+  int rc = IMPZ_OK;
+#define ALLOC(call)                                   \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) {                          \
+      rc = (e_ == cudaErrorMemoryAllocation) ? IMPZ_ERR_NOMEM : cuda_fail(e_, #call); \
+      free_bunch(b);                                  \
+      return rc;                                      \
+    }                                                 \
+  } while (0)
+  ALLOC(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  for (int p = 0; p < 2; p++)
+    for (int c = 0; c < 6; c++) ALLOC(dalloc(&b->pbuf[p][c], (size_t)n));
+  if (flags & IMPZ_FLAG_TRACK_IDS) {
+    ALLOC(dalloc(&b->ids[0], (size_t)n));
+    ALLOC(dalloc(&b->ids[1], (size_t)n));
+  }
+  const size_t G = (size_t)b->G;
+  ALLOC(dalloc(&b->rho, G));
+  ALLOC(cudaMemsetAsync(b->rho, 0, G * sizeof(unsigned long long), b->stream));
+  ALLOC(dalloc(&b->counts, G + 1));
+  ALLOC(cudaMemsetAsync(b->counts, 0, (G + 1) * sizeof(int), b->stream));
+  ALLOC(dalloc(&b->cursor, G + 1));
+  b->nscan = (int)((G + 1 + (1u << IMPZ_SCAN_LOG) - 1) >> IMPZ_SCAN_LOG);
+  ALLOC(dalloc(&b->bsum, (size_t)b->nscan));
+  const size_t esz = b->f32() ? sizeof(float) : sizeof(double);
+  const size_t nspec = (size_t)(nx + 1) * 2 * ny * nz;
+  const size_t noct = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+  ALLOC(cudaMalloc(&b->spec, nspec * 2 * esz));
+  ALLOC(dalloc(&b->F, (size_t)(nx + 2) * (ny + 2) * (nz + 2)));
+  ALLOC(dalloc(&b->Gt, noct));
+  ALLOC(cudaMalloc(&b->ghat, noct * esz));
+  ALLOC(cudaMalloc(&b->phi, G * esz));
+  ALLOC(cudaMalloc(&b->efield, 4 * G * esz));
+  const int lens[3] = {2 * nx, 2 * ny, 2 * nz};
+  for (int d = 0; d < 3; d++) {
+    std::vector<double2> t64;
+    fill_tw(t64, lens[d]);
+    ALLOC(dalloc(&b->tw64[d], t64.size()));
+    ALLOC(cudaMemcpy(b->tw64[d], t64.data(), t64.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    if (b->f32()) {
+      std::vector<float2> t32;
+      fill_tw(t32, lens[d]);
+      ALLOC(cudaMalloc(&b->tw[d], t32.size() * sizeof(float2)));
+      ALLOC(cudaMemcpy(b->tw[d], t32.data(), t32.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    } else {
+      ALLOC(cudaMalloc(&b->tw[d], t64.size() * sizeof(double2)));
+      ALLOC(cudaMemcpy(b->tw[d], t64.data(), t64.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    }
+  }
+  ALLOC(dalloc(&b->st, 1));
+  ALLOC(dalloc(&b->dfine, 2));
+  ALLOC(dalloc(&b->mom_fine, IMPZ_MOMREC));
+  b->grid_adv = (int)std::min<long long>((n + IMPZ_ADV_BLOCK - 1) / IMPZ_ADV_BLOCK,
+                                         (long long)(b->f32() ? fast::max_blocks_advance(true)
+                                                              : exact::max_blocks_advance(false)));
+  b->grid_dep = (int)std::min<long long>(
+      (n + (long long)IMPZ_DEP_BLOCK * IMPZ_DEP_PPT - 1) / ((long long)IMPZ_DEP_BLOCK * IMPZ_DEP_PPT),
+      (long long)exact::max_blocks_deposit());
+  if (b->grid_adv < 1) b->grid_adv = 1;
+  if (b->grid_dep < 1) b->grid_dep = 1;
+  ALLOC(dalloc(&b->mom_part, (size_t)b->grid_adv * IMPZ_RAW_LEN));
+  ALLOC(dalloc(&b->rng_part, (size_t)b->grid_adv * 8));
+  // upload Pts1(9,n) and split it into SoA columns
+  {
+    double* aos = nullptr;
+    unsigned int* bad = nullptr;
+    ALLOC(dalloc(&aos, (size_t)9 * n));
+    ALLOC(dalloc(&bad, 1));
+    ALLOC(cudaMemsetAsync(bad, 0, sizeof(unsigned int), b->stream));
+    ALLOC(cudaMemcpyAsync(aos, pts, (size_t)9 * n * sizeof(double), cudaMemcpyHostToDevice,
+                          b->stream));
+    k_aos_to_soa<<<1184, 256, 0, b->stream>>>(aos, n, b->pbuf[0][0], b->pbuf[0][1],
+                                              b->pbuf[0][2], b->pbuf[0][3], b->pbuf[0][4],
+                                              b->pbuf[0][5], b->ids[0], b->sp.qmi, b->weight,
+                                              bad);
+    unsigned int hbad = 0;
+    ALLOC(cudaMemcpyAsync(&hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, b->stream));
+    ALLOC(cudaStreamSynchronize(b->stream));
+    cudaFree(aos);
+    cudaFree(bad);
+    if (hbad) {
+      free_bunch(b);
+      return IMPZ_ERR_NONUNIFORM;
+    }
+  }
+  DevState hs;
+  std::memset(&hs, 0, sizeof(hs));
+  hs.current = current;
+  hs.npt = n;
+  hs.nlocal = n;
+  hs.nlive = n;
+  ALLOC(cudaMemcpyAsync(b->st, &hs, sizeof(hs), cudaMemcpyHostToDevice, b->stream));
+  ALLOC(cudaStreamSynchronize(b->stream));
+#undef ALLOC
+  b->bytes = (size_t)n * (12 * sizeof(double) + ((flags & IMPZ_FLAG_TRACK_IDS) ? 16 : 0)) +
+             G * (8 + 4 + 4) + nspec * 2 * esz + noct * (8 + esz) +
+             (size_t)(nx + 2) * (ny + 2) * (nz + 2) * 8 + G * esz * 5;
+  *out = b;
+  return IMPZ_OK;
+}
+
+int impz_bunch_destroy(impz_bunch_t b) {
+  if (!b) return IMPZ_ERR_ARG;
+  free_bunch(b);
+  return IMPZ_OK;
+}
+
+void* impz_bunch_stream(impz_bunch_t b) { return b ? (void*)b->stream : nullptr; }
+
+int impz_bunch_info(impz_bunch_t b, double info[11]) {
+  if (!b || !info) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  DevState hs;
+  CK(cudaMemcpyAsync(&hs, b->st, sizeof(hs), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  info[0] = hs.current;
+  info[1] = (double)hs.npt;
+  info[2] = (double)hs.nlocal;
+  for (int c = 0; c < 6; c++) info[3 + c] = b->refptcl[c];
+  info[9] = b->z;
+  info[10] = (double)b->bytes;
+  return IMPZ_OK;
+}
+
+int impz_bunch_download(impz_bunch_t b, double* pts, long long cap, long long* n) {
+  if (!b || !pts || !n) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  DevState hs;
+  CK(cudaMemcpyAsync(&hs, b->st, sizeof(hs), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  *n = hs.nlocal;
+  if (hs.nlocal > cap) return IMPZ_ERR_ARG;
+  double* aos = nullptr;
+  CK(dalloc(&aos, (size_t)9 * std::max<long long>(hs.nlocal, 1)));
+  const int p = b->parity;
+  k_soa_to_aos<<<1184, 256, 0, b->stream>>>(aos, hs.nlocal, b->pbuf[p][0], b->pbuf[p][1],
+                                            b->pbuf[p][2], b->pbuf[p][3], b->pbuf[p][4],
+                                            b->pbuf[p][5], b->ids[p], b->sp.qmi, b->weight);
+  cudaError_t e = cudaMemcpyAsync(pts, aos, (size_t)9 * hs.nlocal * sizeof(double),
+                                  cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  cudaFree(aos);
+  if (e != cudaSuccess) return cuda_fail(e, "download");
+  return IMPZ_OK;
+}
+
+// ---- per-step surface --------------------------------------------------
+static int run_fine_advance(impz_bunch_t b, const StepParams host[2], int kick, int post,
+                            int pre, double* rec) {
+  int r = upload_fine(b, host);
+  if (r) return r;
+  AdvanceArgs a = advance_args(b, b->dfine, 0, kick, post, pre, b->mom_fine, 0);
+  CK(launch_adv(b, a));
+  if (kick) b->parity ^= 1;
+  if (rec) {
+    CK(cudaMemcpyAsync(rec, b->mom_fine, IMPZ_MOMREC * sizeof(double), cudaMemcpyDeviceToHost,
+                       b->stream));
+  }
+  return check_err(b);
+}
+
+int impz_map_half(impz_bunch_t b, const impz_elem_t* e, double zedge, double* z, double tau,
+                  int nst, int* ihlf) {
+  if (!b || !e || !z || !ihlf) return IMPZ_ERR_ARG;
+  if (e->type == 4) return IMPZ_ERR_UNSUPPORTED;  // bends use impz_bend_sector
+  CK(cudaSetDevice(b->device));
+  StepParams h[2];
+  blank_steps(h);
+  int r = half_map_ops(b->P, *e, zedge, *z, tau, nst, *ihlf, b->refptcl, b->sp, h[0].post);
+  if (r) return r;
+  r = run_fine_advance(b, h, 0, 1, 0, nullptr);
+  if (r) return r;
+  *z = *z + tau;
+  *ihlf = *ihlf + 1;
+  b->z = *z;
+  return IMPZ_OK;
+}
+
+int impz_bend_entry(impz_bunch_t b, const impz_elem_t* e) {
+  if (!b || !e || e->type != 4) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  StepParams h[2];
+  blank_steps(h);
+  int r = bend_entry_ops(b->P, *e, b->refptcl, b->sp, b->bend, h[0].post);
+  if (r) return r;
+  return run_fine_advance(b, h, 0, 1, 0, nullptr);
+}
+
+int impz_bend_sector(impz_bunch_t b, double* z, double tau) {
+  if (!b || !z || !b->bend.active) return IMPZ_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  StepParams h[2];
+  blank_steps(h);
+  bend_sector_op(b->P, b->bend, tau, b->sp, h[0].post);
+  int r = run_fine_advance(b, h, 0, 1, 0, nullptr);
+  if (r) return r;
+  *z = *z + tau;
+  b->z = *z;
+  return IMPZ_OK;
+}
+
+int impz_bend_exit(impz_bunch_t b) {
+  if (!b || !b->bend.active) return IMPZ_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  StepParams h[2];
+  blank_steps(h);
+  bend_exit_op(b->P, b->bend, b->sp, h[0].post);
+  b->bend.active = false;
+  return run_fine_advance(b, h, 0, 1, 0, nullptr);
+}
+
+int impz_sc_prepare(impz_bunch_t b, double piperad, double piperad2, long long* nptot,
+                    double ptrange[6], double range[6], double msize[3]) {
+  if (!b) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  StepParams h[2];
+  blank_steps(h);
+  h[0].range_next = 1;
+  h[1].gam = -b->refptcl[5];
+  h[1].rad = (piperad + piperad2) / 2;
+  int r = run_fine_advance(b, h, 0, 0, 1, nullptr);
+  if (r) return r;
+  DevState hs;
+  CK(cudaMemcpyAsync(&hs, b->st, sizeof(hs), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  if (nptot) *nptot = hs.npt;
+  if (ptrange) std::memcpy(ptrange, hs.geom.ptrange, 6 * sizeof(double));
+  if (range) std::memcpy(range, hs.geom.range, 6 * sizeof(double));
+  if (msize) std::memcpy(msize, hs.geom.h, 3 * sizeof(double));
+  b->sc_gam = h[1].gam;
+  b->sc_rad = h[1].rad;
+  b->stage = ST_PREPARED;
+  return IMPZ_OK;
+}
+
+int impz_deposit(impz_bunch_t b, double* chgdens, int* counts) {
+  if (!b) return IMPZ_ERR_ARG;
+  if (b->stage != ST_PREPARED) return IMPZ_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  StepParams h[2];
+  blank_steps(h);
+  h[0].gam = b->sc_gam;
+  h[0].rad = b->sc_rad;
+  int r = upload_fine(b, h);
+  if (r) return r;
+  DepositArgs d = deposit_args(b, b->dfine, 0);
+  CK(exact::launch_deposit(d, b->grid_dep, b->stream));
+  if (counts) {
+    CK(cudaMemcpyAsync(counts, b->counts, b->G * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  }
+  std::vector<long long> q;
+  if (chgdens) {
+    q.resize((size_t)b->G);
+    CK(cudaMemcpyAsync(q.data(), b->rho, b->G * sizeof(long long), cudaMemcpyDeviceToHost,
+                       b->stream));
+  }
+  CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  if (chgdens) {
+    const double qs = b->weight * std::ldexp(1.0, -b->fixbits);
+    for (long long i = 0; i < b->G; i++) chgdens[i] = (double)q[(size_t)i] * qs;
+  }
+  b->stage = ST_DEPOSITED;
+  return IMPZ_OK;
+}
+
+int impz_poisson_open(impz_bunch_t b, double* phi) {
+  if (!b) return IMPZ_ERR_ARG;
+  if (b->stage != ST_DEPOSITED) return IMPZ_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  PoissonBuffers pb = poisson_of(b);
+  if (b->f32()) {
+    CK(launch_green<float>(pb, b->stream));
+    CK(launch_convolve<float>(pb, b->stream));
+  } else {
+    CK(launch_green<double>(pb, b->stream));
+    CK(launch_convolve<double>(pb, b->stream));
+  }
+  if (phi) {
+    if (b->f32()) {
+      double* tmp = nullptr;
+      CK(dalloc(&tmp, (size_t)b->G));
+      k_to_double<<<1184, 256, 0, b->stream>>>((const float*)b->phi, b->G, b->weight, tmp);
+      CK(cudaMemcpyAsync(phi, tmp, b->G * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+      CK(cudaStreamSynchronize(b->stream));
+      cudaFree(tmp);
+    } else {
+      CK(cudaMemcpyAsync(phi, b->phi, b->G * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  b->stage = ST_SOLVED;
+  return IMPZ_OK;
+}
+
+int impz_kick(impz_bunch_t b, double tau, double* egrid) {
+  if (!b) return IMPZ_ERR_ARG;
+  if (b->stage != ST_SOLVED) return IMPZ_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  PoissonBuffers pb = poisson_of(b);
+  if (b->f32()) { CK(launch_efield<float>(pb, b->stream)); }
+  else { CK(launch_efield<double>(pb, b->stream)); }
+  if (egrid) {
+    double* tmp = nullptr;
+    CK(dalloc(&tmp, (size_t)3 * b->G));
+    k_e4_to_grids<<<1184, 256, 0, b->stream>>>(b->efield, b->f32() ? 1 : 0, b->G, tmp);
+    CK(cudaMemcpyAsync(egrid, tmp, 3 * b->G * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    cudaFree(tmp);
+    if (b->f32())
+      for (long long i = 0; i < 3 * b->G; i++) egrid[i] *= b->weight;
+  }
+  StepParams h[2];
+  blank_steps(h);
+  h[0].sc = 1;
+  h[0].gam = b->sc_gam;
+  h[0].rad = b->sc_rad;
+  h[0].tau = tau;
+  b->stage = ST_IDLE;
+  return run_fine_advance(b, h, 1, 0, 0, nullptr);
+}
+
+int impz_moments(impz_bunch_t b, double rec[IMPZ_MOMREC]) {
+  if (!b || !rec) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  StepParams h[2];
+  blank_steps(h);
+  h[0].moments = 1;
+  int r = run_fine_advance(b, h, 0, 1, 0, rec);
+  if (r) return r;
+  CK(cudaStreamSynchronize(b->stream));
+  return IMPZ_OK;
+}
+
+int impz_diag_row(double z, const double rec[IMPZ_MOMREC], const double refptcl[6], double mass,
+                  double freq, double row[IMPZ_DIAG_LEN]) {
+  if (!rec || !refptcl || !row || !(freq > 0)) return IMPZ_ERR_ARG;
+  diag_row(make_phys(freq), z, rec, refptcl, mass, row);
+  return IMPZ_OK;
+}
+
+int impz_maplinear(const impz_elem_t* e, double zedge, double t, double tau, double refpt[6],
+                   double charge, double mass, double freq, double xm[36]) {
+  if (!e || !refpt || !xm || !(freq > 0)) return IMPZ_ERR_ARG;
+  const Phys P = make_phys(freq);
+  if (e->type == 1) {
+    if (e->mapstp < 1) return IMPZ_ERR_ARG;
+    maplinear_quad(P, t, tau, xm, refpt, e->val[0], e->mapstp, charge, mass);
+    return IMPZ_OK;
+  }
+  if (e->type == 103 && e->ndata > 1) {
+    if (e->mapstp < 1) return IMPZ_ERR_ARG;
+    maplinear_ccl(P, t, tau, xm, refpt, zedge, *e, charge, mass);
+    return IMPZ_OK;
+  }
+  return IMPZ_ERR_UNSUPPORTED;
+}
+
+int impz_count_steps(const impz_elem_t* elems, int nelem) {
+  if (!elems || nelem < 0) return IMPZ_ERR_ARG;
+  int k = 0;
+  for (int i = 0; i < nelem; i++) k += elems[i].nseg;
+  return k;
+}
+
+// ---- whole-lattice runner --------------------------------------------
+int impz_run_async(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
+  if (!b || (!elems && nelem > 0) || nelem < 0) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  CompiledLattice& L = b->lat;
+  double z = b->z;
+  double ref[6];
+  std::memcpy(ref, b->refptcl, sizeof(ref));
+  // conv1st/kick see Bcurr, the input beam current (AccSimulator.f90:1121)
+  int r = compile_lattice(b->P, elems, nelem, b->current0, b->sp, ref, &z, L);
+  if (r) return r;
+  const int K = L.nsteps;
+  if ((r = ensure_steps(b, K + 2))) return r;
+  if ((r = ensure_mom(b, K + 1))) return r;
+  CK(cudaMemcpyAsync(b->dsteps, L.steps.data(), (K + 2) * sizeof(StepParams),
+                     cudaMemcpyHostToDevice, b->stream));
+  // prologue: initial record, first half map, first conv1st
+  {
+    AdvanceArgs a = advance_args(b, b->dsteps, 0, 0, 1, 1, b->mom_out, 0);
+    CK(launch_adv(b, a));
+  }
+  for (int s = 1; s <= K; s++) {
+    const bool sc = L.steps[s].sc != 0;
+    if (sc) {
+      r = field_step(b, b->dsteps, s);
+      if (r) return r;
+    }
+    AdvanceArgs a = advance_args(b, b->dsteps, s, sc ? 1 : 0, 1, 1, b->mom_out, s);
+    CK(launch_adv(b, a));
+    if (sc) b->parity ^= 1;
+  }
+  std::memcpy(b->refptcl, ref, sizeof(ref));
+  b->z = z;
+  b->run_pending = true;
+  return IMPZ_OK;
+}
+
+int impz_run_fetch(impz_bunch_t b, double* recs, double* zs, int maxrec, int* nrec) {
+  if (!b || !b->run_pending) return IMPZ_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  const int rows = b->lat.nsteps + 1;
+  const int ncopy = std::min(rows, std::max(maxrec, 0));
+  if (recs && ncopy > 0)
+    CK(cudaMemcpyAsync(recs, b->mom_out, (size_t)ncopy * IMPZ_MOMREC * sizeof(double),
+                       cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  if (zs)
+    for (int i = 0; i < ncopy; i++) zs[i] = b->lat.zrec[i];
+  if (nrec) *nrec = rows;
+  b->run_pending = false;
+  return check_err(b);
+}
+
+int impz_run(impz_bunch_t b, const impz_elem_t* elems, int nelem, double* recs, double* zs,
+             int maxrec, int* nrec) {
+  int r = impz_run_async(b, elems, nelem);
+  if (r) return r;
+  return impz_run_fetch(b, recs, zs, maxrec, nrec);
+}
+
+}  // extern "C"

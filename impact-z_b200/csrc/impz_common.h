@@ -1,0 +1,145 @@
+// impz_common.h -- types shared by the host runtime and the sm_100a kernels.
+//
+// Particle state lives on the device as six FP64 structure-of-arrays columns
+// (x/Scxl, gamma*beta_x, y/Scxl, gamma*beta_y, phase, gamma0-gamma), the
+// first six rows of the reference's Pts1(9,N) (src/Appl/BeamBunch.f90:9-12).
+// Rows 7 (q/m) and 8 (charge weight) are per-bunch constants for the single
+// species the map integrator supports (BeamBunch.f90:13-14); row 9 (id) is an
+// optional int64 column carried through the per-step particle sort.
+#pragma once
+#include <stdint.h>
+
+#define IMPZ_RAW_LEN 44     // 37 moment sums, 6 |max|, 1 max r^2 (Output.f90:133-245)
+#define IMPZ_MAXOPS 4       // map ops per program
+#define IMPZ_OPC 40         // coefficients per map op
+
+namespace impz {
+
+// One per-particle transfer map, with every constant the per-particle loop
+// of the reference routine needs precomputed on the host.
+enum MapKind : int {
+  MAP_NONE = 0,
+  MAP_DRIFT = 1,     // drift1_BeamBunch bitype 0 (BeamBunch.f90:276-298)
+  MAP_XM6 = 2,       // 6x6 linear map loop (BeamBunch.f90:310-320)
+  MAP_KQUAD = 3,     // transfmapK_Quadrupole (Quadrupole.f90:509-607)
+  MAP_IDEALRF = 4,   // ideal RF gap (BeamBunch.f90:324-440)
+  MAP_FPOL = 5,      // Fpol_Dipole (Dipole.f90:466-526)
+  MAP_BPOL = 6,      // Bpol_Dipole (Dipole.f90:528-591)
+  MAP_SECTOR = 7,    // Sector_Dipole (Dipole.f90:693-788)
+};
+
+struct MapOp {
+  int kind;
+  int flags;   // XM6: bitmask of nonzero entries (36 bits in c[36..]); RF: 1 entrance, 2 exit
+  int iparam;  // RF: 2*nseg
+  int pad;
+  double c[IMPZ_OPC];
+};
+
+struct MapProgram {
+  int nops;
+  int pad;
+  MapOp ops[IMPZ_MAXOPS];
+};
+
+// Everything one step needs that the host knows in advance.  Entry s of a
+// step table describes step s; the particle pass of step s applies `post`,
+// records moments, applies `pre_next` and evaluates conv1st for step s+1
+// with steps[s+1].gam and steps[s+1].rad.
+struct StepParams {
+  MapProgram post;     // second half map of this step (after the kick)
+  MapProgram pre_next; // first half map of the next step (+ pole faces)
+  int sc;              // this step kicks (a deposit and a field solve preceded it)
+  int moments;         // record diagnostics after `post`
+  int range_next;      // evaluate conv1st of step s+1 after `pre_next`
+  int pad;
+  double gam;          // -refptcl(6) during this step's conv1st/kick
+  double tau;          // tau2 of the kick
+  double rad;          // (piperad+piperad2)/2 for this step's conv1st loss test
+  double pad2;
+};
+
+#define IMPZ_MOMREC 48   // per recorded step: 44 raw values, npt, nlocal, current, spare
+
+// update_CompDom output for one step, plus the conv1st range that fed it.
+struct Geom {
+  double ptrange[6];   // raw particle range (conv1st)
+  double range[6];     // xmin,xmax,ymin,ymax,zmin,zmax after padding
+  double h[3];         // hx,hy,hz
+  double hi[3];        // 1.0/h
+};
+
+struct DevState {
+  Geom geom;
+  double current;      // BeamBunch%Current after the loss rescale
+  double xycon, tcon;  // scatter1 kick constants of the current step
+  long long npt;       // BeamBunch%Npt
+  long long nlocal;    // particles stored in the current buffer
+  long long nlive;     // particles that survive the pending conv1st
+  int step;            // index of the current step in the step table
+  int parity;          // which particle buffer holds the state
+  unsigned int err;    // sticky error bits (IMPZ_DERR_*)
+  unsigned int done_range, done_mom, done_scan;
+  unsigned int pad0;
+  double charge_unit;  // FP64 form: weight * 2^-fixbits (grid value per quantum)
+  double rhomax;       // unused placeholder for alignment
+};
+
+enum DevErr : unsigned int {
+  DERR_NONFINITE = 1u,   // a particle coordinate became Inf/NaN
+  DERR_OUTSIDE = 2u,     // a live particle fell outside the deposit grid
+  DERR_FIXOVF = 4u,      // fixed-point charge grid overflow guard
+  DERR_SLOT = 8u,        // a sorted slot fell outside the buffer (deposit/pass mismatch)
+};
+
+struct Consts {  // per-bunch constants (PhysConst.f90:25-35 and the species)
+  double Scxl, xk, Clight, Pi, Scfreq;
+  double mass, charge, qm0, qmi;  // qm0 = Charge/Mass, qmi = Pts1(7,:)
+};
+
+// Launch arguments of the fused particle pass.  The step index is either
+// fixed by the host or read from DevState::step, so one captured CUDA graph
+// can replay every step of a lattice.
+struct AdvanceArgs {
+  const double* in[6];
+  double* out[6];
+  const long long* id_in;   // may be null (ids not tracked)
+  long long* id_out;
+  const StepParams* steps;
+  DevState* st;
+  int nx, ny, nz;
+  int pad0;
+  long long cap;            // particle capacity of the output buffer
+  const void* efield;       // per node {Ex,Ey,Ez,0}: double in the FP64 form, float otherwise
+  double efield_scale;      // FP32 form: charge weight (field solved for unit charges)
+  int* cursor;              // per-cell sort cursors (scan-block local offsets)
+  const int* bsum;          // exclusive offset of each scan block
+  double* mom_part;         // [gridDim][IMPZ_RAW_LEN]
+  double* rng_part;         // [gridDim][8]
+  double* mom_out;          // [records][IMPZ_MOMREC]
+  Consts k;
+  int fixed_step;           // >= 0: step index; < 0: read and advance DevState::step
+  int kick;                 // 1: gather + kick (steps[s].sc must be set)
+  int do_post;              // apply steps[s].post (+ moments if steps[s].moments)
+  int do_pre;               // apply steps[s].pre_next (+ conv1st of s+1 if range_next)
+  int mom_index;            // record row for fixed_step launches
+  int pad1;
+};
+
+struct DepositArgs {
+  const double* in[6];
+  const StepParams* steps;
+  DevState* st;
+  int fixed_step;
+  int nx, ny, nz;
+  int fixbits;
+  int pad0;
+  unsigned long long* rho;  // G int64 (two's complement) accumulators
+  int* counts;              // G+1 per-cell particle counts (slot G: live but outside)
+  double xl;
+};
+
+#define IMPZ_SCAN_LOG 13      // 8192 cells per scan block
+#define IMPZ_DEP_TILE 8192    // deposit tile: int64 entries (64 KB) + int32 counts (32 KB)
+
+}  // namespace impz

@@ -1,0 +1,636 @@
+// impz_host.cpp -- host-side builders for the B200 step pipeline.
+//
+// Everything here runs once per element or step on the host: the linear
+// maps integrated by RK6, the per-element constants the device map ops use,
+// the compilation of a lattice into a step table, and the diagnostic
+// formulas.  Built with -ffp-contract=off so the arithmetic rounds like the
+// reference's x86-64 build; expressions keep the reference's left-to-right
+// evaluation order (cited per routine).
+#include "impz_host.h"
+
+#include <cmath>
+#include <cstring>
+
+namespace impz {
+
+Phys make_phys(double freq) {
+  // PhysConst.f90:29-34
+  Phys P;
+  P.Clight = 299792458.0;
+  P.Pi = 2 * std::asin(1.0);
+  P.Scxl = P.Clight / (2 * P.Pi * freq);
+  P.Rad2deg = 180.0 / P.Pi;
+  P.Scfreq = freq;
+  return P;
+}
+
+// ---------------------------------------------------------------------
+// 8-stage RK6 of the reference's rk6i_* routines (Quadrupole.f90:202-252)
+namespace {
+const int NV = 18;
+
+template <typename RHS>
+void rk6(double h, int ns, double t, double* y, RHS rhs) {
+  double yt[NV], a[NV], b[NV], c[NV], d[NV], e[NV], f[NV], g[NV], o[NV], p[NV];
+  const double tint = t;
+  double tt;
+  for (int i = 1; i <= ns; i++) {
+    rhs(t, y, f);
+    for (int v = 0; v < NV; v++) a[v] = h * f[v];
+    for (int v = 0; v < NV; v++) yt[v] = y[v] + a[v] / 9.0;
+    tt = t + h / 9.0;
+    rhs(tt, yt, f);
+    for (int v = 0; v < NV; v++) b[v] = h * f[v];
+    for (int v = 0; v < NV; v++) yt[v] = y[v] + (a[v] + 3.0 * b[v]) / 24.0;
+    tt = t + h / 6.0;
+    rhs(tt, yt, f);
+    for (int v = 0; v < NV; v++) c[v] = h * f[v];
+    for (int v = 0; v < NV; v++) yt[v] = y[v] + (a[v] - 3.0 * b[v] + 4.0 * c[v]) / 6.0;
+    tt = t + h / 3.0;
+    rhs(tt, yt, f);
+    for (int v = 0; v < NV; v++) d[v] = h * f[v];
+    for (int v = 0; v < NV; v++)
+      yt[v] = y[v] + (278.0 * a[v] - 945.0 * b[v] + 840.0 * c[v] + 99.0 * d[v]) / 544.0;
+    tt = t + .5 * h;
+    rhs(tt, yt, f);
+    for (int v = 0; v < NV; v++) e[v] = h * f[v];
+    for (int v = 0; v < NV; v++)
+      yt[v] = y[v] +
+              (-106.0 * a[v] + 273.0 * b[v] - 104.0 * c[v] - 107.0 * d[v] + 48.0 * e[v]) / 6.0;
+    tt = t + 2.0 * h / 3.0;
+    rhs(tt, yt, f);
+    for (int v = 0; v < NV; v++) g[v] = h * f[v];
+    for (int v = 0; v < NV; v++)
+      yt[v] = y[v] + (110974.0 * a[v] - 236799.0 * b[v] + 68376.0 * c[v] + 103803.0 * d[v] -
+                      10240.0 * e[v] + 1926.0 * g[v]) /
+                         45648.0;
+    tt = t + 5.0 * h / 6.0;
+    rhs(tt, yt, f);
+    for (int v = 0; v < NV; v++) o[v] = h * f[v];
+    for (int v = 0; v < NV; v++)
+      yt[v] = y[v] + (-101195.0 * a[v] + 222534.0 * b[v] - 71988.0 * c[v] - 26109.0 * d[v] -
+                      2.e4 * e[v] - 72.0 * g[v] + 22824.0 * o[v]) /
+                         25994.0;
+    tt = t + h;
+    rhs(tt, yt, f);
+    for (int v = 0; v < NV; v++) p[v] = h * f[v];
+    for (int v = 0; v < NV; v++)
+      y[v] = y[v] + (41.0 * a[v] + 216.0 * c[v] + 27.0 * d[v] + 272.0 * e[v] + 27.0 * g[v] +
+                     216.0 * o[v] + 41.0 * p[v]) /
+                        840.0;
+    t = tint + i * h;
+  }
+}
+
+// linear part of every intfunc1_* (Quadrupole.f90:291-304)
+void lin_rhs(double Scxl, const double* y, double* f, double s11, double s33, double s55) {
+  f[6] = y[7] / Scxl;
+  f[7] = -s11 * y[6];
+  f[8] = y[9] / Scxl;
+  f[9] = -s11 * y[8];
+  f[10] = y[11] / Scxl;
+  f[11] = -s33 * y[10];
+  f[12] = y[13] / Scxl;
+  f[13] = -s33 * y[12];
+  f[14] = y[15] / Scxl;
+  f[15] = -s55 * y[14];
+  f[16] = y[17] / Scxl;
+  f[17] = -s55 * y[16];
+}
+
+void y_start(double* y, const double refpt[6]) {
+  std::memset(y, 0, NV * sizeof(double));
+  y[4] = refpt[4];
+  y[5] = refpt[5];
+  y[6] = 1.0; y[9] = 1.0; y[10] = 1.0; y[13] = 1.0; y[14] = 1.0; y[17] = 1.0;
+}
+
+// the xm(6,6) assembly of maplinear_* (Quadrupole.f90:183-198)
+void xm_from_y(double xm[36], const double* y, double squi, double squf, double sqi3,
+               double sqf3, double dlti, double dltf, double thli, double thlf) {
+  std::memset(xm, 0, 36 * sizeof(double));
+  auto X = [&](int j, int k) -> double& { return xm[(j - 1) + 6 * (k - 1)]; };
+  const double* Y = y - 1;
+  X(1, 1) = Y[7] * squi / squf + Y[9] * squi / squf * dlti;
+  X(2, 1) = (Y[8] - Y[7] * dltf) * squi * squf + (Y[10] - Y[9] * dltf) * squi * squf * dlti;
+  X(1, 2) = Y[9] / (squi * squf);
+  X(2, 2) = (Y[10] - Y[9] * dltf) * squf / squi;
+  X(3, 3) = Y[11] * squi / squf + Y[13] * squi / squf * dlti;
+  X(4, 3) = (Y[12] - Y[11] * dltf) * squi * squf + (Y[14] - Y[13] * dltf) * squi * squf * dlti;
+  X(3, 4) = Y[13] / (squi * squf);
+  X(4, 4) = (Y[14] - Y[13] * dltf) * squf / squi;
+  X(5, 5) = Y[15] * sqi3 / sqf3 + Y[17] * sqi3 / sqf3 * thli;
+  X(6, 5) = (Y[16] - Y[15] * thlf) * sqi3 * sqf3 + (Y[18] - Y[17] * thlf) * sqi3 * sqf3 * thli;
+  X(5, 6) = Y[17] / (sqi3 * sqf3);
+  X(6, 6) = (Y[18] - Y[17] * thlf) * sqf3 / sqi3;
+}
+
+void uvals(double g, double& u, double& squ, double& sq3) {
+  const double beta = std::sqrt(g * g - 1.) / g;
+  u = g * beta;
+  squ = std::sqrt(u);
+  const double s = std::sqrt(u);
+  sq3 = s * s * s;
+}
+}  // namespace
+
+void maplinear_quad(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                    double gradient, int mapstp, double chg, double mass) {
+  // maplinear_Quadrupole (Quadrupole.f90:120-200), intfunc1 (254-305)
+  double y[NV];
+  y_start(y, refpt);
+  const double h = tau / mapstp;
+  double ui, squi, sqi3, uf, squf, sqf3;
+  uvals(-refpt[5], ui, squi, sqi3);
+  const double qmcc = chg / mass;
+  rk6(h, mapstp, t, y, [&](double, const double* yy, double* f) {
+    f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+    const double gamma0 = -yy[5];
+    const double beta0 = std::sqrt(gamma0 * gamma0 - 1.) / gamma0;
+    const double gbet = std::sqrt((gamma0 - 1.0) * (gamma0 + 1.0));
+    f[4] = 1.0 / (beta0 * P.Scxl);
+    f[5] = 0.0;
+    const double brho = gbet / P.Clight / qmcc;
+    const double s11 = gradient / brho * P.Scxl;
+    const double s33 = -(gradient / brho * P.Scxl);
+    lin_rhs(P.Scxl, yy, f, s11, s33, 0.0);
+  });
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  uvals(-refpt[5], uf, squf, sqf3);
+  xm_from_y(xm, y, squi, squf, sqi3, sqf3, 0.0, 0.0, 0.0, 0.0);
+}
+
+namespace {
+// getaxfldE_CCL (CCL.f90:331-365): bisection and linear interpolation
+void ccl_field(const impz_elem_t& e, double zedge, double z, double& ez1, double& ezp1,
+               double& ezpp1) {
+  const double escale = e.val[0];
+  const double zz = z - zedge;
+  int klo = 1, khi = e.ndata;
+  const double* zd = e.zdat - 1;
+  const double* ed = e.edat - 1;
+  const double* epd = e.epdat - 1;
+  const double* eppd = e.eppdat - 1;
+  while (khi - klo > 1) {
+    const int k = (khi + klo) / 2;
+    if (zd[k] > zz) khi = k;
+    else klo = k;
+  }
+  const double hstep = zd[khi] - zd[klo];
+  double slope = (ed[khi] - ed[klo]) / hstep;
+  ez1 = ed[klo] + slope * (zz - zd[klo]);
+  slope = (epd[khi] - epd[klo]) / hstep;
+  ezp1 = epd[klo] + slope * (zz - zd[klo]);
+  slope = (eppd[khi] - eppd[klo]) / hstep;
+  ezpp1 = eppd[klo] + slope * (zz - zd[klo]);
+  ez1 = ez1 * escale;
+  ezp1 = ezp1 * escale;
+  ezpp1 = ezpp1 * escale;
+}
+}  // namespace
+
+void maplinear_ccl(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                   double zedge, const impz_elem_t& e, double chg, double mass) {
+  // maplinear_CCL (CCL.f90:122-215), intfunc1_CCL (269-328)
+  const double Scxl = P.Scxl;
+  const double ww = e.val[1] / P.Scfreq;
+  // theta0 = Param(4)*asin(1.0)/90 with a default-real asin(1.0)
+  const double theta0 = e.val[2] * (double)std::asin(1.0f) / 90;
+  const double qmcc = chg / mass;
+  double y[NV];
+  y_start(y, refpt);
+  const double h = tau / e.mapstp;
+  const double gi = -refpt[5];
+  const double betai = std::sqrt(gi * gi - 1.) / gi;
+  double ui, squi, sqi3;
+  uvals(gi, ui, squi, sqi3);
+  double ein, e1in, e2in;
+  ccl_field(e, zedge, t, ein, e1in, e2in);
+  const double sinthi = std::sin(ww * refpt[4] + theta0);
+  const double costhi = std::cos(ww * refpt[4] + theta0);
+  const double uprimi = qmcc * ein / betai * costhi;
+  const double qpwi = 0.5 * qmcc * Scxl / (ui * ww);
+  const double dlti = Scxl * (0.5 * uprimi / ui - qpwi * e1in * sinthi);
+  const double thli = 1.5 * Scxl * (uprimi / ui);
+  rk6(h, e.mapstp, t, y, [&](double tt, const double* yy, double* f) {
+    double ez1, ezp1, ezpp1;
+    ccl_field(e, zedge, tt, ez1, ezp1, ezpp1);
+    f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+    const double gamma0 = -yy[5];
+    const double beta0 = std::sqrt(gamma0 * gamma0 - 1.) / gamma0;
+    const double sinphi = std::sin(ww * yy[4] + theta0);
+    const double cosphi = std::cos(ww * yy[4] + theta0);
+    const double rfdsgn = ez1 * cosphi;
+    f[4] = 1.0 / (beta0 * Scxl);
+    f[5] = -(qmcc * rfdsgn);
+    const double q = qmcc * rfdsgn / (beta0 * beta0) / (gamma0 * gamma0);
+    const double s11tmp =
+        0.5 * (1.0 + 0.5 * (gamma0 * gamma0)) * (q * q) +
+        qmcc * 0.5 / ((beta0 * beta0) * beta0) / ((gamma0 * gamma0) * gamma0) * ez1 * sinphi *
+            ww / Scxl;
+    double s55 = -(1.5 * qmcc / (beta0 * beta0) / gamma0 * ezp1 * cosphi) +
+                 ((beta0 * beta0) + 0.5) / ((beta0 * beta0) * beta0) / gamma0 * qmcc * ez1 *
+                     sinphi * ww / Scxl +
+                 1.5 * (1.0 - 0.5 * (gamma0 * gamma0)) * (q * q);
+    s55 = Scxl * s55;
+    lin_rhs(Scxl, yy, f, s11tmp * Scxl, s11tmp * Scxl, s55);
+  });
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  const double gf = -refpt[5];
+  const double betaf = std::sqrt(gf * gf - 1.) / gf;
+  double uf, squf, sqf3;
+  uvals(gf, uf, squf, sqf3);
+  double ef, e1f, e2f;
+  ccl_field(e, zedge, t + tau, ef, e1f, e2f);
+  const double sinthf = std::sin(ww * refpt[4] + theta0);
+  const double costhf = std::cos(ww * refpt[4] + theta0);
+  const double uprimf = qmcc * ef / betaf * costhf;
+  const double qpwf = 0.5 * qmcc * Scxl / (uf * ww);
+  const double dltf = Scxl * (0.5 * uprimf / uf - qpwf * e1f * sinthf);
+  const double thlf = 1.5 * Scxl * (uprimf / uf);
+  xm_from_y(xm, y, squi, squf, sqi3, sqf3, dlti, dltf, thli, thlf);
+}
+
+// ---------------------------------------------------------------------
+namespace {
+int push_op(MapProgram& prog, const MapOp& op) {
+  if (prog.nops >= IMPZ_MAXOPS) return IMPZ_ERR_UNSUPPORTED;
+  prog.ops[prog.nops++] = op;
+  return IMPZ_OK;
+}
+
+MapOp blank(MapKind k) {
+  MapOp op;
+  std::memset(&op, 0, sizeof(op));
+  op.kind = k;
+  return op;
+}
+
+MapOp op_xm6(const double xm[36]) {
+  MapOp op = blank(MAP_XM6);
+  unsigned long long mask = 0;
+  for (int q = 0; q < 36; q++) {
+    op.c[q] = xm[q];
+    if (xm[q] != 0.0) mask |= 1ull << q;
+  }
+  op.flags = (int)(unsigned)(mask & 0xffffffffull);
+  op.iparam = (int)(unsigned)(mask >> 32);
+  return op;
+}
+
+double pipe_radius(const impz_elem_t& e) {
+  // getradius_BeamLineElem (BeamLineElem.f90:500-552)
+  switch (e.type) {
+    case 0: return e.val[0];
+    case 1: return e.val[2];
+    case 4: return e.val[3];
+    default: return e.val[4];
+  }
+}
+}  // namespace
+
+int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, double tau,
+                 int nst, int ihlf, double refptcl[6], const Species& sp, MapProgram& prog) {
+  const double Scxl = P.Scxl;
+  if (e.type == 0) {
+    // exact drift (BeamBunch.f90:276-298)
+    const double gam0 = -refptcl[5];
+    const double gambet0 = std::sqrt(gam0 * gam0 - 1.0);
+    const double beta0 = gambet0 / gam0;
+    MapOp op = blank(MAP_DRIFT);
+    op.c[0] = gam0; op.c[1] = beta0; op.c[2] = tau; op.c[3] = Scxl;
+    refptcl[4] = refptcl[4] + tau / (Scxl * beta0);
+    return push_op(prog, op);
+  }
+  if (e.type == 1) {
+    const double x3 = e.val[1];
+    if (x3 < -10.0) return IMPZ_ERR_UNSUPPORTED;  // undulator map
+    if (x3 < -1.0e-6) {
+      // transfmapK_Quadrupole (Quadrupole.f90:509-607)
+      const double gambet0 = std::sqrt(refptcl[5] * refptcl[5] - 1.0);
+      const double beta0 = std::sqrt(1.0 - 1.0 / (refptcl[5] * refptcl[5]));
+      MapOp op = blank(MAP_KQUAD);
+      op.c[0] = refptcl[5]; op.c[1] = gambet0; op.c[2] = beta0;
+      op.c[3] = sp.charge / sp.mass; op.c[4] = e.val[0]; op.c[5] = tau;
+      op.c[6] = Scxl; op.c[7] = sp.qmi;
+      refptcl[4] = refptcl[4] + tau / beta0 / Scxl;
+      return push_op(prog, op);
+    }
+    if (x3 > 1.0e-5) return IMPZ_ERR_UNSUPPORTED;  // fringe-field table
+    if (e.mapstp < 1) return IMPZ_ERR_ARG;
+    double xm[36];
+    maplinear_quad(P, z, tau, xm, refptcl, e.val[0], e.mapstp, sp.charge, sp.mass);
+    return push_op(prog, op_xm6(xm));
+  }
+  if (e.type >= 101 && e.type <= 106) {
+    if (e.val[3] < 0.0) {
+      // ideal RF gap (BeamBunch.f90:324-440)
+      const double vtmp = e.val[0] / sp.mass;
+      const double harm = e.val[1] / P.Scfreq;
+      const double phi0lc = e.val[2] * std::asin(1.0) / 90;
+      MapOp op = blank(MAP_IDEALRF);
+      const int nseg = e.nseg;
+      op.flags = ((nst == 1 && ihlf % 2 == 0) ? 1 : 0) | ((nst == nseg && ihlf % 2 == 1) ? 2 : 0);
+      op.iparam = 2 * nseg;
+      const double gam0 = -refptcl[5];
+      const double gambet = std::sqrt(gam0 * gam0 - 1.0);
+      double beta0 = gambet / gam0;
+      refptcl[4] = refptcl[4] + 0.5 * tau / (Scxl * beta0);
+      refptcl[5] = refptcl[5] - tau * vtmp * std::cos(phi0lc);
+      const double gam0o = -refptcl[5];
+      const double gambet0 = std::sqrt(gam0o * gam0o - 1.0);
+      beta0 = gambet0 / gam0o;
+      refptcl[4] = refptcl[4] + 0.5 * tau / (Scxl * beta0);
+      op.c[0] = vtmp; op.c[1] = harm; op.c[2] = phi0lc; op.c[3] = Scxl; op.c[4] = tau;
+      op.c[5] = gam0; op.c[6] = gambet; op.c[7] = gam0o; op.c[8] = std::cos(phi0lc);
+      return push_op(prog, op);
+    }
+    if (e.type == 103 && e.ndata > 1 && e.zdat && e.edat && e.epdat && e.eppdat) {
+      if (e.mapstp < 1) return IMPZ_ERR_ARG;
+      double xm[36];
+      maplinear_ccl(P, z, tau, xm, refptcl, zedge, e, sp.charge, sp.mass);
+      return push_op(prog, op_xm6(xm));
+    }
+    return IMPZ_ERR_UNSUPPORTED;
+  }
+  return IMPZ_ERR_UNSUPPORTED;
+}
+
+namespace {
+MapOp pole_op(const Phys& P, MapKind kind, double h0, double h1, double tanphi, double tanphib,
+              double k1, double psi, double ang, double gam0, const Species& sp, double qm0) {
+  // preamble of Fpol_Dipole / Bpol_Dipole (Dipole.f90:478-486, 541-550)
+  MapOp op = blank(kind);
+  const double tanphi2 = tanphi * tanphi;
+  const double secphi2 = 1.0 + tanphi2;
+  const double secphi = 1.0 / std::cos(ang);
+  const double secphi3 = secphi2 * secphi;
+  const double secphib2 = 1. + tanphib * tanphib;
+  const double beta0 = std::sqrt(1.0 - 1.0 / (gam0 * gam0));
+  const double gambet = beta0 * gam0;
+  const double c[16] = {h0,      h1,       tanphi,  tanphib, k1,  psi, tanphi2, secphi2,
+                        secphi3, secphib2, beta0,   gambet,  gam0, qm0, sp.qmi, P.Scxl};
+  std::memcpy(op.c, c, sizeof(c));
+  return op;
+}
+}  // namespace
+
+int bend_entry_ops(const Phys& P, const impz_elem_t& e, double refptcl[6], const Species& sp,
+                   BendState& bs, MapProgram& prog) {
+  // AccSimulator.f90:1032-1094; dparam(k) = val[k-2]
+  const double* dp = e.val - 2;
+  if (dp[4] > 200) return IMPZ_ERR_UNSUPPORTED;  // CSR inside the bend
+  if (e.length == 0.0) return IMPZ_ERR_ARG;
+  const double blength = e.length;
+  bs.active = true;
+  bs.gamma0 = -refptcl[5];
+  bs.beta0 = std::sqrt(1.0 - 1.0 / bs.gamma0 / bs.gamma0);
+  refptcl[4] = refptcl[4] + blength / (P.Scxl * bs.beta0);
+  const double hgap = 2 * dp[5];
+  const double ang0 = dp[2];
+  bs.hd1 = dp[3];
+  const double angF = dp[6];
+  bs.angB = dp[7];
+  const double hF = dp[8];
+  bs.hB = dp[9];
+  const double dstr1 = dp[10], dstr2 = dstr1;
+  bs.hd0 = ang0 / blength;
+  const double tanphiF = std::tan(angF);
+  const double psi1 =
+      bs.hd0 * hgap * dstr1 * (1.0 + std::sin(angF) * std::sin(angF)) / std::cos(angF);
+  const double tanphiFb = std::tan(angF - psi1);
+  bs.tanphiB = std::tan(bs.angB);
+  bs.psi2 = bs.hd0 * hgap * dstr2 * (1.0 + std::sin(bs.angB) * std::sin(bs.angB)) /
+            std::cos(bs.angB);
+  bs.tanphiBb = std::tan(bs.angB - bs.psi2);
+  bs.qm0 = sp.charge / sp.mass;
+  return push_op(prog, pole_op(P, MAP_FPOL, bs.hd0, hF, tanphiF, tanphiFb, bs.hd1, psi1, angF,
+                               bs.gamma0, sp, bs.qm0));
+}
+
+void bend_sector_op(const Phys& P, const BendState& bs, double len, const Species& sp,
+                    MapProgram& prog) {
+  // Sector_Dipole coefficients (Dipole.f90:709-749)
+  const double h0 = bs.hd0, beta0 = bs.beta0;
+  const double rho = 1.0 / h0, theta = len * h0;
+  const double st = std::sin(theta), ct = std::cos(theta), sh = std::sin(theta / 2.0);
+  MapOp op = blank(MAP_SECTOR);
+  const double R16 = rho * (1.0 - ct), R26 = st;
+  const double T522 = -(0.5 * rho * st);
+  const double gambet = beta0 / std::sqrt(1.0 - beta0 * beta0);
+  const double gam2 = 1.0 / (1.0 - beta0 * beta0);
+  const double gam0 = std::sqrt(gam2);
+  const double c[33] = {ct,
+                        rho * st,
+                        R16,
+                        -st / rho,
+                        ct,
+                        R26,
+                        -R26,
+                        -R16,
+                        rho * (st - (beta0 * beta0) * theta),
+                        -(st * st) / (2.0 * rho),
+                        st * ct,
+                        st * st,
+                        rho * ct * (sh * sh),
+                        -(rho * st * (-1.0 + ct)),
+                        -(rho * (st * st)) / 2.0,
+                        rho * (-1.0 + ct) / 2.0,
+                        st / rho,
+                        -st / 2.0,
+                        -st,
+                        -st / 2.0,
+                        st,
+                        2.0 * rho * (sh * sh),
+                        rho * (theta - st),
+                        T522,
+                        T522,
+                        rho * (ct - 1.0),
+                        len,
+                        beta0,
+                        gambet,
+                        gam0,
+                        bs.qm0,
+                        sp.qmi,
+                        P.Scxl};
+  std::memcpy(op.c, c, sizeof(c));
+  push_op(prog, op);
+}
+
+void bend_exit_op(const Phys& P, const BendState& bs, const Species& sp, MapProgram& prog) {
+  push_op(prog, pole_op(P, MAP_BPOL, bs.hd0, bs.hB, bs.tanphiB, bs.tanphiBb, bs.hd1, bs.psi2,
+                        bs.angB, bs.gamma0, sp, bs.qm0));
+}
+
+// ---------------------------------------------------------------------
+int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double bcurr,
+                    const Species& sp, double refptcl[6], double* zio, CompiledLattice& out) {
+  struct Half {
+    MapProgram prog;
+  };
+  struct Step {
+    MapProgram a, b;
+    int sc;
+    double gam, tau, rad;
+    double z;
+    double ref[6];
+  };
+  std::vector<Step> steps;
+  MapProgram pending;
+  std::memset(&pending, 0, sizeof(pending));
+  double z = *zio;
+  const bool sc_on = !(bcurr < 1.0e-10);
+  for (int ie = 0; ie < nelem; ie++) {
+    const impz_elem_t& e = elems[ie];
+    if (e.type < 0) return IMPZ_ERR_UNSUPPORTED;
+    if (e.nseg < 1) return IMPZ_ERR_ARG;
+    const int bnseg = e.nseg, bitype = e.type;
+    double piperad = pipe_radius(e), piperad2 = piperad;
+    if (bitype == 4) { piperad = 100.0; piperad2 = 100.0; }
+    const double tau1 = 0.5 * e.length / bnseg;
+    const double tau2 = 2.0 * tau1;
+    const double zedge = z;
+    BendState bs;
+    std::memset(&bs, 0, sizeof(bs));
+    if (bitype == 4) {
+      int r = bend_entry_ops(P, e, refptcl, sp, bs, pending);
+      if (r) return r;
+      piperad2 = e.val[3];
+    }
+    int ihlf = 0;
+    for (int j = 1; j <= bnseg; j++) {
+      Step s;
+      std::memset(&s, 0, sizeof(s));
+      s.a = pending;
+      std::memset(&pending, 0, sizeof(pending));
+      for (int half = 0; half < 2; half++) {
+        MapProgram& prog = half == 0 ? s.a : s.b;
+        if (half == 1) {
+          s.sc = sc_on ? 1 : 0;
+          s.gam = -refptcl[5];
+          s.tau = tau2;
+          s.rad = (piperad + piperad2) / 2;
+        }
+        if (bitype == 4) {
+          bend_sector_op(P, bs, tau1, sp, prog);
+        } else {
+          int r = half_map_ops(P, e, zedge, z, tau1, j, ihlf, refptcl, sp, prog);
+          if (r) return r;
+          ihlf++;
+        }
+        z = z + tau1;
+      }
+      s.z = z;
+      std::memcpy(s.ref, refptcl, sizeof(s.ref));
+      steps.push_back(s);
+    }
+    if (bitype == 4) bend_exit_op(P, bs, sp, pending);
+  }
+  const int K = (int)steps.size();
+  out.nsteps = K;
+  out.steps.assign(K + 2, StepParams());
+  for (auto& st : out.steps) std::memset(&st, 0, sizeof(st));
+  out.zrec.assign(K + 1, 0.0);
+  out.refrec.assign(6 * (K + 1), 0.0);
+  // prologue: initial diagnostics, then the first half map of step 1
+  out.zrec[0] = *zio;
+  StepParams& p0 = out.steps[0];
+  p0.moments = 1;
+  p0.gam = 2.0;
+  p0.rad = 1e300;
+  for (int s = 0; s <= K; s++) {
+    StepParams& sp_ = out.steps[s];
+    if (s >= 1) {
+      const Step& cur = steps[s - 1];
+      sp_.post = cur.b;
+      sp_.moments = 1;
+      sp_.sc = cur.sc;
+      sp_.gam = cur.gam;
+      sp_.tau = cur.tau;
+      sp_.rad = cur.rad;
+      out.zrec[s] = cur.z;
+      std::memcpy(&out.refrec[6 * s], cur.ref, 6 * sizeof(double));
+    }
+    if (s < K) {
+      sp_.pre_next = steps[s].a;
+      sp_.range_next = steps[s].sc;
+    } else {
+      sp_.pre_next = pending;  // Bpol of a bend that ends the lattice
+      sp_.range_next = 0;
+    }
+  }
+  StepParams& sent = out.steps[K + 1];
+  sent.gam = 2.0;
+  sent.rad = 1e300;
+  *zio = z;
+  return IMPZ_OK;
+}
+
+// ---------------------------------------------------------------------
+void diag_row(const Phys& P, double z, const double rec[IMPZ_MOMREC], const double refptcl[6],
+              double mass, double row[IMPZ_DIAG_LEN]) {
+  // Output.f90:247-352
+  const double* t = rec;
+  const double qmc = mass / 1.0e6, xl = P.Scxl, xt = P.Rad2deg;
+  const double npt = rec[44], nlocal = rec[45];
+  const double den1 = 1.0 / npt;
+  const double gam = -refptcl[5];
+  const double gambet = std::sqrt(gam * gam - 1.0);
+  const double bet = std::sqrt(gam * gam - 1.0) / gam;
+  const double energy = (gam - 1.) * qmc;
+  const double third = (double)(1.0f / 3.0f);  // (1.0/3.0) in default real
+  auto m3 = [&](double c3, double s2, double m) {
+    return std::pow(std::fabs(c3 - 3 * s2 * m + 2 * m * m * m), third);
+  };
+  auto m4 = [&](double c4, double c3, double s2, double m) {
+    return std::sqrt(std::sqrt(std::fabs(c4 - 4 * c3 * m + 6 * s2 * m * m - 3 * m * m * m * m)));
+  };
+  double mean[6], sq[6], var[6];
+  for (int c = 0; c < 6; c++) {
+    mean[c] = t[c] * den1;
+    sq[c] = t[6 + c] * den1;
+    var[c] = sq[c] - mean[c] * mean[c];
+  }
+  const double xpx = t[12] * den1 - mean[0] * mean[1];
+  const double ypy = t[13] * den1 - mean[2] * mean[3];
+  const double zpz = t[14] * den1 - mean[4] * mean[5];
+  double c3[6], c4[6];
+  for (int c = 0; c < 6; c++) {
+    c3[c] = t[15 + 2 * c] * den1;
+    c4[c] = t[16 + 2 * c] * den1;
+  }
+  double o3[6], o4[6];
+  for (int c = 0; c < 6; c++) {
+    o3[c] = m3(c3[c], sq[c], mean[c]);
+    o4[c] = m4(c4[c], c3[c], sq[c], mean[c]);
+  }
+  const double epsx2 = var[0] * var[1] - xpx * xpx;
+  const double epsy2 = var[2] * var[3] - ypy * ypy;
+  const double epsz2 = var[4] * var[5] - zpz * zpz;
+  const double epx = std::sqrt(std::fmax(epsx2, 0.0));
+  const double epy = std::sqrt(std::fmax(epsy2, 0.0));
+  const double epz = std::sqrt(std::fmax(epsz2, 0.0));
+  double rms[6];
+  for (int c = 0; c < 6; c++) rms[c] = std::sqrt(var[c]);
+  const double* gm = rec + 37;
+  row[0] = z;
+  row[1] = refptcl[4]; row[2] = gam; row[3] = energy; row[4] = bet;
+  row[5] = std::sqrt(rec[43]) * xl;
+  row[6] = mean[0] * xl; row[7] = rms[0] * xl; row[8] = mean[1] / gambet;
+  row[9] = rms[1] / gambet; row[10] = -xpx / epx; row[11] = epx * xl;
+  row[12] = mean[2] * xl; row[13] = rms[2] * xl; row[14] = mean[3] / gambet;
+  row[15] = rms[3] / gambet; row[16] = -ypy / epy; row[17] = epy * xl;
+  row[18] = mean[4] * xt; row[19] = rms[4] * xt; row[20] = mean[5] * qmc;
+  row[21] = rms[5] * qmc; row[22] = -zpz / epz; row[23] = epz * qmc * xt;
+  row[24] = gm[0] * xl; row[25] = gm[1] / gambet; row[26] = gm[2] * xl;
+  row[27] = gm[3] / gambet; row[28] = gm[4] * xt; row[29] = gm[5] * qmc;
+  row[30] = nlocal; row[31] = nlocal; row[32] = npt;
+  row[33] = o3[0] * xl; row[34] = o3[1] / gambet; row[35] = o3[2] * xl;
+  row[36] = o3[3] / gambet; row[37] = o3[4] * xt; row[38] = o3[5] * qmc;
+  row[39] = o4[0] * xl; row[40] = o4[1] / gambet; row[41] = o4[2] * xl;
+  row[42] = o4[3] / gambet; row[43] = o4[4] * xt; row[44] = o4[5] * qmc;
+}
+
+}  // namespace impz

@@ -1,0 +1,60 @@
+// impz_host.h -- host-side builders: transfer-map constants, the RK6 linear
+// maps, the lattice-to-step-table compiler and the diagnostic formulas.
+#pragma once
+#include <vector>
+
+#include "../../include/impz_b200.h"
+#include "impz_common.h"
+
+namespace impz {
+
+struct Phys {  // PhysConst (src/DataStruct/PhysConst.f90:25-35)
+  double Pi, Clight, Scxl, Rad2deg, Scfreq;
+};
+Phys make_phys(double freq);
+
+// maplinear_Quadrupole / maplinear_DriftTube / maplinear_CCL (RK6 of the
+// 18-variable linear ODE); refpt(5), refpt(6) advance like the reference.
+void maplinear_quad(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                    double gradient, int mapstp, double chg, double mass);
+void maplinear_ccl(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                   double zedge, const impz_elem_t& e, double chg, double mass);
+
+struct BendState {  // the bend constants AccSimulator.f90:1057-1093 keeps
+  bool active;
+  double gamma0, beta0, hd0, hd1;
+  double hB, tanphiB, tanphiBb, psi2, angB;
+  double qm0;
+};
+
+struct Species {
+  double charge, mass, qmi;  // qmi = Pts1(7,:)
+};
+
+// One half step of element e (the drift1_BeamBunch dispatch,
+// BeamBunch.f90:250-464); appends its map op to prog, updates refptcl.
+int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, double tau,
+                 int nst, int ihlf, double refptcl[6], const Species& sp, MapProgram& prog);
+// Bend entry (refptcl(5) update + Fpol op), Sector op, Bpol op.
+int bend_entry_ops(const Phys& P, const impz_elem_t& e, double refptcl[6], const Species& sp,
+                   BendState& bs, MapProgram& prog);
+void bend_sector_op(const Phys& P, const BendState& bs, double tau, const Species& sp,
+                    MapProgram& prog);
+void bend_exit_op(const Phys& P, const BendState& bs, const Species& sp, MapProgram& prog);
+
+struct CompiledLattice {
+  std::vector<StepParams> steps;  // [0] prologue, [1..K] steps, [K+1] sentinel
+  std::vector<double> zrec;       // z of each record (K+1)
+  std::vector<double> refrec;     // refptcl of each record, 6 per record
+  int nsteps;
+};
+// run_AccSimulator's element/segment loop (AccSimulator.f90:742-1504)
+// turned into a step table.  refptcl and z advance to the lattice exit.
+int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double bcurr,
+                    const Species& sp, double refptcl[6], double* z, CompiledLattice& out);
+
+// diagnostic1_Output rank-0 formulas (Output.f90:247-352)
+void diag_row(const Phys& P, double z, const double rec[IMPZ_MOMREC], const double refptcl[6],
+              double mass, double row[IMPZ_DIAG_LEN]);
+
+}  // namespace impz

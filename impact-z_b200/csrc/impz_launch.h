@@ -1,0 +1,55 @@
+// impz_launch.h -- host-side launch wrappers of the sm_100a kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "impz_common.h"
+
+namespace impz {
+
+#define IMPZ_ADV_BLOCK 256
+#define IMPZ_DEP_BLOCK 512
+#define IMPZ_DEP_PPT 4
+#define IMPZ_SCAN_THREADS 1024
+
+#define IMPZ_DECLARE_PARTICLE_LAUNCHERS(NS)                                              \
+  namespace NS {                                                                         \
+  cudaError_t launch_advance(const AdvanceArgs& a, bool f32, int grid, cudaStream_t s);  \
+  cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s);            \
+  cudaError_t launch_scan(int* counts, int* cursor, int* bsum, long long total,          \
+                          DevState* st, cudaStream_t s);                                 \
+  int max_blocks_advance(bool f32);                                                      \
+  int max_blocks_deposit();                                                              \
+  }
+IMPZ_DECLARE_PARTICLE_LAUNCHERS(exact)
+IMPZ_DECLARE_PARTICLE_LAUNCHERS(fast)
+
+// Poisson solve (T = double for the FP64 form, float for the FP32 form)
+struct PoissonBuffers {
+  int nx, ny, nz;
+  unsigned long long* rho;  // int64 charge, cleared by the forward pass
+  double qscale;            // grid value of one fixed-point quantum
+  void* spec;               // (nx+1)*2ny*nz complex T
+  double* F;                // (nx+2)(ny+2)(nz+2) IGF corners
+  double* Gt;               // (nx+1)(ny+1)(nz+1) FP64 green octant / DCT work
+  void* ghat;               // (nx+1)(ny+1)(nz+1) T
+  void* phi;                // nx*ny*nz T
+  void* efield;             // 4*nx*ny*nz T
+  const void* twx;          // twiddles of length 2nx, 2ny, 2nz in T
+  const void* twy;
+  const void* twz;
+  const double2* tw64x;     // FP64 twiddles for the DCT of G
+  const double2* tw64y;
+  const double2* tw64z;
+  DevState* st;
+};
+
+template <typename T>
+cudaError_t launch_green(const PoissonBuffers& b, cudaStream_t s);
+template <typename T>
+cudaError_t launch_convolve(const PoissonBuffers& b, cudaStream_t s);
+template <typename T>
+cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s);
+template <typename T>
+size_t poisson_smem_max(int nx, int ny, int nz);
+
+}  // namespace impz

@@ -1,0 +1,919 @@
+// impz_particle.cuh -- per-particle kernels of one space-charge step.
+//
+// This file is compiled twice: once with --fmad=false into namespace
+// impz::exact (the plain FP64 form: every FP64 operation in the reference's
+// order, no contraction, so single-step results reproduce the Fortran
+// arithmetic bit for bit wherever no transcendental function is involved),
+// and once with contraction enabled into impz::fast (the FP32-convolution
+// form, which gathers an FP32 field and may fuse multiply-adds).
+//
+// Kernels:
+//   k_advance  -- the fused particle pass: [CIC gather + kick + z-frame]
+//                 -> second half map -> moments -> next first half map ->
+//                 next conv1st range/loss count -> write (sorted by the
+//                 deposit cell when a kick ran).  The last block of the
+//                 grid reduces moments and range and runs update_CompDom.
+//   k_deposit  -- z->t frame + CIC charge deposit into int64 fixed point
+//                 (shared-memory tiles, global atomics for sparse chunks)
+//                 + per-cell particle counts.
+//   k_scan     -- exclusive scan of the per-cell counts (sort cursors).
+#pragma once
+#include <cuda_runtime.h>
+#include <climits>
+#include <stdint.h>
+
+#include "impz_common.h"
+
+#ifndef IMPZ_NS
+#error "define IMPZ_NS (exact or fast) before including impz_particle.cuh"
+#endif
+
+namespace impz {
+namespace IMPZ_NS {
+
+// conv1st's pilc = 2.0*asin(1.0) evaluated in default (single) precision
+// (BeamBunch.f90:1268), i.e. the float nearest pi, widened.
+__device__ __constant__ const double kPilc = 3.1415927410125732421875;
+
+struct Particle {
+  double x, px, y, py, ph, pt;
+};
+
+// ---------------------------------------------------------------------
+// transfer maps; each follows the cited reference loop body
+__device__ __forceinline__ void map_drift(Particle& p, const double* c) {
+  // BeamBunch.f90:286-295; c = {gam0, beta0, tau, Scxl}
+  const double gam0 = c[0], beta0 = c[1], tau = c[2], Scxl = c[3];
+  double d = p.pt - gam0;
+  double tmph = sqrt(((d * d - 1.0) - p.px * p.px) - p.py * p.py);
+  p.x = p.x + ((p.px * tau) / tmph) / Scxl;
+  p.y = p.y + ((p.py * tau) / tmph) / Scxl;
+  p.ph = p.ph - ((1.0 / beta0 + (p.pt - gam0) / tmph) * tau) / Scxl;
+}
+
+__device__ __forceinline__ void map_xm6(Particle& p, const double* xm, int mask_lo,
+                                        int mask_hi) {
+  // BeamBunch.f90:310-320: temp(j) = sum_k Pts1(k)*xm(j,k) from 0.0; the
+  // zero entries of xm only add signed zeros and are skipped.
+  double in[6] = {p.x, p.px, p.y, p.py, p.ph, p.pt};
+  double out[6];
+  unsigned long long mask = (unsigned long long)(unsigned)mask_lo |
+                            ((unsigned long long)(unsigned)mask_hi << 32);
+#pragma unroll
+  for (int j = 0; j < 6; j++) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      if (mask & (1ull << (j + 6 * k))) s = s + in[k] * xm[j + 6 * k];
+    out[j] = s;
+  }
+  p.x = out[0]; p.px = out[1]; p.y = out[2]; p.py = out[3]; p.ph = out[4]; p.pt = out[5];
+}
+
+__device__ __forceinline__ void map_kquad(Particle& p, const double* c) {
+  // Quadrupole.f90:526-600; c = {refpt6, gambet0, beta0, qmass, K, tau, Scxl, qmi}
+  const double refpt6 = c[0], gambet0 = c[1], beta0 = c[2], qmass = c[3], K = c[4];
+  const double tau = c[5], Scxl = c[6], qmi = c[7];
+  double gam = -refpt6 - p.pt;
+  double gambetz = sqrt(((gam * gam - 1.0) - p.px * p.px) - p.py * p.py);
+  double betaz = gambetz / gam;
+  gambetz = sqrt(gam * gam - 1.0);
+  double kstr = qmi / qmass * gambet0 / gambetz * K;
+  double rtkstr = sqrt(fabs(kstr));
+  double rtkstrzz = rtkstr * tau;
+  double xm11, xm12, xm21, xm22, xm33, xm34, xm43, xm44, cs, ss, t;
+  if (kstr > 0.0) {
+    sincos(rtkstrzz, &ss, &cs);
+    xm11 = cs; xm12 = ss / rtkstr; xm21 = -(rtkstr * ss); xm22 = cs;
+    t = exp(rtkstrzz);
+    cs = (t * t + 1.0) / (t + t);
+    ss = (t * t - 1.0) / (t + t);
+    xm33 = cs; xm34 = ss / rtkstr; xm43 = ss * rtkstr; xm44 = cs;
+  } else if (kstr < 0.0) {
+    t = exp(rtkstrzz);
+    cs = (t * t + 1.0) / (t + t);
+    ss = (t * t - 1.0) / (t + t);
+    xm11 = cs; xm12 = ss / rtkstr; xm21 = rtkstr * ss; xm22 = cs;
+    sincos(rtkstrzz, &ss, &cs);
+    xm33 = cs; xm34 = ss / rtkstr; xm43 = -(ss * rtkstr); xm44 = cs;
+  } else {
+    xm11 = 1.0; xm12 = tau; xm21 = 0.0; xm22 = 1.0;
+    xm33 = 1.0; xm34 = tau; xm43 = 0.0; xm44 = 1.0;
+  }
+  double t1 = xm11 * p.x + xm12 * p.px / gambetz / Scxl;
+  double t2 = gambetz * Scxl * xm21 * p.x + xm22 * p.px;
+  double t3 = xm33 * p.y + xm34 * p.py / gambetz / Scxl;
+  double t4 = gambetz * Scxl * xm43 * p.y + xm44 * p.py;
+  double t5 = p.ph + (1.0 / betaz - 1.0 / beta0) * tau / Scxl;
+  p.x = t1; p.px = t2; p.y = t3; p.py = t4; p.ph = t5;
+}
+
+__device__ __forceinline__ void map_idealrf(Particle& p, const double* c, int flags,
+                                            int twonseg) {
+  // BeamBunch.f90:337-438; c = {vtmp, harm, phi0lc, Scxl, tau, gam0_in,
+  //                            gambet_in, gam0_out, cos(phi0lc)}
+  const double vtmp = c[0], harm = c[1], phi0lc = c[2], Scxl = c[3], tau = c[4];
+  const double gam0 = c[5], gambet = c[6], gam0o = c[7], c0 = c[8];
+  if (flags & 1) {  // entrance focusing kick
+    double gam = gam0 - p.pt;
+    double gambetz = sqrt(((gam * gam - 1.0) - p.px * p.px) - p.py * p.py);
+    double phi = p.ph * harm + phi0lc;
+    double vg = vtmp * cos(phi) * Scxl;
+    p.px = p.px - 0.5 * vg * gambetz / gam * p.x;
+    p.py = p.py - 0.5 * vg * gambetz / gam * p.y;
+  }
+  {
+    double gami_1 = gam0 - p.pt;
+    double gambeti_1 = sqrt(gami_1 * gami_1 - 1.0);
+    double gambetzi_1 = sqrt(((gami_1 * gami_1 - 1.0) - p.px * p.px) - p.py * p.py);
+    double phi = p.ph * harm + phi0lc;
+    double dgami = tau * vtmp * cos(phi);
+    double gami_2 = gami_1 + dgami;
+    double gambeti_2 = sqrt(gami_2 * gami_2 - 1.0);
+    double fact;
+    if (fabs(vtmp) < 1.0e-10)
+      fact = tau / Scxl;
+    else
+      fact = gambeti_1 / dgami * log(gambeti_2 / gambeti_1) * tau / Scxl;
+    p.x = p.x + fact * p.px / gambetzi_1;
+    p.y = p.y + fact * p.py / gambetzi_1;
+    p.ph = p.ph + (tau / Scxl) / (gambet * gambet * gambet) * p.pt;
+  }
+  if (flags & 2) {  // exit focusing kick and energy correction
+    double gam = gam0o - p.pt;
+    double gambetz = sqrt(((gam * gam - 1.0) - p.px * p.px) - p.py * p.py);
+    double phi = p.ph * harm + phi0lc;
+    double vg = vtmp * cos(phi) * Scxl;
+    p.px = p.px + 0.5 * vg * gambetz / gam * p.x;
+    p.py = p.py + 0.5 * vg * gambetz / gam * p.y;
+    phi = p.ph * harm + phi0lc;
+    p.pt = p.pt + (double)twonseg * tau * vtmp * (c0 - cos(phi));
+  }
+}
+
+// Fpol_Dipole / Bpol_Dipole (Dipole.f90:488-524, 551-589).
+// c = {h0, h1, tanphi, tanphib, k1, psi, tanphi2, secphi2, secphi3,
+//      secphib2, beta0, gambet, gam0, qm0, qmi, Scxl}
+template <bool EXIT>
+__device__ __forceinline__ void map_pole(Particle& p, const double* c) {
+  const double h0 = c[0], h1 = c[1], tanphi = c[2], tanphib = c[3], k1 = c[4], psi = c[5];
+  const double tanphi2 = c[6], secphi2 = c[7], secphi3 = c[8], secphib2 = c[9];
+  const double beta0 = c[10], gambet = c[11], gam0 = c[12], qm0 = c[13], qmi = c[14];
+  const double Scxl = c[15];
+  double x = p.x * Scxl;
+  double gamn = gam0 - p.pt;
+  double gambetz = sqrt(((gamn * gamn - 1.0) - p.px * p.px) - p.py * p.py);
+  double xp = p.px / gambetz;
+  double y = p.y * Scxl;
+  double yp = p.py / gambetz;
+  double z5 = -(p.ph * beta0 * Scxl);
+  double d = -(p.pt / beta0 / gambet) - (qmi - qm0) / qm0;
+  double a0, a1, a2, a3;
+  if (!EXIT) {
+    a0 = x - 0.5 * h0 * tanphi2 * (x * x) + 0.5 * h0 * secphi2 * (y * y);
+    a1 = h0 * tanphi * x + xp + h0 * tanphi2 * x * xp +
+         (0.5 * h0 * h1 * secphi3 + k1 * tanphi) * (x * x) -
+         (0.5 * h0 * h1 * secphi3 + k1 * tanphi - (h0 * h0) * tanphi * tanphi2 -
+          0.5 * (h0 * h0) * tanphi) * (y * y) -
+         h0 * tanphi2 * y * yp - h0 * tanphi * x * d;
+    a2 = y + h0 * tanphi2 * x * y;
+    a3 = -(h0 * tanphib * y) + yp - h0 * tanphi2 * x * yp - h0 * secphi2 * xp * y -
+         (h0 * h1 * secphi3 + 2 * k1 * tanphi) * x * y +
+         (h0 * tanphi - h0 * psi * secphib2) * y * d;
+  } else {
+    a0 = x + 0.5 * h0 * tanphi2 * (x * x) - 0.5 * h0 * secphi2 * (y * y);
+    a1 = h0 * tanphi * x + xp - h0 * tanphi2 * x * xp +
+         (0.5 * h0 * h1 * secphi3 + k1 * tanphi - (h0 * h0) * tanphi2 * tanphi / 2) * (x * x) -
+         (0.5 * h0 * h1 * secphi3 + k1 * tanphi + (h0 * h0) * tanphi * tanphi2 / 2) * (y * y) +
+         h0 * tanphi2 * y * yp - h0 * tanphi * x * d;
+    a2 = y - h0 * tanphi2 * x * y;
+    a3 = -(h0 * tanphib * y) + yp + h0 * tanphi2 * x * yp + h0 * secphi2 * xp * y -
+         (h0 * h1 * secphi3 + 2 * k1 * tanphi - (h0 * h0) * secphi2 * tanphi) * x * y +
+         (h0 * tanphi - h0 * psi * secphib2) * y * d;
+  }
+  gambetz = sqrt(gamn * gamn - 1.0) / sqrt((a1 * a1 + a3 * a3) + 1);
+  p.x = a0 / Scxl;
+  p.px = a1 * gambetz;
+  p.y = a2 / Scxl;
+  p.py = a3 * gambetz;
+  p.ph = -z5 / Scxl / beta0;
+  p.pt = -(beta0 * gambet * (d + (qmi - qm0) / qm0));
+}
+
+// Sector_Dipole second-order map (Dipole.f90:745-786).
+// c = {R11,R12,R16,R21,R22,R26,R51,R52,R56, T111,T112,T116,T122,T126,T166,
+//      T144,T216,T222,T266,T244,T314,T324,T346,T522,T544,T526,
+//      len, beta0, gambet, gam0, qm0, qmi, Scxl}
+__device__ __forceinline__ void map_sector(Particle& p, const double* c) {
+  const double R11 = c[0], R12 = c[1], R16 = c[2], R21 = c[3], R22 = c[4], R26 = c[5];
+  const double R51 = c[6], R52 = c[7], R56 = c[8];
+  const double T111 = c[9], T112 = c[10], T116 = c[11], T122 = c[12], T126 = c[13];
+  const double T166 = c[14], T144 = c[15], T216 = c[16], T222 = c[17], T266 = c[18];
+  const double T244 = c[19], T314 = c[20], T324 = c[21], T346 = c[22], T522 = c[23];
+  const double T544 = c[24], T526 = c[25], len = c[26], beta0 = c[27], gambet = c[28];
+  const double gam0 = c[29], qm0 = c[30], qmi = c[31], Scxl = c[32];
+  double gami = -p.pt + gam0;
+  double gambeti = sqrt(gami * gami - 1.0);
+  double gambetz = sqrt((gambeti * gambeti - p.px * p.px) - p.py * p.py);
+  double x0 = p.x * Scxl, xp0 = p.px / gambetz, y0 = p.y * Scxl, yp0 = p.py / gambetz;
+  double z0 = -(p.ph * beta0 * Scxl);
+  double eta = -(p.pt / beta0 / gambet) - (qmi - qm0) / qm0;
+  double a0 = R11 * x0 + R12 * xp0 + R16 * eta + T111 * (x0 * x0) + T112 * x0 * xp0 +
+              T116 * x0 * eta + T122 * (xp0 * xp0) + T126 * xp0 * eta + T166 * (eta * eta) +
+              T144 * (yp0 * yp0);
+  double a1 = R21 * x0 + R22 * xp0 + R26 * eta + T216 * x0 * eta + T222 * (xp0 * xp0) +
+              T266 * (eta * eta) + T244 * (yp0 * yp0);
+  double a2 = y0 + len * yp0 + T314 * x0 * yp0 + T324 * xp0 * yp0 + T346 * yp0 * eta;
+  double a3 = yp0;
+  double a4 = R51 * x0 + R52 * xp0 + z0 + R56 * eta + T522 * (xp0 * xp0) + T544 * (yp0 * yp0) +
+              T526 * xp0 * eta;
+  gambetz = gambeti / sqrt((a1 * a1 + a3 * a3) + 1.0);
+  p.x = a0 / Scxl;
+  p.px = a1 * gambetz;
+  p.y = a2 / Scxl;
+  p.py = a3 * gambetz;
+  p.ph = -a4 / Scxl / beta0;
+  p.pt = -(beta0 * gambet * (eta + (qmi - qm0) / qm0));
+}
+
+__device__ __forceinline__ void apply_program(Particle& p, const MapProgram& prog) {
+  for (int o = 0; o < prog.nops; o++) {
+    const MapOp& op = prog.ops[o];
+    switch (op.kind) {
+      case MAP_DRIFT: map_drift(p, op.c); break;
+      case MAP_XM6: map_xm6(p, op.c, op.flags, op.iparam); break;
+      case MAP_KQUAD: map_kquad(p, op.c); break;
+      case MAP_IDEALRF: map_idealrf(p, op.c, op.flags, op.iparam); break;
+      case MAP_FPOL: map_pole<false>(p, op.c); break;
+      case MAP_BPOL: map_pole<true>(p, op.c); break;
+      case MAP_SECTOR: map_sector(p, op.c); break;
+      default: break;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// conv1st z->t frame (BeamBunch.f90:1290-1340), without storing the result
+struct TFrame {
+  double xt, yt, zt;      // t-frame positions [m]
+  double tmpx, tmpy;      // z-frame x*Scxl, y*Scxl (they enter the range)
+  double ph;              // wrapped phase
+  double rcp, tmpbet;     // 1/gamma_i and 1-beta_i^2-ish (before abs)
+  bool lost;
+};
+
+// Written with explicit round-to-nearest intrinsics: the deposit (plain
+// build) and the fused particle pass (either build) must agree bit for bit
+// on the loss test and the cell, whatever contraction the build allows.
+__device__ __forceinline__ TFrame to_tframe(const Particle& p, double gam, double rad,
+                                            double xl) {
+  TFrame t;
+  int ntmp5 = (int)(p.ph / kPilc);
+  double tmp5 = __dsub_rn(p.ph, __dmul_rn((double)ntmp5, kPilc));
+  t.ph = __dsub_rn(tmp5, __dmul_rn((double)(ntmp5 % 2), kPilc));
+  t.rcp = 1.0 / __dadd_rn(-p.pt, gam);
+  t.tmpbet = __dsub_rn(1.0, __dmul_rn(__dmul_rn(t.rcp, t.rcp),
+                                      __dadd_rn(__dadd_rn(1.0, __dmul_rn(p.px, p.px)),
+                                                __dmul_rn(p.py, p.py))));
+  double betai = sqrt(fabs(t.tmpbet));
+  t.tmpx = __dmul_rn(p.x, xl);
+  t.xt = __dmul_rn(__dsub_rn(p.x, __dmul_rn(__dmul_rn(p.px, t.ph), t.rcp)), xl);
+  t.tmpy = __dmul_rn(p.y, xl);
+  t.yt = __dmul_rn(__dsub_rn(p.y, __dmul_rn(__dmul_rn(p.py, t.ph), t.rcp)), xl);
+  t.zt = -__dmul_rn(__dmul_rn(__dmul_rn(gam, betai), t.ph), xl);
+  double radtest = sqrt(__dadd_rn(__dmul_rn(t.xt, t.xt), __dmul_rn(t.yt, t.yt)));
+  t.lost = (radtest >= rad) || (t.tmpbet <= 0.0);
+  return t;
+}
+
+// deposit_BeamBunch cell and weights (BeamBunch.f90:3737-3742)
+struct Cell {
+  int ix, jx, kx;   // 1-based like the reference
+  double ab, cd, ef;
+};
+
+__device__ __forceinline__ Cell cic_cell(double x, double y, double z, const Geom& g) {
+  Cell c;
+  c.ix = (int)__dadd_rn(__dmul_rn(__dsub_rn(x, g.range[0]), g.hi[0]), 1.0);
+  c.ab = __dmul_rn(__dadd_rn(__dsub_rn(g.range[0], x), __dmul_rn((double)c.ix, g.h[0])), g.hi[0]);
+  c.jx = (int)__dadd_rn(__dmul_rn(__dsub_rn(y, g.range[2]), g.hi[1]), 1.0);
+  c.cd = __dmul_rn(__dadd_rn(__dsub_rn(g.range[2], y), __dmul_rn((double)c.jx, g.h[1])), g.hi[1]);
+  c.kx = (int)__dadd_rn(__dmul_rn(__dsub_rn(z, g.range[4]), g.hi[2]), 1.0);
+  c.ef = __dmul_rn(__dadd_rn(__dsub_rn(g.range[4], z), __dmul_rn((double)c.kx, g.h[2])), g.hi[2]);
+  return c;
+}
+
+__device__ __forceinline__ bool cell_inside(const Cell& c, int nx, int ny, int nz) {
+  return !(c.ix < 1 || c.ix + 1 > nx || c.jx < 1 || c.jx + 1 > ny || c.kx < 1 ||
+           c.kx + 1 > nz);
+}
+
+// ---------------------------------------------------------------------
+// reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// the 37 sums of diagnostic1_Output (Output.f90:133-196), in tmplc order
+__device__ __forceinline__ void moment_accumulate(double* s, const Particle& p) {
+  const double x = p.x, px = p.px, y = p.y, py = p.py, z = p.ph, pz = p.pt;
+  s[0] += x;  s[1] += px; s[2] += y;  s[3] += py; s[4] += z;  s[5] += pz;
+  s[6] += x * x; s[7] += px * px; s[8] += y * y; s[9] += py * py;
+  s[10] += z * z; s[11] += pz * pz;
+  s[12] += x * px; s[13] += y * py; s[14] += z * pz;
+  s[15] += x * x * x; s[16] += x * x * x * x;
+  s[17] += px * px * px; s[18] += px * px * px * px;
+  s[19] += y * y * y; s[20] += y * y * y * y;
+  s[21] += py * py * py; s[22] += py * py * py * py;
+  s[23] += fabs(z * z * z); s[24] += z * z * z * z;
+  s[25] += pz * pz * pz; s[26] += pz * pz * pz * pz;
+  s[27] += x * px * px; s[28] += x * px * px * px; s[29] += x * x * px;
+  s[30] += x * x * px * px; s[31] += x * x * x * px;
+  s[32] += y * py * py; s[33] += y * py * py * py; s[34] += y * y * py;
+  s[35] += y * y * py * py; s[36] += y * y * y * py;
+  s[37] = fmax(s[37], fabs(x)); s[38] = fmax(s[38], fabs(px));
+  s[39] = fmax(s[39], fabs(y)); s[40] = fmax(s[40], fabs(py));
+  s[41] = fmax(s[41], fabs(z)); s[42] = fmax(s[42], fabs(pz));
+  s[43] = fmax(s[43], x * x + y * y);
+}
+
+
+template <bool F32>
+__device__ __forceinline__ void gather_e(const void* ef, const Cell& c, int nx, int ny,
+                                         double& ex, double& ey, double& ez);
+
+// scatter1_BeamBunch gather, FP64 field, reference term order (BeamBunch.f90:2128-2155)
+template <>
+__device__ __forceinline__ void gather_e<false>(const void* ef, const Cell& c, int nx, int ny,
+                                                double& ex, double& ey, double& ez) {
+  const long long sy = nx, sz = (long long)nx * ny;
+  const long long b = (long long)(c.ix - 1) + sy * (c.jx - 1) + sz * (c.kx - 1);
+  const double ab = c.ab, cd = c.cd, efw = c.ef;
+  const double ab1 = 1.0 - ab, cd1 = 1.0 - cd, ef1 = 1.0 - efw;
+  const double2* E = reinterpret_cast<const double2*>(ef);
+  const long long nodes[8] = {b, b + sy, b + sy + sz, b + sz, b + 1 + sz, b + 1 + sy + sz,
+                              b + 1 + sy, b + 1};
+  double2 A[8], B[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    A[q] = __ldg(E + 2 * nodes[q]);
+    B[q] = __ldg(E + 2 * nodes[q] + 1);
+  }
+  // term q: field * w1 * w2 * w3 evaluated left to right like the reference
+#define IMPZ_T(q, w1, w2, w3) \
+  sx = sx + A[q].x * w1 * w2 * w3; sy_ = sy_ + A[q].y * w1 * w2 * w3; sz_ = sz_ + B[q].x * w1 * w2 * w3;
+  double sx = A[0].x * ab * cd * efw, sy_ = A[0].y * ab * cd * efw, sz_ = B[0].x * ab * cd * efw;
+  IMPZ_T(1, ab, cd1, efw)
+  IMPZ_T(2, ab, cd1, ef1)
+  IMPZ_T(3, ab, cd, ef1)
+  IMPZ_T(4, ab1, cd, ef1)
+  IMPZ_T(5, ab1, cd1, ef1)
+  IMPZ_T(6, ab1, cd1, efw)
+  IMPZ_T(7, ab1, cd, efw)
+#undef IMPZ_T
+  ex = sx; ey = sy_; ez = sz_;
+}
+
+// FP32 field gather (FP32-convolution form)
+template <>
+__device__ __forceinline__ void gather_e<true>(const void* ef, const Cell& c, int nx, int ny,
+                                               double& ex, double& ey, double& ez) {
+  const long long sy = nx, sz = (long long)nx * ny;
+  const long long b = (long long)(c.ix - 1) + sy * (c.jx - 1) + sz * (c.kx - 1);
+  const float ab = (float)c.ab, cd = (float)c.cd, efw = (float)c.ef;
+  const float ab1 = 1.0f - ab, cd1 = 1.0f - cd, ef1 = 1.0f - efw;
+  const float4* E = reinterpret_cast<const float4*>(ef);
+  const long long nodes[8] = {b, b + sy, b + sy + sz, b + sz, b + 1 + sz, b + 1 + sy + sz,
+                              b + 1 + sy, b + 1};
+  const float w[8] = {ab * cd * efw, ab * cd1 * efw, ab * cd1 * ef1, ab * cd * ef1,
+                      ab1 * cd * ef1, ab1 * cd1 * ef1, ab1 * cd1 * efw, ab1 * cd * efw};
+  float sx = 0.f, sy_ = 0.f, sz_ = 0.f;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    float4 v = __ldg(E + nodes[q]);
+    sx += v.x * w[q]; sy_ += v.y * w[q]; sz_ += v.z * w[q];
+  }
+  ex = sx; ey = sy_; ez = sz_;
+}
+
+// scatter1 kick constants (BeamBunch.f90:2066-2084); fpei uses the
+// default-real literal 1.0e-7 of the reference.
+__device__ __forceinline__ void kick_consts(const Consts& k, double gam, double curr,
+                                            double& xycon, double& tcon) {
+  const double tmpscale = curr / k.Scfreq;
+  const double twopi = 2.0 * k.Pi;
+  const double fpei = k.Clight * k.Clight * 1.00000001168609742e-07;
+  const double bet = sqrt(gam * gam - 1.0) / gam;
+  const double bbyk = bet / k.xk;
+  const double gambet = gam * bet;
+  const double brho = gambet / (k.Clight * k.charge) * k.mass;
+  const double vz0 = bet * k.Clight;
+  const double perv0 = 2.0 * curr * fpei / (brho * vz0 * vz0 * gam * gam);
+  xycon = 0.5 * perv0 * gambet * bbyk * twopi / tmpscale;
+  tcon = bet * xycon * (gam * gam);
+}
+
+// update_CompDom, Flagbc=1 (CompDom.f90:545-557, 614-622): eps is the
+// default-real 1.0/(Meshnum-3.0)
+__device__ __forceinline__ void compdom(Geom& g, int nx, int ny, int nz) {
+  const int mesh[3] = {nx, ny, nz};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    double t1 = g.ptrange[2 * k], t2 = g.ptrange[2 * k + 1];
+    double eps = (double)(1.0f / ((float)mesh[k] - 3.0f));
+    double mn = t1 - eps * (t2 - t1);
+    double mx = t2 + eps * (t2 - t1);
+    g.range[2 * k] = mn;
+    g.range[2 * k + 1] = mx;
+    g.h[k] = (mx - mn) / (double)(mesh[k] - 1);
+    g.hi[k] = 1.0 / g.h[k];
+  }
+}
+
+__device__ __forceinline__ bool finite6(const Particle& p) {
+  return isfinite(p.x) && isfinite(p.px) && isfinite(p.y) && isfinite(p.py) &&
+         isfinite(p.ph) && isfinite(p.pt);
+}
+
+__device__ __forceinline__ long long lin_cell(const Cell& c, int nx, int ny) {
+  return (long long)(c.ix - 1) + (long long)nx * ((c.jx - 1) + (long long)ny * (c.kx - 1));
+}
+
+// ---------------------------------------------------------------------
+// The fused particle pass of step s (one thread per particle per pass,
+// grid-stride).  Per particle, in the reference's order:
+//   [kick]  conv1st z->t, loss test, deposit cell (sort key),
+//           cvbkforth1st t->z->gather frame, scatter1 gather + kick + z frame
+//   [post]  second half map of step s, then the diagnostic1 sums
+//   [pre]   first half map of step s+1 (and pole faces), conv1st range of s+1
+//   write   to the sorted slot of the deposit cell (kick) or in place.
+// The last block to finish reduces moments and range in block order
+// (deterministic) and performs conv1st's current rescale and update_CompDom.
+template <int BLOCK, bool F32>
+__global__ void __launch_bounds__(BLOCK) k_advance(AdvanceArgs a) {
+  __shared__ double red[BLOCK / 32][IMPZ_RAW_LEN];
+  __shared__ double redr[BLOCK / 32][8];
+  __shared__ unsigned int s_last;
+  DevState* st = a.st;
+  const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
+  const StepParams* __restrict__ sp = a.steps + s;
+  const long long n = st->nlocal;
+  const Geom g = st->geom;
+  const double xl = a.k.Scxl, xk = a.k.xk;
+  const bool kick = a.kick != 0;
+  const bool post = a.do_post != 0;
+  const bool mom = post && sp->moments;
+  const bool pre = a.do_pre != 0;
+  const bool rng = pre && sp->range_next;
+  const double gam = sp->gam, rad = sp->rad;
+  const double gam_n = sp[1].gam, rad_n = sp[1].rad;
+  double txy = 0.0, tt = 0.0;
+  if (kick) {
+    double xycon, tcon;
+    kick_consts(a.k, gam, st->current, xycon, tcon);
+    txy = sp->tau * xycon;
+    tt = sp->tau * tcon;
+  }
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const long long G = (long long)nx * ny * nz;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+
+  double acc[IMPZ_RAW_LEN];
+#pragma unroll
+  for (int v = 0; v < IMPZ_RAW_LEN; v++) acc[v] = 0.0;
+  double rmn[3] = {1e300, 1e300, 1e300}, rmx[3] = {-1e300, -1e300, -1e300};
+  long long nlive = 0, nkept = 0;
+  unsigned int err = 0;
+
+  const long long stride = (long long)gridDim.x * BLOCK;
+  const long long nround = (n + stride - 1) / stride * stride;
+  for (long long i = (long long)blockIdx.x * BLOCK + threadIdx.x; i < nround; i += stride) {
+    bool keep = i < n;
+    Particle p;
+    long long key = 0;
+    if (keep) {
+      p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
+      p.py = a.in[3][i]; p.ph = a.in[4][i]; p.pt = a.in[5][i];
+      if (kick) {
+        TFrame t = to_tframe(p, gam, rad, xl);
+        if (t.lost) {
+          keep = false;
+        } else {
+          Cell cd = cic_cell(t.xt, t.yt, t.zt, g);
+          key = cell_inside(cd, nx, ny, nz) ? lin_cell(cd, nx, ny) : G;
+          // cvbkforth1st (BeamBunch.f90:1681-1699); betai reuses conv1st's
+          // tmpbet, which is the same expression of the same operands
+          const double rcp = t.rcp;
+          const double betai = sqrt(t.tmpbet);
+          double ph1 = t.zt * xk / (-(gam * betai));
+          double x1 = t.xt * xk + p.px * ph1 * rcp;
+          double y1 = t.yt * xk + p.py * ph1 * rcp;
+          const double xg = x1 * xl, yg = y1 * xl;
+          const double zg = -(gam * betai * ph1 * xl);
+          // scatter1 (BeamBunch.f90:2121-2177); indices are clamped to the
+          // grid (the reference reads outside it without a check)
+          Cell cg = cic_cell(xg, yg, zg, g);
+          if (!cell_inside(cg, nx, ny, nz)) {
+            err |= DERR_OUTSIDE;
+            cg.ix = min(max(cg.ix, 1), nx - 1);
+            cg.jx = min(max(cg.jx, 1), ny - 1);
+            cg.kx = min(max(cg.kx, 1), nz - 1);
+          }
+          double ex, ey, ez;
+          gather_e<F32>(a.efield, cg, nx, ny, ex, ey, ez);
+          if (F32) {
+            ex = ex * a.efield_scale;
+            ey = ey * a.efield_scale;
+            ez = ez * a.efield_scale;
+          }
+          const double exn = ex * gam, eyn = ey * gam, ezn = ez;
+          p.x = xg * xk;
+          p.px = p.px + txy * exn;
+          p.y = yg * xk;
+          p.py = p.py + txy * eyn;
+          p.ph = zg * xk / (-(gam * betai));
+          p.pt = p.pt - tt * ezn;
+        }
+      }
+    }
+    if (keep) {
+      if (post) {
+        apply_program(p, sp->post);
+        if (mom) moment_accumulate(acc, p);
+      }
+      if (pre) {
+        apply_program(p, sp->pre_next);
+        if (rng) {
+          TFrame t = to_tframe(p, gam_n, rad_n, xl);
+          rmn[0] = fmin(rmn[0], fmin(t.tmpx, t.xt));
+          rmx[0] = fmax(rmx[0], fmax(t.tmpx, t.xt));
+          rmn[1] = fmin(rmn[1], fmin(t.tmpy, t.yt));
+          rmx[1] = fmax(rmx[1], fmax(t.tmpy, t.yt));
+          rmn[2] = fmin(rmn[2], t.zt);
+          rmx[2] = fmax(rmx[2], t.zt);
+          nlive += t.lost ? 0 : 1;
+        }
+      }
+      if (!finite6(p)) err |= DERR_NONFINITE;
+      nkept++;
+    }
+    // destination slot
+    long long dst = i;
+    if (kick) {
+      const unsigned active = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const unsigned grp = __match_any_sync(active, (unsigned long long)key);
+        const int leader = __ffs(grp) - 1;
+        const int rank = __popc(grp & ((1u << lane) - 1u));
+        int base = 0;
+        if (lane == leader) base = atomicAdd(a.cursor + key, __popc(grp));
+        base = __shfl_sync(grp, base, leader);
+        dst = (long long)base + rank + a.bsum[key >> IMPZ_SCAN_LOG];
+        if (dst < 0 || dst >= a.cap) {  // cannot happen when deposit and pass agree
+          err |= DERR_SLOT;
+          keep = false;
+        }
+      }
+    }
+    if (keep) {
+      a.out[0][dst] = p.x; a.out[1][dst] = p.px; a.out[2][dst] = p.y;
+      a.out[3][dst] = p.py; a.out[4][dst] = p.ph; a.out[5][dst] = p.pt;
+      if (a.id_out) a.id_out[dst] = a.id_in[i];
+    }
+  }
+
+  // ---- block reductions
+  if (mom) {
+#pragma unroll
+    for (int v = 0; v < 37; v++) acc[v] = warp_sum(acc[v]);
+#pragma unroll
+    for (int v = 37; v < IMPZ_RAW_LEN; v++) acc[v] = warp_max(acc[v]);
+    if (lane == 0)
+#pragma unroll
+      for (int v = 0; v < IMPZ_RAW_LEN; v++) red[wid][v] = acc[v];
+  }
+  double cnt_l = (double)warp_sum_ll(nlive), cnt_k = (double)warp_sum_ll(nkept);
+  double r[6];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    r[2 * d] = warp_min(rmn[d]);
+    r[2 * d + 1] = warp_max(rmx[d]);
+  }
+  err = __reduce_or_sync(0xffffffffu, err);
+  if (lane == 0) {
+#pragma unroll
+    for (int d = 0; d < 6; d++) redr[wid][d] = r[d];
+    redr[wid][6] = cnt_l;
+    redr[wid][7] = cnt_k;
+    if (err) atomicOr(&st->err, err);
+  }
+  __syncthreads();
+  const int nw = BLOCK / 32;
+  if (mom && threadIdx.x < IMPZ_RAW_LEN) {
+    const int v = threadIdx.x;
+    double x = red[0][v];
+    for (int w = 1; w < nw; w++) x = v < 37 ? x + red[w][v] : fmax(x, red[w][v]);
+    a.mom_part[(size_t)blockIdx.x * IMPZ_RAW_LEN + v] = x;
+  }
+  if (threadIdx.x < 8) {
+    const int v = threadIdx.x;
+    double x = redr[0][v];
+    for (int w = 1; w < nw; w++) {
+      double y = redr[w][v];
+      x = (v >= 6) ? x + y : ((v & 1) ? fmax(x, y) : fmin(x, y));
+    }
+    a.rng_part[(size_t)blockIdx.x * 8 + v] = x;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&st->done_range, 1u) == gridDim.x - 1) ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // ---- last block: fixed-order reduction over blocks, then bookkeeping
+  const int nb = gridDim.x;
+  const int row = a.fixed_step >= 0 ? a.mom_index : s;
+  if (mom && threadIdx.x < IMPZ_RAW_LEN) {
+    const int v = threadIdx.x;
+    volatile double* mp = a.mom_part;
+    double x = mp[v];
+    for (int b = 1; b < nb; b++) {
+      double y = mp[(size_t)b * IMPZ_RAW_LEN + v];
+      x = v < 37 ? x + y : fmax(x, y);
+    }
+    a.mom_out[(size_t)row * IMPZ_MOMREC + v] = x;
+  }
+  __shared__ double fin[8];
+  if (threadIdx.x < 8) {
+    const int v = threadIdx.x;
+    volatile double* rp = a.rng_part;
+    double x = rp[v];
+    for (int b = 1; b < nb; b++) {
+      double y = rp[(size_t)b * 8 + v];
+      x = (v >= 6) ? x + y : ((v & 1) ? fmax(x, y) : fmin(x, y));
+    }
+    fin[v] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const long long kept = (long long)fin[7];
+    if (mom) {
+      double* m = a.mom_out + (size_t)row * IMPZ_MOMREC;
+      m[44] = (double)st->npt;
+      m[45] = (double)kept;
+      m[46] = st->current;
+      m[47] = 0.0;
+    }
+    st->nlocal = kept;
+    if (rng) {
+      Geom ng;
+      for (int d = 0; d < 6; d++) ng.ptrange[d] = fin[d];
+      compdom(ng, nx, ny, nz);
+      st->geom = ng;
+      const long long nptot = (long long)fin[6];
+      // conv1st: Current = Current*nptot/Npt; Npt = nptot
+      st->current = st->current * (double)nptot / (double)st->npt;
+      st->npt = nptot;
+      st->nlive = nptot;
+    }
+    if (a.fixed_step < 0) st->step = s + 1;
+    if (kick) st->parity ^= 1;
+    st->done_range = 0;
+  }
+}
+
+// ---------------------------------------------------------------------
+// Charge deposit.  Each block takes chunks of BLOCK*PPT consecutive
+// particles.  Because particles are kept sorted by the previous step's
+// deposit cell, a chunk covers a narrow range of linear cell indices: its
+// charge is accumulated with shared-memory atomics into a tile that covers
+// [base, base+span] (plus the +nx*ny plane of the upper nodes), and the
+// tile's nonzero entries are flushed with one global atomic each.  Chunks
+// too wide for the tile use global atomics directly.  Accumulation is in
+// int64 fixed point (2^-fixbits of a unit macro-particle charge), so the
+// result does not depend on the order of the additions; the eighth corner
+// takes 2^fixbits minus the other seven, so every live particle deposits
+// exactly one unit.
+template <int BLOCK, int PPT>
+__global__ void __launch_bounds__(BLOCK) k_deposit(DepositArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned long long* tile = reinterpret_cast<unsigned long long*>(smem_raw);
+  int* ctile = reinterpret_cast<int*>(tile + IMPZ_DEP_TILE);
+  __shared__ int s_min, s_max;
+  const DevState* st = a.st;
+  const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
+  const double gam = a.steps[s].gam, rad = a.steps[s].rad;
+  const long long n = st->nlocal;
+  const Geom g = st->geom;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const long long P = (long long)nx * ny;
+  const long long G = P * nz;
+  const double scale = ldexp(1.0, a.fixbits);
+  const long long unit = 1ll << a.fixbits;
+  const int LT = IMPZ_DEP_TILE, LB = IMPZ_DEP_TILE / 2;
+  for (int e = threadIdx.x; e < LT; e += BLOCK) {
+    tile[e] = 0ull;
+    ctile[e] = 0;
+  }
+  const long long chunk = (long long)BLOCK * PPT;
+  for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
+    long long cell[PPT];
+    double wab[PPT], wcd[PPT], wef[PPT];
+    int lmin = INT_MAX, lmax = -1;
+#pragma unroll
+    for (int q = 0; q < PPT; q++) {
+      const long long i = c0 + (long long)q * BLOCK + threadIdx.x;
+      cell[q] = -1;
+      if (i < n) {
+        Particle p;
+        p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
+        p.py = a.in[3][i]; p.ph = a.in[4][i]; p.pt = a.in[5][i];
+        TFrame t = to_tframe(p, gam, rad, a.xl);
+        if (!t.lost) {
+          Cell c = cic_cell(t.xt, t.yt, t.zt, g);
+          if (cell_inside(c, nx, ny, nz)) {
+            cell[q] = lin_cell(c, nx, ny);
+            wab[q] = c.ab; wcd[q] = c.cd; wef[q] = c.ef;
+            lmin = min(lmin, (int)cell[q]);
+            lmax = max(lmax, (int)cell[q]);
+          } else {
+            atomicAdd(a.counts + G, 1);  // live but outside: keeps its sort slot
+          }
+        }
+      }
+    }
+    // block-wide cell range of this chunk
+    if (threadIdx.x == 0) { s_min = INT_MAX; s_max = -1; }
+    __syncthreads();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lmin = min(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+      lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    }
+    if ((threadIdx.x & 31) == 0 && lmax >= 0) {
+      atomicMin(&s_min, lmin);
+      atomicMax(&s_max, lmax);
+    }
+    __syncthreads();
+    const int base = s_min;
+    const long long span = (long long)s_max - s_min;
+    const long long W = span + nx + 2;
+    // 0: global atomics, 1: contiguous tile, 2: two bands (nodes below and
+    // one x-y plane above the chunk's cells)
+    int mode = 0;
+    if (s_max >= 0) {
+      if (P >= LB && W <= LB) mode = 2;
+      else if (W + P <= LT) mode = 1;
+    }
+#pragma unroll
+    for (int q = 0; q < PPT; q++) {
+      if (cell[q] < 0) continue;
+      const double ab = wab[q], cd = wcd[q], ef = wef[q];
+      // weights in the order of deposit_BeamBunch (BeamBunch.f90:3749-3763)
+      const double w7[7] = {ab * cd * ef,
+                            ab * (1.0 - cd) * ef,
+                            ab * (1.0 - cd) * (1.0 - ef),
+                            ab * cd * (1.0 - ef),
+                            (1.0 - ab) * cd * (1.0 - ef),
+                            (1.0 - ab) * (1.0 - cd) * (1.0 - ef),
+                            (1.0 - ab) * (1.0 - cd) * ef};
+      long long qv[8];
+      long long sum7 = 0;
+#pragma unroll
+      for (int k = 0; k < 7; k++) {
+        qv[k] = __double2ll_rn(w7[k] * scale);
+        sum7 += qv[k];
+      }
+      qv[7] = unit - sum7;
+      const long long c = cell[q];
+      const long long node[8] = {c, c + nx, c + nx + P, c + P, c + 1 + P, c + 1 + nx + P,
+                                 c + 1 + nx, c + 1};
+      if (mode == 0) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) atomicAdd(a.rho + node[k], (unsigned long long)qv[k]);
+        atomicAdd(a.counts + c, 1);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          long long o = node[k] - base;
+          if (mode == 2 && o >= P) o = o - P + LB;
+          atomicAdd(tile + o, (unsigned long long)qv[k]);
+        }
+        atomicAdd(ctile + (c - base), 1);
+      }
+    }
+    __syncthreads();
+    if (mode != 0) {
+      // flush the touched part of the tile and clear it for the next chunk
+      const long long lenA = (mode == 2) ? W : W + P;
+      for (long long e = threadIdx.x; e < lenA; e += BLOCK) {
+        unsigned long long v = tile[e];
+        if (v) {
+          atomicAdd(a.rho + base + e, v);
+          tile[e] = 0ull;
+        }
+      }
+      if (mode == 2)
+        for (long long e = threadIdx.x; e < W; e += BLOCK) {
+          unsigned long long v = tile[LB + e];
+          if (v) {
+            atomicAdd(a.rho + base + P + e, v);
+            tile[LB + e] = 0ull;
+          }
+        }
+      for (long long e = threadIdx.x; e <= span; e += BLOCK) {
+        int v = ctile[e];
+        if (v) {
+          atomicAdd(a.counts + base + e, v);
+          ctile[e] = 0;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Exclusive scan of counts[0..G] into per-block local offsets (cursor) and
+// per-block totals (bsum), clearing counts for the next step; the last
+// block turns bsum into exclusive block offsets.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scan(int* counts, int* cursor, int* bsum,
+                                                long long total, DevState* st) {
+  __shared__ int wsum[BLOCK / 32];
+  __shared__ unsigned int s_last;
+  constexpr int PER = (1 << IMPZ_SCAN_LOG) / BLOCK;
+  const long long base = (long long)blockIdx.x << IMPZ_SCAN_LOG;
+  int v[PER];
+  int tsum = 0;
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    long long i = base + (long long)threadIdx.x * PER + j;
+    v[j] = (i < total) ? counts[i] : 0;
+    if (i < total) counts[i] = 0;
+    tsum += v[j];
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int incl = tsum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    int w = lane < BLOCK / 32 ? wsum[lane] : 0;
+    int wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < BLOCK / 32) wsum[lane] = wi - w;  // exclusive warp offsets
+    if (lane == BLOCK / 32 - 1) bsum[blockIdx.x] = wi;
+  }
+  __syncthreads();
+  int run = wsum[wid] + incl - tsum;
+#pragma unroll
+  for (int j = 0; j < PER; j++) {
+    long long i = base + (long long)threadIdx.x * PER + j;
+    if (i < total) cursor[i] = run;
+    run += v[j];
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&st->done_scan, 1u) == gridDim.x - 1) ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    volatile int* b = bsum;
+    int acc = 0;
+    for (int k = 0; k < (int)gridDim.x; k++) {
+      int t = b[k];
+      b[k] = acc;
+      acc += t;
+    }
+    st->done_scan = 0;
+  }
+}
+
+}  // namespace IMPZ_NS
+}  // namespace impz

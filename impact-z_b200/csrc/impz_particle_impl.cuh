@@ -1,0 +1,64 @@
+// Kernel instantiation and launch wrappers for one numerical form
+// (included by impz_particle_exact.cu and impz_particle_fast.cu).
+#include "impz_launch.h"
+#include "impz_particle.cuh"
+
+namespace impz {
+namespace IMPZ_NS {
+
+static const size_t kDepSmem = IMPZ_DEP_TILE * (sizeof(unsigned long long) + sizeof(int));
+
+cudaError_t launch_advance(const AdvanceArgs& a, bool f32, int grid, cudaStream_t s) {
+  if (f32)
+    k_advance<IMPZ_ADV_BLOCK, true><<<grid, IMPZ_ADV_BLOCK, 0, s>>>(a);
+  else
+    k_advance<IMPZ_ADV_BLOCK, false><<<grid, IMPZ_ADV_BLOCK, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+static cudaError_t dep_attr() {
+  static cudaError_t once = cudaFuncSetAttribute(
+      k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)kDepSmem);
+  return once;
+}
+
+cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s) {
+  cudaError_t e = dep_attr();
+  if (e != cudaSuccess) return e;
+  k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT><<<grid, IMPZ_DEP_BLOCK, kDepSmem, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan(int* counts, int* cursor, int* bsum, long long total, DevState* st,
+                        cudaStream_t s) {
+  const long long nb = (total + (1ll << IMPZ_SCAN_LOG) - 1) >> IMPZ_SCAN_LOG;
+  k_scan<IMPZ_SCAN_THREADS><<<(int)nb, IMPZ_SCAN_THREADS, 0, s>>>(counts, cursor, bsum, total, st);
+  return cudaGetLastError();
+}
+
+int max_blocks_advance(bool f32) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (f32)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, true>,
+                                                  IMPZ_ADV_BLOCK, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, false>,
+                                                  IMPZ_ADV_BLOCK, 0);
+  return sms * (per > 0 ? per : 1);
+}
+
+int max_blocks_deposit() {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  dep_attr();
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>,
+                                                IMPZ_DEP_BLOCK, kDepSmem);
+  return sms * (per > 0 ? per : 1);
+}
+
+}  // namespace IMPZ_NS
+}  // namespace impz

@@ -1,0 +1,384 @@
+// impz_poisson.cuh -- open-boundary Poisson solve on the device.
+//
+// Restates openBC3D + greenf1tIntnew (src/Appl/Field.f90:239-519): Hockney's
+// doubled-grid convolution phi = IFFT(FFT(rho_padded) * FFT(G_even)) with the
+// integrated Green's function G, then kick1's finite-difference field
+// (src/Appl/BeamBunch.f90:1784-2005).  Any correct FFT reproduces the
+// reference's FFTPACK convolution to rounding, so the transforms here are the
+// project's own shared-memory radix-2 kernels laid out for the doubled grid:
+//
+//   xy-forward  one block per z plane: int64 charge -> real, R2C along x
+//               (two real rows packed into one complex FFT of length 2Nx),
+//               C2C along y (length 2Ny, upper half zero), spectrum plane out
+//   z-convolve  one block per (ky, tile of kx): C2C along z (length 2Nz,
+//               upper half zero), times the real even G-hat, inverse C2C,
+//               only the Nz planes the crop needs are written back
+//   xy-inverse  one block per z plane < Nz: inverse C2C along y, C2R along x,
+//               potential plane out (only Nx x Ny of the doubled grid)
+//
+// G is even in every direction, so its transform is real and is computed as
+// three DCT-I passes over the octant (Nx+1)(Ny+1)(Nz+1) (two lines packed
+// into one complex FFT: even real sequences have real transforms).  The
+// 1/(n1 n2 n3) inverse normalisation of Field.f90:321-323 is folded into G-hat.
+//
+// Spectrum layout in HBM: S[z][ky][kx], kx fastest, (Nx+1) x 2Ny x Nz complex.
+// Forward passes use decimation in frequency (natural in, bit-reversed out)
+// and inverse passes decimation in time (bit-reversed in, natural out), so no
+// pass ever permutes data explicitly.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "impz_common.h"
+
+namespace impz {
+
+template <typename T> struct Cplx;
+template <> struct Cplx<double> { typedef double2 type; };
+template <> struct Cplx<float> { typedef float2 type; };
+
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename C>
+__device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+
+__device__ __forceinline__ int bitrev(int v, int logn) {
+  return (int)(__brev((unsigned)v) >> (32 - logn));
+}
+
+// Radix-2 butterflies over `nlines` lines in shared memory; element j of
+// line l sits at buf[l*lstride + j].  tw[k] = exp(-2 pi i k / n), k < n/2.
+// DIF: natural order in, bit-reversed out.  DIT: bit-reversed in, natural out.
+template <typename C>
+__device__ void fft_dif(C* buf, int logn, int nlines, int lstride, int sign, const C* tw) {
+  const int n = 1 << logn, nh = n >> 1;
+  const int total = nlines * nh;
+  for (int lh = logn - 1; lh >= 0; lh--) {
+    const int half = 1 << lh;
+    const int tsh = logn - 1 - lh;  // twiddle index multiplier log2(n/(2*half))
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      const int l = b >> (logn - 1), r = b & (nh - 1);
+      const int k = r & (half - 1);
+      const int i0 = ((r >> lh) << (lh + 1)) + k, i1 = i0 + half;
+      C w = tw[k << tsh];
+      if (sign > 0) w.y = -w.y;
+      C* L = buf + l * lstride;
+      C u = L[i0], v = L[i1];
+      L[i0] = cadd(u, v);
+      L[i1] = cmul(csub(u, v), w);
+    }
+    __syncthreads();
+  }
+}
+
+template <typename C>
+__device__ void fft_dit(C* buf, int logn, int nlines, int lstride, int sign, const C* tw) {
+  const int n = 1 << logn, nh = n >> 1;
+  const int total = nlines * nh;
+  for (int lh = 0; lh < logn; lh++) {
+    const int half = 1 << lh;
+    const int tsh = logn - 1 - lh;
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      const int l = b >> (logn - 1), r = b & (nh - 1);
+      const int k = r & (half - 1);
+      const int i0 = ((r >> lh) << (lh + 1)) + k, i1 = i0 + half;
+      C w = tw[k << tsh];
+      if (sign > 0) w.y = -w.y;
+      C* L = buf + l * lstride;
+      C u = L[i0], v = cmul(L[i1], w);
+      L[i0] = cadd(u, v);
+      L[i1] = csub(u, v);
+    }
+    __syncthreads();
+  }
+}
+
+struct PoissonDims {
+  int nx, ny, nz;
+  int lx, ly, lz;  // log2 of the doubled lengths 2nx, 2ny, 2nz
+};
+
+// ---------------------------------------------------------------------
+// xy-forward: one block per z plane k < nz.
+// smem: Z[ny/2][2nx] (packed row pairs) and Tm[nx+1][2ny+1] (y lines).
+template <typename T>
+__global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho,
+                             const DevState* st, double qscale,
+                             typename Cplx<T>::type* __restrict__ S,
+                             const typename Cplx<T>::type* __restrict__ twx,
+                             const typename Cplx<T>::type* __restrict__ twy) {
+  typedef typename Cplx<T>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = d.nx, ny = d.ny, n1 = 2 * nx, n2 = 2 * ny;
+  const int tp = n2 + 1;  // padded y-line pitch
+  C* Z = reinterpret_cast<C*>(smem_raw);
+  C* Tm = Z + (ny / 2) * n1;
+  const int k = blockIdx.x;
+  const size_t plane = (size_t)nx * ny * k;
+  (void)st;
+  // load two real rows per complex line, natural order, zero padded; clear rho
+  const int hy = ny / 2;
+  for (int e = threadIdx.x; e < hy * n1; e += blockDim.x) {
+    const int l = e / n1, j = e - l * n1;
+    C z;
+    z.x = 0; z.y = 0;
+    if (j < nx) {
+      const size_t ia = plane + (size_t)l * nx + j, ib = plane + (size_t)(l + hy) * nx + j;
+      const long long qa = (long long)rho[ia], qb = (long long)rho[ib];
+      z.x = (T)((double)qa * qscale);
+      z.y = (T)((double)qb * qscale);
+      rho[ia] = 0ull;
+      rho[ib] = 0ull;
+    }
+    Z[l * n1 + j] = z;
+  }
+  __syncthreads();
+  fft_dif<C>(Z, d.lx, hy, n1, -1, twx);
+  // unpack: row a = (Z(k)+conj(Z(n1-k)))/2, row b = (Z(k)-conj(Z(n1-k)))/(2i),
+  // k = 0..nx, into y lines Tm[kx][y] (natural y, zero padded to 2ny)
+  for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
+    const int kx = e / n2, y = e - kx * n2;
+    C v;
+    v.x = 0; v.y = 0;
+    if (y < ny) {
+      const int l = y < hy ? y : y - hy;
+      const C* L = Z + l * n1;
+      const C zk = L[bitrev(kx, d.lx)];
+      const C zm = L[bitrev((n1 - kx) & (n1 - 1), d.lx)];
+      if (y < hy) {
+        v.x = (T)0.5 * (zk.x + zm.x);
+        v.y = (T)0.5 * (zk.y - zm.y);
+      } else {
+        v.x = (T)0.5 * (zk.y + zm.y);
+        v.y = (T)0.5 * (zm.x - zk.x);
+      }
+    }
+    Tm[kx * tp + y] = v;
+  }
+  __syncthreads();
+  fft_dif<C>(Tm, d.ly, nx + 1, tp, -1, twy);
+  // store S[k][ky][kx], kx fastest
+  C* Sk = S + (size_t)k * n2 * (nx + 1);
+  for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
+    const int ky = e / (nx + 1), kx = e - ky * (nx + 1);
+    Sk[e] = Tm[kx * tp + bitrev(ky, d.ly)];
+  }
+}
+
+// z-convolve: block = (tile of TKX kx values, one ky).
+template <typename T, int TKX>
+__global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__ S,
+                             const T* __restrict__ ghat,
+                             const typename Cplx<T>::type* __restrict__ twz) {
+  typedef typename Cplx<T>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = d.nx, ny = d.ny, nz = d.nz, n2 = 2 * ny, n3 = 2 * nz;
+  const int lp = n3 + 1;
+  C* L = reinterpret_cast<C*>(smem_raw);
+  const int kx0 = blockIdx.x * TKX;
+  const int ky = blockIdx.y;
+  const int ntk = min(TKX, nx + 1 - kx0);
+  const size_t pstride = (size_t)n2 * (nx + 1);  // one z plane of S
+  C* base = S + (size_t)ky * (nx + 1) + kx0;
+  for (int e = threadIdx.x; e < TKX * n3; e += blockDim.x) {
+    const int z = e / TKX, t = e - z * TKX;
+    C v;
+    v.x = 0; v.y = 0;
+    if (z < nz && t < ntk) v = base[(size_t)z * pstride + t];
+    L[t * lp + z] = v;
+  }
+  __syncthreads();
+  fft_dif<C>(L, d.lz, TKX, lp, -1, twz);
+  // multiply by G-hat (bit-reversed positions); G-hat octant [kz'][ky'][kx]
+  const int kyp = ky <= ny ? ky : n2 - ky;
+  const size_t gy = (size_t)(nx + 1), gz = (size_t)(nx + 1) * (ny + 1);
+  for (int e = threadIdx.x; e < TKX * n3; e += blockDim.x) {
+    const int t = e / n3, pos = e - t * n3;
+    if (t >= ntk) continue;
+    const int kz = bitrev(pos, d.lz);
+    const int kzp = kz <= nz ? kz : n3 - kz;
+    const T gv = ghat[(size_t)kzp * gz + (size_t)kyp * gy + kx0 + t];
+    C& v = L[t * lp + pos];
+    v.x *= gv;
+    v.y *= gv;
+  }
+  __syncthreads();
+  fft_dit<C>(L, d.lz, TKX, lp, +1, twz);
+  for (int e = threadIdx.x; e < TKX * nz; e += blockDim.x) {
+    const int z = e / TKX, t = e - z * TKX;
+    if (t < ntk) base[(size_t)z * pstride + t] = L[t * lp + z];
+  }
+}
+
+// xy-inverse: one block per z plane k < nz; phi out (nx, ny, nz) real.
+template <typename T>
+__global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __restrict__ S,
+                             T* __restrict__ phi,
+                             const typename Cplx<T>::type* __restrict__ twx,
+                             const typename Cplx<T>::type* __restrict__ twy) {
+  typedef typename Cplx<T>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int nx = d.nx, ny = d.ny, n1 = 2 * nx, n2 = 2 * ny;
+  const int tp = n2 + 1;
+  const int hy = ny / 2;
+  C* Z = reinterpret_cast<C*>(smem_raw);
+  C* Tm = Z + hy * n1;
+  const int k = blockIdx.x;
+  const C* Sk = S + (size_t)k * n2 * (nx + 1);
+  // y lines in bit-reversed order for the DIT inverse
+  for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
+    const int ky = e / (nx + 1), kx = e - ky * (nx + 1);
+    Tm[kx * tp + bitrev(ky, d.ly)] = Sk[e];
+  }
+  __syncthreads();
+  fft_dit<C>(Tm, d.ly, nx + 1, tp, +1, twy);
+  // C2R along x for row pairs (y, y+ny/2), y < ny/2: Z(kx) = Xa(kx) + i Xb(kx),
+  // with X(n1-kx) = conj(X(kx)); placed bit-reversed for the DIT inverse
+  for (int e = threadIdx.x; e < hy * n1; e += blockDim.x) {
+    const int l = e / n1, kk = e - l * n1;
+    const int kxs = kk <= nx ? kk : n1 - kk;
+    C xa = Tm[kxs * tp + l], xb = Tm[kxs * tp + l + hy];
+    if (kk > nx) { xa.y = -xa.y; xb.y = -xb.y; }
+    C z;
+    z.x = xa.x - xb.y;
+    z.y = xa.y + xb.x;
+    Z[l * n1 + bitrev(kk, d.lx)] = z;
+  }
+  __syncthreads();
+  fft_dit<C>(Z, d.lx, hy, n1, +1, twx);
+  T* ph = phi + (size_t)nx * ny * k;
+  for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
+    const int y = e / nx, x = e - y * nx;
+    const C v = Z[(y < hy ? y : y - hy) * n1 + x];
+    ph[e] = y < hy ? v.x : v.y;
+  }
+}
+
+// ---------------------------------------------------------------------
+// greenf1tIntnew corner antiderivative (Field.f90:392-418), FP64, at the
+// (nx+2)(ny+2)(nz+2) corners v = (i-1)h - h/2.
+__global__ void k_igf_corners(int nx, int ny, int nz, const DevState* st, double* F) {
+  const int ax = nx + 2, ay = ny + 2, az = nz + 2;
+  const long long total = (long long)ax * ay * az;
+  const double hx = st->geom.h[0], hy = st->geom.h[1], hz = st->geom.h[2];
+  const double hxyz = hx * hy * hz;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i0 = (int)(e % ax);
+    const int j0 = (int)((e / ax) % ay);
+    const int k0 = (int)(e / ((long long)ax * ay));
+    const double v1 = (double)i0 * hx - hx / 2;
+    const double v2 = (double)j0 * hy - hy / 2;
+    const double v3 = (double)k0 * hz - hz / 2;
+    const double rr = sqrt(v1 * v1 + v2 * v2 + v3 * v3);
+    const double aa = -(v3 * v3 * atan(v1 * v2 / (v3 * rr)) / 2);
+    const double bb = -(v2 * v2 * atan(v1 * v3 / (v2 * rr)) / 2);
+    const double cc = -(v1 * v1 * atan(v2 * v3 / (v1 * rr)) / 2);
+    const double dd = v2 * v3 * log(v1 + rr);
+    const double ee = v1 * v3 * log(v2 + rr);
+    const double ff = v1 * v2 * log(v3 + rr);
+    const double gg2 = aa + bb + cc + dd + ee + ff;
+    F[e] = gg2 / hxyz;
+  }
+}
+
+// 8-corner difference (Field.f90:420-428) into the octant (nx+1)(ny+1)(nz+1)
+__global__ void k_igf_green(int nx, int ny, int nz, const double* __restrict__ F,
+                            double* __restrict__ Gt) {
+  const int ax = nx + 2, ay = ny + 2;
+  const int gx = nx + 1, gy = ny + 1, gz = nz + 1;
+  const long long total = (long long)gx * gy * gz;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % gx);
+    const int j = (int)((e / gx) % gy);
+    const int k = (int)(e / ((long long)gx * gy));
+#define IMPZ_F(a, b, c) __ldg(F + (a) + (size_t)ax * ((b) + (size_t)ay * (c)))
+    Gt[e] = IMPZ_F(i + 1, j + 1, k + 1) - IMPZ_F(i, j + 1, k + 1) - IMPZ_F(i + 1, j, k + 1) +
+            IMPZ_F(i, j, k + 1) - IMPZ_F(i + 1, j + 1, k) + IMPZ_F(i, j + 1, k) +
+            IMPZ_F(i + 1, j, k) - IMPZ_F(i, j, k);
+#undef IMPZ_F
+  }
+}
+
+// DCT-I (transform of the even extension) along one axis of the FP64 octant.
+// Lines have n+1 points spaced by `es`; TL lines spaced by `ls` are handled
+// by one block (consecutive inner lines for coalescing), outer lines are
+// spaced by `os`.  Pairs of lines share one complex FFT of length 2n.
+// If out != nullptr the result, times `scale`, is written there as T.
+template <typename T, int TL>
+__global__ void k_dct1(double* __restrict__ g, int logn, long long es, long long ls,
+                       int ninner, long long os, T* __restrict__ out, double scale,
+                       const double2* __restrict__ tw) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* L = reinterpret_cast<double2*>(smem_raw);
+  const int n = 1 << (logn - 1);  // octant points - 1
+  const int n2 = 2 * n;
+  const int lp = n2 + 1;
+  const int l0 = blockIdx.x * TL;
+  const int nl = min(TL, ninner - l0);
+  double* base = g + (long long)blockIdx.y * os + (long long)l0 * ls;
+  // pair line t with line t + TL/2 (real and imaginary parts)
+  const int np = TL / 2;
+  for (int e = threadIdx.x; e < np * n2; e += blockDim.x) {
+    const int m = e / np, t = e - m * np;  // t fastest for coalescing
+    const int mm = m <= n ? m : n2 - m;
+    double2 v;
+    v.x = t < nl ? base[(long long)t * ls + mm * es] : 0.0;
+    v.y = t + np < nl ? base[(long long)(t + np) * ls + mm * es] : 0.0;
+    L[t * lp + m] = v;
+  }
+  __syncthreads();
+  fft_dif<double2>(L, logn, np, lp, -1, tw);
+  for (int e = threadIdx.x; e < np * (n + 1); e += blockDim.x) {
+    const int m = e / np, t = e - m * np;
+    const double2 v = L[t * lp + bitrev(m, logn)];
+    if (out) {
+      T* ob = out + (long long)blockIdx.y * os + (long long)l0 * ls;
+      if (t < nl) ob[(long long)t * ls + m * es] = (T)(v.x * scale);
+      if (t + np < nl) ob[(long long)(t + np) * ls + m * es] = (T)(v.y * scale);
+    } else {
+      if (t < nl) base[(long long)t * ls + m * es] = v.x;
+      if (t + np < nl) base[(long long)(t + np) * ls + m * es] = v.y;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------
+// kick1_BeamBunch finite differences (BeamBunch.f90:1784-2005), one rank,
+// open BC: centred inside, one-sided on the faces.  Out: {Ex,Ey,Ez,0}.
+template <typename T>
+__global__ void k_efield(int nx, int ny, int nz, const T* __restrict__ phi,
+                         const DevState* st, T* __restrict__ E) {
+  const long long G = (long long)nx * ny * nz;
+  const T hxi = (T)st->geom.hi[0], hyi = (T)st->geom.hi[1], hzi = (T)st->geom.hi[2];
+  const T half = (T)0.5;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < G;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % nx);
+    const int j = (int)((e / nx) % ny);
+    const int k = (int)(e / ((long long)nx * ny));
+    const long long sy = nx, sz = (long long)nx * ny;
+    T ex, ey, ez;
+    if (i == 0) ex = hxi * (phi[e] - phi[e + 1]);
+    else if (i == nx - 1) ex = hxi * (phi[e - 1] - phi[e]);
+    else ex = half * hxi * (phi[e - 1] - phi[e + 1]);
+    if (j == 0) ey = hyi * (phi[e] - phi[e + sy]);
+    else if (j == ny - 1) ey = hyi * (phi[e - sy] - phi[e]);
+    else ey = half * hyi * (phi[e - sy] - phi[e + sy]);
+    if (k == 0) ez = hzi * (phi[e] - phi[e + sz]);
+    else if (k == nz - 1) ez = hzi * (phi[e - sz] - phi[e]);
+    else ez = half * hzi * (phi[e - sz] - phi[e + sz]);
+    T* o = E + 4 * e;
+    o[0] = ex;
+    o[1] = ey;
+    o[2] = ez;
+    o[3] = (T)0;
+  }
+}
+
+}  // namespace impz

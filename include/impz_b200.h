@@ -1,0 +1,159 @@
+/*
+ * impz_b200.h -- C ABI of the B200 space-charge kick and element push.
+ *
+ * Drop-in for the per-step calls that IMPACT-Z's step loop
+ * (src/Contrl/AccSimulator.f90:1099-1488) makes into BeamBunch, CompDom and
+ * FieldQuant.  Every entry point takes plain pointers and scalars (a Fortran
+ * caller binds them with iso_c_binding; see impact-z_b200/fortran/), returns
+ * IMPZ_OK (0) or a negative IMPZ_ERR_* code, and never aborts the caller.
+ * Arrays follow the reference's column-major layout:
+ *   particles  Pts1(9,n): pts[9*i + c], c = x/Scxl, gbx, y/Scxl, gby, phase,
+ *              gamma0-gamma, q/m, charge weight, id   (BeamBunch.f90:9-12)
+ *   grids      (nx,ny,nz): g[i + nx*(j + ny*k)]
+ *   6x6 maps   xm(6,6): xm[(j-1) + 6*(k-1)]
+ * All device work of a bunch runs on that bunch's CUDA stream; the calls
+ * are synchronous unless the name says otherwise.  One host thread at a time
+ * may use a given handle.
+ */
+#ifndef IMPZ_B200_H
+#define IMPZ_B200_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IMPZ_OK 0
+#define IMPZ_ERR_ARG (-1)         /* invalid argument */
+#define IMPZ_ERR_NOMEM (-2)       /* device or host allocation failed */
+#define IMPZ_ERR_CUDA (-3)        /* CUDA runtime error (see impz_last_cuda_error) */
+#define IMPZ_ERR_UNSUPPORTED (-4) /* element / option outside the supported path */
+#define IMPZ_ERR_NONUNIFORM (-5)  /* q/m or charge weight differ between particles */
+#define IMPZ_ERR_STATE (-6)       /* call out of order (e.g. kick before deposit) */
+#define IMPZ_ERR_NONFINITE (-7)   /* a particle coordinate became Inf/NaN */
+#define IMPZ_ERR_NODEVICE (-8)    /* no CUDA device / extension built without GPU */
+#define IMPZ_ERR_BUDGET (-9)      /* admission refused: footprint above budget */
+
+/* numerical forms */
+#define IMPZ_FORM_FP64 0     /* plain: all FP64, reference operation order, no FMA */
+#define IMPZ_FORM_FP32CONV 1 /* FP32 FFT convolution and field gather, FP64 elsewhere */
+
+/* bunch creation flags */
+#define IMPZ_FLAG_TRACK_IDS 1 /* carry Pts1(9,:) through the per-step particle sort */
+
+#define IMPZ_RAW_LEN 44   /* 37 moment sums, 6 |max|, max r^2 */
+#define IMPZ_DIAG_LEN 45  /* one row of fort.18/24-30, see impz_diag_row */
+#define IMPZ_MOMREC 48    /* raw record: IMPZ_RAW_LEN values, Npt, Nptlocal, Current, 0 */
+
+typedef struct impz_bunch_s* impz_bunch_t;
+
+/* One lattice line of ImpactZ.in: "L nseg mapstp type v1 .. v24 /"
+ * (src/Contrl/Input.f90:300-315).  Param(1) of the reference element is
+ * zedge, Param(k) = val[k-2] for k >= 2 (AccSimulator.f90:262-330).
+ * Supported types: 0 drift, 1 quadrupole (gradient, or K map when
+ * v2 in (-10,-1e-6)), 4 dipole (file ID v3 <= 200: no CSR), 101..106 RF gaps
+ * as the ideal-RF model (v4 < 0) and 103 (CCL) as the RK6 linear map over
+ * the on-axis table zdat/edat/epdat/eppdat (rfdataN.in, read1_Data). */
+typedef struct {
+  int type;
+  int nseg;
+  int mapstp;
+  int ndata;
+  double length;
+  double val[24];
+  const double* zdat;
+  const double* edat;
+  const double* epdat;
+  const double* eppdat;
+} impz_elem_t;
+
+/* ---- library ------------------------------------------------------------ */
+const char* impz_version(void);
+const char* impz_error_string(int code);
+const char* impz_last_cuda_error(void);
+/* Select the CUDA device for subsequent calls on this host thread. */
+int impz_set_device(int device);
+
+/* ---- BeamBunch / FieldQuant / CompDom lifetime ------------------------------ */
+/* construct_BeamBunch + setpts (BeamBunch.f90:41-60, 3632-3644) together with
+ * construct_CompDom/construct_FieldQuant of one rank: uploads Pts1(9,n) into
+ * device SoA state and sizes the nx*ny*nz grid (powers of two, >= 4).
+ * freq is Scfreq (PhysConst.f90:25-35).  refptcl[6] as BeamBunch%refptcl. */
+int impz_bunch_create(const double* pts, long long n, double current, double mass,
+                      double charge, double freq, const double refptcl[6], int nx, int ny,
+                      int nz, int form, int flags, impz_bunch_t* out);
+/* getpts_BeamBunch (BeamBunch.f90:3663-3675): copies the live particles back
+ * into pts (capacity cap particles); *n receives the live count.  Without
+ * IMPZ_FLAG_TRACK_IDS column 9 is filled with 1..n in the current order. */
+int impz_bunch_download(impz_bunch_t b, double* pts, long long cap, long long* n);
+int impz_bunch_destroy(impz_bunch_t b);
+/* Current, Npt, Nptlocal, refptcl(1..6), z, device bytes (11 doubles). */
+int impz_bunch_info(impz_bunch_t b, double info[11]);
+/* The bunch's CUDA stream (cudaStream_t) for callers that interleave work. */
+void* impz_bunch_stream(impz_bunch_t b);
+
+/* ---- the reference's per-step call surface ---------------------------- */
+/* drift1_BeamBunch (BeamBunch.f90:250-464): one half-step map of element e
+ * of length tau at position *z; *z += tau, *ihlf += 1.  nst is the segment
+ * (1..nseg) for the ideal-RF entrance/exit kicks.  zedge is Param(1). */
+int impz_map_half(impz_bunch_t b, const impz_elem_t* e, double zedge, double* z, double tau,
+                  int nst, int* ihlf);
+/* Fpol_Dipole at a bend entrance with the constants of AccSimulator.f90:
+ * 1057-1093, after refptcl(5) += L/(Scxl*beta0) (AccSimulator.f90:1063). */
+int impz_bend_entry(impz_bunch_t b, const impz_elem_t* e);
+/* Sector_Dipole(tau) inside the bend entered last (Dipole.f90:693-788); *z += tau. */
+int impz_bend_sector(impz_bunch_t b, double* z, double tau);
+/* Bpol_Dipole at the exit of the bend entered last (AccSimulator.f90:1491-1494). */
+int impz_bend_exit(impz_bunch_t b);
+/* conv1st_BeamBunch (Flagbc=1) + update_CompDom (BeamBunch.f90:1252-1663,
+ * CompDom.f90:509-823): z->t range and loss count on the device, current
+ * rescale.  Outputs (each may be NULL): *nptot, ptrange[6] (the particle
+ * range), range[6] (grid xmin..zmax) and msize[3] (hx,hy,hz). */
+int impz_sc_prepare(impz_bunch_t b, double piperad, double piperad2, long long* nptot,
+                    double ptrange[6], double range[6], double msize[3]);
+/* charge_BeamBunch/deposit_BeamBunch (BeamBunch.f90:3535-3768): CIC into
+ * int64 fixed point.  chgdens (nx*ny*nz, may be NULL) receives the FP64 grid
+ * in Coulomb like the reference; counts (may be NULL) the per-cell counts. */
+int impz_deposit(impz_bunch_t b, double* chgdens, int* counts);
+/* update3O_FieldQuant/openBC3D (Field.f90:108-331) on the deposited charge;
+ * phi (nx*ny*nz, may be NULL) receives the potential as the reference's FieldQ. */
+int impz_poisson_open(impz_bunch_t b, double* phi);
+/* cvbkforth1st + kick1 + scatter1 (BeamBunch.f90:1667-2181) with the
+ * potential of the last impz_poisson_open; drops the particles conv1st lost
+ * and re-sorts the bunch by deposit cell.  egrid (3*nx*ny*nz, may be NULL)
+ * receives Ex, Ey, Ez as kick1's egx/egy/egz. */
+int impz_kick(impz_bunch_t b, double tau, double* egrid);
+/* diagnostic1_Output sums (Output.f90:133-245) of the current state:
+ * rec[IMPZ_MOMREC] = 37 sums, 6 |max|, max r^2, Npt, Nptlocal, Current, 0. */
+int impz_moments(impz_bunch_t b, double rec[IMPZ_MOMREC]);
+/* diagnostic1_Output's formulas and write columns (Output.f90:247-352):
+ * row[0]=z, [1..5] fort.18, [6..11] fort.24, [12..17] fort.25,
+ * [18..23] fort.26, [24..29] fort.27, [30..32] fort.28, [33..38] fort.29,
+ * [39..44] fort.30.  Host-only arithmetic. */
+int impz_diag_row(double z, const double rec[IMPZ_MOMREC], const double refptcl[6],
+                  double mass, double freq, double row[IMPZ_DIAG_LEN]);
+
+/* ---- whole-lattice runner ---------------------------------------------- */
+/* run_AccSimulator's element/segment loop (AccSimulator.f90:742-1504) for
+ * Flagmap=1, Flagbc=1, Flagerr=0, no wake/CSR, one rank, over elements
+ * [0,nelem).  Every step is one fused particle pass plus deposit and field
+ * solve, replayed from a CUDA graph.  recs (capacity maxrec records of
+ * IMPZ_MOMREC doubles, may be NULL) receives the initial record and one per
+ * step; zs (may be NULL) the z of each record; *nrec their number. */
+int impz_run(impz_bunch_t b, const impz_elem_t* elems, int nelem, double* recs, double* zs,
+             int maxrec, int* nrec);
+/* The same, but returns after enqueuing (records land in device memory and
+ * are fetched by impz_run_fetch); lets one host thread drive many bunches. */
+int impz_run_async(impz_bunch_t b, const impz_elem_t* elems, int nelem);
+int impz_run_fetch(impz_bunch_t b, double* recs, double* zs, int maxrec, int* nrec);
+/* Number of steps (records - 1) impz_run would take for this lattice. */
+int impz_count_steps(const impz_elem_t* elems, int nelem);
+
+/* Host-side maps (for checking and for callers that keep their own loop):
+ * maplinear_Quadrupole (Quadrupole.f90:120-252) and maplinear_CCL
+ * (CCL.f90:122-328) by the same RK6; refpt is updated like the reference. */
+int impz_maplinear(const impz_elem_t* e, double zedge, double t, double tau,
+                   double refpt[6], double charge, double mass, double freq, double xm[36]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1297 @@
+/*
+ * impz_oracle.c -- CPU restatement of IMPACT-Z's per-step space-charge kick
+ * and element push.  TEST INFRASTRUCTURE ONLY (the checker and the timed CPU
+ * baseline); the product never links it.  PARITY UNPINNED: no Fortran
+ * compiler is available to run the reference, and the reference ships no
+ * golden outputs; see impz_oracle.h.
+ *
+ * Every routine cites the Fortran it restates (paths relative to the
+ * IMPACT-Z tree).  Expressions keep the reference's evaluation order
+ * (Fortran evaluates a*b*c as (a*b)*c, x**2 as x*x, x**3 as (x*x)*x) and
+ * its default-real (FP32) literals where they change the value:
+ *   asin(1.0) in conv1st, 1.0/(Meshnum-3.0) in update_CompDom,
+ *   1.0e-7 in scatter1, (1.0/3.0) in diagnostic1.
+ * Build with -ffp-contract=off: the x86-64 reference build issues no FMA.
+ */
+#include "impz_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------ */
+static struct {
+  double Pi, Clight, Scxl, Rad2deg, Scfreq;
+} PC;
+
+static int g_threads = 1;
+
+void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+
+/* PhysConst.f90:25-35 */
+void orc_physconst(double freq) {
+  PC.Clight = 299792458.0;
+  PC.Pi = 2 * asin(1.0);
+  PC.Scxl = PC.Clight / (2 * PC.Pi * freq);
+  PC.Rad2deg = 180.0 / PC.Pi;
+  PC.Scfreq = freq;
+}
+
+void orc_get_physconst(double out[5]) {
+  out[0] = PC.Pi;
+  out[1] = PC.Clight;
+  out[2] = PC.Scxl;
+  out[3] = PC.Rad2deg;
+  out[4] = PC.Scfreq;
+}
+
+#define P(i, c) pts[9 * (size_t)(i) + (c)]
+
+/* ------------------------------------------------------------------ */
+/* drift1_BeamBunch, bitype 0: exact drift (BeamBunch.f90:276-298) */
+void orc_drift_exact(double *pts, int n, double refptcl[6], double tau) {
+  const double Scxl = PC.Scxl;
+  double gam0 = -refptcl[5];
+  double gambet0 = sqrt(gam0 * gam0 - 1.0);
+  double beta0 = gambet0 / gam0;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int i = 0; i < n; i++) {
+    double tmppx = P(i, 1), tmppy = P(i, 3), tmppt = P(i, 5);
+    double d = tmppt - gam0;
+    double tmph = sqrt(((d * d - 1) - tmppx * tmppx) - tmppy * tmppy);
+    P(i, 0) = P(i, 0) + ((tmppx * tau) / tmph) / Scxl;
+    P(i, 2) = P(i, 2) + ((tmppy * tau) / tmph) / Scxl;
+    P(i, 4) = P(i, 4) - ((1. / beta0 + (tmppt - gam0) / tmph) * tau) / Scxl;
+  }
+  refptcl[4] = refptcl[4] + tau / (Scxl * beta0);
+}
+
+/* ------------------------------------------------------------------ */
+/* rk6i_* (Quadrupole.f90:202-252, identical in DriftTube/CCL): 8-stage RK6 */
+typedef void (*orc_rhs)(double t, const double *y, double *f, const void *ctx);
+
+static void rk6i(double h, int ns, double *t, double *y, orc_rhs fn, const void *ctx) {
+  enum { NV = 18 };
+  double yt[NV], a[NV], b[NV], c[NV], d[NV], e[NV], f[NV], g[NV], o[NV], p[NV];
+  double tint = *t, tt;
+  int v;
+  for (int i = 1; i <= ns; i++) {
+    fn(*t, y, f, ctx);
+    for (v = 0; v < NV; v++) a[v] = h * f[v];
+    for (v = 0; v < NV; v++) yt[v] = y[v] + a[v] / 9.0;
+    tt = *t + h / 9.0;
+    fn(tt, yt, f, ctx);
+    for (v = 0; v < NV; v++) b[v] = h * f[v];
+    for (v = 0; v < NV; v++) yt[v] = y[v] + (a[v] + 3.0 * b[v]) / 24.0;
+    tt = *t + h / 6.0;
+    fn(tt, yt, f, ctx);
+    for (v = 0; v < NV; v++) c[v] = h * f[v];
+    for (v = 0; v < NV; v++) yt[v] = y[v] + ((a[v] - 3.0 * b[v]) + 4.0 * c[v]) / 6.0;
+    tt = *t + h / 3.0;
+    fn(tt, yt, f, ctx);
+    for (v = 0; v < NV; v++) d[v] = h * f[v];
+    for (v = 0; v < NV; v++)
+      yt[v] = y[v] + (((278.0 * a[v] - 945.0 * b[v]) + 840.0 * c[v]) + 99.0 * d[v]) / 544.0;
+    tt = *t + .5 * h;
+    fn(tt, yt, f, ctx);
+    for (v = 0; v < NV; v++) e[v] = h * f[v];
+    for (v = 0; v < NV; v++)
+      yt[v] = y[v] + (((((-106.0 * a[v]) + 273.0 * b[v]) - 104.0 * c[v]) - 107.0 * d[v]) +
+                      48.0 * e[v]) / 6.0;
+    tt = *t + 2.0 * h / 3.0;
+    fn(tt, yt, f, ctx);
+    for (v = 0; v < NV; v++) g[v] = h * f[v];
+    for (v = 0; v < NV; v++)
+      yt[v] = y[v] + (((((110974.0 * a[v] - 236799.0 * b[v]) + 68376.0 * c[v]) +
+                        103803.0 * d[v]) - 10240.0 * e[v]) + 1926.0 * g[v]) / 45648.0;
+    tt = *t + 5.0 * h / 6.0;
+    fn(tt, yt, f, ctx);
+    for (v = 0; v < NV; v++) o[v] = h * f[v];
+    for (v = 0; v < NV; v++)
+      yt[v] = y[v] + ((((((-101195.0 * a[v]) + 222534.0 * b[v]) - 71988.0 * c[v]) -
+                         26109.0 * d[v]) - 2.e4 * e[v]) - 72.0 * g[v] + 22824.0 * o[v]) /
+                         25994.0;
+    tt = *t + h;
+    fn(tt, yt, f, ctx);
+    for (v = 0; v < NV; v++) p[v] = h * f[v];
+    for (v = 0; v < NV; v++)
+      y[v] = y[v] + ((((((41.0 * a[v] + 216.0 * c[v]) + 27.0 * d[v]) + 272.0 * e[v]) +
+                       27.0 * g[v]) + 216.0 * o[v]) + 41.0 * p[v]) / 840.0;
+    *t = tint + i * h;
+  }
+}
+
+/* the 18 linear-ODE derivatives shared by intfunc1_* given s11,s33,s55 */
+static void lin_rhs(const double *y, double *f, double s11, double s33, double s55) {
+  const double Scxl = PC.Scxl;
+  f[6] = y[7] / Scxl;
+  f[7] = -s11 * y[6];
+  f[8] = y[9] / Scxl;
+  f[9] = -s11 * y[8];
+  f[10] = y[11] / Scxl;
+  f[11] = -s33 * y[10];
+  f[12] = y[13] / Scxl;
+  f[13] = -s33 * y[12];
+  f[14] = y[15] / Scxl;
+  f[15] = -s55 * y[14];
+  f[16] = y[17] / Scxl;
+  f[17] = -s55 * y[16];
+}
+
+typedef struct { double bgrad, qmcc; } quad_ctx;
+
+/* intfunc1_Quadrupole (Quadrupole.f90:254-305), constant gradient */
+static void quad_rhs(double t, const double *y, double *f, const void *vctx) {
+  (void)t;
+  const quad_ctx *q = (const quad_ctx *)vctx;
+  double gamma0, beta0, gbet, brho, s11, s33, s55;
+  f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+  gamma0 = -y[5];
+  beta0 = sqrt(gamma0 * gamma0 - 1.) / gamma0;
+  gbet = sqrt((gamma0 - 1.0) * (gamma0 + 1.0));
+  f[4] = 1.0 / (beta0 * PC.Scxl);
+  f[5] = 0.0;
+  brho = gbet / PC.Clight / q->qmcc;
+  s11 = q->bgrad / brho * PC.Scxl;
+  s33 = -(q->bgrad / brho * PC.Scxl);
+  s55 = 0.0;
+  lin_rhs(y, f, s11, s33, s55);
+}
+
+/* intfunc1_DriftTube (DriftTube.f90:245-288) */
+static void drift_rhs(double t, const double *y, double *f, const void *vctx) {
+  (void)t; (void)vctx;
+  double gamma0 = -y[5];
+  double beta0 = sqrt(gamma0 * gamma0 - 1.) / gamma0;
+  f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+  f[4] = 1.0 / (beta0 * PC.Scxl);
+  f[5] = 0.0;
+  lin_rhs(y, f, 0.0, 0.0, 0.0);
+}
+
+static void y_init(double *y, const double refpt[6]) {
+  memset(y, 0, 18 * sizeof(double));
+  y[4] = refpt[4];
+  y[5] = refpt[5];
+  y[6] = 1.0; y[9] = 1.0; y[10] = 1.0; y[13] = 1.0; y[14] = 1.0; y[17] = 1.0;
+}
+
+#define XM(j, k) xm[((j)-1) + 6 * ((k)-1)]
+
+/* the xm assembly shared by maplinear_* (Quadrupole.f90:183-198) */
+static void xm_assemble(double xm[36], const double *y, double squi, double squf,
+                        double sqi3, double sqf3, double dlti, double dltf,
+                        double thli, double thlf) {
+  const double *Y = y - 1; /* 1-based like the Fortran */
+  XM(1, 1) = Y[7] * squi / squf + Y[9] * squi / squf * dlti;
+  XM(2, 1) = (Y[8] - Y[7] * dltf) * squi * squf + (Y[10] - Y[9] * dltf) * squi * squf * dlti;
+  XM(1, 2) = Y[9] / (squi * squf);
+  XM(2, 2) = (Y[10] - Y[9] * dltf) * squf / squi;
+  XM(3, 3) = Y[11] * squi / squf + Y[13] * squi / squf * dlti;
+  XM(4, 3) = (Y[12] - Y[11] * dltf) * squi * squf + (Y[14] - Y[13] * dltf) * squi * squf * dlti;
+  XM(3, 4) = Y[13] / (squi * squf);
+  XM(4, 4) = (Y[14] - Y[13] * dltf) * squf / squi;
+  XM(5, 5) = Y[15] * sqi3 / sqf3 + Y[17] * sqi3 / sqf3 * thli;
+  XM(6, 5) = (Y[16] - Y[15] * thlf) * sqi3 * sqf3 + (Y[18] - Y[17] * thlf) * sqi3 * sqf3 * thli;
+  XM(5, 6) = Y[17] / (sqi3 * sqf3);
+  XM(6, 6) = (Y[18] - Y[17] * thlf) * sqf3 / sqi3;
+}
+
+/* maplinear_Quadrupole (Quadrupole.f90:120-200) */
+void orc_maplinear_quad(double t, double tau, double xm[36], double refpt[6],
+                        double gradient, int mapstp, double chg, double mass) {
+  double y[18], h, t0, gi, betai, ui, squi, sqi3, gf, betaf, uf, squf, sqf3, s;
+  quad_ctx q = {gradient, chg / mass};
+  memset(xm, 0, 36 * sizeof(double));
+  y_init(y, refpt);
+  h = tau / mapstp;
+  t0 = t;
+  gi = -refpt[5];
+  betai = sqrt(gi * gi - 1.) / gi;
+  ui = gi * betai;
+  squi = sqrt(ui);
+  s = sqrt(ui);
+  sqi3 = s * s * s;
+  rk6i(h, mapstp, &t0, y, quad_rhs, &q);
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  gf = -refpt[5];
+  betaf = sqrt(gf * gf - 1.) / gf;
+  uf = gf * betaf;
+  squf = sqrt(uf);
+  s = sqrt(uf);
+  sqf3 = s * s * s;
+  xm_assemble(xm, y, squi, squf, sqi3, sqf3, 0.0, 0.0, 0.0, 0.0);
+}
+
+/* maplinear_DriftTube (DriftTube.f90:113-191) */
+void orc_maplinear_drift(double t, double tau, double xm[36], double refpt[6],
+                         int mapstp, double chg, double mass) {
+  (void)chg; (void)mass;
+  double y[18], h, t0, gi, betai, ui, squi, sqi3, gf, betaf, uf, squf, sqf3, s;
+  memset(xm, 0, 36 * sizeof(double));
+  y_init(y, refpt);
+  h = tau / mapstp;
+  t0 = t;
+  gi = -refpt[5];
+  betai = sqrt(gi * gi - 1.) / gi;
+  ui = gi * betai;
+  squi = sqrt(ui);
+  s = sqrt(ui);
+  sqi3 = s * s * s;
+  rk6i(h, mapstp, &t0, y, drift_rhs, NULL);
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  gf = -refpt[5];
+  betaf = sqrt(gf * gf - 1.) / gf;
+  uf = gf * betaf;
+  squf = sqrt(uf);
+  s = sqrt(uf);
+  sqf3 = s * s * s;
+  xm_assemble(xm, y, squi, squf, sqi3, sqf3, 0.0, 0.0, 0.0, 0.0);
+}
+
+/* ---- CCL linear gap ---------------------------------------------------- */
+typedef struct {
+  double zedge, escale, ww, theta0, qmcc;
+  int ndata;
+  const double *zdat, *edat, *epdat, *eppdat;
+} ccl_ctx;
+
+/* getaxfldE_CCL (CCL.f90:331-365): bisection + linear interpolation */
+static void ccl_field(double z, const ccl_ctx *c, double *ez1, double *ezp1, double *ezpp1) {
+  double zz = z - c->zedge, hstep, slope;
+  int klo = 1, khi = c->ndata, k;
+  const double *zd = c->zdat - 1, *ed = c->edat - 1, *epd = c->epdat - 1, *eppd = c->eppdat - 1;
+  while (khi - klo > 1) {
+    k = (khi + klo) / 2;
+    if (zd[k] > zz) khi = k; else klo = k;
+  }
+  hstep = zd[khi] - zd[klo];
+  slope = (ed[khi] - ed[klo]) / hstep;
+  *ez1 = ed[klo] + slope * (zz - zd[klo]);
+  slope = (epd[khi] - epd[klo]) / hstep;
+  *ezp1 = epd[klo] + slope * (zz - zd[klo]);
+  slope = (eppd[khi] - eppd[klo]) / hstep;
+  *ezpp1 = eppd[klo] + slope * (zz - zd[klo]);
+  *ez1 = *ez1 * c->escale;
+  *ezp1 = *ezp1 * c->escale;
+  *ezpp1 = *ezpp1 * c->escale;
+}
+
+/* intfunc1_CCL (CCL.f90:269-328) */
+static void ccl_rhs(double t, const double *y, double *f, const void *vctx) {
+  const ccl_ctx *c = (const ccl_ctx *)vctx;
+  const double Scxl = PC.Scxl;
+  double ez1, ezp1, ezpp1, gamma0, beta0, sinphi, cosphi, rfdsgn, s11tmp, s11, s33, s55, q;
+  ccl_field(t, c, &ez1, &ezp1, &ezpp1);
+  f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+  gamma0 = -y[5];
+  beta0 = sqrt(gamma0 * gamma0 - 1.) / gamma0;
+  sinphi = sin(c->ww * y[4] + c->theta0);
+  cosphi = cos(c->ww * y[4] + c->theta0);
+  rfdsgn = ez1 * cosphi;
+  f[4] = 1.0 / (beta0 * Scxl);
+  f[5] = -(c->qmcc * rfdsgn);
+  q = c->qmcc * rfdsgn / (beta0 * beta0) / (gamma0 * gamma0);
+  s11tmp = 0.5 * (1.0 + 0.5 * (gamma0 * gamma0)) * (q * q) +
+           c->qmcc * 0.5 / ((beta0 * beta0) * beta0) / ((gamma0 * gamma0) * gamma0) * ez1 *
+               sinphi * c->ww / Scxl;
+  s11 = s11tmp * Scxl;
+  s33 = s11tmp * Scxl;
+  s55 = -(1.5 * c->qmcc / (beta0 * beta0) / gamma0 * ezp1 * cosphi) +
+        ((beta0 * beta0) + 0.5) / ((beta0 * beta0) * beta0) / gamma0 * c->qmcc * ez1 * sinphi *
+            c->ww / Scxl +
+        1.5 * (1.0 - 0.5 * (gamma0 * gamma0)) * (q * q);
+  s55 = Scxl * s55;
+  lin_rhs(y, f, s11, s33, s55);
+}
+
+/* maplinear_CCL (CCL.f90:122-215) */
+void orc_maplinear_ccl(double t, double tau, double xm[36], double refpt[6],
+                       double zedge, double escale, double freq, double phase_deg,
+                       int mapstp, double chg, double mass,
+                       int ndata, const double *zdat, const double *edat,
+                       const double *epdat, const double *eppdat) {
+  const double Scxl = PC.Scxl;
+  ccl_ctx c;
+  double y[18], h, t0, gi, betai, ui, squi, sqi3, gf, betaf, uf, squf, sqf3, s;
+  double ein, e1in, e2in, ef, e1f, e2f, sinthi, costhi, uprimi, qpwi, dlti, thli;
+  double sinthf, costhf, uprimf, qpwf, dltf, thlf, tfin;
+  c.zedge = zedge;
+  c.escale = escale;
+  c.ww = freq / PC.Scfreq;
+  /* theta0 = Param(4)*asin(1.0)/90 with a default-real asin(1.0) */
+  c.theta0 = phase_deg * (double)asinf(1.0f) / 90;
+  c.qmcc = chg / mass;
+  c.ndata = ndata;
+  c.zdat = zdat; c.edat = edat; c.epdat = epdat; c.eppdat = eppdat;
+  memset(xm, 0, 36 * sizeof(double));
+  y_init(y, refpt);
+  h = tau / mapstp;
+  t0 = t;
+  gi = -refpt[5];
+  betai = sqrt(gi * gi - 1.) / gi;
+  ui = gi * betai;
+  squi = sqrt(ui);
+  s = sqrt(ui);
+  sqi3 = s * s * s;
+  ccl_field(t, &c, &ein, &e1in, &e2in);
+  sinthi = sin(c.ww * refpt[4] + c.theta0);
+  costhi = cos(c.ww * refpt[4] + c.theta0);
+  uprimi = c.qmcc * ein / betai * costhi;
+  qpwi = 0.5 * c.qmcc * Scxl / (ui * c.ww);
+  dlti = Scxl * (0.5 * uprimi / ui - qpwi * e1in * sinthi);
+  thli = 1.5 * Scxl * (uprimi / ui);
+  rk6i(h, mapstp, &t0, y, ccl_rhs, &c);
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  gf = -refpt[5];
+  betaf = sqrt(gf * gf - 1.) / gf;
+  uf = gf * betaf;
+  squf = sqrt(uf);
+  s = sqrt(uf);
+  sqf3 = s * s * s;
+  tfin = t + tau;
+  ccl_field(tfin, &c, &ef, &e1f, &e2f);
+  sinthf = sin(c.ww * refpt[4] + c.theta0);
+  costhf = cos(c.ww * refpt[4] + c.theta0);
+  uprimf = c.qmcc * ef / betaf * costhf;
+  qpwf = 0.5 * c.qmcc * Scxl / (uf * c.ww);
+  dltf = Scxl * (0.5 * uprimf / uf - qpwf * e1f * sinthf);
+  thlf = 1.5 * Scxl * (uprimf / uf);
+  xm_assemble(xm, y, squi, squf, sqi3, sqf3, dlti, dltf, thli, thlf);
+}
+
+/* 6x6 loop of drift1_BeamBunch (BeamBunch.f90:310-320) */
+void orc_apply_xm(double *pts, int n, const double xm[36]) {
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int i = 0; i < n; i++) {
+    double temp[6];
+    for (int j = 0; j < 6; j++) {
+      double s = 0.0;
+      for (int k = 0; k < 6; k++) s = s + P(i, k) * xm[j + 6 * k];
+      temp[j] = s;
+    }
+    for (int j = 0; j < 6; j++) P(i, j) = temp[j];
+  }
+}
+
+/* transfmapK_Quadrupole (Quadrupole.f90:509-607) */
+void orc_transfmapK(double tau, double kquad, double refpt[6], double *pts, int n,
+                    double qmass) {
+  const double Scxl = PC.Scxl;
+  double gambet0 = sqrt(refpt[5] * refpt[5] - 1.0);
+  double beta0 = sqrt(1.0 - 1.0 / (refpt[5] * refpt[5]));
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int i = 0; i < n; i++) {
+    double gam, gambetz, betaz, kstr, rtkstr, rtkstrzz, cs, ss, t;
+    double xm11, xm12, xm21, xm22, xm33, xm34, xm43, xm44, tmp[6];
+    gam = -refpt[5] - P(i, 5);
+    gambetz = sqrt(((gam * gam - 1.0) - P(i, 1) * P(i, 1)) - P(i, 3) * P(i, 3));
+    betaz = gambetz / gam;
+    gambetz = sqrt(gam * gam - 1.0);
+    kstr = P(i, 6) / qmass * gambet0 / gambetz * kquad;
+    rtkstr = sqrt(fabs(kstr));
+    rtkstrzz = rtkstr * tau;
+    if (kstr > 0.0) {
+      cs = cos(rtkstrzz);
+      ss = sin(rtkstrzz);
+      xm11 = cs; xm12 = ss / rtkstr; xm21 = -(rtkstr * ss); xm22 = cs;
+      t = exp(rtkstrzz);
+      cs = (t * t + 1.0) / (t + t);
+      ss = (t * t - 1.0) / (t + t);
+      xm33 = cs; xm34 = ss / rtkstr; xm43 = ss * rtkstr; xm44 = cs;
+    } else if (kstr < 0.0) {
+      t = exp(rtkstrzz);
+      cs = (t * t + 1.0) / (t + t);
+      ss = (t * t - 1.0) / (t + t);
+      xm11 = cs; xm12 = ss / rtkstr; xm21 = rtkstr * ss; xm22 = cs;
+      cs = cos(rtkstrzz);
+      ss = sin(rtkstrzz);
+      xm33 = cs; xm34 = ss / rtkstr; xm43 = -(ss * rtkstr); xm44 = cs;
+    } else {
+      xm11 = 1.0; xm12 = tau; xm21 = 0.0; xm22 = 1.0;
+      xm33 = 1.0; xm34 = tau; xm43 = 0.0; xm44 = 1.0;
+    }
+    tmp[0] = xm11 * P(i, 0) + xm12 * P(i, 1) / gambetz / Scxl;
+    tmp[1] = gambetz * Scxl * xm21 * P(i, 0) + xm22 * P(i, 1);
+    tmp[2] = xm33 * P(i, 2) + xm34 * P(i, 3) / gambetz / Scxl;
+    tmp[3] = gambetz * Scxl * xm43 * P(i, 2) + xm44 * P(i, 3);
+    tmp[4] = P(i, 4) + (1.0 / betaz - 1.0 / beta0) * tau / Scxl;
+    tmp[5] = P(i, 5);
+    for (int j = 0; j < 6; j++) P(i, j) = tmp[j];
+  }
+  refpt[4] = refpt[4] + tau / beta0 / Scxl;
+}
+
+/* ideal RF gap branch of drift1_BeamBunch (BeamBunch.f90:324-440) */
+void orc_ideal_rf(double *pts, int n, double refptcl[6], double mass, double tau,
+                  double vgrad, double rffreq, double phase_deg, int nst, int nseg,
+                  int ihlf) {
+  const double Scxl = PC.Scxl;
+  double vtmp = vgrad / mass;
+  double harm = rffreq / PC.Scfreq;
+  double phi0lc = phase_deg * asin(1.0) / 90;
+  double gam0, gambet, beta0, gambet0;
+  if (nst == 1 && ihlf % 2 == 0) {
+    gam0 = -refptcl[5];
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+    for (int i = 0; i < n; i++) {
+      double gam = gam0 - P(i, 5);
+      double gambetz = sqrt(((gam * gam - 1.0) - P(i, 1) * P(i, 1)) - P(i, 3) * P(i, 3));
+      double phi = P(i, 4) * harm + phi0lc;
+      double cosphi = cos(phi);
+      double vg = vtmp * cosphi * Scxl;
+      P(i, 1) = P(i, 1) - 0.5 * vg * gambetz / gam * P(i, 0);
+      P(i, 3) = P(i, 3) - 0.5 * vg * gambetz / gam * P(i, 2);
+    }
+  }
+  gam0 = -refptcl[5];
+  gambet = sqrt(gam0 * gam0 - 1.0);
+  beta0 = gambet / gam0;
+  refptcl[4] = refptcl[4] + 0.5 * tau / (Scxl * beta0);
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int i = 0; i < n; i++) {
+    double gami_1 = gam0 - P(i, 5);
+    double gambeti_1 = sqrt(gami_1 * gami_1 - 1.0);
+    double gambetzi_1 = sqrt(((gami_1 * gami_1 - 1.0) - P(i, 1) * P(i, 1)) - P(i, 3) * P(i, 3));
+    double phi = P(i, 4) * harm + phi0lc;
+    double dgami = tau * vtmp * cos(phi);
+    double gami_2 = gami_1 + dgami;
+    double gambeti_2 = sqrt(gami_2 * gami_2 - 1.0);
+    double fact;
+    if (fabs(vtmp) < 1.0e-10)
+      fact = tau / Scxl;
+    else
+      fact = gambeti_1 / dgami * log(gambeti_2 / gambeti_1) * tau / Scxl;
+    P(i, 0) = P(i, 0) + fact * P(i, 1) / gambetzi_1;
+    P(i, 2) = P(i, 2) + fact * P(i, 3) / gambetzi_1;
+    P(i, 4) = P(i, 4) + (tau / Scxl) / (gambet * gambet * gambet) * P(i, 5);
+  }
+  refptcl[5] = refptcl[5] - tau * vtmp * cos(phi0lc);
+  gam0 = -refptcl[5];
+  gambet0 = sqrt(gam0 * gam0 - 1.0);
+  beta0 = gambet0 / gam0;
+  refptcl[4] = refptcl[4] + 0.5 * tau / (Scxl * beta0);
+  if (nst == nseg && ihlf % 2 == 1) {
+    gam0 = -refptcl[5];
+    double c0 = cos(phi0lc);
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+    for (int i = 0; i < n; i++) {
+      double gam = gam0 - P(i, 5);
+      double gambetz = sqrt(((gam * gam - 1.0) - P(i, 1) * P(i, 1)) - P(i, 3) * P(i, 3));
+      double phi = P(i, 4) * harm + phi0lc;
+      double cosphi = cos(phi);
+      double vg = vtmp * cosphi * Scxl;
+      P(i, 1) = P(i, 1) + 0.5 * vg * gambetz / gam * P(i, 0);
+      P(i, 3) = P(i, 3) + 0.5 * vg * gambetz / gam * P(i, 2);
+      phi = P(i, 4) * harm + phi0lc;
+      P(i, 5) = P(i, 5) + (double)(2 * nseg) * tau * vtmp * (c0 - cos(phi));
+    }
+  }
+}
+
+/* Fpol_Dipole (Dipole.f90:466-526) */
+void orc_fpol(double h0, double h1, double tanphi, double tanphib, double k1,
+              double psi, double *pts, double ang, int n, double gam0, double qm0) {
+  const double Scxl = PC.Scxl;
+  double tanphi2 = tanphi * tanphi;
+  double secphi2 = 1.0 + tanphi2;
+  double secphi = 1.0 / cos(ang);
+  double secphi3 = secphi2 * secphi;
+  double secphib2 = 1. + tanphib * tanphib;
+  double beta0 = sqrt(1.0 - 1.0 / (gam0 * gam0));
+  double gambet = beta0 * gam0;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int i = 0; i < n; i++) {
+    double a[6], gamn, gambetz;
+    P(i, 0) = P(i, 0) * Scxl;
+    gamn = gam0 - P(i, 5);
+    gambetz = sqrt(((gamn * gamn - 1.0) - P(i, 1) * P(i, 1)) - P(i, 3) * P(i, 3));
+    P(i, 1) = P(i, 1) / gambetz;
+    P(i, 2) = P(i, 2) * Scxl;
+    P(i, 3) = P(i, 3) / gambetz;
+    P(i, 4) = -(P(i, 4) * beta0 * Scxl);
+    P(i, 5) = -(P(i, 5) / beta0 / gambet) - (P(i, 6) - qm0) / qm0;
+    double x = P(i, 0), xp = P(i, 1), y = P(i, 2), yp = P(i, 3), d = P(i, 5);
+    a[0] = x - 0.5 * h0 * tanphi2 * (x * x) + 0.5 * h0 * secphi2 * (y * y);
+    a[1] = h0 * tanphi * x + xp + h0 * tanphi2 * x * xp +
+           (0.5 * h0 * h1 * secphi3 + k1 * tanphi) * (x * x) -
+           (0.5 * h0 * h1 * secphi3 + k1 * tanphi - (h0 * h0) * tanphi * tanphi2 -
+            0.5 * (h0 * h0) * tanphi) * (y * y) -
+           h0 * tanphi2 * y * yp - h0 * tanphi * x * d;
+    a[2] = y + h0 * tanphi2 * x * y;
+    a[3] = -(h0 * tanphib * y) + yp - h0 * tanphi2 * x * yp - h0 * secphi2 * xp * y -
+           (h0 * h1 * secphi3 + 2 * k1 * tanphi) * x * y +
+           (h0 * tanphi - h0 * psi * secphib2) * y * d;
+    a[4] = P(i, 4);
+    a[5] = P(i, 5);
+    gambetz = sqrt(gamn * gamn - 1.0) / sqrt((a[1] * a[1] + a[3] * a[3]) + 1);
+    P(i, 0) = a[0] / Scxl;
+    P(i, 1) = a[1] * gambetz;
+    P(i, 2) = a[2] / Scxl;
+    P(i, 3) = a[3] * gambetz;
+    P(i, 4) = -a[4] / Scxl / beta0;
+    P(i, 5) = -(beta0 * gambet * (a[5] + (P(i, 6) - qm0) / qm0));
+  }
+}
+
+/* Bpol_Dipole (Dipole.f90:528-591) */
+void orc_bpol(double h0, double h1, double tanphi, double tanphib, double k1,
+              double psi, double *pts, double ang, int n, double gam0, double qm0) {
+  const double Scxl = PC.Scxl;
+  double tanphi2 = tanphi * tanphi;
+  double secphi2 = 1.0 + tanphi2;
+  double secphi = 1.0 / cos(ang);
+  double secphi3 = secphi2 * secphi;
+  double secphib2 = 1. + tanphib * tanphib;
+  double beta0 = sqrt(1.0 - 1.0 / (gam0 * gam0));
+  double gambet = beta0 * gam0;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int i = 0; i < n; i++) {
+    double a[6], gamn, gambetz;
+    P(i, 0) = P(i, 0) * Scxl;
+    gamn = gam0 - P(i, 5);
+    gambetz = sqrt(((gamn * gamn - 1.0) - P(i, 1) * P(i, 1)) - P(i, 3) * P(i, 3));
+    P(i, 1) = P(i, 1) / gambetz;
+    P(i, 2) = P(i, 2) * Scxl;
+    P(i, 3) = P(i, 3) / gambetz;
+    P(i, 4) = -(P(i, 4) * beta0 * Scxl);
+    P(i, 5) = -(P(i, 5) / beta0 / gambet) - (P(i, 6) - qm0) / qm0;
+    double x = P(i, 0), xp = P(i, 1), y = P(i, 2), yp = P(i, 3), d = P(i, 5);
+    a[0] = x + 0.5 * h0 * tanphi2 * (x * x) - 0.5 * h0 * secphi2 * (y * y);
+    a[1] = h0 * tanphi * x + xp - h0 * tanphi2 * x * xp +
+           (0.5 * h0 * h1 * secphi3 + k1 * tanphi - (h0 * h0) * tanphi2 * tanphi / 2) * (x * x) -
+           (0.5 * h0 * h1 * secphi3 + k1 * tanphi + (h0 * h0) * tanphi * tanphi2 / 2) * (y * y) +
+           h0 * tanphi2 * y * yp - h0 * tanphi * x * d;
+    a[2] = y - h0 * tanphi2 * x * y;
+    a[3] = -(h0 * tanphib * y) + yp + h0 * tanphi2 * x * yp + h0 * secphi2 * xp * y -
+           (h0 * h1 * secphi3 + 2 * k1 * tanphi - (h0 * h0) * secphi2 * tanphi) * x * y +
+           (h0 * tanphi - h0 * psi * secphib2) * y * d;
+    a[4] = P(i, 4);
+    a[5] = P(i, 5);
+    gambetz = sqrt(gamn * gamn - 1.0) / sqrt((a[1] * a[1] + a[3] * a[3]) + 1);
+    P(i, 0) = a[0] / Scxl;
+    P(i, 1) = a[1] * gambetz;
+    P(i, 2) = a[2] / Scxl;
+    P(i, 3) = a[3] * gambetz;
+    P(i, 4) = -a[4] / Scxl / beta0;
+    P(i, 5) = -(beta0 * gambet * (a[5] + (P(i, 6) - qm0) / qm0));
+  }
+}
+
+/* Sector_Dipole: 2nd-order Brown map (Dipole.f90:693-788) */
+void orc_sector(double len, double beta0, double h0, double k1, double *pts, int n,
+                double qm0) {
+  (void)k1;
+  const double Scxl = PC.Scxl;
+  double rho = 1.0 / h0, theta = len * h0;
+  double st = sin(theta), ct = cos(theta), sh = sin(theta / 2.0);
+  double R11 = ct, R12 = rho * st, R16 = rho * (1.0 - ct), R21 = -st / rho, R22 = ct, R26 = st;
+  double R51 = -R26, R52 = -R16, R56 = rho * (st - (beta0 * beta0) * theta);
+  double T111 = -(st * st) / (2.0 * rho), T112 = st * ct, T116 = st * st;
+  double T122 = rho * ct * (sh * sh);
+  double T126 = -(rho * st * (-1.0 + ct));
+  double T166 = -(rho * (st * st)) / 2.0;
+  double T144 = rho * (-1.0 + ct) / 2.0;
+  double T216 = st / rho, T222 = -st / 2.0, T266 = -st, T244 = -st / 2.0;
+  double T314 = st, T324 = 2.0 * rho * (sh * sh), T346 = rho * (theta - st);
+  double T522 = -(0.5 * rho * st), T544 = T522, T526 = rho * (ct - 1.0);
+  double gambet = beta0 / sqrt(1.0 - beta0 * beta0);
+  double gam2 = 1.0 / (1.0 - beta0 * beta0);
+  double gam0 = sqrt(gam2);
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int i = 0; i < n; i++) {
+    double gami = -P(i, 5) + gam0;
+    double gambeti = sqrt(gami * gami - 1.0);
+    double gambetx = P(i, 1), gambety = P(i, 3);
+    double gambetz = sqrt((gambeti * gambeti - gambetx * gambetx) - gambety * gambety);
+    double x0 = P(i, 0) * Scxl, xp0 = P(i, 1) / gambetz, y0 = P(i, 2) * Scxl;
+    double yp0 = P(i, 3) / gambetz, z0 = -(P(i, 4) * beta0 * Scxl);
+    double eta = -(P(i, 5) / beta0 / gambet) - (P(i, 6) - qm0) / qm0;
+    double a0 = R11 * x0 + R12 * xp0 + R16 * eta + T111 * (x0 * x0) + T112 * x0 * xp0 +
+                T116 * x0 * eta + T122 * (xp0 * xp0) + T126 * xp0 * eta + T166 * (eta * eta) +
+                T144 * (yp0 * yp0);
+    double a1 = R21 * x0 + R22 * xp0 + R26 * eta + T216 * x0 * eta + T222 * (xp0 * xp0) +
+                T266 * (eta * eta) + T244 * (yp0 * yp0);
+    double a2 = y0 + len * yp0 + T314 * x0 * yp0 + T324 * xp0 * yp0 + T346 * yp0 * eta;
+    double a3 = yp0;
+    double a4 = R51 * x0 + R52 * xp0 + z0 + R56 * eta + T522 * (xp0 * xp0) +
+                T544 * (yp0 * yp0) + T526 * xp0 * eta;
+    double a5 = eta;
+    double xp = a1, yp = a3;
+    gambetz = gambeti / sqrt((xp * xp + yp * yp) + 1.0);
+    P(i, 0) = a0 / Scxl;
+    P(i, 1) = a1 * gambetz;
+    P(i, 2) = a2 / Scxl;
+    P(i, 3) = a3 * gambetz;
+    P(i, 4) = -a4 / Scxl / beta0;
+    P(i, 5) = -(beta0 * gambet * (a5 + (P(i, 6) - qm0) / qm0));
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* conv1st_BeamBunch, Flagbc=1 (BeamBunch.f90:1252-1352, 1657-1663) */
+int orc_conv1st(double *pts, int n, double *current, int *npt,
+                const double refptcl[6], double xrad, double yrad,
+                double ptrange[6]) {
+  /* pilc = 2.0*asin(1.0) in default (single) precision */
+  const double pilc = (double)(2.0f * asinf(1.0f));
+  const double xl = PC.Scxl;
+  double gam = -refptcl[5];
+  double rad = (xrad + yrad) / 2;
+  int ilost = 0;
+  for (int k = 0; k < 3; k++) {
+    ptrange[2 * k] = (double)1.0e20f;
+    ptrange[2 * k + 1] = -(double)1.0e20f;
+  }
+  for (int i0 = 0; i0 < n; i0++) {
+    int i = i0 - ilost;
+    int ntmp5 = (int)(P(i0, 4) / pilc);
+    double tmp5 = P(i0, 4) - ntmp5 * pilc;
+    P(i0, 4) = tmp5 - (ntmp5 % 2) * pilc;
+    double rcpgammai = 1.0 / (-P(i0, 5) + gam);
+    double tmpbet = 1.0 - rcpgammai * rcpgammai * ((1 + P(i0, 1) * P(i0, 1)) + P(i0, 3) * P(i0, 3));
+    double betai = sqrt(fabs(tmpbet));
+    double tmpx = P(i0, 0) * xl;
+    P(i, 0) = (P(i0, 0) - P(i0, 1) * P(i0, 4) * rcpgammai) * xl;
+    double tmp0 = fmin(tmpx, P(i, 0));
+    if (ptrange[0] > tmp0) ptrange[0] = tmp0;
+    tmp0 = fmax(tmpx, P(i, 0));
+    if (ptrange[1] < tmp0) ptrange[1] = tmp0;
+    P(i, 1) = P(i0, 1);
+    double tmpy = P(i0, 2) * xl;
+    P(i, 2) = (P(i0, 2) - P(i0, 3) * P(i0, 4) * rcpgammai) * xl;
+    tmp0 = fmin(tmpy, P(i, 2));
+    if (ptrange[2] > tmp0) ptrange[2] = tmp0;
+    tmp0 = fmax(tmpy, P(i, 2));
+    if (ptrange[3] < tmp0) ptrange[3] = tmp0;
+    P(i, 3) = P(i0, 3);
+    P(i, 4) = -(gam * betai * P(i0, 4) * xl);
+    if (ptrange[4] > P(i, 4)) ptrange[4] = P(i, 4);
+    if (ptrange[5] < P(i, 4)) ptrange[5] = P(i, 4);
+    P(i, 5) = P(i0, 5);
+    double radtest = sqrt(P(i, 0) * P(i, 0) + P(i, 2) * P(i, 2));
+    if (radtest >= rad || tmpbet <= 0.0) ilost++;
+    P(i, 6) = P(i0, 6);
+    P(i, 7) = P(i0, 7);
+    P(i, 8) = P(i0, 8);
+  }
+  int nplc = n - ilost;
+  int nptot = nplc; /* MPI_ALLREDUCE over one rank */
+  *current = *current * nptot / *npt;
+  *npt = nptot;
+  return nplc;
+}
+
+/* update_CompDom, Flagbc=1 (CompDom.f90:509-557, 614-622, 803-819) */
+void orc_update_compdom(const double ptrange[6], const int mesh[3],
+                        double range[6], double msize[3]) {
+  for (int k = 0; k < 3; k++) {
+    double t1 = ptrange[2 * k], t2 = ptrange[2 * k + 1];
+    /* eps = 1.0/(Meshnum-3.0) evaluated in default (single) precision */
+    double eps = (double)(1.0f / ((float)mesh[k] - 3.0f));
+    double mn = t1 - eps * (t2 - t1);
+    double mx = t2 + eps * (t2 - t1);
+    range[2 * k] = mn;
+    range[2 * k + 1] = mx;
+    msize[k] = (mx - mn) / (mesh[k] - 1);
+  }
+}
+
+/* deposit_BeamBunch (BeamBunch.f90:3678-3768) */
+void orc_deposit(const double *pts, int n, const int mesh[3], const double range[6],
+                 const double msize[3], double *rho, int *counts, long long *cells) {
+  const int nx = mesh[0], ny = mesh[1], nz = mesh[2];
+  const double hx = msize[0], hy = msize[1], hz = msize[2];
+  const double hxi = 1.0 / hx, hyi = 1.0 / hy, hzi = 1.0 / hz;
+  const double xmin = range[0], ymin = range[2], zmin = range[4];
+  const size_t G = (size_t)nx * ny * nz;
+  memset(rho, 0, G * sizeof(double));
+  if (counts) memset(counts, 0, G * sizeof(int));
+#define R(i, j, k) rho[((i)-1) + (size_t)nx * (((j)-1) + (size_t)ny * ((k)-1))]
+  for (int i = 0; i < n; i++) {
+    int ix = (int)((P(i, 0) - xmin) * hxi + 1);
+    double ab = ((xmin - P(i, 0)) + ix * hx) * hxi;
+    int jx = (int)((P(i, 2) - ymin) * hyi + 1);
+    double cd = ((ymin - P(i, 2)) + jx * hy) * hyi;
+    int kx = (int)((P(i, 4) - zmin) * hzi + 1);
+    double ef = ((zmin - P(i, 4)) + kx * hz) * hzi;
+    int ix1 = ix + 1, jx1 = jx + 1, kx1 = kx + 1;
+    if (ix < 1 || ix1 > nx || jx < 1 || jx1 > ny || kx < 1 || kx1 > nz) {
+      if (cells) cells[i] = -1;
+      continue;
+    }
+    double w = P(i, 7);
+    R(ix, jx, kx) = R(ix, jx, kx) + ab * cd * ef * w;
+    R(ix, jx1, kx) = R(ix, jx1, kx) + ab * (1.0 - cd) * ef * w;
+    R(ix, jx1, kx1) = R(ix, jx1, kx1) + ab * (1.0 - cd) * (1.0 - ef) * w;
+    R(ix, jx, kx1) = R(ix, jx, kx1) + ab * cd * (1.0 - ef) * w;
+    R(ix1, jx, kx1) = R(ix1, jx, kx1) + (1.0 - ab) * cd * (1.0 - ef) * w;
+    R(ix1, jx1, kx1) = R(ix1, jx1, kx1) + (1.0 - ab) * (1.0 - cd) * (1.0 - ef) * w;
+    R(ix1, jx1, kx) = R(ix1, jx1, kx) + (1.0 - ab) * (1.0 - cd) * ef * w;
+    R(ix1, jx, kx) = R(ix1, jx, kx) + (1.0 - ab) * cd * ef * w;
+    long long c = (ix - 1) + (long long)nx * ((jx - 1) + (long long)ny * (kx - 1));
+    if (counts) counts[c]++;
+    if (cells) cells[i] = c;
+  }
+#undef R
+}
+
+/* ------------------------------------------------------------------ */
+/* greenf1tIntnew before its FFTs (Field.f90:392-428) */
+void orc_igf(int nx, int ny, int nz, double hx, double hy, double hz, double *grn) {
+  const int ax = nx + 2, ay = ny + 2, az = nz + 2;
+  double *tmp = (double *)malloc((size_t)ax * ay * az * sizeof(double));
+#define T(i, j, k) tmp[((i)-1) + (size_t)ax * (((j)-1) + (size_t)ay * ((k)-1))]
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int k0 = 1; k0 <= az; k0++)
+    for (int j0 = 1; j0 <= ay; j0++)
+      for (int i0 = 1; i0 <= ax; i0++) {
+        double v1 = (i0 - 1) * hx - hx / 2;
+        double v2 = (j0 - 1) * hy - hy / 2;
+        double v3 = (k0 - 1) * hz - hz / 2;
+        double rr = sqrt(v1 * v1 + v2 * v2 + v3 * v3);
+        double aa = -(v3 * v3 * atan(v1 * v2 / (v3 * rr)) / 2);
+        double bb = -(v2 * v2 * atan(v1 * v3 / (v2 * rr)) / 2);
+        double cc = -(v1 * v1 * atan(v2 * v3 / (v1 * rr)) / 2);
+        double dd = v2 * v3 * log(v1 + rr);
+        double ee = v1 * v3 * log(v2 + rr);
+        double ff = v1 * v2 * log(v3 + rr);
+        double gg2 = aa + bb + cc + dd + ee + ff;
+        T(i0, j0, k0) = gg2 / (hx * hy * hz);
+      }
+  const int gx = nx + 1, gy = ny + 1;
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int k0 = 1; k0 <= nz + 1; k0++)
+    for (int j0 = 1; j0 <= ny + 1; j0++)
+      for (int i0 = 1; i0 <= nx + 1; i0++)
+        grn[(i0 - 1) + (size_t)gx * ((j0 - 1) + (size_t)gy * (k0 - 1))] =
+            T(i0 + 1, j0 + 1, k0 + 1) - T(i0, j0 + 1, k0 + 1) - T(i0 + 1, j0, k0 + 1) +
+            T(i0, j0, k0 + 1) - T(i0 + 1, j0 + 1, k0) + T(i0, j0 + 1, k0) +
+            T(i0 + 1, j0, k0) - T(i0, j0, k0);
+#undef T
+  free(tmp);
+}
+
+/* radix-2 complex FFT, in place, on n points spaced by stride; sign -1 or +1,
+ * unnormalised.  Any correct FFT reproduces the reference's FFTPACK
+ * convolution (FFT.f90:26-250) to rounding. */
+static void fft1(double complex *a, int n, size_t stride, int sign, const double complex *tw) {
+  /* tw[k] = exp(-2 pi i k / n), k < n/2 */
+  for (int i = 1, j = 0; i < n; i++) {
+    int bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) {
+      double complex t = a[i * stride];
+      a[i * stride] = a[j * stride];
+      a[j * stride] = t;
+    }
+  }
+  for (int len = 2; len <= n; len <<= 1) {
+    int step = n / len;
+    for (int i = 0; i < n; i += len)
+      for (int k = 0; k < len / 2; k++) {
+        double complex w = tw[k * step];
+        if (sign > 0) w = conj(w);
+        double complex u = a[(i + k) * stride];
+        double complex v = a[(i + k + len / 2) * stride] * w;
+        a[(i + k) * stride] = u + v;
+        a[(i + k + len / 2) * stride] = u - v;
+      }
+  }
+}
+
+static double complex *twiddles(int n) {
+  double complex *tw = (double complex *)malloc((size_t)(n / 2 + 1) * sizeof(double complex));
+  for (int k = 0; k < n / 2; k++) {
+    double a = -2.0 * PC.Pi * k / n;
+    tw[k] = cos(a) + I * sin(a);
+  }
+  return tw;
+}
+
+static int is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+/* 3D FFT of a (n1,n2,n3) complex array (column-major).  Forward passes run
+ * x, y, z and skip the lines that are still zero (input nonzero only for
+ * j < ey, k < ez); inverse passes run z, y, x and skip the lines the cropped
+ * output does not need.  ey = n2, ez = n3 transforms everything. */
+static void fft3(double complex *a, int n1, int n2, int n3, int ey, int ez, int sign,
+                 int inverse) {
+  double complex *t1 = twiddles(n1), *t2 = twiddles(n2), *t3 = twiddles(n3);
+  for (int pass = 0; pass < 3; pass++) {
+    int axis = inverse ? 2 - pass : pass;
+    if (axis == 0) {
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads) collapse(2)
+      for (int k = 0; k < ez; k++)
+        for (int j = 0; j < ey; j++) fft1(a + (size_t)n1 * (j + (size_t)n2 * k), n1, 1, sign, t1);
+    } else if (axis == 1) {
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads) collapse(2)
+      for (int k = 0; k < ez; k++)
+        for (int i = 0; i < n1; i++) fft1(a + i + (size_t)n1 * n2 * k, n2, n1, sign, t2);
+    } else {
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads) collapse(2)
+      for (int j = 0; j < n2; j++)
+        for (int i = 0; i < n1; i++) fft1(a + i + (size_t)n1 * j, n3, (size_t)n1 * n2, sign, t3);
+    }
+  }
+  free(t1); free(t2); free(t3);
+}
+
+/* openBC3D + greenf1tIntnew's mirroring (Field.f90:239-331, 430-515):
+ * phi = IFFT(FFT(rho_zero_padded) * FFT(G_even_extended)) / (n1 n2 n3), cropped. */
+int orc_poisson_open(int nx, int ny, int nz, double hx, double hy, double hz,
+                     double *rho) {
+  const int n1 = 2 * nx, n2 = 2 * ny, n3 = 2 * nz;
+  if (!is_pow2(n1) || !is_pow2(n2) || !is_pow2(n3)) return -1;
+  const size_t N = (size_t)n1 * n2 * n3;
+  double complex *r = (double complex *)calloc(N, sizeof(double complex));
+  double complex *g = (double complex *)malloc(N * sizeof(double complex));
+  double *grn = (double *)malloc((size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double));
+  if (!r || !g || !grn) { free(r); free(g); free(grn); return -2; }
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        r[i + (size_t)n1 * (j + (size_t)n2 * k)] = rho[i + (size_t)nx * (j + (size_t)ny * k)];
+  orc_igf(nx, ny, nz, hx, hy, hz, grn);
+  for (int k = 0; k < n3; k++) {
+    int kk = k <= nz ? k : n3 - k;
+    for (int j = 0; j < n2; j++) {
+      int jj = j <= ny ? j : n2 - j;
+      for (int i = 0; i < n1; i++) {
+        int ii = i <= nx ? i : n1 - i;
+        g[i + (size_t)n1 * (j + (size_t)n2 * k)] =
+            grn[ii + (size_t)(nx + 1) * (jj + (size_t)(ny + 1) * kk)];
+      }
+    }
+  }
+  fft3(r, n1, n2, n3, ny, nz, -1, 0);
+  fft3(g, n1, n2, n3, n2, n3, -1, 0);
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (size_t q = 0; q < N; q++) r[q] = r[q] * g[q];
+  fft3(r, n1, n2, n3, ny, nz, +1, 1);
+  const double scale = 1.0 / ((double)n1 * n2 * n3);
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        rho[i + (size_t)nx * (j + (size_t)ny * k)] =
+            creal(r[i + (size_t)n1 * (j + (size_t)n2 * k)]) * scale;
+  free(r); free(g); free(grn);
+  return 0;
+}
+
+void orc_poisson_direct(int nx, int ny, int nz, double hx, double hy, double hz,
+                        const double *rho, double *phi) {
+  double *grn = (double *)malloc((size_t)(nx + 1) * (ny + 1) * (nz + 1) * sizeof(double));
+  orc_igf(nx, ny, nz, hx, hy, hz, grn);
+  for (int k = 0; k < nz; k++)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++) {
+        double s = 0.0;
+        for (int c = 0; c < nz; c++)
+          for (int b = 0; b < ny; b++)
+            for (int a = 0; a < nx; a++)
+              s += rho[a + (size_t)nx * (b + (size_t)ny * c)] *
+                   grn[abs(i - a) + (size_t)(nx + 1) * (abs(j - b) + (size_t)(ny + 1) * abs(k - c))];
+        phi[i + (size_t)nx * (j + (size_t)ny * k)] = s;
+      }
+  free(grn);
+}
+
+/* ------------------------------------------------------------------ */
+/* cvbkforth1st_BeamBunch (BeamBunch.f90:1667-1701) */
+void orc_cvbkforth1st(double *pts, int n, const double refptcl[6]) {
+  const double xl = PC.Scxl, xk = 1 / xl;
+  double gamma0 = -refptcl[5];
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int i = 0; i < n; i++) {
+    double rcpgammai = 1.0 / (-P(i, 5) + gamma0);
+    double betai = sqrt(1.0 - rcpgammai * rcpgammai * ((1 + P(i, 1) * P(i, 1)) + P(i, 3) * P(i, 3)));
+    P(i, 4) = P(i, 4) * xk / (-(gamma0 * betai));
+    P(i, 0) = P(i, 0) * xk + P(i, 1) * P(i, 4) * rcpgammai;
+    P(i, 2) = P(i, 2) * xk + P(i, 3) * P(i, 4) * rcpgammai;
+  }
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int i = 0; i < n; i++) {
+    double rcpgammai = 1.0 / (-P(i, 5) + gamma0);
+    double betai = sqrt(1.0 - rcpgammai * rcpgammai * ((1 + P(i, 1) * P(i, 1)) + P(i, 3) * P(i, 3)));
+    P(i, 0) = P(i, 0) * xl;
+    P(i, 2) = P(i, 2) * xl;
+    P(i, 4) = -(gamma0 * betai * P(i, 4) * xl);
+  }
+}
+
+/* kick1_BeamBunch field differences (BeamBunch.f90:1784-2005) + scatter1
+ * (BeamBunch.f90:2041-2181), one rank, Flagbc=1 */
+void orc_kick1(double *pts, int n, const double *phi, const int mesh[3],
+               const double range[6], const double msize[3], double gam,
+               double curr, double tau, double mass, double chrg, double *eg) {
+  if (curr < 1.0e-20) return;
+  const int nx = mesh[0], ny = mesh[1], nz = mesh[2];
+  const size_t G = (size_t)nx * ny * nz;
+  double *egx = eg ? eg : (double *)malloc(3 * G * sizeof(double));
+  double *egy = egx + G, *egz = egy + G;
+  const double hxi = 1.0 / msize[0], hyi = 1.0 / msize[1], hzi = 1.0 / msize[2];
+  const double hx = msize[0], hy = msize[1], hz = msize[2];
+#define IDX(i, j, k) (((i)-1) + (size_t)nx * (((j)-1) + (size_t)ny * ((k)-1)))
+#define PHI(i, j, k) phi[IDX(i, j, k)]
+  for (int k = 1; k <= nz; k++)
+    for (int j = 1; j <= ny; j++) {
+      egx[IDX(1, j, k)] = hxi * (PHI(1, j, k) - PHI(2, j, k));
+      for (int i = 2; i <= nx - 1; i++)
+        egx[IDX(i, j, k)] = 0.5 * hxi * (PHI(i - 1, j, k) - PHI(i + 1, j, k));
+      egx[IDX(nx, j, k)] = hxi * (PHI(nx - 1, j, k) - PHI(nx, j, k));
+    }
+  for (int k = 1; k <= nz; k++) {
+    for (int i = 1; i <= nx; i++) egy[IDX(i, 1, k)] = hyi * (PHI(i, 1, k) - PHI(i, 2, k));
+    for (int j = 2; j <= ny - 1; j++)
+      for (int i = 1; i <= nx; i++)
+        egy[IDX(i, j, k)] = 0.5 * hyi * (PHI(i, j - 1, k) - PHI(i, j + 1, k));
+    for (int i = 1; i <= nx; i++)
+      egy[IDX(i, ny, k)] = hyi * (PHI(i, ny - 1, k) - PHI(i, ny, k));
+  }
+  for (int j = 1; j <= ny; j++)
+    for (int i = 1; i <= nx; i++) egz[IDX(i, j, 1)] = hzi * (PHI(i, j, 1) - PHI(i, j, 2));
+  for (int k = 2; k <= nz - 1; k++)
+    for (int j = 1; j <= ny; j++)
+      for (int i = 1; i <= nx; i++)
+        egz[IDX(i, j, k)] = 0.5 * hzi * (PHI(i, j, k - 1) - PHI(i, j, k + 1));
+  for (int j = 1; j <= ny; j++)
+    for (int i = 1; i <= nx; i++)
+      egz[IDX(i, j, nz)] = hzi * (PHI(i, j, nz - 1) - PHI(i, j, nz));
+
+  /* scatter1_BeamBunch constants (BeamBunch.f90:2066-2084) */
+  const double tmpscale = curr / PC.Scfreq;
+  const double twopi = 2.0 * PC.Pi;
+  const double fpei = PC.Clight * PC.Clight * (double)1.0e-7f;
+  const double xk = 1 / PC.Scxl;
+  const double bet = sqrt(gam * gam - 1.0) / gam;
+  const double bbyk = bet / xk;
+  const double gambet = gam * bet;
+  const double brho = gambet / (PC.Clight * chrg) * mass;
+  const double vz0 = bet * PC.Clight;
+  const double perv0 = 2.0 * curr * fpei / (brho * vz0 * vz0 * gam * gam);
+  const double xycon = 0.5 * perv0 * gambet * bbyk * twopi / tmpscale;
+  const double tcon = bet * xycon * (gam * gam);
+  const double xmin = range[0], ymin = range[2], zmin = range[4];
+#pragma omp parallel for if (g_threads > 1) num_threads(g_threads)
+  for (int q = 0; q < n; q++) {
+    int ix = (int)((P(q, 0) - xmin) * hxi + 1);
+    double ab = ((xmin - P(q, 0)) + ix * hx) * hxi;
+    int jx = (int)((P(q, 2) - ymin) * hyi + 1);
+    double cd = ((ymin - P(q, 2)) + jx * hy) * hyi;
+    int kx = (int)((P(q, 4) - zmin) * hzi + 1);
+    double ef = ((zmin - P(q, 4)) + kx * hz) * hzi;
+    int ix1 = ix + 1, jx1 = jx + 1, kx1 = kx + 1;
+    double E[3];
+    const double *grids[3] = {egx, egy, egz};
+    for (int c = 0; c < 3; c++) {
+      const double *e = grids[c];
+      E[c] = e[IDX(ix, jx, kx)] * ab * cd * ef + e[IDX(ix, jx1, kx)] * ab * (1. - cd) * ef +
+             e[IDX(ix, jx1, kx1)] * ab * (1. - cd) * (1.0 - ef) +
+             e[IDX(ix, jx, kx1)] * ab * cd * (1.0 - ef) +
+             e[IDX(ix1, jx, kx1)] * (1.0 - ab) * cd * (1.0 - ef) +
+             e[IDX(ix1, jx1, kx1)] * (1.0 - ab) * (1.0 - cd) * (1.0 - ef) +
+             e[IDX(ix1, jx1, kx)] * (1.0 - ab) * (1.0 - cd) * ef +
+             e[IDX(ix1, jx, kx)] * (1.0 - ab) * cd * ef;
+    }
+    double exn = E[0] * gam, eyn = E[1] * gam, ezn = E[2];
+    double rcpgammai = 1.0 / (-P(q, 5) + gam);
+    double tmpsq = 1.0 - rcpgammai * rcpgammai * ((1 + P(q, 1) * P(q, 1)) + P(q, 3) * P(q, 3));
+    double betai = sqrt(tmpsq);
+    P(q, 0) = P(q, 0) * xk;
+    P(q, 1) = P(q, 1) + tau * xycon * exn;
+    P(q, 2) = P(q, 2) * xk;
+    P(q, 3) = P(q, 3) + tau * xycon * eyn;
+    P(q, 4) = P(q, 4) * xk / (-(gam * betai));
+    P(q, 5) = P(q, 5) - tau * tcon * ezn;
+  }
+#undef PHI
+#undef IDX
+  if (!eg) free(egx);
+}
+
+/* ------------------------------------------------------------------ */
+/* diagnostic1_Output moment sums (Output.f90:133-234) */
+void orc_moment_sums(const double *pts, int n, double raw[ORC_RAW_LEN]) {
+  double s[37];
+  double mx[6], rmax;
+  memset(s, 0, sizeof(s));
+  if (n != 0) {
+    for (int c = 0; c < 6; c++) mx[c] = fabs(P(0, c));
+    rmax = P(0, 0) * P(0, 0) + P(0, 2) * P(0, 2);
+  } else {
+    for (int c = 0; c < 6; c++) mx[c] = 0.0;
+    rmax = 0.0;
+  }
+  for (int i = 0; i < n; i++) {
+    double x = P(i, 0), px = P(i, 1), y = P(i, 2), py = P(i, 3), z = P(i, 4), pz = P(i, 5);
+    s[0] += x;                           /* x0lc  */
+    s[6] += x * x;                       /* sqsum1 */
+    s[15] += x * x * x;                  /* x0lc3 */
+    s[16] += x * x * x * x;              /* x0lc4 */
+    s[12] += x * px;                     /* xpx */
+    s[27] += x * px * px;                /* xpx2 */
+    s[28] += x * px * px * px;           /* xpx3 */
+    s[29] += x * x * px;                 /* x2px */
+    s[30] += x * x * px * px;            /* x2px2 */
+    s[31] += x * x * x * px;             /* x3px */
+    s[1] += px;
+    s[7] += px * px;
+    s[17] += px * px * px;
+    s[18] += px * px * px * px;
+    s[2] += y;
+    s[8] += y * y;
+    s[19] += y * y * y;
+    s[20] += y * y * y * y;
+    s[13] += y * py;
+    s[32] += y * py * py;
+    s[33] += y * py * py * py;
+    s[34] += y * y * py;
+    s[35] += y * y * py * py;
+    s[36] += y * y * y * py;
+    s[3] += py;
+    s[9] += py * py;
+    s[21] += py * py * py;
+    s[22] += py * py * py * py;
+    s[4] += z;
+    s[10] += z * z;
+    s[23] += fabs(z * z * z);
+    s[24] += z * z * z * z;
+    s[14] += z * pz;
+    s[5] += pz;
+    s[11] += pz * pz;
+    s[25] += pz * pz * pz;
+    s[26] += pz * pz * pz * pz;
+    for (int c = 0; c < 6; c++)
+      if (mx[c] < fabs(P(i, c))) mx[c] = fabs(P(i, c));
+    if (rmax < x * x + y * y) rmax = x * x + y * y;
+  }
+  memcpy(raw, s, sizeof(s));
+  memcpy(raw + 37, mx, sizeof(mx));
+  raw[43] = rmax;
+}
+
+static double cbrt_f32exp(double v) { return pow(fabs(v), (double)(1.0f / 3.0f)); }
+
+/* diagnostic1_Output rank-0 formulas and write statements (Output.f90:247-352) */
+void orc_diag_row(double z, const double raw[ORC_RAW_LEN], int npt, int nlocal,
+                  const double refptcl[6], double mass, double row[ORC_DIAG_LEN]) {
+  const double *t = raw;
+  const double qmc = mass / 1.0e6, xl = PC.Scxl, xt = PC.Rad2deg;
+  double den1 = 1.0 / (double)npt;
+  double gam = -refptcl[5];
+  double gambet = sqrt(gam * gam - 1.0);
+  double bet = sqrt(gam * gam - 1.0) / gam;
+  double energy = (gam - 1.) * qmc;
+  double x0 = t[0] * den1, px0 = t[1] * den1, y0 = t[2] * den1, py0 = t[3] * den1;
+  double z0 = t[4] * den1, pz0 = t[5] * den1;
+  double sqx = t[6] * den1, sqsum1 = sqx - x0 * x0;
+  double sqpx = t[7] * den1, sqsum2 = sqpx - px0 * px0;
+  double sqy = t[8] * den1, sqsum3 = sqy - y0 * y0;
+  double sqpy = t[9] * den1, sqsum4 = sqpy - py0 * py0;
+  double sqz = t[10] * den1, sqsum5 = sqz - z0 * z0;
+  double sqpz = t[11] * den1, sqsum6 = sqpz - pz0 * pz0;
+  double xpx = t[12] * den1 - x0 * px0;
+  double ypy = t[13] * den1 - y0 * py0;
+  double zpz = t[14] * den1 - z0 * pz0;
+  double cubx = t[15] * den1, fthx = t[16] * den1;
+  double x03 = cbrt_f32exp(cubx - 3 * sqx * x0 + 2 * x0 * x0 * x0);
+  double x04 = sqrt(sqrt(fabs(fthx - 4 * cubx * x0 + 6 * sqx * x0 * x0 - 3 * x0 * x0 * x0 * x0)));
+  double cubpx = t[17] * den1, fthpx = t[18] * den1;
+  double px03 = cbrt_f32exp(cubpx - 3 * sqpx * px0 + 2 * px0 * px0 * px0);
+  double px04 = sqrt(sqrt(fabs(fthpx - 4 * cubpx * px0 + 6 * sqpx * px0 * px0 -
+                               3 * px0 * px0 * px0 * px0)));
+  double cuby = t[19] * den1, fthy = t[20] * den1;
+  double y03 = cbrt_f32exp(cuby - 3 * sqy * y0 + 2 * y0 * y0 * y0);
+  double y04 = sqrt(sqrt(fabs(fthy - 4 * cuby * y0 + 6 * sqy * y0 * y0 - 3 * y0 * y0 * y0 * y0)));
+  double cubpy = t[21] * den1, fthpy = t[22] * den1;
+  double py03 = cbrt_f32exp(cubpy - 3 * sqpy * py0 + 2 * py0 * py0 * py0);
+  double py04 = sqrt(sqrt(fabs(fthpy - 4 * cubpy * py0 + 6 * sqpy * py0 * py0 -
+                               3 * py0 * py0 * py0 * py0)));
+  double cubz = t[23] * den1, fthz = t[24] * den1;
+  double z03 = cbrt_f32exp(cubz - 3 * sqz * z0 + 2 * z0 * z0 * z0);
+  double z04 = sqrt(sqrt(fabs(fthz - 4 * cubz * z0 + 6 * sqz * z0 * z0 - 3 * z0 * z0 * z0 * z0)));
+  double cubpz = t[25] * den1, fthpz = t[26] * den1;
+  double pz03 = cbrt_f32exp(cubpz - 3 * sqpz * pz0 + 2 * pz0 * pz0 * pz0);
+  double pz04 = sqrt(sqrt(fabs(fthpz - 4 * cubpz * pz0 + 6 * sqpz * pz0 * pz0 -
+                               3 * pz0 * pz0 * pz0 * pz0)));
+  double epsx2 = sqsum1 * sqsum2 - xpx * xpx;
+  double epsy2 = sqsum3 * sqsum4 - ypy * ypy;
+  double epsz2 = sqsum5 * sqsum6 - zpz * zpz;
+  double epx = sqrt(fmax(epsx2, 0.0)), epy = sqrt(fmax(epsy2, 0.0)), epz = sqrt(fmax(epsz2, 0.0));
+  double xrms = sqrt(sqsum1), pxrms = sqrt(sqsum2), yrms = sqrt(sqsum3);
+  double pyrms = sqrt(sqsum4), zrms = sqrt(sqsum5), pzrms = sqrt(sqsum6);
+  const double *gm = raw + 37;
+  row[0] = z;
+  row[1] = refptcl[4]; row[2] = gam; row[3] = energy; row[4] = bet; row[5] = sqrt(raw[43]) * xl;
+  row[6] = x0 * xl; row[7] = xrms * xl; row[8] = px0 / gambet; row[9] = pxrms / gambet;
+  row[10] = -xpx / epx; row[11] = epx * xl;
+  row[12] = y0 * xl; row[13] = yrms * xl; row[14] = py0 / gambet; row[15] = pyrms / gambet;
+  row[16] = -ypy / epy; row[17] = epy * xl;
+  row[18] = z0 * xt; row[19] = zrms * xt; row[20] = pz0 * qmc; row[21] = pzrms * qmc;
+  row[22] = -zpz / epz; row[23] = epz * qmc * xt;
+  row[24] = gm[0] * xl; row[25] = gm[1] / gambet; row[26] = gm[2] * xl; row[27] = gm[3] / gambet;
+  row[28] = gm[4] * xt; row[29] = gm[5] * qmc;
+  row[30] = nlocal; row[31] = nlocal; row[32] = npt;
+  row[33] = x03 * xl; row[34] = px03 / gambet; row[35] = y03 * xl; row[36] = py03 / gambet;
+  row[37] = z03 * xt; row[38] = pz03 * qmc;
+  row[39] = x04 * xl; row[40] = px04 / gambet; row[41] = y04 * xl; row[42] = py04 / gambet;
+  row[43] = z04 * xt; row[44] = pz04 * qmc;
+}
+
+/* ------------------------------------------------------------------ */
+static double pipe_radius(const orc_elem *e) {
+  /* getradius_BeamLineElem (BeamLineElem.f90:500-552): Param index per type */
+  switch (e->type) {
+    case 0: return e->val[0];  /* DriftTube Param(2) */
+    case 1: return e->val[2];  /* Quadrupole Param(4) */
+    case 4: return e->val[3];  /* Dipole Param(5) */
+    default: return e->val[4]; /* RF gaps Param(6) */
+  }
+}
+
+/* run_AccSimulator element/segment loop (AccSimulator.f90:742-1504) for
+ * Flagmap=1, Flagbc=1, Flagerr=0, Flagsubstep=0, one rank, no wake/CSR. */
+int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
+            double *rows, int maxrows) {
+  const double Scxl = PC.Scxl;
+  const double bcurr = beam->current;
+  const size_t G = (size_t)mesh[0] * mesh[1] * mesh[2];
+  double *rho = (double *)malloc(G * sizeof(double));
+  double raw[ORC_RAW_LEN];
+  int nrows = 0;
+  double z = beam->z;
+  if (!rho) return -2;
+#define DIAG()                                                                    \
+  do {                                                                            \
+    if (nrows < maxrows) {                                                        \
+      orc_moment_sums(beam->pts, beam->nlocal, raw);                              \
+      orc_diag_row(z, raw, beam->npt, beam->nlocal, beam->refptcl, beam->mass,    \
+                   rows + (size_t)ORC_DIAG_LEN * nrows);                          \
+    }                                                                             \
+    nrows++;                                                                      \
+  } while (0)
+  DIAG();
+  for (int ie = 0; ie < nelem; ie++) {
+    const orc_elem *e = &elems[ie];
+    const double blength = e->length;
+    const int bnseg = e->nseg, bitype = e->type;
+    double piperad = pipe_radius(e), piperad2 = piperad;
+    if (bitype < 0) { free(rho); return -3; }
+    if (bitype == 4) { piperad = 100.0; piperad2 = 100.0; }
+    double tau1 = 0.0;
+    if (bitype >= 0) tau1 = 0.5 * blength / bnseg;
+    double tau2 = 2.0 * tau1;
+    double zedge = z;
+    /* bend entry (AccSimulator.f90:1032-1094) */
+    double gamma0 = 0, beta0 = 0, hd0 = 0, hd1 = 0, hB = 0, tanphiB = 0, tanphiBb = 0;
+    double psi2 = 0, angB = 0, qm0 = beam->charge / beam->mass;
+    if (bitype == 4) {
+      const double *dp = e->val - 2; /* dparam(k) = val[k-2] */
+      if (dp[4] > 200) { free(rho); return -4; } /* CSR inside the bend: out of scope */
+      gamma0 = -beam->refptcl[5];
+      beta0 = sqrt(1.0 - 1.0 / gamma0 / gamma0);
+      beam->refptcl[4] = beam->refptcl[4] + blength / (Scxl * beta0);
+      double hgap = 2 * dp[5];
+      piperad2 = dp[5];
+      double ang0 = dp[2];
+      hd1 = dp[3];
+      double angF = dp[6];
+      angB = dp[7];
+      double hF = dp[8];
+      hB = dp[9];
+      double dstr1 = dp[10], dstr2 = dstr1;
+      hd0 = ang0 / blength;
+      double tanphiF = tan(angF);
+      double psi1 = hd0 * hgap * dstr1 * (1.0 + sin(angF) * sin(angF)) / cos(angF);
+      double tanphiFb = tan(angF - psi1);
+      tanphiB = tan(angB);
+      psi2 = hd0 * hgap * dstr2 * (1.0 + sin(angB) * sin(angB)) / cos(angB);
+      tanphiBb = tan(angB - psi2);
+      orc_fpol(hd0, hF, tanphiF, tanphiFb, hd1, psi1, beam->pts, angF, beam->nlocal,
+               gamma0, qm0);
+    }
+    int ihlf = 0;
+    for (int j = 1; j <= bnseg; j++) {
+      /* first half map */
+      for (int half = 0; half < 2; half++) {
+        if (half == 1) {
+          /* space charge between the two half maps */
+          if (!(bcurr < 1.0e-10)) {
+            double ptrange[6], range[6], msize[3];
+            beam->nlocal = orc_conv1st(beam->pts, beam->nlocal, &beam->current, &beam->npt,
+                                       beam->refptcl, piperad, piperad2, ptrange);
+            orc_update_compdom(ptrange, mesh, range, msize);
+            orc_deposit(beam->pts, beam->nlocal, mesh, range, msize, rho, NULL, NULL);
+            if (orc_poisson_open(mesh[0], mesh[1], mesh[2], msize[0], msize[1], msize[2], rho)) {
+              free(rho);
+              return -5;
+            }
+            orc_cvbkforth1st(beam->pts, beam->nlocal, beam->refptcl);
+            orc_kick1(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],
+                      beam->current, tau2, beam->mass, beam->charge, NULL);
+          }
+        }
+        if (bitype == 4) {
+          orc_sector(tau1, beta0, hd0, hd1, beam->pts, beam->nlocal, qm0);
+          z = z + tau1;
+        } else if (bitype == 0) {
+          orc_drift_exact(beam->pts, beam->nlocal, beam->refptcl, tau1);
+          z = z + tau1;
+          ihlf++;
+        } else if (bitype == 1) {
+          double x3 = e->val[1];
+          if (x3 < -10.0) { free(rho); return -6; } /* undulator: out of scope */
+          if (x3 < -1.0e-6) {
+            orc_transfmapK(tau1, e->val[0], beam->refptcl, beam->pts, beam->nlocal, qm0);
+          } else if (x3 > 1.0e-5) {
+            free(rho);
+            return -7; /* fringe-field table: out of scope */
+          } else {
+            double xm[36];
+            orc_maplinear_quad(z, tau1, xm, beam->refptcl, e->val[0], e->mapstp,
+                               beam->charge, beam->mass);
+            orc_apply_xm(beam->pts, beam->nlocal, xm);
+          }
+          z = z + tau1;
+          ihlf++;
+        } else if (bitype >= 101 && bitype <= 106) {
+          if (e->val[3] < 0.0) {
+            orc_ideal_rf(beam->pts, beam->nlocal, beam->refptcl, beam->mass, tau1,
+                         e->val[0], e->val[1], e->val[2], j, bnseg, ihlf);
+          } else if (bitype == 103 && e->ndata > 1) {
+            double xm[36];
+            orc_maplinear_ccl(z, tau1, xm, beam->refptcl, zedge, e->val[0], e->val[1],
+                              e->val[2], e->mapstp, beam->charge, beam->mass, e->ndata,
+                              e->zdat, e->edat, e->epdat, e->eppdat);
+            orc_apply_xm(beam->pts, beam->nlocal, xm);
+          } else {
+            free(rho);
+            return -8;
+          }
+          z = z + tau1;
+          ihlf++;
+        } else {
+          free(rho);
+          return -9;
+        }
+      }
+      DIAG();
+    }
+    if (bitype == 4)
+      orc_bpol(hd0, hB, tanphiB, tanphiBb, hd1, psi2, beam->pts, angB, beam->nlocal, gamma0,
+               qm0);
+  }
+#undef DIAG
+  beam->z = z;
+  free(rho);
+  return nrows;
+}

@@ -1,0 +1,145 @@
+"""ctypes bindings of the CPU oracle (oracle/impz_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by __graft_entry__.smoke() as
+the checker, and by bench.py's CPU-baseline leg.  The product never imports
+it.  PARITY UNPINNED: the oracle restates the reference's Fortran (no
+Fortran compiler or golden output exists to run it against); it is pinned by
+known-answer tests in tests/test_oracle_kat.py.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_impz.so")
+DIAG_LEN = 45
+RAW_LEN = 44
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_LL = ctypes.POINTER(ctypes.c_longlong)
+
+
+class OrcElem(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("nseg", ctypes.c_int),
+        ("mapstp", ctypes.c_int),
+        ("length", ctypes.c_double),
+        ("val", ctypes.c_double * 24),
+        ("ndata", ctypes.c_int),
+        ("zdat", _D), ("edat", _D), ("epdat", _D), ("eppdat", _D),
+    ]
+
+
+class OrcBeam(ctypes.Structure):
+    _fields_ = [
+        ("current", ctypes.c_double), ("mass", ctypes.c_double), ("charge", ctypes.c_double),
+        ("freq", ctypes.c_double), ("npt", ctypes.c_int), ("nlocal", ctypes.c_int),
+        ("pts", _D), ("refptcl", ctypes.c_double * 6), ("z", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-s", "-C", HERE], check=True)
+        L = ctypes.CDLL(LIB_PATH)
+        v = None
+        sig = {
+            "orc_physconst": (v, [ctypes.c_double]),
+            "orc_get_physconst": (v, [_D]),
+            "orc_set_threads": (v, [ctypes.c_int]),
+            "orc_drift_exact": (v, [_D, ctypes.c_int, _D, ctypes.c_double]),
+            "orc_maplinear_quad": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_double,
+                                       ctypes.c_int, ctypes.c_double, ctypes.c_double]),
+            "orc_maplinear_ccl": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_int, _D, _D, _D, _D]),
+            "orc_apply_xm": (v, [_D, ctypes.c_int, _D]),
+            "orc_transfmapK": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_int,
+                                   ctypes.c_double]),
+            "orc_conv1st": (ctypes.c_int, [_D, ctypes.c_int, _D, _I, _D, ctypes.c_double,
+                                           ctypes.c_double, _D]),
+            "orc_update_compdom": (v, [_D, _I, _D, _D]),
+            "orc_deposit": (v, [_D, ctypes.c_int, _I, _D, _D, _D, _I, _LL]),
+            "orc_igf": (v, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                            ctypes.c_double, ctypes.c_double, _D]),
+            "orc_poisson_open": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_double, ctypes.c_double,
+                                                ctypes.c_double, _D]),
+            "orc_poisson_direct": (v, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_double, _D, _D]),
+            "orc_cvbkforth1st": (v, [_D, ctypes.c_int, _D]),
+            "orc_kick1": (v, [_D, ctypes.c_int, _D, _I, _D, _D, ctypes.c_double, ctypes.c_double,
+                              ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]),
+            "orc_moment_sums": (v, [_D, ctypes.c_int, _D]),
+            "orc_diag_row": (v, [ctypes.c_double, _D, ctypes.c_int, ctypes.c_int, _D,
+                                 ctypes.c_double, _D]),
+            "orc_run": (ctypes.c_int, [ctypes.POINTER(OrcElem), ctypes.c_int,
+                                       ctypes.POINTER(OrcBeam), _I, _D, ctypes.c_int]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def dp(a):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+def physconst(freq):
+    lib().orc_physconst(freq)
+    out = np.zeros(5)
+    lib().orc_get_physconst(dp(out))
+    return dict(Pi=out[0], Clight=out[1], Scxl=out[2], Rad2deg=out[3], Scfreq=out[4])
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+def elem_from(e):
+    """Converts an impz_b200 ElemStruct (or any object with the same fields)."""
+    o = OrcElem()
+    o.type, o.nseg, o.mapstp, o.length = e.type, e.nseg, e.mapstp, e.length
+    for i in range(24):
+        o.val[i] = e.val[i]
+    o.ndata = getattr(e, "ndata", 0)
+    if o.ndata:
+        o.zdat, o.edat, o.epdat, o.eppdat = e.zdat, e.edat, e.epdat, e.eppdat
+    return o
+
+
+def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0):
+    """orc_run over a lattice: returns (rows, final pts, final beam)."""
+    physconst(freq)
+    arr = (OrcElem * len(elems))(*[elem_from(e) for e in elems])
+    keep = [getattr(e, "_keep", None) for e in elems]
+    p = np.ascontiguousarray(pts, dtype=np.float64).copy()
+    beam = OrcBeam()
+    beam.current, beam.mass, beam.charge, beam.freq = current, mass, charge, freq
+    beam.npt = beam.nlocal = p.shape[0]
+    beam.pts = dp(p)
+    for i in range(6):
+        beam.refptcl[i] = refptcl[i]
+    beam.z = z
+    mesh = np.array(grid, dtype=np.int32)
+    nsteps = sum(e.nseg for e in elems)
+    rows = np.zeros((nsteps + 1, DIAG_LEN))
+    n = lib().orc_run(arr, len(elems), ctypes.byref(beam), mesh.ctypes.data_as(_I), dp(rows),
+                      nsteps + 1)
+    del keep
+    if n < 0:
+        raise RuntimeError("orc_run failed: %d" % n)
+    return rows[:n], p[: beam.nlocal].copy(), beam

@@ -1,0 +1,95 @@
+"""The C-ABI library loads and exports every entry point of include/impz_b200.h;
+its host-only entry points (RK6 maps, diagnostic formulas, step counting)
+agree bit for bit with the oracle.  No GPU needed."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import load_impz, load_oracle
+
+impz = load_impz()
+orc = load_oracle()
+from impz_b200 import beams  # noqa: E402
+
+
+def test_library_exports_every_declared_symbol():
+    L = impz.lib()
+    declared = impz.declared_symbols()
+    assert len(declared) >= 20
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_error_strings_and_version():
+    assert "sm_100a" in impz.lib().impz_version().decode()
+    for code in range(0, -10, -1):
+        assert impz.error_string(code) != "unknown error"
+
+
+def test_create_rejects_bad_arguments_without_device():
+    pts, ref = beams.gaussian_bunch(64)
+    h = ctypes.c_void_p()
+    r = pts.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    rf = ref.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    L = impz.lib()
+    # non-power-of-two grid: refused before any device call
+    assert L.impz_bunch_create(r, 64, 0.03, 938e6, 1.0, 402.5e6, rf, 30, 32, 64, 0, 0,
+                               ctypes.byref(h)) == impz.ERR_UNSUPPORTED
+    assert L.impz_bunch_create(r, 0, 0.03, 938e6, 1.0, 402.5e6, rf, 32, 32, 64, 0, 0,
+                               ctypes.byref(h)) == impz.ERR_ARG
+
+
+@pytest.mark.parametrize("mapstp", [1, 3])
+def test_quad_linear_map_matches_oracle_bitwise(mapstp):
+    freq, mass, charge = 402.5e6, beams.PROTON_MASS_EV, 1.0
+    ref = beams.refptcl_for(2.5e6, mass)
+    e = impz.elem(1, 0.1, 4, mapstp, [20.0, 0.0, 1.0])
+    xm_p, ref_p = impz.maplinear(e, 0.0, 0.3, 0.0125, ref, charge, mass, freq)
+    orc.physconst(freq)
+    xm_o = np.zeros(36)
+    ref_o = ref.copy()
+    orc.lib().orc_maplinear_quad(0.3, 0.0125, orc.dp(xm_o), orc.dp(ref_o), 20.0, mapstp, charge,
+                                 mass)
+    np.testing.assert_array_equal(xm_p, xm_o.reshape(6, 6, order="F"))
+    np.testing.assert_array_equal(ref_p, ref_o)
+
+
+def test_ccl_linear_map_matches_oracle_bitwise():
+    freq, mass, charge = 402.5e6, beams.PROTON_MASS_EV, 1.0
+    ref = beams.refptcl_for(2.5e6, mass)
+    zt = np.linspace(0.0, 0.2, 41)
+    ez = 1e6 * np.sin(np.pi * zt / 0.2)
+    ezp = 1e6 * np.pi / 0.2 * np.cos(np.pi * zt / 0.2)
+    ezpp = -1e6 * (np.pi / 0.2) ** 2 * np.sin(np.pi * zt / 0.2)
+    e = impz.elem(103, 0.2, 4, 5, [1.0, 402.5e6, -30.0, 1.0, 0.01], rf=(zt, ez, ezp, ezpp))
+    xm_p, ref_p = impz.maplinear(e, 0.0, 0.05, 0.025, ref, charge, mass, freq)
+    orc.physconst(freq)
+    xm_o = np.zeros(36)
+    ref_o = ref.copy()
+    cols = [np.ascontiguousarray(c) for c in (zt, ez, ezp, ezpp)]
+    orc.lib().orc_maplinear_ccl(0.05, 0.025, orc.dp(xm_o), orc.dp(ref_o), 0.0, 1.0, 402.5e6,
+                                -30.0, 5, charge, mass, len(zt), *[orc.dp(c) for c in cols])
+    np.testing.assert_array_equal(xm_p, xm_o.reshape(6, 6, order="F"))
+    np.testing.assert_array_equal(ref_p, ref_o)
+
+
+def test_diag_row_matches_oracle_bitwise():
+    freq, mass = 402.5e6, beams.PROTON_MASS_EV
+    pts, ref = beams.gaussian_bunch(5000, seed=3)
+    orc.physconst(freq)
+    raw = np.zeros(orc.RAW_LEN)
+    orc.lib().orc_moment_sums(orc.dp(np.ascontiguousarray(pts)), pts.shape[0], orc.dp(raw))
+    row_o = np.zeros(orc.DIAG_LEN)
+    orc.lib().orc_diag_row(0.7, orc.dp(raw), pts.shape[0], pts.shape[0], orc.dp(ref), mass,
+                           orc.dp(row_o))
+    rec = np.zeros(impz.MOMREC)
+    rec[:44] = raw
+    rec[44] = rec[45] = pts.shape[0]
+    row_p = impz.diag_row(0.7, rec, ref, mass, freq)
+    np.testing.assert_array_equal(row_p, row_o)
+
+
+def test_count_steps():
+    assert impz.count_steps(beams.fodo(10)) == 160
+    assert impz.count_steps(beams.fodo(25, nseg=10)) == 1000

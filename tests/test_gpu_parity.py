@@ -1,0 +1,214 @@
+"""GPU parity: the CUDA path, called through the C ABI, against the CPU oracle.
+
+Tolerances (plain FP64 form):
+  * grid geometry, cell indices, per-cell counts: bit-exact
+  * charge density, potential, fields: relative L2 <= 1e-12
+  * particle coordinates after one kick and half map: max relative error
+    <= 1e-11 of each column's rms (the potential differs at rounding level)
+  * rms sizes, emittances, centroids after a full lattice: rel <= 1e-8
+FP32-convolution form: rms moments within 1e-5 relative of the FP64 oracle.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import load_impz, load_oracle
+
+pytestmark = pytest.mark.gpu
+
+impz = load_impz()
+orc = load_oracle()
+from impz_b200 import beams  # noqa: E402
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def oracle_step(pts, cfg, e_first, tau, piperad):
+    """One space-charge step of the reference sequence on the oracle:
+    drift1 half map -> conv1st -> update_CompDom -> deposit -> openBC3D ->
+    cvbkforth1st -> kick1 (AccSimulator.f90:1109-1426)."""
+    P = orc.physconst(cfg["freq"])
+    L = orc.lib()
+    p = np.ascontiguousarray(pts, dtype=np.float64).copy()
+    n = p.shape[0]
+    ref = np.array(cfg["refptcl"], dtype=np.float64)
+    L.orc_drift_exact(orc.dp(p), n, orc.dp(ref), tau / 2)
+    cur = ctypes.c_double(cfg["current"])
+    npt = ctypes.c_int(n)
+    ptrange = np.zeros(6)
+    nl = L.orc_conv1st(orc.dp(p), n, ctypes.byref(cur), ctypes.byref(npt), orc.dp(ref),
+                       piperad, piperad, orc.dp(ptrange))
+    mesh = np.array(cfg["grid"], dtype=np.int32)
+    rng, msize = np.zeros(6), np.zeros(3)
+    L.orc_update_compdom(orc.dp(ptrange), mesh.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                         orc.dp(rng), orc.dp(msize))
+    G = int(np.prod(cfg["grid"]))
+    rho = np.zeros(G)
+    counts = np.zeros(G, dtype=np.int32)
+    cells = np.zeros(nl, dtype=np.int64)
+    L.orc_deposit(orc.dp(p), nl, mesh.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), orc.dp(rng),
+                  orc.dp(msize), orc.dp(rho), counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                  cells.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
+    phi = rho.copy()
+    assert L.orc_poisson_open(int(mesh[0]), int(mesh[1]), int(mesh[2]), msize[0], msize[1],
+                              msize[2], orc.dp(phi)) == 0
+    L.orc_cvbkforth1st(orc.dp(p), nl, orc.dp(ref))
+    eg = np.zeros(3 * G)
+    L.orc_kick1(orc.dp(p), nl, orc.dp(phi), mesh.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                orc.dp(rng), orc.dp(msize), -ref[5], cur.value, tau, cfg["mass"], cfg["charge"],
+                orc.dp(eg))
+    L.orc_drift_exact(orc.dp(p), nl, orc.dp(ref), tau / 2)
+    return dict(pts=p[:nl], ptrange=ptrange, range=rng, msize=msize, rho=rho, counts=counts,
+                phi=phi, eg=eg, nptot=npt.value, current=cur.value, ref=ref)
+
+
+def gpu_step(pts, cfg, e_first, tau, piperad, form=impz.FORM_FP64):
+    b = impz.Bunch(pts, cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"], cfg["refptcl"],
+                   cfg["grid"], form=form, track_ids=True)
+    z, ih = b.map_half(e_first, 0.0, 0.0, tau / 2, 1, 0)
+    nptot, ptrange, rng, msize = b.sc_prepare(piperad, piperad)
+    rho, counts = b.deposit()
+    phi = b.poisson()
+    eg = b.kick(tau, want_e=True)
+    z, ih = b.map_half(e_first, 0.0, z, tau / 2, 1, ih)
+    out = dict(pts=b.download(), ptrange=ptrange, range=rng, msize=msize, rho=rho, counts=counts,
+               phi=phi, eg=eg, nptot=nptot, info=b.info())
+    b.close()
+    return out
+
+
+@pytest.fixture(scope="module")
+def small():
+    cfg = beams.config0(n=20_000, seed=beams.SEED0 + 7)
+    return cfg
+
+
+def test_single_step_fp64_parity(small):
+    cfg = small
+    e = impz.elem(0, 0.1, 4, 1, [1.0])
+    tau = 0.1 / 4
+    o = oracle_step(cfg["pts"], cfg, e, tau, 1.0)
+    g = gpu_step(cfg["pts"], cfg, e, tau, 1.0)
+    # geometry and cells bit-exact
+    assert g["nptot"] == o["nptot"]
+    np.testing.assert_array_equal(g["ptrange"], o["ptrange"])
+    np.testing.assert_array_equal(g["range"], o["range"])
+    np.testing.assert_array_equal(g["msize"], o["msize"])
+    np.testing.assert_array_equal(g["counts"], o["counts"])
+    assert rel_l2(g["rho"], o["rho"]) <= 1e-12
+    assert rel_l2(g["phi"], o["phi"]) <= 1e-12
+    assert rel_l2(g["eg"], o["eg"]) <= 1e-12
+    # particles, matched by id
+    gp = g["pts"][np.argsort(g["pts"][:, 8])]
+    op = o["pts"][np.argsort(o["pts"][:, 8])]
+    np.testing.assert_array_equal(gp[:, 8], op[:, 8])
+    for c in range(6):
+        scale = np.sqrt(np.mean(op[:, c] ** 2))
+        err = np.max(np.abs(gp[:, c] - op[:, c])) / scale
+        assert err <= 1e-11, (c, err)
+
+
+def test_charge_conservation_and_counts(small):
+    cfg = small
+    e = impz.elem(0, 0.1, 4, 1, [1.0])
+    g = gpu_step(cfg["pts"], cfg, e, 0.025, 1.0)
+    n = cfg["pts"].shape[0]
+    w = cfg["pts"][0, 7]
+    assert int(g["counts"].sum()) == n
+    assert abs(g["rho"].sum() - n * w) <= 1e-12 * n * abs(w)
+
+
+def test_quad_kmap_and_linear_map_parity(small):
+    cfg = small
+    n = 4096
+    pts = cfg["pts"][:n].copy()
+    # gradient quad: RK6 linear map built on the host, applied on the GPU
+    eq = impz.elem(1, 0.1, 4, 3, [20.0, 0.0, 1.0])
+    P = orc.physconst(cfg["freq"])
+    xm_o = np.zeros(36)
+    ref_o = np.array(cfg["refptcl"])
+    orc.lib().orc_maplinear_quad(0.0, 0.0125, orc.dp(xm_o), orc.dp(ref_o), 20.0, 3,
+                                 cfg["charge"], cfg["mass"])
+    p_o = pts.copy()
+    orc.lib().orc_apply_xm(orc.dp(p_o), n, orc.dp(xm_o))
+    b = impz.Bunch(pts, cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"], cfg["refptcl"],
+                   (32, 32, 64), track_ids=True)
+    b.map_half(eq, 0.0, 0.0, 0.0125, 1, 0)
+    p_g = b.download()
+    np.testing.assert_array_equal(p_g[:, :6], p_o[:, :6])
+    np.testing.assert_array_equal(b.info()["refptcl"], ref_o)
+    b.close()
+    # K-map (file ID in (-10,-1e-6)): per-particle cos/cosh, CUDA libm
+    ek = impz.elem(1, 0.1, 4, 1, [30.0, -1.0, 1.0])
+    p_o = pts.copy()
+    ref_o = np.array(cfg["refptcl"])
+    orc.lib().orc_transfmapK(0.0125, 30.0, orc.dp(ref_o), orc.dp(p_o), n,
+                             cfg["charge"] / cfg["mass"])
+    b = impz.Bunch(pts, cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"], cfg["refptcl"],
+                   (32, 32, 64), track_ids=True)
+    b.map_half(ek, 0.0, 0.0, 0.0125, 1, 0)
+    p_g = b.download()
+    for c in range(6):
+        scale = np.sqrt(np.mean(p_o[:, c] ** 2)) + 1e-300
+        assert np.max(np.abs(p_g[:, c] - p_o[:, c])) / scale <= 1e-13
+    b.close()
+
+
+def _row_cmp(rows_g, rows_o, cols, tol):
+    worst = 0.0
+    for c in cols:
+        scale = np.max(np.abs(rows_o[:, c])) + 1e-300
+        worst = max(worst, float(np.max(np.abs(rows_g[:, c] - rows_o[:, c])) / scale))
+    assert worst <= tol, worst
+    return worst
+
+
+RMS_COLS = [6, 7, 8, 9, 11, 12, 13, 14, 15, 17, 18, 19, 20, 21, 23]
+
+
+def gpu_rows(cfg, form):
+    b = impz.Bunch(cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=form, track_ids=False)
+    recs, zs = b.run(cfg["lattice"])
+    # the reference particle of each record follows the same host arithmetic
+    rows_g = []
+    b.close()
+    return recs, zs
+
+
+def test_full_lattice_fp64_moments():
+    cfg = beams.config0(n=20_000, seed=beams.SEED0 + 11)
+    cfg["lattice"] = beams.fodo(2)  # 32 steps
+    rows_o, p_o, beam = orc.run(cfg["lattice"], cfg["pts"], cfg["current"], cfg["mass"],
+                                cfg["charge"], cfg["freq"], cfg["refptcl"], cfg["grid"])
+    recs, zs = gpu_rows(cfg, impz.FORM_FP64)
+    assert recs.shape[0] == rows_o.shape[0]
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    # rebuild rows with the oracle's reference trajectory (fort.18 columns)
+    rows_g = np.array([impz.diag_row(rows_o[i, 0], recs[i], _ref_of(rows_o[i], cfg), cfg["mass"],
+                                     cfg["freq"]) for i in range(len(recs))])
+    _row_cmp(rows_g, rows_o, RMS_COLS, 1e-8)
+
+
+def test_full_lattice_fp32conv_moments():
+    cfg = beams.config0(n=20_000, seed=beams.SEED0 + 11)
+    cfg["lattice"] = beams.fodo(2)
+    rows_o, p_o, beam = orc.run(cfg["lattice"], cfg["pts"], cfg["current"], cfg["mass"],
+                                cfg["charge"], cfg["freq"], cfg["refptcl"], cfg["grid"])
+    recs, zs = gpu_rows(cfg, impz.FORM_FP32CONV)
+    rows_g = np.array([impz.diag_row(rows_o[i, 0], recs[i], _ref_of(rows_o[i], cfg), cfg["mass"],
+                                     cfg["freq"]) for i in range(len(recs))])
+    _row_cmp(rows_g, rows_o, [7, 9, 11, 13, 15, 17, 19, 21, 23], 1e-5)
+
+
+def _ref_of(row, cfg):
+    """refptcl from a fort.18 row: refptcl(5) and -gamma."""
+    r = np.zeros(6)
+    r[4] = row[1]
+    r[5] = -row[2]
+    return r
