@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -26,6 +27,7 @@ using namespace impz;
 namespace {
 
 thread_local char g_cuda_err[256] = "";
+std::atomic<long long> g_launches{0};
 
 int cuda_fail(cudaError_t e, const char* where) {
   std::snprintf(g_cuda_err, sizeof(g_cuda_err), "%s: %s", where, cudaGetErrorString(e));
@@ -144,12 +146,42 @@ struct impz_bunch_s {
   CompiledLattice lat;
   bool run_pending = false;
   size_t bytes = 0;
+  // instrumentation
+  bool prof_on = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  std::vector<int> ev_cat;  // category of each (start, stop) pair
 
   double* cur(int c) { return pbuf[parity][c]; }
   bool f32() const { return form == IMPZ_FORM_FP32CONV; }
 };
 
 namespace {
+
+// CUDA events around one kernel group (only when profiling is on)
+struct ProfScope {
+  impz_bunch_t b;
+  int cat;
+  int nk;
+  ProfScope(impz_bunch_t b_, int cat_, int nkernels) : b(b_), cat(cat_), nk(nkernels) {
+    g_launches += nk;
+    if (!b->prof_on) return;
+    record();
+  }
+  ~ProfScope() {
+    if (!b->prof_on) return;
+    record();
+    b->ev_cat.push_back(cat);
+  }
+  void record() {
+    if (b->ev_used >= b->ev_pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      b->ev_pool.push_back(e);
+    }
+    cudaEventRecord(b->ev_pool[b->ev_used++], b->stream);
+  }
+};
 
 PoissonBuffers poisson_of(impz_bunch_t b) {
   PoissonBuffers pb;
@@ -198,6 +230,7 @@ AdvanceArgs advance_args(impz_bunch_t b, const StepParams* table, int fixed, int
 }
 
 cudaError_t launch_adv(impz_bunch_t b, const AdvanceArgs& a) {
+  ProfScope ps(b, IMPZ_PROF_PUSH, 1);
   if (b->f32()) return fast::launch_advance(a, true, b->grid_adv, b->stream);
   return exact::launch_advance(a, false, b->grid_adv, b->stream);
 }
@@ -217,22 +250,46 @@ DepositArgs deposit_args(impz_bunch_t b, const StepParams* table, int fixed) {
   return d;
 }
 
+int solve_green(impz_bunch_t b) {
+  ProfScope ps(b, IMPZ_PROF_GREEN, 5);
+  PoissonBuffers pb = poisson_of(b);
+  if (b->f32()) { CK(launch_green<float>(pb, b->stream)); }
+  else { CK(launch_green<double>(pb, b->stream)); }
+  return IMPZ_OK;
+}
+
+int solve_conv(impz_bunch_t b) {
+  ProfScope ps(b, IMPZ_PROF_CONV, 3);
+  PoissonBuffers pb = poisson_of(b);
+  if (b->f32()) { CK(launch_convolve<float>(pb, b->stream)); }
+  else { CK(launch_convolve<double>(pb, b->stream)); }
+  return IMPZ_OK;
+}
+
+int solve_efield(impz_bunch_t b) {
+  ProfScope ps(b, IMPZ_PROF_EFIELD, 1);
+  PoissonBuffers pb = poisson_of(b);
+  if (b->f32()) { CK(launch_efield<float>(pb, b->stream)); }
+  else { CK(launch_efield<double>(pb, b->stream)); }
+  return IMPZ_OK;
+}
+
 // deposit + scan + field solve + E for step `fixed` of `table`
 int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
   DepositArgs d = deposit_args(b, table, fixed);
-  CK(exact::launch_deposit(d, b->grid_dep, b->stream));
-  CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
-  PoissonBuffers pb = poisson_of(b);
-  if (b->f32()) {
-    CK(launch_green<float>(pb, b->stream));
-    CK(launch_convolve<float>(pb, b->stream));
-    CK(launch_efield<float>(pb, b->stream));
-  } else {
-    CK(launch_green<double>(pb, b->stream));
-    CK(launch_convolve<double>(pb, b->stream));
-    CK(launch_efield<double>(pb, b->stream));
+  {
+    ProfScope ps(b, IMPZ_PROF_DEPOSIT, 1);
+    CK(exact::launch_deposit(d, b->grid_dep, b->stream));
   }
-  return IMPZ_OK;
+  {
+    ProfScope ps(b, IMPZ_PROF_SCAN, 1);
+    CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
+  }
+  int r = solve_green(b);
+  if (r) return r;
+  r = solve_conv(b);
+  if (r) return r;
+  return solve_efield(b);
 }
 
 int upload_fine(impz_bunch_t b, const StepParams* host2) {
@@ -297,6 +354,7 @@ void free_bunch(impz_bunch_t b) {
                   b->tw64[2], b->st, b->dsteps, b->dfine, b->mom_part, b->rng_part,
                   b->mom_out, b->mom_fine};
   for (void* p : ptrs) cudaFree(p);
+  for (cudaEvent_t e : b->ev_pool) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -619,7 +677,10 @@ int impz_deposit(impz_bunch_t b, double* chgdens, int* counts) {
   int r = upload_fine(b, h);
   if (r) return r;
   DepositArgs d = deposit_args(b, b->dfine, 0);
-  CK(exact::launch_deposit(d, b->grid_dep, b->stream));
+  {
+    ProfScope ps(b, IMPZ_PROF_DEPOSIT, 1);
+    CK(exact::launch_deposit(d, b->grid_dep, b->stream));
+  }
   if (counts) {
     CK(cudaMemcpyAsync(counts, b->counts, b->G * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
   }
@@ -629,7 +690,10 @@ int impz_deposit(impz_bunch_t b, double* chgdens, int* counts) {
     CK(cudaMemcpyAsync(q.data(), b->rho, b->G * sizeof(long long), cudaMemcpyDeviceToHost,
                        b->stream));
   }
-  CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
+  {
+    ProfScope ps(b, IMPZ_PROF_SCAN, 1);
+    CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
+  }
   CK(cudaStreamSynchronize(b->stream));
   if (chgdens) {
     const double qs = b->weight * std::ldexp(1.0, -b->fixbits);
@@ -643,14 +707,10 @@ int impz_poisson_open(impz_bunch_t b, double* phi) {
   if (!b) return IMPZ_ERR_ARG;
   if (b->stage != ST_DEPOSITED) return IMPZ_ERR_STATE;
   CK(cudaSetDevice(b->device));
-  PoissonBuffers pb = poisson_of(b);
-  if (b->f32()) {
-    CK(launch_green<float>(pb, b->stream));
-    CK(launch_convolve<float>(pb, b->stream));
-  } else {
-    CK(launch_green<double>(pb, b->stream));
-    CK(launch_convolve<double>(pb, b->stream));
-  }
+  int r = solve_green(b);
+  if (r) return r;
+  r = solve_conv(b);
+  if (r) return r;
   if (phi) {
     if (b->f32()) {
       double* tmp = nullptr;
@@ -672,9 +732,8 @@ int impz_kick(impz_bunch_t b, double tau, double* egrid) {
   if (!b) return IMPZ_ERR_ARG;
   if (b->stage != ST_SOLVED) return IMPZ_ERR_STATE;
   CK(cudaSetDevice(b->device));
-  PoissonBuffers pb = poisson_of(b);
-  if (b->f32()) { CK(launch_efield<float>(pb, b->stream)); }
-  else { CK(launch_efield<double>(pb, b->stream)); }
+  int r = solve_efield(b);
+  if (r) return r;
   if (egrid) {
     double* tmp = nullptr;
     CK(dalloc(&tmp, (size_t)3 * b->G));
@@ -736,6 +795,74 @@ int impz_count_steps(const impz_elem_t* elems, int nelem) {
   int k = 0;
   for (int i = 0; i < nelem; i++) k += elems[i].nseg;
   return k;
+}
+
+int impz_profile_enable(impz_bunch_t b, int on) {
+  if (!b) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  b->prof_on = on != 0;
+  b->ev_used = 0;
+  b->ev_cat.clear();
+  return IMPZ_OK;
+}
+
+int impz_profile_fetch(impz_bunch_t b, double ms[IMPZ_PROF_NCAT],
+                       long long launches[IMPZ_PROF_NCAT]) {
+  if (!b || !ms || !launches) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  for (int c = 0; c < IMPZ_PROF_NCAT; c++) {
+    ms[c] = 0.0;
+    launches[c] = 0;
+  }
+  for (size_t i = 0; i < b->ev_cat.size(); i++) {
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, b->ev_pool[2 * i], b->ev_pool[2 * i + 1]));
+    ms[b->ev_cat[i]] += t;
+    launches[b->ev_cat[i]] += 1;
+  }
+  return IMPZ_OK;
+}
+
+long long impz_kernel_launches(void) { return g_launches.load(); }
+
+int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double current,
+                      const double refptcl[6]) {
+  if (!b || !pts || !refptcl || n < 1 || n > b->cap) return IMPZ_ERR_ARG;
+  if (pts[6] != b->sp.qmi || pts[7] != b->weight) return IMPZ_ERR_NONUNIFORM;
+  CK(cudaSetDevice(b->device));
+  double* aos = nullptr;
+  unsigned int* bad = nullptr;
+  CK(dalloc(&aos, (size_t)9 * n));
+  CK(dalloc(&bad, 1));
+  CK(cudaMemsetAsync(bad, 0, sizeof(unsigned int), b->stream));
+  CK(cudaMemcpyAsync(aos, pts, (size_t)9 * n * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+  b->parity = 0;
+  k_aos_to_soa<<<1184, 256, 0, b->stream>>>(aos, n, b->pbuf[0][0], b->pbuf[0][1], b->pbuf[0][2],
+                                            b->pbuf[0][3], b->pbuf[0][4], b->pbuf[0][5],
+                                            b->ids[0], b->sp.qmi, b->weight, bad);
+  g_launches += 1;
+  DevState hs;
+  std::memset(&hs, 0, sizeof(hs));
+  hs.current = current;
+  hs.npt = n;
+  hs.nlocal = n;
+  hs.nlive = n;
+  CK(cudaMemcpyAsync(b->st, &hs, sizeof(hs), cudaMemcpyHostToDevice, b->stream));
+  unsigned int hbad = 0;
+  CK(cudaMemcpyAsync(&hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  cudaFree(aos);
+  cudaFree(bad);
+  if (hbad) return IMPZ_ERR_NONUNIFORM;
+  b->current0 = current;
+  std::memcpy(b->refptcl, refptcl, sizeof(b->refptcl));
+  b->z = 0.0;
+  b->stage = ST_IDLE;
+  b->bend.active = false;
+  b->run_pending = false;
+  return IMPZ_OK;
 }
 
 // ---- whole-lattice runner --------------------------------------------

@@ -147,6 +147,28 @@ int impz_run_fetch(impz_bunch_t b, double* recs, double* zs, int maxrec, int* nr
 /* Number of steps (records - 1) impz_run would take for this lattice. */
 int impz_count_steps(const impz_elem_t* elems, int nelem);
 
+/* ---- instrumentation --------------------------------------------------- */
+/* Kernel groups timed by impz_profile_*: */
+#define IMPZ_PROF_DEPOSIT 0  /* charge deposit */
+#define IMPZ_PROF_SCAN 1     /* per-cell count scan (sort cursors) */
+#define IMPZ_PROF_GREEN 2    /* integrated Green function + its DCT-I */
+#define IMPZ_PROF_CONV 3     /* doubled-grid FFT convolution (3 kernels) */
+#define IMPZ_PROF_EFIELD 4   /* finite-difference field */
+#define IMPZ_PROF_PUSH 5     /* fused gather/kick/map/moments/range/sort pass */
+#define IMPZ_PROF_NCAT 6
+/* When on, CUDA events bracket every kernel group on the bunch's stream. */
+int impz_profile_enable(impz_bunch_t b, int on);
+/* Synchronizes; accumulated milliseconds and launches per group since enable. */
+int impz_profile_fetch(impz_bunch_t b, double ms[IMPZ_PROF_NCAT],
+                       long long launches[IMPZ_PROF_NCAT]);
+/* Process-wide number of kernels this library has launched. */
+long long impz_kernel_launches(void);
+/* Replace the particles of an existing bunch (same grid and form); n may
+ * not exceed the capacity the bunch was created with.  Resets Current to
+ * `current` and the bunch's reference particle to refptcl. */
+int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double current,
+                      const double refptcl[6]);
+
 /* Host-side maps (for checking and for callers that keep their own loop):
  * maplinear_Quadrupole (Quadrupole.f90:120-252) and maplinear_CCL
  * (CCL.f90:122-328) by the same RK6; refpt is updated like the reference. */
