@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Throughput of the B200 space-charge kick and element push.
+
+Workload (one step = one space-charge step: deposit, open-boundary field
+solve, fused gather/kick/push pass): 4e6 protons at 2.5 MeV, 30 mA,
+402.5 MHz, uncorrelated 6D Gaussian (Philox-seeded), 64x64x128 grid, the
+FODO lattice with 10 steps per 0.1 m element, FP32-convolution form.
+`value` = particle-steps/s with the particles resident in HBM, timed with
+CUDA events on the bunch's own stream; `e2e` = the same through the C ABI
+with the particles uploaded from and downloaded to pinned host memory and
+the per-step lattice table and moment records crossing PCIe, wall clock.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N>1 runs one replica per GPU under torchrun (weak scaling, no collective on
+the data path); rank 0 prints one JSON line.
+"""
+import argparse
+import ctypes
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+N_PARTICLES = 4_000_000
+GRID = (64, 64, 128)
+METRIC = "particle-steps/s at <=1e-5 moment error vs plain FP64 GPU"
+UNIT = "particle-steps/s"
+
+
+def load(name, path, pkg_dir=None):
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(
+        name, path, submodule_search_locations=[pkg_dir] if pkg_dir else None)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def impz_pkg():
+    pkg = os.path.join(ROOT, "impact-z_b200")
+    return load("impz_b200", os.path.join(pkg, "__init__.py"), pkg)
+
+
+def oracle_pkg():
+    return load("impz_oracle", os.path.join(ROOT, "oracle", "oracle.py"))
+
+
+def workload_config(steps, n=N_PARTICLES):
+    return {"workload": "configs[1] proton FODO: %d protons 2.5 MeV 30 mA 402.5 MHz, "
+                        "6D Gaussian, grid %dx%dx%d, 10 steps per 0.1 m element" % ((n,) + GRID),
+            "particles": n, "grid": list(GRID), "steps": steps, "form": "fp32-convolution",
+            "l2": "no flush: 384 MB resident particle state per step exceeds the 126 MB L2",
+            "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline_port(n, threads, steps, max_seconds=None):
+    """The oracle (C restatement of the reference's Fortran) on the host: a
+    bounded sample of the same workload.  Returns (value, seconds, steps)."""
+    impz = impz_pkg()
+    orc = oracle_pkg()
+    from impz_b200 import beams
+    pts, ref = beams.gaussian_bunch(n)
+    orc.set_threads(threads)
+    done = 0
+    t_total = 0.0
+    p = pts
+    refc = ref.copy()
+    z = 0.0
+    chunk = 1
+    while done < steps:
+        lat = _steps_slice(beams, done, chunk)
+        t0 = time.perf_counter()
+        rows, p, beam = orc.run(lat, p, 0.030, beams.PROTON_MASS_EV, 1.0, 402.5e6, refc, GRID, z)
+        t_total += time.perf_counter() - t0
+        refc = np.array(beam.refptcl[:])
+        z = beam.z
+        done += chunk
+        if max_seconds is not None and t_total > max_seconds:
+            break
+    orc.set_threads(1)
+    return n * done / t_total, t_total, done
+
+
+def _steps_slice(beams, start, count):
+    """Elements covering steps [start, start+count) of the configs[1] lattice."""
+    from impz_b200 import elem
+    full = beams.fodo_steps(start + count)
+    out, pos = [], 0
+    for e in full:
+        lo, hi = pos, pos + e.nseg
+        a, b = max(lo, start), min(hi, start + count)
+        if a < b:
+            k = b - a
+            vals = [e.val[i] for i in range(24)]
+            out.append(elem(e.type, e.length * k / e.nseg, k, e.mapstp, vals))
+        pos = hi
+    return out
+
+
+def run_reference(args):
+    """Reference arm: the oracle port of the reference's CPU path, all host threads."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    n = N_PARTICLES
+    # one warm-up step, then as many timed steps as fit in ~2 minutes
+    v0, t0, _ = cpu_baseline_port(n, threads, 1)
+    budget = max(1, min(args.steps, int(120.0 / max(t0, 1e-3))))
+    value, secs, done = cpu_baseline_port(n, threads, budget)
+    sample = "%d of %d steps of the %d-particle %dx%dx%d workload (oracle port, %d threads)" % (
+        done, args.steps, n, *GRID, threads)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": done, "warmup": 1,
+            "ms_per_step": 1e3 * secs / done, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (Philox-seeded Gaussian)",
+            "config": workload_config(done),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="impz", choices=["impz", "reference"])
+    ap.add_argument("--particles", type=int, default=N_PARTICLES)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-check", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    impz = impz_pkg()
+    from impz_b200 import beams
+    if impz.lib().impz_set_device(local) != 0:
+        raise SystemExit("no CUDA device")
+    n = args.particles
+    K, W = args.steps, args.warmup
+    pts, ref = beams.gaussian_bunch(n, seed=beams.SEED0 + rank)
+    lat = beams.fodo_steps(K)
+    warm = beams.fodo_steps(W)
+
+    b = impz.Bunch(pts, 0.030, beams.PROTON_MASS_EV, 1.0, 402.5e6, ref, GRID,
+                   form=impz.FORM_FP32CONV, track_ids=False)
+    b.run(warm)                          # warm-up steps (untimed)
+    b.upload(pts, 0.030, ref)
+    stream = torch.cuda.ExternalStream(b.stream())
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+
+    # ---- device-timed region: K steps, state resident in HBM
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.2)
+    b.profile_enable(True)
+    l0 = impz.kernel_launches()
+    ev0.record(stream)
+    b.run_async(lat)
+    ev1.record(stream)
+    recs32, zs = b.run_fetch()
+    torch.cuda.synchronize()
+    l1 = impz.kernel_launches()
+    clk = clocks.stop()
+    prof = b.profile_fetch()
+    b.profile_enable(False)
+    t = ev0.elapsed_time(ev1) / 1e3
+    if dist:
+        tt = torch.tensor([t], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    value = world * n * K / t
+
+    # ---- moment error of this run against the plain FP64 GPU form
+    moment_err = None
+    if not args.no_check:
+        b64 = impz.Bunch(pts, 0.030, beams.PROTON_MASS_EV, 1.0, 402.5e6, ref, GRID,
+                         form=impz.FORM_FP64, track_ids=False)
+        recs64, _ = b64.run(lat)
+        b64.close()
+        moment_err = moment_error(impz, recs32, recs64, zs, ref)
+
+    # ---- e2e through the C ABI with pinned host buffers
+    hp = torch.empty((n, 9), dtype=torch.float64, pin_memory=True).numpy()
+    hp[:] = pts
+    hout = torch.empty((n, 9), dtype=torch.float64, pin_memory=True).numpy()
+    arr = impz.elem_array(lat)
+    nrec = ctypes.c_int()
+    recs = np.zeros((K + 1, impz.MOMREC))
+    zz = np.zeros(K + 1)
+    L = impz.lib()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    L.impz_bunch_upload(b.h, hp.ctypes.data_as(impz._D), n, 0.030, ref.ctypes.data_as(impz._D))
+    L.impz_run(b.h, arr, len(lat), recs.ctypes.data_as(impz._D), zz.ctypes.data_as(impz._D),
+               K + 1, ctypes.byref(nrec))
+    nout = ctypes.c_longlong()
+    L.impz_bunch_download(b.h, hout.ctypes.data_as(impz._D), n, ctypes.byref(nout))
+    te = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([te], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
+    step_table_bytes = 2752 * (K + 2)  # sizeof(StepParams) per step
+    e2e = {"value": world * n * K / te, "unit": UNIT,
+           "h2d_bytes_per_step": int((72 * n + step_table_bytes) / K),
+           "d2h_bytes_per_step": int((72 * n + 8 * impz.MOMREC * (K + 1)) / K),
+           "scope": "per job of K steps: Pts1 upload from pinned memory, lattice step table, "
+                    "K steps, moment records and Pts1 download"}
+    b.close()
+
+    # ---- roofline of the dominant kernel group
+    peak, peak_kind = measured_peak()
+    G = GRID[0] * GRID[1] * GRID[2]
+    alg = {"deposit": 48 * n + 16 * G, "scan": 12 * G, "green": 48 * G, "convolve": 76 * G,
+           "efield": 4 * G + 16 * G, "push": 96 * n + 16 * G}
+    kernels = {}
+    for k, (ms, launches) in prof.items():
+        if launches:
+            avg = ms / launches / 1e3
+            kernels[k] = {"launches": launches, "ms_total": round(ms, 3),
+                          "us_per_launch": round(avg * 1e6, 2),
+                          "share": round(ms / sum(v[0] for v in prof.values()), 4),
+                          "gbs": round(alg[k] / avg / 1e9, 1)}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_total"])
+    traffic = committed_traffic().get(dom)
+    achieved = kernels[dom]["gbs"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                "traffic": traffic, "algorithmic_bytes_per_launch": alg[dom]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, secs, done = cpu_baseline_port(n, 1, 3, max_seconds=30.0)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "%d steps of the %d-particle %dx%dx%d workload, oracle port, 1 thread "
+                         "(%.1f s)" % (done, n, *GRID, secs)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+                "warmup": W, "ms_per_step": 1e3 * t / K, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (Philox-seeded 6D Gaussian protons)",
+                "config": workload_config(K, n), "clocks": clk, "e2e": e2e,
+                "gpu_launches": int(l1 - l0), "roofline": roofline, "cpu_baseline": cpu,
+                "kernels": kernels, "moment_rel_err_vs_fp64": moment_err}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def moment_error(impz, recs_a, recs_b, zs, ref):
+    """Max relative difference of rms sizes, emittances and centroid spreads."""
+    from impz_b200 import beams
+    cols = [7, 9, 11, 13, 15, 17, 19, 21, 23]
+    worst = 0.0
+    for i in range(len(recs_a)):
+        ra = impz.diag_row(zs[i], recs_a[i], ref, beams.PROTON_MASS_EV, 402.5e6)
+        rb = impz.diag_row(zs[i], recs_b[i], ref, beams.PROTON_MASS_EV, 402.5e6)
+        for c in cols:
+            d = abs(ra[c] - rb[c]) / max(abs(rb[c]), 1e-300)
+            worst = max(worst, d)
+    return worst
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -94,7 +94,18 @@ _SIGS = {
     "impz_count_steps": (ctypes.c_int, [_E, ctypes.c_int]),
     "impz_maplinear": (ctypes.c_int, [_E, ctypes.c_double, ctypes.c_double, ctypes.c_double, _D,
                                       ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]),
+    "impz_profile_enable": (ctypes.c_int, [_B, ctypes.c_int]),
+    "impz_profile_fetch": (ctypes.c_int, [_B, _D, _LL]),
+    "impz_kernel_launches": (ctypes.c_longlong, []),
+    "impz_bunch_upload": (ctypes.c_int, [_B, _D, ctypes.c_longlong, ctypes.c_double, _D]),
 }
+
+PROF_NAMES = ("deposit", "scan", "green", "convolve", "efield", "push")
+
+
+def kernel_launches():
+    """Process-wide number of kernels the library has launched."""
+    return int(lib().impz_kernel_launches())
 
 
 def lib():
@@ -223,6 +234,26 @@ class Bunch:
 
     def __exit__(self, *a):
         self.close()
+
+    def stream(self):
+        """The bunch's cudaStream_t as an integer handle."""
+        return int(lib().impz_bunch_stream(self.h) or 0)
+
+    def upload(self, pts, current, refptcl):
+        pts = np.ascontiguousarray(pts, dtype=np.float64)
+        ref = np.ascontiguousarray(refptcl, dtype=np.float64)
+        _check(lib().impz_bunch_upload(self.h, _dp(pts), pts.shape[0], current, _dp(ref)),
+               "impz_bunch_upload")
+
+    def profile_enable(self, on=True):
+        _check(lib().impz_profile_enable(self.h, 1 if on else 0), "impz_profile_enable")
+
+    def profile_fetch(self):
+        ms = np.zeros(len(PROF_NAMES))
+        la = np.zeros(len(PROF_NAMES), dtype=np.int64)
+        _check(lib().impz_profile_fetch(self.h, _dp(ms), la.ctypes.data_as(_LL)),
+               "impz_profile_fetch")
+        return {k: (float(ms[i]), int(la[i])) for i, k in enumerate(PROF_NAMES)}
 
     def info(self):
         out = np.zeros(11)

@@ -142,3 +142,19 @@ def config1(n=4_000_000, seed=SEED0, periods=25, nseg=10):
     pts, ref = gaussian_bunch(n, seed)
     return dict(pts=pts, refptcl=ref, current=0.030, mass=PROTON_MASS_EV, charge=1.0,
                 freq=402.5e6, grid=(64, 64, 128), lattice=fodo(periods, nseg=nseg))
+
+
+def fodo_steps(nsteps, gradient=20.0, ldrift=0.1, lquad=0.1, nseg=10, radius=1.0):
+    """The configs[1] FODO pattern (10 steps per 0.1 m element) cut to exactly
+    `nsteps` space-charge steps; a final partial element keeps the step length."""
+    from . import elem
+    pattern = [(0, ldrift, [radius]), (1, lquad, [gradient, 0.0, radius]),
+               (0, ldrift, [radius]), (1, lquad, [-gradient, 0.0, radius])]
+    out, left, i = [], int(nsteps), 0
+    while left > 0:
+        t, length, vals = pattern[i % 4]
+        k = min(nseg, left)
+        out.append(elem(t, length * k / nseg, k, 1, vals))
+        left -= k
+        i += 1
+    return out
