@@ -66,8 +66,21 @@ def _deps(src):
     return [src] + hdrs + [os.path.abspath(__file__)]
 
 
-def build_lib(verbose=False):
-    os.makedirs(OBJ, exist_ok=True)
+def build_lib(verbose=False, defines=(), lib=None, obj=None):
+    """Builds the library; `defines` (e.g. ["-DIMPZ_ADV_U=2"]) and an
+    alternative output path allow side-by-side launch-shape variants."""
+    global OBJ
+    lib = lib or LIB
+    obj_dir = obj or OBJ
+    os.makedirs(obj_dir, exist_ok=True)
+    saved, OBJ = OBJ, obj_dir
+    try:
+        return _build_lib(verbose, list(defines), lib)
+    finally:
+        OBJ = saved
+
+
+def _build_lib(verbose, defines, lib_path):
     nv = nvcc()
     jobs = []
     objs = []
@@ -76,7 +89,7 @@ def build_lib(verbose=False):
         o = os.path.join(OBJ, src + ".o")
         objs.append(o)
         if not _newer(o, _deps(s)):
-            jobs.append([nv] + NVCC_COMMON + extra + ["-c", s, "-o", o])
+            jobs.append([nv] + NVCC_COMMON + extra + defines + ["-c", s, "-o", o])
     for src in HOST_UNITS:
         s = os.path.join(CSRC, src)
         o = os.path.join(OBJ, src + ".o")
@@ -88,10 +101,10 @@ def build_lib(verbose=False):
         for out in ex.map(_run, jobs):
             if verbose and out.strip():
                 print(out)
-    if jobs or not os.path.exists(LIB):
-        _run([nv] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl",
-                                                             "-lpthread"])
-    return LIB
+    if jobs or not os.path.exists(lib_path):
+        _run([nv] + ARCH + ["-shared", "-o", lib_path] + objs + ["-lcudart_static", "-lrt",
+                                                                  "-ldl", "-lpthread"])
+    return lib_path
 
 
 def build_oracle():

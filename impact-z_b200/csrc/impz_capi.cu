@@ -102,6 +102,8 @@ enum Stage { ST_IDLE = 0, ST_PREPARED = 1, ST_DEPOSITED = 2, ST_SOLVED = 3 };
 struct impz_bunch_s {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t stream2 = nullptr;   // Green-function build, overlapped with the deposit
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int form = 0, flags = 0;
   long long cap = 0;
   int nx = 0, ny = 0, nz = 0;
@@ -163,7 +165,9 @@ struct ProfScope {
   impz_bunch_t b;
   int cat;
   int nk;
-  ProfScope(impz_bunch_t b_, int cat_, int nkernels) : b(b_), cat(cat_), nk(nkernels) {
+  cudaStream_t s;
+  ProfScope(impz_bunch_t b_, int cat_, int nkernels, cudaStream_t s_ = nullptr)
+      : b(b_), cat(cat_), nk(nkernels), s(s_ ? s_ : b_->stream) {
     g_launches += nk;
     if (!b->prof_on) return;
     record();
@@ -179,7 +183,7 @@ struct ProfScope {
       cudaEventCreate(&e);
       b->ev_pool.push_back(e);
     }
-    cudaEventRecord(b->ev_pool[b->ev_used++], b->stream);
+    cudaEventRecord(b->ev_pool[b->ev_used++], s);
   }
 };
 
@@ -250,11 +254,11 @@ DepositArgs deposit_args(impz_bunch_t b, const StepParams* table, int fixed) {
   return d;
 }
 
-int solve_green(impz_bunch_t b) {
-  ProfScope ps(b, IMPZ_PROF_GREEN, 5);
+int solve_green(impz_bunch_t b, cudaStream_t s) {
+  ProfScope ps(b, IMPZ_PROF_GREEN, 5, s);
   PoissonBuffers pb = poisson_of(b);
-  if (b->f32()) { CK(launch_green<float>(pb, b->stream)); }
-  else { CK(launch_green<double>(pb, b->stream)); }
+  if (b->f32()) { CK(launch_green<float>(pb, s)); }
+  else { CK(launch_green<double>(pb, s)); }
   return IMPZ_OK;
 }
 
@@ -274,8 +278,15 @@ int solve_efield(impz_bunch_t b) {
   return IMPZ_OK;
 }
 
-// deposit + scan + field solve + E for step `fixed` of `table`
+// deposit + scan + field solve + E for step `fixed` of `table`.  The Green
+// function depends only on this step's grid geometry, so it is built on the
+// second stream while the deposit and the forward transforms run.
 int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
+  CK(cudaEventRecord(b->ev_fork, b->stream));
+  CK(cudaStreamWaitEvent(b->stream2, b->ev_fork, 0));
+  int r = solve_green(b, b->stream2);
+  if (r) return r;
+  CK(cudaEventRecord(b->ev_join, b->stream2));
   DepositArgs d = deposit_args(b, table, fixed);
   {
     ProfScope ps(b, IMPZ_PROF_DEPOSIT, 1);
@@ -285,10 +296,18 @@ int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
     ProfScope ps(b, IMPZ_PROF_SCAN, 1);
     CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
   }
-  int r = solve_green(b);
-  if (r) return r;
-  r = solve_conv(b);
-  if (r) return r;
+  PoissonBuffers pb = poisson_of(b);
+  {
+    ProfScope ps(b, IMPZ_PROF_CONV, 1);
+    if (b->f32()) { CK(launch_conv_forward<float>(pb, b->stream)); }
+    else { CK(launch_conv_forward<double>(pb, b->stream)); }
+  }
+  CK(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
+  {
+    ProfScope ps(b, IMPZ_PROF_CONV, 2);
+    if (b->f32()) { CK(launch_conv_rest<float>(pb, b->stream)); }
+    else { CK(launch_conv_rest<double>(pb, b->stream)); }
+  }
   return solve_efield(b);
 }
 
@@ -355,6 +374,10 @@ void free_bunch(impz_bunch_t b) {
                   b->mom_out, b->mom_fine};
   for (void* p : ptrs) cudaFree(p);
   for (cudaEvent_t e : b->ev_pool) cudaEventDestroy(e);
+  if (b->stream2) cudaStreamSynchronize(b->stream2);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_join) cudaEventDestroy(b->ev_join);
+  if (b->stream2) cudaStreamDestroy(b->stream2);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -441,6 +464,9 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
     }                                                 \
   } while (0)
   ALLOC(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  ALLOC(cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking));
+  ALLOC(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+  ALLOC(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
   for (int p = 0; p < 2; p++)
     for (int c = 0; c < 6; c++) ALLOC(dalloc(&b->pbuf[p][c], (size_t)n));
   if (flags & IMPZ_FLAG_TRACK_IDS) {
@@ -707,7 +733,7 @@ int impz_poisson_open(impz_bunch_t b, double* phi) {
   if (!b) return IMPZ_ERR_ARG;
   if (b->stage != ST_DEPOSITED) return IMPZ_ERR_STATE;
   CK(cudaSetDevice(b->device));
-  int r = solve_green(b);
+  int r = solve_green(b, b->stream);
   if (r) return r;
   r = solve_conv(b);
   if (r) return r;

@@ -7,8 +7,19 @@
 namespace impz {
 
 #define IMPZ_ADV_BLOCK 256
+#ifndef IMPZ_ADV_U
+#define IMPZ_ADV_U 1
+#endif
+#ifndef IMPZ_ADV_MINB
+#define IMPZ_ADV_MINB 2
+#endif
 #define IMPZ_DEP_BLOCK 512
+#ifndef IMPZ_DEP_PPT
 #define IMPZ_DEP_PPT 4
+#endif
+#ifndef IMPZ_DEP_MINB
+#define IMPZ_DEP_MINB 1
+#endif
 #define IMPZ_SCAN_THREADS 1024
 
 #define IMPZ_DECLARE_PARTICLE_LAUNCHERS(NS)                                              \
@@ -47,6 +58,11 @@ template <typename T>
 cudaError_t launch_green(const PoissonBuffers& b, cudaStream_t s);
 template <typename T>
 cudaError_t launch_convolve(const PoissonBuffers& b, cudaStream_t s);
+// the convolution split at the point where G-hat is first needed
+template <typename T>
+cudaError_t launch_conv_forward(const PoissonBuffers& b, cudaStream_t s);
+template <typename T>
+cudaError_t launch_conv_rest(const PoissonBuffers& b, cudaStream_t s);
 template <typename T>
 cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s);
 template <typename T>

@@ -20,6 +20,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <climits>
+#include <cstddef>
 #include <stdint.h>
 
 #include "impz_common.h"
@@ -41,7 +42,7 @@ struct Particle {
 
 // ---------------------------------------------------------------------
 // transfer maps; each follows the cited reference loop body
-__device__ __forceinline__ void map_drift(Particle& p, const double* c) {
+__device__ __forceinline__ void map_drift(Particle& p, const volatile double* c) {
   // BeamBunch.f90:286-295; c = {gam0, beta0, tau, Scxl}
   const double gam0 = c[0], beta0 = c[1], tau = c[2], Scxl = c[3];
   double d = p.pt - gam0;
@@ -51,7 +52,7 @@ __device__ __forceinline__ void map_drift(Particle& p, const double* c) {
   p.ph = p.ph - ((1.0 / beta0 + (p.pt - gam0) / tmph) * tau) / Scxl;
 }
 
-__device__ __forceinline__ void map_xm6(Particle& p, const double* xm, int mask_lo,
+__device__ __forceinline__ void map_xm6(Particle& p, const volatile double* xm, int mask_lo,
                                         int mask_hi) {
   // BeamBunch.f90:310-320: temp(j) = sum_k Pts1(k)*xm(j,k) from 0.0; the
   // zero entries of xm only add signed zeros and are skipped.
@@ -70,7 +71,7 @@ __device__ __forceinline__ void map_xm6(Particle& p, const double* xm, int mask_
   p.x = out[0]; p.px = out[1]; p.y = out[2]; p.py = out[3]; p.ph = out[4]; p.pt = out[5];
 }
 
-__device__ __forceinline__ void map_kquad(Particle& p, const double* c) {
+__device__ __forceinline__ void map_kquad(Particle& p, const volatile double* c) {
   // Quadrupole.f90:526-600; c = {refpt6, gambet0, beta0, qmass, K, tau, Scxl, qmi}
   const double refpt6 = c[0], gambet0 = c[1], beta0 = c[2], qmass = c[3], K = c[4];
   const double tau = c[5], Scxl = c[6], qmi = c[7];
@@ -108,7 +109,7 @@ __device__ __forceinline__ void map_kquad(Particle& p, const double* c) {
   p.x = t1; p.px = t2; p.y = t3; p.py = t4; p.ph = t5;
 }
 
-__device__ __forceinline__ void map_idealrf(Particle& p, const double* c, int flags,
+__device__ __forceinline__ void map_idealrf(Particle& p, const volatile double* c, int flags,
                                             int twonseg) {
   // BeamBunch.f90:337-438; c = {vtmp, harm, phi0lc, Scxl, tau, gam0_in,
   //                            gambet_in, gam0_out, cos(phi0lc)}
@@ -155,7 +156,7 @@ __device__ __forceinline__ void map_idealrf(Particle& p, const double* c, int fl
 // c = {h0, h1, tanphi, tanphib, k1, psi, tanphi2, secphi2, secphi3,
 //      secphib2, beta0, gambet, gam0, qm0, qmi, Scxl}
 template <bool EXIT>
-__device__ __forceinline__ void map_pole(Particle& p, const double* c) {
+__device__ __forceinline__ void map_pole(Particle& p, const volatile double* c) {
   const double h0 = c[0], h1 = c[1], tanphi = c[2], tanphib = c[3], k1 = c[4], psi = c[5];
   const double tanphi2 = c[6], secphi2 = c[7], secphi3 = c[8], secphib2 = c[9];
   const double beta0 = c[10], gambet = c[11], gam0 = c[12], qm0 = c[13], qmi = c[14];
@@ -204,7 +205,7 @@ __device__ __forceinline__ void map_pole(Particle& p, const double* c) {
 // c = {R11,R12,R16,R21,R22,R26,R51,R52,R56, T111,T112,T116,T122,T126,T166,
 //      T144,T216,T222,T266,T244,T314,T324,T346,T522,T544,T526,
 //      len, beta0, gambet, gam0, qm0, qmi, Scxl}
-__device__ __forceinline__ void map_sector(Particle& p, const double* c) {
+__device__ __forceinline__ void map_sector(Particle& p, const volatile double* c) {
   const double R11 = c[0], R12 = c[1], R16 = c[2], R21 = c[3], R22 = c[4], R26 = c[5];
   const double R51 = c[6], R52 = c[7], R56 = c[8];
   const double T111 = c[9], T112 = c[10], T116 = c[11], T122 = c[12], T126 = c[13];
@@ -236,9 +237,14 @@ __device__ __forceinline__ void map_sector(Particle& p, const double* c) {
   p.pt = -(beta0 * gambet * (eta + (qmi - qm0) / qm0));
 }
 
-__device__ __forceinline__ void apply_program(Particle& p, const MapProgram& prog) {
-  for (int o = 0; o < prog.nops; o++) {
-    const MapOp& op = prog.ops[o];
+// Map programs are staged in shared memory and read through volatile
+// pointers inside the particle loop: the coefficients are re-read (a
+// broadcast shared load) per particle instead of being hoisted into
+// registers for every map kind the switch could take.
+__device__ __forceinline__ void apply_program(Particle& p, const volatile MapProgram& prog) {
+  const int nops = prog.nops;
+  for (int o = 0; o < nops; o++) {
+    const volatile MapOp& op = prog.ops[o];
     switch (op.kind) {
       case MAP_DRIFT: map_drift(p, op.c); break;
       case MAP_XM6: map_xm6(p, op.c, op.flags, op.iparam); break;
@@ -250,6 +256,14 @@ __device__ __forceinline__ void apply_program(Particle& p, const MapProgram& pro
       default: break;
     }
   }
+}
+
+// Copies a step's programs into shared memory (whole block).
+__device__ __forceinline__ void stage_programs(MapProgram* dst, const StepParams* sp) {
+  const int nw = (int)(2 * sizeof(MapProgram) / sizeof(int));
+  const int* src0 = reinterpret_cast<const int*>(&sp->post);
+  int* d = reinterpret_cast<int*>(dst);
+  for (int e = threadIdx.x; e < nw; e += blockDim.x) d[e] = src0[e];
 }
 
 // ---------------------------------------------------------------------
@@ -292,7 +306,8 @@ struct Cell {
   double ab, cd, ef;
 };
 
-__device__ __forceinline__ Cell cic_cell(double x, double y, double z, const Geom& g) {
+template <typename GT>
+__device__ __forceinline__ Cell cic_cell(double x, double y, double z, const GT& g) {
   Cell c;
   c.ix = (int)__dadd_rn(__dmul_rn(__dsub_rn(x, g.range[0]), g.hi[0]), 1.0);
   c.ab = __dmul_rn(__dadd_rn(__dsub_rn(g.range[0], x), __dmul_rn((double)c.ix, g.h[0])), g.hi[0]);
@@ -457,25 +472,143 @@ __device__ __forceinline__ long long lin_cell(const Cell& c, int nx, int ny) {
 }
 
 // ---------------------------------------------------------------------
-// The fused particle pass of step s (one thread per particle per pass,
-// grid-stride).  Per particle, in the reference's order:
+// The fused particle pass of step s.  Per particle, in the reference's order:
 //   [kick]  conv1st z->t, loss test, deposit cell (sort key),
 //           cvbkforth1st t->z->gather frame, scatter1 gather + kick + z frame
 //   [post]  second half map of step s, then the diagnostic1 sums
 //   [pre]   first half map of step s+1 (and pole faces), conv1st range of s+1
 //   write   to the sorted slot of the deposit cell (kick) or in place.
-// The last block to finish reduces moments and range in block order
-// (deterministic) and performs conv1st's current rescale and update_CompDom.
-template <int BLOCK, bool F32>
-__global__ void __launch_bounds__(BLOCK) k_advance(AdvanceArgs a) {
+// Each thread carries U particles per iteration (U loads in flight).  The
+// 37 moment sums and 7 maxima are not held per thread: every iteration each
+// warp reduce-scatters them in groups of eight with a shuffle butterfly
+// into its own shared-memory accumulators.  The last block to finish
+// reduces moments and range in block order (deterministic) and performs
+// conv1st's current rescale and update_CompDom.
+struct Contrib {  // per-lane particle coordinates feeding the moment sums
+  double x, px, y, py, z, pz;
+};
+
+// value v (0..43, tmplc order of Output.f90:198-234, then |max| and r^2)
+__device__ __forceinline__ double moment_value(const Contrib& c, int v) {
+  const double x = c.x, px = c.px, y = c.y, py = c.py, z = c.z, pz = c.pz;
+  switch (v) {
+    case 0: return x;            case 1: return px;           case 2: return y;
+    case 3: return py;           case 4: return z;            case 5: return pz;
+    case 6: return x * x;        case 7: return px * px;      case 8: return y * y;
+    case 9: return py * py;      case 10: return z * z;       case 11: return pz * pz;
+    case 12: return x * px;      case 13: return y * py;      case 14: return z * pz;
+    case 15: return x * x * x;   case 16: return x * x * x * x;
+    case 17: return px * px * px; case 18: return px * px * px * px;
+    case 19: return y * y * y;   case 20: return y * y * y * y;
+    case 21: return py * py * py; case 22: return py * py * py * py;
+    case 23: return fabs(z * z * z); case 24: return z * z * z * z;
+    case 25: return pz * pz * pz; case 26: return pz * pz * pz * pz;
+    case 27: return x * px * px; case 28: return x * px * px * px;
+    case 29: return x * x * px;  case 30: return x * x * px * px;
+    case 31: return x * x * x * px;
+    case 32: return y * py * py; case 33: return y * py * py * py;
+    case 34: return y * y * py;  case 35: return y * y * py * py;
+    case 36: return y * y * y * py;
+    case 37: return fabs(x);     case 38: return fabs(px);    case 39: return fabs(y);
+    case 40: return fabs(py);    case 41: return fabs(z);     case 42: return fabs(pz);
+    case 43: return x * x + y * y;
+    default: return 0.0;
+  }
+}
+
+// Reduce-scatter eight per-lane values over the warp (9 shuffles); lanes
+// with (lane & 3) == 0 receive the total of value ((lane >> 2) & 7).
+template <bool MAX>
+__device__ __forceinline__ double warp_rs8(const double (&v)[8], int lane) {
+  double w[4], x[2], y;
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const double send = b4 ? v[k] : v[k + 4];
+    const double keep = b4 ? v[k + 4] : v[k];
+    const double recv = __shfl_xor_sync(0xffffffffu, send, 16);
+    w[k] = MAX ? fmax(keep, recv) : keep + recv;
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const double send = b3 ? w[k] : w[k + 2];
+    const double keep = b3 ? w[k + 2] : w[k];
+    const double recv = __shfl_xor_sync(0xffffffffu, send, 8);
+    x[k] = MAX ? fmax(keep, recv) : keep + recv;
+  }
+  {
+    const double send = b2 ? x[0] : x[1];
+    const double keep = b2 ? x[1] : x[0];
+    const double recv = __shfl_xor_sync(0xffffffffu, send, 4);
+    y = MAX ? fmax(keep, recv) : keep + recv;
+  }
+  double t = __shfl_xor_sync(0xffffffffu, y, 2);
+  y = MAX ? fmax(y, t) : y + t;
+  t = __shfl_xor_sync(0xffffffffu, y, 1);
+  y = MAX ? fmax(y, t) : y + t;
+  return y;
+}
+
+// value index a lane owns after warp_rs8 (bit 4 -> 4, bit 3 -> 2, bit 2 -> 1)
+__device__ __forceinline__ int rs8_index(int lane) {
+  return ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+}
+
+template <int U>
+__device__ __forceinline__ void warp_moments(double* accw, const Contrib (&c)[U], int lane) {
+  // groups: sums 0-7, 8-15, 16-23, 24-31, 32-36 (+3 pad); maxima 37-43 (+1 pad)
+#pragma unroll
+  for (int g = 0; g < 5; g++) {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int idx = g * 8 + k;
+      double s = 0.0;
+      if (idx < 37) {
+#pragma unroll
+        for (int u = 0; u < U; u++) s = s + moment_value(c[u], idx);
+      }
+      v[k] = s;
+    }
+    const double r = warp_rs8<false>(v, lane);
+    const int idx = g * 8 + rs8_index(lane);
+    if ((lane & 3) == 0 && idx < 37) accw[idx] += r;
+  }
+  {
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int idx = 37 + k;
+      double m = 0.0;
+      if (idx < IMPZ_RAW_LEN) {
+#pragma unroll
+        for (int u = 0; u < U; u++) m = fmax(m, moment_value(c[u], idx));
+      }
+      v[k] = m;
+    }
+    const double r = warp_rs8<true>(v, lane);
+    const int idx = 37 + rs8_index(lane);
+    if ((lane & 3) == 0 && idx < IMPZ_RAW_LEN) accw[idx] = fmax(accw[idx], r);
+  }
+}
+
+template <int BLOCK, bool F32, int U>
+__global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a) {
   __shared__ double red[BLOCK / 32][IMPZ_RAW_LEN];
   __shared__ double redr[BLOCK / 32][8];
   __shared__ unsigned int s_last;
+  __shared__ double fin[8];
+  __shared__ MapProgram progs[2];  // post, pre_next
+  __shared__ Geom sgeom;
   DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
   const StepParams* __restrict__ sp = a.steps + s;
   const long long n = st->nlocal;
-  const Geom g = st->geom;
+  static_assert(offsetof(StepParams, pre_next) == sizeof(MapProgram), "program layout");
+  stage_programs(progs, sp);
+  if (threadIdx.x == 0) sgeom = st->geom;
+  __syncthreads();
+  const volatile Geom& g = sgeom;
   const double xl = a.k.Scxl, xk = a.k.xk;
   const bool kick = a.kick != 0;
   const bool post = a.do_post != 0;
@@ -494,41 +627,53 @@ __global__ void __launch_bounds__(BLOCK) k_advance(AdvanceArgs a) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const long long G = (long long)nx * ny * nz;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double* accw = red[wid];
+  for (int v = lane; v < IMPZ_RAW_LEN; v += 32) accw[v] = 0.0;
+  __syncwarp();
 
-  double acc[IMPZ_RAW_LEN];
-#pragma unroll
-  for (int v = 0; v < IMPZ_RAW_LEN; v++) acc[v] = 0.0;
   double rmn[3] = {1e300, 1e300, 1e300}, rmx[3] = {-1e300, -1e300, -1e300};
   long long nlive = 0, nkept = 0;
   unsigned int err = 0;
 
-  const long long stride = (long long)gridDim.x * BLOCK;
+  const long long stride = (long long)gridDim.x * BLOCK * U;
   const long long nround = (n + stride - 1) / stride * stride;
-  for (long long i = (long long)blockIdx.x * BLOCK + threadIdx.x; i < nround; i += stride) {
-    bool keep = i < n;
-    Particle p;
-    long long key = 0;
-    if (keep) {
-      p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
-      p.py = a.in[3][i]; p.ph = a.in[4][i]; p.pt = a.in[5][i];
-      if (kick) {
-        TFrame t = to_tframe(p, gam, rad, xl);
+  for (long long i0 = (long long)blockIdx.x * BLOCK * U + threadIdx.x; i0 < nround;
+       i0 += stride) {
+    Particle p[U];
+    bool keep[U];
+    long long key[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const long long i = i0 + (long long)u * BLOCK;
+      keep[u] = i < n;
+      key[u] = 0;
+      if (keep[u]) {
+        p[u].x = a.in[0][i]; p[u].px = a.in[1][i]; p[u].y = a.in[2][i];
+        p[u].py = a.in[3][i]; p[u].ph = a.in[4][i]; p[u].pt = a.in[5][i];
+      } else {
+        p[u].x = 0; p[u].px = 0; p[u].y = 0; p[u].py = 0; p[u].ph = 0; p[u].pt = 0;
+      }
+    }
+    Contrib c[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (keep[u] && kick) {
+        TFrame t = to_tframe(p[u], gam, rad, xl);
         if (t.lost) {
-          keep = false;
+          keep[u] = false;
         } else {
           Cell cd = cic_cell(t.xt, t.yt, t.zt, g);
-          key = cell_inside(cd, nx, ny, nz) ? lin_cell(cd, nx, ny) : G;
+          key[u] = cell_inside(cd, nx, ny, nz) ? lin_cell(cd, nx, ny) : G;
           // cvbkforth1st (BeamBunch.f90:1681-1699); betai reuses conv1st's
-          // tmpbet, which is the same expression of the same operands
+          // tmpbet, the same expression of the same operands
           const double rcp = t.rcp;
           const double betai = sqrt(t.tmpbet);
-          double ph1 = t.zt * xk / (-(gam * betai));
-          double x1 = t.xt * xk + p.px * ph1 * rcp;
-          double y1 = t.yt * xk + p.py * ph1 * rcp;
+          const double ph1 = t.zt * xk / (-(gam * betai));
+          const double x1 = t.xt * xk + p[u].px * ph1 * rcp;
+          const double y1 = t.yt * xk + p[u].py * ph1 * rcp;
           const double xg = x1 * xl, yg = y1 * xl;
           const double zg = -(gam * betai * ph1 * xl);
-          // scatter1 (BeamBunch.f90:2121-2177); indices are clamped to the
-          // grid (the reference reads outside it without a check)
+          // scatter1 (BeamBunch.f90:2121-2177); indices clamped into the grid
           Cell cg = cic_cell(xg, yg, zg, g);
           if (!cell_inside(cg, nx, ny, nz)) {
             err |= DERR_OUTSIDE;
@@ -544,24 +689,29 @@ __global__ void __launch_bounds__(BLOCK) k_advance(AdvanceArgs a) {
             ez = ez * a.efield_scale;
           }
           const double exn = ex * gam, eyn = ey * gam, ezn = ez;
-          p.x = xg * xk;
-          p.px = p.px + txy * exn;
-          p.y = yg * xk;
-          p.py = p.py + txy * eyn;
-          p.ph = zg * xk / (-(gam * betai));
-          p.pt = p.pt - tt * ezn;
+          p[u].x = xg * xk;
+          p[u].px = p[u].px + txy * exn;
+          p[u].y = yg * xk;
+          p[u].py = p[u].py + txy * eyn;
+          p[u].ph = zg * xk / (-(gam * betai));
+          p[u].pt = p[u].pt - tt * ezn;
         }
       }
-    }
-    if (keep) {
-      if (post) {
-        apply_program(p, sp->post);
-        if (mom) moment_accumulate(acc, p);
+      if (keep[u] && post) apply_program(p[u], progs[0]);
+      if (keep[u]) {
+        c[u].x = p[u].x; c[u].px = p[u].px; c[u].y = p[u].y;
+        c[u].py = p[u].py; c[u].z = p[u].ph; c[u].pz = p[u].pt;
+      } else {
+        c[u].x = 0; c[u].px = 0; c[u].y = 0; c[u].py = 0; c[u].z = 0; c[u].pz = 0;
       }
-      if (pre) {
-        apply_program(p, sp->pre_next);
+    }
+    if (mom) warp_moments<U>(accw, c, lane);
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (keep[u] && pre) {
+        apply_program(p[u], progs[1]);
         if (rng) {
-          TFrame t = to_tframe(p, gam_n, rad_n, xl);
+          TFrame t = to_tframe(p[u], gam_n, rad_n, xl);
           rmn[0] = fmin(rmn[0], fmin(t.tmpx, t.xt));
           rmx[0] = fmax(rmx[0], fmax(t.tmpx, t.xt));
           rmn[1] = fmin(rmn[1], fmin(t.tmpy, t.yt));
@@ -571,44 +721,37 @@ __global__ void __launch_bounds__(BLOCK) k_advance(AdvanceArgs a) {
           nlive += t.lost ? 0 : 1;
         }
       }
-      if (!finite6(p)) err |= DERR_NONFINITE;
-      nkept++;
-    }
-    // destination slot
-    long long dst = i;
-    if (kick) {
-      const unsigned active = __ballot_sync(0xffffffffu, keep);
-      if (keep) {
-        const unsigned grp = __match_any_sync(active, (unsigned long long)key);
-        const int leader = __ffs(grp) - 1;
-        const int rank = __popc(grp & ((1u << lane) - 1u));
-        int base = 0;
-        if (lane == leader) base = atomicAdd(a.cursor + key, __popc(grp));
-        base = __shfl_sync(grp, base, leader);
-        dst = (long long)base + rank + a.bsum[key >> IMPZ_SCAN_LOG];
-        if (dst < 0 || dst >= a.cap) {  // cannot happen when deposit and pass agree
-          err |= DERR_SLOT;
-          keep = false;
+      if (keep[u]) {
+        if (!finite6(p[u])) err |= DERR_NONFINITE;
+        nkept++;
+      }
+      // destination slot
+      long long dst = i0 + (long long)u * BLOCK;
+      if (kick) {
+        const unsigned active = __ballot_sync(0xffffffffu, keep[u]);
+        if (keep[u]) {
+          const unsigned grp = __match_any_sync(active, (unsigned long long)key[u]);
+          const int leader = __ffs(grp) - 1;
+          const int rank = __popc(grp & ((1u << lane) - 1u));
+          int base = 0;
+          if (lane == leader) base = atomicAdd(a.cursor + key[u], __popc(grp));
+          base = __shfl_sync(grp, base, leader);
+          dst = (long long)base + rank + a.bsum[key[u] >> IMPZ_SCAN_LOG];
+          if (dst < 0 || dst >= a.cap) {  // cannot happen when deposit and pass agree
+            err |= DERR_SLOT;
+            keep[u] = false;
+          }
         }
       }
-    }
-    if (keep) {
-      a.out[0][dst] = p.x; a.out[1][dst] = p.px; a.out[2][dst] = p.y;
-      a.out[3][dst] = p.py; a.out[4][dst] = p.ph; a.out[5][dst] = p.pt;
-      if (a.id_out) a.id_out[dst] = a.id_in[i];
+      if (keep[u]) {
+        a.out[0][dst] = p[u].x; a.out[1][dst] = p[u].px; a.out[2][dst] = p[u].y;
+        a.out[3][dst] = p[u].py; a.out[4][dst] = p[u].ph; a.out[5][dst] = p[u].pt;
+        if (a.id_out) a.id_out[dst] = a.id_in[i0 + (long long)u * BLOCK];
+      }
     }
   }
 
   // ---- block reductions
-  if (mom) {
-#pragma unroll
-    for (int v = 0; v < 37; v++) acc[v] = warp_sum(acc[v]);
-#pragma unroll
-    for (int v = 37; v < IMPZ_RAW_LEN; v++) acc[v] = warp_max(acc[v]);
-    if (lane == 0)
-#pragma unroll
-      for (int v = 0; v < IMPZ_RAW_LEN; v++) red[wid][v] = acc[v];
-  }
   double cnt_l = (double)warp_sum_ll(nlive), cnt_k = (double)warp_sum_ll(nkept);
   double r[6];
 #pragma unroll
@@ -660,7 +803,6 @@ __global__ void __launch_bounds__(BLOCK) k_advance(AdvanceArgs a) {
     }
     a.mom_out[(size_t)row * IMPZ_MOMREC + v] = x;
   }
-  __shared__ double fin[8];
   if (threadIdx.x < 8) {
     const int v = threadIdx.x;
     volatile double* rp = a.rng_part;
@@ -702,17 +844,19 @@ __global__ void __launch_bounds__(BLOCK) k_advance(AdvanceArgs a) {
 // ---------------------------------------------------------------------
 // Charge deposit.  Each block takes chunks of BLOCK*PPT consecutive
 // particles.  Because particles are kept sorted by the previous step's
-// deposit cell, a chunk covers a narrow range of linear cell indices: its
-// charge is accumulated with shared-memory atomics into a tile that covers
-// [base, base+span] (plus the +nx*ny plane of the upper nodes), and the
-// tile's nonzero entries are flushed with one global atomic each.  Chunks
-// too wide for the tile use global atomics directly.  Accumulation is in
-// int64 fixed point (2^-fixbits of a unit macro-particle charge), so the
-// result does not depend on the order of the additions; the eighth corner
-// takes 2^fixbits minus the other seven, so every live particle deposits
-// exactly one unit.
+// deposit cell, a chunk covers a narrow range of linear cell indices and
+// consecutive lanes of a warp usually share a cell: lanes with the same cell
+// first add their eight fixed-point corner charges with warp reductions,
+// then one lane adds the sums into a shared-memory tile that covers the
+// chunk's cells (plus the +nx*ny plane of the upper nodes), and the tile's
+// nonzero entries are flushed with one global atomic each.  Chunks too wide
+// for the tile use global atomics directly.  Accumulation is in int64 fixed
+// point (2^-fixbits of a unit macro-particle charge), so the result does not
+// depend on the order of the additions; the corner with the largest weight
+// takes 2^fixbits minus the other seven (never negative), so every live
+// particle deposits exactly one unit.
 template <int BLOCK, int PPT>
-__global__ void __launch_bounds__(BLOCK) k_deposit(DepositArgs a) {
+__global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned long long* tile = reinterpret_cast<unsigned long long*>(smem_raw);
   int* ctile = reinterpret_cast<int*>(tile + IMPZ_DEP_TILE);
@@ -728,19 +872,21 @@ __global__ void __launch_bounds__(BLOCK) k_deposit(DepositArgs a) {
   const double scale = ldexp(1.0, a.fixbits);
   const long long unit = 1ll << a.fixbits;
   const int LT = IMPZ_DEP_TILE, LB = IMPZ_DEP_TILE / 2;
+  const int lane = threadIdx.x & 31;
   for (int e = threadIdx.x; e < LT; e += BLOCK) {
     tile[e] = 0ull;
     ctile[e] = 0;
   }
   const long long chunk = (long long)BLOCK * PPT;
   for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
-    long long cell[PPT];
+    int cell[PPT];
     double wab[PPT], wcd[PPT], wef[PPT];
     int lmin = INT_MAX, lmax = -1;
 #pragma unroll
     for (int q = 0; q < PPT; q++) {
       const long long i = c0 + (long long)q * BLOCK + threadIdx.x;
       cell[q] = -1;
+      wab[q] = wcd[q] = wef[q] = 0.0;
       if (i < n) {
         Particle p;
         p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
@@ -749,10 +895,10 @@ __global__ void __launch_bounds__(BLOCK) k_deposit(DepositArgs a) {
         if (!t.lost) {
           Cell c = cic_cell(t.xt, t.yt, t.zt, g);
           if (cell_inside(c, nx, ny, nz)) {
-            cell[q] = lin_cell(c, nx, ny);
+            cell[q] = (int)lin_cell(c, nx, ny);
             wab[q] = c.ab; wcd[q] = c.cd; wef[q] = c.ef;
-            lmin = min(lmin, (int)cell[q]);
-            lmax = max(lmax, (int)cell[q]);
+            lmin = min(lmin, cell[q]);
+            lmax = max(lmax, cell[q]);
           } else {
             atomicAdd(a.counts + G, 1);  // live but outside: keeps its sort slot
           }
@@ -767,7 +913,7 @@ __global__ void __launch_bounds__(BLOCK) k_deposit(DepositArgs a) {
       lmin = min(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
       lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
     }
-    if ((threadIdx.x & 31) == 0 && lmax >= 0) {
+    if (lane == 0 && lmax >= 0) {
       atomicMin(&s_min, lmin);
       atomicMax(&s_max, lmax);
     }
@@ -784,39 +930,67 @@ __global__ void __launch_bounds__(BLOCK) k_deposit(DepositArgs a) {
     }
 #pragma unroll
     for (int q = 0; q < PPT; q++) {
-      if (cell[q] < 0) continue;
+      const bool live = cell[q] >= 0;
+      const unsigned active = __ballot_sync(0xffffffffu, live);
+      if (!live) continue;
       const double ab = wab[q], cd = wcd[q], ef = wef[q];
       // weights in the order of deposit_BeamBunch (BeamBunch.f90:3749-3763)
-      const double w7[7] = {ab * cd * ef,
+      const double w8[8] = {ab * cd * ef,
                             ab * (1.0 - cd) * ef,
                             ab * (1.0 - cd) * (1.0 - ef),
                             ab * cd * (1.0 - ef),
                             (1.0 - ab) * cd * (1.0 - ef),
                             (1.0 - ab) * (1.0 - cd) * (1.0 - ef),
-                            (1.0 - ab) * (1.0 - cd) * ef};
-      long long qv[8];
-      long long sum7 = 0;
+                            (1.0 - ab) * (1.0 - cd) * ef,
+                            (1.0 - ab) * cd * ef};
+      int big = 0;
+      double wbig = w8[0];
 #pragma unroll
-      for (int k = 0; k < 7; k++) {
-        qv[k] = __double2ll_rn(w7[k] * scale);
+      for (int k = 1; k < 8; k++)
+        if (w8[k] > wbig) { wbig = w8[k]; big = k; }
+      unsigned long long qv[8];
+      unsigned long long sum7 = 0;
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        qv[k] = (k == big) ? 0ull : (unsigned long long)__double2ll_rn(w8[k] * scale);
         sum7 += qv[k];
       }
-      qv[7] = unit - sum7;
-      const long long c = cell[q];
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+        if (k == big) qv[k] = (unsigned long long)unit - sum7;
+      // lanes with the same cell add their corners first (each quantum is
+      // below 2^41, so 24-bit low and high halves sum exactly in 32 bits)
+      const int c = cell[q];
+      const unsigned grp = __match_any_sync(active, c);
+      const int leader = __ffs(grp) - 1;
+      unsigned long long tot[8];
+      if (__popc(grp) > 1) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const unsigned lo = __reduce_add_sync(grp, (unsigned)(qv[k] & 0xffffffull));
+          const unsigned hi = __reduce_add_sync(grp, (unsigned)(qv[k] >> 24));
+          tot[k] = ((unsigned long long)hi << 24) + (unsigned long long)lo;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; k++) tot[k] = qv[k];
+      }
+      if (lane != leader) continue;
+      const int cnt = __popc(grp);
       const long long node[8] = {c, c + nx, c + nx + P, c + P, c + 1 + P, c + 1 + nx + P,
                                  c + 1 + nx, c + 1};
       if (mode == 0) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) atomicAdd(a.rho + node[k], (unsigned long long)qv[k]);
-        atomicAdd(a.counts + c, 1);
+        for (int k = 0; k < 8; k++) atomicAdd(a.rho + node[k], tot[k]);
+        atomicAdd(a.counts + c, cnt);
       } else {
 #pragma unroll
         for (int k = 0; k < 8; k++) {
           long long o = node[k] - base;
           if (mode == 2 && o >= P) o = o - P + LB;
-          atomicAdd(tile + o, (unsigned long long)qv[k]);
+          atomicAdd(tile + o, tot[k]);
         }
-        atomicAdd(ctile + (c - base), 1);
+        atomicAdd(ctile + (c - base), cnt);
       }
     }
     __syncthreads();

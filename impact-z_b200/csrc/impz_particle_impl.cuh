@@ -10,9 +10,9 @@ static const size_t kDepSmem = IMPZ_DEP_TILE * (sizeof(unsigned long long) + siz
 
 cudaError_t launch_advance(const AdvanceArgs& a, bool f32, int grid, cudaStream_t s) {
   if (f32)
-    k_advance<IMPZ_ADV_BLOCK, true><<<grid, IMPZ_ADV_BLOCK, 0, s>>>(a);
+    k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U><<<grid, IMPZ_ADV_BLOCK, 0, s>>>(a);
   else
-    k_advance<IMPZ_ADV_BLOCK, false><<<grid, IMPZ_ADV_BLOCK, 0, s>>>(a);
+    k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U><<<grid, IMPZ_ADV_BLOCK, 0, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -42,10 +42,10 @@ int max_blocks_advance(bool f32) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (f32)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, true>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U>,
                                                   IMPZ_ADV_BLOCK, 0);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, false>,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U>,
                                                   IMPZ_ADV_BLOCK, 0);
   return sms * (per > 0 ? per : 1);
 }

@@ -92,15 +92,24 @@ cudaError_t launch_green(const PoissonBuffers& b, cudaStream_t s) {
 }
 
 template <typename T>
-cudaError_t launch_convolve(const PoissonBuffers& b, cudaStream_t s) {
+cudaError_t launch_conv_forward(const PoissonBuffers& b, cudaStream_t s) {
   typedef typename Cplx<T>::type C;
   const PoissonDims d = dims_of(b);
   cudaError_t e;
   const size_t sxy = xy_smem<T>(b.nx, b.ny);
   if ((e = allow_smem(k_fft_xy_fwd<T>, sxy)) != cudaSuccess) return e;
-  if ((e = allow_smem(k_fft_xy_inv<T>, sxy)) != cudaSuccess) return e;
   k_fft_xy_fwd<T><<<b.nz, 512, sxy, s>>>(d, b.rho, b.st, b.qscale, (C*)b.spec,
                                          (const C*)b.twx, (const C*)b.twy);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_conv_rest(const PoissonBuffers& b, cudaStream_t s) {
+  typedef typename Cplx<T>::type C;
+  const PoissonDims d = dims_of(b);
+  cudaError_t e;
+  const size_t sxy = xy_smem<T>(b.nx, b.ny);
+  if ((e = allow_smem(k_fft_xy_inv<T>, sxy)) != cudaSuccess) return e;
   const int tk = ztile<T>();
   const size_t sz = z_smem<T>(b.nz);
   dim3 gz((b.nx + 1 + tk - 1) / tk, 2 * b.ny);
@@ -117,6 +126,13 @@ cudaError_t launch_convolve(const PoissonBuffers& b, cudaStream_t s) {
 }
 
 template <typename T>
+cudaError_t launch_convolve(const PoissonBuffers& b, cudaStream_t s) {
+  cudaError_t e = launch_conv_forward<T>(b, s);
+  if (e != cudaSuccess) return e;
+  return launch_conv_rest<T>(b, s);
+}
+
+template <typename T>
 cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s) {
   const long long G = (long long)b.nx * b.ny * b.nz;
   k_efield<T><<<grid_for(G, 256), 256, 0, s>>>(b.nx, b.ny, b.nz, (const T*)b.phi, b.st,
@@ -127,6 +143,10 @@ cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s) {
 template cudaError_t launch_green<double>(const PoissonBuffers&, cudaStream_t);
 template cudaError_t launch_green<float>(const PoissonBuffers&, cudaStream_t);
 template cudaError_t launch_convolve<double>(const PoissonBuffers&, cudaStream_t);
+template cudaError_t launch_conv_forward<double>(const PoissonBuffers&, cudaStream_t);
+template cudaError_t launch_conv_forward<float>(const PoissonBuffers&, cudaStream_t);
+template cudaError_t launch_conv_rest<double>(const PoissonBuffers&, cudaStream_t);
+template cudaError_t launch_conv_rest<float>(const PoissonBuffers&, cudaStream_t);
 template cudaError_t launch_convolve<float>(const PoissonBuffers&, cudaStream_t);
 template cudaError_t launch_efield<double>(const PoissonBuffers&, cudaStream_t);
 template cudaError_t launch_efield<float>(const PoissonBuffers&, cudaStream_t);

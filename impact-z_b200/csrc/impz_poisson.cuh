@@ -53,47 +53,112 @@ __device__ __forceinline__ int bitrev(int v, int logn) {
 // Radix-2 butterflies over `nlines` lines in shared memory; element j of
 // line l sits at buf[l*lstride + j].  tw[k] = exp(-2 pi i k / n), k < n/2.
 // DIF: natural order in, bit-reversed out.  DIT: bit-reversed in, natural out.
+// Up to three consecutive radix-2 stages act on the eight elements spaced by
+// a quarter of the widest span, so each thread runs them in registers (one
+// barrier and one shared-memory round trip per three stages); the
+// butterflies, twiddles and output order are those of plain radix-2.
+template <typename C>
+__device__ __forceinline__ C twid(const C* tw, int idx, int sign) {
+  C w = tw[idx];
+  if (sign > 0) w.y = -w.y;
+  return w;
+}
+
+// stages with half-spans 2^lh, 2^(lh-1), .., 2^(lh-ns+1) (DIF, ns = 1..3)
+template <typename C, int NS>
+__device__ __forceinline__ void dif_group(C* L, int logn, int lh, int k, int sign, const C* tw) {
+  constexpr int E = 1 << NS;
+  const int q = 1 << (lh - NS + 1);  // spacing of the E elements
+  C v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = L[k + e * q];
+#pragma unroll
+  for (int m = 0; m < NS; m++) {
+    const int ls = lh - m;            // this stage's half-span 2^ls
+    const int se = E >> (m + 1);      // local pair distance
+    const int tsh = logn - 1 - ls;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (e & se) continue;
+      const int pos = (k + e * q) & ((1 << ls) - 1);
+      const C w = twid(tw, pos << tsh, sign);
+      const C u = v[e], t = v[e + se];
+      v[e] = cadd(u, t);
+      v[e + se] = cmul(csub(u, t), w);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < E; e++) L[k + e * q] = v[e];
+}
+
+// stages with half-spans 2^lh, .., 2^(lh+ns-1) (DIT)
+template <typename C, int NS>
+__device__ __forceinline__ void dit_group(C* L, int logn, int lh, int k, int sign, const C* tw) {
+  constexpr int E = 1 << NS;
+  const int q = 1 << lh;
+  C v[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) v[e] = L[k + e * q];
+#pragma unroll
+  for (int m = 0; m < NS; m++) {
+    const int ls = lh + m;
+    const int se = 1 << m;
+    const int tsh = logn - 1 - ls;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (e & se) continue;
+      const int pos = (k + e * q) & ((1 << ls) - 1);
+      const C w = twid(tw, pos << tsh, sign);
+      const C u = v[e], t = cmul(v[e + se], w);
+      v[e] = cadd(u, t);
+      v[e + se] = csub(u, t);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < E; e++) L[k + e * q] = v[e];
+}
+
 template <typename C>
 __device__ void fft_dif(C* buf, int logn, int nlines, int lstride, int sign, const C* tw) {
-  const int n = 1 << logn, nh = n >> 1;
-  const int total = nlines * nh;
-  for (int lh = logn - 1; lh >= 0; lh--) {
-    const int half = 1 << lh;
-    const int tsh = logn - 1 - lh;  // twiddle index multiplier log2(n/(2*half))
+  int lh = logn - 1;
+  while (lh >= 0) {
+    const int ns = lh >= 2 ? 3 : lh + 1;
+    const int span = 1 << (lh + 1);          // elements in one group block
+    const int per = 1 << (lh - ns + 1);      // groups per block
+    const int ngl = (1 << logn) >> ns;       // groups per line
+    const int total = nlines * ngl;
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      const int l = b >> (logn - 1), r = b & (nh - 1);
-      const int k = r & (half - 1);
-      const int i0 = ((r >> lh) << (lh + 1)) + k, i1 = i0 + half;
-      C w = tw[k << tsh];
-      if (sign > 0) w.y = -w.y;
-      C* L = buf + l * lstride;
-      C u = L[i0], v = L[i1];
-      L[i0] = cadd(u, v);
-      L[i1] = cmul(csub(u, v), w);
+      const int l = b / ngl, r = b - l * ngl;
+      const int blk = r / per, k = r - blk * per;
+      C* Lp = buf + l * lstride + blk * span;
+      if (ns == 3) dif_group<C, 3>(Lp, logn, lh, k, sign, tw);
+      else if (ns == 2) dif_group<C, 2>(Lp, logn, lh, k, sign, tw);
+      else dif_group<C, 1>(Lp, logn, lh, k, sign, tw);
     }
     __syncthreads();
+    lh -= ns;
   }
 }
 
 template <typename C>
 __device__ void fft_dit(C* buf, int logn, int nlines, int lstride, int sign, const C* tw) {
-  const int n = 1 << logn, nh = n >> 1;
-  const int total = nlines * nh;
-  for (int lh = 0; lh < logn; lh++) {
-    const int half = 1 << lh;
-    const int tsh = logn - 1 - lh;
+  int lh = 0;
+  while (lh < logn) {
+    const int ns = (logn - lh) >= 3 ? 3 : logn - lh;
+    const int span = 1 << (lh + ns);
+    const int per = 1 << lh;
+    const int ngl = (1 << logn) >> ns;
+    const int total = nlines * ngl;
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      const int l = b >> (logn - 1), r = b & (nh - 1);
-      const int k = r & (half - 1);
-      const int i0 = ((r >> lh) << (lh + 1)) + k, i1 = i0 + half;
-      C w = tw[k << tsh];
-      if (sign > 0) w.y = -w.y;
-      C* L = buf + l * lstride;
-      C u = L[i0], v = cmul(L[i1], w);
-      L[i0] = cadd(u, v);
-      L[i1] = csub(u, v);
+      const int l = b / ngl, r = b - l * ngl;
+      const int blk = r / per, k = r - blk * per;
+      C* Lp = buf + l * lstride + blk * span;
+      if (ns == 3) dit_group<C, 3>(Lp, logn, lh, k, sign, tw);
+      else if (ns == 2) dit_group<C, 2>(Lp, logn, lh, k, sign, tw);
+      else dit_group<C, 1>(Lp, logn, lh, k, sign, tw);
     }
     __syncthreads();
+    lh += ns;
   }
 }
 
