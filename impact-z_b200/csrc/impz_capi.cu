@@ -104,6 +104,7 @@ struct impz_bunch_s {
   cudaStream_t stream = nullptr;
   cudaStream_t stream2 = nullptr;   // Green-function build, overlapped with the deposit
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool serial_green = false;
   int form = 0, flags = 0;
   long long cap = 0;
   int nx = 0, ny = 0, nz = 0;
@@ -148,6 +149,11 @@ struct impz_bunch_s {
   CompiledLattice lat;
   bool run_pending = false;
   size_t bytes = 0;
+  // graphs of two space-charge steps, per start parity
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  const StepParams* g_steps[2] = {nullptr, nullptr};
+  const double* g_mom[2] = {nullptr, nullptr};
+  int h_step0 = 0;
   // instrumentation
   bool prof_on = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -282,11 +288,16 @@ int solve_efield(impz_bunch_t b) {
 // function depends only on this step's grid geometry, so it is built on the
 // second stream while the deposit and the forward transforms run.
 int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
-  CK(cudaEventRecord(b->ev_fork, b->stream));
-  CK(cudaStreamWaitEvent(b->stream2, b->ev_fork, 0));
-  int r = solve_green(b, b->stream2);
+  // IMPZ_SERIAL_GREEN=1 keeps the Green build on the main stream (clean
+  // per-kernel timing when profiling)
+  cudaStream_t gs = b->serial_green ? b->stream : b->stream2;
+  if (!b->serial_green) {
+    CK(cudaEventRecord(b->ev_fork, b->stream));
+    CK(cudaStreamWaitEvent(b->stream2, b->ev_fork, 0));
+  }
+  int r = solve_green(b, gs);
   if (r) return r;
-  CK(cudaEventRecord(b->ev_join, b->stream2));
+  if (!b->serial_green) CK(cudaEventRecord(b->ev_join, b->stream2));
   DepositArgs d = deposit_args(b, table, fixed);
   {
     ProfScope ps(b, IMPZ_PROF_DEPOSIT, 1);
@@ -302,7 +313,7 @@ int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
     if (b->f32()) { CK(launch_conv_forward<float>(pb, b->stream)); }
     else { CK(launch_conv_forward<double>(pb, b->stream)); }
   }
-  CK(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
+  if (!b->serial_green) CK(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
   {
     ProfScope ps(b, IMPZ_PROF_CONV, 2);
     if (b->f32()) { CK(launch_conv_rest<float>(pb, b->stream)); }
@@ -374,6 +385,8 @@ void free_bunch(impz_bunch_t b) {
                   b->mom_out, b->mom_fine};
   for (void* p : ptrs) cudaFree(p);
   for (cudaEvent_t e : b->ev_pool) cudaEventDestroy(e);
+  for (int p = 0; p < 2; p++)
+    if (b->gexec[p]) cudaGraphExecDestroy(b->gexec[p]);
   if (b->stream2) cudaStreamSynchronize(b->stream2);
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->ev_join) cudaEventDestroy(b->ev_join);
@@ -431,6 +444,10 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
   cudaGetDevice(&b->device);
   b->form = form;
   b->flags = flags;
+  {
+    const char* sg = std::getenv("IMPZ_SERIAL_GREEN");
+    b->serial_green = sg && sg[0] == '1';
+  }
   b->cap = n;
   b->nx = nx; b->ny = ny; b->nz = nz;
   b->G = (long long)nx * ny * nz;
@@ -892,6 +909,52 @@ int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double cur
 }
 
 // ---- whole-lattice runner --------------------------------------------
+// One step s (read from DevState::step on the device) as direct launches.
+static int launch_step(impz_bunch_t b, bool sc) {
+  if (sc) {
+    int r = field_step(b, b->dsteps, -1);
+    if (r) return r;
+  }
+  AdvanceArgs a = advance_args(b, b->dsteps, -1, sc ? 1 : 0, 1, 1, b->mom_out, 0);
+  CK(launch_adv(b, a));
+  if (sc) b->parity ^= 1;
+  return IMPZ_OK;
+}
+
+// Two space-charge steps captured as one CUDA graph (parity returns to its
+// start value), cached per start parity and re-captured when the step table
+// or the record buffer move.
+static int graph_pair(impz_bunch_t b) {
+  const int p = b->parity;
+  if (b->gexec[p] && (b->g_steps[p] != b->dsteps || b->g_mom[p] != b->mom_out)) {
+    cudaGraphExecDestroy(b->gexec[p]);
+    b->gexec[p] = nullptr;
+  }
+  if (!b->gexec[p]) {
+    cudaGraph_t g = nullptr;
+    const long long counted = g_launches.load();
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int r = launch_step(b, true);
+    if (!r) r = launch_step(b, true);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    g_launches = counted;  // capture recorded the launches without running them
+    if (r) {
+      if (g) cudaGraphDestroy(g);
+      return r;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&b->gexec[p], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    b->g_steps[p] = b->dsteps;
+    b->g_mom[p] = b->mom_out;
+    b->parity = p;  // capture did not execute anything
+  }
+  g_launches += 2 * 12;
+  CK(cudaGraphLaunch(b->gexec[p], b->stream));
+  return IMPZ_OK;
+}
+
 int impz_run_async(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   if (!b || (!elems && nelem > 0) || nelem < 0) return IMPZ_ERR_ARG;
   CK(cudaSetDevice(b->device));
@@ -907,20 +970,29 @@ int impz_run_async(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   if ((r = ensure_mom(b, K + 1))) return r;
   CK(cudaMemcpyAsync(b->dsteps, L.steps.data(), (K + 2) * sizeof(StepParams),
                      cudaMemcpyHostToDevice, b->stream));
-  // prologue: initial record, first half map, first conv1st
+  // the device step counter drives every launch: 0 is the prologue (initial
+  // record, first half map, first conv1st)
+  b->h_step0 = 0;
+  CK(cudaMemcpyAsync(&b->st->step, &b->h_step0, sizeof(int), cudaMemcpyHostToDevice,
+                     b->stream));
   {
-    AdvanceArgs a = advance_args(b, b->dsteps, 0, 0, 1, 1, b->mom_out, 0);
+    AdvanceArgs a = advance_args(b, b->dsteps, -1, 0, 1, 1, b->mom_out, 0);
     CK(launch_adv(b, a));
   }
-  for (int s = 1; s <= K; s++) {
+  // replay two-step graphs over runs of space-charge steps; profiling keeps
+  // direct launches so that every kernel group is bracketed by events
+  int s = 1;
+  while (s <= K) {
     const bool sc = L.steps[s].sc != 0;
-    if (sc) {
-      r = field_step(b, b->dsteps, s);
+    if (!b->prof_on && sc && s + 1 <= K && L.steps[s + 1].sc) {
+      r = graph_pair(b);
       if (r) return r;
+      s += 2;
+    } else {
+      r = launch_step(b, sc);
+      if (r) return r;
+      s += 1;
     }
-    AdvanceArgs a = advance_args(b, b->dsteps, s, sc ? 1 : 0, 1, 1, b->mom_out, s);
-    CK(launch_adv(b, a));
-    if (sc) b->parity ^= 1;
   }
   std::memcpy(b->refptcl, ref, sizeof(ref));
   b->z = z;

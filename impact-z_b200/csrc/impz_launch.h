@@ -13,12 +13,14 @@ namespace impz {
 #ifndef IMPZ_ADV_MINB
 #define IMPZ_ADV_MINB 2
 #endif
-#define IMPZ_DEP_BLOCK 512
+#ifndef IMPZ_DEP_BLOCK
+#define IMPZ_DEP_BLOCK 256
+#endif
 #ifndef IMPZ_DEP_PPT
-#define IMPZ_DEP_PPT 4
+#define IMPZ_DEP_PPT 2
 #endif
 #ifndef IMPZ_DEP_MINB
-#define IMPZ_DEP_MINB 1
+#define IMPZ_DEP_MINB 3
 #endif
 #define IMPZ_SCAN_THREADS 1024
 

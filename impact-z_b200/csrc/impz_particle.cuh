@@ -25,6 +25,10 @@
 
 #include "impz_common.h"
 
+#ifndef IMPZ_FASTMATH
+#define IMPZ_FASTMATH 0
+#endif
+
 #ifndef IMPZ_NS
 #error "define IMPZ_NS (exact or fast) before including impz_particle.cuh"
 #endif
@@ -46,10 +50,19 @@ __device__ __forceinline__ void map_drift(Particle& p, const volatile double* c)
   // BeamBunch.f90:286-295; c = {gam0, beta0, tau, Scxl}
   const double gam0 = c[0], beta0 = c[1], tau = c[2], Scxl = c[3];
   double d = p.pt - gam0;
+#if IMPZ_FASTMATH
+  // one reciprocal square root instead of seven divisions
+  const double rt = rsqrt(((d * d - 1.0) - p.px * p.px) - p.py * p.py);
+  const double ts = tau / Scxl;
+  p.x = p.x + p.px * ts * rt;
+  p.y = p.y + p.py * ts * rt;
+  p.ph = p.ph - (1.0 / beta0 + d * rt) * ts;
+#else
   double tmph = sqrt(((d * d - 1.0) - p.px * p.px) - p.py * p.py);
   p.x = p.x + ((p.px * tau) / tmph) / Scxl;
   p.y = p.y + ((p.py * tau) / tmph) / Scxl;
   p.ph = p.ph - ((1.0 / beta0 + (p.pt - gam0) / tmph) * tau) / Scxl;
+#endif
 }
 
 __device__ __forceinline__ void map_xm6(Particle& p, const volatile double* xm, int mask_lo,
@@ -282,9 +295,15 @@ struct TFrame {
 __device__ __forceinline__ TFrame to_tframe(const Particle& p, double gam, double rad,
                                             double xl) {
   TFrame t;
-  int ntmp5 = (int)(p.ph / kPilc);
-  double tmp5 = __dsub_rn(p.ph, __dmul_rn((double)ntmp5, kPilc));
-  t.ph = __dsub_rn(tmp5, __dmul_rn((double)(ntmp5 % 2), kPilc));
+  if (fabs(p.ph) < kPilc) {
+    // |ph/pilc| < 1 truncates to 0 (the quotient cannot round up to 1), and
+    // tmp5 - 0*pilc is ph itself: the wrap is the identity, no division
+    t.ph = p.ph;
+  } else {
+    int ntmp5 = (int)(p.ph / kPilc);
+    double tmp5 = __dsub_rn(p.ph, __dmul_rn((double)ntmp5, kPilc));
+    t.ph = __dsub_rn(tmp5, __dmul_rn((double)(ntmp5 % 2), kPilc));
+  }
   t.rcp = 1.0 / __dadd_rn(-p.pt, gam);
   t.tmpbet = __dsub_rn(1.0, __dmul_rn(__dmul_rn(t.rcp, t.rcp),
                                       __dadd_rn(__dadd_rn(1.0, __dmul_rn(p.px, p.px)),
@@ -295,8 +314,15 @@ __device__ __forceinline__ TFrame to_tframe(const Particle& p, double gam, doubl
   t.tmpy = __dmul_rn(p.y, xl);
   t.yt = __dmul_rn(__dsub_rn(p.y, __dmul_rn(__dmul_rn(p.py, t.ph), t.rcp)), xl);
   t.zt = -__dmul_rn(__dmul_rn(__dmul_rn(gam, betai), t.ph), xl);
-  double radtest = sqrt(__dadd_rn(__dmul_rn(t.xt, t.xt), __dmul_rn(t.yt, t.yt)));
-  t.lost = (radtest >= rad) || (t.tmpbet <= 0.0);
+  // radtest = sqrt(r2) >= rad; the square root is taken only when r2 lies
+  // within 1e-12 of rad^2 (sqrt is monotone and correctly rounded)
+  const double r2 = __dadd_rn(__dmul_rn(t.xt, t.xt), __dmul_rn(t.yt, t.yt));
+  const double rr = rad * rad;
+  bool out;
+  if (r2 < rr * (1.0 - 4e-12)) out = false;
+  else if (r2 > rr * (1.0 + 4e-12)) out = true;
+  else out = sqrt(r2) >= rad;
+  t.lost = out || (t.tmpbet <= 0.0);
   return t;
 }
 
@@ -516,80 +542,37 @@ __device__ __forceinline__ double moment_value(const Contrib& c, int v) {
   }
 }
 
-// Reduce-scatter eight per-lane values over the warp (9 shuffles); lanes
-// with (lane & 3) == 0 receive the total of value ((lane >> 2) & 7).
-template <bool MAX>
-__device__ __forceinline__ double warp_rs8(const double (&v)[8], int lane) {
-  double w[4], x[2], y;
-  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const double send = b4 ? v[k] : v[k + 4];
-    const double keep = b4 ? v[k + 4] : v[k];
-    const double recv = __shfl_xor_sync(0xffffffffu, send, 16);
-    w[k] = MAX ? fmax(keep, recv) : keep + recv;
-  }
-#pragma unroll
-  for (int k = 0; k < 2; k++) {
-    const double send = b3 ? w[k] : w[k + 2];
-    const double keep = b3 ? w[k + 2] : w[k];
-    const double recv = __shfl_xor_sync(0xffffffffu, send, 8);
-    x[k] = MAX ? fmax(keep, recv) : keep + recv;
-  }
-  {
-    const double send = b2 ? x[0] : x[1];
-    const double keep = b2 ? x[1] : x[0];
-    const double recv = __shfl_xor_sync(0xffffffffu, send, 4);
-    y = MAX ? fmax(keep, recv) : keep + recv;
-  }
-  double t = __shfl_xor_sync(0xffffffffu, y, 2);
-  y = MAX ? fmax(y, t) : y + t;
-  t = __shfl_xor_sync(0xffffffffu, y, 1);
-  y = MAX ? fmax(y, t) : y + t;
-  return y;
-}
-
-// value index a lane owns after warp_rs8 (bit 4 -> 4, bit 3 -> 2, bit 2 -> 1)
-__device__ __forceinline__ int rs8_index(int lane) {
-  return ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-}
-
+// Per-warp reduction of the 37 moment sums by a shared-memory transpose:
+// every lane writes its sums into its row of a 32 x 37 tile, then lane l
+// adds column l (and lanes 0..4 column 32+l) over the 32 rows into its own
+// register accumulators.  Rows have an odd length, so neither the row
+// writes nor the column reads conflict.  The seven maxima stay per lane.
+#define IMPZ_MSUMS 37
 template <int U>
-__device__ __forceinline__ void warp_moments(double* accw, const Contrib (&c)[U], int lane) {
-  // groups: sums 0-7, 8-15, 16-23, 24-31, 32-36 (+3 pad); maxima 37-43 (+1 pad)
+__device__ __forceinline__ void warp_moments(double* tile, const Contrib (&c)[U], int lane,
+                                             double& acc0, double& acc1, double (&mx)[7]) {
+  double* row = tile + lane * IMPZ_MSUMS;
 #pragma unroll
-  for (int g = 0; g < 5; g++) {
-    double v[8];
+  for (int v = 0; v < IMPZ_MSUMS; v++) {
+    double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const int idx = g * 8 + k;
-      double s = 0.0;
-      if (idx < 37) {
-#pragma unroll
-        for (int u = 0; u < U; u++) s = s + moment_value(c[u], idx);
-      }
-      v[k] = s;
-    }
-    const double r = warp_rs8<false>(v, lane);
-    const int idx = g * 8 + rs8_index(lane);
-    if ((lane & 3) == 0 && idx < 37) accw[idx] += r;
+    for (int u = 0; u < U; u++) s = s + moment_value(c[u], v);
+    row[v] = s;
   }
-  {
-    double v[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const int idx = 37 + k;
-      double m = 0.0;
-      if (idx < IMPZ_RAW_LEN) {
+  for (int u = 0; u < U; u++)
 #pragma unroll
-        for (int u = 0; u < U; u++) m = fmax(m, moment_value(c[u], idx));
-      }
-      v[k] = m;
-    }
-    const double r = warp_rs8<true>(v, lane);
-    const int idx = 37 + rs8_index(lane);
-    if ((lane & 3) == 0 && idx < IMPZ_RAW_LEN) accw[idx] = fmax(accw[idx], r);
+    for (int v = 0; v < 7; v++) mx[v] = fmax(mx[v], moment_value(c[u], 37 + v));
+  __syncwarp();
+  double s0 = 0.0, s1 = 0.0;
+#pragma unroll 8
+  for (int r = 0; r < 32; r++) {
+    s0 = s0 + tile[r * IMPZ_MSUMS + lane];
+    if (lane < IMPZ_MSUMS - 32) s1 = s1 + tile[r * IMPZ_MSUMS + 32 + lane];
   }
+  acc0 = acc0 + s0;
+  acc1 = acc1 + s1;
+  __syncwarp();
 }
 
 template <int BLOCK, bool F32, int U>
@@ -599,6 +582,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   __shared__ unsigned int s_last;
   __shared__ double fin[8];
   __shared__ MapProgram progs[2];  // post, pre_next
+  extern __shared__ __align__(16) double mtile_dyn[];  // [BLOCK/32][32*IMPZ_MSUMS]
   __shared__ Geom sgeom;
   DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
@@ -627,9 +611,8 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const long long G = (long long)nx * ny * nz;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double* accw = red[wid];
-  for (int v = lane; v < IMPZ_RAW_LEN; v += 32) accw[v] = 0.0;
-  __syncwarp();
+  double macc0 = 0.0, macc1 = 0.0;
+  double mmax[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
   double rmn[3] = {1e300, 1e300, 1e300}, rmx[3] = {-1e300, -1e300, -1e300};
   long long nlive = 0, nkept = 0;
@@ -667,8 +650,15 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
           // cvbkforth1st (BeamBunch.f90:1681-1699); betai reuses conv1st's
           // tmpbet, the same expression of the same operands
           const double rcp = t.rcp;
+#if IMPZ_FASTMATH
+          const double rb = rsqrt(t.tmpbet);  // 1/betai
+          const double betai = t.tmpbet * rb;
+          const double xkg = -xk / gam;
+          const double ph1 = t.zt * xkg * rb;
+#else
           const double betai = sqrt(t.tmpbet);
           const double ph1 = t.zt * xk / (-(gam * betai));
+#endif
           const double x1 = t.xt * xk + p[u].px * ph1 * rcp;
           const double y1 = t.yt * xk + p[u].py * ph1 * rcp;
           const double xg = x1 * xl, yg = y1 * xl;
@@ -693,7 +683,11 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
           p[u].px = p[u].px + txy * exn;
           p[u].y = yg * xk;
           p[u].py = p[u].py + txy * eyn;
+#if IMPZ_FASTMATH
+          p[u].ph = zg * xkg * rb;
+#else
           p[u].ph = zg * xk / (-(gam * betai));
+#endif
           p[u].pt = p[u].pt - tt * ezn;
         }
       }
@@ -705,7 +699,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
         c[u].x = 0; c[u].px = 0; c[u].y = 0; c[u].py = 0; c[u].z = 0; c[u].pz = 0;
       }
     }
-    if (mom) warp_moments<U>(accw, c, lane);
+    if (mom) warp_moments<U>(mtile_dyn + wid * 32 * IMPZ_MSUMS, c, lane, macc0, macc1, mmax);
 #pragma unroll
     for (int u = 0; u < U; u++) {
       if (keep[u] && pre) {
@@ -752,6 +746,15 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   }
 
   // ---- block reductions
+  if (mom) {
+    red[wid][lane] = macc0;
+    if (lane < IMPZ_MSUMS - 32) red[wid][32 + lane] = macc1;
+#pragma unroll
+    for (int v = 0; v < 7; v++) {
+      const double m = warp_max(mmax[v]);
+      if (lane == 0) red[wid][IMPZ_MSUMS + v] = m;
+    }
+  }
   double cnt_l = (double)warp_sum_ll(nlive), cnt_k = (double)warp_sum_ll(nkept);
   double r[6];
 #pragma unroll
@@ -842,51 +845,45 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
 }
 
 // ---------------------------------------------------------------------
-// Charge deposit.  Each block takes chunks of BLOCK*PPT consecutive
-// particles.  Because particles are kept sorted by the previous step's
-// deposit cell, a chunk covers a narrow range of linear cell indices and
-// consecutive lanes of a warp usually share a cell: lanes with the same cell
-// first add their eight fixed-point corner charges with warp reductions,
-// then one lane adds the sums into a shared-memory tile that covers the
-// chunk's cells (plus the +nx*ny plane of the upper nodes), and the tile's
-// nonzero entries are flushed with one global atomic each.  Chunks too wide
-// for the tile use global atomics directly.  Accumulation is in int64 fixed
-// point (2^-fixbits of a unit macro-particle charge), so the result does not
-// depend on the order of the additions; the corner with the largest weight
-// takes 2^fixbits minus the other seven (never negative), so every live
-// particle deposits exactly one unit.
-template <int BLOCK, int PPT>
+// Charge deposit.  Grid-stride over the particles, U per thread per pass.
+// Particles are kept sorted by the previous step's deposit cell, so the
+// lanes of a warp mostly share a cell: lanes with the same cell add their
+// eight fixed-point corner charges with warp reductions first, and one lane
+// adds the sums to the int64 grid with native 64-bit global reductions.
+// Accumulation is in int64 fixed point (2^-fixbits of a unit macro-particle
+// charge), so the result does not depend on the order of the additions; the
+// corner with the largest weight takes 2^fixbits minus the other seven (never
+// negative), so every live particle deposits exactly one unit.
+template <int BLOCK, int U>
 __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  unsigned long long* tile = reinterpret_cast<unsigned long long*>(smem_raw);
-  int* ctile = reinterpret_cast<int*>(tile + IMPZ_DEP_TILE);
-  __shared__ int s_min, s_max;
   const DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
   const double gam = a.steps[s].gam, rad = a.steps[s].rad;
   const long long n = st->nlocal;
-  const Geom g = st->geom;
+  __shared__ Geom sg;
+  if (threadIdx.x == 0) sg = st->geom;
+  __syncthreads();
+  const volatile Geom& g = sg;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const long long P = (long long)nx * ny;
   const long long G = P * nz;
   const double scale = ldexp(1.0, a.fixbits);
-  const long long unit = 1ll << a.fixbits;
-  const int LT = IMPZ_DEP_TILE, LB = IMPZ_DEP_TILE / 2;
+  const unsigned long long unit = 1ull << a.fixbits;
+  // round-to-nearest-even of w*2^f (exact below 2^51) by the 1.5*2^52 shift
+  const double magic = 6755399441055744.0;
+  const long long magic_bits = 0x4338000000000000ll;
   const int lane = threadIdx.x & 31;
-  for (int e = threadIdx.x; e < LT; e += BLOCK) {
-    tile[e] = 0ull;
-    ctile[e] = 0;
-  }
-  const long long chunk = (long long)BLOCK * PPT;
-  for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
-    int cell[PPT];
-    double wab[PPT], wcd[PPT], wef[PPT];
-    int lmin = INT_MAX, lmax = -1;
+  const long long stride = (long long)gridDim.x * BLOCK * U;
+  const long long nround = (n + stride - 1) / stride * stride;
+  for (long long i0 = (long long)blockIdx.x * BLOCK * U + threadIdx.x; i0 < nround;
+       i0 += stride) {
+    int cell[U];
+    double wab[U], wcd[U], wef[U];
 #pragma unroll
-    for (int q = 0; q < PPT; q++) {
-      const long long i = c0 + (long long)q * BLOCK + threadIdx.x;
-      cell[q] = -1;
-      wab[q] = wcd[q] = wef[q] = 0.0;
+    for (int u = 0; u < U; u++) {
+      const long long i = i0 + (long long)u * BLOCK;
+      cell[u] = -1;
+      wab[u] = wcd[u] = wef[u] = 0.0;
       if (i < n) {
         Particle p;
         p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
@@ -895,45 +892,20 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
         if (!t.lost) {
           Cell c = cic_cell(t.xt, t.yt, t.zt, g);
           if (cell_inside(c, nx, ny, nz)) {
-            cell[q] = (int)lin_cell(c, nx, ny);
-            wab[q] = c.ab; wcd[q] = c.cd; wef[q] = c.ef;
-            lmin = min(lmin, cell[q]);
-            lmax = max(lmax, cell[q]);
+            cell[u] = (int)lin_cell(c, nx, ny);
+            wab[u] = c.ab; wcd[u] = c.cd; wef[u] = c.ef;
           } else {
             atomicAdd(a.counts + G, 1);  // live but outside: keeps its sort slot
           }
         }
       }
     }
-    // block-wide cell range of this chunk
-    if (threadIdx.x == 0) { s_min = INT_MAX; s_max = -1; }
-    __syncthreads();
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      lmin = min(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
-      lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
-    }
-    if (lane == 0 && lmax >= 0) {
-      atomicMin(&s_min, lmin);
-      atomicMax(&s_max, lmax);
-    }
-    __syncthreads();
-    const int base = s_min;
-    const long long span = (long long)s_max - s_min;
-    const long long W = span + nx + 2;
-    // 0: global atomics, 1: contiguous tile, 2: two bands (nodes below and
-    // one x-y plane above the chunk's cells)
-    int mode = 0;
-    if (s_max >= 0) {
-      if (P >= LB && W <= LB) mode = 2;
-      else if (W + P <= LT) mode = 1;
-    }
-#pragma unroll
-    for (int q = 0; q < PPT; q++) {
-      const bool live = cell[q] >= 0;
+    for (int u = 0; u < U; u++) {
+      const bool live = cell[u] >= 0;
       const unsigned active = __ballot_sync(0xffffffffu, live);
       if (!live) continue;
-      const double ab = wab[q], cd = wcd[q], ef = wef[q];
+      const double ab = wab[u], cd = wcd[u], ef = wef[u];
       // weights in the order of deposit_BeamBunch (BeamBunch.f90:3749-3763)
       const double w8[8] = {ab * cd * ef,
                             ab * (1.0 - cd) * ef,
@@ -952,75 +924,33 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
       unsigned long long sum7 = 0;
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        qv[k] = (k == big) ? 0ull : (unsigned long long)__double2ll_rn(w8[k] * scale);
+        const double sh = __dadd_rn(__dmul_rn(w8[k], scale), magic);
+        qv[k] = (k == big) ? 0ull : (unsigned long long)(__double_as_longlong(sh) - magic_bits);
         sum7 += qv[k];
       }
 #pragma unroll
       for (int k = 0; k < 8; k++)
-        if (k == big) qv[k] = (unsigned long long)unit - sum7;
-      // lanes with the same cell add their corners first (each quantum is
-      // below 2^41, so 24-bit low and high halves sum exactly in 32 bits)
-      const int c = cell[q];
+        if (k == big) qv[k] = unit - sum7;
+      // lanes with the same cell add their corners first (each quantum is at
+      // most 2^40, so 24-bit low and high halves of 32 lanes sum in 32 bits)
+      const int c = cell[u];
       const unsigned grp = __match_any_sync(active, c);
-      const int leader = __ffs(grp) - 1;
-      unsigned long long tot[8];
-      if (__popc(grp) > 1) {
+      const int cnt = __popc(grp);
+      if (cnt > 1) {
 #pragma unroll
         for (int k = 0; k < 8; k++) {
           const unsigned lo = __reduce_add_sync(grp, (unsigned)(qv[k] & 0xffffffull));
           const unsigned hi = __reduce_add_sync(grp, (unsigned)(qv[k] >> 24));
-          tot[k] = ((unsigned long long)hi << 24) + (unsigned long long)lo;
+          qv[k] = ((unsigned long long)hi << 24) + (unsigned long long)lo;
         }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 8; k++) tot[k] = qv[k];
       }
-      if (lane != leader) continue;
-      const int cnt = __popc(grp);
+      if (lane != __ffs(grp) - 1) continue;
       const long long node[8] = {c, c + nx, c + nx + P, c + P, c + 1 + P, c + 1 + nx + P,
                                  c + 1 + nx, c + 1};
-      if (mode == 0) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) atomicAdd(a.rho + node[k], tot[k]);
-        atomicAdd(a.counts + c, cnt);
-      } else {
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          long long o = node[k] - base;
-          if (mode == 2 && o >= P) o = o - P + LB;
-          atomicAdd(tile + o, tot[k]);
-        }
-        atomicAdd(ctile + (c - base), cnt);
-      }
+      for (int k = 0; k < 8; k++) atomicAdd(a.rho + node[k], qv[k]);
+      atomicAdd(a.counts + c, cnt);
     }
-    __syncthreads();
-    if (mode != 0) {
-      // flush the touched part of the tile and clear it for the next chunk
-      const long long lenA = (mode == 2) ? W : W + P;
-      for (long long e = threadIdx.x; e < lenA; e += BLOCK) {
-        unsigned long long v = tile[e];
-        if (v) {
-          atomicAdd(a.rho + base + e, v);
-          tile[e] = 0ull;
-        }
-      }
-      if (mode == 2)
-        for (long long e = threadIdx.x; e < W; e += BLOCK) {
-          unsigned long long v = tile[LB + e];
-          if (v) {
-            atomicAdd(a.rho + base + P + e, v);
-            tile[LB + e] = 0ull;
-          }
-        }
-      for (long long e = threadIdx.x; e <= span; e += BLOCK) {
-        int v = ctile[e];
-        if (v) {
-          atomicAdd(a.counts + base + e, v);
-          ctile[e] = 0;
-        }
-      }
-    }
-    __syncthreads();
   }
 }
 

@@ -6,22 +6,29 @@
 namespace impz {
 namespace IMPZ_NS {
 
-static const size_t kDepSmem = IMPZ_DEP_TILE * (sizeof(unsigned long long) + sizeof(int));
+static const size_t kDepSmem = 0;
+
+static const size_t kAdvSmem = (size_t)(IMPZ_ADV_BLOCK / 32) * 32 * 37 * sizeof(double);
+
+template <bool F32>
+static cudaError_t adv_attr() {
+  static cudaError_t once = cudaFuncSetAttribute(
+      k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)kAdvSmem);
+  return once;
+}
 
 cudaError_t launch_advance(const AdvanceArgs& a, bool f32, int grid, cudaStream_t s) {
+  cudaError_t e = f32 ? adv_attr<true>() : adv_attr<false>();
+  if (e != cudaSuccess) return e;
   if (f32)
-    k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U><<<grid, IMPZ_ADV_BLOCK, 0, s>>>(a);
+    k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U><<<grid, IMPZ_ADV_BLOCK, kAdvSmem, s>>>(a);
   else
-    k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U><<<grid, IMPZ_ADV_BLOCK, 0, s>>>(a);
+    k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U><<<grid, IMPZ_ADV_BLOCK, kAdvSmem, s>>>(a);
   return cudaGetLastError();
 }
 
-static cudaError_t dep_attr() {
-  static cudaError_t once = cudaFuncSetAttribute(
-      k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      (int)kDepSmem);
-  return once;
-}
+static cudaError_t dep_attr() { return cudaSuccess; }
 
 cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s) {
   cudaError_t e = dep_attr();
@@ -41,12 +48,15 @@ int max_blocks_advance(bool f32) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (f32)
+  if (f32) {
+    adv_attr<true>();
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U>,
-                                                  IMPZ_ADV_BLOCK, 0);
-  else
+                                                  IMPZ_ADV_BLOCK, kAdvSmem);
+  } else {
+    adv_attr<false>();
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U>,
-                                                  IMPZ_ADV_BLOCK, 0);
+                                                  IMPZ_ADV_BLOCK, kAdvSmem);
+  }
   return sms * (per > 0 ? per : 1);
 }
 

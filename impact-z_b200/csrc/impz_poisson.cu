@@ -22,16 +22,19 @@ static PoissonDims dims_of(const PoissonBuffers& b) {
 template <typename T>
 static size_t xy_smem(int nx, int ny) {
   return sizeof(typename Cplx<T>::type) *
-         ((size_t)(ny / 2) * (2 * nx) + (size_t)(nx + 1) * (2 * ny + 1));
+         ((size_t)(ny / 2) * (2 * nx) + (size_t)(nx + 1) * (2 * ny + 1) + nx + ny);
 }
 template <typename T>
 static int ztile() { return sizeof(T) == 8 ? 8 : 16; }
 template <typename T>
 static size_t z_smem(int nz) {
-  return sizeof(typename Cplx<T>::type) * (size_t)ztile<T>() * (2 * nz + 1);
+  return sizeof(typename Cplx<T>::type) * ((size_t)ztile<T>() * (2 * nz + 1) + nz);
 }
 static const int kDctLines = 16;
-static size_t dct_smem(int n) { return sizeof(double2) * (size_t)(kDctLines / 2) * (2 * n + 1); }
+template <typename T>
+static size_t dct_smem(int n) {
+  return sizeof(typename Cplx<T>::type) * ((size_t)(kDctLines / 2) * (2 * n + 1) + n);
+}
 
 template <typename T>
 size_t poisson_smem_max(int nx, int ny, int nz) {
@@ -39,7 +42,7 @@ size_t poisson_smem_max(int nx, int ny, int nz) {
   m = m > z_smem<T>(nz) ? m : z_smem<T>(nz);
   int nmax = nx > ny ? nx : ny;
   nmax = nmax > nz ? nmax : nz;
-  return m > dct_smem(nmax) ? m : dct_smem(nmax);
+  return m > dct_smem<T>(nmax) ? m : dct_smem<T>(nmax);
 }
 
 template <typename K>
@@ -54,8 +57,13 @@ static int grid_for(long long work, int block) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// The Green function: FP64 corners and 8-corner difference (the difference
+// cancels catastrophically, Field.f90:420-428), then three DCT-I passes in
+// the convolution's type T (FP64 in the plain form, FP32 in the
+// FP32-convolution form, whose first pass converts the FP64 octant).
 template <typename T>
 cudaError_t launch_green(const PoissonBuffers& b, cudaStream_t s) {
+  typedef typename Cplx<T>::type C;
   const int nx = b.nx, ny = b.ny, nz = b.nz;
   const long long nc = (long long)(nx + 2) * (ny + 2) * (nz + 2);
   const long long ng = (long long)(nx + 1) * (ny + 1) * (nz + 1);
@@ -63,30 +71,32 @@ cudaError_t launch_green(const PoissonBuffers& b, cudaStream_t s) {
   k_igf_green<<<grid_for(ng, 256), 256, 0, s>>>(nx, ny, nz, b.F, b.Gt);
   const long long gx = nx + 1, gxy = (long long)(nx + 1) * (ny + 1);
   const double scale = 1.0 / ((double)(2 * nx) * (double)(2 * ny) * (double)(2 * nz));
+  T* work = (T*)b.ghat;
   cudaError_t e;
   // along x: lines j (inner, stride gx) x k (outer); points contiguous
   {
-    size_t sm = dct_smem(nx);
-    if ((e = allow_smem(k_dct1<T, kDctLines>, sm)) != cudaSuccess) return e;
+    auto kern = k_dct1<double, T, T, kDctLines>;
+    const size_t sm = dct_smem<T>(nx);
+    if ((e = allow_smem(kern, sm)) != cudaSuccess) return e;
     dim3 g((ny + 1 + kDctLines - 1) / kDctLines, nz + 1);
-    k_dct1<T, kDctLines><<<g, 256, sm, s>>>(b.Gt, ilog2(2 * nx), 1, gx, ny + 1, gxy,
-                                            (T*)nullptr, 1.0, b.tw64x);
+    kern<<<g, 256, sm, s>>>(b.Gt, work, ilog2(2 * nx), 1, gx, ny + 1, gxy, 1.0, (const C*)b.twx);
   }
   // along y: lines i (inner, stride 1) x k (outer); points stride gx
   {
-    size_t sm = dct_smem(ny);
-    if ((e = allow_smem(k_dct1<T, kDctLines>, sm)) != cudaSuccess) return e;
+    auto kern = k_dct1<T, T, T, kDctLines>;
+    const size_t sm = dct_smem<T>(ny);
+    if ((e = allow_smem(kern, sm)) != cudaSuccess) return e;
     dim3 g((nx + 1 + kDctLines - 1) / kDctLines, nz + 1);
-    k_dct1<T, kDctLines><<<g, 256, sm, s>>>(b.Gt, ilog2(2 * ny), gx, 1, nx + 1, gxy,
-                                            (T*)nullptr, 1.0, b.tw64y);
+    kern<<<g, 256, sm, s>>>(work, work, ilog2(2 * ny), gx, 1, nx + 1, gxy, 1.0, (const C*)b.twy);
   }
-  // along z: lines i (inner) x j (outer, stride gx); points stride gxy; out T
+  // along z: lines i (inner) x j (outer, stride gx); points stride gxy
   {
-    size_t sm = dct_smem(nz);
-    if ((e = allow_smem(k_dct1<T, kDctLines>, sm)) != cudaSuccess) return e;
+    auto kern = k_dct1<T, T, T, kDctLines>;
+    const size_t sm = dct_smem<T>(nz);
+    if ((e = allow_smem(kern, sm)) != cudaSuccess) return e;
     dim3 g((nx + 1 + kDctLines - 1) / kDctLines, ny + 1);
-    k_dct1<T, kDctLines><<<g, 256, sm, s>>>(b.Gt, ilog2(2 * nz), gxy, 1, nx + 1, gx,
-                                            (T*)b.ghat, scale, b.tw64z);
+    kern<<<g, 256, sm, s>>>(work, work, ilog2(2 * nz), gxy, 1, nx + 1, gx, scale,
+                            (const C*)b.twz);
   }
   return cudaGetLastError();
 }

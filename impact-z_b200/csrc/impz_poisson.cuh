@@ -162,6 +162,12 @@ __device__ void fft_dit(C* buf, int logn, int nlines, int lstride, int sign, con
   }
 }
 
+// copies n/2 twiddles into shared memory (whole block, no barrier)
+template <typename C>
+__device__ __forceinline__ void stage_tw(C* dst, const C* __restrict__ src, int n) {
+  for (int e = threadIdx.x; e < n / 2; e += blockDim.x) dst[e] = src[e];
+}
+
 struct PoissonDims {
   int nx, ny, nz;
   int lx, ly, lz;  // log2 of the doubled lengths 2nx, 2ny, 2nz
@@ -182,6 +188,10 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
   const int tp = n2 + 1;  // padded y-line pitch
   C* Z = reinterpret_cast<C*>(smem_raw);
   C* Tm = Z + (ny / 2) * n1;
+  C* twxs = Tm + (nx + 1) * tp;
+  C* twys = twxs + n1 / 2;
+  stage_tw(twxs, twx, n1);
+  stage_tw(twys, twy, n2);
   const int k = blockIdx.x;
   const size_t plane = (size_t)nx * ny * k;
   (void)st;
@@ -202,7 +212,7 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
     Z[l * n1 + j] = z;
   }
   __syncthreads();
-  fft_dif<C>(Z, d.lx, hy, n1, -1, twx);
+  fft_dif<C>(Z, d.lx, hy, n1, -1, twxs);
   // unpack: row a = (Z(k)+conj(Z(n1-k)))/2, row b = (Z(k)-conj(Z(n1-k)))/(2i),
   // k = 0..nx, into y lines Tm[kx][y] (natural y, zero padded to 2ny)
   for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
@@ -225,7 +235,7 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
     Tm[kx * tp + y] = v;
   }
   __syncthreads();
-  fft_dif<C>(Tm, d.ly, nx + 1, tp, -1, twy);
+  fft_dif<C>(Tm, d.ly, nx + 1, tp, -1, twys);
   // store S[k][ky][kx], kx fastest
   C* Sk = S + (size_t)k * n2 * (nx + 1);
   for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
@@ -244,6 +254,8 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
   const int nx = d.nx, ny = d.ny, nz = d.nz, n2 = 2 * ny, n3 = 2 * nz;
   const int lp = n3 + 1;
   C* L = reinterpret_cast<C*>(smem_raw);
+  C* twzs = L + TKX * lp;
+  stage_tw(twzs, twz, n3);
   const int kx0 = blockIdx.x * TKX;
   const int ky = blockIdx.y;
   const int ntk = min(TKX, nx + 1 - kx0);
@@ -257,7 +269,7 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
     L[t * lp + z] = v;
   }
   __syncthreads();
-  fft_dif<C>(L, d.lz, TKX, lp, -1, twz);
+  fft_dif<C>(L, d.lz, TKX, lp, -1, twzs);
   // multiply by G-hat (bit-reversed positions); G-hat octant [kz'][ky'][kx]
   const int kyp = ky <= ny ? ky : n2 - ky;
   const size_t gy = (size_t)(nx + 1), gz = (size_t)(nx + 1) * (ny + 1);
@@ -272,7 +284,7 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
     v.y *= gv;
   }
   __syncthreads();
-  fft_dit<C>(L, d.lz, TKX, lp, +1, twz);
+  fft_dit<C>(L, d.lz, TKX, lp, +1, twzs);
   for (int e = threadIdx.x; e < TKX * nz; e += blockDim.x) {
     const int z = e / TKX, t = e - z * TKX;
     if (t < ntk) base[(size_t)z * pstride + t] = L[t * lp + z];
@@ -292,6 +304,10 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
   const int hy = ny / 2;
   C* Z = reinterpret_cast<C*>(smem_raw);
   C* Tm = Z + hy * n1;
+  C* twxs = Tm + (nx + 1) * tp;
+  C* twys = twxs + n1 / 2;
+  stage_tw(twxs, twx, n1);
+  stage_tw(twys, twy, n2);
   const int k = blockIdx.x;
   const C* Sk = S + (size_t)k * n2 * (nx + 1);
   // y lines in bit-reversed order for the DIT inverse
@@ -300,7 +316,7 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
     Tm[kx * tp + bitrev(ky, d.ly)] = Sk[e];
   }
   __syncthreads();
-  fft_dit<C>(Tm, d.ly, nx + 1, tp, +1, twy);
+  fft_dit<C>(Tm, d.ly, nx + 1, tp, +1, twys);
   // C2R along x for row pairs (y, y+ny/2), y < ny/2: Z(kx) = Xa(kx) + i Xb(kx),
   // with X(n1-kx) = conj(X(kx)); placed bit-reversed for the DIT inverse
   for (int e = threadIdx.x; e < hy * n1; e += blockDim.x) {
@@ -314,7 +330,7 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
     Z[l * n1 + bitrev(kk, d.lx)] = z;
   }
   __syncthreads();
-  fft_dit<C>(Z, d.lx, hy, n1, +1, twx);
+  fft_dit<C>(Z, d.lx, hy, n1, +1, twxs);
   T* ph = phi + (size_t)nx * ny * k;
   for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
     const int y = e / nx, x = e - y * nx;
@@ -370,46 +386,46 @@ __global__ void k_igf_green(int nx, int ny, int nz, const double* __restrict__ F
   }
 }
 
-// DCT-I (transform of the even extension) along one axis of the FP64 octant.
+// DCT-I (transform of the even extension) along one axis of the octant.
 // Lines have n+1 points spaced by `es`; TL lines spaced by `ls` are handled
 // by one block (consecutive inner lines for coalescing), outer lines are
-// spaced by `os`.  Pairs of lines share one complex FFT of length 2n.
-// If out != nullptr the result, times `scale`, is written there as T.
-template <typename T, int TL>
-__global__ void k_dct1(double* __restrict__ g, int logn, long long es, long long ls,
-                       int ninner, long long os, T* __restrict__ out, double scale,
-                       const double2* __restrict__ tw) {
+// spaced by `os`.  Pairs of lines share one complex FFT of length 2n in the
+// compute type CT.  Reads `in` (TI), writes `out` (TO, may alias `in`: each
+// block owns its lines) times `scale`.
+template <typename TI, typename TO, typename CT, int TL>
+__global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long ls, int ninner,
+                       long long os, double scale,
+                       const typename Cplx<CT>::type* __restrict__ tw) {
+  typedef typename Cplx<CT>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double2* L = reinterpret_cast<double2*>(smem_raw);
+  C* L = reinterpret_cast<C*>(smem_raw);
   const int n = 1 << (logn - 1);  // octant points - 1
   const int n2 = 2 * n;
   const int lp = n2 + 1;
+  C* tws = L + (TL / 2) * lp;
+  stage_tw(tws, tw, n2);
   const int l0 = blockIdx.x * TL;
   const int nl = min(TL, ninner - l0);
-  double* base = g + (long long)blockIdx.y * os + (long long)l0 * ls;
+  const long long off = (long long)blockIdx.y * os + (long long)l0 * ls;
+  const TI* ib = in + off;
+  TO* ob = out + off;
   // pair line t with line t + TL/2 (real and imaginary parts)
   const int np = TL / 2;
   for (int e = threadIdx.x; e < np * n2; e += blockDim.x) {
     const int m = e / np, t = e - m * np;  // t fastest for coalescing
     const int mm = m <= n ? m : n2 - m;
-    double2 v;
-    v.x = t < nl ? base[(long long)t * ls + mm * es] : 0.0;
-    v.y = t + np < nl ? base[(long long)(t + np) * ls + mm * es] : 0.0;
+    C v;
+    v.x = t < nl ? (CT)ib[(long long)t * ls + mm * es] : (CT)0;
+    v.y = t + np < nl ? (CT)ib[(long long)(t + np) * ls + mm * es] : (CT)0;
     L[t * lp + m] = v;
   }
   __syncthreads();
-  fft_dif<double2>(L, logn, np, lp, -1, tw);
+  fft_dif<C>(L, logn, np, lp, -1, tws);
   for (int e = threadIdx.x; e < np * (n + 1); e += blockDim.x) {
     const int m = e / np, t = e - m * np;
-    const double2 v = L[t * lp + bitrev(m, logn)];
-    if (out) {
-      T* ob = out + (long long)blockIdx.y * os + (long long)l0 * ls;
-      if (t < nl) ob[(long long)t * ls + m * es] = (T)(v.x * scale);
-      if (t + np < nl) ob[(long long)(t + np) * ls + m * es] = (T)(v.y * scale);
-    } else {
-      if (t < nl) base[(long long)t * ls + m * es] = v.x;
-      if (t + np < nl) base[(long long)(t + np) * ls + m * es] = v.y;
-    }
+    const C v = L[t * lp + bitrev(m, logn)];
+    if (t < nl) ob[(long long)t * ls + m * es] = (TO)((double)v.x * scale);
+    if (t + np < nl) ob[(long long)(t + np) * ls + m * es] = (TO)((double)v.y * scale);
   }
 }
 
