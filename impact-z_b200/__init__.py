@@ -98,6 +98,22 @@ _SIGS = {
     "impz_profile_fetch": (ctypes.c_int, [_B, _D, _LL]),
     "impz_kernel_launches": (ctypes.c_longlong, []),
     "impz_bunch_upload": (ctypes.c_int, [_B, _D, ctypes.c_longlong, ctypes.c_double, _D]),
+    "impz_run_batch": (ctypes.c_int, [ctypes.POINTER(_B), ctypes.POINTER(_E),
+                                      ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "impz_run_begin": (ctypes.c_int, [_B, _E, ctypes.c_int]),
+    "impz_run_advance": (ctypes.c_int, [_B, ctypes.c_int, _I]),
+    "impz_bunch_footprint": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int]),
+    "impz_server_create": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, ctypes.POINTER(_B)]),
+    "impz_server_submit": (ctypes.c_int, [_B, _D, ctypes.c_longlong, ctypes.c_double,
+                                          ctypes.c_double, ctypes.c_double, ctypes.c_double, _D,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          _E, ctypes.c_int, _LL]),
+    "impz_server_wait": (ctypes.c_int, [_B, ctypes.c_longlong, ctypes.c_double, _D, ctypes.c_int,
+                                        _I, _D]),
+    "impz_server_stats": (ctypes.c_int, [_B, _D]),
+    "impz_server_destroy": (ctypes.c_int, [_B]),
 }
 
 PROF_NAMES = ("deposit", "scan", "green", "convolve", "efield", "push")
@@ -180,6 +196,20 @@ def elem_array(elems):
 def count_steps(elems):
     arr = elem_array(elems)
     return lib().impz_count_steps(arr, len(elems))
+
+
+def run_batch(bunches, lattices):
+    """Runs every bunch over its own lattice with interleaved steps; returns
+    [(records, zs)] in bunch order."""
+    nb = len(bunches)
+    arrs = [elem_array(l) for l in lattices]
+    hs = (_B * nb)(*[b.h for b in bunches])
+    ptrs = (_E * nb)(*[ctypes.cast(a, _E) for a in arrs])
+    ns = (ctypes.c_int * nb)(*[len(l) for l in lattices])
+    for b, l, a in zip(bunches, lattices, arrs):
+        b._pending = (a, count_steps(l) + 1)
+    _check(lib().impz_run_batch(hs, ptrs, ns, nb), "impz_run_batch")
+    return [b.run_fetch() for b in bunches]
 
 
 def maplinear(e, zedge, t, tau, refpt, charge, mass, freq):
@@ -343,3 +373,68 @@ class Bunch:
                "impz_run_fetch")
         self._pending = None
         return recs[: nrec.value], zs[: nrec.value]
+
+
+def footprint(n, grid, form=FORM_FP32CONV, track_ids=False, nsteps=0):
+    """Device bytes of a bunch running nsteps steps (the serving loop admits by it)."""
+    nx, ny, nz = grid
+    return int(lib().impz_bunch_footprint(n, nx, ny, nz, form,
+                                          FLAG_TRACK_IDS if track_ids else 0, nsteps))
+
+
+class Server:
+    """The serving loop: submitted jobs share the GPU with continuous batching
+    under an HBM budget (impz_server_*)."""
+
+    def __init__(self, budget_bytes=160e9, max_active=64):
+        h = _B()
+        _check(lib().impz_server_create(budget_bytes, max_active, ctypes.byref(h)),
+               "impz_server_create")
+        self.h = h
+        self._caps = {}
+
+    def submit(self, pts, current, mass, charge, freq, refptcl, grid, lattice,
+               form=FORM_FP32CONV):
+        pts = np.ascontiguousarray(pts, dtype=np.float64)
+        ref = np.ascontiguousarray(refptcl, dtype=np.float64)
+        arr = elem_array(lattice)
+        job = ctypes.c_longlong()
+        nx, ny, nz = grid
+        _check(lib().impz_server_submit(self.h, _dp(pts), pts.shape[0], current, mass, charge,
+                                        freq, _dp(ref), nx, ny, nz, form, arr, len(lattice),
+                                        ctypes.byref(job)), "impz_server_submit")
+        self._caps[job.value] = count_steps(lattice) + 1
+        return job.value
+
+    def wait(self, job, timeout=-1.0):
+        """Returns (records, latency_s, queued_s, measured_bytes) or None if
+        the timeout expired."""
+        cap = self._caps[job]
+        recs = np.zeros((cap, MOMREC))
+        nrec = ctypes.c_int()
+        times = np.zeros(3)
+        rc = lib().impz_server_wait(self.h, job, timeout, _dp(recs), cap, ctypes.byref(nrec),
+                                    _dp(times))
+        if rc == 1:
+            return None
+        _check(rc, "impz_server_wait")
+        del self._caps[job]
+        return recs[: nrec.value], float(times[0]), float(times[1]), int(times[2])
+
+    def stats(self):
+        out = np.zeros(8)
+        _check(lib().impz_server_stats(self.h, _dp(out)), "impz_server_stats")
+        keys = ("completed", "failed", "particle_steps", "span_s", "admitted_bytes",
+                "peak_admitted_bytes", "peak_measured_job_bytes", "queued")
+        return dict(zip(keys, out.tolist()))
+
+    def close(self):
+        if self.h:
+            lib().impz_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

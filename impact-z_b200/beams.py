@@ -129,14 +129,14 @@ def chicane(angle_deg=3.0, lbend=0.2, ldrift_in=20.0, ldrift_mid=1.0, ldrift_c=0
 
 
 # benchmark configurations -------------------------------------------------
-def config0(n=100_000, seed=SEED0):
+def fodo_1e5(n=100_000, seed=SEED0):
     """Proton FODO, 1e5 particles, 32x32x64, 160 steps (plain FP64)."""
     pts, ref = gaussian_bunch(n, seed)
     return dict(pts=pts, refptcl=ref, current=0.030, mass=PROTON_MASS_EV, charge=1.0,
                 freq=402.5e6, grid=(32, 32, 64), lattice=fodo(10))
 
 
-def config1(n=4_000_000, seed=SEED0, periods=25, nseg=10):
+def fodo_4e6(n=4_000_000, seed=SEED0, periods=25, nseg=10):
     """The same beam with 4e6 particles on 64x64x128; 25 FODO periods with
     10 steps per element = 1000 steps."""
     pts, ref = gaussian_bunch(n, seed)
@@ -145,7 +145,7 @@ def config1(n=4_000_000, seed=SEED0, periods=25, nseg=10):
 
 
 def fodo_steps(nsteps, gradient=20.0, ldrift=0.1, lquad=0.1, nseg=10, radius=1.0):
-    """The configs[1] FODO pattern (10 steps per 0.1 m element) cut to exactly
+    """The 4e6-particle FODO pattern (10 steps per 0.1 m element) cut to exactly
     `nsteps` space-charge steps; a final partial element keeps the step length."""
     from . import elem
     pattern = [(0, ldrift, [radius]), (1, lquad, [gradient, 0.0, radius]),
@@ -157,4 +157,50 @@ def fodo_steps(nsteps, gradient=20.0, ldrift=0.1, lquad=0.1, nseg=10, radius=1.0
         out.append(elem(t, length * k / nseg, k, 1, vals))
         left -= k
         i += 1
+    return out
+
+
+def scan_jobs(nbunch=256, seed=SEED0, nmin=1e4, nmax=2e6, steps_periods=25):
+    """A batched parameter scan: independent proton bunches built as in fodo_1e5 with
+    particle counts log-uniform in [nmin, nmax], grids drawn from {16^3,
+    32x32x64, 64x64x128}, quad gradient U[10,30] T/m, current U[5,50] mA,
+    25 FODO periods of 4 steps per element (400 steps).  Returns dicts with
+    the lattice and a `make()` that generates the bunch (seed + index)."""
+    rng = np.random.Generator(np.random.Philox(key=seed + 7777))
+    grids = [(16, 16, 16), (32, 32, 64), (64, 64, 128)]
+    out = []
+    for i in range(nbunch):
+        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        grid = grids[int(rng.integers(0, 3))]
+        grad = float(rng.uniform(10.0, 30.0))
+        cur = float(rng.uniform(0.005, 0.050))
+        out.append(dict(index=i, n=n, grid=grid, gradient=grad, current=cur,
+                        lattice=fodo(steps_periods, gradient=grad), seed=seed + 1000 + i))
+    return out
+
+
+def make_scan_bunch(job):
+    pts, ref = gaussian_bunch(job["n"], seed=job["seed"], current=job["current"])
+    return pts, ref
+
+
+def serve_jobs(njobs, rate, seed=SEED0, nmin=1e4, nmax=4e6, smax=2000):
+    """A served job stream: a Poisson stream of proton jobs (arrival rate `rate`/s),
+    particle counts log-uniform in [nmin, nmax], grid from {32^3, 64^3,
+    64x64x128}, 10-50 FODO periods with gradient U[10,30] T/m, and 100-2000
+    steps (the period count is cut to the drawn step count)."""
+    rng = np.random.Generator(np.random.Philox(key=seed + 9999))
+    grids = [(32, 32, 32), (64, 64, 64), (64, 64, 128)]
+    t = 0.0
+    out = []
+    for i in range(njobs):
+        t += float(rng.exponential(1.0 / rate))
+        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        grid = grids[int(rng.integers(0, 3))]
+        periods = int(rng.integers(10, 51))
+        grad = float(rng.uniform(10.0, 30.0))
+        steps = min(int(rng.integers(100, min(smax, 2000) + 1)), periods * 16)
+        lat = fodo_steps(steps, gradient=grad, nseg=4)
+        out.append(dict(index=i, arrival=t, n=n, grid=grid, gradient=grad, steps=steps,
+                        lattice=lat, seed=seed + 5000 + i))
     return out

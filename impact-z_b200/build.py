@@ -31,6 +31,7 @@ UNITS = [
     ("impz_particle_fast.cu", []),
     ("impz_poisson.cu", ["--fmad=false"]),
     ("impz_capi.cu", []),
+    ("impz_serve.cu", []),
 ]
 HOST_UNITS = ["impz_host.cpp"]
 

@@ -40,14 +40,6 @@ int cuda_fail(cudaError_t e, const char* where) {
     if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
   } while (0)
 
-// device buffers -------------------------------------------------------
-template <typename T>
-cudaError_t dalloc(T** p, size_t count) {
-  *p = nullptr;
-  if (count == 0) count = 1;
-  return cudaMalloc((void**)p, count * sizeof(T));
-}
-
 __global__ void k_aos_to_soa(const double* __restrict__ aos, long long n, double* x, double* px,
                              double* y, double* py, double* ph, double* pt, long long* ids,
                              double qm_ref, double w_ref, unsigned int* bad) {
@@ -60,7 +52,7 @@ __global__ void k_aos_to_soa(const double* __restrict__ aos, long long n, double
   }
 }
 
-__global__ void k_soa_to_aos(double* __restrict__ aos, long long n, const double* x,
+__global__ void k_soa_to_aos(double* __restrict__ aos, long long n, long long i0, const double* x,
                              const double* px, const double* y, const double* py,
                              const double* ph, const double* pt, const long long* ids,
                              double qm, double w) {
@@ -69,16 +61,14 @@ __global__ void k_soa_to_aos(double* __restrict__ aos, long long n, const double
     double* r = aos + 9 * i;
     r[0] = x[i]; r[1] = px[i]; r[2] = y[i]; r[3] = py[i]; r[4] = ph[i]; r[5] = pt[i];
     r[6] = qm; r[7] = w;
-    r[8] = ids ? (double)ids[i] : (double)(i + 1);
+    r[8] = ids ? (double)ids[i] : (double)(i0 + i + 1);
   }
 }
 
-__global__ void k_e4_to_grids(const void* e4, int f32, long long G, double* out) {
+__global__ void k_e4_to_grid(const void* e4, int f32, long long G, int c, double* out) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < G;
-       i += (long long)gridDim.x * blockDim.x) {
-    for (int c = 0; c < 3; c++)
-      out[c * G + i] = f32 ? (double)((const float*)e4)[4 * i + c] : ((const double*)e4)[4 * i + c];
-  }
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = f32 ? (double)((const float*)e4)[4 * i + c] : ((const double*)e4)[4 * i + c];
 }
 
 __global__ void k_to_double(const float* in, long long n, double scale, double* out) {
@@ -93,6 +83,76 @@ int ilog2i(long long n) {
   int l = 0;
   while ((1ll << l) < n) l++;
   return l;
+}
+
+// ---- device memory layout -------------------------------------------
+// Every persistent buffer of a bunch lives in ONE device allocation (the
+// arena), carved at 256-byte boundaries, so the bunch's footprint is known
+// exactly before it is created and creation is a single cudaMalloc.  The
+// run tables (step table + moment records) of a lattice are a second
+// allocation sized by its step count.  Transfers of Pts1 stage through the
+// idle particle buffer set (the one the next push writes), so no call
+// after creation allocates except a run that needs larger tables.
+constexpr size_t kAlign = 256;
+constexpr size_t kGranule = 2u << 20;   // the driver's allocation granule
+constexpr int kMaxAdvGrid = 2048;       // cap on push blocks (partial sums)
+
+size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+struct Layout {
+  size_t pbuf[2][6], ids[2], rho, counts, cursor, bsum, spec, F, Gt, ghat, phi, efield;
+  size_t tw[3], tw64[3], st, dfine, mom_fine, mom_part, rng_part, flag;
+  size_t total;
+  int nscan;
+};
+
+Layout plan_layout(long long n, int nx, int ny, int nz, int form, int flags) {
+  Layout L;
+  std::memset(&L, 0, sizeof(L));
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off += round_up(bytes > 0 ? bytes : 1, kAlign);
+    return o;
+  };
+  const size_t N = (size_t)n;
+  const size_t G = (size_t)nx * ny * nz;
+  const size_t esz = form == IMPZ_FORM_FP32CONV ? sizeof(float) : sizeof(double);
+  // the columns of one parity are adjacent: together they are the staging area
+  for (int p = 0; p < 2; p++)
+    for (int c = 0; c < 6; c++) L.pbuf[p][c] = take(N * sizeof(double));
+  for (int p = 0; p < 2; p++)
+    L.ids[p] = (flags & IMPZ_FLAG_TRACK_IDS) ? take(N * sizeof(long long)) : (size_t)-1;
+  L.rho = take(G * sizeof(unsigned long long));
+  L.counts = take((G + 1) * sizeof(int));
+  L.cursor = take((G + 1) * sizeof(int));
+  L.nscan = (int)((G + 1 + (1u << IMPZ_SCAN_LOG) - 1) >> IMPZ_SCAN_LOG);
+  L.bsum = take((size_t)L.nscan * sizeof(int));
+  L.spec = take((size_t)(nx + 1) * 2 * ny * nz * 2 * esz);
+  L.F = take((size_t)(nx + 2) * (ny + 2) * (nz + 2) * sizeof(double));
+  const size_t noct = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+  L.Gt = take(noct * sizeof(double));
+  L.ghat = take(noct * esz);
+  L.phi = take(G * esz);
+  L.efield = take(4 * G * esz);
+  const int half[3] = {nx, ny, nz};  // a length-2m transform keeps m twiddles
+  for (int d = 0; d < 3; d++) {
+    L.tw64[d] = take((size_t)half[d] * sizeof(double2));
+    L.tw[d] = take((size_t)half[d] * 2 * esz);
+  }
+  L.st = take(sizeof(DevState));
+  L.dfine = take(2 * sizeof(StepParams));
+  L.mom_fine = take(IMPZ_MOMREC * sizeof(double));
+  L.mom_part = take((size_t)kMaxAdvGrid * IMPZ_RAW_LEN * sizeof(double));
+  L.rng_part = take((size_t)kMaxAdvGrid * 8 * sizeof(double));
+  L.flag = take(sizeof(unsigned int));
+  L.total = off;
+  return L;
+}
+
+size_t tables_bytes(int entries, int rows) {
+  return round_up((size_t)entries * sizeof(StepParams), kAlign) +
+         round_up((size_t)rows * IMPZ_MOMREC * sizeof(double), kAlign);
 }
 
 enum Stage { ST_IDLE = 0, ST_PREPARED = 1, ST_DEPOSITED = 2, ST_SOLVED = 3 };
@@ -116,6 +176,10 @@ struct impz_bunch_s {
   double z = 0;
   Consts k;
   int fixbits = 40;
+  char* arena = nullptr;         // every persistent buffer below (plan_layout)
+  char* tables = nullptr;        // dsteps + mom_out of the largest run so far
+  int tables_entries = 0, tables_rows = 0;
+  unsigned int* flag = nullptr;  // scratch word for validity checks
   double* pbuf[2][6] = {{nullptr}};
   long long* ids[2] = {nullptr, nullptr};
   int parity = 0;
@@ -134,12 +198,10 @@ struct impz_bunch_s {
   double2* tw64[3] = {nullptr, nullptr, nullptr};
   DevState* st = nullptr;
   StepParams* dsteps = nullptr;
-  int dsteps_cap = 0;
   StepParams* dfine = nullptr;  // 2-entry table of the per-call surface
   double* mom_part = nullptr;
   double* rng_part = nullptr;
   double* mom_out = nullptr;
-  int mom_cap = 0;
   double* mom_fine = nullptr;
   int grid_adv = 0, grid_dep = 0;
   BendState bend;
@@ -154,6 +216,9 @@ struct impz_bunch_s {
   const StepParams* g_steps[2] = {nullptr, nullptr};
   const double* g_mom[2] = {nullptr, nullptr};
   int h_step0 = 0;
+  int run_next = 0;       // next step of the run in progress
+  double run_z = 0;       // z and refptcl at the end of the run in progress
+  double run_ref[6] = {0};
   // instrumentation
   bool prof_on = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -288,16 +353,17 @@ int solve_efield(impz_bunch_t b) {
 // function depends only on this step's grid geometry, so it is built on the
 // second stream while the deposit and the forward transforms run.
 int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
-  // IMPZ_SERIAL_GREEN=1 keeps the Green build on the main stream (clean
-  // per-kernel timing when profiling)
-  cudaStream_t gs = b->serial_green ? b->stream : b->stream2;
-  if (!b->serial_green) {
+  // The Green build stays on the main stream with IMPZ_SERIAL_GREEN=1 and
+  // while profiling, so the kernel-group intervals are disjoint.
+  const bool serial = b->serial_green || b->prof_on;
+  cudaStream_t gs = serial ? b->stream : b->stream2;
+  if (!serial) {
     CK(cudaEventRecord(b->ev_fork, b->stream));
     CK(cudaStreamWaitEvent(b->stream2, b->ev_fork, 0));
   }
   int r = solve_green(b, gs);
   if (r) return r;
-  if (!b->serial_green) CK(cudaEventRecord(b->ev_join, b->stream2));
+  if (!serial) CK(cudaEventRecord(b->ev_join, b->stream2));
   DepositArgs d = deposit_args(b, table, fixed);
   {
     ProfScope ps(b, IMPZ_PROF_DEPOSIT, 1);
@@ -313,7 +379,7 @@ int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
     if (b->f32()) { CK(launch_conv_forward<float>(pb, b->stream)); }
     else { CK(launch_conv_forward<double>(pb, b->stream)); }
   }
-  if (!b->serial_green) CK(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
+  if (!serial) CK(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
   {
     ProfScope ps(b, IMPZ_PROF_CONV, 2);
     if (b->f32()) { CK(launch_conv_rest<float>(pb, b->stream)); }
@@ -343,22 +409,59 @@ int check_err(impz_bunch_t b) {
   return IMPZ_OK;
 }
 
-int ensure_steps(impz_bunch_t b, int n) {
-  if (n <= b->dsteps_cap) return IMPZ_OK;
-  if (b->dsteps) cudaFree(b->dsteps);
+// step table (entries) and moment records (rows) of a run, one allocation
+int ensure_tables(impz_bunch_t b, int entries, int rows) {
+  if (entries <= b->tables_entries && rows <= b->tables_rows) return IMPZ_OK;
+  entries = std::max(entries, b->tables_entries);
+  rows = std::max(rows, b->tables_rows);
+  if (b->tables) {
+    CK(cudaStreamSynchronize(b->stream));
+    cudaFree(b->tables);
+  }
+  b->tables = nullptr;
   b->dsteps = nullptr;
-  CK(dalloc(&b->dsteps, (size_t)n));
-  b->dsteps_cap = n;
+  b->mom_out = nullptr;
+  b->tables_entries = b->tables_rows = 0;
+  CK(cudaMalloc((void**)&b->tables, tables_bytes(entries, rows)));
+  b->dsteps = (StepParams*)b->tables;
+  b->mom_out = (double*)(b->tables + round_up((size_t)entries * sizeof(StepParams), kAlign));
+  b->tables_entries = entries;
+  b->tables_rows = rows;
   return IMPZ_OK;
 }
 
-int ensure_mom(impz_bunch_t b, int rows) {
-  if (rows <= b->mom_cap) return IMPZ_OK;
-  if (b->mom_out) cudaFree(b->mom_out);
-  b->mom_out = nullptr;
-  CK(dalloc(&b->mom_out, (size_t)rows * IMPZ_MOMREC));
-  b->mom_cap = rows;
-  return IMPZ_OK;
+// Pts1 staging: the parity set the next push overwrites, 6 adjacent columns
+double* staging(impz_bunch_t b, long long* cap_particles) {
+  const int q = 1 - b->parity;
+  const size_t bytes = (size_t)((char*)b->pbuf[q][5] - (char*)b->pbuf[q][0]) +
+                       round_up((size_t)b->cap * sizeof(double), kAlign);
+  *cap_particles = (long long)(bytes / (9 * sizeof(double)));
+  return b->pbuf[q][0];
+}
+
+// Pts1(9,n) host array -> SoA columns of parity 0, through the staging area
+// in chunks; returns IMPZ_ERR_NONUNIFORM when a particle's charge/mass or
+// weight differs from the bunch's.
+int upload_pts(impz_bunch_t b, const double* pts, long long n) {
+  b->parity = 0;
+  long long chunk = 0;
+  double* stg = staging(b, &chunk);
+  CK(cudaMemsetAsync(b->flag, 0, sizeof(unsigned int), b->stream));
+  for (long long i0 = 0; i0 < n; i0 += chunk) {
+    const long long m = std::min(chunk, n - i0);
+    CK(cudaMemcpyAsync(stg, pts + 9 * i0, (size_t)9 * m * sizeof(double),
+                       cudaMemcpyHostToDevice, b->stream));
+    k_aos_to_soa<<<1184, 256, 0, b->stream>>>(
+        stg, m, b->pbuf[0][0] + i0, b->pbuf[0][1] + i0, b->pbuf[0][2] + i0, b->pbuf[0][3] + i0,
+        b->pbuf[0][4] + i0, b->pbuf[0][5] + i0, b->ids[0] ? b->ids[0] + i0 : nullptr,
+        b->sp.qmi, b->weight, b->flag);
+    CK(cudaGetLastError());
+    g_launches += 1;
+  }
+  unsigned int hbad = 0;
+  CK(cudaMemcpyAsync(&hbad, b->flag, sizeof(hbad), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return hbad ? IMPZ_ERR_NONUNIFORM : IMPZ_OK;
 }
 
 template <typename C>
@@ -375,15 +478,9 @@ void free_bunch(impz_bunch_t b) {
   if (!b) return;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
-  for (int p = 0; p < 2; p++) {
-    for (int c = 0; c < 6; c++) cudaFree(b->pbuf[p][c]);
-    cudaFree(b->ids[p]);
-  }
-  void* ptrs[] = {b->rho, b->counts, b->cursor, b->bsum, b->spec, b->F, b->Gt, b->ghat,
-                  b->phi, b->efield, b->tw[0], b->tw[1], b->tw[2], b->tw64[0], b->tw64[1],
-                  b->tw64[2], b->st, b->dsteps, b->dfine, b->mom_part, b->rng_part,
-                  b->mom_out, b->mom_fine};
-  for (void* p : ptrs) cudaFree(p);
+  if (b->stream2) cudaStreamSynchronize(b->stream2);
+  if (b->arena) cudaFree(b->arena);
+  if (b->tables) cudaFree(b->tables);
   for (cudaEvent_t e : b->ev_pool) cudaEventDestroy(e);
   for (int p = 0; p < 2; p++)
     if (b->gexec[p]) cudaGraphExecDestroy(b->gexec[p]);
@@ -484,80 +581,66 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
   ALLOC(cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking));
   ALLOC(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
   ALLOC(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
-  for (int p = 0; p < 2; p++)
-    for (int c = 0; c < 6; c++) ALLOC(dalloc(&b->pbuf[p][c], (size_t)n));
-  if (flags & IMPZ_FLAG_TRACK_IDS) {
-    ALLOC(dalloc(&b->ids[0], (size_t)n));
-    ALLOC(dalloc(&b->ids[1], (size_t)n));
+  const Layout L = plan_layout(n, nx, ny, nz, form, flags);
+  ALLOC(cudaMalloc((void**)&b->arena, L.total));
+  char* base = b->arena;
+  auto at = [&](size_t off) -> void* { return off == (size_t)-1 ? nullptr : (void*)(base + off); };
+  for (int p = 0; p < 2; p++) {
+    for (int c = 0; c < 6; c++) b->pbuf[p][c] = (double*)at(L.pbuf[p][c]);
+    b->ids[p] = (long long*)at(L.ids[p]);
   }
+  b->rho = (unsigned long long*)at(L.rho);
+  b->counts = (int*)at(L.counts);
+  b->cursor = (int*)at(L.cursor);
+  b->bsum = (int*)at(L.bsum);
+  b->nscan = L.nscan;
+  b->spec = at(L.spec);
+  b->F = (double*)at(L.F);
+  b->Gt = (double*)at(L.Gt);
+  b->ghat = at(L.ghat);
+  b->phi = at(L.phi);
+  b->efield = at(L.efield);
+  for (int d = 0; d < 3; d++) {
+    b->tw64[d] = (double2*)at(L.tw64[d]);
+    b->tw[d] = at(L.tw[d]);
+  }
+  b->st = (DevState*)at(L.st);
+  b->dfine = (StepParams*)at(L.dfine);
+  b->mom_fine = (double*)at(L.mom_fine);
+  b->mom_part = (double*)at(L.mom_part);
+  b->rng_part = (double*)at(L.rng_part);
+  b->flag = (unsigned int*)at(L.flag);
   const size_t G = (size_t)b->G;
-  ALLOC(dalloc(&b->rho, G));
+  // the deposit accumulates into rho and counts, which start at zero
   ALLOC(cudaMemsetAsync(b->rho, 0, G * sizeof(unsigned long long), b->stream));
-  ALLOC(dalloc(&b->counts, G + 1));
   ALLOC(cudaMemsetAsync(b->counts, 0, (G + 1) * sizeof(int), b->stream));
-  ALLOC(dalloc(&b->cursor, G + 1));
-  b->nscan = (int)((G + 1 + (1u << IMPZ_SCAN_LOG) - 1) >> IMPZ_SCAN_LOG);
-  ALLOC(dalloc(&b->bsum, (size_t)b->nscan));
-  const size_t esz = b->f32() ? sizeof(float) : sizeof(double);
-  const size_t nspec = (size_t)(nx + 1) * 2 * ny * nz;
-  const size_t noct = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
-  ALLOC(cudaMalloc(&b->spec, nspec * 2 * esz));
-  ALLOC(dalloc(&b->F, (size_t)(nx + 2) * (ny + 2) * (nz + 2)));
-  ALLOC(dalloc(&b->Gt, noct));
-  ALLOC(cudaMalloc(&b->ghat, noct * esz));
-  ALLOC(cudaMalloc(&b->phi, G * esz));
-  ALLOC(cudaMalloc(&b->efield, 4 * G * esz));
   const int lens[3] = {2 * nx, 2 * ny, 2 * nz};
   for (int d = 0; d < 3; d++) {
     std::vector<double2> t64;
     fill_tw(t64, lens[d]);
-    ALLOC(dalloc(&b->tw64[d], t64.size()));
     ALLOC(cudaMemcpy(b->tw64[d], t64.data(), t64.size() * sizeof(double2), cudaMemcpyHostToDevice));
     if (b->f32()) {
       std::vector<float2> t32;
       fill_tw(t32, lens[d]);
-      ALLOC(cudaMalloc(&b->tw[d], t32.size() * sizeof(float2)));
       ALLOC(cudaMemcpy(b->tw[d], t32.data(), t32.size() * sizeof(float2), cudaMemcpyHostToDevice));
     } else {
-      ALLOC(cudaMalloc(&b->tw[d], t64.size() * sizeof(double2)));
       ALLOC(cudaMemcpy(b->tw[d], t64.data(), t64.size() * sizeof(double2), cudaMemcpyHostToDevice));
     }
   }
-  ALLOC(dalloc(&b->st, 1));
-  ALLOC(dalloc(&b->dfine, 2));
-  ALLOC(dalloc(&b->mom_fine, IMPZ_MOMREC));
   b->grid_adv = (int)std::min<long long>((n + IMPZ_ADV_BLOCK - 1) / IMPZ_ADV_BLOCK,
                                          (long long)(b->f32() ? fast::max_blocks_advance(true)
                                                               : exact::max_blocks_advance(false)));
+  b->grid_adv = std::min(b->grid_adv, kMaxAdvGrid);
   b->grid_dep = (int)std::min<long long>(
       (n + (long long)IMPZ_DEP_BLOCK * IMPZ_DEP_PPT - 1) / ((long long)IMPZ_DEP_BLOCK * IMPZ_DEP_PPT),
       (long long)exact::max_blocks_deposit());
   if (b->grid_adv < 1) b->grid_adv = 1;
   if (b->grid_dep < 1) b->grid_dep = 1;
-  ALLOC(dalloc(&b->mom_part, (size_t)b->grid_adv * IMPZ_RAW_LEN));
-  ALLOC(dalloc(&b->rng_part, (size_t)b->grid_adv * 8));
-  // upload Pts1(9,n) and split it into SoA columns
-  {
-    double* aos = nullptr;
-    unsigned int* bad = nullptr;
-    ALLOC(dalloc(&aos, (size_t)9 * n));
-    ALLOC(dalloc(&bad, 1));
-    ALLOC(cudaMemsetAsync(bad, 0, sizeof(unsigned int), b->stream));
-    ALLOC(cudaMemcpyAsync(aos, pts, (size_t)9 * n * sizeof(double), cudaMemcpyHostToDevice,
-                          b->stream));
-    k_aos_to_soa<<<1184, 256, 0, b->stream>>>(aos, n, b->pbuf[0][0], b->pbuf[0][1],
-                                              b->pbuf[0][2], b->pbuf[0][3], b->pbuf[0][4],
-                                              b->pbuf[0][5], b->ids[0], b->sp.qmi, b->weight,
-                                              bad);
-    unsigned int hbad = 0;
-    ALLOC(cudaMemcpyAsync(&hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, b->stream));
-    ALLOC(cudaStreamSynchronize(b->stream));
-    cudaFree(aos);
-    cudaFree(bad);
-    if (hbad) {
-      free_bunch(b);
-      return IMPZ_ERR_NONUNIFORM;
-    }
+  b->bytes = L.total;
+  rc = upload_pts(b, pts, n);
+  if (rc) {
+    free_bunch(b);
+    return rc;
   }
   DevState hs;
   std::memset(&hs, 0, sizeof(hs));
@@ -568,11 +651,18 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
   ALLOC(cudaMemcpyAsync(b->st, &hs, sizeof(hs), cudaMemcpyHostToDevice, b->stream));
   ALLOC(cudaStreamSynchronize(b->stream));
 #undef ALLOC
-  b->bytes = (size_t)n * (12 * sizeof(double) + ((flags & IMPZ_FLAG_TRACK_IDS) ? 16 : 0)) +
-             G * (8 + 4 + 4) + nspec * 2 * esz + noct * (8 + esz) +
-             (size_t)(nx + 2) * (ny + 2) * (nz + 2) * 8 + G * esz * 5;
   *out = b;
   return IMPZ_OK;
+}
+
+long long impz_bunch_footprint(long long n, int nx, int ny, int nz, int form, int flags,
+                               int nsteps) {
+  if (n < 1 || nx < 1 || ny < 1 || nz < 1 || nsteps < 0) return -1;
+  const Layout L = plan_layout(n, nx, ny, nz, form, flags);
+  long long total = (long long)round_up(L.total, kGranule);
+  if (nsteps > 0) total += (long long)round_up(tables_bytes(nsteps + 2, nsteps + 1), kGranule);
+  // graph executables, events and streams of the bunch
+  return total + (long long)kGranule;
 }
 
 int impz_bunch_destroy(impz_bunch_t b) {
@@ -606,17 +696,21 @@ int impz_bunch_download(impz_bunch_t b, double* pts, long long cap, long long* n
   CK(cudaStreamSynchronize(b->stream));
   *n = hs.nlocal;
   if (hs.nlocal > cap) return IMPZ_ERR_ARG;
-  double* aos = nullptr;
-  CK(dalloc(&aos, (size_t)9 * std::max<long long>(hs.nlocal, 1)));
   const int p = b->parity;
-  k_soa_to_aos<<<1184, 256, 0, b->stream>>>(aos, hs.nlocal, b->pbuf[p][0], b->pbuf[p][1],
-                                            b->pbuf[p][2], b->pbuf[p][3], b->pbuf[p][4],
-                                            b->pbuf[p][5], b->ids[p], b->sp.qmi, b->weight);
-  cudaError_t e = cudaMemcpyAsync(pts, aos, (size_t)9 * hs.nlocal * sizeof(double),
-                                  cudaMemcpyDeviceToHost, b->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-  cudaFree(aos);
-  if (e != cudaSuccess) return cuda_fail(e, "download");
+  long long chunk = 0;
+  double* stg = staging(b, &chunk);
+  for (long long i0 = 0; i0 < hs.nlocal; i0 += chunk) {
+    const long long m = std::min(chunk, hs.nlocal - i0);
+    k_soa_to_aos<<<1184, 256, 0, b->stream>>>(
+        stg, m, i0, b->pbuf[p][0] + i0, b->pbuf[p][1] + i0, b->pbuf[p][2] + i0,
+        b->pbuf[p][3] + i0, b->pbuf[p][4] + i0, b->pbuf[p][5] + i0,
+        b->ids[p] ? b->ids[p] + i0 : nullptr, b->sp.qmi, b->weight);
+    CK(cudaGetLastError());
+    g_launches += 1;
+    CK(cudaMemcpyAsync(pts + 9 * i0, stg, (size_t)9 * m * sizeof(double), cudaMemcpyDeviceToHost,
+                       b->stream));
+  }
+  CK(cudaStreamSynchronize(b->stream));
   return IMPZ_OK;
 }
 
@@ -756,12 +850,12 @@ int impz_poisson_open(impz_bunch_t b, double* phi) {
   if (r) return r;
   if (phi) {
     if (b->f32()) {
-      double* tmp = nullptr;
-      CK(dalloc(&tmp, (size_t)b->G));
+      // the spectrum is free once phi is out; it holds 16 G bytes in this form
+      double* tmp = (double*)b->spec;
       k_to_double<<<1184, 256, 0, b->stream>>>((const float*)b->phi, b->G, b->weight, tmp);
+      g_launches += 1;
       CK(cudaMemcpyAsync(phi, tmp, b->G * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
       CK(cudaStreamSynchronize(b->stream));
-      cudaFree(tmp);
     } else {
       CK(cudaMemcpyAsync(phi, b->phi, b->G * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     }
@@ -778,12 +872,15 @@ int impz_kick(impz_bunch_t b, double tau, double* egrid) {
   int r = solve_efield(b);
   if (r) return r;
   if (egrid) {
-    double* tmp = nullptr;
-    CK(dalloc(&tmp, (size_t)3 * b->G));
-    k_e4_to_grids<<<1184, 256, 0, b->stream>>>(b->efield, b->f32() ? 1 : 0, b->G, tmp);
-    CK(cudaMemcpyAsync(egrid, tmp, 3 * b->G * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    // one component at a time through the (now free) spectrum, >= 16 G bytes
+    double* tmp = (double*)b->spec;
+    for (int c = 0; c < 3; c++) {
+      k_e4_to_grid<<<1184, 256, 0, b->stream>>>(b->efield, b->f32() ? 1 : 0, b->G, c, tmp);
+      g_launches += 1;
+      CK(cudaMemcpyAsync(egrid + c * b->G, tmp, b->G * sizeof(double), cudaMemcpyDeviceToHost,
+                         b->stream));
+    }
     CK(cudaStreamSynchronize(b->stream));
-    cudaFree(tmp);
     if (b->f32())
       for (long long i = 0; i < 3 * b->G; i++) egrid[i] *= b->weight;
   }
@@ -875,17 +972,7 @@ int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double cur
   if (!b || !pts || !refptcl || n < 1 || n > b->cap) return IMPZ_ERR_ARG;
   if (pts[6] != b->sp.qmi || pts[7] != b->weight) return IMPZ_ERR_NONUNIFORM;
   CK(cudaSetDevice(b->device));
-  double* aos = nullptr;
-  unsigned int* bad = nullptr;
-  CK(dalloc(&aos, (size_t)9 * n));
-  CK(dalloc(&bad, 1));
-  CK(cudaMemsetAsync(bad, 0, sizeof(unsigned int), b->stream));
-  CK(cudaMemcpyAsync(aos, pts, (size_t)9 * n * sizeof(double), cudaMemcpyHostToDevice, b->stream));
-  b->parity = 0;
-  k_aos_to_soa<<<1184, 256, 0, b->stream>>>(aos, n, b->pbuf[0][0], b->pbuf[0][1], b->pbuf[0][2],
-                                            b->pbuf[0][3], b->pbuf[0][4], b->pbuf[0][5],
-                                            b->ids[0], b->sp.qmi, b->weight, bad);
-  g_launches += 1;
+  const int rc = upload_pts(b, pts, n);
   DevState hs;
   std::memset(&hs, 0, sizeof(hs));
   hs.current = current;
@@ -893,12 +980,8 @@ int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double cur
   hs.nlocal = n;
   hs.nlive = n;
   CK(cudaMemcpyAsync(b->st, &hs, sizeof(hs), cudaMemcpyHostToDevice, b->stream));
-  unsigned int hbad = 0;
-  CK(cudaMemcpyAsync(&hbad, bad, sizeof(hbad), cudaMemcpyDeviceToHost, b->stream));
   CK(cudaStreamSynchronize(b->stream));
-  cudaFree(aos);
-  cudaFree(bad);
-  if (hbad) return IMPZ_ERR_NONUNIFORM;
+  if (rc) return rc;
   b->current0 = current;
   std::memcpy(b->refptcl, refptcl, sizeof(b->refptcl));
   b->z = 0.0;
@@ -955,19 +1038,21 @@ static int graph_pair(impz_bunch_t b) {
   return IMPZ_OK;
 }
 
-int impz_run_async(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
-  if (!b || (!elems && nelem > 0) || nelem < 0) return IMPZ_ERR_ARG;
+// A run in three parts so that many bunches can be interleaved: begin
+// compiles the lattice, uploads the step table and launches the prologue;
+// advance launches up to `budget` further steps; the run is complete when
+// every step is launched.
+static int run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   CK(cudaSetDevice(b->device));
+  b->run_pending = false;
   CompiledLattice& L = b->lat;
-  double z = b->z;
-  double ref[6];
-  std::memcpy(ref, b->refptcl, sizeof(ref));
+  b->run_z = b->z;
+  std::memcpy(b->run_ref, b->refptcl, sizeof(b->run_ref));
   // conv1st/kick see Bcurr, the input beam current (AccSimulator.f90:1121)
-  int r = compile_lattice(b->P, elems, nelem, b->current0, b->sp, ref, &z, L);
+  int r = compile_lattice(b->P, elems, nelem, b->current0, b->sp, b->run_ref, &b->run_z, L);
   if (r) return r;
   const int K = L.nsteps;
-  if ((r = ensure_steps(b, K + 2))) return r;
-  if ((r = ensure_mom(b, K + 1))) return r;
+  if ((r = ensure_tables(b, K + 2, K + 1))) return r;
   CK(cudaMemcpyAsync(b->dsteps, L.steps.data(), (K + 2) * sizeof(StepParams),
                      cudaMemcpyHostToDevice, b->stream));
   // the device step counter drives every launch: 0 is the prologue (initial
@@ -975,28 +1060,91 @@ int impz_run_async(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   b->h_step0 = 0;
   CK(cudaMemcpyAsync(&b->st->step, &b->h_step0, sizeof(int), cudaMemcpyHostToDevice,
                      b->stream));
-  {
-    AdvanceArgs a = advance_args(b, b->dsteps, -1, 0, 1, 1, b->mom_out, 0);
-    CK(launch_adv(b, a));
-  }
-  // replay two-step graphs over runs of space-charge steps; profiling keeps
-  // direct launches so that every kernel group is bracketed by events
-  int s = 1;
-  while (s <= K) {
+  AdvanceArgs a = advance_args(b, b->dsteps, -1, 0, 1, 1, b->mom_out, 0);
+  CK(launch_adv(b, a));
+  b->run_next = 1;
+  return IMPZ_OK;
+}
+
+// Launches up to `budget` steps (at least one).  Two-step graphs replay runs
+// of space-charge steps; profiling keeps direct launches so that every
+// kernel group is bracketed by events.
+static int run_advance(impz_bunch_t b, int budget) {
+  CompiledLattice& L = b->lat;
+  const int K = L.nsteps;
+  int done = 0;
+  while (b->run_next <= K && (done == 0 || done < budget)) {
+    const int s = b->run_next;
     const bool sc = L.steps[s].sc != 0;
+    int r;
     if (!b->prof_on && sc && s + 1 <= K && L.steps[s + 1].sc) {
       r = graph_pair(b);
-      if (r) return r;
-      s += 2;
+      b->run_next += 2;
+      done += 2;
     } else {
       r = launch_step(b, sc);
+      b->run_next += 1;
+      done += 1;
+    }
+    if (r) return r;
+  }
+  return IMPZ_OK;
+}
+
+static void run_end(impz_bunch_t b) {
+  std::memcpy(b->refptcl, b->run_ref, sizeof(b->run_ref));
+  b->z = b->run_z;
+  b->run_pending = true;
+}
+
+int impz_run_async(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
+  if (!b || (!elems && nelem > 0) || nelem < 0) return IMPZ_ERR_ARG;
+  int r = run_begin(b, elems, nelem);
+  if (r) return r;
+  r = run_advance(b, b->lat.nsteps);
+  if (r) return r;
+  run_end(b);
+  return IMPZ_OK;
+}
+
+int impz_run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
+  if (!b || (!elems && nelem > 0) || nelem < 0) return IMPZ_ERR_ARG;
+  return run_begin(b, elems, nelem);
+}
+
+int impz_run_advance(impz_bunch_t b, int budget, int* remaining) {
+  if (!b) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  int r = run_advance(b, budget);
+  if (remaining) *remaining = std::max(0, b->lat.nsteps + 1 - b->run_next);
+  if (!r && b->run_next > b->lat.nsteps && !b->run_pending) run_end(b);
+  return r;
+}
+
+int impz_run_batch(impz_bunch_t* bunches, const impz_elem_t* const* lattices,
+                   const int* nelem, int nb) {
+  if (!bunches || !lattices || !nelem || nb < 0) return IMPZ_ERR_ARG;
+  for (int i = 0; i < nb; i++)
+    if (!bunches[i] || (!lattices[i] && nelem[i] > 0) || nelem[i] < 0) return IMPZ_ERR_ARG;
+  for (int i = 0; i < nb; i++) {
+    int r = run_begin(bunches[i], lattices[i], nelem[i]);
+    if (r) return r;
+  }
+  // round robin, two steps per bunch per turn, so that every bunch's
+  // stream holds work and small bunches fill the gaps of large ones
+  bool left = true;
+  while (left) {
+    left = false;
+    for (int i = 0; i < nb; i++) {
+      impz_bunch_t b = bunches[i];
+      if (b->run_next > b->lat.nsteps) continue;
+      CK(cudaSetDevice(b->device));
+      int r = run_advance(b, 2);
       if (r) return r;
-      s += 1;
+      left = left || b->run_next <= b->lat.nsteps;
     }
   }
-  std::memcpy(b->refptcl, ref, sizeof(ref));
-  b->z = z;
-  b->run_pending = true;
+  for (int i = 0; i < nb; i++) run_end(bunches[i]);
   return IMPZ_OK;
 }
 

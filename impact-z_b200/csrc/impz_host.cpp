@@ -269,6 +269,25 @@ MapOp blank(MapKind k) {
 }
 
 MapOp op_xm6(const double xm[36]) {
+  // block-diagonal maps (every maplinear_* of the path) use the 12-entry op
+  bool diag = true;
+  for (int j = 0; j < 6 && diag; j++)
+    for (int k = 0; k < 6; k++)
+      if (xm[j + 6 * k] != 0.0 && (j / 2) != (k / 2)) {
+        diag = false;
+        break;
+      }
+  if (diag) {
+    MapOp op = blank(MAP_XM2);
+    for (int b = 0; b < 3; b++) {
+      const int r = 2 * b;
+      op.c[4 * b + 0] = xm[r + 6 * r];
+      op.c[4 * b + 1] = xm[r + 6 * (r + 1)];
+      op.c[4 * b + 2] = xm[(r + 1) + 6 * r];
+      op.c[4 * b + 3] = xm[(r + 1) + 6 * (r + 1)];
+    }
+    return op;
+  }
   MapOp op = blank(MAP_XM6);
   unsigned long long mask = 0;
   for (int q = 0; q < 36; q++) {

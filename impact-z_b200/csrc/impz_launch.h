@@ -10,17 +10,20 @@ namespace impz {
 #ifndef IMPZ_ADV_U
 #define IMPZ_ADV_U 1
 #endif
+#ifndef IMPZ_ADV_PREFETCH
+#define IMPZ_ADV_PREFETCH 0
+#endif
 #ifndef IMPZ_ADV_MINB
 #define IMPZ_ADV_MINB 2
 #endif
 #ifndef IMPZ_DEP_BLOCK
-#define IMPZ_DEP_BLOCK 256
+#define IMPZ_DEP_BLOCK 512
 #endif
 #ifndef IMPZ_DEP_PPT
-#define IMPZ_DEP_PPT 2
+#define IMPZ_DEP_PPT 4
 #endif
 #ifndef IMPZ_DEP_MINB
-#define IMPZ_DEP_MINB 3
+#define IMPZ_DEP_MINB 2
 #endif
 #define IMPZ_SCAN_THREADS 1024
 

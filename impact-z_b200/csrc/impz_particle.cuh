@@ -84,6 +84,20 @@ __device__ __forceinline__ void map_xm6(Particle& p, const volatile double* xm, 
   p.x = out[0]; p.px = out[1]; p.y = out[2]; p.py = out[3]; p.ph = out[4]; p.pt = out[5];
 }
 
+// the same loop when xm is block diagonal (drift, quadrupole and RF-gap
+// linear maps, xm_from_y in the host builder): row j sums its two nonzero
+// entries from 0.0 in column order, exactly as the full loop does.
+// c = {xm11, xm12, xm21, xm22, xm33, xm34, xm43, xm44, xm55, xm56, xm65, xm66}
+__device__ __forceinline__ void map_xm2(Particle& p, const volatile double* c) {
+  const double x = p.x, px = p.px, y = p.y, py = p.py, z = p.ph, pz = p.pt;
+  p.x = (0.0 + x * c[0]) + px * c[1];
+  p.px = (0.0 + x * c[2]) + px * c[3];
+  p.y = (0.0 + y * c[4]) + py * c[5];
+  p.py = (0.0 + y * c[6]) + py * c[7];
+  p.ph = (0.0 + z * c[8]) + pz * c[9];
+  p.pt = (0.0 + z * c[10]) + pz * c[11];
+}
+
 __device__ __forceinline__ void map_kquad(Particle& p, const volatile double* c) {
   // Quadrupole.f90:526-600; c = {refpt6, gambet0, beta0, qmass, K, tau, Scxl, qmi}
   const double refpt6 = c[0], gambet0 = c[1], beta0 = c[2], qmass = c[3], K = c[4];
@@ -266,6 +280,7 @@ __device__ __forceinline__ void apply_program(Particle& p, const volatile MapPro
       case MAP_FPOL: map_pole<false>(p, op.c); break;
       case MAP_BPOL: map_pole<true>(p, op.c); break;
       case MAP_SECTOR: map_sector(p, op.c); break;
+      case MAP_XM2: map_xm2(p, op.c); break;
       default: break;
     }
   }
@@ -620,23 +635,42 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
 
   const long long stride = (long long)gridDim.x * BLOCK * U;
   const long long nround = (n + stride - 1) / stride * stride;
+  // the next pass's particles are loaded while this pass computes (each
+  // thread reads its own slots only; in-place launches write slot i back)
+  Particle nxt[U];
+  auto fetch = [&](long long ib) {
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const long long i = ib + (long long)u * BLOCK;
+      if (i < n) {
+        nxt[u].x = a.in[0][i]; nxt[u].px = a.in[1][i]; nxt[u].y = a.in[2][i];
+        nxt[u].py = a.in[3][i]; nxt[u].ph = a.in[4][i]; nxt[u].pt = a.in[5][i];
+      } else {
+        nxt[u].x = 0; nxt[u].px = 0; nxt[u].y = 0; nxt[u].py = 0; nxt[u].ph = 0; nxt[u].pt = 0;
+      }
+    }
+  };
+#if IMPZ_ADV_PREFETCH
+  fetch((long long)blockIdx.x * BLOCK * U + threadIdx.x);
+#endif
   for (long long i0 = (long long)blockIdx.x * BLOCK * U + threadIdx.x; i0 < nround;
        i0 += stride) {
     Particle p[U];
     bool keep[U];
     long long key[U];
+#if !IMPZ_ADV_PREFETCH
+    fetch(i0);
+#endif
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const long long i = i0 + (long long)u * BLOCK;
       keep[u] = i < n;
       key[u] = 0;
-      if (keep[u]) {
-        p[u].x = a.in[0][i]; p[u].px = a.in[1][i]; p[u].y = a.in[2][i];
-        p[u].py = a.in[3][i]; p[u].ph = a.in[4][i]; p[u].pt = a.in[5][i];
-      } else {
-        p[u].x = 0; p[u].px = 0; p[u].y = 0; p[u].py = 0; p[u].ph = 0; p[u].pt = 0;
-      }
+      p[u] = nxt[u];
     }
+#if IMPZ_ADV_PREFETCH
+    if (i0 + stride < nround) fetch(i0 + stride);
+#endif
     Contrib c[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
@@ -845,23 +879,42 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
 }
 
 // ---------------------------------------------------------------------
-// Charge deposit.  Grid-stride over the particles, U per thread per pass.
-// Particles are kept sorted by the previous step's deposit cell, so the
-// lanes of a warp mostly share a cell: lanes with the same cell add their
-// eight fixed-point corner charges with warp reductions first, and one lane
-// adds the sums to the int64 grid with native 64-bit global reductions.
-// Accumulation is in int64 fixed point (2^-fixbits of a unit macro-particle
-// charge), so the result does not depend on the order of the additions; the
-// corner with the largest weight takes 2^fixbits minus the other seven (never
-// negative), so every live particle deposits exactly one unit.
+// Charge deposit.  Each block takes chunks of BLOCK*U consecutive particles.
+// Particles are kept sorted by the previous step's deposit cell, so a chunk
+// covers a narrow range of linear cell indices: its charge is accumulated in
+// a shared-memory tile over that range (a contiguous window, or two bands one
+// x-y plane apart holding the lower and upper nodes), and every touched node
+// is flushed with one 64-bit global reduction.  Lanes of a warp that share a
+// cell first add their corners with warp reductions, and only the group's
+// first lane adds to the tile.  The tile keeps each node's fixed-point sum as
+// two 32-bit halves (low 20 bits and the rest) so that native 32-bit shared
+// atomics suffice: a chunk of at most 2048 particles cannot overflow either
+// half (2048 low halves stay below 2^31, the high halves below 2^31).  Chunks too wide for the tile reduce straight
+// into the grid.  Accumulation is in int64 fixed point (2^-fixbits of a unit
+// macro-particle charge), so the result does not depend on the order of the
+// additions; the corner with the largest weight takes 2^fixbits minus the
+// other seven (never negative), so every live particle deposits exactly one
+// unit.
+#define IMPZ_DEP_LOBITS 20
 template <int BLOCK, int U>
 __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a) {
+  static_assert(BLOCK * U <= 2048, "tile halves sized for chunks of at most 2048 particles");
+  extern __shared__ __align__(16) unsigned int tsm[];
+  unsigned int* tlo = tsm;                      // [IMPZ_DEP_TILE]
+  unsigned int* thi = tsm + IMPZ_DEP_TILE;      // [IMPZ_DEP_TILE]
+  unsigned int* tcnt = tsm + 2 * IMPZ_DEP_TILE; // [IMPZ_DEP_TILE]
+  __shared__ int s_min, s_max;
+  __shared__ Geom sg;
   const DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
   const double gam = a.steps[s].gam, rad = a.steps[s].rad;
   const long long n = st->nlocal;
-  __shared__ Geom sg;
   if (threadIdx.x == 0) sg = st->geom;
+  for (int e = threadIdx.x; e < IMPZ_DEP_TILE; e += BLOCK) {
+    tlo[e] = 0u;
+    thi[e] = 0u;
+    tcnt[e] = 0u;
+  }
   __syncthreads();
   const volatile Geom& g = sg;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
@@ -872,16 +925,16 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
   // round-to-nearest-even of w*2^f (exact below 2^51) by the 1.5*2^52 shift
   const double magic = 6755399441055744.0;
   const long long magic_bits = 0x4338000000000000ll;
-  const int lane = threadIdx.x & 31;
-  const long long stride = (long long)gridDim.x * BLOCK * U;
-  const long long nround = (n + stride - 1) / stride * stride;
-  for (long long i0 = (long long)blockIdx.x * BLOCK * U + threadIdx.x; i0 < nround;
-       i0 += stride) {
+  const unsigned lomask = (1u << IMPZ_DEP_LOBITS) - 1u;
+  const int LT = IMPZ_DEP_TILE, LB = IMPZ_DEP_TILE / 2;
+  const long long chunk = (long long)BLOCK * U;
+  for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
     int cell[U];
     double wab[U], wcd[U], wef[U];
+    int lmin = INT_MAX, lmax = -1;
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      const long long i = i0 + (long long)u * BLOCK;
+      const long long i = c0 + (long long)u * BLOCK + threadIdx.x;
       cell[u] = -1;
       wab[u] = wcd[u] = wef[u] = 0.0;
       if (i < n) {
@@ -894,17 +947,39 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
           if (cell_inside(c, nx, ny, nz)) {
             cell[u] = (int)lin_cell(c, nx, ny);
             wab[u] = c.ab; wcd[u] = c.cd; wef[u] = c.ef;
+            lmin = min(lmin, cell[u]);
+            lmax = max(lmax, cell[u]);
           } else {
             atomicAdd(a.counts + G, 1);  // live but outside: keeps its sort slot
           }
         }
       }
     }
+    if (threadIdx.x == 0) { s_min = INT_MAX; s_max = -1; }
+    __syncthreads();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lmin = min(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+      lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    }
+    if ((threadIdx.x & 31) == 0 && lmax >= 0) {
+      atomicMin(&s_min, lmin);
+      atomicMax(&s_max, lmax);
+    }
+    __syncthreads();
+    const int base = s_min;
+    const long long span = (long long)s_max - s_min;
+    const long long W = span + nx + 2;
+    // 0: straight into the grid, 1: contiguous window, 2: two bands
+    int mode = 0;
+    if (s_max >= 0) {
+      if (P >= LB && W <= LB) mode = 2;
+      else if (W + P <= LT) mode = 1;
+    }
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      const bool live = cell[u] >= 0;
-      const unsigned active = __ballot_sync(0xffffffffu, live);
-      if (!live) continue;
+      const unsigned active = __ballot_sync(0xffffffffu, cell[u] >= 0);
+      if (cell[u] < 0) continue;
       const double ab = wab[u], cd = wcd[u], ef = wef[u];
       // weights in the order of deposit_BeamBunch (BeamBunch.f90:3749-3763)
       const double w8[8] = {ab * cd * ef,
@@ -932,9 +1007,11 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
       for (int k = 0; k < 8; k++)
         if (k == big) qv[k] = unit - sum7;
       // lanes with the same cell add their corners first (each quantum is at
-      // most 2^40, so 24-bit low and high halves of 32 lanes sum in 32 bits)
-      const int c = cell[u];
-      const unsigned grp = __match_any_sync(active, c);
+      // most 2^40, so 24-bit low and high halves of 32 lanes sum in 32 bits);
+      // only the group's first lane touches the tile or the grid, so shared
+      // atomics of one instruction never collide
+      const int cc = cell[u];
+      const unsigned grp = __match_any_sync(active, cc);
       const int cnt = __popc(grp);
       if (cnt > 1) {
 #pragma unroll
@@ -944,13 +1021,57 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
           qv[k] = ((unsigned long long)hi << 24) + (unsigned long long)lo;
         }
       }
-      if (lane != __ffs(grp) - 1) continue;
+      if ((threadIdx.x & 31) != __ffs(grp) - 1) continue;
+      const long long c = cc;
       const long long node[8] = {c, c + nx, c + nx + P, c + P, c + 1 + P, c + 1 + nx + P,
                                  c + 1 + nx, c + 1};
+      if (mode == 0) {
 #pragma unroll
-      for (int k = 0; k < 8; k++) atomicAdd(a.rho + node[k], qv[k]);
-      atomicAdd(a.counts + c, cnt);
+        for (int k = 0; k < 8; k++) atomicAdd(a.rho + node[k], qv[k]);
+        atomicAdd(a.counts + c, cnt);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          long long o = node[k] - base;
+          if (mode == 2 && o >= P) o = o - P + LB;
+          atomicAdd(tlo + o, (unsigned)(qv[k] & lomask));
+          atomicAdd(thi + o, (unsigned)(qv[k] >> IMPZ_DEP_LOBITS));
+        }
+        atomicAdd(tcnt + (c - base), (unsigned)cnt);
+      }
     }
+    __syncthreads();
+    if (mode != 0) {
+      // flush the touched part of the tile and clear it for the next chunk
+      const long long lenA = (mode == 2) ? W : W + P;
+      for (long long e = threadIdx.x; e < lenA; e += BLOCK) {
+        const unsigned lo = tlo[e], hi = thi[e];
+        if (lo | hi) {
+          atomicAdd(a.rho + base + e,
+                    ((unsigned long long)hi << IMPZ_DEP_LOBITS) + (unsigned long long)lo);
+          tlo[e] = 0u;
+          thi[e] = 0u;
+        }
+      }
+      if (mode == 2)
+        for (long long e = threadIdx.x; e < W; e += BLOCK) {
+          const unsigned lo = tlo[LB + e], hi = thi[LB + e];
+          if (lo | hi) {
+            atomicAdd(a.rho + base + P + e,
+                      ((unsigned long long)hi << IMPZ_DEP_LOBITS) + (unsigned long long)lo);
+            tlo[LB + e] = 0u;
+            thi[LB + e] = 0u;
+          }
+        }
+      for (long long e = threadIdx.x; e <= span; e += BLOCK) {
+        const unsigned v = tcnt[e];
+        if (v) {
+          atomicAdd(a.counts + base + e, (int)v);
+          tcnt[e] = 0u;
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 

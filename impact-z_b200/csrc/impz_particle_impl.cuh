@@ -6,7 +6,7 @@
 namespace impz {
 namespace IMPZ_NS {
 
-static const size_t kDepSmem = 0;
+static const size_t kDepSmem = (size_t)3 * IMPZ_DEP_TILE * sizeof(unsigned int);
 
 static const size_t kAdvSmem = (size_t)(IMPZ_ADV_BLOCK / 32) * 32 * 37 * sizeof(double);
 
@@ -28,7 +28,12 @@ cudaError_t launch_advance(const AdvanceArgs& a, bool f32, int grid, cudaStream_
   return cudaGetLastError();
 }
 
-static cudaError_t dep_attr() { return cudaSuccess; }
+static cudaError_t dep_attr() {
+  static cudaError_t once = cudaFuncSetAttribute(
+      k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)kDepSmem);
+  return once;
+}
 
 cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s) {
   cudaError_t e = dep_attr();

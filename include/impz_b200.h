@@ -85,6 +85,13 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
  * IMPZ_FLAG_TRACK_IDS column 9 is filled with 1..n in the current order. */
 int impz_bunch_download(impz_bunch_t b, double* pts, long long cap, long long* n);
 int impz_bunch_destroy(impz_bunch_t b);
+/* Device bytes a bunch of n particles on an nx*ny*nz grid holds while it runs
+ * a lattice of nsteps steps (0: the bunch alone), at the driver's 2 MiB
+ * allocation granularity: the bunch is one allocation, the run tables a
+ * second, and no other call allocates.  The serving loop admits by it.
+ * No reference counterpart (the reference allocates per process). */
+long long impz_bunch_footprint(long long n, int nx, int ny, int nz, int form, int flags,
+                               int nsteps);
 /* Current, Npt, Nptlocal, refptcl(1..6), z, device bytes (11 doubles). */
 int impz_bunch_info(impz_bunch_t b, double info[11]);
 /* The bunch's CUDA stream (cudaStream_t) for callers that interleave work. */
@@ -144,6 +151,18 @@ int impz_run(impz_bunch_t b, const impz_elem_t* elems, int nelem, double* recs, 
  * are fetched by impz_run_fetch); lets one host thread drive many bunches. */
 int impz_run_async(impz_bunch_t b, const impz_elem_t* elems, int nelem);
 int impz_run_fetch(impz_bunch_t b, double* recs, double* zs, int maxrec, int* nrec);
+/* impz_run_async in parts, for callers that interleave many bunches:
+ * begin compiles the lattice and enqueues the prologue; each advance enqueues
+ * up to `budget` further steps (at least one) and reports how many remain;
+ * once none remain the records can be fetched with impz_run_fetch. */
+int impz_run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem);
+int impz_run_advance(impz_bunch_t b, int budget, int* remaining);
+/* Runs nb bunches, each over its own lattice, with their steps interleaved
+ * two at a time on the bunches' own streams so that their kernels overlap on
+ * the device (batched scans).  Returns once everything is enqueued; fetch
+ * each bunch's records with impz_run_fetch. */
+int impz_run_batch(impz_bunch_t* bunches, const impz_elem_t* const* lattices,
+                   const int* nelem, int nb);
 /* Number of steps (records - 1) impz_run would take for this lattice. */
 int impz_count_steps(const impz_elem_t* elems, int nelem);
 
@@ -156,7 +175,9 @@ int impz_count_steps(const impz_elem_t* elems, int nelem);
 #define IMPZ_PROF_EFIELD 4   /* finite-difference field */
 #define IMPZ_PROF_PUSH 5     /* fused gather/kick/map/moments/range/sort pass */
 #define IMPZ_PROF_NCAT 6
-/* When on, CUDA events bracket every kernel group on the bunch's stream. */
+/* When on, CUDA events bracket every kernel group on the bunch's stream;
+ * runs launch directly (no graph replay) and the Green build runs on the
+ * bunch's stream, so the groups' intervals are disjoint. */
 int impz_profile_enable(impz_bunch_t b, int on);
 /* Synchronizes; accumulated milliseconds and launches per group since enable. */
 int impz_profile_fetch(impz_bunch_t b, double ms[IMPZ_PROF_NCAT],
@@ -168,6 +189,30 @@ long long impz_kernel_launches(void);
  * `current` and the bunch's reference particle to refptcl. */
 int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double current,
                       const double refptcl[6]);
+
+/* ---- serving loop ------------------------------------------------------- */
+/* Jobs (a bunch plus its lattice) submitted over time share the GPU: a worker
+ * thread admits them in arrival order as soon as their footprint fits the
+ * HBM budget and one of max_active slots is free, keeps each job's state
+ * resident in HBM, and advances all running jobs a few steps at a time round
+ * robin so that their kernels overlap (continuous batching). */
+typedef struct impz_server_s* impz_server_t;
+int impz_server_create(double hbm_budget_bytes, int max_active, impz_server_t* out);
+/* Copies the inputs and queues the job; *job receives its id. */
+int impz_server_submit(impz_server_t s, const double* pts, long long n, double current,
+                       double mass, double charge, double freq, const double refptcl[6],
+                       int nx, int ny, int nz, int form, const impz_elem_t* elems, int nelem,
+                       long long* job);
+/* Waits up to timeout_s (< 0: forever; returns 1 if still running) for the
+ * job; copies its records (as impz_run) and times[3] = latency from submit
+ * to completion [s], time queued [s], measured device bytes. */
+int impz_server_wait(impz_server_t s, long long job, double timeout_s, double* recs, int maxrec,
+                     int* nrec, double times[3]);
+/* completed, failed, particle-steps done, seconds from first submit to last
+ * completion, bytes admitted now, peak admitted, peak measured per job, queued. */
+int impz_server_stats(impz_server_t s, double out[8]);
+/* Finishes the queued and running jobs, then stops the worker. */
+int impz_server_destroy(impz_server_t s);
 
 /* Host-side maps (for checking and for callers that keep their own loop):
  * maplinear_Quadrupole (Quadrupole.f90:120-252) and maplinear_CCL

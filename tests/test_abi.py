@@ -93,3 +93,19 @@ def test_diag_row_matches_oracle_bitwise():
 def test_count_steps():
     assert impz.count_steps(beams.fodo(10)) == 160
     assert impz.count_steps(beams.fodo(25, nseg=10)) == 1000
+
+
+def test_footprint_is_exact_arena_plus_tables():
+    mib2 = 2 << 20
+    grid = (64, 64, 128)
+    f0 = impz.footprint(4_000_000, grid)
+    # particles (two parity sets of six FP64 columns) dominate; granule-rounded
+    assert f0 % mib2 == 0
+    assert f0 >= 4_000_000 * 96 + 64 * 64 * 128 * 16
+    assert impz.footprint(4_000_000, grid, track_ids=True) >= f0 + 4_000_000 * 16
+    # the FP32 form holds smaller spectra than the FP64 form
+    assert impz.footprint(4_000_000, grid, form=impz.FORM_FP64) > f0
+    # a run's tables add to the bunch alone
+    assert impz.footprint(4_000_000, grid, nsteps=1000) > f0
+    assert impz.lib().impz_bunch_footprint(0, 64, 64, 128, 1, 0, 0) == -1
+    assert impz.lib().impz_bunch_footprint(10, 64, 64, 128, 1, 0, -1) == -1

@@ -84,7 +84,7 @@ def gpu_step(pts, cfg, e_first, tau, piperad, form=impz.FORM_FP64):
 
 @pytest.fixture(scope="module")
 def small():
-    cfg = beams.config0(n=20_000, seed=beams.SEED0 + 7)
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 7)
     return cfg
 
 
@@ -182,7 +182,7 @@ def gpu_rows(cfg, form):
 
 
 def test_full_lattice_fp64_moments():
-    cfg = beams.config0(n=20_000, seed=beams.SEED0 + 11)
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 11)
     cfg["lattice"] = beams.fodo(2)  # 32 steps
     rows_o, p_o, beam = orc.run(cfg["lattice"], cfg["pts"], cfg["current"], cfg["mass"],
                                 cfg["charge"], cfg["freq"], cfg["refptcl"], cfg["grid"])
@@ -196,7 +196,7 @@ def test_full_lattice_fp64_moments():
 
 
 def test_full_lattice_fp32conv_moments():
-    cfg = beams.config0(n=20_000, seed=beams.SEED0 + 11)
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 11)
     cfg["lattice"] = beams.fodo(2)
     rows_o, p_o, beam = orc.run(cfg["lattice"], cfg["pts"], cfg["current"], cfg["mass"],
                                 cfg["charge"], cfg["freq"], cfg["refptcl"], cfg["grid"])

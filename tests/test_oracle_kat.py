@@ -189,7 +189,7 @@ def test_gaussian_moments_match_sigma():
 
 
 def test_full_lattice_runs_and_conserves_particles():
-    cfg = beams.config0(n=3000)
+    cfg = beams.fodo_1e5(n=3000)
     cfg["lattice"] = beams.fodo(1)
     rows, p, beam = orc.run(cfg["lattice"], cfg["pts"], cfg["current"], cfg["mass"],
                             cfg["charge"], cfg["freq"], cfg["refptcl"], cfg["grid"])
