@@ -141,6 +141,8 @@ struct DepositArgs {
 };
 
 #define IMPZ_SCAN_LOG 13      // 8192 cells per scan block
-#define IMPZ_DEP_TILE 8192    // deposit tile: int64 entries (64 KB) + int32 counts (32 KB)
+#ifndef IMPZ_DEP_TILE
+#define IMPZ_DEP_TILE 8192    // deposit tile entries: two int32 halves + an int32 count (96 KB)
+#endif
 
 }  // namespace impz

@@ -880,30 +880,37 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
 
 // ---------------------------------------------------------------------
 // Charge deposit.  Each block takes chunks of BLOCK*U consecutive particles.
-// Particles are kept sorted by the previous step's deposit cell, so a chunk
-// covers a narrow range of linear cell indices: its charge is accumulated in
-// a shared-memory tile over that range (a contiguous window, or two bands one
-// x-y plane apart holding the lower and upper nodes), and every touched node
-// is flushed with one 64-bit global reduction.  Lanes of a warp that share a
-// cell first add their corners with warp reductions, and only the group's
-// first lane adds to the tile.  The tile keeps each node's fixed-point sum as
-// two 32-bit halves (low 20 bits and the rest) so that native 32-bit shared
-// atomics suffice: a chunk of at most 2048 particles cannot overflow either
-// half (2048 low halves stay below 2^31, the high halves below 2^31).  Chunks too wide for the tile reduce straight
-// into the grid.  Accumulation is in int64 fixed point (2^-fixbits of a unit
-// macro-particle charge), so the result does not depend on the order of the
-// additions; the corner with the largest weight takes 2^fixbits minus the
-// other seven (never negative), so every live particle deposits exactly one
-// unit.
+// Particles are kept sorted by the previous step's deposit cell, so after the
+// grid is refitted a chunk still covers a small box of cells, give or take
+// one cell per axis.  Its charge is accumulated in a shared-memory tile over
+// that box (the chunk's min..max+1 in each of x, y, z) and every touched node
+// is flushed with one 64-bit global reduction; chunks whose box exceeds the
+// tile (the sparse tails) reduce straight into the grid.  Sorted particles
+// put many lanes of a warp on the same cell, where shared atomics serialize,
+// so the tile holds R copies of the box (R = tile / box, at most 32) and
+// lane l adds to copy l % R; the copies sit 1 mod 32 words apart so the same
+// node of different copies falls in different banks, and the flush adds the
+// copies.  Small boxes (the dense core) thus get many copies, large boxes
+// (sparse regions, few lanes per cell) few.  Each tile word keeps a node's
+// fixed-point sum as two 32-bit halves (the low 20 bits and the rest) so
+// that native 32-bit shared atomics suffice: a chunk of at most 2048
+// particles cannot overflow either half.  Accumulation is in int64 fixed
+// point (2^-fixbits of a unit macro-particle charge), so the result does not
+// depend on the order of the additions; the corner with the largest weight
+// takes 2^fixbits minus the other seven (never negative), so every live
+// particle deposits exactly one unit.
+#ifndef IMPZ_DEP_RMAX
+#define IMPZ_DEP_RMAX 32
+#endif
 #define IMPZ_DEP_LOBITS 20
 template <int BLOCK, int U>
 __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a) {
   static_assert(BLOCK * U <= 2048, "tile halves sized for chunks of at most 2048 particles");
   extern __shared__ __align__(16) unsigned int tsm[];
-  unsigned int* tlo = tsm;                      // [IMPZ_DEP_TILE]
-  unsigned int* thi = tsm + IMPZ_DEP_TILE;      // [IMPZ_DEP_TILE]
-  unsigned int* tcnt = tsm + 2 * IMPZ_DEP_TILE; // [IMPZ_DEP_TILE]
-  __shared__ int s_min, s_max;
+  unsigned int* tlo = tsm;                       // [IMPZ_DEP_TILE]
+  unsigned int* thi = tsm + IMPZ_DEP_TILE;       // [IMPZ_DEP_TILE]
+  unsigned int* tcnt = tsm + 2 * IMPZ_DEP_TILE;  // [IMPZ_DEP_TILE]
+  __shared__ int s_box[6];
   __shared__ Geom sg;
   const DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
@@ -926,16 +933,18 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
   const double magic = 6755399441055744.0;
   const long long magic_bits = 0x4338000000000000ll;
   const unsigned lomask = (1u << IMPZ_DEP_LOBITS) - 1u;
-  const int LT = IMPZ_DEP_TILE, LB = IMPZ_DEP_TILE / 2;
   const long long chunk = (long long)BLOCK * U;
+  const int lane = threadIdx.x & 31;
   for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
     int cell[U];
+    unsigned pk[U];  // x | y << 10 | z << 20 (nx, ny <= 64, nz <= 4096)
     double wab[U], wcd[U], wef[U];
-    int lmin = INT_MAX, lmax = -1;
+    int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {-1, -1, -1};
 #pragma unroll
     for (int u = 0; u < U; u++) {
       const long long i = c0 + (long long)u * BLOCK + threadIdx.x;
       cell[u] = -1;
+      pk[u] = 0u;
       wab[u] = wcd[u] = wef[u] = 0.0;
       if (i < n) {
         Particle p;
@@ -946,39 +955,46 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
           Cell c = cic_cell(t.xt, t.yt, t.zt, g);
           if (cell_inside(c, nx, ny, nz)) {
             cell[u] = (int)lin_cell(c, nx, ny);
+            pk[u] = (unsigned)(c.ix - 1) | ((unsigned)(c.jx - 1) << 10) |
+                    ((unsigned)(c.kx - 1) << 20);
             wab[u] = c.ab; wcd[u] = c.cd; wef[u] = c.ef;
-            lmin = min(lmin, cell[u]);
-            lmax = max(lmax, cell[u]);
+            mn[0] = min(mn[0], c.ix - 1); mx[0] = max(mx[0], c.ix - 1);
+            mn[1] = min(mn[1], c.jx - 1); mx[1] = max(mx[1], c.jx - 1);
+            mn[2] = min(mn[2], c.kx - 1); mx[2] = max(mx[2], c.kx - 1);
           } else {
             atomicAdd(a.counts + G, 1);  // live but outside: keeps its sort slot
           }
         }
       }
     }
-    if (threadIdx.x == 0) { s_min = INT_MAX; s_max = -1; }
+    if (threadIdx.x < 3) { s_box[threadIdx.x] = INT_MAX; s_box[3 + threadIdx.x] = -1; }
     __syncthreads();
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      lmin = min(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
-      lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    for (int d = 0; d < 3; d++) {
+      mn[d] = __reduce_min_sync(0xffffffffu, mn[d]);
+      mx[d] = __reduce_max_sync(0xffffffffu, mx[d]);
     }
-    if ((threadIdx.x & 31) == 0 && lmax >= 0) {
-      atomicMin(&s_min, lmin);
-      atomicMax(&s_max, lmax);
+    if (lane == 0 && mx[0] >= 0) {
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        atomicMin(&s_box[d], mn[d]);
+        atomicMax(&s_box[3 + d], mx[d]);
+      }
     }
     __syncthreads();
-    const int base = s_min;
-    const long long span = (long long)s_max - s_min;
-    const long long W = span + nx + 2;
-    // 0: straight into the grid, 1: contiguous window, 2: two bands
-    int mode = 0;
-    if (s_max >= 0) {
-      if (P >= LB && W <= LB) mode = 2;
-      else if (W + P <= LT) mode = 1;
-    }
+    // the box of nodes: lower cell corners min..max, plus one
+    const bool any = s_box[3] >= 0;
+    const int x0 = any ? s_box[0] : 0, y0 = any ? s_box[1] : 0, z0 = any ? s_box[2] : 0;
+    const int bx = any ? s_box[3] - x0 + 2 : 0, by = any ? s_box[4] - y0 + 2 : 0;
+    const int bz = any ? s_box[5] - z0 + 2 : 0;
+    const long long V = (long long)bx * by * bz;
+    const int S = (int)(((V + 31) & ~31ll) + 1);  // copy stride, 1 mod 32
+    const bool tiled = any && V + 32 <= IMPZ_DEP_TILE;
+    const int R = tiled ? min(IMPZ_DEP_RMAX, IMPZ_DEP_TILE / S) : 1;
+    const int mycopy = (lane % R) * S;
+    const int bxy = bx * by;
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      const unsigned active = __ballot_sync(0xffffffffu, cell[u] >= 0);
       if (cell[u] < 0) continue;
       const double ab = wab[u], cd = wcd[u], ef = wef[u];
       // weights in the order of deposit_BeamBunch (BeamBunch.f90:3749-3763)
@@ -1006,68 +1022,49 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
 #pragma unroll
       for (int k = 0; k < 8; k++)
         if (k == big) qv[k] = unit - sum7;
-      // lanes with the same cell add their corners first (each quantum is at
-      // most 2^40, so 24-bit low and high halves of 32 lanes sum in 32 bits);
-      // only the group's first lane touches the tile or the grid, so shared
-      // atomics of one instruction never collide
-      const int cc = cell[u];
-      const unsigned grp = __match_any_sync(active, cc);
-      const int cnt = __popc(grp);
-      if (cnt > 1) {
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const unsigned lo = __reduce_add_sync(grp, (unsigned)(qv[k] & 0xffffffull));
-          const unsigned hi = __reduce_add_sync(grp, (unsigned)(qv[k] >> 24));
-          qv[k] = ((unsigned long long)hi << 24) + (unsigned long long)lo;
-        }
-      }
-      if ((threadIdx.x & 31) != __ffs(grp) - 1) continue;
-      const long long c = cc;
-      const long long node[8] = {c, c + nx, c + nx + P, c + P, c + 1 + P, c + 1 + nx + P,
-                                 c + 1 + nx, c + 1};
-      if (mode == 0) {
+      if (!tiled) {
+        const long long c = cell[u];
+        const long long node[8] = {c, c + nx, c + nx + P, c + P, c + 1 + P, c + 1 + nx + P,
+                                   c + 1 + nx, c + 1};
 #pragma unroll
         for (int k = 0; k < 8; k++) atomicAdd(a.rho + node[k], qv[k]);
-        atomicAdd(a.counts + c, cnt);
+        atomicAdd(a.counts + c, 1);
       } else {
+        const int t = mycopy + ((int)(pk[u] & 1023u) - x0) +
+                      bx * (((int)((pk[u] >> 10) & 1023u) - y0) + by * ((int)(pk[u] >> 20) - z0));
+        const int node[8] = {t, t + bx, t + bx + bxy, t + bxy, t + 1 + bxy, t + 1 + bx + bxy,
+                             t + 1 + bx, t + 1};
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-          long long o = node[k] - base;
-          if (mode == 2 && o >= P) o = o - P + LB;
-          atomicAdd(tlo + o, (unsigned)(qv[k] & lomask));
-          atomicAdd(thi + o, (unsigned)(qv[k] >> IMPZ_DEP_LOBITS));
+          atomicAdd(tlo + node[k], (unsigned)(qv[k] & lomask));
+          atomicAdd(thi + node[k], (unsigned)(qv[k] >> IMPZ_DEP_LOBITS));
         }
-        atomicAdd(tcnt + (c - base), (unsigned)cnt);
+        atomicAdd(tcnt + t, 1u);
       }
     }
     __syncthreads();
-    if (mode != 0) {
-      // flush the touched part of the tile and clear it for the next chunk
-      const long long lenA = (mode == 2) ? W : W + P;
-      for (long long e = threadIdx.x; e < lenA; e += BLOCK) {
-        const unsigned lo = tlo[e], hi = thi[e];
-        if (lo | hi) {
-          atomicAdd(a.rho + base + e,
-                    ((unsigned long long)hi << IMPZ_DEP_LOBITS) + (unsigned long long)lo);
-          tlo[e] = 0u;
-          thi[e] = 0u;
-        }
-      }
-      if (mode == 2)
-        for (long long e = threadIdx.x; e < W; e += BLOCK) {
-          const unsigned lo = tlo[LB + e], hi = thi[LB + e];
-          if (lo | hi) {
-            atomicAdd(a.rho + base + P + e,
-                      ((unsigned long long)hi << IMPZ_DEP_LOBITS) + (unsigned long long)lo);
-            tlo[LB + e] = 0u;
-            thi[LB + e] = 0u;
+    if (tiled) {
+      // add the copies, flush the box and clear it for the next chunk
+      for (int e = threadIdx.x; e < (int)V; e += BLOCK) {
+        unsigned long long q = 0ull;
+        unsigned int k = 0u;
+        for (int r = 0, o = e; r < R; r++, o += S) {
+          const unsigned lo = tlo[o], hi = thi[o], c = tcnt[o];
+          if (lo | hi | c) {
+            q += ((unsigned long long)hi << IMPZ_DEP_LOBITS) + (unsigned long long)lo;
+            k += c;
+            tlo[o] = 0u;
+            thi[o] = 0u;
+            tcnt[o] = 0u;
           }
         }
-      for (long long e = threadIdx.x; e <= span; e += BLOCK) {
-        const unsigned v = tcnt[e];
-        if (v) {
-          atomicAdd(a.counts + base + e, (int)v);
-          tcnt[e] = 0u;
+        if (q | k) {
+          const int lz = e / bxy, r = e - lz * bxy;
+          const int ly = r / bx, lx = r - ly * bx;
+          const long long gi = (long long)(x0 + lx) + nx * ((long long)(y0 + ly) +
+                                                           (long long)ny * (z0 + lz));
+          if (q) atomicAdd(a.rho + gi, q);
+          if (k) atomicAdd(a.counts + gi, (int)k);
         }
       }
     }

@@ -41,7 +41,10 @@ struct Job {
   std::vector<impz_elem_t> elems;
   std::vector<std::vector<double>> tables;  // RF on-axis tables, 4 per element
   // state
-  int status = 0;  // 0 queued, 1 running, 2 done, <0 error code
+  // 0 queued, 1 running, 2 done, <0 error code; written under the server
+  // mutex, and set to 2 or an error only once the worker is done with the job
+  int status = 0;
+  int fin = 0;     // worker-private outcome: 0 running, 2 done, <0 error code
   impz_bunch_t bunch = nullptr;
   long long footprint = 0, measured = 0;
   int remaining = 0, chunks = 0;
@@ -116,7 +119,7 @@ void release(impz_server_t s, Job* j) {
 bool service(impz_server_t s, std::vector<Job*>& running) {
   bool progress = false;
   for (Job* j : running) {
-    if (j->status != 1) continue;
+    if (j->fin != 0) continue;
     cudaStream_t st = (cudaStream_t)impz_bunch_stream(j->bunch);
     if (j->remaining > 0) {
       // at most two chunks in flight: chunk k may go once chunk k-2 is done
@@ -125,7 +128,7 @@ bool service(impz_server_t s, std::vector<Job*>& running) {
       int left = 0;
       int r = impz_run_advance(j->bunch, s->chunk, &left);
       if (r) {
-        j->status = r;
+        j->fin = r;
         continue;
       }
       j->remaining = left;
@@ -138,7 +141,7 @@ bool service(impz_server_t s, std::vector<Job*>& running) {
       j->zs.assign(cap, 0.0);
       int r = impz_run_fetch(j->bunch, j->recs.data(), j->zs.data(), cap, &j->nrec);
       j->t_done = Clock::now();
-      j->status = r ? r : 2;
+      j->fin = r ? r : 2;
       progress = true;
     }
   }
@@ -172,36 +175,37 @@ void worker_main(impz_server_t s) {
       j->t_start = Clock::now();
       int r = admit(s, j);
       if (r) {
-        j->status = r;
         j->t_done = Clock::now();
         release(s, j);
         std::lock_guard<std::mutex> g(s->mu);
         s->failed++;
+        j->status = r;  // the waiter may free the job from here on
         s->cv_done.notify_all();
         continue;
       }
-      j->status = 1;
       running.push_back(j);
       std::lock_guard<std::mutex> g(s->mu);
+      j->status = 1;
       s->peak_measured = std::max(s->peak_measured, j->measured);
     }
     const bool progress = service(s, running);
     // retire finished jobs
     std::vector<Job*> still;
     for (Job* j : running) {
-      if (j->status == 1) {
+      if (j->fin == 0) {
         still.push_back(j);
         continue;
       }
       release(s, j);
       std::lock_guard<std::mutex> g(s->mu);
-      if (j->status == 2) {
+      if (j->fin == 2) {
         s->completed++;
         s->particle_steps += (double)j->n * (double)j->steps;
         s->t_last = j->t_done;
       } else {
         s->failed++;
       }
+      j->status = j->fin;  // the waiter may free the job from here on
       s->cv_done.notify_all();
     }
     running.swap(still);
