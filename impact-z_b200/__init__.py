@@ -22,6 +22,8 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "impz_b200.h")
 OK = 0
 ERR_ARG, ERR_NOMEM, ERR_CUDA, ERR_UNSUPPORTED = -1, -2, -3, -4
 ERR_NONUNIFORM, ERR_STATE, ERR_NONFINITE, ERR_NODEVICE, ERR_BUDGET = -5, -6, -7, -8, -9
+ERR_LIMIT = -10
+STATIC_MAX_CELLS = 1 << 19
 FORM_FP64 = 0
 FORM_FP32CONV = 1
 FLAG_TRACK_IDS = 1
@@ -105,6 +107,10 @@ _SIGS = {
     "impz_bunch_footprint": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_int]),
+    "impz_deposit_static": (ctypes.c_int, [ctypes.c_void_p] * 6 + [
+        ctypes.c_longlong, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+        ctypes.c_double, _D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+        ctypes.c_void_p]),
     "impz_server_create": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, ctypes.POINTER(_B)]),
     "impz_server_submit": (ctypes.c_int, [_B, _D, ctypes.c_longlong, ctypes.c_double,
                                           ctypes.c_double, ctypes.c_double, ctypes.c_double, _D,

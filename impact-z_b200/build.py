@@ -32,6 +32,7 @@ UNITS = [
     ("impz_poisson.cu", ["--fmad=false"]),
     ("impz_capi.cu", []),
     ("impz_serve.cu", []),
+    ("impz_static.cu", ["--fmad=false"]),
 ]
 HOST_UNITS = ["impz_host.cpp"]
 

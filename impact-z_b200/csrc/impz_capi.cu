@@ -495,6 +495,10 @@ void free_bunch(impz_bunch_t b) {
 }  // namespace
 
 // =====================================================================
+namespace impz {
+int report_cuda_error(cudaError_t e, const char* where) { return cuda_fail(e, where); }
+}  // namespace impz
+
 extern "C" {
 
 const char* impz_version(void) { return "impz_b200 0.1 (sm_100a)"; }
@@ -511,6 +515,7 @@ const char* impz_error_string(int code) {
     case IMPZ_ERR_NONFINITE: return "non-finite particle coordinate";
     case IMPZ_ERR_NODEVICE: return "no CUDA device";
     case IMPZ_ERR_BUDGET: return "footprint above budget";
+    case IMPZ_ERR_LIMIT: return "size above the fixed scratch of impz_deposit_static";
     default: return "unknown error";
   }
 }

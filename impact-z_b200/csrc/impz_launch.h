@@ -73,4 +73,8 @@ cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s);
 template <typename T>
 size_t poisson_smem_max(int nx, int ny, int nz);
 
+// Records a CUDA failure for impz_last_cuda_error and returns IMPZ_ERR_CUDA
+// (for translation units other than the C-ABI core).
+int report_cuda_error(cudaError_t e, const char* where);
+
 }  // namespace impz

@@ -31,6 +31,7 @@ extern "C" {
 #define IMPZ_ERR_NONFINITE (-7)   /* a particle coordinate became Inf/NaN */
 #define IMPZ_ERR_NODEVICE (-8)    /* no CUDA device / extension built without GPU */
 #define IMPZ_ERR_BUDGET (-9)      /* admission refused: footprint above budget */
+#define IMPZ_ERR_LIMIT (-10)      /* grid above IMPZ_STATIC_MAX_CELLS (impz_deposit_static) */
 
 /* numerical forms */
 #define IMPZ_FORM_FP64 0     /* plain: all FP64, reference operation order, no FMA */
@@ -219,6 +220,36 @@ int impz_server_destroy(impz_server_t s);
  * (CCL.f90:122-328) by the same RK6; refpt is updated like the reference. */
 int impz_maplinear(const impz_elem_t* e, double zedge, double t, double tau,
                    double refpt[6], double charge, double mass, double freq, double xm[36]);
+
+/* ---- charge deposit without device allocation ---------------------------
+ * No counterpart in the reference (its deposit works on arrays its own code
+ * allocated).  For callers that may not allocate device memory while they
+ * run: a host code whose GPU memory all comes from its own pool or arena,
+ * or a timed loop that cannot take the device-wide synchronization that
+ * cudaMalloc and cudaFree imply.  The caller passes the particles and the
+ * output in device memory it owns; the only scratch, the int64 accumulator,
+ * is a fixed array of IMPZ_STATIC_MAX_CELLS nodes (4 MiB) in the library's
+ * device image, which every GPU that loads the library holds until exit.
+ *
+ * Deposits the charge density of deposit_BeamBunch (BeamBunch.f90:3678-3768)
+ * after conv1st's z->t conversion and loss test, with the same fixed-point
+ * sums as impz_deposit, so for the same particles and geometry chgdens
+ * equals impz_deposit's chgdens bit for bit.  x..pt: device columns of
+ * Pts1 rows 1..6 (n particles); gam = -refptcl(6); piperad, piperad2 as for
+ * impz_sc_prepare; freq = Scfreq; weight = Pts1 row 8; range[6] (host) =
+ * the mesh box (impz_sc_prepare's range); chgdens: device, nx*ny*nz doubles,
+ * x fastest.  Launches on `stream` (a cudaStream_t, 0 = default) and returns
+ * without synchronizing; IMPZ_ERR_LIMIT if nx*ny*nz > IMPZ_STATIC_MAX_CELLS.
+ * The first call on each device (the current one) looks up the array's
+ * device address; make that first call before any stream capture.  All
+ * calls share the array: calls whose kernels can overlap on the GPU (other
+ * streams, other host threads) race and give wrong sums. */
+#define IMPZ_STATIC_MAX_CELLS (1 << 19)
+int impz_deposit_static(const double* x, const double* px, const double* y, const double* py,
+                        const double* ph, const double* pt, long long n, double gam,
+                        double piperad, double piperad2, double freq, double weight,
+                        const double range[6], int nx, int ny, int nz, double* chgdens,
+                        void* stream);
 
 #ifdef __cplusplus
 }
