@@ -209,12 +209,14 @@ struct impz_bunch_s {
   double sc_gam = 0, sc_rad = 0;
   // last impz_run_async
   CompiledLattice lat;
+  bool run_light = false;  // the run's programs need only the light particle pass
   bool run_pending = false;
   size_t bytes = 0;
   // graphs of two space-charge steps, per start parity
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   const StepParams* g_steps[2] = {nullptr, nullptr};
   const double* g_mom[2] = {nullptr, nullptr};
+  bool g_light[2] = {false, false};  // which particle pass the graph holds
   int h_step0 = 0;
   int run_next = 0;       // next step of the run in progress
   double run_z = 0;       // z and refptcl at the end of the run in progress
@@ -304,10 +306,26 @@ AdvanceArgs advance_args(impz_bunch_t b, const StepParams* table, int fixed, int
   return a;
 }
 
-cudaError_t launch_adv(impz_bunch_t b, const AdvanceArgs& a) {
+// `light`: every program of the table holds only drifts and block-diagonal
+// maps, so the particle pass without the other map kinds can run it
+cudaError_t launch_adv(impz_bunch_t b, const AdvanceArgs& a, bool light) {
   ProfScope ps(b, IMPZ_PROF_PUSH, 1);
-  if (b->f32()) return fast::launch_advance(a, true, b->grid_adv, b->stream);
-  return exact::launch_advance(a, false, b->grid_adv, b->stream);
+  if (b->f32()) return fast::launch_advance(a, true, light, b->grid_adv, b->stream);
+  return exact::launch_advance(a, false, light, b->grid_adv, b->stream);
+}
+
+bool program_is_light(const MapProgram& prog) {
+  for (int o = 0; o < prog.nops; o++) {
+    const int k = prog.ops[o].kind;
+    if (k != MAP_DRIFT && k != MAP_XM2 && k != MAP_NONE) return false;
+  }
+  return true;
+}
+
+bool table_is_light(const std::vector<StepParams>& steps) {
+  for (const StepParams& sp : steps)
+    if (!program_is_light(sp.post) || !program_is_light(sp.pre_next)) return false;
+  return true;
 }
 
 DepositArgs deposit_args(impz_bunch_t b, const StepParams* table, int fixed) {
@@ -725,7 +743,7 @@ static int run_fine_advance(impz_bunch_t b, const StepParams host[2], int kick, 
   int r = upload_fine(b, host);
   if (r) return r;
   AdvanceArgs a = advance_args(b, b->dfine, 0, kick, post, pre, b->mom_fine, 0);
-  CK(launch_adv(b, a));
+  CK(launch_adv(b, a, false));
   if (kick) b->parity ^= 1;
   if (rec) {
     CK(cudaMemcpyAsync(rec, b->mom_fine, IMPZ_MOMREC * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1004,7 +1022,7 @@ static int launch_step(impz_bunch_t b, bool sc) {
     if (r) return r;
   }
   AdvanceArgs a = advance_args(b, b->dsteps, -1, sc ? 1 : 0, 1, 1, b->mom_out, 0);
-  CK(launch_adv(b, a));
+  CK(launch_adv(b, a, b->run_light));
   if (sc) b->parity ^= 1;
   return IMPZ_OK;
 }
@@ -1014,7 +1032,8 @@ static int launch_step(impz_bunch_t b, bool sc) {
 // or the record buffer move.
 static int graph_pair(impz_bunch_t b) {
   const int p = b->parity;
-  if (b->gexec[p] && (b->g_steps[p] != b->dsteps || b->g_mom[p] != b->mom_out)) {
+  if (b->gexec[p] && (b->g_steps[p] != b->dsteps || b->g_mom[p] != b->mom_out ||
+                      b->g_light[p] != b->run_light)) {
     cudaGraphExecDestroy(b->gexec[p]);
     b->gexec[p] = nullptr;
   }
@@ -1036,6 +1055,7 @@ static int graph_pair(impz_bunch_t b) {
     if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
     b->g_steps[p] = b->dsteps;
     b->g_mom[p] = b->mom_out;
+    b->g_light[p] = b->run_light;
     b->parity = p;  // capture did not execute anything
   }
   g_launches += 2 * 12;
@@ -1057,6 +1077,7 @@ static int run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   int r = compile_lattice(b->P, elems, nelem, b->current0, b->sp, b->run_ref, &b->run_z, L);
   if (r) return r;
   const int K = L.nsteps;
+  b->run_light = table_is_light(L.steps);
   if ((r = ensure_tables(b, K + 2, K + 1))) return r;
   CK(cudaMemcpyAsync(b->dsteps, L.steps.data(), (K + 2) * sizeof(StepParams),
                      cudaMemcpyHostToDevice, b->stream));
@@ -1066,7 +1087,7 @@ static int run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   CK(cudaMemcpyAsync(&b->st->step, &b->h_step0, sizeof(int), cudaMemcpyHostToDevice,
                      b->stream));
   AdvanceArgs a = advance_args(b, b->dsteps, -1, 0, 1, 1, b->mom_out, 0);
-  CK(launch_adv(b, a));
+  CK(launch_adv(b, a, b->run_light));
   b->run_next = 1;
   return IMPZ_OK;
 }

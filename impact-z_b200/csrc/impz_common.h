@@ -142,7 +142,7 @@ struct DepositArgs {
 
 #define IMPZ_SCAN_LOG 13      // 8192 cells per scan block
 #ifndef IMPZ_DEP_TILE
-#define IMPZ_DEP_TILE 8192    // deposit tile entries: two int32 halves + an int32 count (96 KB)
+#define IMPZ_DEP_TILE 4096    // deposit tile entries: two int32 halves + an int32 count (48 KB)
 #endif
 
 }  // namespace impz

@@ -17,19 +17,20 @@ namespace impz {
 #define IMPZ_ADV_MINB 2
 #endif
 #ifndef IMPZ_DEP_BLOCK
-#define IMPZ_DEP_BLOCK 512
+#define IMPZ_DEP_BLOCK 256
 #endif
 #ifndef IMPZ_DEP_PPT
 #define IMPZ_DEP_PPT 4
 #endif
 #ifndef IMPZ_DEP_MINB
-#define IMPZ_DEP_MINB 2
+#define IMPZ_DEP_MINB 4
 #endif
 #define IMPZ_SCAN_THREADS 1024
 
 #define IMPZ_DECLARE_PARTICLE_LAUNCHERS(NS)                                              \
   namespace NS {                                                                         \
-  cudaError_t launch_advance(const AdvanceArgs& a, bool f32, int grid, cudaStream_t s);  \
+  cudaError_t launch_advance(const AdvanceArgs& a, bool f32, bool light, int grid,       \
+                             cudaStream_t s);                                            \
   cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s);            \
   cudaError_t launch_scan(int* counts, int* cursor, int* bsum, long long total,          \
                           DevState* st, cudaStream_t s);                                 \

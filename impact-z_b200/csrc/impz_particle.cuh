@@ -268,10 +268,20 @@ __device__ __forceinline__ void map_sector(Particle& p, const volatile double* c
 // pointers inside the particle loop: the coefficients are re-read (a
 // broadcast shared load) per particle instead of being hoisted into
 // registers for every map kind the switch could take.
+// LIGHT programs hold only drifts and block-diagonal linear maps (the
+// drift/quadrupole lattices); the host picks that instantiation when every
+// step of a run qualifies, which keeps the other map kinds' code and
+// registers out of the particle pass.
+template <bool LIGHT>
 __device__ __forceinline__ void apply_program(Particle& p, const volatile MapProgram& prog) {
   const int nops = prog.nops;
   for (int o = 0; o < nops; o++) {
     const volatile MapOp& op = prog.ops[o];
+    if (LIGHT) {
+      if (op.kind == MAP_DRIFT) map_drift(p, op.c);
+      else if (op.kind == MAP_XM2) map_xm2(p, op.c);
+      continue;
+    }
     switch (op.kind) {
       case MAP_DRIFT: map_drift(p, op.c); break;
       case MAP_XM6: map_xm6(p, op.c, op.flags, op.iparam); break;
@@ -559,9 +569,12 @@ __device__ __forceinline__ double moment_value(const Contrib& c, int v) {
 
 // Per-warp reduction of the 37 moment sums by a shared-memory transpose:
 // every lane writes its sums into its row of a 32 x 37 tile, then lane l
-// adds column l (and lanes 0..4 column 32+l) over the 32 rows into its own
-// register accumulators.  Rows have an odd length, so neither the row
-// writes nor the column reads conflict.  The seven maxima stay per lane.
+// adds column l over the 32 rows into acc0, and the five columns 32..36 are
+// split among all lanes: lane l adds column 32 + l%5 over rows 6*(l/5) ..
+// 6*(l/5)+5 into acc1 (the lanes sharing a column cover its 32 rows; they
+// are added together once, at the end of the pass, by moment_tail).  Rows
+// have an odd length, so the row writes and the column-l reads do not
+// conflict.  The seven maxima stay per lane.
 #define IMPZ_MSUMS 37
 template <int U>
 __device__ __forceinline__ void warp_moments(double* tile, const Contrib (&c)[U], int lane,
@@ -581,16 +594,30 @@ __device__ __forceinline__ void warp_moments(double* tile, const Contrib (&c)[U]
   __syncwarp();
   double s0 = 0.0, s1 = 0.0;
 #pragma unroll 8
-  for (int r = 0; r < 32; r++) {
-    s0 = s0 + tile[r * IMPZ_MSUMS + lane];
-    if (lane < IMPZ_MSUMS - 32) s1 = s1 + tile[r * IMPZ_MSUMS + 32 + lane];
-  }
+  for (int r = 0; r < 32; r++) s0 = s0 + tile[r * IMPZ_MSUMS + lane];
+  const int c1 = 32 + lane % 5, r1 = 6 * (lane / 5);
+#pragma unroll
+  for (int j = 0; j < 6; j++)
+    if (r1 + j < 32) s1 = s1 + tile[(r1 + j) * IMPZ_MSUMS + c1];
   acc0 = acc0 + s0;
   acc1 = acc1 + s1;
   __syncwarp();
 }
 
-template <int BLOCK, bool F32, int U>
+// Column 32+m of a warp's sums (m = lane < 5): the acc1 partials of lanes
+// m, m+5, m+10, ... added in lane order.
+__device__ __forceinline__ double moment_tail(double acc1, int lane) {
+  double t = 0.0;
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    const int src = 5 * k + lane % 5;
+    const double v = __shfl_sync(0xffffffffu, acc1, src & 31);
+    if (src < 32) t = t + v;
+  }
+  return t;
+}
+
+template <int BLOCK, bool F32, int U, bool LIGHT>
 __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a) {
   __shared__ double red[BLOCK / 32][IMPZ_RAW_LEN];
   __shared__ double redr[BLOCK / 32][8];
@@ -725,7 +752,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
           p[u].pt = p[u].pt - tt * ezn;
         }
       }
-      if (keep[u] && post) apply_program(p[u], progs[0]);
+      if (keep[u] && post) apply_program<LIGHT>(p[u], progs[0]);
       if (keep[u]) {
         c[u].x = p[u].x; c[u].px = p[u].px; c[u].y = p[u].y;
         c[u].py = p[u].py; c[u].z = p[u].ph; c[u].pz = p[u].pt;
@@ -737,7 +764,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
 #pragma unroll
     for (int u = 0; u < U; u++) {
       if (keep[u] && pre) {
-        apply_program(p[u], progs[1]);
+        apply_program<LIGHT>(p[u], progs[1]);
         if (rng) {
           TFrame t = to_tframe(p[u], gam_n, rad_n, xl);
           rmn[0] = fmin(rmn[0], fmin(t.tmpx, t.xt));
@@ -782,7 +809,8 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   // ---- block reductions
   if (mom) {
     red[wid][lane] = macc0;
-    if (lane < IMPZ_MSUMS - 32) red[wid][32 + lane] = macc1;
+    const double tail = moment_tail(macc1, lane);
+    if (lane < IMPZ_MSUMS - 32) red[wid][32 + lane] = tail;
 #pragma unroll
     for (int v = 0; v < 7; v++) {
       const double m = warp_max(mmax[v]);

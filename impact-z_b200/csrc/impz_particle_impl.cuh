@@ -10,22 +10,25 @@ static const size_t kDepSmem = (size_t)3 * IMPZ_DEP_TILE * sizeof(unsigned int);
 
 static const size_t kAdvSmem = (size_t)(IMPZ_ADV_BLOCK / 32) * 32 * 37 * sizeof(double);
 
-template <bool F32>
+template <bool F32, bool LIGHT>
 static cudaError_t adv_attr() {
   static cudaError_t once = cudaFuncSetAttribute(
-      k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-      (int)kAdvSmem);
+      k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT>,
+      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdvSmem);
   return once;
 }
 
-cudaError_t launch_advance(const AdvanceArgs& a, bool f32, int grid, cudaStream_t s) {
-  cudaError_t e = f32 ? adv_attr<true>() : adv_attr<false>();
+template <bool F32, bool LIGHT>
+static cudaError_t launch_adv_t(const AdvanceArgs& a, int grid, cudaStream_t s) {
+  cudaError_t e = adv_attr<F32, LIGHT>();
   if (e != cudaSuccess) return e;
-  if (f32)
-    k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U><<<grid, IMPZ_ADV_BLOCK, kAdvSmem, s>>>(a);
-  else
-    k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U><<<grid, IMPZ_ADV_BLOCK, kAdvSmem, s>>>(a);
+  k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT><<<grid, IMPZ_ADV_BLOCK, kAdvSmem, s>>>(a);
   return cudaGetLastError();
+}
+
+cudaError_t launch_advance(const AdvanceArgs& a, bool f32, bool light, int grid, cudaStream_t s) {
+  if (f32) return light ? launch_adv_t<true, true>(a, grid, s) : launch_adv_t<true, false>(a, grid, s);
+  return light ? launch_adv_t<false, true>(a, grid, s) : launch_adv_t<false, false>(a, grid, s);
 }
 
 static cudaError_t dep_attr() {
@@ -53,14 +56,15 @@ int max_blocks_advance(bool f32) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // the full instantiation bounds the light one (at most its registers)
   if (f32) {
-    adv_attr<true>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U>,
-                                                  IMPZ_ADV_BLOCK, kAdvSmem);
+    adv_attr<true, false>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per, k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U, false>, IMPZ_ADV_BLOCK, kAdvSmem);
   } else {
-    adv_attr<false>();
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U>,
-                                                  IMPZ_ADV_BLOCK, kAdvSmem);
+    adv_attr<false, false>();
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per, k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U, false>, IMPZ_ADV_BLOCK, kAdvSmem);
   }
   return sms * (per > 0 ? per : 1);
 }

@@ -212,3 +212,32 @@ def _ref_of(row, cfg):
     r[4] = row[1]
     r[5] = -row[2]
     return r
+
+
+def mixed_lattice():
+    """Drift, quadrupoles, an ideal RF gap (v4 < 0) and a sector bend: every
+    map kind of the runner beyond drifts and block-diagonal maps."""
+    rf = impz.elem(101, 0.1, 4, 1, [1.0e6, 402.5e6, -30.0, -1.0, 1.0])
+    bend = impz.elem(4, 0.2, 4, 1, [0.05, 0.0, 150.0, 0.01, 0.0, 0.0, 0.0, 0.0, 0.0])
+    return (beams.fodo(1) + [rf, impz.elem(0, 0.1, 4, 1, [1.0]), bend,
+                             impz.elem(0, 0.1, 4, 1, [1.0])])
+
+
+def test_mixed_lattice_after_light_run_fp64_moments():
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 12)
+    lat = mixed_lattice()
+    rows_o, p_o, beam = orc.run(lat, cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"],
+                                cfg["freq"], cfg["refptcl"], cfg["grid"])
+    b = impz.Bunch(cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=impz.FORM_FP64, track_ids=False)
+    # a drift/quadrupole run first: its graphs hold the light particle pass,
+    # which must not be replayed for the bend and RF steps
+    b.run(beams.fodo(1))
+    b.upload(cfg["pts"], cfg["current"], cfg["refptcl"])
+    recs, zs = b.run(lat)
+    b.close()
+    assert recs.shape[0] == rows_o.shape[0]
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    rows_g = np.array([impz.diag_row(rows_o[i, 0], recs[i], _ref_of(rows_o[i], cfg), cfg["mass"],
+                                     cfg["freq"]) for i in range(len(recs))])
+    _row_cmp(rows_g, rows_o, RMS_COLS, 1e-8)
