@@ -560,6 +560,9 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
   if (!(mass > 0) || !(freq > 0) || charge == 0.0) return IMPZ_ERR_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return IMPZ_ERR_NODEVICE;
+  if (!(form == IMPZ_FORM_FP32CONV ? poisson_fits<float>(nx, ny, nz)
+                                   : poisson_fits<double>(nx, ny, nz)))
+    return IMPZ_ERR_UNSUPPORTED;  // a z line of the doubled grid exceeds shared memory
   impz_bunch_t b = new impz_bunch_s();
   cudaGetDevice(&b->device);
   b->form = form;

@@ -140,7 +140,7 @@ struct DepositArgs {
   double xl;
 };
 
-#define IMPZ_SCAN_LOG 13      // 8192 cells per scan block
+#define IMPZ_SCAN_LOG 12      // 4096 cells per scan block (1024 threads x 4)
 #ifndef IMPZ_DEP_TILE
 #define IMPZ_DEP_TILE 4096    // deposit tile entries: two int32 halves + an int32 count (48 KB)
 #endif

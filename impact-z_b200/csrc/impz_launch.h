@@ -71,8 +71,9 @@ template <typename T>
 cudaError_t launch_conv_rest(const PoissonBuffers& b, cudaStream_t s);
 template <typename T>
 cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s);
+// true when every Poisson kernel of the form fits the device's shared memory
 template <typename T>
-size_t poisson_smem_max(int nx, int ny, int nz);
+bool poisson_fits(int nx, int ny, int nz);
 
 // Records a CUDA failure for impz_last_cuda_error and returns IMPZ_ERR_CUDA
 // (for translation units other than the C-ABI core).

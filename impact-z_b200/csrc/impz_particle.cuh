@@ -1100,69 +1100,94 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
   }
 }
 
-// Exclusive scan of counts[0..G] into per-block local offsets (cursor) and
-// per-block totals (bsum), clearing counts for the next step; the last
-// block turns bsum into exclusive block offsets.
+// Exclusive scan over the block of one value per thread; *total gets the
+// block's sum.  wsum: BLOCK/32 ints of shared memory.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_scan(int* counts, int* cursor, int* bsum,
-                                                long long total, DevState* st) {
-  __shared__ int wsum[BLOCK / 32];
-  __shared__ unsigned int s_last;
-  constexpr int PER = (1 << IMPZ_SCAN_LOG) / BLOCK;
-  const long long base = (long long)blockIdx.x << IMPZ_SCAN_LOG;
-  int v[PER];
-  int tsum = 0;
-#pragma unroll
-  for (int j = 0; j < PER; j++) {
-    long long i = base + (long long)threadIdx.x * PER + j;
-    v[j] = (i < total) ? counts[i] : 0;
-    if (i < total) counts[i] = 0;
-    tsum += v[j];
-  }
+__device__ __forceinline__ int block_exclusive_scan(int x, int* wsum, int* total) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int incl = tsum;
+  int incl = x;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= o) incl += y;
   }
+  __syncthreads();  // wsum may still be read by a previous call
   if (lane == 31) wsum[wid] = incl;
   __syncthreads();
   if (wid == 0) {
-    int w = lane < BLOCK / 32 ? wsum[lane] : 0;
+    const int w = lane < BLOCK / 32 ? wsum[lane] : 0;
     int wi = w;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, wi, o);
+      const int y = __shfl_up_sync(0xffffffffu, wi, o);
       if (lane >= o) wi += y;
     }
     if (lane < BLOCK / 32) wsum[lane] = wi - w;  // exclusive warp offsets
-    if (lane == BLOCK / 32 - 1) bsum[blockIdx.x] = wi;
+    if (lane == BLOCK / 32 - 1) wsum[BLOCK / 32] = wi;
   }
   __syncthreads();
-  int run = wsum[wid] + incl - tsum;
+  *total = wsum[BLOCK / 32];
+  return wsum[wid] + incl - x;
+}
+
+// Exclusive scan of counts[0..total) into per-block local offsets (cursor)
+// and per-block totals (bsum), clearing counts for the next step; the last
+// block to finish turns bsum into exclusive block offsets.  Each thread
+// takes four consecutive cells (one 16-byte load and store).
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scan(int* counts, int* cursor, int* bsum,
+                                                long long total, DevState* st) {
+  static_assert((BLOCK << 2) == (1 << IMPZ_SCAN_LOG), "four cells per thread");
+  __shared__ int wsum[BLOCK / 32 + 1];
+  __shared__ unsigned int s_last;
+  const long long i0 = ((long long)blockIdx.x << IMPZ_SCAN_LOG) + 4ll * threadIdx.x;
+  int v[4];
+  const bool full = i0 + 3 < total;
+  if (full) {
+    const int4 q = *reinterpret_cast<const int4*>(counts + i0);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    *reinterpret_cast<int4*>(counts + i0) = make_int4(0, 0, 0, 0);
+  } else {
 #pragma unroll
-  for (int j = 0; j < PER; j++) {
-    long long i = base + (long long)threadIdx.x * PER + j;
-    if (i < total) cursor[i] = run;
+    for (int j = 0; j < 4; j++) {
+      v[j] = (i0 + j < total) ? counts[i0 + j] : 0;
+      if (i0 + j < total) counts[i0 + j] = 0;
+    }
+  }
+  int btotal = 0;
+  int run = block_exclusive_scan<BLOCK>(v[0] + v[1] + v[2] + v[3], wsum, &btotal);
+  int o[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    o[j] = run;
     run += v[j];
   }
+  if (full) {
+    *reinterpret_cast<int4*>(cursor + i0) = make_int4(o[0], o[1], o[2], o[3]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (i0 + j < total) cursor[i0 + j] = o[j];
+  }
+  if (threadIdx.x == 0) bsum[blockIdx.x] = btotal;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) s_last = (atomicAdd(&st->done_scan, 1u) == gridDim.x - 1) ? 1u : 0u;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  if (threadIdx.x == 0) {
-    volatile int* b = bsum;
-    int acc = 0;
-    for (int k = 0; k < (int)gridDim.x; k++) {
-      int t = b[k];
-      b[k] = acc;
-      acc += t;
-    }
-    st->done_scan = 0;
+  // block totals -> exclusive block offsets, BLOCK at a time with a carry
+  const int nb = (int)gridDim.x;
+  int carry = 0;
+  for (int k0 = 0; k0 < nb; k0 += BLOCK) {
+    const int k = k0 + threadIdx.x;
+    const int t = k < nb ? __ldcg(bsum + k) : 0;
+    int sum = 0;
+    const int ex = block_exclusive_scan<BLOCK>(t, wsum, &sum);
+    if (k < nb) bsum[k] = carry + ex;
+    carry += sum;
   }
+  if (threadIdx.x == 0) st->done_scan = 0;
 }
 
 }  // namespace IMPZ_NS

@@ -22,27 +22,47 @@ static PoissonDims dims_of(const PoissonBuffers& b) {
 template <typename T>
 static size_t xy_smem(int nx, int ny) {
   return sizeof(typename Cplx<T>::type) *
-         ((size_t)(ny / 2) * (2 * nx) + (size_t)(nx + 1) * (2 * ny + 1) + nx + ny);
+         ((size_t)(ny / 2) * line_pitch(2 * nx) + (size_t)(nx + 1) * line_pitch(2 * ny) + nx +
+          ny);
+}
+// largest dynamic shared memory one block may opt into on this device
+static size_t smem_optin() {
+  int dev = 0, v = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return (size_t)v;
 }
 template <typename T>
-static int ztile() { return sizeof(T) == 8 ? 8 : 16; }
+static size_t z_smem(int nz, int tkx) {
+  return sizeof(typename Cplx<T>::type) * ((size_t)tkx * line_pitch(2 * nz) + nz);
+}
+// z lines per block: 8 (FP64) or 16 (FP32) for 128-byte rows, fewer when
+// long lines do not fit
 template <typename T>
-static size_t z_smem(int nz) {
-  return sizeof(typename Cplx<T>::type) * ((size_t)ztile<T>() * (2 * nz + 1) + nz);
+static int ztile(int nz) {
+  int t = sizeof(T) == 8 ? 8 : 16;
+  while (t > 1 && z_smem<T>(nz, t) > smem_optin()) t /= 2;
+  return t;
 }
 static const int kDctLines = 16;
 template <typename T>
-static size_t dct_smem(int n) {
-  return sizeof(typename Cplx<T>::type) * ((size_t)(kDctLines / 2) * (2 * n + 1) + n);
+static size_t dct_smem(int n, int lines) {
+  return sizeof(typename Cplx<T>::type) * ((size_t)(lines / 2) * line_pitch(2 * n) + n);
+}
+template <typename T>
+static int dct_lines(int n) {
+  int t = kDctLines;
+  while (t > 2 && dct_smem<T>(n, t) > smem_optin()) t /= 2;
+  return t;
 }
 
+// true when every Poisson kernel fits the device's shared memory
 template <typename T>
-size_t poisson_smem_max(int nx, int ny, int nz) {
-  size_t m = xy_smem<T>(nx, ny);
-  m = m > z_smem<T>(nz) ? m : z_smem<T>(nz);
+bool poisson_fits(int nx, int ny, int nz) {
+  const size_t lim = smem_optin();
   int nmax = nx > ny ? nx : ny;
   nmax = nmax > nz ? nmax : nz;
-  return m > dct_smem<T>(nmax) ? m : dct_smem<T>(nmax);
+  return xy_smem<T>(nx, ny) <= lim && z_smem<T>(nz, 1) <= lim && dct_smem<T>(nmax, 2) <= lim;
 }
 
 template <typename K>
@@ -55,6 +75,43 @@ static int grid_for(long long work, int block) {
   long long g = (work + block - 1) / block;
   if (g > 148 * 16) g = 148 * 16;
   return (int)(g < 1 ? 1 : g);
+}
+
+// One DCT-I pass of length n+1 over ninner x nouter lines, as many lines
+// per block as fit in shared memory (16 for the usual sizes).
+template <typename TI, typename T, int TL>
+static cudaError_t dct_pass_t(const TI* in, T* out, int n, long long es, long long ls, int ninner,
+                              long long os, int nouter, double scale,
+                              const typename Cplx<T>::type* tw, cudaStream_t s) {
+  auto kern = k_dct1<TI, T, T, TL>;
+  const size_t sm = dct_smem<T>(n, TL);
+  cudaError_t e = allow_smem(kern, sm);
+  if (e != cudaSuccess) return e;
+  dim3 g((ninner + TL - 1) / TL, nouter);
+  kern<<<g, 256, sm, s>>>(in, out, ilog2(2 * n), es, ls, ninner, os, scale, tw);
+  return cudaGetLastError();
+}
+template <typename TI, typename T>
+static cudaError_t dct_pass(const TI* in, T* out, int n, long long es, long long ls, int ninner,
+                            long long os, int nouter, double scale,
+                            const typename Cplx<T>::type* tw, cudaStream_t s) {
+  switch (dct_lines<T>(n)) {
+    case 16: return dct_pass_t<TI, T, 16>(in, out, n, es, ls, ninner, os, nouter, scale, tw, s);
+    case 8: return dct_pass_t<TI, T, 8>(in, out, n, es, ls, ninner, os, nouter, scale, tw, s);
+    case 4: return dct_pass_t<TI, T, 4>(in, out, n, es, ls, ninner, os, nouter, scale, tw, s);
+    default: return dct_pass_t<TI, T, 2>(in, out, n, es, ls, ninner, os, nouter, scale, tw, s);
+  }
+}
+
+template <typename T, int TKX>
+static cudaError_t zconv_t(const PoissonBuffers& b, const PoissonDims& d, cudaStream_t s) {
+  typedef typename Cplx<T>::type C;
+  const size_t sz = z_smem<T>(b.nz, TKX);
+  cudaError_t e = allow_smem(k_fft_z_conv<T, TKX>, sz);
+  if (e != cudaSuccess) return e;
+  dim3 gz((b.nx + 1 + TKX - 1) / TKX, 2 * b.ny);
+  k_fft_z_conv<T, TKX><<<gz, 256, sz, s>>>(d, (C*)b.spec, (const T*)b.ghat, (const C*)b.twz);
+  return cudaGetLastError();
 }
 
 // The Green function: FP64 corners and 8-corner difference (the difference
@@ -74,30 +131,17 @@ cudaError_t launch_green(const PoissonBuffers& b, cudaStream_t s) {
   T* work = (T*)b.ghat;
   cudaError_t e;
   // along x: lines j (inner, stride gx) x k (outer); points contiguous
-  {
-    auto kern = k_dct1<double, T, T, kDctLines>;
-    const size_t sm = dct_smem<T>(nx);
-    if ((e = allow_smem(kern, sm)) != cudaSuccess) return e;
-    dim3 g((ny + 1 + kDctLines - 1) / kDctLines, nz + 1);
-    kern<<<g, 256, sm, s>>>(b.Gt, work, ilog2(2 * nx), 1, gx, ny + 1, gxy, 1.0, (const C*)b.twx);
-  }
+  if ((e = dct_pass<double, T>(b.Gt, work, nx, 1, gx, ny + 1, gxy, nz + 1, 1.0, (const C*)b.twx,
+                               s)) != cudaSuccess)
+    return e;
   // along y: lines i (inner, stride 1) x k (outer); points stride gx
-  {
-    auto kern = k_dct1<T, T, T, kDctLines>;
-    const size_t sm = dct_smem<T>(ny);
-    if ((e = allow_smem(kern, sm)) != cudaSuccess) return e;
-    dim3 g((nx + 1 + kDctLines - 1) / kDctLines, nz + 1);
-    kern<<<g, 256, sm, s>>>(work, work, ilog2(2 * ny), gx, 1, nx + 1, gxy, 1.0, (const C*)b.twy);
-  }
+  if ((e = dct_pass<T, T>(work, work, ny, gx, 1, nx + 1, gxy, nz + 1, 1.0, (const C*)b.twy, s)) !=
+      cudaSuccess)
+    return e;
   // along z: lines i (inner) x j (outer, stride gx); points stride gxy
-  {
-    auto kern = k_dct1<T, T, T, kDctLines>;
-    const size_t sm = dct_smem<T>(nz);
-    if ((e = allow_smem(kern, sm)) != cudaSuccess) return e;
-    dim3 g((nx + 1 + kDctLines - 1) / kDctLines, ny + 1);
-    kern<<<g, 256, sm, s>>>(work, work, ilog2(2 * nz), gxy, 1, nx + 1, gx, scale,
-                            (const C*)b.twz);
-  }
+  if ((e = dct_pass<T, T>(work, work, nz, gxy, 1, nx + 1, gx, ny + 1, scale, (const C*)b.twz,
+                          s)) != cudaSuccess)
+    return e;
   return cudaGetLastError();
 }
 
@@ -120,16 +164,14 @@ cudaError_t launch_conv_rest(const PoissonBuffers& b, cudaStream_t s) {
   cudaError_t e;
   const size_t sxy = xy_smem<T>(b.nx, b.ny);
   if ((e = allow_smem(k_fft_xy_inv<T>, sxy)) != cudaSuccess) return e;
-  const int tk = ztile<T>();
-  const size_t sz = z_smem<T>(b.nz);
-  dim3 gz((b.nx + 1 + tk - 1) / tk, 2 * b.ny);
-  if (tk == 8) {
-    if ((e = allow_smem(k_fft_z_conv<T, 8>, sz)) != cudaSuccess) return e;
-    k_fft_z_conv<T, 8><<<gz, 256, sz, s>>>(d, (C*)b.spec, (const T*)b.ghat, (const C*)b.twz);
-  } else {
-    if ((e = allow_smem(k_fft_z_conv<T, 16>, sz)) != cudaSuccess) return e;
-    k_fft_z_conv<T, 16><<<gz, 256, sz, s>>>(d, (C*)b.spec, (const T*)b.ghat, (const C*)b.twz);
+  switch (ztile<T>(b.nz)) {
+    case 16: e = zconv_t<T, 16>(b, d, s); break;
+    case 8: e = zconv_t<T, 8>(b, d, s); break;
+    case 4: e = zconv_t<T, 4>(b, d, s); break;
+    case 2: e = zconv_t<T, 2>(b, d, s); break;
+    default: e = zconv_t<T, 1>(b, d, s); break;
   }
+  if (e != cudaSuccess) return e;
   k_fft_xy_inv<T><<<b.nz, 512, sxy, s>>>(d, (const C*)b.spec, (T*)b.phi, (const C*)b.twx,
                                          (const C*)b.twy);
   return cudaGetLastError();
@@ -160,7 +202,7 @@ template cudaError_t launch_conv_rest<float>(const PoissonBuffers&, cudaStream_t
 template cudaError_t launch_convolve<float>(const PoissonBuffers&, cudaStream_t);
 template cudaError_t launch_efield<double>(const PoissonBuffers&, cudaStream_t);
 template cudaError_t launch_efield<float>(const PoissonBuffers&, cudaStream_t);
-template size_t poisson_smem_max<double>(int, int, int);
-template size_t poisson_smem_max<float>(int, int, int);
+template bool poisson_fits<double>(int, int, int);
+template bool poisson_fits<float>(int, int, int);
 
 }  // namespace impz

@@ -50,8 +50,17 @@ __device__ __forceinline__ int bitrev(int v, int logn) {
   return (int)(__brev((unsigned)v) >> (32 - logn));
 }
 
+// Lines in shared memory keep one spare slot after every eight elements:
+// element j of a line sits at sw(j).  The butterfly groups read eight
+// elements a fixed spacing apart, and at the small spans consecutive
+// threads start eight elements apart, which without the spare slots would
+// put 16 threads of a warp on the same banks.
+__device__ __forceinline__ int sw(int j) { return j + (j >> 3); }
+// line pitch (in elements) for lines of n >= 8 elements: odd, past sw(n-1)
+__host__ __device__ constexpr int line_pitch(int n) { return n + n / 8 + 1; }
+
 // Radix-2 butterflies over `nlines` lines in shared memory; element j of
-// line l sits at buf[l*lstride + j].  tw[k] = exp(-2 pi i k / n), k < n/2.
+// line l sits at buf[l*lstride + sw(j)].  tw[k] = exp(-2 pi i k / n), k < n/2.
 // DIF: natural order in, bit-reversed out.  DIT: bit-reversed in, natural out.
 // Up to three consecutive radix-2 stages act on the eight elements spaced by
 // a quarter of the widest span, so each thread runs them in registers (one
@@ -66,12 +75,13 @@ __device__ __forceinline__ C twid(const C* tw, int idx, int sign) {
 
 // stages with half-spans 2^lh, 2^(lh-1), .., 2^(lh-ns+1) (DIF, ns = 1..3)
 template <typename C, int NS>
-__device__ __forceinline__ void dif_group(C* L, int logn, int lh, int k, int sign, const C* tw) {
+__device__ __forceinline__ void dif_group(C* L, int o, int logn, int lh, int k, int sign,
+                                          const C* tw) {
   constexpr int E = 1 << NS;
   const int q = 1 << (lh - NS + 1);  // spacing of the E elements
   C v[E];
 #pragma unroll
-  for (int e = 0; e < E; e++) v[e] = L[k + e * q];
+  for (int e = 0; e < E; e++) v[e] = L[sw(o + k + e * q)];
 #pragma unroll
   for (int m = 0; m < NS; m++) {
     const int ls = lh - m;            // this stage's half-span 2^ls
@@ -88,17 +98,18 @@ __device__ __forceinline__ void dif_group(C* L, int logn, int lh, int k, int sig
     }
   }
 #pragma unroll
-  for (int e = 0; e < E; e++) L[k + e * q] = v[e];
+  for (int e = 0; e < E; e++) L[sw(o + k + e * q)] = v[e];
 }
 
 // stages with half-spans 2^lh, .., 2^(lh+ns-1) (DIT)
 template <typename C, int NS>
-__device__ __forceinline__ void dit_group(C* L, int logn, int lh, int k, int sign, const C* tw) {
+__device__ __forceinline__ void dit_group(C* L, int o, int logn, int lh, int k, int sign,
+                                          const C* tw) {
   constexpr int E = 1 << NS;
   const int q = 1 << lh;
   C v[E];
 #pragma unroll
-  for (int e = 0; e < E; e++) v[e] = L[k + e * q];
+  for (int e = 0; e < E; e++) v[e] = L[sw(o + k + e * q)];
 #pragma unroll
   for (int m = 0; m < NS; m++) {
     const int ls = lh + m;
@@ -115,7 +126,7 @@ __device__ __forceinline__ void dit_group(C* L, int logn, int lh, int k, int sig
     }
   }
 #pragma unroll
-  for (int e = 0; e < E; e++) L[k + e * q] = v[e];
+  for (int e = 0; e < E; e++) L[sw(o + k + e * q)] = v[e];
 }
 
 template <typename C>
@@ -123,17 +134,16 @@ __device__ void fft_dif(C* buf, int logn, int nlines, int lstride, int sign, con
   int lh = logn - 1;
   while (lh >= 0) {
     const int ns = lh >= 2 ? 3 : lh + 1;
-    const int span = 1 << (lh + 1);          // elements in one group block
-    const int per = 1 << (lh - ns + 1);      // groups per block
-    const int ngl = (1 << logn) >> ns;       // groups per line
-    const int total = nlines * ngl;
+    const int lper = lh - ns + 1;            // log2 of the groups per block
+    const int lngl = logn - ns;              // log2 of the groups per line
+    const int total = nlines << lngl;
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      const int l = b / ngl, r = b - l * ngl;
-      const int blk = r / per, k = r - blk * per;
-      C* Lp = buf + l * lstride + blk * span;
-      if (ns == 3) dif_group<C, 3>(Lp, logn, lh, k, sign, tw);
-      else if (ns == 2) dif_group<C, 2>(Lp, logn, lh, k, sign, tw);
-      else dif_group<C, 1>(Lp, logn, lh, k, sign, tw);
+      const int l = b >> lngl, r = b & ((1 << lngl) - 1);
+      const int o = (r >> lper) << (lh + 1), k = r & ((1 << lper) - 1);
+      C* Lp = buf + l * lstride;
+      if (ns == 3) dif_group<C, 3>(Lp, o, logn, lh, k, sign, tw);
+      else if (ns == 2) dif_group<C, 2>(Lp, o, logn, lh, k, sign, tw);
+      else dif_group<C, 1>(Lp, o, logn, lh, k, sign, tw);
     }
     __syncthreads();
     lh -= ns;
@@ -145,17 +155,15 @@ __device__ void fft_dit(C* buf, int logn, int nlines, int lstride, int sign, con
   int lh = 0;
   while (lh < logn) {
     const int ns = (logn - lh) >= 3 ? 3 : logn - lh;
-    const int span = 1 << (lh + ns);
-    const int per = 1 << lh;
-    const int ngl = (1 << logn) >> ns;
-    const int total = nlines * ngl;
+    const int lngl = logn - ns;
+    const int total = nlines << lngl;
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      const int l = b / ngl, r = b - l * ngl;
-      const int blk = r / per, k = r - blk * per;
-      C* Lp = buf + l * lstride + blk * span;
-      if (ns == 3) dit_group<C, 3>(Lp, logn, lh, k, sign, tw);
-      else if (ns == 2) dit_group<C, 2>(Lp, logn, lh, k, sign, tw);
-      else dit_group<C, 1>(Lp, logn, lh, k, sign, tw);
+      const int l = b >> lngl, r = b & ((1 << lngl) - 1);
+      const int o = (r >> lh) << (lh + ns), k = r & ((1 << lh) - 1);
+      C* Lp = buf + l * lstride;
+      if (ns == 3) dit_group<C, 3>(Lp, o, logn, lh, k, sign, tw);
+      else if (ns == 2) dit_group<C, 2>(Lp, o, logn, lh, k, sign, tw);
+      else dit_group<C, 1>(Lp, o, logn, lh, k, sign, tw);
     }
     __syncthreads();
     lh += ns;
@@ -185,9 +193,9 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nx = d.nx, ny = d.ny, n1 = 2 * nx, n2 = 2 * ny;
-  const int tp = n2 + 1;  // padded y-line pitch
+  const int zp = line_pitch(n1), tp = line_pitch(n2);  // x-line and y-line pitches
   C* Z = reinterpret_cast<C*>(smem_raw);
-  C* Tm = Z + (ny / 2) * n1;
+  C* Tm = Z + (ny / 2) * zp;
   C* twxs = Tm + (nx + 1) * tp;
   C* twys = twxs + n1 / 2;
   stage_tw(twxs, twx, n1);
@@ -209,10 +217,10 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
       rho[ia] = 0ull;
       rho[ib] = 0ull;
     }
-    Z[l * n1 + j] = z;
+    Z[l * zp + sw(j)] = z;
   }
   __syncthreads();
-  fft_dif<C>(Z, d.lx, hy, n1, -1, twxs);
+  fft_dif<C>(Z, d.lx, hy, zp, -1, twxs);
   // unpack: row a = (Z(k)+conj(Z(n1-k)))/2, row b = (Z(k)-conj(Z(n1-k)))/(2i),
   // k = 0..nx, into y lines Tm[kx][y] (natural y, zero padded to 2ny)
   for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
@@ -221,9 +229,9 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
     v.x = 0; v.y = 0;
     if (y < ny) {
       const int l = y < hy ? y : y - hy;
-      const C* L = Z + l * n1;
-      const C zk = L[bitrev(kx, d.lx)];
-      const C zm = L[bitrev((n1 - kx) & (n1 - 1), d.lx)];
+      const C* L = Z + l * zp;
+      const C zk = L[sw(bitrev(kx, d.lx))];
+      const C zm = L[sw(bitrev((n1 - kx) & (n1 - 1), d.lx))];
       if (y < hy) {
         v.x = (T)0.5 * (zk.x + zm.x);
         v.y = (T)0.5 * (zk.y - zm.y);
@@ -232,7 +240,7 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
         v.y = (T)0.5 * (zm.x - zk.x);
       }
     }
-    Tm[kx * tp + y] = v;
+    Tm[kx * tp + sw(y)] = v;
   }
   __syncthreads();
   fft_dif<C>(Tm, d.ly, nx + 1, tp, -1, twys);
@@ -240,7 +248,7 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
   C* Sk = S + (size_t)k * n2 * (nx + 1);
   for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
     const int ky = e / (nx + 1), kx = e - ky * (nx + 1);
-    Sk[e] = Tm[kx * tp + bitrev(ky, d.ly)];
+    Sk[e] = Tm[kx * tp + sw(bitrev(ky, d.ly))];
   }
 }
 
@@ -252,7 +260,7 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nx = d.nx, ny = d.ny, nz = d.nz, n2 = 2 * ny, n3 = 2 * nz;
-  const int lp = n3 + 1;
+  const int lp = line_pitch(n3);
   C* L = reinterpret_cast<C*>(smem_raw);
   C* twzs = L + TKX * lp;
   stage_tw(twzs, twz, n3);
@@ -266,7 +274,7 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
     C v;
     v.x = 0; v.y = 0;
     if (z < nz && t < ntk) v = base[(size_t)z * pstride + t];
-    L[t * lp + z] = v;
+    L[t * lp + sw(z)] = v;
   }
   __syncthreads();
   fft_dif<C>(L, d.lz, TKX, lp, -1, twzs);
@@ -279,7 +287,7 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
     const int kz = bitrev(pos, d.lz);
     const int kzp = kz <= nz ? kz : n3 - kz;
     const T gv = ghat[(size_t)kzp * gz + (size_t)kyp * gy + kx0 + t];
-    C& v = L[t * lp + pos];
+    C& v = L[t * lp + sw(pos)];
     v.x *= gv;
     v.y *= gv;
   }
@@ -287,7 +295,7 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
   fft_dit<C>(L, d.lz, TKX, lp, +1, twzs);
   for (int e = threadIdx.x; e < TKX * nz; e += blockDim.x) {
     const int z = e / TKX, t = e - z * TKX;
-    if (t < ntk) base[(size_t)z * pstride + t] = L[t * lp + z];
+    if (t < ntk) base[(size_t)z * pstride + t] = L[t * lp + sw(z)];
   }
 }
 
@@ -300,10 +308,10 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int nx = d.nx, ny = d.ny, n1 = 2 * nx, n2 = 2 * ny;
-  const int tp = n2 + 1;
+  const int zp = line_pitch(n1), tp = line_pitch(n2);
   const int hy = ny / 2;
   C* Z = reinterpret_cast<C*>(smem_raw);
-  C* Tm = Z + hy * n1;
+  C* Tm = Z + hy * zp;
   C* twxs = Tm + (nx + 1) * tp;
   C* twys = twxs + n1 / 2;
   stage_tw(twxs, twx, n1);
@@ -313,7 +321,7 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
   // y lines in bit-reversed order for the DIT inverse
   for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
     const int ky = e / (nx + 1), kx = e - ky * (nx + 1);
-    Tm[kx * tp + bitrev(ky, d.ly)] = Sk[e];
+    Tm[kx * tp + sw(bitrev(ky, d.ly))] = Sk[e];
   }
   __syncthreads();
   fft_dit<C>(Tm, d.ly, nx + 1, tp, +1, twys);
@@ -322,19 +330,19 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
   for (int e = threadIdx.x; e < hy * n1; e += blockDim.x) {
     const int l = e / n1, kk = e - l * n1;
     const int kxs = kk <= nx ? kk : n1 - kk;
-    C xa = Tm[kxs * tp + l], xb = Tm[kxs * tp + l + hy];
+    C xa = Tm[kxs * tp + sw(l)], xb = Tm[kxs * tp + sw(l + hy)];
     if (kk > nx) { xa.y = -xa.y; xb.y = -xb.y; }
     C z;
     z.x = xa.x - xb.y;
     z.y = xa.y + xb.x;
-    Z[l * n1 + bitrev(kk, d.lx)] = z;
+    Z[l * zp + sw(bitrev(kk, d.lx))] = z;
   }
   __syncthreads();
-  fft_dit<C>(Z, d.lx, hy, n1, +1, twxs);
+  fft_dit<C>(Z, d.lx, hy, zp, +1, twxs);
   T* ph = phi + (size_t)nx * ny * k;
   for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
     const int y = e / nx, x = e - y * nx;
-    const C v = Z[(y < hy ? y : y - hy) * n1 + x];
+    const C v = Z[(y < hy ? y : y - hy) * zp + sw(x)];
     ph[e] = y < hy ? v.x : v.y;
   }
 }
@@ -401,7 +409,7 @@ __global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long 
   C* L = reinterpret_cast<C*>(smem_raw);
   const int n = 1 << (logn - 1);  // octant points - 1
   const int n2 = 2 * n;
-  const int lp = n2 + 1;
+  const int lp = line_pitch(n2);
   C* tws = L + (TL / 2) * lp;
   stage_tw(tws, tw, n2);
   const int l0 = blockIdx.x * TL;
@@ -417,13 +425,13 @@ __global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long 
     C v;
     v.x = t < nl ? (CT)ib[(long long)t * ls + mm * es] : (CT)0;
     v.y = t + np < nl ? (CT)ib[(long long)(t + np) * ls + mm * es] : (CT)0;
-    L[t * lp + m] = v;
+    L[t * lp + sw(m)] = v;
   }
   __syncthreads();
   fft_dif<C>(L, logn, np, lp, -1, tws);
   for (int e = threadIdx.x; e < np * (n + 1); e += blockDim.x) {
     const int m = e / np, t = e - m * np;
-    const C v = L[t * lp + bitrev(m, logn)];
+    const C v = L[t * lp + sw(bitrev(m, logn))];
     if (t < nl) ob[(long long)t * ls + m * es] = (TO)((double)v.x * scale);
     if (t + np < nl) ob[(long long)(t + np) * ls + m * es] = (TO)((double)v.y * scale);
   }

@@ -241,3 +241,22 @@ def test_mixed_lattice_after_light_run_fp64_moments():
     rows_g = np.array([impz.diag_row(rows_o[i, 0], recs[i], _ref_of(rows_o[i], cfg), cfg["mass"],
                                      cfg["freq"]) for i in range(len(recs))])
     _row_cmp(rows_g, rows_o, RMS_COLS, 1e-8)
+
+
+@pytest.mark.parametrize("grid,form,tol,etol", [((16, 16, 1024), impz.FORM_FP64, 1e-12, 1e-10),
+                                                ((16, 16, 2048), impz.FORM_FP32CONV, 1e-5, 1e-4)])
+def test_single_step_long_z_grid(grid, form, tol, etol):
+    """Long z lines: the z convolution and the Green DCT take fewer lines per
+    block (shared memory), down to four; the potential matches the oracle to
+    `tol` (FP64: 1e-12; FP32 convolution: 1e-5 relative L2).  The field is a
+    centred difference of neighbouring potentials, which on a 1024-cell axis
+    differ by ~1e-3 of their value, so it carries the potential's rounding
+    amplified ~1e3: `etol` = 100 tol."""
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 13)
+    cfg["grid"] = grid
+    e = impz.elem(0, 0.1, 4, 1, [1.0])
+    o = oracle_step(cfg["pts"], cfg, e, 0.025, 1.0)
+    g = gpu_step(cfg["pts"], cfg, e, 0.025, 1.0, form=form)
+    np.testing.assert_array_equal(g["counts"], o["counts"])
+    assert rel_l2(g["phi"], o["phi"]) <= tol
+    assert rel_l2(g["eg"], o["eg"]) <= etol
