@@ -8,7 +8,7 @@ namespace impz {
 
 #define IMPZ_ADV_BLOCK 256
 #ifndef IMPZ_ADV_U
-#define IMPZ_ADV_U 1
+#define IMPZ_ADV_U 2
 #endif
 #ifndef IMPZ_ADV_PREFETCH
 #define IMPZ_ADV_PREFETCH 0
