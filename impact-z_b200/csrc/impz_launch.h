@@ -6,7 +6,9 @@
 
 namespace impz {
 
+#ifndef IMPZ_ADV_BLOCK
 #define IMPZ_ADV_BLOCK 256
+#endif
 #ifndef IMPZ_ADV_U
 #define IMPZ_ADV_U 2
 #endif

@@ -855,25 +855,42 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  // ---- last block: fixed-order reduction over blocks, then bookkeeping
+  // ---- last block: fixed-order reduction over blocks, then bookkeeping.
+  // Warp w reduces blocks [w*nb/nw, (w+1)*nb/nw) of every value (lane l:
+  // values l and l+32; 0..43 moments, 44..51 range), then thread v combines
+  // the warps' partials in warp order: a fixed order, and the loads of one
+  // lane are independent, so they overlap instead of chaining.
   const int nb = gridDim.x;
   const int row = a.fixed_step >= 0 ? a.mom_index : s;
+  const int b0 = wid * nb / nw, b1 = (wid + 1) * nb / nw;
+  for (int v = lane; v < IMPZ_RAW_LEN + 8; v += 32) {
+    const bool isrng = v >= IMPZ_RAW_LEN;
+    const int r = v - IMPZ_RAW_LEN;  // range value 0..7
+    if (!isrng && !mom) continue;
+    // identities: sums 0, maxima of |.| 0, range min +1e300 / max -1e300
+    double x = (isrng && r < 6) ? ((r & 1) ? -1e300 : 1e300) : 0.0;
+#pragma unroll 4
+    for (int b = b0; b < b1; b++) {
+      const double y = isrng ? __ldcg(a.rng_part + (size_t)b * 8 + r)
+                             : __ldcg(a.mom_part + (size_t)b * IMPZ_RAW_LEN + v);
+      if (isrng) x = (r >= 6) ? x + y : ((r & 1) ? fmax(x, y) : fmin(x, y));
+      else x = v < IMPZ_MSUMS ? x + y : fmax(x, y);
+    }
+    if (isrng) redr[wid][r] = x;
+    else red[wid][v] = x;
+  }
+  __syncthreads();
   if (mom && threadIdx.x < IMPZ_RAW_LEN) {
     const int v = threadIdx.x;
-    volatile double* mp = a.mom_part;
-    double x = mp[v];
-    for (int b = 1; b < nb; b++) {
-      double y = mp[(size_t)b * IMPZ_RAW_LEN + v];
-      x = v < 37 ? x + y : fmax(x, y);
-    }
+    double x = red[0][v];
+    for (int w = 1; w < nw; w++) x = v < IMPZ_MSUMS ? x + red[w][v] : fmax(x, red[w][v]);
     a.mom_out[(size_t)row * IMPZ_MOMREC + v] = x;
   }
   if (threadIdx.x < 8) {
     const int v = threadIdx.x;
-    volatile double* rp = a.rng_part;
-    double x = rp[v];
-    for (int b = 1; b < nb; b++) {
-      double y = rp[(size_t)b * 8 + v];
+    double x = redr[0][v];
+    for (int w = 1; w < nw; w++) {
+      const double y = redr[w][v];
       x = (v >= 6) ? x + y : ((v & 1) ? fmax(x, y) : fmin(x, y));
     }
     fin[v] = x;
