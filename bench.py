@@ -349,7 +349,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, secs, done = cpu_baseline_port(n, 1, 3, max_seconds=30.0)
+        v, secs, done = cpu_baseline_port(n, 1, 6, max_seconds=30.0)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": "%d steps of the %d-particle %dx%dx%d workload, oracle port, 1 thread "
                          "(%.1f s)" % (done, n, *GRID, secs)}

@@ -591,8 +591,10 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
   b->k.charge = charge;
   b->k.qm0 = charge / mass;
   b->k.qmi = b->sp.qmi;
-  // fixed point: no cell can exceed n units, so n * 2^fixbits < 2^62
-  b->fixbits = std::min(40, 62 - ilog2i(n + 1));
+  // fixed point: no cell can exceed n units, so n * 2^fixbits < 2^62.  The
+  // FP32-convolution form keeps 2^-21 of a macro charge (finer than the FP32
+  // transforms that follow), which lets the deposit sum a chunk in one word
+  b->fixbits = std::min(form == IMPZ_FORM_FP32CONV ? 21 : 40, 62 - ilog2i(n + 1));
   int rc = IMPZ_OK;
 #define ALLOC(call)                                   \
   do {                                                \

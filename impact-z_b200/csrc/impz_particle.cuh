@@ -939,7 +939,9 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
 // (sparse regions, few lanes per cell) few.  Each tile word keeps a node's
 // fixed-point sum as two 32-bit halves (the low 20 bits and the rest) so
 // that native 32-bit shared atomics suffice: a chunk of at most 2048
-// particles cannot overflow either half.  Accumulation is in int64 fixed
+// particles cannot overflow either half.  With quanta of at most 2^21 (the
+// FP32-convolution form) one word holds a chunk's sum and the high half is
+// not used.  Accumulation is in int64 fixed
 // point (2^-fixbits of a unit macro-particle charge), so the result does not
 // depend on the order of the additions; the corner with the largest weight
 // takes 2^fixbits minus the other seven (never negative), so every live
@@ -948,9 +950,10 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
 #define IMPZ_DEP_RMAX 32
 #endif
 #define IMPZ_DEP_LOBITS 20
+#define IMPZ_DEP_FIXBITS_1WORD 21
 template <int BLOCK, int U>
 __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a) {
-  static_assert(BLOCK * U <= 2048, "tile halves sized for chunks of at most 2048 particles");
+  static_assert(BLOCK * U <= 1024, "one-word tile sums sized for chunks of at most 1024");
   extern __shared__ __align__(16) unsigned int tsm[];
   unsigned int* tlo = tsm;                       // [IMPZ_DEP_TILE]
   unsigned int* thi = tsm + IMPZ_DEP_TILE;       // [IMPZ_DEP_TILE]
@@ -978,6 +981,9 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
   const double magic = 6755399441055744.0;
   const long long magic_bits = 0x4338000000000000ll;
   const unsigned lomask = (1u << IMPZ_DEP_LOBITS) - 1u;
+  // quanta of at most 2^21 (the FP32-convolution form's resolution): a
+  // chunk's sum at one node stays below 2^31 in a single word
+  const bool split = a.fixbits > IMPZ_DEP_FIXBITS_1WORD;
   const long long chunk = (long long)BLOCK * U;
   const int lane = threadIdx.x & 31;
   for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
@@ -1079,10 +1085,15 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
                       bx * (((int)((pk[u] >> 10) & 1023u) - y0) + by * ((int)(pk[u] >> 20) - z0));
         const int node[8] = {t, t + bx, t + bx + bxy, t + bxy, t + 1 + bxy, t + 1 + bx + bxy,
                              t + 1 + bx, t + 1};
+        if (split) {
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-          atomicAdd(tlo + node[k], (unsigned)(qv[k] & lomask));
-          atomicAdd(thi + node[k], (unsigned)(qv[k] >> IMPZ_DEP_LOBITS));
+          for (int k = 0; k < 8; k++) {
+            atomicAdd(tlo + node[k], (unsigned)(qv[k] & lomask));
+            atomicAdd(thi + node[k], (unsigned)(qv[k] >> IMPZ_DEP_LOBITS));
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 8; k++) atomicAdd(tlo + node[k], (unsigned)qv[k]);
         }
         atomicAdd(tcnt + t, 1u);
       }
