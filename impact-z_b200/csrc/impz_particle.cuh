@@ -1105,12 +1105,12 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
         unsigned long long q = 0ull;
         unsigned int k = 0u;
         for (int r = 0, o = e; r < R; r++, o += S) {
-          const unsigned lo = tlo[o], hi = thi[o], c = tcnt[o];
+          const unsigned lo = tlo[o], hi = split ? thi[o] : 0u, c = tcnt[o];
           if (lo | hi | c) {
             q += ((unsigned long long)hi << IMPZ_DEP_LOBITS) + (unsigned long long)lo;
             k += c;
             tlo[o] = 0u;
-            thi[o] = 0u;
+            if (split) thi[o] = 0u;
             tcnt[o] = 0u;
           }
         }
