@@ -62,10 +62,12 @@ __host__ __device__ constexpr int line_pitch(int n) { return n + n / 8 + 1; }
 // Radix-2 butterflies over `nlines` lines in shared memory; element j of
 // line l sits at buf[l*lstride + sw(j)].  tw[k] = exp(-2 pi i k / n), k < n/2.
 // DIF: natural order in, bit-reversed out.  DIT: bit-reversed in, natural out.
-// Up to three consecutive radix-2 stages act on the eight elements spaced by
-// a quarter of the widest span, so each thread runs them in registers (one
-// barrier and one shared-memory round trip per three stages); the
-// butterflies, twiddles and output order are those of plain radix-2.
+// Up to three consecutive radix-2 stages act on the 2^NS elements spaced by
+// the narrowest span, so each thread runs them in registers (one barrier and
+// one shared-memory round trip per NS stages); the butterflies, twiddles and output order are those of plain
+// radix-2.  Within a group, a stage with pair distance se uses only se
+// distinct twiddles: element e pairs at position k + (e mod se) q, so the se
+// twiddles are loaded once per stage and shared by its butterflies.
 template <typename C>
 __device__ __forceinline__ C twid(const C* tw, int idx, int sign) {
   C w = tw[idx];
@@ -73,7 +75,7 @@ __device__ __forceinline__ C twid(const C* tw, int idx, int sign) {
   return w;
 }
 
-// stages with half-spans 2^lh, 2^(lh-1), .., 2^(lh-ns+1) (DIF, ns = 1..3)
+// stages with half-spans 2^lh, 2^(lh-1), .., 2^(lh-NS+1) (DIF)
 template <typename C, int NS>
 __device__ __forceinline__ void dif_group(C* L, int o, int logn, int lh, int k, int sign,
                                           const C* tw) {
@@ -84,24 +86,24 @@ __device__ __forceinline__ void dif_group(C* L, int o, int logn, int lh, int k, 
   for (int e = 0; e < E; e++) v[e] = L[sw(o + k + e * q)];
 #pragma unroll
   for (int m = 0; m < NS; m++) {
-    const int ls = lh - m;            // this stage's half-span 2^ls
-    const int se = E >> (m + 1);      // local pair distance
-    const int tsh = logn - 1 - ls;
+    const int se = E >> (m + 1);      // pair distance; 2^(lh-m) = se * q
+    const int tsh = logn - 1 - (lh - m);
+    C w[E / 2];
+#pragma unroll
+    for (int j = 0; j < se; j++) w[j] = twid(tw, (k + j * q) << tsh, sign);
 #pragma unroll
     for (int e = 0; e < E; e++) {
       if (e & se) continue;
-      const int pos = (k + e * q) & ((1 << ls) - 1);
-      const C w = twid(tw, pos << tsh, sign);
       const C u = v[e], t = v[e + se];
       v[e] = cadd(u, t);
-      v[e + se] = cmul(csub(u, t), w);
+      v[e + se] = cmul(csub(u, t), w[e & (se - 1)]);
     }
   }
 #pragma unroll
   for (int e = 0; e < E; e++) L[sw(o + k + e * q)] = v[e];
 }
 
-// stages with half-spans 2^lh, .., 2^(lh+ns-1) (DIT)
+// stages with half-spans 2^lh, .., 2^(lh+NS-1) (DIT)
 template <typename C, int NS>
 __device__ __forceinline__ void dit_group(C* L, int o, int logn, int lh, int k, int sign,
                                           const C* tw) {
@@ -112,15 +114,15 @@ __device__ __forceinline__ void dit_group(C* L, int o, int logn, int lh, int k, 
   for (int e = 0; e < E; e++) v[e] = L[sw(o + k + e * q)];
 #pragma unroll
   for (int m = 0; m < NS; m++) {
-    const int ls = lh + m;
-    const int se = 1 << m;
-    const int tsh = logn - 1 - ls;
+    const int se = 1 << m;            // pair distance; 2^(lh+m) = se * q
+    const int tsh = logn - 1 - (lh + m);
+    C w[E / 2];
+#pragma unroll
+    for (int j = 0; j < se; j++) w[j] = twid(tw, (k + j * q) << tsh, sign);
 #pragma unroll
     for (int e = 0; e < E; e++) {
       if (e & se) continue;
-      const int pos = (k + e * q) & ((1 << ls) - 1);
-      const C w = twid(tw, pos << tsh, sign);
-      const C u = v[e], t = cmul(v[e + se], w);
+      const C u = v[e], t = cmul(v[e + se], w[e & (se - 1)]);
       v[e] = cadd(u, t);
       v[e + se] = csub(u, t);
     }
@@ -129,11 +131,20 @@ __device__ __forceinline__ void dit_group(C* L, int o, int logn, int lh, int k, 
   for (int e = 0; e < E; e++) L[sw(o + k + e * q)] = v[e];
 }
 
+// widest group: three stages (four for FP32 lines spent more registers than
+// the fewer rounds saved)
+#ifndef IMPZ_FFT_NS_F32
+#define IMPZ_FFT_NS_F32 3
+#endif
+template <typename C>
+struct MaxStages { static constexpr int value = sizeof(C) == 8 ? IMPZ_FFT_NS_F32 : 3; };
+
 template <typename C>
 __device__ void fft_dif(C* buf, int logn, int nlines, int lstride, int sign, const C* tw) {
+  constexpr int MS = MaxStages<C>::value;
   int lh = logn - 1;
   while (lh >= 0) {
-    const int ns = lh >= 2 ? 3 : lh + 1;
+    const int ns = lh + 1 >= MS ? MS : lh + 1;
     const int lper = lh - ns + 1;            // log2 of the groups per block
     const int lngl = logn - ns;              // log2 of the groups per line
     const int total = nlines << lngl;
@@ -141,7 +152,8 @@ __device__ void fft_dif(C* buf, int logn, int nlines, int lstride, int sign, con
       const int l = b >> lngl, r = b & ((1 << lngl) - 1);
       const int o = (r >> lper) << (lh + 1), k = r & ((1 << lper) - 1);
       C* Lp = buf + l * lstride;
-      if (ns == 3) dif_group<C, 3>(Lp, o, logn, lh, k, sign, tw);
+      if (MS >= 4 && ns == 4) dif_group<C, (MS >= 4 ? 4 : 1)>(Lp, o, logn, lh, k, sign, tw);
+      else if (ns == 3) dif_group<C, 3>(Lp, o, logn, lh, k, sign, tw);
       else if (ns == 2) dif_group<C, 2>(Lp, o, logn, lh, k, sign, tw);
       else dif_group<C, 1>(Lp, o, logn, lh, k, sign, tw);
     }
@@ -152,16 +164,18 @@ __device__ void fft_dif(C* buf, int logn, int nlines, int lstride, int sign, con
 
 template <typename C>
 __device__ void fft_dit(C* buf, int logn, int nlines, int lstride, int sign, const C* tw) {
+  constexpr int MS = MaxStages<C>::value;
   int lh = 0;
   while (lh < logn) {
-    const int ns = (logn - lh) >= 3 ? 3 : logn - lh;
+    const int ns = (logn - lh) >= MS ? MS : logn - lh;
     const int lngl = logn - ns;
     const int total = nlines << lngl;
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
       const int l = b >> lngl, r = b & ((1 << lngl) - 1);
       const int o = (r >> lh) << (lh + ns), k = r & ((1 << lh) - 1);
       C* Lp = buf + l * lstride;
-      if (ns == 3) dit_group<C, 3>(Lp, o, logn, lh, k, sign, tw);
+      if (MS >= 4 && ns == 4) dit_group<C, (MS >= 4 ? 4 : 1)>(Lp, o, logn, lh, k, sign, tw);
+      else if (ns == 3) dit_group<C, 3>(Lp, o, logn, lh, k, sign, tw);
       else if (ns == 2) dit_group<C, 2>(Lp, o, logn, lh, k, sign, tw);
       else dit_group<C, 1>(Lp, o, logn, lh, k, sign, tw);
     }
@@ -206,7 +220,7 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
   // load two real rows per complex line, natural order, zero padded; clear rho
   const int hy = ny / 2;
   for (int e = threadIdx.x; e < hy * n1; e += blockDim.x) {
-    const int l = e / n1, j = e - l * n1;
+    const int l = e >> d.lx, j = e & (n1 - 1);
     C z;
     z.x = 0; z.y = 0;
     if (j < nx) {
@@ -224,7 +238,7 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
   // unpack: row a = (Z(k)+conj(Z(n1-k)))/2, row b = (Z(k)-conj(Z(n1-k)))/(2i),
   // k = 0..nx, into y lines Tm[kx][y] (natural y, zero padded to 2ny)
   for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
-    const int kx = e / n2, y = e - kx * n2;
+    const int kx = e >> d.ly, y = e & (n2 - 1);
     C v;
     v.x = 0; v.y = 0;
     if (y < ny) {
@@ -246,9 +260,16 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
   fft_dif<C>(Tm, d.ly, nx + 1, tp, -1, twys);
   // store S[k][ky][kx], kx fastest
   C* Sk = S + (size_t)k * n2 * (nx + 1);
-  for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
-    const int ky = e / (nx + 1), kx = e - ky * (nx + 1);
-    Sk[e] = Tm[kx * tp + sw(bitrev(ky, d.ly))];
+  {
+    // e = ky*(nx+1) + kx walked with a carry instead of a division
+    const int w = nx + 1, dky = blockDim.x / w, dkx = blockDim.x - dky * w;
+    int ky = threadIdx.x / w, kx = threadIdx.x - ky * w;
+    for (int e = threadIdx.x; e < w * n2; e += blockDim.x) {
+      Sk[e] = Tm[kx * tp + sw(bitrev(ky, d.ly))];
+      kx += dkx;
+      ky += dky;
+      if (kx >= w) { kx -= w; ky++; }
+    }
   }
 }
 
@@ -282,7 +303,7 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
   const int kyp = ky <= ny ? ky : n2 - ky;
   const size_t gy = (size_t)(nx + 1), gz = (size_t)(nx + 1) * (ny + 1);
   for (int e = threadIdx.x; e < TKX * n3; e += blockDim.x) {
-    const int t = e / n3, pos = e - t * n3;
+    const int t = e >> d.lz, pos = e & (n3 - 1);
     if (t >= ntk) continue;
     const int kz = bitrev(pos, d.lz);
     const int kzp = kz <= nz ? kz : n3 - kz;
@@ -319,16 +340,22 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
   const int k = blockIdx.x;
   const C* Sk = S + (size_t)k * n2 * (nx + 1);
   // y lines in bit-reversed order for the DIT inverse
-  for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
-    const int ky = e / (nx + 1), kx = e - ky * (nx + 1);
-    Tm[kx * tp + sw(bitrev(ky, d.ly))] = Sk[e];
+  {
+    const int w = nx + 1, dky = blockDim.x / w, dkx = blockDim.x - dky * w;
+    int ky = threadIdx.x / w, kx = threadIdx.x - ky * w;
+    for (int e = threadIdx.x; e < w * n2; e += blockDim.x) {
+      Tm[kx * tp + sw(bitrev(ky, d.ly))] = Sk[e];
+      kx += dkx;
+      ky += dky;
+      if (kx >= w) { kx -= w; ky++; }
+    }
   }
   __syncthreads();
   fft_dit<C>(Tm, d.ly, nx + 1, tp, +1, twys);
   // C2R along x for row pairs (y, y+ny/2), y < ny/2: Z(kx) = Xa(kx) + i Xb(kx),
   // with X(n1-kx) = conj(X(kx)); placed bit-reversed for the DIT inverse
   for (int e = threadIdx.x; e < hy * n1; e += blockDim.x) {
-    const int l = e / n1, kk = e - l * n1;
+    const int l = e >> d.lx, kk = e & (n1 - 1);
     const int kxs = kk <= nx ? kk : n1 - kk;
     C xa = Tm[kxs * tp + sw(l)], xb = Tm[kxs * tp + sw(l + hy)];
     if (kk > nx) { xa.y = -xa.y; xb.y = -xb.y; }
@@ -341,7 +368,7 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
   fft_dit<C>(Z, d.lx, hy, zp, +1, twxs);
   T* ph = phi + (size_t)nx * ny * k;
   for (int e = threadIdx.x; e < nx * ny; e += blockDim.x) {
-    const int y = e / nx, x = e - y * nx;
+    const int y = e >> (d.lx - 1), x = e & (nx - 1);
     const C v = Z[(y < hy ? y : y - hy) * zp + sw(x)];
     ph[e] = y < hy ? v.x : v.y;
   }
