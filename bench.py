@@ -209,6 +209,17 @@ def run_reference(args):
     return 0
 
 
+def max_over_ranks(dist, t, device):
+    """The largest of the ranks' times (each rank's own when not distributed):
+    every multi-GPU number is the slowest replica's."""
+    if dist is None:
+        return t
+    import torch
+    tt = torch.tensor([t], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 # ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -269,11 +280,7 @@ def main():
     torch.cuda.synchronize()
     l1 = impz.kernel_launches()
     clk = clocks.stop()
-    t = ev0.elapsed_time(ev1) / 1e3
-    if dist:
-        tt = torch.tensor([t], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
+    t = max_over_ranks(dist, ev0.elapsed_time(ev1) / 1e3, "cuda")
     value = world * n * K / t
 
     # ---- per-kernel CUDA-event times: the same K steps again, every kernel
@@ -311,11 +318,7 @@ def main():
                K + 1, ctypes.byref(nrec))
     nout = ctypes.c_longlong()
     L.impz_bunch_download(b.h, hout.ctypes.data_as(impz._D), n, ctypes.byref(nout))
-    te = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([te], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
+    te = max_over_ranks(dist, time.perf_counter() - t0, "cuda")
     step_table_bytes = 2752 * (K + 2)  # sizeof(StepParams) per step
     e2e = {"value": world * n * K / te, "unit": UNIT,
            "h2d_bytes_per_step": int((72 * n + step_table_bytes) / K),
