@@ -100,6 +100,7 @@ _SIGS = {
     "impz_profile_fetch": (ctypes.c_int, [_B, _D, _LL]),
     "impz_kernel_launches": (ctypes.c_longlong, []),
     "impz_bunch_upload": (ctypes.c_int, [_B, _D, ctypes.c_longlong, ctypes.c_double, _D]),
+    "impz_bunching": (ctypes.c_int, [_B, ctypes.c_double, _D]),
     "impz_run_batch": (ctypes.c_int, [ctypes.POINTER(_B), ctypes.POINTER(_E),
                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
     "impz_run_begin": (ctypes.c_int, [_B, _E, ctypes.c_int]),
@@ -338,6 +339,13 @@ class Bunch:
                                   cnt.ctypes.data_as(_I) if cnt is not None else None),
                "impz_deposit")
         return rho, cnt
+
+    def bunching(self, wavenumber):
+        """(1/N) sum exp(-i k z) of the live particles (complex); abs() is the
+        bunching factor at wavenumber k [1/m]."""
+        out = np.zeros(2)
+        _check(lib().impz_bunching(self.h, wavenumber, _dp(out)), "impz_bunching")
+        return complex(out[0], out[1])
 
     def poisson(self, want_phi=True):
         phi = np.zeros(int(np.prod(self.grid))) if want_phi else None

@@ -110,9 +110,11 @@ def fodo(periods=10, gradient=20.0, ldrift=0.1, lquad=0.1, nseg=4, mapstp=1, rad
     return out
 
 
-def chicane(angle_deg=3.0, lbend=0.2, ldrift_in=20.0, ldrift_mid=1.0, ldrift_c=0.5, nseg_bend=8,
-            nseg_drift=4, drift_steps_in=400, half_gap=0.01):
-    """20 m of drift then a 4-dipole chicane (+a, -a, -a, +a sector bends).
+def chicane(angle_deg=3.0, lbend=0.2, ldrift_in=20.0, ldrift_mid=3.5, ldrift_c=0.5, nseg_bend=8,
+            nseg_drift=4, drift_steps_in=756, half_gap=0.01):
+    """20 m of drift then a 4-dipole chicane (+a, -a, -a, +a sector bends);
+    800 steps by default.  R56 = -2 a^2 (ldrift_mid + 2 lbend / 3) is about
+    -20 mm for 3 degree bends 3.5 m apart.
     Dipole deck values: v1 angle[rad], v2 k1, v3 file ID (150: z map + SC,
     no CSR), v4 half gap (Dipole.f90:19-31, AccSimulator.f90:1060-1074)."""
     from . import elem

@@ -71,6 +71,33 @@ __global__ void k_e4_to_grid(const void* e4, int f32, long long G, int c, double
     out[i] = f32 ? (double)((const float*)e4)[4 * i + c] : ((const double*)e4)[4 * i + c];
 }
 
+// per-block sums of cos(kz * phase) and sin(kz * phase) (bunching factor)
+__global__ void __launch_bounds__(256) k_bunching(const double* __restrict__ ph, long long n,
+                                                  double kz, double* part) {
+  __shared__ double sc[8], ss[8];
+  double c = 0.0, s = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double si, co;
+    sincos(kz * ph[i], &si, &co);
+    c += co;
+    s += si;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { sc[wid] = c; ss[wid] = s; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tc = 0.0, ts = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { tc += sc[w]; ts += ss[w]; }
+    part[2 * blockIdx.x] = tc;
+    part[2 * blockIdx.x + 1] = ts;
+  }
+}
+
 __global__ void k_to_double(const float* in, long long n, double scale, double* out) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -713,6 +740,38 @@ int impz_bunch_info(impz_bunch_t b, double info[11]) {
   for (int c = 0; c < 6; c++) info[3 + c] = b->refptcl[c];
   info[9] = b->z;
   info[10] = (double)b->bytes;
+  return IMPZ_OK;
+}
+
+int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]) {
+  if (!b || !out) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  DevState hs;
+  CK(cudaMemcpyAsync(&hs, b->st, sizeof(hs), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  out[0] = out[1] = 0.0;
+  if (hs.nlocal < 1) return IMPZ_OK;
+  // z = -phase * beta0 * Scxl, so k z = kz * phase
+  const double gam0 = -b->refptcl[5];
+  const double beta0 = std::sqrt(1.0 - 1.0 / (gam0 * gam0));
+  const double kz = -wavenumber * beta0 * b->P.Scxl;
+  const int nb = (int)std::min<long long>((hs.nlocal + 255) / 256, kMaxAdvGrid);
+  // the push's partial-sum scratch is free between calls
+  k_bunching<<<nb, 256, 0, b->stream>>>(b->pbuf[b->parity][4], hs.nlocal, kz, b->mom_part);
+  CK(cudaGetLastError());
+  g_launches += 1;
+  std::vector<double> part((size_t)2 * nb);
+  CK(cudaMemcpyAsync(part.data(), b->mom_part, part.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  double c = 0.0, sn = 0.0;
+  for (int i = 0; i < nb; i++) {
+    c += part[2 * i];
+    sn += part[2 * i + 1];
+  }
+  // (1/N) sum exp(-i k z) = (sum cos - i sum sin) / N
+  out[0] = c / (double)hs.nlocal;
+  out[1] = -sn / (double)hs.nlocal;
   return IMPZ_OK;
 }
 

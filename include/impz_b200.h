@@ -93,6 +93,11 @@ int impz_bunch_destroy(impz_bunch_t b);
  * No reference counterpart (the reference allocates per process). */
 long long impz_bunch_footprint(long long n, int nx, int ny, int nz, int form, int flags,
                                int nsteps);
+/* Bunching factor of the live particles at wavenumber k [1/m]:
+ * out[0] + i out[1] = (1/N) sum_j exp(-i k z_j), z_j = -phase_j beta0 Scxl
+ * their longitudinal position; |out| is the bunching factor.  No reference
+ * counterpart (a diagnostic of the chicane study on this path). */
+int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]);
 /* Current, Npt, Nptlocal, refptcl(1..6), z, device bytes (11 doubles). */
 int impz_bunch_info(impz_bunch_t b, double info[11]);
 /* The bunch's CUDA stream (cudaStream_t) for callers that interleave work. */
