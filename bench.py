@@ -230,14 +230,21 @@ def main():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true")
-    ap.add_argument("--workload", default="fodo", choices=["fodo", "chicane"],
-                    help="fodo: the headline 4e6-proton line; chicane: 5e7 electrons, 64x64x2048")
+    ap.add_argument("--workload", default="fodo", choices=["fodo", "chicane", "scan", "serve"],
+                    help="fodo: the headline 4e6-proton line; chicane: 5e7 electrons, "
+                         "64x64x2048; scan: 256 bunches batched; serve: Poisson job stream")
+    ap.add_argument("--jobs", type=int, default=0, help="scan/serve: number of bunches or jobs")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "chicane":
         return run_chicane(args)
+    if args.workload == "scan":
+        return run_scan(args)
+    if args.workload == "serve":
+        return run_serve(args)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -431,6 +438,118 @@ def run_chicane(args):
                        "form": "fp32-convolution"},
             "clocks": clk, "bunching_10um": {"before": b0, "after": b1},
             "live_particles": info["nlocal"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_scan(args):
+    """The batched parameter scan: 256 independent proton bunches (N
+    log-uniform in [1e4, 2e6], grids 16^3 / 32x32x64 / 64x64x128, gradient and
+    current drawn per bunch, 25 FODO periods = 400 steps), all advanced
+    together by impz_run_batch, against the same bunches run one after the
+    other.  Wall clock around each (the calls are synchronous)."""
+    import torch
+    impz = impz_pkg()
+    from impz_b200 import beams
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    impz.lib().impz_set_device(local)
+    jobs = beams.scan_jobs(nbunch=args.jobs or 256)
+    data = [beams.make_scan_bunch(j) for j in jobs]
+    bunches = [impz.Bunch(p, j["current"], beams.PROTON_MASS_EV, 1.0, 402.5e6, r, j["grid"],
+                          form=impz.FORM_FP32CONV, track_ids=False)
+               for j, (p, r) in zip(jobs, data)]
+    lats = [j["lattice"] for j in jobs]
+    work = sum(j["n"] * impz.count_steps(j["lattice"]) for j in jobs)
+    warm = [beams.fodo_steps(args.warmup, nseg=4)] * len(jobs)
+    impz.run_batch(bunches, warm)
+
+    def reload():
+        for b, j, (p, r) in zip(bunches, jobs, data):
+            b.upload(p, j["current"], r)
+        torch.cuda.synchronize()
+
+    reload()
+    t0 = time.perf_counter()
+    impz.run_batch(bunches, lats)
+    tb = time.perf_counter() - t0
+    reload()
+    t0 = time.perf_counter()
+    for b, lat in zip(bunches, lats):
+        b.run(lat)
+    ts = time.perf_counter() - t0
+    for b in bunches:
+        b.close()
+    line = {"metric": METRIC, "value": work / tb, "unit": UNIT, "n_gpus": 1,
+            "steps": int(sum(impz.count_steps(l) for l in lats)), "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (Philox-seeded Gaussian)",
+            "config": {"workload": "batched scan: %d proton bunches, %d particles in all, "
+                                   "400 steps each" % (len(jobs), sum(j["n"] for j in jobs)),
+                       "form": "fp32-convolution", "timing": "wall clock, synchronous calls"},
+            "batched_s": tb, "one_by_one_s": ts, "one_by_one_value": work / ts,
+            "batch_speedup": ts / tb}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(args):
+    """The served stream: jobs arrive as a Poisson process (`--rate` per s),
+    N log-uniform in [1e4, 4e6], grids 32^3 / 64^3 / 64x64x128, 100-2000
+    FODO steps; the serving loop admits them under a 160 GB HBM budget.
+    Reports the particle-steps/s over the whole stream and the p50/p99 job
+    latency from submission to completion."""
+    import threading as th
+    import torch
+    impz = impz_pkg()
+    from impz_b200 import beams
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    impz.lib().impz_set_device(local)
+    jobs = beams.serve_jobs(args.jobs or 100, args.rate)
+    data = [beams.gaussian_bunch(j["n"], seed=j["seed"]) for j in jobs]
+    work = sum(j["n"] * impz.count_steps(j["lattice"]) for j in jobs)
+    budget = 160e9
+    with impz.Server(budget_bytes=budget, max_active=64) as srv:
+        # warm-up job (kernels loaded, graphs instantiated once)
+        p, r = beams.gaussian_bunch(20_000)
+        srv.wait(srv.submit(p, 0.03, beams.PROTON_MASS_EV, 1.0, 402.5e6, r, (32, 32, 32),
+                            beams.fodo_steps(args.warmup, nseg=4)))
+        ids = [None] * len(jobs)
+        t0 = time.perf_counter()
+
+        def feeder():
+            for i, (j, (pp, rr)) in enumerate(zip(jobs, data)):
+                delay = t0 + j["arrival"] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                ids[i] = srv.submit(pp, 0.03, beams.PROTON_MASS_EV, 1.0, 402.5e6, rr, j["grid"],
+                                    j["lattice"])
+
+        f = th.Thread(target=feeder)
+        f.start()
+        lat = []
+        for i in range(len(jobs)):
+            while ids[i] is None:
+                time.sleep(0.001)
+            recs, latency, queued, measured = srv.wait(ids[i])
+            lat.append(latency)
+        f.join()
+        span = time.perf_counter() - t0
+        st = srv.stats()
+    lat = np.array(lat)
+    line = {"metric": METRIC, "value": work / span, "unit": UNIT, "n_gpus": 1,
+            "steps": int(sum(impz.count_steps(j["lattice"]) for j in jobs)),
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (Philox-seeded Gaussian)",
+            "config": {"workload": "served stream: %d proton jobs, Poisson arrivals at %g/s, "
+                                   "160 GB budget" % (len(jobs), args.rate),
+                       "form": "fp32-convolution", "timing": "wall clock from the first arrival"},
+            "latency_s": {"p50": float(np.percentile(lat, 50)),
+                          "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "span_s": span, "peak_admitted_bytes": st["peak_admitted_bytes"],
+            "completed": st["completed"], "failed": st["failed"]}
     print(json.dumps(line), flush=True)
     return 0
 
