@@ -190,7 +190,7 @@ struct impz_bunch_s {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t stream2 = nullptr;   // Green-function build, overlapped with the deposit
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_dep = nullptr;
   bool serial_green = false;
   int form = 0, flags = 0;
   long long cap = 0;
@@ -398,8 +398,9 @@ int solve_efield(impz_bunch_t b) {
 // function depends only on this step's grid geometry, so it is built on the
 // second stream while the deposit and the forward transforms run.
 int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
-  // The Green build stays on the main stream with IMPZ_SERIAL_GREEN=1 and
-  // while profiling, so the kernel-group intervals are disjoint.
+  // The Green build and the scan stay on the main stream with
+  // IMPZ_SERIAL_GREEN=1 and while profiling, so the kernel-group intervals
+  // are disjoint.
   const bool serial = b->serial_green || b->prof_on;
   cudaStream_t gs = serial ? b->stream : b->stream2;
   if (!serial) {
@@ -408,16 +409,22 @@ int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
   }
   int r = solve_green(b, gs);
   if (r) return r;
-  if (!serial) CK(cudaEventRecord(b->ev_join, b->stream2));
   DepositArgs d = deposit_args(b, table, fixed);
   {
     ProfScope ps(b, IMPZ_PROF_DEPOSIT, 1);
     CK(exact::launch_deposit(d, b->grid_dep, b->stream));
   }
-  {
-    ProfScope ps(b, IMPZ_PROF_SCAN, 1);
-    CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
+  // the scan of the counts is needed only by the push: on the second stream
+  // it runs beside the forward transform
+  if (!serial) {
+    CK(cudaEventRecord(b->ev_dep, b->stream));
+    CK(cudaStreamWaitEvent(b->stream2, b->ev_dep, 0));
   }
+  {
+    ProfScope ps(b, IMPZ_PROF_SCAN, 1, gs);
+    CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, gs));
+  }
+  if (!serial) CK(cudaEventRecord(b->ev_join, b->stream2));
   PoissonBuffers pb = poisson_of(b);
   {
     ProfScope ps(b, IMPZ_PROF_CONV, 1);
@@ -532,6 +539,7 @@ void free_bunch(impz_bunch_t b) {
   if (b->stream2) cudaStreamSynchronize(b->stream2);
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   if (b->ev_join) cudaEventDestroy(b->ev_join);
+  if (b->ev_dep) cudaEventDestroy(b->ev_dep);
   if (b->stream2) cudaStreamDestroy(b->stream2);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -636,6 +644,7 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
   ALLOC(cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking));
   ALLOC(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
   ALLOC(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+  ALLOC(cudaEventCreateWithFlags(&b->ev_dep, cudaEventDisableTiming));
   const Layout L = plan_layout(n, nx, ny, nz, form, flags);
   ALLOC(cudaMalloc((void**)&b->arena, L.total));
   char* base = b->arena;

@@ -25,6 +25,19 @@ static size_t xy_smem(int nx, int ny) {
          ((size_t)(ny / 2) * line_pitch(2 * nx) + (size_t)(nx + 1) * line_pitch(2 * ny) + nx +
           ny);
 }
+#ifndef IMPZ_XY_PARTS
+#define IMPZ_XY_PARTS 1
+#endif
+#ifndef IMPZ_XY_THREADS
+#define IMPZ_XY_THREADS 512
+#endif
+template <typename T>
+static size_t xyf_smem(int nx, int ny, int parts) {
+  return sizeof(typename Cplx<T>::type) *
+         ((size_t)(ny / 2) * line_pitch(2 * nx) +
+          (size_t)((nx + 1 + parts - 1) / parts) * line_pitch(2 * ny) + nx + ny);
+}
+
 // largest dynamic shared memory one block may opt into on this device
 static size_t smem_optin() {
   int dev = 0, v = 0;
@@ -62,7 +75,8 @@ bool poisson_fits(int nx, int ny, int nz) {
   const size_t lim = smem_optin();
   int nmax = nx > ny ? nx : ny;
   nmax = nmax > nz ? nmax : nz;
-  return xy_smem<T>(nx, ny) <= lim && z_smem<T>(nz, 1) <= lim && dct_smem<T>(nmax, 2) <= lim;
+  return xy_smem<T>(nx, ny) <= lim && xyf_smem<T>(nx, ny, 1) <= lim && z_smem<T>(nz, 1) <= lim &&
+         dct_smem<T>(nmax, 2) <= lim;
 }
 
 template <typename K>
@@ -150,11 +164,13 @@ cudaError_t launch_conv_forward(const PoissonBuffers& b, cudaStream_t s) {
   typedef typename Cplx<T>::type C;
   const PoissonDims d = dims_of(b);
   cudaError_t e;
-  const size_t sxy = xy_smem<T>(b.nx, b.ny);
-  if ((e = allow_smem(k_fft_xy_fwd<T>, sxy)) != cudaSuccess) return e;
-  k_fft_xy_fwd<T><<<b.nz, 512, sxy, s>>>(d, b.rho, b.st, b.qscale, (C*)b.spec,
-                                         (const C*)b.twx, (const C*)b.twy);
-  return cudaGetLastError();
+  const size_t sm = xyf_smem<T>(b.nx, b.ny, IMPZ_XY_PARTS);
+  if ((e = allow_smem(k_fft_xy_fwd<T, IMPZ_XY_PARTS>, sm)) != cudaSuccess) return e;
+  k_fft_xy_fwd<T, IMPZ_XY_PARTS><<<dim3(IMPZ_XY_PARTS, b.nz), IMPZ_XY_THREADS, sm, s>>>(
+      d, b.rho, b.qscale, (C*)b.spec, (const C*)b.twx, (const C*)b.twy);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  // the next deposit accumulates into a cleared charge grid
+  return cudaMemsetAsync(b.rho, 0, (size_t)b.nx * b.ny * b.nz * sizeof(unsigned long long), s);
 }
 
 template <typename T>

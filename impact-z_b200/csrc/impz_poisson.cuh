@@ -196,49 +196,50 @@ struct PoissonDims {
 };
 
 // ---------------------------------------------------------------------
-// xy-forward: one block per z plane k < nz.
-// smem: Z[ny/2][2nx] (packed row pairs) and Tm[nx+1][2ny+1] (y lines).
-template <typename T>
-__global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho,
-                             const DevState* st, double qscale,
-                             typename Cplx<T>::type* __restrict__ S,
+// xy-forward: PARTS blocks per z plane k < nz (one by default: splitting a
+// plane measured slower at 64x64).  Each block transforms all the plane's
+// rows along x and then unpacks, transforms along y and stores its own share
+// of the nx+1 kx lines.  The charge is cleared by the caller after the pass
+// (a memset, not stores interleaved with the transform's loads).
+// smem: Z[ny/2][2nx] (packed row pairs) and Tm[own kx][2ny] (y lines).
+template <typename T, int PARTS>
+__global__ void k_fft_xy_fwd(PoissonDims d, const unsigned long long* __restrict__ rho,
+                             double qscale, typename Cplx<T>::type* __restrict__ S,
                              const typename Cplx<T>::type* __restrict__ twx,
                              const typename Cplx<T>::type* __restrict__ twy) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int nx = d.nx, ny = d.ny, n1 = 2 * nx, n2 = 2 * ny;
+  const int nx = d.nx, ny = d.ny, n1 = 2 * nx, n2 = 2 * ny, w = nx + 1;
   const int zp = line_pitch(n1), tp = line_pitch(n2);  // x-line and y-line pitches
+  const int hy = ny / 2;
+  const int part = blockIdx.x, k = blockIdx.y;
+  const int kx_lo = w * part / PARTS, nown = w * (part + 1) / PARTS - kx_lo;
   C* Z = reinterpret_cast<C*>(smem_raw);
-  C* Tm = Z + (ny / 2) * zp;
-  C* twxs = Tm + (nx + 1) * tp;
+  C* Tm = Z + hy * zp;
+  C* twxs = Tm + ((w + PARTS - 1) / PARTS) * tp;
   C* twys = twxs + n1 / 2;
   stage_tw(twxs, twx, n1);
   stage_tw(twys, twy, n2);
-  const int k = blockIdx.x;
   const size_t plane = (size_t)nx * ny * k;
-  (void)st;
-  // load two real rows per complex line, natural order, zero padded; clear rho
-  const int hy = ny / 2;
+  // load two real rows per complex line, natural order, zero padded
   for (int e = threadIdx.x; e < hy * n1; e += blockDim.x) {
     const int l = e >> d.lx, j = e & (n1 - 1);
     C z;
     z.x = 0; z.y = 0;
     if (j < nx) {
       const size_t ia = plane + (size_t)l * nx + j, ib = plane + (size_t)(l + hy) * nx + j;
-      const long long qa = (long long)rho[ia], qb = (long long)rho[ib];
-      z.x = (T)((double)qa * qscale);
-      z.y = (T)((double)qb * qscale);
-      rho[ia] = 0ull;
-      rho[ib] = 0ull;
+      z.x = (T)((double)(long long)rho[ia] * qscale);
+      z.y = (T)((double)(long long)rho[ib] * qscale);
     }
     Z[l * zp + sw(j)] = z;
   }
   __syncthreads();
   fft_dif<C>(Z, d.lx, hy, zp, -1, twxs);
   // unpack: row a = (Z(k)+conj(Z(n1-k)))/2, row b = (Z(k)-conj(Z(n1-k)))/(2i),
-  // k = 0..nx, into y lines Tm[kx][y] (natural y, zero padded to 2ny)
-  for (int e = threadIdx.x; e < (nx + 1) * n2; e += blockDim.x) {
-    const int kx = e >> d.ly, y = e & (n2 - 1);
+  // own kx, into y lines Tm[kx - kx_lo][y] (natural y, zero padded to 2ny)
+  for (int e = threadIdx.x; e < nown * n2; e += blockDim.x) {
+    const int kl = e >> d.ly, y = e & (n2 - 1);
+    const int kx = kx_lo + kl;
     C v;
     v.x = 0; v.y = 0;
     if (y < ny) {
@@ -254,21 +255,20 @@ __global__ void k_fft_xy_fwd(PoissonDims d, unsigned long long* __restrict__ rho
         v.y = (T)0.5 * (zm.x - zk.x);
       }
     }
-    Tm[kx * tp + sw(y)] = v;
+    Tm[kl * tp + sw(y)] = v;
   }
   __syncthreads();
-  fft_dif<C>(Tm, d.ly, nx + 1, tp, -1, twys);
-  // store S[k][ky][kx], kx fastest
-  C* Sk = S + (size_t)k * n2 * (nx + 1);
+  fft_dif<C>(Tm, d.ly, nown, tp, -1, twys);
+  // store S[k][ky][kx] for the own kx, (ky, kl) walked with a carry
+  C* Sk = S + (size_t)k * n2 * w + kx_lo;
   {
-    // e = ky*(nx+1) + kx walked with a carry instead of a division
-    const int w = nx + 1, dky = blockDim.x / w, dkx = blockDim.x - dky * w;
-    int ky = threadIdx.x / w, kx = threadIdx.x - ky * w;
-    for (int e = threadIdx.x; e < w * n2; e += blockDim.x) {
-      Sk[e] = Tm[kx * tp + sw(bitrev(ky, d.ly))];
-      kx += dkx;
+    const int dky = blockDim.x / nown, dkl = blockDim.x - dky * nown;
+    int ky = threadIdx.x / nown, kl = threadIdx.x - ky * nown;
+    for (int e = threadIdx.x; e < nown * n2; e += blockDim.x) {
+      Sk[(size_t)ky * w + kl] = Tm[kl * tp + sw(bitrev(ky, d.ly))];
+      kl += dkl;
       ky += dky;
-      if (kx >= w) { kx -= w; ky++; }
+      if (kl >= nown) { kl -= nown; ky++; }
     }
   }
 }
