@@ -101,6 +101,7 @@ _SIGS = {
     "impz_kernel_launches": (ctypes.c_longlong, []),
     "impz_bunch_upload": (ctypes.c_int, [_B, _D, ctypes.c_longlong, ctypes.c_double, _D]),
     "impz_bunching": (ctypes.c_int, [_B, ctypes.c_double, _D]),
+    "impz_run_reference": (ctypes.c_int, [_B, _D, ctypes.c_int, _I]),
     "impz_run_batch": (ctypes.c_int, [ctypes.POINTER(_B), ctypes.POINTER(_E),
                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
     "impz_run_begin": (ctypes.c_int, [_B, _E, ctypes.c_int]),
@@ -339,6 +340,15 @@ class Bunch:
                                   cnt.ctypes.data_as(_I) if cnt is not None else None),
                "impz_deposit")
         return rho, cnt
+
+    def run_reference(self):
+        """refptcl at each record of the last run, shape (records, 6)."""
+        nrec = ctypes.c_int()
+        lib().impz_run_reference(self.h, None, 0, ctypes.byref(nrec))
+        out = np.zeros((max(nrec.value, 1), 6))
+        _check(lib().impz_run_reference(self.h, _dp(out), nrec.value, ctypes.byref(nrec)),
+               "impz_run_reference")
+        return out[: nrec.value]
 
     def bunching(self, wavenumber):
         """(1/N) sum exp(-i k z) of the live particles (complex); abs() is the

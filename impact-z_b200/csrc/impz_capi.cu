@@ -1263,6 +1263,16 @@ int impz_run_fetch(impz_bunch_t b, double* recs, double* zs, int maxrec, int* nr
   return check_err(b);
 }
 
+int impz_run_reference(impz_bunch_t b, double* refrec, int maxrec, int* nrec) {
+  if (!b) return IMPZ_ERR_ARG;
+  const int rows = (int)(b->lat.refrec.size() / 6);
+  const int ncopy = std::min(rows, std::max(maxrec, 0));
+  if (refrec && ncopy > 0)
+    std::memcpy(refrec, b->lat.refrec.data(), (size_t)6 * ncopy * sizeof(double));
+  if (nrec) *nrec = rows;
+  return IMPZ_OK;
+}
+
 int impz_run(impz_bunch_t b, const impz_elem_t* elems, int nelem, double* recs, double* zs,
              int maxrec, int* nrec) {
   int r = impz_run_async(b, elems, nelem);

@@ -500,6 +500,8 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
   MapProgram pending;
   std::memset(&pending, 0, sizeof(pending));
   double z = *zio;
+  double ref0[6];  // the initial record's reference particle
+  std::memcpy(ref0, refptcl, sizeof(ref0));
   const bool sc_on = !(bcurr < 1.0e-10);
   for (int ie = 0; ie < nelem; ie++) {
     const impz_elem_t& e = elems[ie];
@@ -555,6 +557,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
   out.refrec.assign(6 * (K + 1), 0.0);
   // prologue: initial diagnostics, then the first half map of step 1
   out.zrec[0] = *zio;
+  std::memcpy(&out.refrec[0], ref0, sizeof(ref0));
   StepParams& p0 = out.steps[0];
   p0.moments = 1;
   p0.gam = 2.0;

@@ -1,0 +1,306 @@
+"""The reference's on-disk formats and a standalone runner over them.
+
+* `read_deck` parses ImpactZ.in as in1_Input/in2_Input do
+  (src/Contrl/Input.f90:37-385): Fortran list-directed records, lines whose
+  first token starts with "!" are comments, a "/" ends a record (the rest
+  of the line is free text, the missing values stay zero), "d" exponents.
+* `read_particles` / `write_particles`: particle.in of readin_Dist
+  (src/Appl/Distribution.f90:1666-1714): the count, then Pts1 one particle
+  per line (9 values).
+* `read_rfdata`: rfdataN.in of read1_Data (src/DataStruct/Data.f90:139-215):
+  z, Ez, Ez', Ez'' per line, z shifted to start at 0.
+* `write_diag`: fort.18 and fort.24-30 of diagnostic1_Output
+  (src/Contrl/Output.f90:341-352), one record per line; the reference
+  prints with `g0` (shortest width), here `%.17g` (the same digits).
+* `write_phase`: the phase-space dump of a type -2 element, phase_Output
+  (src/Contrl/Output.f90:1776-1855), fort.<mapstp>, every samplePeriod-th
+  particle.
+* `run_deck` runs a deck of the map integrator with open boundaries and a
+  particle.in distribution (Flagmap=1, Flagbc=1, Flagdist=19) on the GPU
+  runner, splitting the lattice at control elements (types < 0,
+  `lattice_segments`): -2 dumps phase space, -99 ends the lattice, the types
+  listed in `skip` are passed over (reported), any other is refused.
+"""
+import os
+import re
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_NUM = re.compile(r"([0-9.])[dD]([-+]?[0-9])")
+
+
+def _values(line):
+    """List-directed values of one record: text after '/' is ignored."""
+    rec = line.split("/", 1)[0]
+    rec = _NUM.sub(r"\1e\2", rec).replace(",", " ")
+    return rec.split()
+
+
+def _is_comment(line):
+    t = line.strip()
+    return t == "" or t.startswith("!")
+
+
+@dataclass
+class Element:
+    length: float
+    nseg: int
+    mapstp: int
+    type: int
+    vals: list = field(default_factory=lambda: [0.0] * 24)
+
+
+@dataclass
+class Deck:
+    npcol: int = 1
+    nprow: int = 1
+    dim: int = 6
+    np: int = 0
+    flagmap: int = 1
+    flagerr: int = 0
+    flagdiag: int = 1
+    nx: int = 0
+    ny: int = 0
+    nz: int = 0
+    flagbc: int = 1
+    xrad: float = 0.0
+    yrad: float = 0.0
+    perdlen: float = 0.0
+    flagdist: int = 19
+    restart: int = 0
+    subcycle: int = 0
+    nchrg: int = 1
+    nptlist: list = field(default_factory=list)
+    currlist: list = field(default_factory=list)
+    qmcclist: list = field(default_factory=list)
+    distparam: list = field(default_factory=lambda: [0.0] * 21)
+    bcurr: float = 0.0
+    bkenergy: float = 0.0
+    bmass: float = 0.0
+    bcharge: float = 0.0
+    bfreq: float = 0.0
+    phsini: float = 0.0
+    elements: list = field(default_factory=list)
+
+    def refptcl(self):
+        """construct_BeamBunch's reference particle (BeamBunch.f90:56-58)."""
+        r = [0.0] * 6
+        r[4] = self.phsini
+        r[5] = -(1.0 + self.bkenergy / self.bmass)
+        return np.array(r)
+
+
+def read_deck(path):
+    """ImpactZ.in -> Deck (in1_Input / in2_Input, Input.f90:37-385)."""
+    with open(path) as f:
+        lines = [ln for ln in f.read().splitlines() if not _is_comment(ln)]
+    it = iter(lines)
+
+    def record(n):
+        # list-directed: a record may continue on the next lines until n values
+        vals = []
+        while len(vals) < n:
+            ln = next(it)
+            vals += _values(ln)
+            if "/" in ln:
+                break
+        return vals + ["0"] * (n - len(vals))
+
+    d = Deck()
+    v = record(2)
+    d.npcol, d.nprow = int(v[0]), int(v[1])
+    v = record(5)
+    d.dim, d.np, d.flagmap, d.flagerr, d.flagdiag = (int(float(x)) for x in v[:5])
+    v = record(7)
+    d.nx, d.ny, d.nz, d.flagbc = (int(float(x)) for x in v[:4])
+    d.xrad, d.yrad, d.perdlen = (float(x) for x in v[4:7])
+    v = record(4)
+    d.flagdist, d.restart, d.subcycle, d.nchrg = (int(float(x)) for x in v[:4])
+    d.nptlist = [int(float(x)) for x in record(d.nchrg)[: d.nchrg]]
+    d.currlist = [float(x) for x in record(d.nchrg)[: d.nchrg]]
+    d.qmcclist = [float(x) for x in record(d.nchrg)[: d.nchrg]]
+    d.distparam = [float(x) for x in record(7)[:7] + record(7)[:7] + record(7)[:7]]
+    v = record(6)
+    d.bcurr, d.bkenergy, d.bmass, d.bcharge, d.bfreq, d.phsini = (float(x) for x in v[:6])
+    for ln in it:
+        v = _values(ln)
+        if len(v) < 4:
+            continue
+        e = Element(float(v[0]), int(float(v[1])), int(float(v[2])), int(float(v[3])))
+        vals = [float(x) for x in v[4:28]]
+        e.vals = vals + [0.0] * (24 - len(vals))
+        d.elements.append(e)
+        if e.type == -99:
+            break
+    return d
+
+
+def write_deck(path, d):
+    """A Deck as ImpactZ.in (the layout read_deck and in1_Input read)."""
+    g = lambda x: "%.17g" % x  # noqa: E731
+    out = ["! written by impz_b200.deck", "%d %d" % (d.npcol, d.nprow),
+           "%d %d %d %d %d" % (d.dim, d.np, d.flagmap, d.flagerr, d.flagdiag),
+           "%d %d %d %d %s %s %s" % (d.nx, d.ny, d.nz, d.flagbc, g(d.xrad), g(d.yrad),
+                                     g(d.perdlen)),
+           "%d %d %d %d" % (d.flagdist, d.restart, d.subcycle, d.nchrg),
+           " ".join(str(n) for n in d.nptlist), " ".join(g(c) for c in d.currlist),
+           " ".join(g(q) for q in d.qmcclist)]
+    for r in range(3):
+        out.append(" ".join(g(x) for x in d.distparam[7 * r:7 * r + 7]))
+    out.append(" ".join(g(x) for x in (d.bcurr, d.bkenergy, d.bmass, d.bcharge, d.bfreq,
+                                       d.phsini)))
+    for e in d.elements:
+        last = max([i + 1 for i, x in enumerate(e.vals) if x != 0.0] or [0])
+        out.append("%s %d %d %d %s /" % (g(e.length), e.nseg, e.mapstp, e.type,
+                                         " ".join(g(x) for x in e.vals[:last])))
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+
+
+def read_particles(path):
+    """particle.in -> Pts1 as an (n, 9) array (readin_Dist)."""
+    with open(path) as f:
+        first = f.readline()
+        n = int(float(_values(first)[0]))
+        vals = np.array(_values(f.read().replace("\n", " ")), dtype=np.float64)
+    if vals.size < 9 * n:
+        raise ValueError("particle.in holds %d values for %d particles" % (vals.size, n))
+    return vals[: 9 * n].reshape(n, 9)
+
+
+def write_particles(path, pts, sample=1):
+    """Pts1 rows as particle.in / a phase_Output dump (9(g0,1x))."""
+    pts = np.asarray(pts)[:: max(1, sample)]
+    with open(path, "w") as f:
+        f.write("%d\n" % pts.shape[0])
+        for row in pts:
+            f.write(" ".join("%.17g" % x for x in row) + "\n")
+
+
+def write_phase(path, pts, sample):
+    """phase_Output for samplePeriod >= 0: every sample-th particle, 9 values
+    per line, no count line (Output.f90:1776-1855)."""
+    pts = np.asarray(pts)[:: max(1, int(sample))]
+    with open(path, "w") as f:
+        for row in pts:
+            f.write(" ".join("%.17g" % x for x in row) + "\n")
+
+
+def read_rfdata(path):
+    """rfdataN.in -> (z, Ez, Ez', Ez'') with z shifted to start at 0."""
+    rows = []
+    with open(path) as f:
+        for ln in f:
+            v = _values(ln)
+            if len(v) >= 4:
+                rows.append([float(x) for x in v[:4]])
+    tab = np.array(rows)
+    tab[:, 0] -= tab[0, 0]
+    return tab[:, 0].copy(), tab[:, 1].copy(), tab[:, 2].copy(), tab[:, 3].copy()
+
+
+# the 45 columns of impz_diag_row: z, then the files' columns in order
+_FILES = (("fort.18", 1, 6), ("fort.24", 6, 12), ("fort.25", 12, 18), ("fort.26", 18, 24),
+          ("fort.27", 24, 30), ("fort.28", 30, 33), ("fort.29", 33, 39), ("fort.30", 39, 45))
+
+
+def write_diag(outdir, rows):
+    """fort.18 and fort.24-30 (diagnostic1_Output) from diag rows."""
+    rows = np.asarray(rows)
+    for name, a, b in _FILES:
+        with open(os.path.join(outdir, name), "w") as f:
+            for r in rows:
+                if name == "fort.28":
+                    f.write("%.17g %10d %10d %10d\n" % (r[0], int(r[30]), int(r[31]), int(r[32])))
+                else:
+                    f.write(" ".join("%.17g" % x for x in [r[0]] + list(r[a:b])) + "\n")
+
+
+def read_diag(outdir, name):
+    """One fort.* file back as an array of floats."""
+    with open(os.path.join(outdir, name)) as f:
+        return np.array([[float(x) for x in ln.split()] for ln in f if ln.strip()])
+
+
+def lattice_segments(deck, workdir, skip=()):
+    """The lattice cut at its control elements, for a runner: yields
+    ("run", [impz_elem_t]) for each stretch of beam-line elements (RF tables
+    read from workdir), ("dump", Element) for each type -2 phase dump, and
+    last ("skipped", [types]) for the control elements passed over because
+    they are in `skip`.  -99 ends the lattice; any other control element is
+    refused (ValueError)."""
+    from . import elem
+
+    def to_elem(e):
+        rf = None
+        if 101 <= e.type <= 106 and e.vals[3] >= 0.0:
+            rf = read_rfdata(os.path.join(workdir, "rfdata%d.in" % int(e.vals[3])))
+        return elem(e.type, e.length, e.nseg, e.mapstp, list(e.vals), rf=rf)
+
+    seg, skipped = [], []
+    for e in deck.elements:
+        if e.type >= 0:
+            seg.append(to_elem(e))
+            continue
+        if seg:
+            yield "run", seg
+            seg = []
+        if e.type == -99:
+            break
+        if e.type == -2:
+            yield "dump", e
+        elif e.type in skip:
+            skipped.append(e.type)
+        else:
+            raise ValueError("control element type %d is outside this path" % e.type)
+    if seg:
+        yield "run", seg
+    yield "skipped", skipped
+
+
+def check_supported(deck):
+    """The runner covers the map integrator with open boundaries, one charge
+    state and a particle.in distribution."""
+    if deck.flagmap != 1 or deck.flagbc != 1 or deck.flagdist != 19 or deck.nchrg != 1:
+        raise ValueError("this runner needs Flagmap=1, Flagbc=1, Flagdist=19 and one charge "
+                         "state (deck has %d, %d, %d, %d)" % (deck.flagmap, deck.flagbc,
+                                                             deck.flagdist, deck.nchrg))
+
+
+def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
+    """Runs ImpactZ.in + particle.in of `workdir` on the GPU and writes
+    fort.18/24-30 and the -2 phase dumps into `outdir` (default: workdir).
+    Returns {"rows": diag rows, "skipped": [types passed over], "pts": final
+    Pts1}."""
+    from . import FORM_FP64, Bunch, diag_row
+    outdir = outdir or workdir
+    deck = read_deck(os.path.join(workdir, "ImpactZ.in"))
+    check_supported(deck)
+    pts = read_particles(os.path.join(workdir, "particle.in"))
+    b = Bunch(pts, deck.bcurr, deck.bmass, deck.bcharge, deck.bfreq, deck.refptcl(),
+              (deck.nx, deck.ny, deck.nz), form=FORM_FP64 if form is None else form,
+              track_ids=True)
+    rows, skipped = [], []
+    try:
+        for kind, item in lattice_segments(deck, workdir, set(skip)):
+            if kind == "skipped":
+                skipped = item
+            elif kind == "dump":
+                if write:
+                    write_phase(os.path.join(outdir, "fort.%d" % item.mapstp), b.download(),
+                                max(1, int(item.vals[0])))
+            else:
+                recs, zs = b.run(item)
+                refs = b.run_reference()
+                seg = [diag_row(zs[i], recs[i], refs[i], deck.bmass, deck.bfreq)
+                       for i in range(len(recs))]
+                # a stretch's first record repeats the previous stretch's last
+                rows += seg[1:] if rows else seg
+        final = b.download()
+    finally:
+        b.close()
+    rows = np.array(rows)
+    if write:
+        write_diag(outdir, rows)
+    return {"rows": rows, "skipped": skipped, "pts": final}

@@ -170,6 +170,10 @@ int impz_run_advance(impz_bunch_t b, int budget, int* remaining);
 int impz_run_batch(impz_bunch_t* bunches, const impz_elem_t* const* lattices,
                    const int* nelem, int nb);
 /* Number of steps (records - 1) impz_run would take for this lattice. */
+/* refptcl(1..6) at each record of the last run (6 doubles per record, as
+ * BeamBunch%refptcl when diagnostic1_Output wrote that record), for
+ * impz_diag_row; *nrec receives the record count (refrec may be NULL). */
+int impz_run_reference(impz_bunch_t b, double* refrec, int maxrec, int* nrec);
 int impz_count_steps(const impz_elem_t* elems, int nelem);
 
 /* ---- instrumentation --------------------------------------------------- */

@@ -1,0 +1,96 @@
+"""The reference's on-disk formats (impz_b200.deck): ImpactZ.in, particle.in,
+rfdataN.in, fort.18/24-30.  The reference's own example decks are parsed
+where its source tree is present (this container); round trips of the
+writers always run.  No GPU needed."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import load_impz, load_oracle
+
+impz = load_impz()
+from impz_b200 import beams, deck  # noqa: E402
+
+EXAMPLES = "/root/reference/examples"
+have_examples = pytest.mark.skipif(not os.path.isdir(EXAMPLES),
+                                   reason="reference examples not present")
+
+
+@have_examples
+def test_reads_the_reference_example_decks():
+    d1 = deck.read_deck(os.path.join(EXAMPLES, "Example1", "ImpactZ.in"))
+    assert (d1.np, d1.flagmap, d1.flagdist, d1.nx, d1.ny, d1.nz) == (200, 2, 19, 32, 32, 64)
+    assert d1.bfreq == 324.0e6 and d1.qmcclist == [-1.064629e-9]
+    d2 = deck.read_deck(os.path.join(EXAMPLES, "Example2", "ImpactZ.in"))
+    assert (d2.np, d2.flagmap, d2.flagdist, d2.nchrg) == (160000, 1, 3, 1)
+    assert d2.bkenergy == 230.0e6 and d2.bcharge == -1.0
+    d3 = deck.read_deck(os.path.join(EXAMPLES, "Example3", "ImpactZ.in"))
+    assert (d3.np, d3.flagmap, d3.flagbc, d3.flagdist) == (3134, 1, 1, 19)
+    assert (d3.nx, d3.ny, d3.nz) == (32, 32, 32)
+    types = [e.type for e in d3.elements]
+    assert types.count(4) == 4 and types.count(103) == 5 and types.count(-41) == 10
+    bend = next(e for e in d3.elements if e.type == 4)
+    assert bend.nseg == 10 and bend.vals[2] == 150.0  # file ID: no CSR
+    # "d" exponents and text after "/" are read as the reference reads them
+    assert d3.qmcclist == [-1.95692801440299e-06] and d3.bfreq == 1.3e9
+    p = deck.read_particles(os.path.join(EXAMPLES, "Example3", "particle.in"))
+    assert p.shape == (3134, 9) and p[0, 8] == 1.0 and p[0, 6] == -1.956928e-06
+
+
+@have_examples
+def test_example3_lattice_runs_on_the_path_with_its_wake_controls_skipped():
+    """Example3 (map integrator, open BC, particle.in) maps onto the path's
+    elements once its wake (-41), laser-heater (-52) and slice-output (-8)
+    controls are passed over; the oracle runs it (138 steps)."""
+    orc = load_oracle()
+    wd = os.path.join(EXAMPLES, "Example3")
+    d = deck.read_deck(os.path.join(wd, "ImpactZ.in"))
+    deck.check_supported(d)
+    with pytest.raises(ValueError):
+        list(deck.lattice_segments(d, wd))
+    pts = deck.read_particles(os.path.join(wd, "particle.in"))
+    ref, z, nrows, skipped = d.refptcl(), 0.0, 0, None
+    for kind, item in deck.lattice_segments(d, wd, {-8, -41, -52}):
+        if kind == "run":
+            rows, pts, beam = orc.run(item, pts, d.bcurr, d.bmass, d.bcharge, d.bfreq, ref,
+                                      (d.nx, d.ny, d.nz), z)
+            ref, z = np.array(beam.refptcl[:]), beam.z
+            nrows += len(rows) - (1 if nrows else 0)
+        elif kind == "skipped":
+            skipped = item
+    assert nrows == 139 and sorted(set(skipped)) == [-52, -41, -8]
+    assert np.all(np.isfinite(pts)) and pts.shape[0] == 3134
+    assert -ref[5] * d.bmass > 1.5 * (d.bkenergy + d.bmass)  # the cavities accelerate
+
+
+def test_deck_round_trip(tmp_path):
+    d = deck.Deck(np=1000, nx=16, ny=16, nz=32, xrad=0.02, yrad=0.02, perdlen=0.1,
+                  nptlist=[1000], currlist=[0.13], qmcclist=[-1.95692801440299e-06],
+                  bcurr=0.13, bkenergy=98.169272e6, bmass=0.511005e6, bcharge=-1.0,
+                  bfreq=1.3e9)
+    d.elements = [deck.Element(0.0, 0, 1001, -2, [1.0] + [0.0] * 23),
+                  deck.Element(0.5, 4, 1, 0, [0.014] + [0.0] * 23),
+                  deck.Element(0.1, 4, 1, 1, [12.5, 0.0, 0.014] + [0.0] * 21),
+                  deck.Element(0.0, 0, 0, -99, [0.0] * 24)]
+    p = tmp_path / "ImpactZ.in"
+    deck.write_deck(str(p), d)
+    r = deck.read_deck(str(p))
+    assert r == d
+
+
+def test_particles_and_diag_files_round_trip(tmp_path):
+    pts, _ = beams.gaussian_bunch(257, seed=beams.SEED0 + 3)
+    deck.write_particles(str(tmp_path / "particle.in"), pts)
+    np.testing.assert_array_equal(deck.read_particles(str(tmp_path / "particle.in")), pts)
+    rows = np.random.default_rng(5).standard_normal((7, impz.DIAG_LEN))
+    rows[:, 30:33] = np.abs(np.round(rows[:, 30:33] * 1000))
+    deck.write_diag(str(tmp_path), rows)
+    np.testing.assert_array_equal(deck.read_diag(str(tmp_path), "fort.24"),
+                                  np.c_[rows[:, 0], rows[:, 6:12]])
+    np.testing.assert_array_equal(deck.read_diag(str(tmp_path), "fort.18"),
+                                  np.c_[rows[:, 0], rows[:, 1:6]])
+    np.testing.assert_array_equal(deck.read_diag(str(tmp_path), "fort.28"),
+                                  np.c_[rows[:, 0], rows[:, 30:33]])
+    np.testing.assert_array_equal(deck.read_diag(str(tmp_path), "fort.30"),
+                                  np.c_[rows[:, 0], rows[:, 39:45]])

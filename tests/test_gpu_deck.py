@@ -1,0 +1,81 @@
+"""The standalone deck runner on the GPU against the oracle: a deck shaped
+like the reference's Example3 (98 MeV electrons, phase dumps, drifts,
+quadrupoles, ideal-RF cavities, 150-type dipoles, a slice-output control
+that is passed over), written with impz_b200.deck, run by run_deck (FP64)
+and by the oracle over the same lattice_segments.  fort.24-30 rms columns
+within 1e-8, z exact, the phase dump holds every particle."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import load_impz, load_oracle
+
+pytestmark = pytest.mark.gpu
+
+impz = load_impz()
+orc = load_oracle()
+from impz_b200 import beams, deck  # noqa: E402
+
+RMS_COLS = [6, 7, 8, 9, 11, 12, 13, 14, 15, 17, 18, 19, 20, 21, 23]
+
+
+def example_like_deck(workdir, n=4000):
+    pts, ref = beams.gaussian_bunch(n, seed=beams.SEED0 + 41, mass=beams.ELECTRON_MASS_EV,
+                                    charge=-1.0, ekin=98.169272e6, current=0.13, freq=1.3e9,
+                                    sig_x=0.5e-3, sig_y=0.5e-3, sig_xp=0.05e-3, sig_yp=0.05e-3,
+                                    sig_phase_deg=1.0, sig_e=50e3)
+    d = deck.Deck(np=n, nx=16, ny=16, nz=32, xrad=1.0, yrad=1.0, perdlen=7.64,
+                  nptlist=[n], currlist=[0.13], qmcclist=[float(pts[0, 6])], bcurr=0.13,
+                  bkenergy=98.169272e6, bmass=beams.ELECTRON_MASS_EV, bcharge=-1.0,
+                  bfreq=1.3e9, phsini=0.0)
+    z24 = lambda *v: list(v) + [0.0] * (24 - len(v))  # noqa: E731
+    d.elements = [
+        deck.Element(0.0, 0, 201, -8, z24(101.0)),
+        deck.Element(0.0, 0, 1001, -2, z24(1.0)),
+        deck.Element(0.5, 4, 1, 0, z24(1.0)),
+        deck.Element(0.1, 4, 1, 1, z24(10.0, 0.0, 1.0)),
+        deck.Element(0.3, 4, 1, 0, z24(1.0)),
+        deck.Element(0.1, 4, 1, 1, z24(-10.0, 0.0, 1.0)),
+        deck.Element(1.037743, 4, 1, 103, z24(0.1090744783e8, 1.3e9, -17.43982832, -1.01, 1.0)),
+        deck.Element(0.124410139621, 6, 1, 4, z24(0.0221138265963, 0.0, 150, 0.03, 0.0,
+                                                   0.0221138265963, 0.0, 0.0, 0.40)),
+        deck.Element(0.5, 4, 1, 0, z24(1.0)),
+        deck.Element(0.124410139621, 6, 1, 4, z24(-0.0221138265963, 0.0, 150, 0.03,
+                                                   -0.0221138265963, 0.0, 0.0, 0.0, 0.40)),
+        deck.Element(0.0, 0, 1002, -2, z24(1.0)),
+        deck.Element(0.4, 4, 1, 0, z24(1.0)),
+        deck.Element(0.0, 0, 0, -99, z24()),
+    ]
+    deck.write_deck(os.path.join(workdir, "ImpactZ.in"), d)
+    deck.write_particles(os.path.join(workdir, "particle.in"), pts)
+    return d
+
+
+def test_deck_runner_matches_the_oracle(tmp_path):
+    wd = str(tmp_path)
+    d = example_like_deck(wd)
+    out = deck.run_deck(wd, skip={-8})
+    assert out["skipped"] == [-8]
+    # the oracle over the same segments
+    pts = deck.read_particles(os.path.join(wd, "particle.in"))
+    ref, z, rows_o = d.refptcl(), 0.0, []
+    for kind, item in deck.lattice_segments(d, wd, {-8}):
+        if kind == "run":
+            seg, pts, beam = orc.run(item, pts, d.bcurr, d.bmass, d.bcharge, d.bfreq, ref,
+                                     (d.nx, d.ny, d.nz), z)
+            ref, z = np.array(beam.refptcl[:]), beam.z
+            rows_o += list(seg[1:] if rows_o else seg)
+    rows_o = np.array(rows_o)
+    rows_g = out["rows"]
+    assert rows_g.shape == rows_o.shape
+    np.testing.assert_allclose(rows_g[:, 0], rows_o[:, 0], rtol=0, atol=0)
+    for c in RMS_COLS:
+        scale = np.max(np.abs(rows_o[:, c])) + 1e-300
+        assert np.max(np.abs(rows_g[:, c] - rows_o[:, c])) / scale <= 1e-8, c
+    # files: the diagnostics and both phase dumps
+    f24 = deck.read_diag(wd, "fort.24")
+    np.testing.assert_array_equal(f24, np.c_[rows_g[:, 0], rows_g[:, 6:12]])
+    for name in ("fort.1001", "fort.1002"):
+        dump = np.loadtxt(os.path.join(wd, name))
+        assert dump.shape == (d.np, 9)
