@@ -94,3 +94,43 @@ def test_particles_and_diag_files_round_trip(tmp_path):
                                   np.c_[rows[:, 0], rows[:, 30:33]])
     np.testing.assert_array_equal(deck.read_diag(str(tmp_path), "fort.30"),
                                   np.c_[rows[:, 0], rows[:, 39:45]])
+
+
+GUI_READER = "/root/reference/GUI/src/ImpactFile.py"
+
+
+@pytest.mark.skipif(not os.path.exists(GUI_READER), reason="reference GUI not present")
+@pytest.mark.parametrize("example", ["Example1", "Example2", "Example3"])
+def test_deck_reader_agrees_with_the_reference_gui_reader(example):
+    """The reference's own Python deck reader (GUI/src/ImpactFile.py,
+    conciseReadInput) gives the tokens of every non-comment line; the header
+    values and each element's values up to its "/" equal read_deck's."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("impactz_gui_file", GUI_READER)
+    gui = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gui)
+    path = os.path.join(EXAMPLES, example, "ImpactZ.in")
+    lines = gui.conciseReadInput(path)
+    d = deck.read_deck(path)
+    nums = lambda toks, k: [float(t) for t in toks[:k]]  # noqa: E731
+    head = [nums(lines[0], 2), nums(lines[1], 5), nums(lines[2], 7), nums(lines[3], 4),
+            nums(lines[4], d.nchrg), nums(lines[5], d.nchrg), nums(lines[6], d.nchrg),
+            nums(lines[7], 7), nums(lines[8], 7), nums(lines[9], 7), nums(lines[10], 6)]
+    mine = [[d.npcol, d.nprow], [d.dim, d.np, d.flagmap, d.flagerr, d.flagdiag],
+            [d.nx, d.ny, d.nz, d.flagbc, d.xrad, d.yrad, d.perdlen],
+            [d.flagdist, d.restart, d.subcycle, d.nchrg], d.nptlist, d.currlist, d.qmcclist,
+            d.distparam[0:7], d.distparam[7:14], d.distparam[14:21],
+            [d.bcurr, d.bkenergy, d.bmass, d.bcharge, d.bfreq, d.phsini]]
+    assert head == mine
+    elems = [toks for toks in lines[11:] if len(toks) >= 4]
+    assert len(elems) == len(d.elements)
+    for toks, e in zip(elems, d.elements):
+        vals = []
+        for t in toks:
+            if t.startswith("/"):
+                break
+            vals.append(float(t.rstrip("/")))
+            if t.endswith("/"):
+                break
+        assert vals[:4] == [e.length, e.nseg, e.mapstp, e.type]
+        assert vals[4:] == e.vals[:len(vals) - 4]
