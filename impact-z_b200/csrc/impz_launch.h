@@ -6,6 +6,26 @@
 
 namespace impz {
 
+// Launches `kernel` on `s` with programmatic stream serialization: its grid
+// may be scheduled while the stream's previous kernel drains, which hides
+// the launch gap; the kernel calls griddep_wait() before it reads what that
+// kernel wrote.
+template <typename... KP, typename... A>
+inline cudaError_t launch_pdl(void (*kernel)(KP...), dim3 grid, dim3 block, size_t smem,
+                              cudaStream_t s, A... args) {
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KP>(args)...);
+}
+
 #ifndef IMPZ_ADV_BLOCK
 #define IMPZ_ADV_BLOCK 256
 #endif

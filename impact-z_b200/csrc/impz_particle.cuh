@@ -24,6 +24,7 @@
 #include <stdint.h>
 
 #include "impz_common.h"
+#include "impz_device.cuh"
 
 #ifndef IMPZ_FASTMATH
 #define IMPZ_FASTMATH 0
@@ -626,6 +627,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   __shared__ MapProgram progs[2];  // post, pre_next
   extern __shared__ __align__(16) double mtile_dyn[];  // [BLOCK/32][32*IMPZ_MSUMS]
   __shared__ Geom sgeom;
+  griddep_wait();  // step state, geometry and field come from earlier kernels
   DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
   const StepParams* __restrict__ sp = a.steps + s;
@@ -960,6 +962,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
   unsigned int* tcnt = tsm + 2 * IMPZ_DEP_TILE;  // [IMPZ_DEP_TILE]
   __shared__ int s_box[6];
   __shared__ Geom sg;
+  griddep_wait();  // the geometry comes from the previous push
   const DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
   const double gam = a.steps[s].gam, rad = a.steps[s].rad;

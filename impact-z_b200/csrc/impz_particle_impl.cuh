@@ -22,8 +22,8 @@ template <bool F32, bool LIGHT>
 static cudaError_t launch_adv_t(const AdvanceArgs& a, int grid, cudaStream_t s) {
   cudaError_t e = adv_attr<F32, LIGHT>();
   if (e != cudaSuccess) return e;
-  k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT><<<grid, IMPZ_ADV_BLOCK, kAdvSmem, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT>, dim3(grid),
+                    dim3(IMPZ_ADV_BLOCK), kAdvSmem, s, a);
 }
 
 cudaError_t launch_advance(const AdvanceArgs& a, bool f32, bool light, int grid, cudaStream_t s) {
@@ -41,8 +41,8 @@ static cudaError_t dep_attr() {
 cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s) {
   cudaError_t e = dep_attr();
   if (e != cudaSuccess) return e;
-  k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT><<<grid, IMPZ_DEP_BLOCK, kDepSmem, s>>>(a);
-  return cudaGetLastError();
+  return launch_pdl(k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>, dim3(grid), dim3(IMPZ_DEP_BLOCK),
+                    kDepSmem, s, a);
 }
 
 cudaError_t launch_scan(int* counts, int* cursor, int* bsum, long long total, DevState* st,

@@ -124,8 +124,8 @@ static cudaError_t zconv_t(const PoissonBuffers& b, const PoissonDims& d, cudaSt
   cudaError_t e = allow_smem(k_fft_z_conv<T, TKX>, sz);
   if (e != cudaSuccess) return e;
   dim3 gz((b.nx + 1 + TKX - 1) / TKX, 2 * b.ny);
-  k_fft_z_conv<T, TKX><<<gz, 256, sz, s>>>(d, (C*)b.spec, (const T*)b.ghat, (const C*)b.twz);
-  return cudaGetLastError();
+  return launch_pdl(k_fft_z_conv<T, TKX>, gz, dim3(256), sz, s, d, (C*)b.spec,
+                    (const T*)b.ghat, (const C*)b.twz);
 }
 
 // The Green function: FP64 corners and 8-corner difference (the difference
@@ -166,11 +166,9 @@ cudaError_t launch_conv_forward(const PoissonBuffers& b, cudaStream_t s) {
   cudaError_t e;
   const size_t sm = xyf_smem<T>(b.nx, b.ny, IMPZ_XY_PARTS);
   if ((e = allow_smem(k_fft_xy_fwd<T, IMPZ_XY_PARTS>, sm)) != cudaSuccess) return e;
-  k_fft_xy_fwd<T, IMPZ_XY_PARTS><<<dim3(IMPZ_XY_PARTS, b.nz), IMPZ_XY_THREADS, sm, s>>>(
-      d, b.rho, b.qscale, (C*)b.spec, (const C*)b.twx, (const C*)b.twy);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  // the next deposit accumulates into a cleared charge grid
-  return cudaMemsetAsync(b.rho, 0, (size_t)b.nx * b.ny * b.nz * sizeof(unsigned long long), s);
+  return launch_pdl(k_fft_xy_fwd<T, IMPZ_XY_PARTS>, dim3(IMPZ_XY_PARTS, b.nz),
+                    dim3(IMPZ_XY_THREADS), sm, s, d, (const unsigned long long*)b.rho, b.qscale,
+                    (C*)b.spec, (const C*)b.twx, (const C*)b.twy);
 }
 
 template <typename T>
@@ -188,9 +186,8 @@ cudaError_t launch_conv_rest(const PoissonBuffers& b, cudaStream_t s) {
     default: e = zconv_t<T, 1>(b, d, s); break;
   }
   if (e != cudaSuccess) return e;
-  k_fft_xy_inv<T><<<b.nz, 512, sxy, s>>>(d, (const C*)b.spec, (T*)b.phi, (const C*)b.twx,
-                                         (const C*)b.twy);
-  return cudaGetLastError();
+  return launch_pdl(k_fft_xy_inv<T>, dim3(b.nz), dim3(512), sxy, s, d, (const C*)b.spec,
+                    (T*)b.phi, (const C*)b.twx, (const C*)b.twy);
 }
 
 template <typename T>
@@ -203,9 +200,8 @@ cudaError_t launch_convolve(const PoissonBuffers& b, cudaStream_t s) {
 template <typename T>
 cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s) {
   const long long G = (long long)b.nx * b.ny * b.nz;
-  k_efield<T><<<grid_for(G, 256), 256, 0, s>>>(b.nx, b.ny, b.nz, (const T*)b.phi, b.st,
-                                                (T*)b.efield);
-  return cudaGetLastError();
+  return launch_pdl(k_efield<T>, dim3(grid_for(G, 256)), dim3(256), 0, s, b.nx, b.ny, b.nz,
+                    (const T*)b.phi, (const DevState*)b.st, (T*)b.efield, b.rho);
 }
 
 template cudaError_t launch_green<double>(const PoissonBuffers&, cudaStream_t);

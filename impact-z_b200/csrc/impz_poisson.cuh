@@ -30,6 +30,7 @@
 #include <stdint.h>
 
 #include "impz_common.h"
+#include "impz_device.cuh"
 
 namespace impz {
 
@@ -199,8 +200,8 @@ struct PoissonDims {
 // xy-forward: PARTS blocks per z plane k < nz (one by default: splitting a
 // plane measured slower at 64x64).  Each block transforms all the plane's
 // rows along x and then unpacks, transforms along y and stores its own share
-// of the nx+1 kx lines.  The charge is cleared by the caller after the pass
-// (a memset, not stores interleaved with the transform's loads).
+// of the nx+1 kx lines.  The charge is cleared later, by k_efield (not by
+// stores interleaved with the transform's loads).
 // smem: Z[ny/2][2nx] (packed row pairs) and Tm[own kx][2ny] (y lines).
 template <typename T, int PARTS>
 __global__ void k_fft_xy_fwd(PoissonDims d, const unsigned long long* __restrict__ rho,
@@ -209,6 +210,7 @@ __global__ void k_fft_xy_fwd(PoissonDims d, const unsigned long long* __restrict
                              const typename Cplx<T>::type* __restrict__ twy) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  griddep_wait();
   const int nx = d.nx, ny = d.ny, n1 = 2 * nx, n2 = 2 * ny, w = nx + 1;
   const int zp = line_pitch(n1), tp = line_pitch(n2);  // x-line and y-line pitches
   const int hy = ny / 2;
@@ -280,6 +282,7 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
                              const typename Cplx<T>::type* __restrict__ twz) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  griddep_wait();
   const int nx = d.nx, ny = d.ny, nz = d.nz, n2 = 2 * ny, n3 = 2 * nz;
   const int lp = line_pitch(n3);
   C* L = reinterpret_cast<C*>(smem_raw);
@@ -328,6 +331,7 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
                              const typename Cplx<T>::type* __restrict__ twy) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  griddep_wait();
   const int nx = d.nx, ny = d.ny, n1 = 2 * nx, n2 = 2 * ny;
   const int zp = line_pitch(n1), tp = line_pitch(n2);
   const int hy = ny / 2;
@@ -467,9 +471,13 @@ __global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long 
 // ---------------------------------------------------------------------
 // kick1_BeamBunch finite differences (BeamBunch.f90:1784-2005), one rank,
 // open BC: centred inside, one-sided on the faces.  Out: {Ex,Ey,Ez,0}.
+// Also clears the charge grid (its last reader, the forward transform, is
+// done) for the next deposit.
 template <typename T>
 __global__ void k_efield(int nx, int ny, int nz, const T* __restrict__ phi,
-                         const DevState* st, T* __restrict__ E) {
+                         const DevState* st, T* __restrict__ E,
+                         unsigned long long* __restrict__ rho) {
+  griddep_wait();
   const long long G = (long long)nx * ny * nz;
   const T hxi = (T)st->geom.hi[0], hyi = (T)st->geom.hi[1], hzi = (T)st->geom.hi[2];
   const T half = (T)0.5;
@@ -489,6 +497,7 @@ __global__ void k_efield(int nx, int ny, int nz, const T* __restrict__ phi,
     if (k == 0) ez = hzi * (phi[e] - phi[e + sz]);
     else if (k == nz - 1) ez = hzi * (phi[e - sz] - phi[e]);
     else ez = half * hzi * (phi[e - sz] - phi[e + sz]);
+    rho[e] = 0ull;  // the next deposit accumulates into a cleared charge grid
     T* o = E + 4 * e;
     o[0] = ex;
     o[1] = ey;
