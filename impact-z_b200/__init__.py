@@ -101,6 +101,8 @@ _SIGS = {
     "impz_kernel_launches": (ctypes.c_longlong, []),
     "impz_bunch_upload": (ctypes.c_int, [_B, _D, ctypes.c_longlong, ctypes.c_double, _D]),
     "impz_bunching": (ctypes.c_int, [_B, ctypes.c_double, _D]),
+    "impz_wake_set": (ctypes.c_int, [_B, _D, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+    "impz_wake_off": (ctypes.c_int, [_B]),
     "impz_run_reference": (ctypes.c_int, [_B, _D, ctypes.c_int, _I]),
     "impz_run_batch": (ctypes.c_int, [ctypes.POINTER(_B), ctypes.POINTER(_E),
                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
@@ -124,7 +126,7 @@ _SIGS = {
     "impz_server_destroy": (ctypes.c_int, [_B]),
 }
 
-PROF_NAMES = ("deposit", "scan", "green", "convolve", "efield", "push")
+PROF_NAMES = ("deposit", "scan", "green", "convolve", "efield", "push", "wake")
 
 
 def kernel_launches():
@@ -356,6 +358,20 @@ class Bunch:
         out = np.zeros(2)
         _check(lib().impz_bunching(self.h, wavenumber, _dp(out)), "impz_bunching")
         return complex(out[0], out[1])
+
+    def wake(self, table, scale=1.0, transverse=False):
+        """Read-in wakefield on for the space-charge steps that follow (a
+        type -41 element with Param(4) > 0): table rows (z, Ez wake, x wake,
+        y wake) as in rfdataN.in, scale = Param(2), transverse False when
+        Param(4) < 10."""
+        t = np.ascontiguousarray(table, dtype=np.float64)
+        if t.ndim != 2 or t.shape[1] != 4:
+            raise ValueError("wake table: rows of (z, Ez, Ex, Ey) wake")
+        _check(lib().impz_wake_set(self.h, _dp(t), t.shape[0], float(scale),
+                                   int(bool(transverse))), "impz_wake_set")
+
+    def wake_off(self):
+        _check(lib().impz_wake_off(self.h), "impz_wake_off")
 
     def poisson(self, want_phi=True):
         phi = np.zeros(int(np.prod(self.grid))) if want_phi else None

@@ -244,6 +244,16 @@ struct impz_bunch_s {
   const StepParams* g_steps[2] = {nullptr, nullptr};
   const double* g_mom[2] = {nullptr, nullptr};
   bool g_light[2] = {false, false};  // which particle pass the graph holds
+  int g_wake[2] = {-1, -1};          // wake generation the graph holds
+  // read-in wakefield (impz_wake_set): table [3][ntab], then the line sums
+  // [3][nz] and the per-plane field [3][nz] in one allocation
+  bool wk_on = false, wk_tr = false;
+  int wk_ntab = 0, wk_gen = 0, wk_fixbits = 40, grid_wake = 1;
+  double wk_hwk = 0.0, wk_scale = 1.0;
+  char* wk_mem = nullptr;
+  double* wk_tab = nullptr;
+  unsigned long long* wk_line = nullptr;
+  double* wk_field = nullptr;
   int h_step0 = 0;
   int run_next = 0;       // next step of the run in progress
   double run_z = 0;       // z and refptcl at the end of the run in progress
@@ -297,6 +307,7 @@ PoissonBuffers poisson_of(impz_bunch_t b) {
   pb.twx = b->tw[0]; pb.twy = b->tw[1]; pb.twz = b->tw[2];
   pb.tw64x = b->tw64[0]; pb.tw64y = b->tw64[1]; pb.tw64z = b->tw64[2];
   pb.st = b->st;
+  pb.wake = b->wk_on ? b->wk_field : nullptr;
   return pb;
 }
 
@@ -370,6 +381,28 @@ DepositArgs deposit_args(impz_bunch_t b, const StepParams* table, int fixed) {
   return d;
 }
 
+WakeArgs wake_args(impz_bunch_t b, const StepParams* table, int fixed) {
+  WakeArgs w;
+  std::memset(&w, 0, sizeof(w));
+  for (int c = 0; c < 6; c++) w.in[c] = b->pbuf[b->parity][c];
+  w.steps = table;
+  w.st = b->st;
+  w.fixed_step = fixed;
+  w.nz = b->nz;
+  w.fixbits = b->wk_fixbits;
+  w.transverse = b->wk_tr ? 1 : 0;
+  w.ntab = b->wk_ntab;
+  w.line = b->wk_line;
+  w.table = b->wk_tab;
+  w.wfield = b->wk_field;
+  w.hwk = b->wk_hwk;
+  w.scale = b->wk_scale;
+  w.unit = b->f32() ? b->weight : 1.0;
+  w.xl = b->P.Scxl;
+  w.k = b->k;
+  return w;
+}
+
 int solve_green(impz_bunch_t b, cudaStream_t s) {
   ProfScope ps(b, IMPZ_PROF_GREEN, 5, s);
   PoissonBuffers pb = poisson_of(b);
@@ -425,6 +458,10 @@ int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
     CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, gs));
   }
   if (!serial) CK(cudaEventRecord(b->ev_join, b->stream2));
+  if (b->wk_on) {
+    ProfScope ps(b, IMPZ_PROF_WAKE, 2);
+    CK(exact::launch_wake(wake_args(b, table, fixed), b->grid_wake, b->stream));
+  }
   PoissonBuffers pb = poisson_of(b);
   {
     ProfScope ps(b, IMPZ_PROF_CONV, 1);
@@ -533,6 +570,7 @@ void free_bunch(impz_bunch_t b) {
   if (b->stream2) cudaStreamSynchronize(b->stream2);
   if (b->arena) cudaFree(b->arena);
   if (b->tables) cudaFree(b->tables);
+  if (b->wk_mem) cudaFree(b->wk_mem);
   for (cudaEvent_t e : b->ev_pool) cudaEventDestroy(e);
   for (int p = 0; p < 2; p++)
     if (b->gexec[p]) cudaGraphExecDestroy(b->gexec[p]);
@@ -781,6 +819,62 @@ int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]) {
   // (1/N) sum exp(-i k z) = (sum cos - i sum sin) / N
   out[0] = c / (double)hs.nlocal;
   out[1] = -sn / (double)hs.nlocal;
+  return IMPZ_OK;
+}
+
+int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, int transverse) {
+  if (!b || !table || ntab < 2) return IMPZ_ERR_ARG;
+  // read1wk_Data shifts z to start at 0; hwk = zdatwk(2) - zdatwk(1)
+  const double hwk = (table[4] - table[0]) - (table[0] - table[0]);
+  if (!(hwk > 0.0) || b->nz < 2 || b->nz > 4096) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  CK(exact::prepare_wake());  // outside any stream capture
+  const size_t tab_bytes = round_up((size_t)3 * ntab * sizeof(double), kAlign);
+  const size_t line_bytes = round_up((size_t)3 * b->nz * sizeof(unsigned long long), kAlign);
+  const size_t bytes = tab_bytes + line_bytes + (size_t)3 * b->nz * sizeof(double);
+  std::vector<double> cols((size_t)3 * ntab);
+  for (int i = 0; i < ntab; i++)
+    for (int c = 0; c < 3; c++) cols[(size_t)c * ntab + i] = table[4 * (size_t)i + 1 + c];
+  // the stream may still read the previous table
+  CK(cudaStreamSynchronize(b->stream));
+  if (b->wk_mem && b->wk_ntab != ntab) {
+    cudaFree(b->wk_mem);
+    b->wk_mem = nullptr;
+  }
+  if (!b->wk_mem) {
+    cudaError_t e = cudaMalloc(&b->wk_mem, bytes);
+    if (e != cudaSuccess) {
+      b->wk_mem = nullptr;
+      b->wk_on = false;
+      ++b->wk_gen;
+      return e == cudaErrorMemoryAllocation ? IMPZ_ERR_NOMEM : cuda_fail(e, "cudaMalloc");
+    }
+  }
+  b->wk_tab = (double*)b->wk_mem;
+  b->wk_line = (unsigned long long*)(b->wk_mem + tab_bytes);
+  b->wk_field = (double*)(b->wk_mem + tab_bytes + line_bytes);
+  CK(cudaMemset(b->wk_line, 0, line_bytes));
+  CK(cudaMemcpy(b->wk_tab, cols.data(), cols.size() * sizeof(double), cudaMemcpyHostToDevice));
+  b->wk_ntab = ntab;
+  b->wk_hwk = hwk;
+  b->wk_scale = scale;
+  b->wk_tr = transverse != 0;
+  // the line sums hold at most cap particles' weights of 2^wk_fixbits
+  b->wk_fixbits = std::min(40, 62 - ilog2i(b->cap + 1));
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  b->grid_wake = (int)std::max<long long>(
+      1, std::min<long long>((b->cap + 255) / 256, (long long)sms * 8));
+  b->wk_on = true;
+  ++b->wk_gen;
+  return IMPZ_OK;
+}
+
+int impz_wake_off(impz_bunch_t b) {
+  if (!b) return IMPZ_ERR_ARG;
+  b->wk_on = false;
+  ++b->wk_gen;
   return IMPZ_OK;
 }
 
@@ -1106,7 +1200,7 @@ static int launch_step(impz_bunch_t b, bool sc) {
 static int graph_pair(impz_bunch_t b) {
   const int p = b->parity;
   if (b->gexec[p] && (b->g_steps[p] != b->dsteps || b->g_mom[p] != b->mom_out ||
-                      b->g_light[p] != b->run_light)) {
+                      b->g_light[p] != b->run_light || b->g_wake[p] != b->wk_gen)) {
     cudaGraphExecDestroy(b->gexec[p]);
     b->gexec[p] = nullptr;
   }
@@ -1129,9 +1223,10 @@ static int graph_pair(impz_bunch_t b) {
     b->g_steps[p] = b->dsteps;
     b->g_mom[p] = b->mom_out;
     b->g_light[p] = b->run_light;
+    b->g_wake[p] = b->wk_gen;
     b->parity = p;  // capture did not execute anything
   }
-  g_launches += 2 * 12;
+  g_launches += 2 * (12 + (b->wk_on ? 2 : 0));
   CK(cudaGraphLaunch(b->gexec[p], b->stream));
   return IMPZ_OK;
 }

@@ -140,6 +140,29 @@ struct DepositArgs {
   double xl;
 };
 
+// Read-in wakefield of type -41 elements: the line density (and, with the
+// transverse wake, the x/y moments) on the z grid, then the per-plane field
+// added to the node fields before the gather.
+struct WakeArgs {
+  const double* in[6];
+  const StepParams* steps;
+  const DevState* st;
+  int fixed_step;
+  int nz;
+  int fixbits;               // fixed-point resolution of the line sums
+  int transverse;            // 1: x/y moments and the transverse wakes too
+  int ntab;                  // wake table rows
+  int pad0;
+  unsigned long long* line;  // [3][nz] int64 sums (density, x, y), left cleared
+  const double* table;       // [3][ntab]: longitudinal, x and y wake columns
+  double* wfield;            // [3][nz] out: added to Ex, Ey, Ez of plane k
+  double hwk;                // table spacing (second z minus first)
+  double scale;              // the element's wake scale (Param(2))
+  double unit;               // grid-field unit: 1 (FP64 form) or the charge weight (FP32 form)
+  double xl;
+  Consts k;
+};
+
 #define IMPZ_SCAN_LOG 12      // 4096 cells per scan block (1024 threads x 4)
 #ifndef IMPZ_DEP_TILE
 #define IMPZ_DEP_TILE 4096    // deposit tile entries: two int32 halves + an int32 count (48 KB)

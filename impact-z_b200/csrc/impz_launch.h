@@ -54,6 +54,8 @@ inline cudaError_t launch_pdl(void (*kernel)(KP...), dim3 grid, dim3 block, size
   cudaError_t launch_advance(const AdvanceArgs& a, bool f32, bool light, int grid,       \
                              cudaStream_t s);                                            \
   cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s);            \
+  cudaError_t launch_wake(const WakeArgs& a, int grid, cudaStream_t s);                  \
+  cudaError_t prepare_wake();                                                            \
   cudaError_t launch_scan(int* counts, int* cursor, int* bsum, long long total,          \
                           DevState* st, cudaStream_t s);                                 \
   int max_blocks_advance(bool f32);                                                      \
@@ -80,6 +82,7 @@ struct PoissonBuffers {
   const double2* tw64y;
   const double2* tw64z;
   DevState* st;
+  const double* wake;       // per-plane {dEx, dEy, dEz}[nz] added to E, or null
 };
 
 template <typename T>

@@ -1221,5 +1221,167 @@ __global__ void __launch_bounds__(BLOCK) k_scan(int* counts, int* cursor, int* b
   if (threadIdx.x == 0) st->done_scan = 0;
 }
 
+// ---------------------------------------------------------------------
+// Read-in wakefield, step part 1: the line density on the z grid
+// (AccSimulator.f90:1279-1296).  Every live particle adds ab and 1-ab to
+// planes iizz and iizz+1, with the reference's division by hzwake, and with
+// the transverse wake x*ab, x*(1-ab) and the same in y.  The sums are int64
+// fixed point: the density in units of 2^-fixbits, the moments in units of
+// 2^-fixbits of the smallest power of two above the grid's largest |x|
+// (|y|), so they do not depend on the order of the additions.  Sorted
+// particles put a warp mostly on one plane: such a warp adds each sum with
+// one global atomic, any other warp lane by lane.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_wake_line(WakeArgs a) {
+  const DevState* st = a.st;
+  const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
+  const double gam = a.steps[s].gam, rad = a.steps[s].rad;
+  const long long n = st->nlocal;
+  const int nz = a.nz;
+  const double zmin = st->geom.range[4];
+  const double hzw = (st->geom.range[5] - zmin) / (nz - 1);
+  const double sc = ldexp(1.0, a.fixbits);
+  int ex, ey;
+  frexp(fmax(fabs(st->geom.range[0]), fabs(st->geom.range[1])), &ex);
+  frexp(fmax(fabs(st->geom.range[2]), fabs(st->geom.range[3])), &ey);
+  const double sx = ldexp(1.0, a.fixbits - ex), sy = ldexp(1.0, a.fixbits - ey);
+  const int nq = a.transverse ? 6 : 2;
+  const int lane = threadIdx.x & 31;
+  for (long long base = (long long)blockIdx.x * BLOCK + (threadIdx.x & ~31); base < n;
+       base += (long long)gridDim.x * BLOCK) {
+    const long long i = base + lane;
+    int kz = -1;
+    long long q[6] = {0, 0, 0, 0, 0, 0};
+    if (i < n) {
+      Particle p;
+      p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
+      p.py = a.in[3][i]; p.ph = a.in[4][i]; p.pt = a.in[5][i];
+      const TFrame t = to_tframe(p, gam, rad, a.xl);
+      if (!t.lost) {
+        const int iizz = (int)((t.zt - zmin) / hzw + 1);
+        const double ab = ((zmin - t.zt) + iizz * hzw) / hzw;
+        if (iizz >= 1 && iizz < nz) {
+          kz = iizz - 1;
+          q[0] = llrint(ab * sc);
+          q[1] = llrint((1.0 - ab) * sc);
+          if (a.transverse) {
+            q[2] = llrint(t.xt * ab * sx);
+            q[3] = llrint(t.xt * (1.0 - ab) * sx);
+            q[4] = llrint(t.yt * ab * sy);
+            q[5] = llrint(t.yt * (1.0 - ab) * sy);
+          }
+        }
+      }
+    }
+    const int kmin = __reduce_min_sync(0xffffffffu, kz < 0 ? INT_MAX : kz);
+    const int kmax = __reduce_max_sync(0xffffffffu, kz);
+    if (kmax < 0) continue;
+    if (kmin == kmax) {
+      for (int c = 0; c < nq; c++) {
+        long long v = q[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0)
+          atomicAdd(a.line + (long long)(c >> 1) * nz + kmin + (c & 1), (unsigned long long)v);
+      }
+    } else if (kz >= 0) {
+      for (int c = 0; c < nq; c++)
+        atomicAdd(a.line + (long long)(c >> 1) * nz + kz + (c & 1), (unsigned long long)q[c]);
+    }
+  }
+}
+
+// greenwake of wakefieldread_FieldQuant (Field.f90:818-830): the table at
+// zz = j*hz with the reference's weight ab = iwk*hwk - zwk (not divided by
+// hwk); rows past the table read zero, as the reference's zero-filled module
+// arrays do.
+__device__ __forceinline__ double wake_green(const double* e, int ntab, double hwk, int j,
+                                             double hz) {
+  const double zz = j * hz;
+  const double zwk = zz - 0.0;
+  const int iwk = (int)(zwk / hwk + 1);
+  const double ab = iwk * hwk - zwk;
+  const double e0 = (iwk >= 1 && iwk <= ntab) ? e[iwk - 1] : 0.0;
+  const double e1 = (iwk >= 0 && iwk < ntab) ? e[iwk] : 0.0;  // row iwk + 1
+  return e0 * ab + e1 * (1.0 - ab);
+}
+
+// Read-in wakefield, step part 2 (one block): the line charge density
+// recvdensz (AccSimulator.f90:1297-1322), its convolution with the wake
+// table (wakefieldread_FieldQuant, Field.f90:783-1001) and the per-plane
+// field that kick1wake adds to the node fields (BeamBunch.f90:5015-5033).
+// The reference convolves on a doubled grid by FFT with a Green function
+// that is 0.5 W(0) at 0, zero at 1..Nz-1 and W((2Nz-k) hz) above; for k < Nz
+// that circular convolution is the causal sum
+//   conv_z(k) = 0.5 W(0) d(k) + sum_{m>k} d(m) W((m-k) hz),
+// evaluated here directly (Nz^2/2 terms), and the transverse ones (zero at 0
+// too) conv_x(k) = sum_{m>k} d(m) xbar(m) Wx((m-k) hz).  Clears the line
+// sums for the next step.
+__global__ void __launch_bounds__(1024) k_wake_field(WakeArgs a) {
+  extern __shared__ double wsm[];
+  const int nz = a.nz;
+  double* d = wsm;
+  double* dx = wsm + nz;
+  double* dy = wsm + 2 * nz;
+  double* gz = wsm + 3 * nz;
+  double* gx = wsm + 4 * nz;
+  double* gy = wsm + 5 * nz;
+  const DevState* st = a.st;
+  const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
+  const double gam = a.steps[s].gam;
+  const double cur = st->current;
+  const double npt = (double)st->npt;
+  double hzw = (st->geom.range[5] - st->geom.range[4]) / (nz - 1);
+  hzw = hzw / gam;
+  const double sc = ldexp(1.0, a.fixbits);
+  int ex, ey;
+  frexp(fmax(fabs(st->geom.range[0]), fabs(st->geom.range[1])), &ex);
+  frexp(fmax(fabs(st->geom.range[2]), fabs(st->geom.range[3])), &ey);
+  const double sx = ldexp(1.0, a.fixbits - ex), sy = ldexp(1.0, a.fixbits - ey);
+  const double chrg = a.k.charge, mass = a.k.mass;
+  const int ntab = a.ntab;
+  for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+    const double dens = (double)(long long)a.line[k] / sc;
+    const double dk = dens * cur / a.k.Scfreq / npt / hzw * chrg / fabs(chrg);
+    double xw = 0.0, yw = 0.0;
+    if (a.transverse && dens != 0.0) {
+      xw = ((double)(long long)a.line[nz + k] / sx) / dens;
+      yw = ((double)(long long)a.line[2 * nz + k] / sy) / dens;
+    }
+    d[k] = dk;
+    dx[k] = dk * xw;
+    dy[k] = dk * yw;
+    gz[k] = wake_green(a.table, ntab, a.hwk, k, hzw);
+    gx[k] = a.transverse ? wake_green(a.table + ntab, ntab, a.hwk, k, hzw) : 0.0;
+    gy[k] = a.transverse ? wake_green(a.table + 2 * ntab, ntab, a.hwk, k, hzw) : 0.0;
+    a.line[k] = 0ull;
+    a.line[nz + k] = 0ull;
+    a.line[2 * nz + k] = 0ull;
+  }
+  __syncthreads();
+  double xycon, tcon;
+  kick_consts(a.k, gam, cur, xycon, tcon);
+  const double bet = sqrt(gam * gam - 1.0) / gam;
+  const double g0 = 0.5 * gz[0];
+  for (int k = threadIdx.x; k < nz; k += blockDim.x) {
+    double cz = d[k] * g0, cx = 0.0, cy = 0.0;
+    if (a.transverse) {
+      for (int m = k + 1; m < nz; m++) {
+        cz = cz + d[m] * gz[m - k];
+        cx = cx + dx[m] * gx[m - k];
+        cy = cy + dy[m] * gy[m - k];
+      }
+    } else {
+      for (int m = k + 1; m < nz; m++) cz = cz + d[m] * gz[m - k];
+    }
+    const double ezwake = a.scale * (-cz * hzw);
+    const double exwake = a.scale * (cx * hzw);
+    const double eywake = a.scale * (cy * hzw);
+    a.wfield[k] = chrg * exwake / xycon / mass / bet / gam / a.unit;
+    a.wfield[nz + k] = chrg * eywake / xycon / mass / bet / gam / a.unit;
+    a.wfield[2 * nz + k] = chrg * ezwake / tcon / mass / a.unit;
+  }
+}
+
 }  // namespace IMPZ_NS
 }  // namespace impz

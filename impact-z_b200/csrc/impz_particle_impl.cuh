@@ -45,6 +45,26 @@ cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s) {
                     kDepSmem, s, a);
 }
 
+#define IMPZ_WAKE_BLOCK 256
+static const size_t kWakeSmemMax = (size_t)6 * 4096 * sizeof(double);
+
+cudaError_t prepare_wake() {
+  static cudaError_t once = cudaFuncSetAttribute(
+      k_wake_field, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWakeSmemMax);
+  return once;
+}
+
+cudaError_t launch_wake(const WakeArgs& a, int grid, cudaStream_t s) {
+  cudaError_t once = prepare_wake();
+  if (once != cudaSuccess) return once;
+  if (a.nz < 2 || (size_t)6 * a.nz * sizeof(double) > kWakeSmemMax) return cudaErrorInvalidValue;
+  k_wake_line<IMPZ_WAKE_BLOCK><<<grid, IMPZ_WAKE_BLOCK, 0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_wake_field<<<1, 1024, (size_t)6 * a.nz * sizeof(double), s>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_scan(int* counts, int* cursor, int* bsum, long long total, DevState* st,
                         cudaStream_t s) {
   const long long nb = (total + (1ll << IMPZ_SCAN_LOG) - 1) >> IMPZ_SCAN_LOG;

@@ -472,11 +472,14 @@ __global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long 
 // kick1_BeamBunch finite differences (BeamBunch.f90:1784-2005), one rank,
 // open BC: centred inside, one-sided on the faces.  Out: {Ex,Ey,Ez,0}.
 // Also clears the charge grid (its last reader, the forward transform, is
-// done) for the next deposit.
+// done) for the next deposit.  With a read-in wake, adds its per-plane field
+// wake = {dEx, dEy, dEz}[nz] to every node of the plane (kick1wake,
+// BeamBunch.f90:5015-5033).
 template <typename T>
 __global__ void k_efield(int nx, int ny, int nz, const T* __restrict__ phi,
                          const DevState* st, T* __restrict__ E,
-                         unsigned long long* __restrict__ rho) {
+                         unsigned long long* __restrict__ rho,
+                         const double* __restrict__ wake) {
   griddep_wait();
   const long long G = (long long)nx * ny * nz;
   const T hxi = (T)st->geom.hi[0], hyi = (T)st->geom.hi[1], hzi = (T)st->geom.hi[2];
@@ -497,6 +500,11 @@ __global__ void k_efield(int nx, int ny, int nz, const T* __restrict__ phi,
     if (k == 0) ez = hzi * (phi[e] - phi[e + sz]);
     else if (k == nz - 1) ez = hzi * (phi[e - sz] - phi[e]);
     else ez = half * hzi * (phi[e - sz] - phi[e + sz]);
+    if (wake) {
+      ex = ex + (T)wake[k];
+      ey = ey + (T)wake[nz + k];
+      ez = ez + (T)wake[2 * nz + k];
+    }
     rho[e] = 0ull;  // the next deposit accumulates into a cleared charge grid
     T* o = E + 4 * e;
     o[0] = ex;

@@ -18,8 +18,11 @@
 * `run_deck` runs a deck of the map integrator with open boundaries and a
   particle.in distribution (Flagmap=1, Flagbc=1, Flagdist=19) on the GPU
   runner, splitting the lattice at control elements (types < 0,
-  `lattice_segments`): -2 dumps phase space, -99 ends the lattice, the types
-  listed in `skip` are passed over (reported), any other is refused.
+  `lattice_segments`): -2 dumps phase space, -41 turns the read-in wake on
+  or off, -99 ends the lattice, the types listed in `skip` are passed over
+  (reported), any other is refused.
+* `read_wake`: rfdataN.in as the wake table of a -41 element, read1wk_Data
+  (src/DataStruct/Data.f90:559-633).
 """
 import os
 import re
@@ -200,6 +203,19 @@ def read_rfdata(path):
     return tab[:, 0].copy(), tab[:, 1].copy(), tab[:, 2].copy(), tab[:, 3].copy()
 
 
+def read_wake(path):
+    """rfdataN.in as a wake table, read1wk_Data (src/DataStruct/Data.f90:
+    559-633): rows (z, longitudinal, x, y wake); z is shifted to start at 0
+    by the bunch's wake call, as the reference does after reading."""
+    rows = []
+    with open(path) as f:
+        for ln in f:
+            v = _values(ln)
+            if len(v) >= 4:
+                rows.append([float(x) for x in v[:4]])
+    return np.array(rows)
+
+
 # the 45 columns of impz_diag_row: z, then the files' columns in order
 _FILES = (("fort.18", 1, 6), ("fort.24", 6, 12), ("fort.25", 12, 18), ("fort.26", 18, 24),
           ("fort.27", 24, 30), ("fort.28", 30, 33), ("fort.29", 33, 39), ("fort.30", 39, 45))
@@ -226,10 +242,17 @@ def read_diag(outdir, name):
 def lattice_segments(deck, workdir, skip=()):
     """The lattice cut at its control elements, for a runner: yields
     ("run", [impz_elem_t]) for each stretch of beam-line elements (RF tables
-    read from workdir), ("dump", Element) for each type -2 phase dump, and
-    last ("skipped", [types]) for the control elements passed over because
-    they are in `skip`.  -99 ends the lattice; any other control element is
-    refused (ValueError)."""
+    read from workdir), ("dump", Element) for each type -2 phase dump,
+    ("wake", {"on", "table", "scale", "transverse"}) for each type -41
+    read-in wake control, and last ("skipped", [types]) for the control
+    elements passed over because they are in `skip`.  -99 ends the lattice;
+    any other control element is refused (ValueError).
+
+    A -41 element (src/Contrl/AccSimulator.f90:959-978) reads the table
+    rfdata<Param(3)>.in when Param(3) > 0, turns the wake on with scale
+    Param(2) when Param(4) > 0 and off otherwise; a Param(4) below 10 drops
+    the transverse wake for the rest of the run (flagbtw = 2 is never
+    reset)."""
     from . import elem
 
     def to_elem(e):
@@ -239,6 +262,7 @@ def lattice_segments(deck, workdir, skip=()):
         return elem(e.type, e.length, e.nseg, e.mapstp, list(e.vals), rf=rf)
 
     seg, skipped = [], []
+    table, no_transverse = None, False
     for e in deck.elements:
         if e.type >= 0:
             seg.append(to_elem(e))
@@ -252,6 +276,18 @@ def lattice_segments(deck, workdir, skip=()):
             yield "dump", e
         elif e.type in skip:
             skipped.append(e.type)
+        elif e.type == -41:
+            scale, rfile, onoff = e.vals[0], e.vals[1], e.vals[2]
+            if rfile > 0.0:
+                table = read_wake(os.path.join(workdir, "rfdata%d.in" % int(rfile + 0.1)))
+            if onoff > 0.0:
+                if table is None:
+                    raise ValueError("a -41 element turns the wake on before any table is read")
+                no_transverse = no_transverse or onoff < 10.0
+                yield "wake", {"on": True, "table": table, "scale": scale,
+                               "transverse": not no_transverse}
+            else:
+                yield "wake", {"on": False}
         else:
             raise ValueError("control element type %d is outside this path" % e.type)
     if seg:
@@ -286,6 +322,11 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
         for kind, item in lattice_segments(deck, workdir, set(skip)):
             if kind == "skipped":
                 skipped = item
+            elif kind == "wake":
+                if item["on"]:
+                    b.wake(item["table"], item["scale"], item["transverse"])
+                else:
+                    b.wake_off()
             elif kind == "dump":
                 if write:
                     write_phase(os.path.join(outdir, "fort.%d" % item.mapstp), b.download(),

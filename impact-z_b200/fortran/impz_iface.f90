@@ -153,5 +153,21 @@
             real(c_double), intent(out) :: recs(48, *), zs(*)
             integer(c_int), intent(out) :: nrec
           end function
+
+          ! read-in wakefield of a type -41 element: table(4, ntab) holds
+          ! the rows (z, Ez, Ex, Ey wake) that read1wk_Data read
+          integer(c_int) function impz_wake_set(bunch, table, ntab, scale, transverse) &
+              bind(C, name="impz_wake_set")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), intent(in) :: table(4, *)
+            integer(c_int), value :: ntab, transverse
+            real(c_double), value :: scale
+          end function
+
+          integer(c_int) function impz_wake_off(bunch) bind(C, name="impz_wake_off")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: bunch
+          end function
         end interface
       end module impz_iface

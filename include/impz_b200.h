@@ -89,7 +89,8 @@ int impz_bunch_destroy(impz_bunch_t b);
 /* Device bytes a bunch of n particles on an nx*ny*nz grid holds while it runs
  * a lattice of nsteps steps (0: the bunch alone), at the driver's 2 MiB
  * allocation granularity: the bunch is one allocation, the run tables a
- * second, and no other call allocates.  The serving loop admits by it.
+ * second, and no other call allocates but impz_wake_set (its table and
+ * per-step buffers, a few 10 KB).  The serving loop admits by it.
  * No reference counterpart (the reference allocates per process). */
 long long impz_bunch_footprint(long long n, int nx, int ny, int nz, int form, int flags,
                                int nsteps);
@@ -98,6 +99,20 @@ long long impz_bunch_footprint(long long n, int nx, int ny, int nz, int form, in
  * their longitudinal position; |out| is the bunching factor.  No reference
  * counterpart (a diagnostic of the chicane study on this path). */
 int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]);
+/* Read-in wakefield of a type -41 element (AccSimulator.f90:959-978):
+ * impz_wake_set turns it on for every space-charge step that follows, as
+ * the reference's flagwake does, with table = ntab rows of (z, longitudinal,
+ * x, y wake) as in rfdataN.in (read1wk_Data, Data.f90:559-633; z is
+ * shifted to start at 0 here), scale = Param(2) (scwk) and transverse = 0
+ * when Param(4) < 10 (flagbtw = 2: no transverse wake).  Each step then
+ * forms the line density on the z grid, convolves it with the table
+ * (wakefieldread_FieldQuant, Field.f90:783-1001) and adds the per-plane
+ * field to the node fields before the gather (kick1wake_BeamBunch,
+ * BeamBunch.f90:4694-5046).  Allocates the table and its per-step buffers
+ * (outside impz_bunch_footprint).  IMPZ_ERR_ARG for ntab < 2, a
+ * non-increasing z, or nz > 4096.  impz_wake_off is Param(4) <= 0. */
+int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, int transverse);
+int impz_wake_off(impz_bunch_t b);
 /* Current, Npt, Nptlocal, refptcl(1..6), z, device bytes (11 doubles). */
 int impz_bunch_info(impz_bunch_t b, double info[11]);
 /* The bunch's CUDA stream (cudaStream_t) for callers that interleave work. */
@@ -184,7 +199,8 @@ int impz_count_steps(const impz_elem_t* elems, int nelem);
 #define IMPZ_PROF_CONV 3     /* doubled-grid FFT convolution (3 kernels) */
 #define IMPZ_PROF_EFIELD 4   /* finite-difference field */
 #define IMPZ_PROF_PUSH 5     /* fused gather/kick/map/moments/range/sort pass */
-#define IMPZ_PROF_NCAT 6
+#define IMPZ_PROF_WAKE 6     /* read-in wake: line density + wake field (2 kernels) */
+#define IMPZ_PROF_NCAT 7
 /* When on, CUDA events bracket every kernel group on the bunch's stream;
  * runs launch directly (no graph replay) and the Green build runs on the
  * bunch's stream, so the groups' intervals are disjoint. */

@@ -933,6 +933,17 @@ void orc_cvbkforth1st(double *pts, int n, const double refptcl[6]) {
 void orc_kick1(double *pts, int n, const double *phi, const int mesh[3],
                const double range[6], const double msize[3], double gam,
                double curr, double tau, double mass, double chrg, double *eg) {
+  orc_kick1w(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, eg, NULL);
+}
+
+/* kick1wake_BeamBunch (BeamBunch.f90:4694-5046): kick1 with a per-plane
+ * field added to the node fields before the gather (BeamBunch.f90:5015-5033);
+ * wfield = {dEx[nz], dEy[nz], dEz[nz]} in grid-field units (orc_wake_field),
+ * NULL for none. */
+void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
+                const double range[6], const double msize[3], double gam,
+                double curr, double tau, double mass, double chrg, double *eg,
+                const double *wfield) {
   if (curr < 1.0e-20) return;
   const int nx = mesh[0], ny = mesh[1], nz = mesh[2];
   const size_t G = (size_t)nx * ny * nz;
@@ -966,6 +977,14 @@ void orc_kick1(double *pts, int n, const double *phi, const int mesh[3],
   for (int j = 1; j <= ny; j++)
     for (int i = 1; i <= nx; i++)
       egz[IDX(i, j, nz)] = hzi * (PHI(i, j, nz - 1) - PHI(i, j, nz));
+  if (wfield)
+    for (int k = 1; k <= nz; k++)
+      for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+          egx[IDX(i, j, k)] = egx[IDX(i, j, k)] + wfield[k - 1];
+          egy[IDX(i, j, k)] = egy[IDX(i, j, k)] + wfield[nz + k - 1];
+          egz[IDX(i, j, k)] = egz[IDX(i, j, k)] + wfield[2 * nz + k - 1];
+        }
 
   /* scatter1_BeamBunch constants (BeamBunch.f90:2066-2084) */
   const double tmpscale = curr / PC.Scfreq;
@@ -1148,6 +1167,139 @@ void orc_diag_row(double z, const double raw[ORC_RAW_LEN], int npt, int nlocal,
 }
 
 /* ------------------------------------------------------------------ */
+/* Read-in wakefield (type -41 elements, AccSimulator.f90:959-978).  The
+ * table is read1wk_Data's (Data.f90:559-633): columns z, longitudinal,
+ * x and y wake, z shifted to start at 0; the module arrays hold Ndataini =
+ * 5000 rows and are zero beyond the rows read, which the table lookup below
+ * reproduces by reading zero past the last row. */
+static struct {
+  int on, transverse, ntab;
+  double scale, hwk;
+  double *ew, *epw, *eppw;
+} WK;
+
+void orc_wake_off(void) { WK.on = 0; }
+
+int orc_wake_set(const double *z, const double *ew, const double *epw, const double *eppw,
+                 int ntab, double scale, int transverse) {
+  if (ntab < 2) return -1;
+  double *t = (double *)realloc(WK.ew, 3 * (size_t)ntab * sizeof(double));
+  if (!t) return -2;
+  WK.ew = t;
+  WK.epw = t + ntab;
+  WK.eppw = t + 2 * (size_t)ntab;
+  memcpy(WK.ew, ew, ntab * sizeof(double));
+  memcpy(WK.epw, epw, ntab * sizeof(double));
+  memcpy(WK.eppw, eppw, ntab * sizeof(double));
+  /* zdatwk(i) = zdatwk(i) - zdatwk(1); hwk = zdatwk(2) - zdatwk(1) */
+  WK.hwk = (z[1] - z[0]) - (z[0] - z[0]);
+  WK.ntab = ntab;
+  WK.scale = scale;
+  WK.transverse = transverse;
+  WK.on = 1;
+  return 0;
+}
+
+static double wk_at(const double *e, int idx1) { /* 1-based, zero past the table */
+  return (idx1 >= 1 && idx1 <= WK.ntab) ? e[idx1 - 1] : 0.0;
+}
+
+/* greenwake of wakefieldread_FieldQuant (Field.f90:818-830): the table at
+ * zz = j*hz with the reference's interpolation weight ab = iwk*hwk - zwk
+ * (not divided by hwk) */
+static double wk_green(const double *e, int j, double hz) {
+  const double zz = j * hz;
+  const double zwk = zz - 0.0;
+  const int iwk = (int)(zwk / WK.hwk + 1);
+  const double ab = iwk * WK.hwk - zwk;
+  /* row iwk + 1, written without overflowing iwk + 1 */
+  const double e1 = (iwk >= 0 && iwk < WK.ntab) ? e[iwk] : 0.0;
+  return wk_at(e, iwk) * ab + e1 * (1.0 - ab);
+}
+
+/* line density and transverse moments on the z grid
+ * (AccSimulator.f90:1279-1296), particles in the conv1st frame */
+void orc_wake_line(const double *pts, int n, int nz, const double range[6], double *densz,
+                   double *xsum, double *ysum) {
+  const double hzwake = (range[5] - range[4]) / (nz - 1);
+  memset(densz, 0, nz * sizeof(double));
+  memset(xsum, 0, nz * sizeof(double));
+  memset(ysum, 0, nz * sizeof(double));
+  for (int q = 0; q < n; q++) {
+    const int iizz = (int)((P(q, 4) - range[4]) / hzwake + 1);
+    const int iizz1 = iizz + 1;
+    const double ab = ((range[4] - P(q, 4)) + iizz * hzwake) / hzwake;
+    if (iizz < 1 || iizz1 > nz) continue; /* cannot happen inside update_CompDom's range */
+    xsum[iizz - 1] = xsum[iizz - 1] + P(q, 0) * ab;
+    xsum[iizz1 - 1] = xsum[iizz1 - 1] + P(q, 0) * (1.0 - ab);
+    ysum[iizz - 1] = ysum[iizz - 1] + P(q, 2) * ab;
+    ysum[iizz1 - 1] = ysum[iizz1 - 1] + P(q, 2) * (1.0 - ab);
+    densz[iizz - 1] = densz[iizz - 1] + ab;
+    densz[iizz1 - 1] = densz[iizz1 - 1] + 1.0 - ab;
+  }
+}
+
+/* The wake fields of one step in grid-field units, added per plane to the
+ * node fields by kick1wake (BeamBunch.f90:5015-5033).  The reference
+ * convolves on a doubled grid by FFT (wakefieldread_FieldQuant,
+ * Field.f90:783-1001); its greenwake has 0.5*W(0) at 0, zeros at 1..Nz-1
+ * and W((2Nz-k)hz) above, so for k < Nz the circular convolution is
+ *   conv_z(k) = 0.5 W(0) d(k) + sum_{m>k} d(m) W((m-k) hz),
+ * evaluated here as that direct sum (the FFT's own rounding aside), and the
+ * transverse ones (greenwake zero at 0 too)
+ *   conv_x(k) = sum_{m>k} d(m) xbar(m) Wx((m-k) hz).
+ * d is recvdensz (AccSimulator.f90:1297-1322).  out = {dEx, dEy, dEz}[nz]. */
+void orc_wake_field(int nz, const double *densz, const double *xsum, const double *ysum,
+                    const double range[6], double gam, double curr, int npt, double mass,
+                    double chrg, double *out) {
+  double *d = (double *)malloc(3 * (size_t)nz * sizeof(double));
+  double *dx = d + nz, *dy = d + 2 * (size_t)nz;
+  double hzwake = (range[5] - range[4]) / (nz - 1);
+  hzwake = hzwake / gam;
+  for (int k = 0; k < nz; k++) {
+    d[k] = densz[k] * curr / PC.Scfreq / npt / hzwake * chrg / fabs(chrg);
+    double xw = 0.0, yw = 0.0;
+    if (densz[k] != 0.0) {
+      xw = xsum[k] / densz[k];
+      yw = ysum[k] / densz[k];
+    }
+    dx[k] = d[k] * xw;
+    dy[k] = d[k] * yw;
+  }
+  /* kick1wake's constants (BeamBunch.f90:4989-5006) */
+  const double twopi = 2.0 * PC.Pi;
+  const double tmpscale = curr / PC.Scfreq;
+  const double fpei = PC.Clight * PC.Clight * (double)1.0e-7f;
+  const double xk = 1 / PC.Scxl;
+  const double bet = sqrt(gam * gam - 1.0) / gam;
+  const double bbyk = bet / xk;
+  const double gambet = gam * bet;
+  const double brho = gambet / (PC.Clight * chrg) * mass;
+  const double vz0 = bet * PC.Clight;
+  const double perv0 = 2.0 * curr * fpei / (brho * vz0 * vz0 * gam * gam);
+  const double xycon = 0.5 * perv0 * gambet * bbyk * twopi / tmpscale;
+  const double tcon = bet * xycon * (gam * gam);
+  const double g0 = 0.5 * wk_green(WK.ew, 0, hzwake);
+  for (int k = 0; k < nz; k++) {
+    double cz = d[k] * g0, cx = 0.0, cy = 0.0;
+    for (int m = k + 1; m < nz; m++) {
+      cz = cz + d[m] * wk_green(WK.ew, m - k, hzwake);
+      if (WK.transverse) {
+        cx = cx + dx[m] * wk_green(WK.epw, m - k, hzwake);
+        cy = cy + dy[m] * wk_green(WK.eppw, m - k, hzwake);
+      }
+    }
+    const double ezwake = WK.scale * (-cz * hzwake);
+    const double exwake = WK.scale * (cx * hzwake);
+    const double eywake = WK.scale * (cy * hzwake);
+    out[k] = chrg * exwake / xycon / mass / bet / gam;
+    out[nz + k] = chrg * eywake / xycon / mass / bet / gam;
+    out[2 * nz + k] = chrg * ezwake / tcon / mass;
+  }
+  free(d);
+}
+
+/* ------------------------------------------------------------------ */
 static double pipe_radius(const orc_elem *e) {
   /* getradius_BeamLineElem (BeamLineElem.f90:500-552): Param index per type */
   switch (e->type) {
@@ -1159,7 +1311,8 @@ static double pipe_radius(const orc_elem *e) {
 }
 
 /* run_AccSimulator element/segment loop (AccSimulator.f90:742-1504) for
- * Flagmap=1, Flagbc=1, Flagerr=0, Flagsubstep=0, one rank, no wake/CSR. */
+ * Flagmap=1, Flagbc=1, Flagerr=0, Flagsubstep=0, one rank, no CSR; the read-in
+ * wake of orc_wake_set applies to every space-charge kick while it is on. */
 int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
             double *rows, int maxrows) {
   const double Scxl = PC.Scxl;
@@ -1235,9 +1388,21 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
               free(rho);
               return -5;
             }
+            double *wf = NULL;
+            if (WK.on) { /* AccSimulator.f90:1273-1340 */
+              const int nz = mesh[2];
+              wf = (double *)malloc(6 * (size_t)nz * sizeof(double));
+              double *line = wf + 3 * (size_t)nz;
+              orc_wake_line(beam->pts, beam->nlocal, nz, range, line, line + nz,
+                            line + 2 * (size_t)nz);
+              orc_wake_field(nz, line, line + nz, line + 2 * (size_t)nz, range,
+                             -beam->refptcl[5], beam->current, beam->npt, beam->mass,
+                             beam->charge, wf);
+            }
             orc_cvbkforth1st(beam->pts, beam->nlocal, beam->refptcl);
-            orc_kick1(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],
-                      beam->current, tau2, beam->mass, beam->charge, NULL);
+            orc_kick1w(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],
+                       beam->current, tau2, beam->mass, beam->charge, NULL, wf);
+            free(wf);
           }
         }
         if (bitype == 4) {

@@ -98,6 +98,20 @@ void orc_cvbkforth1st(double *pts, int n, const double refptcl[6]);
 void orc_kick1(double *pts, int n, const double *phi, const int mesh[3],
                const double range[6], const double msize[3], double gam,
                double curr, double tau, double mass, double chrg, double *eg);
+void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
+                const double range[6], const double msize[3], double gam,
+                double curr, double tau, double mass, double chrg, double *eg,
+                const double *wfield);
+/* read-in wakefield of type -41 elements (Data.f90:559-633,
+ * AccSimulator.f90:959-978, 1273-1340, Field.f90:783-1001) */
+int orc_wake_set(const double *z, const double *ew, const double *epw, const double *eppw,
+                 int ntab, double scale, int transverse);
+void orc_wake_off(void);
+void orc_wake_line(const double *pts, int n, int nz, const double range[6], double *densz,
+                   double *xsum, double *ysum);
+void orc_wake_field(int nz, const double *densz, const double *xsum, const double *ysum,
+                    const double range[6], double gam, double curr, int npt, double mass,
+                    double chrg, double *out);
 /* diagnostic1_Output (Output.f90:20-371): raw sums and one derived row */
 void orc_moment_sums(const double *pts, int n, double raw[ORC_RAW_LEN]);
 void orc_diag_row(double z, const double raw[ORC_RAW_LEN], int npt, int nlocal,

@@ -80,6 +80,16 @@ def lib():
             "orc_cvbkforth1st": (v, [_D, ctypes.c_int, _D]),
             "orc_kick1": (v, [_D, ctypes.c_int, _D, _I, _D, _D, ctypes.c_double, ctypes.c_double,
                               ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]),
+            "orc_kick1w": (v, [_D, ctypes.c_int, _D, _I, _D, _D, ctypes.c_double,
+                               ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_double, _D, _D]),
+            "orc_wake_set": (ctypes.c_int, [_D, _D, _D, _D, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_int]),
+            "orc_wake_off": (v, []),
+            "orc_wake_line": (v, [_D, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D]),
+            "orc_wake_field": (v, [ctypes.c_int, _D, _D, _D, _D, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                   ctypes.c_double, _D]),
             "orc_moment_sums": (v, [_D, ctypes.c_int, _D]),
             "orc_diag_row": (v, [ctypes.c_double, _D, ctypes.c_int, ctypes.c_int, _D,
                                  ctypes.c_double, _D]),
@@ -103,6 +113,20 @@ def physconst(freq):
     out = np.zeros(5)
     lib().orc_get_physconst(dp(out))
     return dict(Pi=out[0], Clight=out[1], Scxl=out[2], Rad2deg=out[3], Scfreq=out[4])
+
+
+def wake_set(table, scale=1.0, transverse=False):
+    """Turns the read-in wake on (a type -41 element with Param(4) > 0):
+    table rows (z, Ez wake, x wake, y wake) as in rfdataN.in."""
+    t = np.ascontiguousarray(np.asarray(table, dtype=np.float64).T)
+    r = lib().orc_wake_set(dp(t[0]), dp(t[1]), dp(t[2]), dp(t[3]), t.shape[1], float(scale),
+                           int(bool(transverse)))
+    if r:
+        raise ValueError("orc_wake_set: %d" % r)
+
+
+def wake_off():
+    lib().orc_wake_off()
 
 
 def set_threads(n):
