@@ -111,17 +111,20 @@ def fodo(periods=10, gradient=20.0, ldrift=0.1, lquad=0.1, nseg=4, mapstp=1, rad
 
 
 def chicane(angle_deg=3.0, lbend=0.2, ldrift_in=20.0, ldrift_mid=3.5, ldrift_c=0.5, nseg_bend=8,
-            nseg_drift=4, drift_steps_in=756, half_gap=0.01):
+            nseg_drift=4, drift_steps_in=756, half_gap=0.01, file_id=150.0):
     """20 m of drift then a 4-dipole chicane (+a, -a, -a, +a sector bends);
     800 steps by default.  R56 = -2 a^2 (ldrift_mid + 2 lbend / 3) is about
     -20 mm for 3 degree bends 3.5 m apart.
     Dipole deck values: v1 angle[rad], v2 k1, v3 file ID (150: z map + SC,
-    no CSR), v4 half gap (Dipole.f90:19-31, AccSimulator.f90:1060-1074)."""
+    no CSR; above 200: CSR inside the bends; above 500: also the transient
+    CSR downstream), v4 half gap (Dipole.f90:19-31,
+    AccSimulator.f90:1035-1074, 1131-1138)."""
     from . import elem
     a = math.radians(angle_deg)
 
     def bend(sgn):
-        return elem(4, lbend, nseg_bend, 1, [sgn * a, 0.0, 150.0, half_gap, 0.0, 0.0, 0.0, 0.0, 0.0])
+        return elem(4, lbend, nseg_bend, 1, [sgn * a, 0.0, file_id, half_gap, 0.0, 0.0, 0.0, 0.0,
+                                             0.0])
 
     out = [elem(0, ldrift_in, drift_steps_in, 1, [1.0])]
     out += [bend(+1), elem(0, ldrift_mid, nseg_drift, 1, [1.0]), bend(-1),

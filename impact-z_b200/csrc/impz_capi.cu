@@ -248,6 +248,10 @@ struct impz_bunch_s {
   // read-in wakefield (impz_wake_set): table [3][ntab], then the line sums
   // [3][nz] and the per-plane field [3][nz] in one allocation
   bool wk_on = false, wk_tr = false;
+  // CSR bend bookkeeping (committed at the end of each run) and whether the
+  // run in progress has CSR steps
+  CsrState csr, csr_run;
+  bool run_csr = false;
   int wk_ntab = 0, wk_gen = 0, wk_fixbits = 40, grid_wake = 1;
   double wk_hwk = 0.0, wk_scale = 1.0;
   char* wk_mem = nullptr;
@@ -307,7 +311,9 @@ PoissonBuffers poisson_of(impz_bunch_t b) {
   pb.twx = b->tw[0]; pb.twy = b->tw[1]; pb.twz = b->tw[2];
   pb.tw64x = b->tw64[0]; pb.tw64y = b->tw64[1]; pb.tw64z = b->tw64[2];
   pb.st = b->st;
-  pb.wake = b->wk_on ? b->wk_field : nullptr;
+  const bool wake = b->wk_on || b->run_csr;
+  pb.wake = wake ? b->wk_field : nullptr;
+  pb.wake_line = wake ? b->wk_line : nullptr;
   return pb;
 }
 
@@ -392,6 +398,7 @@ WakeArgs wake_args(impz_bunch_t b, const StepParams* table, int fixed) {
   w.fixbits = b->wk_fixbits;
   w.transverse = b->wk_tr ? 1 : 0;
   w.ntab = b->wk_ntab;
+  w.on = b->wk_on ? 1 : 0;
   w.line = b->wk_line;
   w.table = b->wk_tab;
   w.wfield = b->wk_field;
@@ -458,7 +465,7 @@ int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
     CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, gs));
   }
   if (!serial) CK(cudaEventRecord(b->ev_join, b->stream2));
-  if (b->wk_on) {
+  if (b->wk_on || b->run_csr) {
     ProfScope ps(b, IMPZ_PROF_WAKE, 2);
     CK(exact::launch_wake(wake_args(b, table, fixed), b->grid_wake, b->stream));
   }
@@ -822,50 +829,27 @@ int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]) {
   return IMPZ_OK;
 }
 
+static int wake_alloc(impz_bunch_t b, int ntab);
+
 int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, int transverse) {
   if (!b || !table || ntab < 2) return IMPZ_ERR_ARG;
   // read1wk_Data shifts z to start at 0; hwk = zdatwk(2) - zdatwk(1)
   const double hwk = (table[4] - table[0]) - (table[0] - table[0]);
   if (!(hwk > 0.0) || b->nz < 2 || b->nz > 4096) return IMPZ_ERR_ARG;
   CK(cudaSetDevice(b->device));
-  CK(exact::prepare_wake());  // outside any stream capture
-  const size_t tab_bytes = round_up((size_t)3 * ntab * sizeof(double), kAlign);
-  const size_t line_bytes = round_up((size_t)3 * b->nz * sizeof(unsigned long long), kAlign);
-  const size_t bytes = tab_bytes + line_bytes + (size_t)3 * b->nz * sizeof(double);
   std::vector<double> cols((size_t)3 * ntab);
   for (int i = 0; i < ntab; i++)
     for (int c = 0; c < 3; c++) cols[(size_t)c * ntab + i] = table[4 * (size_t)i + 1 + c];
-  // the stream may still read the previous table
-  CK(cudaStreamSynchronize(b->stream));
-  if (b->wk_mem && b->wk_ntab != ntab) {
-    cudaFree(b->wk_mem);
-    b->wk_mem = nullptr;
+  int r = wake_alloc(b, ntab);
+  if (r) {
+    b->wk_on = false;
+    ++b->wk_gen;
+    return r;
   }
-  if (!b->wk_mem) {
-    cudaError_t e = cudaMalloc(&b->wk_mem, bytes);
-    if (e != cudaSuccess) {
-      b->wk_mem = nullptr;
-      b->wk_on = false;
-      ++b->wk_gen;
-      return e == cudaErrorMemoryAllocation ? IMPZ_ERR_NOMEM : cuda_fail(e, "cudaMalloc");
-    }
-  }
-  b->wk_tab = (double*)b->wk_mem;
-  b->wk_line = (unsigned long long*)(b->wk_mem + tab_bytes);
-  b->wk_field = (double*)(b->wk_mem + tab_bytes + line_bytes);
-  CK(cudaMemset(b->wk_line, 0, line_bytes));
   CK(cudaMemcpy(b->wk_tab, cols.data(), cols.size() * sizeof(double), cudaMemcpyHostToDevice));
-  b->wk_ntab = ntab;
   b->wk_hwk = hwk;
   b->wk_scale = scale;
   b->wk_tr = transverse != 0;
-  // the line sums hold at most cap particles' weights of 2^wk_fixbits
-  b->wk_fixbits = std::min(40, 62 - ilog2i(b->cap + 1));
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  b->grid_wake = (int)std::max<long long>(
-      1, std::min<long long>((b->cap + 255) / 256, (long long)sms * 8));
   b->wk_on = true;
   ++b->wk_gen;
   return IMPZ_OK;
@@ -941,6 +925,7 @@ int impz_bend_entry(impz_bunch_t b, const impz_elem_t* e) {
   CK(cudaSetDevice(b->device));
   StepParams h[2];
   blank_steps(h);
+  if (e->val[2] > 200) return IMPZ_ERR_UNSUPPORTED;  // CSR bends: the whole-lattice runner
   int r = bend_entry_ops(b->P, *e, b->refptcl, b->sp, b->bend, h[0].post);
   if (r) return r;
   return run_fine_advance(b, h, 0, 1, 0, nullptr);
@@ -1175,6 +1160,7 @@ int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double cur
   b->current0 = current;
   std::memcpy(b->refptcl, refptcl, sizeof(b->refptcl));
   b->z = 0.0;
+  b->csr = CsrState();
   b->stage = ST_IDLE;
   b->bend.active = false;
   b->run_pending = false;
@@ -1194,13 +1180,54 @@ static int launch_step(impz_bunch_t b, bool sc) {
   return IMPZ_OK;
 }
 
+// The wake buffers: a table of ntab rows (read-in wake; 0 for CSR alone),
+// then the line sums [3][nz] and the per-plane field [3][nz] in one
+// allocation, kept while the table size stays.
+static int wake_alloc(impz_bunch_t b, int ntab) {
+  if (b->nz < 2 || b->nz > 4096) return IMPZ_ERR_UNSUPPORTED;
+  CK(exact::prepare_wake());  // outside any stream capture
+  const size_t tab_bytes = round_up((size_t)3 * (ntab > 0 ? ntab : 1) * sizeof(double), kAlign);
+  const size_t line_bytes = round_up((size_t)3 * b->nz * sizeof(unsigned long long), kAlign);
+  const size_t bytes = tab_bytes + line_bytes + (size_t)3 * b->nz * sizeof(double);
+  // the stream may still read the previous buffers
+  CK(cudaStreamSynchronize(b->stream));
+  if (b->wk_mem && b->wk_ntab != ntab && ntab > 0) {
+    cudaFree(b->wk_mem);
+    b->wk_mem = nullptr;
+  }
+  if (!b->wk_mem) {
+    cudaError_t e = cudaMalloc(&b->wk_mem, bytes);
+    if (e != cudaSuccess) {
+      b->wk_mem = nullptr;
+      return e == cudaErrorMemoryAllocation ? IMPZ_ERR_NOMEM : cuda_fail(e, "cudaMalloc");
+    }
+    b->wk_ntab = ntab;
+  }
+  const size_t tb = round_up((size_t)3 * (b->wk_ntab > 0 ? b->wk_ntab : 1) * sizeof(double), kAlign);
+  b->wk_tab = (double*)b->wk_mem;
+  b->wk_line = (unsigned long long*)(b->wk_mem + tb);
+  b->wk_field = (double*)(b->wk_mem + tb + line_bytes);
+  CK(cudaMemset(b->wk_line, 0, line_bytes));
+  // the line sums hold at most cap particles' weights of 2^wk_fixbits
+  b->wk_fixbits = std::min(40, 62 - ilog2i(b->cap + 1));
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  b->grid_wake = (int)std::max<long long>(
+      1, std::min<long long>((b->cap + 255) / 256, (long long)sms * 8));
+  return IMPZ_OK;
+}
+
+// which wake kernels a captured step holds
+static int wake_key(impz_bunch_t b) { return 2 * b->wk_gen + (b->run_csr ? 1 : 0); }
+
 // Two space-charge steps captured as one CUDA graph (parity returns to its
 // start value), cached per start parity and re-captured when the step table
 // or the record buffer move.
 static int graph_pair(impz_bunch_t b) {
   const int p = b->parity;
   if (b->gexec[p] && (b->g_steps[p] != b->dsteps || b->g_mom[p] != b->mom_out ||
-                      b->g_light[p] != b->run_light || b->g_wake[p] != b->wk_gen)) {
+                      b->g_light[p] != b->run_light || b->g_wake[p] != wake_key(b))) {
     cudaGraphExecDestroy(b->gexec[p]);
     b->gexec[p] = nullptr;
   }
@@ -1223,10 +1250,10 @@ static int graph_pair(impz_bunch_t b) {
     b->g_steps[p] = b->dsteps;
     b->g_mom[p] = b->mom_out;
     b->g_light[p] = b->run_light;
-    b->g_wake[p] = b->wk_gen;
+    b->g_wake[p] = wake_key(b);
     b->parity = p;  // capture did not execute anything
   }
-  g_launches += 2 * (12 + (b->wk_on ? 2 : 0));
+  g_launches += 2 * (12 + (b->wk_on || b->run_csr ? 2 : 0));
   CK(cudaGraphLaunch(b->gexec[p], b->stream));
   return IMPZ_OK;
 }
@@ -1242,8 +1269,12 @@ static int run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   b->run_z = b->z;
   std::memcpy(b->run_ref, b->refptcl, sizeof(b->run_ref));
   // conv1st/kick see Bcurr, the input beam current (AccSimulator.f90:1121)
-  int r = compile_lattice(b->P, elems, nelem, b->current0, b->sp, b->run_ref, &b->run_z, L);
+  b->csr_run = b->csr;
+  int r = compile_lattice(b->P, elems, nelem, b->current0, b->sp, b->run_ref, &b->run_z,
+                          b->csr_run, L);
   if (r) return r;
+  b->run_csr = L.has_csr;
+  if (b->run_csr && !b->wk_mem && (r = wake_alloc(b, 0))) return r;
   const int K = L.nsteps;
   b->run_light = table_is_light(L.steps);
   if ((r = ensure_tables(b, K + 2, K + 1))) return r;
@@ -1288,6 +1319,7 @@ static int run_advance(impz_bunch_t b, int budget) {
 static void run_end(impz_bunch_t b) {
   std::memcpy(b->refptcl, b->run_ref, sizeof(b->run_ref));
   b->z = b->run_z;
+  b->csr = b->csr_run;
   b->run_pending = true;
 }
 

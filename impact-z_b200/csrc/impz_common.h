@@ -53,10 +53,13 @@ struct StepParams {
   int sc;              // this step kicks (a deposit and a field solve preceded it)
   int moments;         // record diagnostics after `post`
   int range_next;      // evaluate conv1st of step s+1 after `pre_next`
-  int pad;
+  int csr;             // this step's kick includes the CSR wake (csr_* below)
   double gam;          // -refptcl(6) during this step's conv1st/kick
   double tau;          // tau2 of the kick
   double rad;          // (piperad+piperad2)/2 for this step's conv1st loss test
+  double csr_r0;       // CSR: radius of the bend
+  double csr_s0;       // CSR: distance of the kick from the bend entrance (z - zbleng [+ sentr])
+  double csr_blen;     // CSR: bend length
   double pad2;
 };
 
@@ -152,7 +155,7 @@ struct WakeArgs {
   int fixbits;               // fixed-point resolution of the line sums
   int transverse;            // 1: x/y moments and the transverse wakes too
   int ntab;                  // wake table rows
-  int pad0;
+  int on;                    // the read-in wake is on (else only CSR steps have a field)
   unsigned long long* line;  // [3][nz] int64 sums (density, x, y), left cleared
   const double* table;       // [3][ntab]: longitudinal, x and y wake columns
   double* wfield;            // [3][nz] out: added to Ex, Ey, Ez of plane k

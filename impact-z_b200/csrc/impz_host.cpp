@@ -400,7 +400,6 @@ int bend_entry_ops(const Phys& P, const impz_elem_t& e, double refptcl[6], const
                    BendState& bs, MapProgram& prog) {
   // AccSimulator.f90:1032-1094; dparam(k) = val[k-2]
   const double* dp = e.val - 2;
-  if (dp[4] > 200) return IMPZ_ERR_UNSUPPORTED;  // CSR inside the bend
   if (e.length == 0.0) return IMPZ_ERR_ARG;
   const double blength = e.length;
   bs.active = true;
@@ -485,14 +484,16 @@ void bend_exit_op(const Phys& P, const BendState& bs, const Species& sp, MapProg
 
 // ---------------------------------------------------------------------
 int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double bcurr,
-                    const Species& sp, double refptcl[6], double* zio, CompiledLattice& out) {
+                    const Species& sp, double refptcl[6], double* zio, CsrState& csr,
+                    CompiledLattice& out) {
   struct Half {
     MapProgram prog;
   };
   struct Step {
     MapProgram a, b;
-    int sc;
+    int sc, csr;
     double gam, tau, rad;
+    double csr_r0, csr_s0, csr_blen;
     double z;
     double ref[6];
   };
@@ -519,6 +520,15 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
       int r = bend_entry_ops(P, e, refptcl, sp, bs, pending);
       if (r) return r;
       piperad2 = e.val[3];
+      // AccSimulator.f90:1035-1051, 1088: dparam(4) = val[2]
+      csr.r0 = std::fabs(1.0 / bs.hd0);
+      if (bcurr > 0.0 && e.val[2] > 500) {
+        csr.flagbendcsr = 1;
+        csr.bendlencsr = e.length;
+        csr.sentr = 0.0;
+      } else {
+        csr.flagbendcsr = 0;
+      }
     }
     int ihlf = 0;
     for (int j = 1; j <= bnseg; j++) {
@@ -533,6 +543,14 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
           s.gam = -refptcl[5];
           s.tau = tau2;
           s.rad = (piperad + piperad2) / 2;
+          // CSR inside a bend with dparam(4) > 200, after one with > 500
+          // (AccSimulator.f90:1131-1138, 1374-1385)
+          if (sc_on && (bitype == 4 ? e.val[2] > 200 : csr.flagbendcsr != 0)) {
+            s.csr = 1;
+            s.csr_r0 = csr.r0;
+            s.csr_s0 = bitype == 4 ? z - csr.zbleng : z - csr.zbleng + csr.sentr;
+            s.csr_blen = bitype == 4 ? e.length : csr.bendlencsr;
+          }
         }
         if (bitype == 4) {
           bend_sector_op(P, bs, tau1, sp, prog);
@@ -548,9 +566,12 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
       steps.push_back(s);
     }
     if (bitype == 4) bend_exit_op(P, bs, sp, pending);
+    csr.zbleng = csr.zbleng + e.length;  // AccSimulator.f90:1498-1499
+    csr.sentr = csr.sentr + e.length;
   }
   const int K = (int)steps.size();
   out.nsteps = K;
+  out.has_csr = false;
   out.steps.assign(K + 2, StepParams());
   for (auto& st : out.steps) std::memset(&st, 0, sizeof(st));
   out.zrec.assign(K + 1, 0.0);
@@ -569,6 +590,11 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
       sp_.post = cur.b;
       sp_.moments = 1;
       sp_.sc = cur.sc;
+      sp_.csr = cur.csr;
+      sp_.csr_r0 = cur.csr_r0;
+      sp_.csr_s0 = cur.csr_s0;
+      sp_.csr_blen = cur.csr_blen;
+      if (cur.csr) out.has_csr = true;
       sp_.gam = cur.gam;
       sp_.tau = cur.tau;
       sp_.rad = cur.rad;

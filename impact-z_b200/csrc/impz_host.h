@@ -47,11 +47,23 @@ struct CompiledLattice {
   std::vector<double> zrec;       // z of each record (K+1)
   std::vector<double> refrec;     // refptcl of each record, 6 per record
   int nsteps;
+  bool has_csr;                   // some step kicks with the CSR wake
+};
+// The bend bookkeeping of run_AccSimulator that decides where the CSR wake
+// acts (AccSimulator.f90:638-740, 1032-1051, 1131-1138, 1498-1499).
+struct CsrState {
+  double zbleng = 0.0;      // sum of the lengths of the elements passed
+  double sentr = 0.0;       // distance from the last CSR bend's entrance
+  double bendlencsr = 0.0;  // that bend's length
+  double r0 = 0.0;          // radius of the last bend
+  int flagbendcsr = 0;      // the last bend had dparam(4) > 500
 };
 // run_AccSimulator's element/segment loop (AccSimulator.f90:742-1504)
-// turned into a step table.  refptcl and z advance to the lattice exit.
+// turned into a step table.  refptcl, z and the CSR state advance to the
+// lattice exit.
 int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double bcurr,
-                    const Species& sp, double refptcl[6], double* z, CompiledLattice& out);
+                    const Species& sp, double refptcl[6], double* z, CsrState& csr,
+                    CompiledLattice& out);
 
 // diagnostic1_Output rank-0 formulas (Output.f90:247-352)
 void diag_row(const Phys& P, double z, const double rec[IMPZ_MOMREC], const double refptcl[6],

@@ -83,6 +83,7 @@ struct PoissonBuffers {
   const double2* tw64z;
   DevState* st;
   const double* wake;       // per-plane {dEx, dEy, dEz}[nz] added to E, or null
+  unsigned long long* wake_line;  // the wake's [3][nz] line sums, cleared with the charge
 };
 
 template <typename T>

@@ -1235,6 +1235,7 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_wake_line(WakeArgs a) {
   const DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
+  if (!a.steps[s].csr && !a.on) return;  // no wake acts in this step
   const double gam = a.steps[s].gam, rad = a.steps[s].rad;
   const long long n = st->nlocal;
   const int nz = a.nz;
@@ -1306,29 +1307,236 @@ __device__ __forceinline__ double wake_green(const double* e, int ntab, double h
   return e0 * ab + e1 * (1.0 - ab);
 }
 
-// Read-in wakefield, step part 2 (one block): the line charge density
-// recvdensz (AccSimulator.f90:1297-1322), its convolution with the wake
-// table (wakefieldread_FieldQuant, Field.f90:783-1001) and the per-plane
-// field that kick1wake adds to the node fields (BeamBunch.f90:5015-5033).
-// The reference convolves on a doubled grid by FFT with a Green function
-// that is 0.5 W(0) at 0, zero at 1..Nz-1 and W((2Nz-k) hz) above; for k < Nz
-// that circular convolution is the causal sum
+// 1D CSR wake with integrated Green functions (csrwakeTrIGF_FieldQuant,
+// Field.f90:1003-1303): the field at node i of the line density rho on the
+// lab-frame grid ptmin + (i-1) hx, for a bend of radius r0 and length
+// blength.  Sources within the entrance transient use case A, the steady
+// state case B, and past the bend exit cases C and D; case D's retarded
+// angle solves a quartic by Newton-Raphson with a bisection safeguard in a
+// bracket (the published "rtsafe" method), with the reference's handling
+// of the bracket ends and its 100-step limit.  One thread per node.
+struct CsrKernel {
+  double r0, gam, xk2, g3, epstol;
+  __device__ double caseA(double phih, double ssh) const {
+    const double p2 = phih * phih, p3 = p2 * phih, p4 = p3 * phih;
+    const double bb = 2 * phih + p3 / 3 - 2 * ssh;
+    const double cc = p2 + p4 / 12 - 2 * ssh * phih;
+    const double yh = (-bb + sqrt(bb * bb - 4 * cc)) / 2;
+    const double phpy = phih + yh;
+    return xk2 * (-(2 * phpy + p3) / (phpy * phpy + p4 / 4) + 1.0 / ssh);
+  }
+  __device__ double caseB(double ssh) const {
+    const double aa = sqrt(64.0 + 144.0 * (ssh * ssh));
+    const double uuh = pow(aa + 12 * ssh, 1.0 / 3.0) - pow(aa - 12 * ssh, 1.0 / 3.0);
+    const double u2 = uuh * uuh;
+    return xk2 * (-4 * uuh * (u2 + 8) / ((u2 + 4.0) * (u2 + 12.0)));
+  }
+  __device__ double caseC(double phimh, double xxbarh, double ssh) const {
+    const double p2 = phimh * phimh, p3 = p2 * phimh;
+    const double bb = 2 * (phimh + xxbarh) - 2 * ssh + p3 / 3 + p2 * xxbarh;
+    const double cc = (phimh + xxbarh) * (phimh + xxbarh) +
+                      p2 * (p2 + 4 * phimh * xxbarh) / 12 - 2 * ssh * (phimh + xxbarh);
+    const double yh = (-bb + sqrt(bb * bb - 4 * cc)) / 2;
+    const double pa = phimh + xxbarh + yh;
+    const double pb = phimh * xxbarh + phimh * phimh / 2.0;
+    return xk2 * (-2.0 * (pa + phimh * pb) / (pa * pa + pb * pb) + 1.0 / ssh);
+  }
+  __device__ static void quartic(double psi, double xxh, double ds, double& f, double& df) {
+    const double p2 = psi * psi, p3 = p2 * psi, p4 = p3 * psi;
+    f = p4 / 12 + xxh * p3 / 3 + p2 + (2 * xxh - 2 * ds) * psi - 2 * ds * xxh + xxh * xxh;
+    df = p3 / 3 + xxh * p2 + 2 * psi + 2 * xxh - 2 * ds;
+  }
+  __device__ static double root(double x1, double x2, double xacc, double ds, double xxh) {
+    double fl, fh, f, df, xl, xh;
+    quartic(x1, xxh, ds, fl, df);
+    quartic(x2, xxh, ds, fh, df);
+    if (fabs(fl) < xacc) return x1;
+    if (fabs(fh) < xacc) return x2;
+    if (fl < 0.0) { xl = x1; xh = x2; } else { xh = x1; xl = x2; }
+    double rts = 0.5 * (x1 + x2);
+    double dxold = fabs(x2 - x1), dx = dxold;
+    quartic(rts, xxh, ds, f, df);
+    for (int j = 1; j <= 100; j++) {
+      if (((rts - xh) * df - f) * ((rts - xl) * df - f) > 0.0 ||
+          fabs(2.0 * f) > fabs(dxold * df)) {
+        dxold = dx;
+        dx = 0.5 * (xh - xl);
+        rts = xl + dx;
+        if (xl == rts) return rts;
+      } else {
+        dxold = dx;
+        dx = f / df;
+        const double temp = rts;
+        rts = rts - dx;
+        if (temp == rts) return rts;
+      }
+      if (fabs(dx) < xacc) return rts;
+      quartic(rts, xxh, ds, f, df);
+      if (f < 0.0) xl = rts; else xh = rts;
+    }
+    return rts;
+  }
+  __device__ double caseD(double xxbarh, double psimax, double ssh) const {
+    const double psi = root(-epstol, psimax * (1.0 + epstol), epstol, ssh, xxbarh);
+    const double pa = psi + xxbarh;
+    const double pb = psi * (xxbarh + psi / 2.0);
+    return xk2 * (-2.0 * (pa + psi * pb) / (pa * pa + pb * pb) + 1.0 / ssh);
+  }
+};
+
+__device__ double csr_node(int i, const double* __restrict__ rho, double r0, double ptmin,
+                           double hx, double blength, double gam) {
+  const double pilc = 2 * asin(1.0);
+  const double phim = blength / r0;
+  const double xconst = 1.0 / (4 * pilc * 8.854187817e-12);
+  CsrKernel K;
+  K.r0 = r0;
+  K.gam = gam;
+  K.xk2 = gam / r0;
+  K.g3 = gam * gam * gam;
+  K.epstol = 2.0e-9;
+  if (i == 1) return 0.0;
+  const double xx = ptmin + (i - 1) * hx;
+  const double t = xx / r0;
+  const double xxl = t * t * t * r0 / 24;
+  const int ni = i;
+  double e = 0.0;
+#define RHO(j) rho[(j)-1]
+#define SSH(xxp) ((xx - (xxp)) * K.g3 / r0)
+  if (xx <= 0) {
+  } else if (xx <= blength) {
+    const double xslp = (xx / r0) * r0 / 2 / gam / gam + xxl;
+    const int islp1 = (int)((xx - xslp - ptmin) / hx) + 1;
+    const double phih = xx / r0 * gam;
+    for (int j = 2; j <= islp1 - 1; j++) {
+      const double c2 = K.caseA(phih, SSH(ptmin + (j - 1) * hx + hx / 2));
+      const double c1 = K.caseA(phih, SSH(ptmin + (j - 1) * hx - hx / 2));
+      e = e + RHO(j) * (c1 - c2);
+    }
+    if (islp1 >= 2) {
+      double c2 = K.caseA(phih, SSH(xx - xslp));
+      double c1 = K.caseA(phih, SSH(ptmin + (islp1 - 1) * hx - hx / 2));
+      e = e + RHO(islp1) * (c1 - c2);
+      c2 = K.caseA(phih, SSH(ptmin + hx / 2));
+      c1 = K.caseA(phih, SSH(ptmin));
+      e = e + RHO(1) * (c1 - c2);
+    } else if (islp1 == 1) {
+      const double c2 = K.caseA(phih, SSH(xx - xslp));
+      const double c1 = K.caseA(phih, SSH(ptmin + (islp1 - 1) * hx));
+      e = e + RHO(islp1) * (c1 - c2);
+    }
+    const int jstart = islp1 > 1 ? islp1 : 1;
+    for (int j = jstart + 2; j <= ni - 1; j++) {
+      const double c2 = K.caseB(SSH(ptmin + (j - 1) * hx + hx / 2));
+      const double c1 = K.caseB(SSH(ptmin + (j - 1) * hx - hx / 2));
+      e = e + RHO(j) * (c1 - c2);
+    }
+    if (jstart <= ni - 2) {
+      double c2 = K.caseB(SSH(ptmin + (ni - 1) * hx));
+      double c1 = K.caseB(SSH(ptmin + (ni - 1) * hx - hx / 2));
+      e = e + RHO(ni) * (c1 - c2);
+      if (islp1 < 1) {
+        c2 = K.caseB(SSH(ptmin + hx / 2));
+        c1 = K.caseB(SSH(ptmin));
+        e = e + RHO(1) * (c1 - c2);
+      } else {
+        const int j = islp1 + 1;
+        c2 = K.caseB(SSH(ptmin + (j - 1) * hx + hx / 2));
+        c1 = K.caseB(SSH(xx - xslp));
+        e = e + RHO(j) * (c1 - c2);
+      }
+    } else if (jstart == ni - 1) {
+      const double c2 = K.caseB(SSH(ptmin + (ni - 1) * hx));
+      const double c1 = K.caseB(SSH(xx - xslp));
+      e = e + RHO(ni) * (c1 - c2);
+    }
+  } else {
+    const double xxbar = xx - blength;
+    const double rp = r0 * phim;
+    const double xslp = (rp + xxbar) / 2 / gam / gam +
+                        r0 * (phim * phim * phim) / 24 * (rp + 4 * xxbar) / (rp + xxbar);
+    const int islp1 = (int)((xx - xslp - ptmin) / hx) + 1;
+    const double xslpN = xxbar / 2.0 / gam / gam;
+    const int islpN1 = (int)((xx - xslpN - ptmin) / hx) + 1;
+    const double xxbarh = xxbar * gam / r0;
+    const double phimh = phim * gam;
+    for (int j = 2; j <= islp1 - 1; j++) {
+      const double c2 = K.caseC(phimh, xxbarh, SSH(ptmin + (j - 1) * hx + hx / 2));
+      const double c1 = K.caseC(phimh, xxbarh, SSH(ptmin + (j - 1) * hx - hx / 2));
+      e = e + RHO(j) * (c1 - c2);
+    }
+    if (islp1 >= 2) {
+      double c2 = K.caseC(phimh, xxbarh, SSH(xx - xslp));
+      double c1 = K.caseC(phimh, xxbarh, SSH(ptmin + (islp1 - 1) * hx - hx / 2));
+      e = e + RHO(islp1) * (c1 - c2);
+      c2 = K.caseC(phimh, xxbarh, SSH(ptmin + hx / 2));
+      c1 = K.caseC(phimh, xxbarh, SSH(ptmin));
+      e = e + RHO(1) * (c1 - c2);
+    } else if (islp1 == 1) {
+      const double c2 = K.caseC(phimh, xxbarh, SSH(xx - xslp));
+      const double c1 = K.caseC(phimh, xxbarh, SSH(ptmin));
+      e = e + RHO(islp1) * (c1 - c2);
+    }
+    const double psimax = phim * gam;
+    const int jstart = islp1 > 0 ? islp1 : 0;
+    for (int j = jstart + 2; j <= islpN1 - 1; j++) {
+      const double c2 = K.caseD(xxbarh, psimax, SSH(ptmin + (j - 1) * hx + hx / 2));
+      const double c1 = K.caseD(xxbarh, psimax, SSH(ptmin + (j - 1) * hx - hx / 2));
+      e = e + RHO(j) * (c1 - c2);
+    }
+    if (islpN1 >= jstart + 2) {
+      double c2 = K.caseD(xxbarh, psimax, xslpN * K.g3 / r0);
+      double c1 = K.caseD(xxbarh, psimax, SSH(ptmin + (islpN1 - 1) * hx - hx / 2));
+      e = e + RHO(islpN1) * (c1 - c2);
+      c2 = K.caseD(xxbarh, psimax, SSH(ptmin + jstart * hx + hx / 2));
+      c1 = K.caseD(xxbarh, psimax, xslp * K.g3 / r0);
+      e = e + RHO(jstart + 1) * (c1 - c2);
+    } else if (islpN1 == jstart + 1) {
+      const double c2 = K.caseD(xxbarh, psimax, xslpN * K.g3 / r0);
+      const double c1 = K.caseD(xxbarh, psimax, xslp * K.g3 / r0);
+      e = e + RHO(jstart + 1) * (c1 - c2);
+    }
+  }
+#undef SSH
+#undef RHO
+  return e * xconst;
+}
+
+// Wake step part 2: the line charge density recvdensz
+// (AccSimulator.f90:1297-1322 and 1360-1368) and from it the per-plane field
+// that kick1wake adds to the node fields before the gather
+// (BeamBunch.f90:5015-5033).  A step with CSR takes the CSR wake
+// (AccSimulator.f90:1344-1390, which replaces a read-in wake), else the
+// read-in wake, else the field is zero.  The read-in wake: the reference
+// convolves on a doubled grid by FFT (wakefieldread_FieldQuant,
+// Field.f90:783-1001) with a Green function that is 0.5 W(0) at 0, zero at
+// 1..Nz-1 and W((2Nz-k) hz) above; for k < Nz that circular convolution is
+// the causal sum
 //   conv_z(k) = 0.5 W(0) d(k) + sum_{m>k} d(m) W((m-k) hz),
-// evaluated here directly (Nz^2/2 terms), and the transverse ones (zero at 0
-// too) conv_x(k) = sum_{m>k} d(m) xbar(m) Wx((m-k) hz).  Clears the line
-// sums for the next step.
-__global__ void __launch_bounds__(1024) k_wake_field(WakeArgs a) {
+// evaluated here directly, and the transverse ones (zero at 0 too)
+// conv_x(k) = sum_{m>k} d(m) xbar(m) Wx((m-k) hz).  Every block builds the
+// density in shared memory; each thread then owns one plane.  The line sums
+// are cleared by the field kernel that follows.
+__global__ void __launch_bounds__(256) k_wake_field(WakeArgs a) {
   extern __shared__ double wsm[];
   const int nz = a.nz;
+  const DevState* st = a.st;
+  const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
+  const StepParams& sp = a.steps[s];
+  const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!sp.csr && !a.on) {
+    if (kk < nz) a.wfield[kk] = a.wfield[nz + kk] = a.wfield[2 * nz + kk] = 0.0;
+    return;
+  }
+  const bool csr = sp.csr != 0;
+  const bool tr = !csr && a.transverse;
   double* d = wsm;
   double* dx = wsm + nz;
   double* dy = wsm + 2 * nz;
   double* gz = wsm + 3 * nz;
   double* gx = wsm + 4 * nz;
   double* gy = wsm + 5 * nz;
-  const DevState* st = a.st;
-  const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
-  const double gam = a.steps[s].gam;
+  const double gam = sp.gam;
   const double cur = st->current;
   const double npt = (double)st->npt;
   double hzw = (st->geom.range[5] - st->geom.range[4]) / (nz - 1);
@@ -1344,43 +1552,50 @@ __global__ void __launch_bounds__(1024) k_wake_field(WakeArgs a) {
     const double dens = (double)(long long)a.line[k] / sc;
     const double dk = dens * cur / a.k.Scfreq / npt / hzw * chrg / fabs(chrg);
     double xw = 0.0, yw = 0.0;
-    if (a.transverse && dens != 0.0) {
+    if (tr && dens != 0.0) {
       xw = ((double)(long long)a.line[nz + k] / sx) / dens;
       yw = ((double)(long long)a.line[2 * nz + k] / sy) / dens;
     }
     d[k] = dk;
-    dx[k] = dk * xw;
-    dy[k] = dk * yw;
-    gz[k] = wake_green(a.table, ntab, a.hwk, k, hzw);
-    gx[k] = a.transverse ? wake_green(a.table + ntab, ntab, a.hwk, k, hzw) : 0.0;
-    gy[k] = a.transverse ? wake_green(a.table + 2 * ntab, ntab, a.hwk, k, hzw) : 0.0;
-    a.line[k] = 0ull;
-    a.line[nz + k] = 0ull;
-    a.line[2 * nz + k] = 0ull;
+    if (!csr) {
+      dx[k] = dk * xw;
+      dy[k] = dk * yw;
+      gz[k] = wake_green(a.table, ntab, a.hwk, k, hzw);
+      gx[k] = tr ? wake_green(a.table + ntab, ntab, a.hwk, k, hzw) : 0.0;
+      gy[k] = tr ? wake_green(a.table + 2 * ntab, ntab, a.hwk, k, hzw) : 0.0;
+    }
   }
   __syncthreads();
+  const int k = kk;
+  if (k >= nz) return;
   double xycon, tcon;
   kick_consts(a.k, gam, cur, xycon, tcon);
+  if (csr) {
+    const double zwkmin = st->geom.range[4] / gam + sp.csr_s0;
+    const double ez = csr_node(k + 1, d, sp.csr_r0, zwkmin, hzw, sp.csr_blen, gam);
+    a.wfield[k] = 0.0;
+    a.wfield[nz + k] = 0.0;
+    a.wfield[2 * nz + k] = chrg * ez / tcon / mass / a.unit;
+    return;
+  }
   const double bet = sqrt(gam * gam - 1.0) / gam;
   const double g0 = 0.5 * gz[0];
-  for (int k = threadIdx.x; k < nz; k += blockDim.x) {
-    double cz = d[k] * g0, cx = 0.0, cy = 0.0;
-    if (a.transverse) {
-      for (int m = k + 1; m < nz; m++) {
-        cz = cz + d[m] * gz[m - k];
-        cx = cx + dx[m] * gx[m - k];
-        cy = cy + dy[m] * gy[m - k];
-      }
-    } else {
-      for (int m = k + 1; m < nz; m++) cz = cz + d[m] * gz[m - k];
+  double cz = d[k] * g0, cx = 0.0, cy = 0.0;
+  if (tr) {
+    for (int m = k + 1; m < nz; m++) {
+      cz = cz + d[m] * gz[m - k];
+      cx = cx + dx[m] * gx[m - k];
+      cy = cy + dy[m] * gy[m - k];
     }
-    const double ezwake = a.scale * (-cz * hzw);
-    const double exwake = a.scale * (cx * hzw);
-    const double eywake = a.scale * (cy * hzw);
-    a.wfield[k] = chrg * exwake / xycon / mass / bet / gam / a.unit;
-    a.wfield[nz + k] = chrg * eywake / xycon / mass / bet / gam / a.unit;
-    a.wfield[2 * nz + k] = chrg * ezwake / tcon / mass / a.unit;
+  } else {
+    for (int m = k + 1; m < nz; m++) cz = cz + d[m] * gz[m - k];
   }
+  const double ezwake = a.scale * (-cz * hzw);
+  const double exwake = a.scale * (cx * hzw);
+  const double eywake = a.scale * (cy * hzw);
+  a.wfield[k] = chrg * exwake / xycon / mass / bet / gam / a.unit;
+  a.wfield[nz + k] = chrg * eywake / xycon / mass / bet / gam / a.unit;
+  a.wfield[2 * nz + k] = chrg * ezwake / tcon / mass / a.unit;
 }
 
 }  // namespace IMPZ_NS

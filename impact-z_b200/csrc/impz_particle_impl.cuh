@@ -61,7 +61,7 @@ cudaError_t launch_wake(const WakeArgs& a, int grid, cudaStream_t s) {
   k_wake_line<IMPZ_WAKE_BLOCK><<<grid, IMPZ_WAKE_BLOCK, 0, s>>>(a);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_wake_field<<<1, 1024, (size_t)6 * a.nz * sizeof(double), s>>>(a);
+  k_wake_field<<<(a.nz + 255) / 256, 256, (size_t)6 * a.nz * sizeof(double), s>>>(a);
   return cudaGetLastError();
 }
 

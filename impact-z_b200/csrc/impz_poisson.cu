@@ -201,7 +201,8 @@ template <typename T>
 cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s) {
   const long long G = (long long)b.nx * b.ny * b.nz;
   return launch_pdl(k_efield<T>, dim3(grid_for(G, 256)), dim3(256), 0, s, b.nx, b.ny, b.nz,
-                    (const T*)b.phi, (const DevState*)b.st, (T*)b.efield, b.rho, b.wake);
+                    (const T*)b.phi, (const DevState*)b.st, (T*)b.efield, b.rho, b.wake,
+                    b.wake_line);
 }
 
 template cudaError_t launch_green<double>(const PoissonBuffers&, cudaStream_t);

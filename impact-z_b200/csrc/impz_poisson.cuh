@@ -472,15 +472,19 @@ __global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long 
 // kick1_BeamBunch finite differences (BeamBunch.f90:1784-2005), one rank,
 // open BC: centred inside, one-sided on the faces.  Out: {Ex,Ey,Ez,0}.
 // Also clears the charge grid (its last reader, the forward transform, is
-// done) for the next deposit.  With a read-in wake, adds its per-plane field
-// wake = {dEx, dEy, dEz}[nz] to every node of the plane (kick1wake,
-// BeamBunch.f90:5015-5033).
+// done) for the next deposit.  With a wake (read-in or CSR), adds its
+// per-plane field wake = {dEx, dEy, dEz}[nz] to every node of the plane
+// (kick1wake, BeamBunch.f90:5015-5033) and clears the wake's line sums.
 template <typename T>
 __global__ void k_efield(int nx, int ny, int nz, const T* __restrict__ phi,
                          const DevState* st, T* __restrict__ E,
                          unsigned long long* __restrict__ rho,
-                         const double* __restrict__ wake) {
+                         const double* __restrict__ wake,
+                         unsigned long long* __restrict__ wake_line) {
   griddep_wait();
+  if (wake_line)
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 3 * nz; e += gridDim.x * blockDim.x)
+      wake_line[e] = 0ull;
   const long long G = (long long)nx * ny * nz;
   const T hxi = (T)st->geom.hi[0], hyi = (T)st->geom.hi[1], hzi = (T)st->geom.hi[2];
   const T half = (T)0.5;

@@ -50,7 +50,8 @@ typedef struct impz_bunch_s* impz_bunch_t;
  * (src/Contrl/Input.f90:300-315).  Param(1) of the reference element is
  * zedge, Param(k) = val[k-2] for k >= 2 (AccSimulator.f90:262-330).
  * Supported types: 0 drift, 1 quadrupole (gradient, or K map when
- * v2 in (-10,-1e-6)), 4 dipole (file ID v3 <= 200: no CSR), 101..106 RF gaps
+ * v2 in (-10,-1e-6)), 4 dipole (file ID v3 <= 200: no CSR; above 200 CSR
+ * inside the bend, above 500 also downstream: impz_run only), 101..106 RF gaps
  * as the ideal-RF model (v4 < 0) and 103 (CCL) as the RK6 linear map over
  * the on-axis table zdat/edat/epdat/eppdat (rfdataN.in, read1_Data). */
 typedef struct {
@@ -89,8 +90,9 @@ int impz_bunch_destroy(impz_bunch_t b);
 /* Device bytes a bunch of n particles on an nx*ny*nz grid holds while it runs
  * a lattice of nsteps steps (0: the bunch alone), at the driver's 2 MiB
  * allocation granularity: the bunch is one allocation, the run tables a
- * second, and no other call allocates but impz_wake_set (its table and
- * per-step buffers, a few 10 KB).  The serving loop admits by it.
+ * second, and no other call allocates but impz_wake_set and the first run
+ * with CSR steps (the wake table and per-step line buffers, a few 10 KB).
+ * The serving loop admits by it.
  * No reference counterpart (the reference allocates per process). */
 long long impz_bunch_footprint(long long n, int nx, int ny, int nz, int form, int flags,
                                int nsteps);
@@ -125,7 +127,9 @@ void* impz_bunch_stream(impz_bunch_t b);
 int impz_map_half(impz_bunch_t b, const impz_elem_t* e, double zedge, double* z, double tau,
                   int nst, int* ihlf);
 /* Fpol_Dipole at a bend entrance with the constants of AccSimulator.f90:
- * 1057-1093, after refptcl(5) += L/(Scxl*beta0) (AccSimulator.f90:1063). */
+ * 1057-1093, after refptcl(5) += L/(Scxl*beta0) (AccSimulator.f90:1063).
+ * IMPZ_ERR_UNSUPPORTED for a CSR bend (file ID v3 > 200): the whole-lattice
+ * runner carries the CSR wake. */
 int impz_bend_entry(impz_bunch_t b, const impz_elem_t* e);
 /* Sector_Dipole(tau) inside the bend entered last (Dipole.f90:693-788); *z += tau. */
 int impz_bend_sector(impz_bunch_t b, double* z, double tau);
@@ -161,9 +165,14 @@ int impz_diag_row(double z, const double rec[IMPZ_MOMREC], const double refptcl[
 
 /* ---- whole-lattice runner ---------------------------------------------- */
 /* run_AccSimulator's element/segment loop (AccSimulator.f90:742-1504) for
- * Flagmap=1, Flagbc=1, Flagerr=0, no wake/CSR, one rank, over elements
- * [0,nelem).  Every step is one fused particle pass plus deposit and field
- * solve, replayed from a CUDA graph.  recs (capacity maxrec records of
+ * Flagmap=1, Flagbc=1, Flagerr=0, one rank, over elements [0,nelem).
+ * Every step is one fused particle pass plus deposit and field solve,
+ * replayed from a CUDA graph; with a read-in wake on (impz_wake_set) or in
+ * and after CSR bends the step adds the wake's line density and field
+ * kernels.  The CSR bookkeeping (AccSimulator.f90:1035-1051, 1131-1138,
+ * 1498-1499: lengths passed, distance from the last CSR bend) carries from
+ * one run to the next, as one element loop of the reference would; upload
+ * resets it.  recs (capacity maxrec records of
  * IMPZ_MOMREC doubles, may be NULL) receives the initial record and one per
  * step; zs (may be NULL) the z of each record; *nrec their number. */
 int impz_run(impz_bunch_t b, const impz_elem_t* elems, int nelem, double* recs, double* zs,

@@ -1300,6 +1300,252 @@ void orc_wake_field(int nz, const double *densz, const double *xsum, const doubl
 }
 
 /* ------------------------------------------------------------------ */
+/* 1D CSR wake with integrated Green functions, steady state and transients
+ * (csrwakeTrIGF_FieldQuant, Field.f90:1003-1251, with IcsrCaseA..D at
+ * Field.f90:1253-1303).  Case D's retarded angle is the root of the quartic
+ * of funcd (Field.f90:1370-1388), found by Newton-Raphson with bisection
+ * safeguard in a bracket, the published "rtsafe" method (Numerical Recipes
+ * 9.4) as the reference's `root` (Field.f90:1305-1368) applies it: a
+ * bracket end within xacc of a root is returned as is; no bracket or no
+ * convergence in maxit steps returns the last iterate. */
+static double csr_caseA(double phih, double ssh, double xk2) {
+  const double p2 = phih * phih, p3 = p2 * phih, p4 = p3 * phih;
+  const double bb = 2 * phih + p3 / 3 - 2 * ssh;
+  const double cc = p2 + p4 / 12 - 2 * ssh * phih;
+  const double yh = (-bb + sqrt(bb * bb - 4 * cc)) / 2;
+  const double phpy = phih + yh;
+  return xk2 * (-(2 * phpy + p3) / (phpy * phpy + p4 / 4) + 1.0 / ssh);
+}
+
+static double csr_caseB(double ssh, double xk2) {
+  const double aa = sqrt(64.0 + 144.0 * (ssh * ssh));
+  const double uuh = pow(aa + 12 * ssh, 1.0 / 3.0) - pow(aa - 12 * ssh, 1.0 / 3.0);
+  const double u2 = uuh * uuh;
+  return xk2 * (-4 * uuh * (u2 + 8) / ((u2 + 4.0) * (u2 + 12.0)));
+}
+
+static double csr_caseC(double phimh, double xxbarh, double ssh, double xk2) {
+  const double p2 = phimh * phimh, p3 = p2 * phimh;
+  const double bb = 2 * (phimh + xxbarh) - 2 * ssh + p3 / 3 + p2 * xxbarh;
+  const double cc = (phimh + xxbarh) * (phimh + xxbarh) +
+                    p2 * (p2 + 4 * phimh * xxbarh) / 12 - 2 * ssh * (phimh + xxbarh);
+  const double yh = (-bb + sqrt(bb * bb - 4 * cc)) / 2;
+  const double pa = phimh + xxbarh + yh;
+  const double pb = phimh * xxbarh + phimh * phimh / 2.0;
+  return xk2 * (-2.0 * (pa + phimh * pb) / (pa * pa + pb * pb) + 1.0 / ssh);
+}
+
+static void csr_quartic(double psi, double xxh, double ds, double *f, double *df) {
+  const double p2 = psi * psi, p3 = p2 * psi, p4 = p3 * psi;
+  *f = p4 / 12 + xxh * p3 / 3 + p2 + (2 * xxh - 2 * ds) * psi - 2 * ds * xxh + xxh * xxh;
+  *df = p3 / 3 + xxh * p2 + 2 * psi + 2 * xxh - 2 * ds;
+}
+
+static double csr_root(double x1, double x2, double xacc, int maxit, double ds, double xxh) {
+  double fl, fh, f, df, xl, xh;
+  csr_quartic(x1, xxh, ds, &fl, &df);
+  csr_quartic(x2, xxh, ds, &fh, &df);
+  if (fabs(fl) < xacc) return x1;
+  if (fabs(fh) < xacc) return x2;
+  if (fl < 0.0) { xl = x1; xh = x2; } else { xh = x1; xl = x2; }
+  double rts = 0.5 * (x1 + x2);
+  double dxold = fabs(x2 - x1), dx = dxold;
+  csr_quartic(rts, xxh, ds, &f, &df);
+  for (int j = 1; j <= maxit; j++) {
+    if (((rts - xh) * df - f) * ((rts - xl) * df - f) > 0.0 || fabs(2.0 * f) > fabs(dxold * df)) {
+      dxold = dx;
+      dx = 0.5 * (xh - xl);
+      rts = xl + dx;
+      if (xl == rts) return rts;
+    } else {
+      dxold = dx;
+      dx = f / df;
+      const double temp = rts;
+      rts = rts - dx;
+      if (temp == rts) return rts;
+    }
+    if (fabs(dx) < xacc) return rts;
+    csr_quartic(rts, xxh, ds, &f, &df);
+    if (f < 0.0) xl = rts; else xh = rts;
+  }
+  return rts;
+}
+
+static double csr_caseD(double xxbarh, double psimax, double ssh, double xk2, double epstol,
+                        int nmax) {
+  const double psi = csr_root(-epstol, psimax * (1.0 + epstol), epstol, nmax, ssh, xxbarh);
+  const double pa = psi + xxbarh;
+  const double pb = psi * (xxbarh + psi / 2.0);
+  return xk2 * (-2.0 * (pa + psi * pb) / (pa * pa + pb * pb) + 1.0 / ssh);
+}
+
+void orc_csr_wake(int nx, double r0, double ptmin, double hx, double blength,
+                  const double *rho, double gam, double *ez) {
+  const double epstol = 2.0e-9;
+  const int nmax = 100;
+  const double pilc = 2 * asin(1.0);
+  const double phim = blength / r0;
+  const double xconst = 1.0 / (4 * pilc * 8.854187817e-12);
+  const double xk2 = gam / r0;
+  const double g3 = gam * gam * gam;
+#define RHO(j) rho[(j)-1]
+#define SSH(xxp) ((xx - (xxp)) * g3 / r0)
+  ez[0] = 0.0;
+  for (int i = 2; i <= nx; i++) {
+    const double xx = ptmin + (i - 1) * hx;
+    const double t = xx / r0;
+    const double xxl = t * t * t * r0 / 24;
+    const int ni = i;
+    double e = 0.0;
+    if (xx <= 0) {
+    } else if (xx <= blength) {
+      const double xslp = (xx / r0) * r0 / 2 / gam / gam + xxl;
+      const int islp0 = (int)((xx - xslp - ptmin) / hx);
+      const int islp1 = islp0 + 1;
+      const double phih = xx / r0 * gam;
+      /* Case A (entrance transient) */
+      for (int j = 2; j <= islp1 - 1; j++) {
+        const double c2 = csr_caseA(phih, SSH(ptmin + (j - 1) * hx + hx / 2), xk2);
+        const double c1 = csr_caseA(phih, SSH(ptmin + (j - 1) * hx - hx / 2), xk2);
+        e = e + RHO(j) * (c1 - c2);
+      }
+      if (islp1 >= 2) {
+        double c2 = csr_caseA(phih, SSH(xx - xslp), xk2);
+        double c1 = csr_caseA(phih, SSH(ptmin + (islp1 - 1) * hx - hx / 2), xk2);
+        e = e + RHO(islp1) * (c1 - c2);
+        c2 = csr_caseA(phih, SSH(ptmin + hx / 2), xk2);
+        c1 = csr_caseA(phih, SSH(ptmin), xk2);
+        e = e + RHO(1) * (c1 - c2);
+      } else if (islp1 == 1) {
+        const double c2 = csr_caseA(phih, SSH(xx - xslp), xk2);
+        const double c1 = csr_caseA(phih, SSH(ptmin + (islp1 - 1) * hx), xk2);
+        e = e + RHO(islp1) * (c1 - c2);
+      }
+      /* Case B (steady state) */
+      const int jstart = islp1 > 1 ? islp1 : 1;
+      for (int j = jstart + 2; j <= ni - 1; j++) {
+        const double c2 = csr_caseB(SSH(ptmin + (j - 1) * hx + hx / 2), xk2);
+        const double c1 = csr_caseB(SSH(ptmin + (j - 1) * hx - hx / 2), xk2);
+        e = e + RHO(j) * (c1 - c2);
+      }
+      if (jstart <= ni - 2) {
+        double c2 = csr_caseB(SSH(ptmin + (ni - 1) * hx), xk2);
+        double c1 = csr_caseB(SSH(ptmin + (ni - 1) * hx - hx / 2), xk2);
+        e = e + RHO(ni) * (c1 - c2);
+        if (islp1 < 1) {
+          const int j = 1;
+          c2 = csr_caseB(SSH(ptmin + (j - 1) * hx + hx / 2), xk2);
+          c1 = csr_caseB(SSH(ptmin + (j - 1) * hx), xk2);
+          e = e + RHO(j) * (c1 - c2);
+        } else {
+          const int j = islp1 + 1;
+          c2 = csr_caseB(SSH(ptmin + (j - 1) * hx + hx / 2), xk2);
+          c1 = csr_caseB(SSH(xx - xslp), xk2);
+          e = e + RHO(j) * (c1 - c2);
+        }
+      } else if (jstart == ni - 1) {
+        const int j = ni;
+        const double c2 = csr_caseB(SSH(ptmin + (j - 1) * hx), xk2);
+        const double c1 = csr_caseB(SSH(xx - xslp), xk2);
+        e = e + RHO(j) * (c1 - c2);
+      }
+    } else {
+      const double xxbar = xx - blength;
+      const double rp = r0 * phim;
+      const double xslp = (rp + xxbar) / 2 / gam / gam +
+                          r0 * (phim * phim * phim) / 24 * (rp + 4 * xxbar) / (rp + xxbar);
+      const int islp0 = (int)((xx - xslp - ptmin) / hx);
+      const int islp1 = islp0 + 1;
+      const double xslpN = xxbar / 2.0 / gam / gam;
+      const int islpN = (int)((xx - xslpN - ptmin) / hx);
+      const int islpN1 = islpN + 1;
+      /* Case C (exit transient, source in the bend) */
+      const double xxbarh = xxbar * gam / r0;
+      const double phimh = phim * gam;
+      for (int j = 2; j <= islp1 - 1; j++) {
+        const double c2 = csr_caseC(phimh, xxbarh, SSH(ptmin + (j - 1) * hx + hx / 2), xk2);
+        const double c1 = csr_caseC(phimh, xxbarh, SSH(ptmin + (j - 1) * hx - hx / 2), xk2);
+        e = e + RHO(j) * (c1 - c2);
+      }
+      if (islp1 >= 2) {
+        double c2 = csr_caseC(phimh, xxbarh, SSH(xx - xslp), xk2);
+        double c1 = csr_caseC(phimh, xxbarh, SSH(ptmin + (islp1 - 1) * hx - hx / 2), xk2);
+        e = e + RHO(islp1) * (c1 - c2);
+        c2 = csr_caseC(phimh, xxbarh, SSH(ptmin + hx / 2), xk2);
+        c1 = csr_caseC(phimh, xxbarh, SSH(ptmin), xk2);
+        e = e + RHO(1) * (c1 - c2);
+      } else if (islp1 == 1) {
+        const double c2 = csr_caseC(phimh, xxbarh, SSH(xx - xslp), xk2);
+        const double c1 = csr_caseC(phimh, xxbarh, SSH(ptmin), xk2);
+        e = e + RHO(islp1) * (c1 - c2);
+      }
+      /* Case D (exit transient, source before the exit) */
+      const double psimax = phim * gam;
+      const int jstart = islp1 > 0 ? islp1 : 0;
+      for (int j = jstart + 2; j <= islpN1 - 1; j++) {
+        const double c2 = csr_caseD(xxbarh, psimax, SSH(ptmin + (j - 1) * hx + hx / 2), xk2,
+                                    epstol, nmax);
+        const double c1 = csr_caseD(xxbarh, psimax, SSH(ptmin + (j - 1) * hx - hx / 2), xk2,
+                                    epstol, nmax);
+        e = e + RHO(j) * (c1 - c2);
+      }
+      if (islpN1 >= jstart + 2) {
+        double c2 = csr_caseD(xxbarh, psimax, xslpN * g3 / r0, xk2, epstol, nmax);
+        double c1 = csr_caseD(xxbarh, psimax, SSH(ptmin + (islpN1 - 1) * hx - hx / 2), xk2,
+                              epstol, nmax);
+        e = e + RHO(islpN1) * (c1 - c2);
+        c2 = csr_caseD(xxbarh, psimax, SSH(ptmin + jstart * hx + hx / 2), xk2, epstol, nmax);
+        c1 = csr_caseD(xxbarh, psimax, xslp * g3 / r0, xk2, epstol, nmax);
+        e = e + RHO(jstart + 1) * (c1 - c2);
+      } else if (islpN1 == jstart + 1) {
+        const double c2 = csr_caseD(xxbarh, psimax, xslpN * g3 / r0, xk2, epstol, nmax);
+        const double c1 = csr_caseD(xxbarh, psimax, xslp * g3 / r0, xk2, epstol, nmax);
+        e = e + RHO(jstart + 1) * (c1 - c2);
+      }
+    }
+    ez[i - 1] = e * xconst;
+  }
+#undef SSH
+#undef RHO
+}
+
+/* The CSR glue of one step (AccSimulator.f90:1344-1390) and kick1wake's
+ * addition (BeamBunch.f90:5015-5033): densz from orc_wake_line, s0 the
+ * distance of the step from the bend entrance, blen the bend length; out =
+ * {0, 0, dEz}[nz]. */
+void orc_csr_field(int nz, const double *densz, const double range[6], double gam,
+                   double curr, int npt, double mass, double chrg, double r0, double s0,
+                   double blen, double *out) {
+  double *d = (double *)malloc(2 * (size_t)nz * sizeof(double));
+  double *ez = d + nz;
+  double hzwake = (range[5] - range[4]) / (nz - 1);
+  hzwake = hzwake / gam;
+  for (int k = 0; k < nz; k++)
+    d[k] = densz[k] * curr / PC.Scfreq / npt / hzwake * chrg / fabs(chrg);
+  const double zwkmin = range[4] / gam + s0;
+  orc_csr_wake(nz, r0, zwkmin, hzwake, blen, d, gam, ez);
+  /* kick1wake's constants (BeamBunch.f90:4989-5006) */
+  const double twopi = 2.0 * PC.Pi;
+  const double tmpscale = curr / PC.Scfreq;
+  const double fpei = PC.Clight * PC.Clight * (double)1.0e-7f;
+  const double xk = 1 / PC.Scxl;
+  const double bet = sqrt(gam * gam - 1.0) / gam;
+  const double bbyk = bet / xk;
+  const double gambet = gam * bet;
+  const double brho = gambet / (PC.Clight * chrg) * mass;
+  const double vz0 = bet * PC.Clight;
+  const double perv0 = 2.0 * curr * fpei / (brho * vz0 * vz0 * gam * gam);
+  const double xycon = 0.5 * perv0 * gambet * bbyk * twopi / tmpscale;
+  const double tcon = bet * xycon * (gam * gam);
+  for (int k = 0; k < nz; k++) {
+    out[k] = 0.0;
+    out[nz + k] = 0.0;
+    out[2 * nz + k] = chrg * ez[k] / tcon / mass;
+  }
+  free(d);
+}
+
+/* ------------------------------------------------------------------ */
 static double pipe_radius(const orc_elem *e) {
   /* getradius_BeamLineElem (BeamLineElem.f90:500-552): Param index per type */
   switch (e->type) {
@@ -1311,8 +1557,10 @@ static double pipe_radius(const orc_elem *e) {
 }
 
 /* run_AccSimulator element/segment loop (AccSimulator.f90:742-1504) for
- * Flagmap=1, Flagbc=1, Flagerr=0, Flagsubstep=0, one rank, no CSR; the read-in
- * wake of orc_wake_set applies to every space-charge kick while it is on. */
+ * Flagmap=1, Flagbc=1, Flagerr=0, Flagsubstep=0, one rank; the read-in wake
+ * of orc_wake_set applies to every space-charge kick while it is on, the
+ * CSR wake inside bends with dparam(4) > 200 and after bends with
+ * dparam(4) > 500 (bend state carried in the beam between calls). */
 int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
             double *rows, int maxrows) {
   const double Scxl = PC.Scxl;
@@ -1349,7 +1597,6 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     double psi2 = 0, angB = 0, qm0 = beam->charge / beam->mass;
     if (bitype == 4) {
       const double *dp = e->val - 2; /* dparam(k) = val[k-2] */
-      if (dp[4] > 200) { free(rho); return -4; } /* CSR inside the bend: out of scope */
       gamma0 = -beam->refptcl[5];
       beta0 = sqrt(1.0 - 1.0 / gamma0 / gamma0);
       beam->refptcl[4] = beam->refptcl[4] + blength / (Scxl * beta0);
@@ -1363,6 +1610,15 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
       hB = dp[9];
       double dstr1 = dp[10], dstr2 = dstr1;
       hd0 = ang0 / blength;
+      /* CSR bookkeeping of the bend entry (AccSimulator.f90:1032-1051, 1088) */
+      beam->r0 = fabs(1.0 / hd0);
+      if (bcurr > 0.0 && dp[4] > 500) {
+        beam->flagbendcsr = 1;
+        beam->bendlencsr = blength;
+        beam->sentr = 0.0;
+      } else {
+        beam->flagbendcsr = 0;
+      }
       double tanphiF = tan(angF);
       double psi1 = hd0 * hgap * dstr1 * (1.0 + sin(angF) * sin(angF)) / cos(angF);
       double tanphiFb = tan(angF - psi1);
@@ -1389,7 +1645,25 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
               return -5;
             }
             double *wf = NULL;
-            if (WK.on) { /* AccSimulator.f90:1273-1340 */
+            /* CSR inside a bend with dparam(4) > 200, and downstream of a
+             * bend with dparam(4) > 500 (AccSimulator.f90:1131-1138) */
+            int flagcsr = 0;
+            if (bitype == 4) {
+              if (e->val[2] > 200) flagcsr = 1;
+            } else if (beam->flagbendcsr) {
+              flagcsr = 1;
+            }
+            if (flagcsr) { /* AccSimulator.f90:1344-1390: replaces any read-in wake */
+              const int nz = mesh[2];
+              wf = (double *)calloc(6 * (size_t)nz, sizeof(double));
+              double *line = wf + 3 * (size_t)nz;
+              orc_wake_line(beam->pts, beam->nlocal, nz, range, line, line + nz,
+                            line + 2 * (size_t)nz);
+              const double s0 = bitype == 4 ? z - beam->zbleng : z - beam->zbleng + beam->sentr;
+              orc_csr_field(nz, line, range, -beam->refptcl[5], beam->current, beam->npt,
+                            beam->mass, beam->charge, beam->r0, s0,
+                            bitype == 4 ? blength : beam->bendlencsr, wf);
+            } else if (WK.on) { /* AccSimulator.f90:1273-1340 */
               const int nz = mesh[2];
               wf = (double *)malloc(6 * (size_t)nz * sizeof(double));
               double *line = wf + 3 * (size_t)nz;
@@ -1454,6 +1728,8 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     if (bitype == 4)
       orc_bpol(hd0, hB, tanphiB, tanphiBb, hd1, psi2, beam->pts, angB, beam->nlocal, gamma0,
                qm0);
+    beam->zbleng = beam->zbleng + blength; /* AccSimulator.f90:1498-1499 */
+    beam->sentr = beam->sentr + blength;
   }
 #undef DIAG
   beam->z = z;

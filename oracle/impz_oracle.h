@@ -112,6 +112,13 @@ void orc_wake_line(const double *pts, int n, int nz, const double range[6], doub
 void orc_wake_field(int nz, const double *densz, const double *xsum, const double *ysum,
                     const double range[6], double gam, double curr, int npt, double mass,
                     double chrg, double *out);
+/* CSR wake (csrwakeTrIGF_FieldQuant, Field.f90:1003-1303) and its glue
+ * (AccSimulator.f90:1344-1390) */
+void orc_csr_wake(int nx, double r0, double ptmin, double hx, double blength,
+                  const double *rho, double gam, double *ez);
+void orc_csr_field(int nz, const double *densz, const double range[6], double gam,
+                   double curr, int npt, double mass, double chrg, double r0, double s0,
+                   double blen, double *out);
 /* diagnostic1_Output (Output.f90:20-371): raw sums and one derived row */
 void orc_moment_sums(const double *pts, int n, double raw[ORC_RAW_LEN]);
 void orc_diag_row(double z, const double raw[ORC_RAW_LEN], int npt, int nlocal,
@@ -135,6 +142,9 @@ typedef struct {
   double *pts;                         /* Pts1(9,nlocal) */
   double refptcl[6];
   double z;
+  /* CSR bend bookkeeping of run_AccSimulator (AccSimulator.f90:638-740) */
+  double zbleng, sentr, bendlencsr, r0;
+  int flagbendcsr;
 } orc_beam;
 
 /* runs elements [0,nelem); writes one ORC_DIAG_LEN row per diagnostic

@@ -39,7 +39,12 @@ class OrcBeam(ctypes.Structure):
         ("current", ctypes.c_double), ("mass", ctypes.c_double), ("charge", ctypes.c_double),
         ("freq", ctypes.c_double), ("npt", ctypes.c_int), ("nlocal", ctypes.c_int),
         ("pts", _D), ("refptcl", ctypes.c_double * 6), ("z", ctypes.c_double),
+        ("zbleng", ctypes.c_double), ("sentr", ctypes.c_double),
+        ("bendlencsr", ctypes.c_double), ("r0", ctypes.c_double),
+        ("flagbendcsr", ctypes.c_int),
     ]
+
+CSR_FIELDS = ("zbleng", "sentr", "bendlencsr", "r0", "flagbendcsr")
 
 
 _lib = None
@@ -90,6 +95,11 @@ def lib():
             "orc_wake_field": (v, [ctypes.c_int, _D, _D, _D, _D, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                    ctypes.c_double, _D]),
+            "orc_csr_wake": (v, [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_double, _D, ctypes.c_double, _D]),
+            "orc_csr_field": (v, [ctypes.c_int, _D, _D, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]),
             "orc_moment_sums": (v, [_D, ctypes.c_int, _D]),
             "orc_diag_row": (v, [ctypes.c_double, _D, ctypes.c_int, ctypes.c_int, _D,
                                  ctypes.c_double, _D]),
@@ -145,8 +155,10 @@ def elem_from(e):
     return o
 
 
-def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0):
-    """orc_run over a lattice: returns (rows, final pts, final beam)."""
+def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0, state=None):
+    """orc_run over a lattice: returns (rows, final pts, final beam).  `state`
+    (a beam returned by an earlier call) carries the CSR bend bookkeeping
+    across calls, as one element loop of the reference would."""
     physconst(freq)
     arr = (OrcElem * len(elems))(*[elem_from(e) for e in elems])
     keep = [getattr(e, "_keep", None) for e in elems]
@@ -158,6 +170,9 @@ def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0):
     for i in range(6):
         beam.refptcl[i] = refptcl[i]
     beam.z = z
+    if state is not None:
+        for f in CSR_FIELDS:
+            setattr(beam, f, getattr(state, f))
     mesh = np.array(grid, dtype=np.int32)
     nsteps = sum(e.nseg for e in elems)
     rows = np.zeros((nsteps + 1, DIAG_LEN))
