@@ -250,8 +250,8 @@ struct impz_bunch_s {
   bool wk_on = false, wk_tr = false;
   // CSR bend bookkeeping (committed at the end of each run) and whether the
   // run in progress has CSR steps
-  CsrState csr, csr_run;
-  bool run_csr = false;
+  LoopState csr, csr_run;
+  bool run_wake = false;
   int wk_ntab = 0, wk_gen = 0, wk_fixbits = 40, grid_wake = 1;
   double wk_hwk = 0.0, wk_scale = 1.0;
   char* wk_mem = nullptr;
@@ -311,7 +311,7 @@ PoissonBuffers poisson_of(impz_bunch_t b) {
   pb.twx = b->tw[0]; pb.twy = b->tw[1]; pb.twz = b->tw[2];
   pb.tw64x = b->tw64[0]; pb.tw64y = b->tw64[1]; pb.tw64z = b->tw64[2];
   pb.st = b->st;
-  const bool wake = b->wk_on || b->run_csr;
+  const bool wake = b->run_wake;
   pb.wake = wake ? b->wk_field : nullptr;
   pb.wake_line = wake ? b->wk_line : nullptr;
   return pb;
@@ -398,7 +398,6 @@ WakeArgs wake_args(impz_bunch_t b, const StepParams* table, int fixed) {
   w.fixbits = b->wk_fixbits;
   w.transverse = b->wk_tr ? 1 : 0;
   w.ntab = b->wk_ntab;
-  w.on = b->wk_on ? 1 : 0;
   w.line = b->wk_line;
   w.table = b->wk_tab;
   w.wfield = b->wk_field;
@@ -465,7 +464,7 @@ int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
     CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, gs));
   }
   if (!serial) CK(cudaEventRecord(b->ev_join, b->stream2));
-  if (b->wk_on || b->run_csr) {
+  if (b->run_wake) {
     ProfScope ps(b, IMPZ_PROF_WAKE, 2);
     CK(exact::launch_wake(wake_args(b, table, fixed), b->grid_wake, b->stream));
   }
@@ -851,6 +850,9 @@ int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, i
   b->wk_scale = scale;
   b->wk_tr = transverse != 0;
   b->wk_on = true;
+  // a -41 element with Param(4) > 0: flagwake = flagwakeread = 1
+  b->csr.flagwake = b->csr.flagwakeread = 1;
+  b->csr_run.flagwake = b->csr_run.flagwakeread = 1;
   ++b->wk_gen;
   return IMPZ_OK;
 }
@@ -858,6 +860,9 @@ int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, i
 int impz_wake_off(impz_bunch_t b) {
   if (!b) return IMPZ_ERR_ARG;
   b->wk_on = false;
+  // a -41 element with Param(4) <= 0: flagwake = flagwakeread = 0
+  b->csr.flagwake = b->csr.flagwakeread = 0;
+  b->csr_run.flagwake = b->csr_run.flagwakeread = 0;
   ++b->wk_gen;
   return IMPZ_OK;
 }
@@ -1160,7 +1165,10 @@ int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double cur
   b->current0 = current;
   std::memcpy(b->refptcl, refptcl, sizeof(b->refptcl));
   b->z = 0.0;
-  b->csr = CsrState();
+  // a new beam at z = 0: the bend bookkeeping restarts; the wake switch is
+  // the one impz_wake_set / impz_wake_off left
+  b->csr = LoopState();
+  b->csr.flagwake = b->csr.flagwakeread = b->wk_on ? 1 : 0;
   b->stage = ST_IDLE;
   b->bend.active = false;
   b->run_pending = false;
@@ -1219,7 +1227,7 @@ static int wake_alloc(impz_bunch_t b, int ntab) {
 }
 
 // which wake kernels a captured step holds
-static int wake_key(impz_bunch_t b) { return 2 * b->wk_gen + (b->run_csr ? 1 : 0); }
+static int wake_key(impz_bunch_t b) { return 2 * b->wk_gen + (b->run_wake ? 1 : 0); }
 
 // Two space-charge steps captured as one CUDA graph (parity returns to its
 // start value), cached per start parity and re-captured when the step table
@@ -1253,7 +1261,7 @@ static int graph_pair(impz_bunch_t b) {
     b->g_wake[p] = wake_key(b);
     b->parity = p;  // capture did not execute anything
   }
-  g_launches += 2 * (12 + (b->wk_on || b->run_csr ? 2 : 0));
+  g_launches += 2 * (12 + (b->run_wake ? 2 : 0));
   CK(cudaGraphLaunch(b->gexec[p], b->stream));
   return IMPZ_OK;
 }
@@ -1273,8 +1281,8 @@ static int run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   int r = compile_lattice(b->P, elems, nelem, b->current0, b->sp, b->run_ref, &b->run_z,
                           b->csr_run, L);
   if (r) return r;
-  b->run_csr = L.has_csr;
-  if (b->run_csr && !b->wk_mem && (r = wake_alloc(b, 0))) return r;
+  b->run_wake = L.has_wake;
+  if (b->run_wake && !b->wk_mem && (r = wake_alloc(b, 0))) return r;
   const int K = L.nsteps;
   b->run_light = table_is_light(L.steps);
   if ((r = ensure_tables(b, K + 2, K + 1))) return r;

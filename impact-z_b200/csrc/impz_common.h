@@ -60,7 +60,9 @@ struct StepParams {
   double csr_r0;       // CSR: radius of the bend
   double csr_s0;       // CSR: distance of the kick from the bend entrance (z - zbleng [+ sentr])
   double csr_blen;     // CSR: bend length
-  double pad2;
+  int wake;            // wake of this step's kick: 0 none, 1 read-in table, 2 analytic
+  int pad3;
+  double wk_aa, wk_gg, wk_len;  // analytic wake: iris radius, gap, period (Param(13..15))
 };
 
 #define IMPZ_MOMREC 48   // per recorded step: 44 raw values, npt, nlocal, current, spare
@@ -155,7 +157,7 @@ struct WakeArgs {
   int fixbits;               // fixed-point resolution of the line sums
   int transverse;            // 1: x/y moments and the transverse wakes too
   int ntab;                  // wake table rows
-  int on;                    // the read-in wake is on (else only CSR steps have a field)
+  int pad0;
   unsigned long long* line;  // [3][nz] int64 sums (density, x, y), left cleared
   const double* table;       // [3][ntab]: longitudinal, x and y wake columns
   double* wfield;            // [3][nz] out: added to Ex, Ey, Ez of plane k

@@ -484,16 +484,17 @@ void bend_exit_op(const Phys& P, const BendState& bs, const Species& sp, MapProg
 
 // ---------------------------------------------------------------------
 int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double bcurr,
-                    const Species& sp, double refptcl[6], double* zio, CsrState& csr,
+                    const Species& sp, double refptcl[6], double* zio, LoopState& csr,
                     CompiledLattice& out) {
   struct Half {
     MapProgram prog;
   };
   struct Step {
     MapProgram a, b;
-    int sc, csr;
+    int sc, csr, wake;
     double gam, tau, rad;
     double csr_r0, csr_s0, csr_blen;
+    double wk_aa, wk_gg, wk_len;
     double z;
     double ref[6];
   };
@@ -510,6 +511,15 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     if (e.nseg < 1) return IMPZ_ERR_ARG;
     const int bnseg = e.nseg, bitype = e.type;
     double piperad = pipe_radius(e), piperad2 = piperad;
+    // the wake switch of each element (AccSimulator.f90:865-875)
+    if (bitype == 105 || bitype == 106) {
+      csr.aawk = e.val[11];
+      csr.ggwk = e.val[12];
+      csr.lengwk = e.val[13];
+      csr.flagwake = csr.lengwk > 0.0 ? 1 : 0;
+    } else if (!csr.flagwakeread) {
+      csr.flagwake = 0;
+    }
     if (bitype == 4) { piperad = 100.0; piperad2 = 100.0; }
     const double tau1 = 0.5 * e.length / bnseg;
     const double tau2 = 2.0 * tau1;
@@ -551,6 +561,12 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
             s.csr_s0 = bitype == 4 ? z - csr.zbleng : z - csr.zbleng + csr.sentr;
             s.csr_blen = bitype == 4 ? e.length : csr.bendlencsr;
           }
+          if (sc_on && csr.flagwake) {
+            s.wake = csr.flagwakeread ? 1 : 2;
+            s.wk_aa = csr.aawk;
+            s.wk_gg = csr.ggwk;
+            s.wk_len = csr.lengwk;
+          }
         }
         if (bitype == 4) {
           bend_sector_op(P, bs, tau1, sp, prog);
@@ -571,7 +587,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
   }
   const int K = (int)steps.size();
   out.nsteps = K;
-  out.has_csr = false;
+  out.has_wake = false;
   out.steps.assign(K + 2, StepParams());
   for (auto& st : out.steps) std::memset(&st, 0, sizeof(st));
   out.zrec.assign(K + 1, 0.0);
@@ -594,7 +610,11 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
       sp_.csr_r0 = cur.csr_r0;
       sp_.csr_s0 = cur.csr_s0;
       sp_.csr_blen = cur.csr_blen;
-      if (cur.csr) out.has_csr = true;
+      sp_.wake = cur.wake;
+      sp_.wk_aa = cur.wk_aa;
+      sp_.wk_gg = cur.wk_gg;
+      sp_.wk_len = cur.wk_len;
+      if (cur.csr || cur.wake) out.has_wake = true;
       sp_.gam = cur.gam;
       sp_.tau = cur.tau;
       sp_.rad = cur.rad;

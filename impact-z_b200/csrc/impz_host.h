@@ -47,22 +47,27 @@ struct CompiledLattice {
   std::vector<double> zrec;       // z of each record (K+1)
   std::vector<double> refrec;     // refptcl of each record, 6 per record
   int nsteps;
-  bool has_csr;                   // some step kicks with the CSR wake
+  bool has_wake;                  // some step kicks with a wake (read-in, analytic or CSR)
 };
-// The bend bookkeeping of run_AccSimulator that decides where the CSR wake
-// acts (AccSimulator.f90:638-740, 1032-1051, 1131-1138, 1498-1499).
-struct CsrState {
+// The state of run_AccSimulator's element loop that decides where wakes
+// act: the bend bookkeeping of CSR (AccSimulator.f90:638-740, 1032-1051,
+// 1131-1138, 1498-1499) and the wake switches (flagwake, flagwakeread of
+// -41 elements and 105/106 structures, AccSimulator.f90:865-875, 959-978).
+struct LoopState {
   double zbleng = 0.0;      // sum of the lengths of the elements passed
   double sentr = 0.0;       // distance from the last CSR bend's entrance
   double bendlencsr = 0.0;  // that bend's length
   double r0 = 0.0;          // radius of the last bend
   int flagbendcsr = 0;      // the last bend had dparam(4) > 500
+  int flagwake = 0;         // the kicks include a wake
+  int flagwakeread = 0;     // ... the read-in one (-41), else the analytic one
+  double aawk = 0.0, ggwk = 0.0, lengwk = 0.0;  // the last 105/106's Param(13..15)
 };
 // run_AccSimulator's element/segment loop (AccSimulator.f90:742-1504)
 // turned into a step table.  refptcl, z and the CSR state advance to the
 // lattice exit.
 int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double bcurr,
-                    const Species& sp, double refptcl[6], double* z, CsrState& csr,
+                    const Species& sp, double refptcl[6], double* z, LoopState& csr,
                     CompiledLattice& out);
 
 // diagnostic1_Output rank-0 formulas (Output.f90:247-352)

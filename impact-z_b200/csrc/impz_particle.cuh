@@ -1235,7 +1235,11 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_wake_line(WakeArgs a) {
   const DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
-  if (!a.steps[s].csr && !a.on) return;  // no wake acts in this step
+  const StepParams& sp = a.steps[s];
+  if (!sp.csr && !sp.wake) return;  // no wake acts in this step
+  // the x/y moments feed the transverse wakes: the analytic one always, the
+  // read-in one unless the table's transverse columns are off; CSR has none
+  const bool tr = !sp.csr && (sp.wake == 2 || (sp.wake == 1 && a.transverse));
   const double gam = a.steps[s].gam, rad = a.steps[s].rad;
   const long long n = st->nlocal;
   const int nz = a.nz;
@@ -1246,7 +1250,7 @@ __global__ void __launch_bounds__(BLOCK) k_wake_line(WakeArgs a) {
   frexp(fmax(fabs(st->geom.range[0]), fabs(st->geom.range[1])), &ex);
   frexp(fmax(fabs(st->geom.range[2]), fabs(st->geom.range[3])), &ey);
   const double sx = ldexp(1.0, a.fixbits - ex), sy = ldexp(1.0, a.fixbits - ey);
-  const int nq = a.transverse ? 6 : 2;
+  const int nq = tr ? 6 : 2;
   const int lane = threadIdx.x & 31;
   for (long long base = (long long)blockIdx.x * BLOCK + (threadIdx.x & ~31); base < n;
        base += (long long)gridDim.x * BLOCK) {
@@ -1265,7 +1269,7 @@ __global__ void __launch_bounds__(BLOCK) k_wake_line(WakeArgs a) {
           kz = iizz - 1;
           q[0] = llrint(ab * sc);
           q[1] = llrint((1.0 - ab) * sc);
-          if (a.transverse) {
+          if (tr) {
             q[2] = llrint(t.xt * ab * sx);
             q[3] = llrint(t.xt * (1.0 - ab) * sx);
             q[4] = llrint(t.yt * ab * sy);
@@ -1502,12 +1506,44 @@ __device__ double csr_node(int i, const double* __restrict__ rho, double r0, dou
   return e * xconst;
 }
 
+// The analytic wake of wakefield_FieldQuant (Field.f90:590-782), the short-
+// range wakes of a periodic structure of iris radius aa, gap gg, period
+// leng: W_L(z) = Z0 c exp(-sqrt(z/z0)) / (pi aa^2) and
+// W_T(z) = 4 Z0 c z1 / (pi aa^4) (1 - (1 + sqrt(z/z1)) exp(-sqrt(z/z1)));
+// the fits z0, z1 (Field.f90:627-629, 694-695) keep the reference's default-
+// real literals.
+struct AnalyticWake {
+  double z0l, z0t, coef1, zc, Z0, pilc, aa;
+  __device__ static AnalyticWake of(double aa, double gg, double leng, double clight) {
+    AnalyticWake w;
+    w.pilc = 2 * asin(1.0);
+    w.aa = aa;
+    w.z0l = (double)0.41f * pow(aa / leng, (double)0.8f) * pow(gg / leng, (double)1.6f) * aa;
+    w.Z0 = 120 * w.pilc;
+    w.zc = w.Z0 * clight;
+    w.z0t = (double)0.169f * aa * pow(aa / leng, (double)1.17f) * pow(gg / aa, (double)0.38f);
+    w.coef1 = 4 * w.Z0 * clight * w.z0t / (w.pilc * aa * aa * aa * aa);
+    return w;
+  }
+  __device__ double wl(int j, double hz) const {
+    const double zz = j * hz;
+    return zc * exp(-sqrt(zz / z0l)) / (pilc * aa * aa);
+  }
+  __device__ double wt(int j, double hz) const {
+    const double zz = j * hz;
+    return coef1 * (1.0 - (1. + sqrt(zz / z0t)) * exp(-sqrt(zz / z0t)));
+  }
+  __device__ double w0_half(double clight) const {
+    return 0.5 * Z0 * clight * exp(-sqrt(0.0 / z0l)) / (pilc * aa * aa);
+  }
+};
+
 // Wake step part 2: the line charge density recvdensz
 // (AccSimulator.f90:1297-1322 and 1360-1368) and from it the per-plane field
 // that kick1wake adds to the node fields before the gather
 // (BeamBunch.f90:5015-5033).  A step with CSR takes the CSR wake
-// (AccSimulator.f90:1344-1390, which replaces a read-in wake), else the
-// read-in wake, else the field is zero.  The read-in wake: the reference
+// (AccSimulator.f90:1344-1390, which replaces any other wake), else the
+// step's wake (the read-in table or the analytic one), else zero.  The read-in wake: the reference
 // convolves on a doubled grid by FFT (wakefieldread_FieldQuant,
 // Field.f90:783-1001) with a Green function that is 0.5 W(0) at 0, zero at
 // 1..Nz-1 and W((2Nz-k) hz) above; for k < Nz that circular convolution is
@@ -1524,12 +1560,14 @@ __global__ void __launch_bounds__(256) k_wake_field(WakeArgs a) {
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
   const StepParams& sp = a.steps[s];
   const int kk = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!sp.csr && !a.on) {
+  if (!sp.csr && !sp.wake) {
     if (kk < nz) a.wfield[kk] = a.wfield[nz + kk] = a.wfield[2 * nz + kk] = 0.0;
     return;
   }
   const bool csr = sp.csr != 0;
-  const bool tr = !csr && a.transverse;
+  const bool analytic = !csr && sp.wake == 2;
+  const bool tr = analytic || (!csr && sp.wake == 1 && a.transverse);
+  const AnalyticWake aw = AnalyticWake::of(sp.wk_aa, sp.wk_gg, sp.wk_len, a.k.Clight);
   double* d = wsm;
   double* dx = wsm + nz;
   double* dy = wsm + 2 * nz;
@@ -1557,7 +1595,12 @@ __global__ void __launch_bounds__(256) k_wake_field(WakeArgs a) {
       yw = ((double)(long long)a.line[2 * nz + k] / sy) / dens;
     }
     d[k] = dk;
-    if (!csr) {
+    if (analytic) {
+      dx[k] = dk * xw;
+      dy[k] = dk * yw;
+      gz[k] = aw.wl(k, hzw);
+      gx[k] = gy[k] = aw.wt(k, hzw);
+    } else if (!csr) {
       dx[k] = dk * xw;
       dy[k] = dk * yw;
       gz[k] = wake_green(a.table, ntab, a.hwk, k, hzw);
@@ -1579,7 +1622,9 @@ __global__ void __launch_bounds__(256) k_wake_field(WakeArgs a) {
     return;
   }
   const double bet = sqrt(gam * gam - 1.0) / gam;
-  const double g0 = 0.5 * gz[0];
+  // greenwake(1) = 0.5 W(0), in each form as the reference writes it
+  const double g0 = analytic ? aw.w0_half(a.k.Clight) : 0.5 * gz[0];
+  const double scale = analytic ? 1.0 : a.scale;
   double cz = d[k] * g0, cx = 0.0, cy = 0.0;
   if (tr) {
     for (int m = k + 1; m < nz; m++) {
@@ -1590,9 +1635,9 @@ __global__ void __launch_bounds__(256) k_wake_field(WakeArgs a) {
   } else {
     for (int m = k + 1; m < nz; m++) cz = cz + d[m] * gz[m - k];
   }
-  const double ezwake = a.scale * (-cz * hzw);
-  const double exwake = a.scale * (cx * hzw);
-  const double eywake = a.scale * (cy * hzw);
+  const double ezwake = scale * (-cz * hzw);
+  const double exwake = scale * (cx * hzw);
+  const double eywake = scale * (cy * hzw);
   a.wfield[k] = chrg * exwake / xycon / mass / bet / gam / a.unit;
   a.wfield[nz + k] = chrg * eywake / xycon / mass / bet / gam / a.unit;
   a.wfield[2 * nz + k] = chrg * ezwake / tcon / mass / a.unit;

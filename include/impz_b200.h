@@ -112,7 +112,11 @@ int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]);
  * field to the node fields before the gather (kick1wake_BeamBunch,
  * BeamBunch.f90:4694-5046).  Allocates the table and its per-step buffers
  * (outside impz_bunch_footprint).  IMPZ_ERR_ARG for ntab < 2, a
- * non-increasing z, or nz > 4096.  impz_wake_off is Param(4) <= 0. */
+ * non-increasing z, or nz > 4096.  impz_wake_off is Param(4) <= 0.
+ * Type 105/106 structures with Param(15) > 0 carry the analytic wake of
+ * Param(13..15) (wakefield_FieldQuant, Field.f90:590-782) without a call,
+ * and switch a wake as AccSimulator.f90:865-875 does; the switch state
+ * carries from one impz_run to the next. */
 int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, int transverse);
 int impz_wake_off(impz_bunch_t b);
 /* Current, Npt, Nptlocal, refptcl(1..6), z, device bytes (11 doubles). */

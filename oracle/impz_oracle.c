@@ -1173,12 +1173,34 @@ void orc_diag_row(double z, const double raw[ORC_RAW_LEN], int npt, int nlocal,
  * 5000 rows and are zero beyond the rows read, which the table lookup below
  * reproduces by reading zero past the last row. */
 static struct {
-  int on, transverse, ntab;
+  int read, flag;       /* flagwakeread, flagwake of run_AccSimulator */
+  int transverse, ntab; /* flagbtw != 2; table rows */
   double scale, hwk;
   double *ew, *epw, *eppw;
+  double aa, gg, leng;  /* aawk, ggwk, lengwk of the last 105/106 element */
 } WK;
 
-void orc_wake_off(void) { WK.on = 0; }
+void orc_wake_off(void) {
+  WK.read = 0;
+  WK.flag = 0;
+  WK.scale = 1.0;
+}
+
+/* The wake switch at each element (AccSimulator.f90:865-875): a type 105
+ * or 106 structure turns the wake on when its Param(15) (period length)
+ * is positive, with the analytic wake of Param(13..15) unless a read-in
+ * wake is on, and off otherwise; any other element turns off a wake that
+ * is not a read-in one. */
+void orc_wake_elem(int bitype, const double *val) {
+  if (bitype == 105 || bitype == 106) {
+    WK.aa = val[11];
+    WK.gg = val[12];
+    WK.leng = val[13];
+    WK.flag = WK.leng > 0.0;
+  } else if (!WK.read) {
+    WK.flag = 0;
+  }
+}
 
 int orc_wake_set(const double *z, const double *ew, const double *epw, const double *eppw,
                  int ntab, double scale, int transverse) {
@@ -1196,7 +1218,8 @@ int orc_wake_set(const double *z, const double *ew, const double *epw, const dou
   WK.ntab = ntab;
   WK.scale = scale;
   WK.transverse = transverse;
-  WK.on = 1;
+  WK.read = 1;
+  WK.flag = 1;
   return 0;
 }
 
@@ -1249,9 +1272,70 @@ void orc_wake_line(const double *pts, int n, int nz, const double range[6], doub
  * transverse ones (greenwake zero at 0 too)
  *   conv_x(k) = sum_{m>k} d(m) xbar(m) Wx((m-k) hz).
  * d is recvdensz (AccSimulator.f90:1297-1322).  out = {dEx, dEy, dEz}[nz]. */
+static void wake_field(int nz, const double *densz, const double *xsum, const double *ysum,
+                       const double range[6], double gam, double curr, int npt, double mass,
+                       double chrg, int analytic, double *out);
+
 void orc_wake_field(int nz, const double *densz, const double *xsum, const double *ysum,
                     const double range[6], double gam, double curr, int npt, double mass,
                     double chrg, double *out) {
+  wake_field(nz, densz, xsum, ysum, range, gam, curr, npt, mass, chrg, 0, out);
+}
+
+/* The analytic wake of wakefield_FieldQuant (Field.f90:590-782), the short-
+ * range wakes of a periodic structure of iris radius aa, gap gg and period
+ * leng: W_L(z) = Z0 c exp(-sqrt(z/z0)) / (pi aa^2) and
+ * W_T(z) = 4 Z0 c z1 / (pi aa^4) (1 - (1 + sqrt(z/z1)) exp(-sqrt(z/z1))),
+ * with z0, z1 the fits of Field.f90:627-629 and 694-695 (their literals in
+ * default real precision, as the reference writes them).  The same causal
+ * sums as the read-in wake, the transverse wakes always on. */
+void orc_wake_field_analytic(int nz, const double *densz, const double *xsum,
+                             const double *ysum, const double range[6], double gam, double curr,
+                             int npt, double mass, double chrg, double aa, double gg,
+                             double leng, double *out) {
+  const double s_aa = WK.aa, s_gg = WK.gg, s_leng = WK.leng;
+  WK.aa = aa;
+  WK.gg = gg;
+  WK.leng = leng;
+  wake_field(nz, densz, xsum, ysum, range, gam, curr, npt, mass, chrg, 1, out);
+  WK.aa = s_aa;
+  WK.gg = s_gg;
+  WK.leng = s_leng;
+}
+
+typedef struct {
+  double z0l, z0t, coef1, zc, Z0, pilc, aa;
+} analytic_wake;
+
+static analytic_wake analytic_of(double aa, double gg, double leng) {
+  analytic_wake w;
+  w.pilc = 2 * asin(1.0);
+  w.aa = aa;
+  w.z0l = (double)0.41f * pow(aa / leng, (double)0.8f) * pow(gg / leng, (double)1.6f) * aa;
+  const double Z0 = 120 * w.pilc;
+  w.Z0 = Z0;
+  w.zc = Z0 * PC.Clight;
+  w.z0t = (double)0.169f * aa * pow(aa / leng, (double)1.17f) * pow(gg / aa, (double)0.38f);
+  w.coef1 = 4 * Z0 * PC.Clight * w.z0t / (w.pilc * aa * aa * aa * aa);
+  return w;
+}
+
+static double analytic_wl(const analytic_wake *w, int j, double hz) {
+  const double zz = j * hz;
+  return w->zc * exp(-sqrt(zz / w->z0l)) / (w->pilc * w->aa * w->aa);
+}
+
+static double analytic_wt(const analytic_wake *w, int j, double hz) {
+  const double zz = j * hz;
+  return w->coef1 * (1.0 - (1. + sqrt(zz / w->z0t)) * exp(-sqrt(zz / w->z0t)));
+}
+
+static void wake_field(int nz, const double *densz, const double *xsum, const double *ysum,
+                       const double range[6], double gam, double curr, int npt, double mass,
+                       double chrg, int analytic, double *out) {
+  const analytic_wake aw = analytic ? analytic_of(WK.aa, WK.gg, WK.leng) : (analytic_wake){0};
+  const int tr = analytic || WK.transverse;
+  const double scale = analytic ? 1.0 : WK.scale;
   double *d = (double *)malloc(3 * (size_t)nz * sizeof(double));
   double *dx = d + nz, *dy = d + 2 * (size_t)nz;
   double hzwake = (range[5] - range[4]) / (nz - 1);
@@ -1279,19 +1363,29 @@ void orc_wake_field(int nz, const double *densz, const double *xsum, const doubl
   const double perv0 = 2.0 * curr * fpei / (brho * vz0 * vz0 * gam * gam);
   const double xycon = 0.5 * perv0 * gambet * bbyk * twopi / tmpscale;
   const double tcon = bet * xycon * (gam * gam);
-  const double g0 = 0.5 * wk_green(WK.ew, 0, hzwake);
+  /* greenwake(1): 0.5 W(0), written as the reference writes each form */
+  const double g0 = analytic ? 0.5 * aw.Z0 * PC.Clight * exp(-sqrt(0.0 / aw.z0l)) /
+                                   (aw.pilc * aw.aa * aw.aa)
+                             : 0.5 * wk_green(WK.ew, 0, hzwake);
   for (int k = 0; k < nz; k++) {
     double cz = d[k] * g0, cx = 0.0, cy = 0.0;
     for (int m = k + 1; m < nz; m++) {
-      cz = cz + d[m] * wk_green(WK.ew, m - k, hzwake);
-      if (WK.transverse) {
-        cx = cx + dx[m] * wk_green(WK.epw, m - k, hzwake);
-        cy = cy + dy[m] * wk_green(WK.eppw, m - k, hzwake);
+      if (analytic) {
+        cz = cz + d[m] * analytic_wl(&aw, m - k, hzwake);
+        const double wt = analytic_wt(&aw, m - k, hzwake);
+        cx = cx + dx[m] * wt;
+        cy = cy + dy[m] * wt;
+      } else {
+        cz = cz + d[m] * wk_green(WK.ew, m - k, hzwake);
+        if (tr) {
+          cx = cx + dx[m] * wk_green(WK.epw, m - k, hzwake);
+          cy = cy + dy[m] * wk_green(WK.eppw, m - k, hzwake);
+        }
       }
     }
-    const double ezwake = WK.scale * (-cz * hzwake);
-    const double exwake = WK.scale * (cx * hzwake);
-    const double eywake = WK.scale * (cy * hzwake);
+    const double ezwake = scale * (-cz * hzwake);
+    const double exwake = scale * (cx * hzwake);
+    const double eywake = scale * (cy * hzwake);
     out[k] = chrg * exwake / xycon / mass / bet / gam;
     out[nz + k] = chrg * eywake / xycon / mass / bet / gam;
     out[2 * nz + k] = chrg * ezwake / tcon / mass;
@@ -1587,6 +1681,7 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     const int bnseg = e->nseg, bitype = e->type;
     double piperad = pipe_radius(e), piperad2 = piperad;
     if (bitype < 0) { free(rho); return -3; }
+    orc_wake_elem(bitype, e->val);
     if (bitype == 4) { piperad = 100.0; piperad2 = 100.0; }
     double tau1 = 0.0;
     if (bitype >= 0) tau1 = 0.5 * blength / bnseg;
@@ -1663,15 +1758,14 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
               orc_csr_field(nz, line, range, -beam->refptcl[5], beam->current, beam->npt,
                             beam->mass, beam->charge, beam->r0, s0,
                             bitype == 4 ? blength : beam->bendlencsr, wf);
-            } else if (WK.on) { /* AccSimulator.f90:1273-1340 */
+            } else if (WK.flag) { /* AccSimulator.f90:1273-1340 */
               const int nz = mesh[2];
               wf = (double *)malloc(6 * (size_t)nz * sizeof(double));
               double *line = wf + 3 * (size_t)nz;
               orc_wake_line(beam->pts, beam->nlocal, nz, range, line, line + nz,
                             line + 2 * (size_t)nz);
-              orc_wake_field(nz, line, line + nz, line + 2 * (size_t)nz, range,
-                             -beam->refptcl[5], beam->current, beam->npt, beam->mass,
-                             beam->charge, wf);
+              wake_field(nz, line, line + nz, line + 2 * (size_t)nz, range, -beam->refptcl[5],
+                         beam->current, beam->npt, beam->mass, beam->charge, !WK.read, wf);
             }
             orc_cvbkforth1st(beam->pts, beam->nlocal, beam->refptcl);
             orc_kick1w(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],

@@ -107,6 +107,11 @@ void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
 int orc_wake_set(const double *z, const double *ew, const double *epw, const double *eppw,
                  int ntab, double scale, int transverse);
 void orc_wake_off(void);
+void orc_wake_elem(int bitype, const double *val);
+void orc_wake_field_analytic(int nz, const double *densz, const double *xsum,
+                             const double *ysum, const double range[6], double gam, double curr,
+                             int npt, double mass, double chrg, double aa, double gg,
+                             double leng, double *out);
 void orc_wake_line(const double *pts, int n, int nz, const double range[6], double *densz,
                    double *xsum, double *ysum);
 void orc_wake_field(int nz, const double *densz, const double *xsum, const double *ysum,

@@ -91,6 +91,11 @@ def lib():
             "orc_wake_set": (ctypes.c_int, [_D, _D, _D, _D, ctypes.c_int, ctypes.c_double,
                                             ctypes.c_int]),
             "orc_wake_off": (v, []),
+            "orc_wake_elem": (v, [ctypes.c_int, _D]),
+            "orc_wake_field_analytic": (v, [ctypes.c_int, _D, _D, _D, _D, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_double, _D]),
             "orc_wake_line": (v, [_D, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D]),
             "orc_wake_field": (v, [ctypes.c_int, _D, _D, _D, _D, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_int, ctypes.c_double,

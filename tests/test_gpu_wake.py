@@ -148,3 +148,68 @@ def test_deck_runner_with_wake_controls_matches_the_oracle(tmp_path):
     assert rows_g.shape == rows_o.shape
     np.testing.assert_allclose(rows_g[:, 0], rows_o[:, 0], rtol=0, atol=0)
     assert worst(rows_g, rows_o, RMS_COLS) <= 1e-8
+
+
+def structure(wake, length=0.3, nseg=6):
+    """A 1.3 GHz structure as an ideal-RF gap (type 105, v4 < 0) with, when
+    `wake`, the analytic wake of Param(13..15): iris radius 11.6 mm, gap
+    29 mm, period 35 mm (AccSimulator.f90:865-875)."""
+    v = [2.0e6, 1.3e9, 0.0, -1.0, 1.0] + [0.0] * 19
+    if wake:
+        v[11], v[12], v[13] = 0.0116, 0.029, 0.035
+    return impz.elem(105, length, nseg, 1, v)
+
+
+@pytest.mark.parametrize("form,cols,tol", [
+    (impz.FORM_FP64, RMS_COLS, 1e-8),
+    (impz.FORM_FP32CONV, [7, 9, 11, 13, 15, 17, 19, 21, 23], 1e-5)])
+def test_analytic_structure_wake_matches_the_oracle(form, cols, tol):
+    """A drift, a 105 structure with its analytic wake (longitudinal and
+    transverse), a drift: the wake acts only inside the structure."""
+    cfg = electron_cfg()
+    cfg["lattice"] = [impz.elem(0, 0.3, 6, 1, [1.0]), structure(True),
+                      impz.elem(0, 0.3, 6, 1, [1.0])]
+    rows_o = oracle_rows(cfg, None)
+    plain = dict(cfg, lattice=[cfg["lattice"][0], structure(False), cfg["lattice"][2]])
+    rows_plain = oracle_rows(plain, None)
+    assert worst(rows_plain, rows_o, [21, 23]) > 1e3 * tol
+    b = impz.Bunch(cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=form, track_ids=False)
+    try:
+        rows_g = gpu_rows(b, cfg, rows_o)
+    finally:
+        b.close()
+    assert worst(rows_g, rows_o, cols) <= tol
+
+
+def test_read_in_wake_switched_off_by_a_structure_without_wake():
+    """With a read-in wake on, a 105 structure whose Param(15) is 0 sets
+    flagwake = 0, and the read-in wake stays off after it, into the next
+    run, until the next -41 (AccSimulator.f90:865-875): GPU = oracle over
+    two runs, and != the wake kept on."""
+    cfg = electron_cfg()
+    drift = impz.elem(0, 0.3, 6, 1, [1.0])
+    lat = [drift, structure(False), drift]
+    wake = (synthetic_table(), 1.0, False)
+    try:
+        orc.wake_set(*wake)
+        r1, p1, beam1 = orc.run(lat, cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"],
+                                cfg["freq"], cfg["refptcl"], cfg["grid"])
+        r2, _, _ = orc.run([drift], p1, cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                           np.array(beam1.refptcl[:]), cfg["grid"], beam1.z, beam1)
+        orc.wake_set(*wake)
+        rk, _, _ = orc.run([drift, drift, drift], cfg["pts"], cfg["current"], cfg["mass"],
+                           cfg["charge"], cfg["freq"], cfg["refptcl"], cfg["grid"])
+    finally:
+        orc.wake_off()
+    b = impz.Bunch(cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=impz.FORM_FP64, track_ids=False)
+    try:
+        b.wake(*wake)
+        g1 = gpu_rows(b, dict(cfg, lattice=lat), r1)
+        g2 = gpu_rows(b, dict(cfg, lattice=[drift]), r2)
+    finally:
+        b.close()
+    assert worst(g1, r1, RMS_COLS) <= 1e-8
+    assert worst(g2, r2, RMS_COLS) <= 1e-8
+    assert worst(rk[: r1.shape[0]], r1, [21, 23]) > 1e-5

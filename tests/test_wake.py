@@ -51,14 +51,18 @@ def green_ref(col, table, nz, hz):
     return g
 
 
-def fft_wake(table, recv, xbar, ybar, hz, transverse):
-    """Field.f90:783-1001 with numpy's FFT: returns (exwake, eywake, ezwake)."""
+def fft_wake(table, recv, xbar, ybar, hz, transverse, greens=None):
+    """Field.f90:783-1001 (or, with greens = (W_L, W_T) sampled at 0..Nz,
+    Field.f90:590-782) with numpy's FFT: returns (exwake, eywake, ezwake)."""
     nz = recv.shape[0]
     n2 = 2 * nz
 
     def conv(dens, col, transverse_green):
         d2 = np.r_[dens, np.zeros(nz)]
-        w = green_ref(col, table, nz, hz)
+        if greens is not None:
+            w = greens[1 if transverse_green else 0]
+        else:
+            w = green_ref(col, table, nz, hz)
         g = np.zeros(n2)
         g[: nz + 1] = w
         g[0] = 0.5 * w[0]
@@ -70,11 +74,12 @@ def fft_wake(table, recv, xbar, ybar, hz, transverse):
             g[1:nz] = 0.0  # kz = 2..Nz
         return np.fft.irfft(np.fft.rfft(d2) * np.fft.rfft(g), n2)[:nz]
 
-    ez = -conv(recv, table[:, 1], False) * hz
+    col = (lambda c: None) if table is None else (lambda c: table[:, c])  # noqa: E731
+    ez = -conv(recv, col(1), False) * hz
     if not transverse:
         return np.zeros(nz), np.zeros(nz), ez
-    ex = conv(recv * xbar, table[:, 2], True) * hz
-    ey = conv(recv * ybar, table[:, 3], True) * hz
+    ex = conv(recv * xbar, col(2), True) * hz
+    ey = conv(recv * ybar, col(3), True) * hz
     return ex, ey, ez
 
 
@@ -131,6 +136,85 @@ def test_direct_wake_sum_equals_the_doubled_grid_fft(nz, transverse):
     np.testing.assert_allclose(out, want, rtol=0, atol=1e-12 * scale)
     if not transverse:
         assert not out[: 2 * nz].any()
+
+
+def analytic_greens(aa, gg, leng, nz, hz):
+    """Field.f90:623-641 and 694-700: the fits in default real literals."""
+    f32 = lambda x: float(np.float32(x))  # noqa: E731
+    pilc, clight = 2 * np.arcsin(1.0), 299792458.0
+    z0 = f32(0.41) * (aa / leng) ** f32(0.8) * (gg / leng) ** f32(1.6) * aa
+    z0_0 = 120 * pilc
+    zz = np.arange(nz + 1) * hz
+    wl = z0_0 * clight * np.exp(-np.sqrt(zz / z0)) / (pilc * aa * aa)
+    z1 = f32(0.169) * aa * (aa / leng) ** f32(1.17) * (gg / aa) ** f32(0.38)
+    coef1 = 4 * z0_0 * clight * z1 / (pilc * aa ** 4)
+    wt = coef1 * (1.0 - (1.0 + np.sqrt(zz / z1)) * np.exp(-np.sqrt(zz / z1)))
+    return wl, wt
+
+
+@pytest.mark.parametrize("nz", [32, 128])
+def test_analytic_wake_sum_equals_the_doubled_grid_fft(nz):
+    """wakefield_FieldQuant (Field.f90:590-782): the short-range wakes of a
+    periodic structure (iris radius 11.6 mm, gap 29 mm, period 35 mm), both
+    planes, as the oracle's direct sums."""
+    L = orc.lib()
+    freq, curr, mass, chrg, gam, npt = 1.3e9, 0.13, 0.51099895e6, -1.0, 190.0, 20000
+    aa, gg, leng = 0.0116, 0.029, 0.035
+    orc.physconst(freq)
+    rng = np.random.default_rng(nz + 1)
+    densz = npt * np.exp(-0.5 * ((np.arange(nz) - nz / 2) / (nz / 6)) ** 2)
+    densz[[0, -1]] = 0.0
+    xsum = densz * 1e-4 * rng.standard_normal(nz)
+    ysum = densz * 1e-4 * rng.standard_normal(nz)
+    rng6 = np.array([-1e-3, 1e-3, -1e-3, 1e-3, -0.9e-3, 1.1e-3]) * 190
+    out = np.zeros(3 * nz)
+    L.orc_wake_field_analytic(nz, orc.dp(densz), orc.dp(xsum), orc.dp(ysum), orc.dp(rng6), gam,
+                              curr, npt, mass, chrg, aa, gg, leng, orc.dp(out))
+    hz = (rng6[5] - rng6[4]) / (nz - 1) / gam
+    recv = densz * curr / freq / npt / hz * chrg / abs(chrg)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        xbar = np.where(densz != 0, xsum / densz, 0.0)
+        ybar = np.where(densz != 0, ysum / densz, 0.0)
+    ex, ey, ez = fft_wake(None, recv, xbar, ybar, hz, True,
+                          greens=analytic_greens(aa, gg, leng, nz, hz))
+    xycon, tcon, bet = kick_consts(gam, curr, mass, chrg, freq)
+    want = np.r_[chrg * ex / xycon / mass / bet / gam, chrg * ey / xycon / mass / bet / gam,
+                 chrg * ez / tcon / mass]
+    for part in range(3):
+        w, o = want[part * nz:(part + 1) * nz], out[part * nz:(part + 1) * nz]
+        assert np.abs(w).max() > 0
+        np.testing.assert_allclose(o, w, rtol=0, atol=1e-11 * np.abs(w).max())
+
+
+def test_wake_switch_of_the_element_loop():
+    """AccSimulator.f90:865-875 with -41's flags: 105/106 with Param(15) > 0
+    turns the (analytic, or the read-in if on) wake on, without it off; other
+    elements turn off only a wake that is not a read-in one.  Observed
+    through orc_run: a lattice of an RF structure with wake parameters then
+    a drift, against the same with the parameters zeroed."""
+    cfg_pts = np.zeros((1000, 9))
+    rng = np.random.default_rng(5)
+    cfg_pts[:, :6] = 1e-3 * rng.standard_normal((1000, 6))
+    cfg_pts[:, 6] = -1.0 / 0.51099895e6
+    cfg_pts[:, 7] = 1e-3 / 1.3e9 / 1000
+    cfg_pts[:, 8] = np.arange(1000) + 1
+    ref = np.array([0, 0, 0, 0, 0, -200.0])
+
+    def rf(wake):
+        v = [1.0e6, 1.3e9, 0.0, -1.0, 1.0] + [0.0] * 19
+        if wake:
+            v[11], v[12], v[13] = 0.0116, 0.029, 0.035
+        return impz.elem(105, 0.2, 4, 1, v)
+
+    drift = impz.elem(0, 0.2, 4, 1, [1.0])
+    orc.wake_off()
+    res = {}
+    for name, lat in (("wake", [rf(True), drift]), ("plain", [rf(False), drift])):
+        rows, p, _ = orc.run(lat, cfg_pts, 1.0, 0.51099895e6, -1.0, 1.3e9, ref, (8, 8, 32))
+        res[name] = rows
+    # identical through nothing, different after the structure's steps
+    assert np.array_equal(res["wake"][0], res["plain"][0])
+    assert not np.allclose(res["wake"][4, 21], res["plain"][4, 21], rtol=1e-12, atol=0)
 
 
 def test_wake_line_density_sums_to_the_particle_count():
