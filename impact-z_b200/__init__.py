@@ -77,6 +77,8 @@ _SIGS = {
     "impz_bunch_download": (ctypes.c_int, [_B, _D, ctypes.c_longlong, _LL]),
     "impz_bunch_destroy": (ctypes.c_int, [_B]),
     "impz_bunch_info": (ctypes.c_int, [_B, _D]),
+    "impz_bunch_geom": (ctypes.c_int, [_B, _D, _D]),
+    "impz_bunch_set_z": (ctypes.c_int, [_B, ctypes.c_double]),
     "impz_bunch_stream": (ctypes.c_void_p, [_B]),
     "impz_map_half": (ctypes.c_int, [_B, _E, ctypes.c_double, _D, ctypes.c_double, ctypes.c_int,
                                      _I]),
@@ -300,6 +302,15 @@ class Bunch:
         _check(lib().impz_bunch_info(self.h, _dp(out)), "impz_bunch_info")
         return {"current": out[0], "npt": int(out[1]), "nlocal": int(out[2]),
                 "refptcl": out[3:9].copy(), "z": out[9], "bytes": int(out[10])}
+
+    def geom(self):
+        """(range[6], msize[3]) of the last space-charge step."""
+        rng, ms = np.zeros(6), np.zeros(3)
+        _check(lib().impz_bunch_geom(self.h, _dp(rng), _dp(ms)), "impz_bunch_geom")
+        return rng, ms
+
+    def set_z(self, z):
+        _check(lib().impz_bunch_set_z(self.h, float(z)), "impz_bunch_set_z")
 
     def download(self):
         pts = np.zeros((self.n0, 9))

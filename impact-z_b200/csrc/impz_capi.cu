@@ -796,6 +796,23 @@ int impz_bunch_info(impz_bunch_t b, double info[11]) {
   return IMPZ_OK;
 }
 
+int impz_bunch_geom(impz_bunch_t b, double range[6], double msize[3]) {
+  if (!b || !range || !msize) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  DevState hs;
+  CK(cudaMemcpyAsync(&hs, b->st, sizeof(hs), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  for (int c = 0; c < 6; c++) range[c] = hs.geom.range[c];
+  for (int c = 0; c < 3; c++) msize[c] = hs.geom.h[c];
+  return IMPZ_OK;
+}
+
+int impz_bunch_set_z(impz_bunch_t b, double z) {
+  if (!b) return IMPZ_ERR_ARG;
+  b->z = z;
+  return IMPZ_OK;
+}
+
 int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]) {
   if (!b || !out) return IMPZ_ERR_ARG;
   CK(cudaSetDevice(b->device));

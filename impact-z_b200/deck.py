@@ -23,6 +23,11 @@
   (reported), any other is refused.
 * `read_wake`: rfdataN.in as the wake table of a -41 element, read1wk_Data
   (src/DataStruct/Data.f90:559-633).
+* `write_checkpoint` / `read_checkpoint`: the -7 checkpoint of
+  outpoint_Output / inpoint_Output (src/Contrl/Output.f90:1733-1774,
+  1371-1437), gfortran's unformatted sequential records; `run_deck` writes
+  one at each -7 and, with the deck's restart flag set, continues from the
+  last -7's file after that element.
 """
 import os
 import re
@@ -216,6 +221,66 @@ def read_wake(path):
     return np.array(rows)
 
 
+def _records(f):
+    """Fortran unformatted sequential records as gfortran writes them: a
+    4-byte little-endian length before and after each record."""
+    while True:
+        head = f.read(4)
+        if not head:
+            return
+        n = int(np.frombuffer(head, "<i4")[0])
+        body = f.read(n)
+        tail = int(np.frombuffer(f.read(4), "<i4")[0])
+        if tail != n or len(body) != n:
+            raise ValueError("not a Fortran unformatted sequential file")
+        yield body
+
+
+def write_checkpoint(path, z, inb, jstp, ibal, nstep, msize, rng, grid, refptcl, pts):
+    """The -7 checkpoint of one rank, outpoint_Output
+    (src/Contrl/Output.f90:1733-1774): z; element index, segment, balance
+    and step counters; mesh size; range; the local mesh table (Nz, Ny) and
+    range table (zmin, zmax, ymin, ymax) of the single rank; Nptlocal;
+    refptcl; Pts1(9, Nptlocal)."""
+    pts = np.ascontiguousarray(pts, dtype="<f8")
+    rng = np.asarray(rng, dtype="<f8")
+    recs = [np.array([z], "<f8"), np.array([inb, jstp, ibal, nstep], "<i4"),
+            np.asarray(msize, "<f8"), rng, np.array([grid[2], grid[1]], "<i4"),
+            np.array([rng[4], rng[5], rng[2], rng[3]], "<f8"), np.array([pts.shape[0]], "<i4"),
+            np.asarray(refptcl, "<f8"), pts]
+    with open(path, "wb") as f:
+        for r in recs:
+            b = r.tobytes()
+            n = np.array([len(b)], "<i4").tobytes()
+            f.write(n + b + n)
+
+
+def read_checkpoint(path):
+    """A -7 checkpoint back (inpoint_Output, src/Contrl/Output.f90:
+    1371-1437, one rank)."""
+    with open(path, "rb") as f:
+        r = list(_records(f))
+    if len(r) != 9:
+        raise ValueError("%s: %d records, a one-rank checkpoint has 9" % (path, len(r)))
+    n = int(np.frombuffer(r[6], "<i4")[0])
+    inb, jstp, ibal, nstep = (int(v) for v in np.frombuffer(r[1], "<i4"))
+    return {"z": float(np.frombuffer(r[0], "<f8")[0]), "inb": inb, "jstp": jstp, "ibal": ibal,
+            "nstep": nstep, "msize": np.frombuffer(r[2], "<f8").copy(),
+            "range": np.frombuffer(r[3], "<f8").copy(),
+            "refptcl": np.frombuffer(r[7], "<f8").copy(),
+            "pts": np.frombuffer(r[8], "<f8").reshape(n, 9).copy()}
+
+
+def checkpoint_file(deck):
+    """nfileout: the file number of the deck's last -7 element, which a
+    restart reads (Input.f90:260, AccSimulator.f90:558-561)."""
+    n = None
+    for e in deck.elements:
+        if e.type == -7:
+            n = e.mapstp
+    return n
+
+
 # the 45 columns of impz_diag_row: z, then the files' columns in order
 _FILES = (("fort.18", 1, 6), ("fort.24", 6, 12), ("fort.25", 12, 18), ("fort.26", 18, 24),
           ("fort.27", 24, 30), ("fort.28", 30, 33), ("fort.29", 33, 39), ("fort.30", 39, 45))
@@ -239,14 +304,16 @@ def read_diag(outdir, name):
         return np.array([[float(x) for x in ln.split()] for ln in f if ln.strip()])
 
 
-def lattice_segments(deck, workdir, skip=()):
+def lattice_segments(deck, workdir, skip=(), start=0):
     """The lattice cut at its control elements, for a runner: yields
     ("run", [impz_elem_t]) for each stretch of beam-line elements (RF tables
     read from workdir), ("dump", Element) for each type -2 phase dump,
     ("wake", {"on", "table", "scale", "transverse"}) for each type -41
-    read-in wake control, and last ("skipped", [types]) for the control
-    elements passed over because they are in `skip`.  -99 ends the lattice;
-    any other control element is refused (ValueError).
+    read-in wake control, ("checkpoint", {"element", "inb", "jstp", "nstep"})
+    for each type -7 checkpoint, and last ("skipped", [types]) for the
+    control elements passed over because they are in `skip`.  -99 ends the
+    lattice; any other control element is refused (ValueError).  `start`
+    skips the first elements (a restart continues after element iend).
 
     A -41 element (src/Contrl/AccSimulator.f90:959-978) reads the table
     rfdata<Param(3)>.in when Param(3) > 0, turns the wake on with scale
@@ -263,9 +330,14 @@ def lattice_segments(deck, workdir, skip=()):
 
     seg, skipped = [], []
     table, no_transverse = None, False
-    for e in deck.elements:
+    nstep, jlast = 0, 0
+    for i, e in enumerate(deck.elements):
+        if i < start:
+            continue
         if e.type >= 0:
             seg.append(to_elem(e))
+            nstep += e.nseg
+            jlast = e.nseg + 1
             continue
         if seg:
             yield "run", seg
@@ -274,6 +346,10 @@ def lattice_segments(deck, workdir, skip=()):
             break
         if e.type == -2:
             yield "dump", e
+        elif e.type == -7:
+            # outpoint_Output's counters: the element (1-based), the segment
+            # loop index the previous element left, the steps so far
+            yield "checkpoint", {"element": e, "inb": i + 1, "jstp": jlast, "nstep": nstep}
         elif e.type in skip:
             skipped.append(e.type)
         elif e.type == -41:
@@ -313,13 +389,20 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
     outdir = outdir or workdir
     deck = read_deck(os.path.join(workdir, "ImpactZ.in"))
     check_supported(deck)
-    pts = read_particles(os.path.join(workdir, "particle.in"))
-    b = Bunch(pts, deck.bcurr, deck.bmass, deck.bcharge, deck.bfreq, deck.refptcl(),
+    start, z0, ref = 0, 0.0, deck.refptcl()
+    if deck.restart == 1:
+        # Rstartflg = 1: continue from the last -7 checkpoint
+        ck = read_checkpoint(os.path.join(workdir, "fort.%d" % checkpoint_file(deck)))
+        pts, ref, z0, start = ck["pts"], ck["refptcl"], ck["z"], ck["inb"]
+    else:
+        pts = read_particles(os.path.join(workdir, "particle.in"))
+    b = Bunch(pts, deck.bcurr, deck.bmass, deck.bcharge, deck.bfreq, ref,
               (deck.nx, deck.ny, deck.nz), form=FORM_FP64 if form is None else form,
               track_ids=True)
+    b.set_z(z0)
     rows, skipped = [], []
     try:
-        for kind, item in lattice_segments(deck, workdir, set(skip)):
+        for kind, item in lattice_segments(deck, workdir, set(skip), start):
             if kind == "skipped":
                 skipped = item
             elif kind == "wake":
@@ -327,6 +410,14 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
                     b.wake(item["table"], item["scale"], item["transverse"])
                 else:
                     b.wake_off()
+            elif kind == "checkpoint":
+                if write:
+                    rng, ms = b.geom()
+                    info = b.info()
+                    write_checkpoint(os.path.join(outdir, "fort.%d" % item["element"].mapstp),
+                                     info["z"], item["inb"], item["jstp"], item["nstep"],
+                                     item["nstep"], ms, rng, (deck.nx, deck.ny, deck.nz),
+                                     info["refptcl"], b.download())
             elif kind == "dump":
                 if write:
                     write_phase(os.path.join(outdir, "fort.%d" % item.mapstp), b.download(),

@@ -121,6 +121,13 @@ int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, i
 int impz_wake_off(impz_bunch_t b);
 /* Current, Npt, Nptlocal, refptcl(1..6), z, device bytes (11 doubles). */
 int impz_bunch_info(impz_bunch_t b, double info[11]);
+/* The computational domain of the last space-charge step (getrange_CompDom
+ * and getmsize_CompDom, CompDom.f90), as a checkpoint records it
+ * (outpoint_Output, Output.f90:1733-1774); zeros before the first one. */
+int impz_bunch_geom(impz_bunch_t b, double range[6], double msize[3]);
+/* Sets the position z [m] of the bunch, as a restart from a checkpoint does
+ * (inpoint_Output, Output.f90:1371-1437); call it between runs. */
+int impz_bunch_set_z(impz_bunch_t b, double z);
 /* The bunch's CUDA stream (cudaStream_t) for callers that interleave work. */
 void* impz_bunch_stream(impz_bunch_t b);
 

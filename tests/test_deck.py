@@ -134,3 +134,37 @@ def test_deck_reader_agrees_with_the_reference_gui_reader(example):
                 break
         assert vals[:4] == [e.length, e.nseg, e.mapstp, e.type]
         assert vals[4:] == e.vals[:len(vals) - 4]
+
+
+def test_checkpoint_round_trip_and_records(tmp_path):
+    """-7 checkpoints (outpoint_Output, Output.f90:1733-1774): nine gfortran
+    unformatted records, read back unchanged."""
+    rng = np.random.default_rng(9)
+    pts = rng.standard_normal((37, 9))
+    path = str(tmp_path / "fort.1234")
+    deck.write_checkpoint(path, 1.25, 7, 3, 40, 40, [1e-4, 2e-4, 3e-4],
+                          [-1, 1, -2, 2, -3, 3], (8, 16, 32), np.arange(6.0), pts)
+    raw = open(path, "rb").read()
+    assert np.frombuffer(raw[:4], "<i4")[0] == 8 and np.frombuffer(raw[12:16], "<i4")[0] == 8
+    assert len(raw) == 9 * 8 + 8 + 16 + 24 + 48 + 8 + 32 + 4 + 48 + 72 * 37
+    ck = deck.read_checkpoint(path)
+    assert ck["z"] == 1.25 and (ck["inb"], ck["jstp"], ck["ibal"], ck["nstep"]) == (7, 3, 40, 40)
+    np.testing.assert_array_equal(ck["pts"], pts)
+    np.testing.assert_array_equal(ck["refptcl"], np.arange(6.0))
+    np.testing.assert_array_equal(ck["range"], [-1, 1, -2, 2, -3, 3])
+
+
+def test_checkpoint_controls_in_the_lattice(tmp_path):
+    """A -7 element yields its counters; a restart skips the elements up to
+    and including it."""
+    z24 = lambda *v: list(v) + [0.0] * (24 - len(v))  # noqa: E731
+    d = deck.Deck(nx=8, ny=8, nz=8)
+    d.elements = [deck.Element(0.5, 3, 1, 0, z24(1.0)), deck.Element(0.0, 0, 1001, -7, z24()),
+                  deck.Element(0.4, 2, 1, 0, z24(1.0)), deck.Element(0.0, 0, 1002, -7, z24())]
+    segs = list(deck.lattice_segments(d, str(tmp_path)))
+    cks = [item for k, item in segs if k == "checkpoint"]
+    assert [(c["inb"], c["jstp"], c["nstep"]) for c in cks] == [(2, 4, 3), (4, 3, 5)]
+    assert deck.checkpoint_file(d) == 1002
+    rest = list(deck.lattice_segments(d, str(tmp_path), start=2))
+    assert [k for k, _ in rest] == ["run", "checkpoint", "skipped"]
+    assert rest[0][1][0].length == 0.4

@@ -79,3 +79,36 @@ def test_deck_runner_matches_the_oracle(tmp_path):
     for name in ("fort.1001", "fort.1002"):
         dump = np.loadtxt(os.path.join(wd, name))
         assert dump.shape == (d.np, 9)
+
+
+def test_checkpoint_and_restart(tmp_path):
+    """A -7 checkpoint after the quadrupoles; the deck run again with its
+    restart flag from that file reproduces the rest of the full run
+    (records after the checkpoint within 1e-10: the restart re-sorts the
+    particles, so moment sums differ at rounding level)."""
+    import shutil
+
+    wd = str(tmp_path / "full")
+    os.makedirs(wd)
+    d = example_like_deck(wd)
+    z24 = lambda *v: list(v) + [0.0] * (24 - len(v))  # noqa: E731
+    cav = next(i for i, e in enumerate(d.elements) if e.type == 103)
+    d.elements.insert(cav, deck.Element(0.0, 0, 2001, -7, z24()))
+    deck.write_deck(os.path.join(wd, "ImpactZ.in"), d)
+    full = deck.run_deck(wd, skip={-8})
+    ck = deck.read_checkpoint(os.path.join(wd, "fort.2001"))
+    assert ck["pts"].shape[0] == 4000 and ck["inb"] == cav + 1
+    rd = str(tmp_path / "restart")
+    os.makedirs(rd)
+    shutil.copy(os.path.join(wd, "fort.2001"), rd)
+    d.restart = 1
+    deck.write_deck(os.path.join(rd, "ImpactZ.in"), d)
+    rest = deck.run_deck(rd, skip={-8})
+    rows_f, rows_r = full["rows"], rest["rows"]
+    k0 = int(np.argmin(np.abs(rows_f[:, 0] - ck["z"])))
+    tail = rows_f[k0:]
+    assert tail.shape == rows_r.shape
+    np.testing.assert_allclose(rows_r[:, 0], tail[:, 0], rtol=0, atol=0)
+    for c in RMS_COLS:
+        scale = np.max(np.abs(tail[:, c])) + 1e-300
+        assert np.max(np.abs(rows_r[:, c] - tail[:, c])) / scale <= 1e-10, c
