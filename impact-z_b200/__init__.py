@@ -78,6 +78,7 @@ _SIGS = {
     "impz_bunch_destroy": (ctypes.c_int, [_B]),
     "impz_bunch_info": (ctypes.c_int, [_B, _D]),
     "impz_bunch_geom": (ctypes.c_int, [_B, _D, _D]),
+    "impz_laser_heater": (ctypes.c_int, [_B, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
     "impz_bunch_set_z": (ctypes.c_int, [_B, ctypes.c_double]),
     "impz_bunch_stream": (ctypes.c_void_p, [_B]),
     "impz_map_half": (ctypes.c_int, [_B, _E, ctypes.c_double, _D, ctypes.c_double, ctypes.c_int,
@@ -308,6 +309,11 @@ class Bunch:
         rng, ms = np.zeros(6), np.zeros(3)
         _check(lib().impz_bunch_geom(self.h, _dp(rng), _dp(ms)), "impz_bunch_geom")
         return rng, ms
+
+    def laser_heater(self, rsig, wavelength, ez):
+        """The energy kick of a type -52 laser heater element."""
+        _check(lib().impz_laser_heater(self.h, float(rsig), float(wavelength), float(ez)),
+               "impz_laser_heater")
 
     def set_z(self, z):
         _check(lib().impz_bunch_set_z(self.h, float(z)), "impz_bunch_set_z")

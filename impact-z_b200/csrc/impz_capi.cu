@@ -98,6 +98,45 @@ __global__ void __launch_bounds__(256) k_bunching(const double* __restrict__ ph,
   }
 }
 
+// per-block sums of x and x^2 (the laser heater's beam size)
+__global__ void __launch_bounds__(256) k_xsums(const double* __restrict__ x, long long n,
+                                               double* part) {
+  __shared__ double s1[8], s2[8];
+  double a = 0.0, q = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    a += x[i];
+    q += x[i] * x[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    q += __shfl_xor_sync(0xffffffffu, q, o);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) { s1[wid] = a; s2[wid] = q; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0.0, tq = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) { ta += s1[w]; tq += s2[w]; }
+    part[2 * blockIdx.x] = ta;
+    part[2 * blockIdx.x + 1] = tq;
+  }
+}
+
+// laser heater energy kick of a type -52 element (AccSimulator.f90:1001-1006):
+// pt -= amp * sin(-harm * phase) * exp(-(x^2 + y^2) / tmp2)
+__global__ void __launch_bounds__(256) k_laser_kick(const double* __restrict__ x,
+                                                    const double* __restrict__ y,
+                                                    const double* __restrict__ ph,
+                                                    double* __restrict__ pt, long long n,
+                                                    double amp, double harm, double tmp2) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double rr = (x[i] * x[i] + y[i] * y[i]) / tmp2;
+    pt[i] = pt[i] - amp * sin(-harm * ph[i]) * exp(-rr);
+  }
+}
+
 __global__ void k_to_double(const float* in, long long n, double scale, double* out) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -881,6 +920,45 @@ int impz_wake_off(impz_bunch_t b) {
   b->csr.flagwake = b->csr.flagwakeread = 0;
   b->csr_run.flagwake = b->csr_run.flagwakeread = 0;
   ++b->wk_gen;
+  return IMPZ_OK;
+}
+
+int impz_laser_heater(impz_bunch_t b, double rsig, double wavelength, double ez) {
+  if (!b || !(rsig > 0.0) || !(wavelength > 0.0)) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  DevState hs;
+  CK(cudaMemcpyAsync(&hs, b->st, sizeof(hs), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  if (hs.nlocal < 1) return IMPZ_OK;
+  double* const* p = b->pbuf[b->parity];
+  const int nb = (int)std::min<long long>((hs.nlocal + 255) / 256, kMaxAdvGrid);
+  // the push's partial-sum scratch is free between calls
+  k_xsums<<<nb, 256, 0, b->stream>>>(p[0], hs.nlocal, b->mom_part);
+  CK(cudaGetLastError());
+  std::vector<double> part((size_t)2 * nb);
+  CK(cudaMemcpyAsync(part.data(), b->mom_part, part.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  double xygl[2] = {0.0, 0.0};
+  for (int i = 0; i < nb; i++) {
+    xygl[0] += part[2 * i];
+    xygl[1] += part[2 * i + 1];
+  }
+  // AccSimulator.f90:982-1006
+  xygl[0] = xygl[0] / (double)hs.npt;
+  xygl[1] = xygl[1] / (double)hs.npt;
+  const double Scxl = b->P.Scxl, Clight = 299792458.0;
+  const double sigx2 = (xygl[1] - xygl[0] * xygl[0]) * Scxl * Scxl;
+  const double tmp1 = std::sqrt(2 * (sigx2 + rsig * rsig) / (rsig * rsig));
+  const double freqlaser = Clight / wavelength;
+  const double harm = freqlaser / b->P.Scfreq;
+  const double tmp2 = 4 * rsig * rsig / Scxl / Scxl;
+  const double ezlaser = ez / b->k.mass;
+  k_laser_kick<<<nb, 256, 0, b->stream>>>(p[0], p[2], p[4], p[5], hs.nlocal, tmp1 * ezlaser,
+                                          harm, tmp2);
+  CK(cudaGetLastError());
+  g_launches += 2;
+  CK(cudaStreamSynchronize(b->stream));
   return IMPZ_OK;
 }
 

@@ -18,8 +18,9 @@
 * `run_deck` runs a deck of the map integrator with open boundaries and a
   particle.in distribution (Flagmap=1, Flagbc=1, Flagdist=19) on the GPU
   runner, splitting the lattice at control elements (types < 0,
-  `lattice_segments`): -2 dumps phase space, -41 turns the read-in wake on
-  or off, -99 ends the lattice, the types listed in `skip` are passed over
+  `lattice_segments`): -2 dumps phase space, -7 writes a checkpoint, -41
+  turns the read-in wake on or off, -52 applies the laser heater's energy
+  kick, -99 ends the lattice, the types listed in `skip` are passed over
   (reported), any other is refused.
 * `read_wake`: rfdataN.in as the wake table of a -41 element, read1wk_Data
   (src/DataStruct/Data.f90:559-633).
@@ -310,7 +311,8 @@ def lattice_segments(deck, workdir, skip=(), start=0):
     read from workdir), ("dump", Element) for each type -2 phase dump,
     ("wake", {"on", "table", "scale", "transverse"}) for each type -41
     read-in wake control, ("checkpoint", {"element", "inb", "jstp", "nstep"})
-    for each type -7 checkpoint, and last ("skipped", [types]) for the
+    for each type -7 checkpoint, ("laser", {"rsig", "wavelength", "ez"}) for
+    each type -52 laser heater, and last ("skipped", [types]) for the
     control elements passed over because they are in `skip`.  -99 ends the
     lattice; any other control element is refused (ValueError).  `start`
     skips the first elements (a restart continues after element iend).
@@ -346,12 +348,15 @@ def lattice_segments(deck, workdir, skip=(), start=0):
             break
         if e.type == -2:
             yield "dump", e
+        elif e.type in skip:
+            skipped.append(e.type)
+        elif e.type == -52:
+            # laser heater (AccSimulator.f90:982-1006): Param(2..4)
+            yield "laser", {"rsig": e.vals[0], "wavelength": e.vals[1], "ez": e.vals[2]}
         elif e.type == -7:
             # outpoint_Output's counters: the element (1-based), the segment
             # loop index the previous element left, the steps so far
             yield "checkpoint", {"element": e, "inb": i + 1, "jstp": jlast, "nstep": nstep}
-        elif e.type in skip:
-            skipped.append(e.type)
         elif e.type == -41:
             scale, rfile, onoff = e.vals[0], e.vals[1], e.vals[2]
             if rfile > 0.0:
@@ -410,6 +415,8 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
                     b.wake(item["table"], item["scale"], item["transverse"])
                 else:
                     b.wake_off()
+            elif kind == "laser":
+                b.laser_heater(item["rsig"], item["wavelength"], item["ez"])
             elif kind == "checkpoint":
                 if write:
                     rng, ms = b.geom()

@@ -119,6 +119,12 @@ int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]);
  * carries from one impz_run to the next. */
 int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, int transverse);
 int impz_wake_off(impz_bunch_t b);
+/* Laser heater of a type -52 element (AccSimulator.f90:982-1006): the
+ * energy kick pt -= A sin(-h phase) exp(-(x^2+y^2)/(4 rsig^2/Scxl^2)) with
+ * A = sqrt(2 (sigx^2 + rsig^2) / rsig^2) ez / mass from the beam's rms x,
+ * h the laser frequency over Scfreq; rsig = Param(2) [m], wavelength =
+ * Param(3) [m], ez = Param(4) [eV].  Applied between runs. */
+int impz_laser_heater(impz_bunch_t b, double rsig, double wavelength, double ez);
 /* Current, Npt, Nptlocal, refptcl(1..6), z, device bytes (11 doubles). */
 int impz_bunch_info(impz_bunch_t b, double info[11]);
 /* The computational domain of the last space-charge step (getrange_CompDom

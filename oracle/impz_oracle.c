@@ -1640,6 +1640,29 @@ void orc_csr_field(int nz, const double *densz, const double range[6], double ga
 }
 
 /* ------------------------------------------------------------------ */
+/* Laser heater of a type -52 element (AccSimulator.f90:982-1006), one rank */
+void orc_laser_heater(double *pts, int n, int npt, double rsig, double wavelength, double ez,
+                      double mass) {
+  double xygl[2] = {0.0, 0.0};
+  for (int i = 0; i < n; i++) {
+    xygl[0] = xygl[0] + P(i, 0);
+    xygl[1] = xygl[1] + P(i, 0) * P(i, 0);
+  }
+  xygl[0] = xygl[0] / npt;
+  xygl[1] = xygl[1] / npt;
+  const double sigx2 = (xygl[1] - xygl[0] * xygl[0]) * PC.Scxl * PC.Scxl;
+  const double tmp1 = sqrt(2 * (sigx2 + rsig * rsig) / (rsig * rsig));
+  const double freqlaser = PC.Clight / wavelength;
+  const double harm = freqlaser / PC.Scfreq;
+  const double tmp2 = 4 * rsig * rsig / PC.Scxl / PC.Scxl;
+  const double ezlaser = ez / mass;
+  for (int i = 0; i < n; i++) {
+    const double rr = (P(i, 0) * P(i, 0) + P(i, 2) * P(i, 2)) / tmp2;
+    P(i, 5) = P(i, 5) - tmp1 * ezlaser * sin(-harm * P(i, 4)) * exp(-rr);
+  }
+}
+
+/* ------------------------------------------------------------------ */
 static double pipe_radius(const orc_elem *e) {
   /* getradius_BeamLineElem (BeamLineElem.f90:500-552): Param index per type */
   switch (e->type) {

@@ -124,6 +124,8 @@ void orc_csr_wake(int nx, double r0, double ptmin, double hx, double blength,
 void orc_csr_field(int nz, const double *densz, const double range[6], double gam,
                    double curr, int npt, double mass, double chrg, double r0, double s0,
                    double blen, double *out);
+void orc_laser_heater(double *pts, int n, int npt, double rsig, double wavelength, double ez,
+                      double mass);
 /* diagnostic1_Output (Output.f90:20-371): raw sums and one derived row */
 void orc_moment_sums(const double *pts, int n, double raw[ORC_RAW_LEN]);
 void orc_diag_row(double z, const double raw[ORC_RAW_LEN], int npt, int nlocal,

@@ -105,6 +105,8 @@ def lib():
             "orc_csr_field": (v, [ctypes.c_int, _D, _D, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, _D]),
+            "orc_laser_heater": (v, [_D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_double]),
             "orc_moment_sums": (v, [_D, ctypes.c_int, _D]),
             "orc_diag_row": (v, [ctypes.c_double, _D, ctypes.c_int, ctypes.c_int, _D,
                                  ctypes.c_double, _D]),

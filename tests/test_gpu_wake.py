@@ -111,8 +111,9 @@ def test_wake_launches_are_counted():
 
 def test_deck_runner_with_wake_controls_matches_the_oracle(tmp_path):
     """An Example3-shaped deck with -41 controls around its cavity (wake on
-    with the table of rfdata41.in, off again after the first bend) through
-    run_deck (FP64) and through the oracle over the same segments."""
+    with the table of rfdata41.in, off again after the first bend) and a
+    -52 laser heater before it, through run_deck (FP64) and through the
+    oracle over the same segments."""
     from test_gpu_deck import example_like_deck
 
     wd = str(tmp_path)
@@ -122,11 +123,13 @@ def test_deck_runner_with_wake_controls_matches_the_oracle(tmp_path):
     d.elements.insert(cav, deck.Element(0.0, 0, 1, -41, z24(1.0, 41, 1.0)))
     bend = next(i for i, e in enumerate(d.elements) if e.type == 4)
     d.elements.insert(bend + 1, deck.Element(0.0, 0, 1, -41, z24(1.0, 41, -1.0)))
+    # laser heater: 1 mm laser spot, 1030 nm, 200 keV amplitude
+    d.elements.insert(cav, deck.Element(0.0, 0, 1, -52, z24(1.0e-3, 1.03e-6, 2.0e5)))
     deck.write_deck(os.path.join(wd, "ImpactZ.in"), d)
     np.savetxt(os.path.join(wd, "rfdata41.in"), synthetic_table())
     out = deck.run_deck(wd, skip={-8})
     pts = deck.read_particles(os.path.join(wd, "particle.in"))
-    ref, z, rows_o, nwake = d.refptcl(), 0.0, [], 0
+    ref, z, rows_o, nwake, nlaser = d.refptcl(), 0.0, [], 0, 0
     try:
         for kind, item in deck.lattice_segments(d, wd, {-8}):
             if kind == "run":
@@ -140,9 +143,15 @@ def test_deck_runner_with_wake_controls_matches_the_oracle(tmp_path):
                     orc.wake_set(item["table"], item["scale"], item["transverse"])
                 else:
                     orc.wake_off()
+            elif kind == "laser":
+                nlaser += 1
+                pts = np.ascontiguousarray(pts)
+                orc.lib().orc_laser_heater(orc.dp(pts), pts.shape[0], pts.shape[0],
+                                           item["rsig"], item["wavelength"], item["ez"],
+                                           d.bmass)
     finally:
         orc.wake_off()
-    assert nwake == 2
+    assert nwake == 2 and nlaser == 1
     rows_o = np.array(rows_o)
     rows_g = out["rows"]
     assert rows_g.shape == rows_o.shape
@@ -213,3 +222,27 @@ def test_read_in_wake_switched_off_by_a_structure_without_wake():
     assert worst(g1, r1, RMS_COLS) <= 1e-8
     assert worst(g2, r2, RMS_COLS) <= 1e-8
     assert worst(rk[: r1.shape[0]], r1, [21, 23]) > 1e-5
+
+
+def test_laser_heater_kick_matches_the_oracle():
+    """impz_laser_heater (AccSimulator.f90:982-1006) on the device = the
+    oracle's kick on the same particles, per particle (sin/exp to 1e-12 of
+    the kick's scale), and it moves pt by far more than that."""
+    cfg = electron_cfg(n=20_000)
+    b = impz.Bunch(cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=impz.FORM_FP64, track_ids=True)
+    try:
+        b.laser_heater(1.0e-3, 1.03e-6, 2.0e5)
+        got = b.download()
+    finally:
+        b.close()
+    orc.physconst(cfg["freq"])
+    want = np.ascontiguousarray(cfg["pts"]).copy()
+    orc.lib().orc_laser_heater(orc.dp(want), want.shape[0], want.shape[0], 1.0e-3, 1.03e-6,
+                               2.0e5, cfg["mass"])
+    got = got[np.argsort(got[:, 8])]
+    want = want[np.argsort(want[:, 8])]
+    kick = np.abs(want[:, 5] - cfg["pts"][np.argsort(cfg["pts"][:, 8])][:, 5]).max()
+    assert kick > 1e-3 * np.abs(want[:, 5]).max()
+    np.testing.assert_array_equal(got[:, :5], want[:, :5])
+    assert np.abs(got[:, 5] - want[:, 5]).max() <= 1e-12 * kick

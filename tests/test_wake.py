@@ -269,15 +269,16 @@ def test_deck_wake_controls():
 @pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference examples not present")
 def test_example3_runs_with_its_wake_on_the_oracle():
     """Example3's ten -41 controls switch the cavities' read-in wake
-    (rfdata41.in) on and off around the 1.3 GHz cavities: the oracle runs
-    the deck with them and the wake changes the final energy spread."""
+    (rfdata41.in) on and off around the 1.3 GHz cavities, and its -52 laser
+    heater kicks the energy: the oracle runs the whole deck (its slice
+    output -8 passed over) and the wake changes the final energy spread."""
     wd = os.path.join(EXAMPLES, "Example3")
     d = deck.read_deck(os.path.join(wd, "ImpactZ.in"))
     pts0 = deck.read_particles(os.path.join(wd, "particle.in"))
     finals = {}
     for with_wake in (True, False):
         pts, ref, z, nwake = pts0, d.refptcl(), 0.0, 0
-        skip = {-8, -52} | (set() if with_wake else {-41})
+        skip = {-8} | (set() if with_wake else {-41})
         try:
             for kind, item in deck.lattice_segments(d, wd, skip):
                 if kind == "run":
@@ -290,6 +291,11 @@ def test_example3_runs_with_its_wake_on_the_oracle():
                         orc.wake_set(item["table"], item["scale"], item["transverse"])
                     else:
                         orc.wake_off()
+                elif kind == "laser":
+                    p = np.ascontiguousarray(pts)
+                    orc.lib().orc_laser_heater(orc.dp(p), p.shape[0], p.shape[0], item["rsig"],
+                                               item["wavelength"], item["ez"], d.bmass)
+                    pts = p
         finally:
             orc.wake_off()
         assert nwake == (10 if with_wake else 0)
