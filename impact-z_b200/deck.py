@@ -18,7 +18,9 @@
 * `run_deck` runs a deck of the map integrator with open boundaries and a
   particle.in distribution (Flagmap=1, Flagbc=1, Flagdist=19) on the GPU
   runner, splitting the lattice at control elements (types < 0,
-  `lattice_segments`): -2 dumps phase space, -7 writes a checkpoint, -41
+  `lattice_segments`): -2 dumps phase space, -7 writes a checkpoint, -8
+  appends a slice table (`slice_output`, sliceprocdep_Output of
+  src/Contrl/Output.f90:3002-3215), -41
   turns the read-in wake on or off, -52 applies the laser heater's energy
   kick, -99 ends the lattice, the types listed in `skip` are passed over
   (reported), any other is refused.
@@ -272,6 +274,87 @@ def read_checkpoint(path):
             "pts": np.frombuffer(r[8], "<f8").reshape(n, 9).copy()}
 
 
+def slice_output(pts, npt, nslice, qchg, pmass, alphax0, betax0, alphay0, betay0, gam0, scxl):
+    """The slice table of a type -8 element, sliceprocdep_Output
+    (src/Contrl/Output.f90:3002-3215), for one rank: Pts1 (z frame) cut into
+    nslice linearly weighted slices in phase over the bunch (its extent
+    widened by 0.5e-5 at each end); per slice the columns -z [m], weight,
+    current [A], rms emittances x, y [m rad], -<pt>/gamma0, uncorrelated
+    energy spread [eV], centroids x, y [m] and the mismatch factors against
+    (alpha0, beta0).  The reference's quirks are kept: its speed of light
+    2.99792e8 in the current and the uncentred <x px> in alpha."""
+    pts = np.asarray(pts, dtype=np.float64)
+    f32 = lambda v: float(np.float32(v))  # noqa: E731
+    clite = 2.99792e8
+    sclcur = clite * qchg / npt
+    with np.errstate(divide="ignore", invalid="ignore"):  # a zero beta0 gives inf, as there
+        gamx0 = np.float64(1.0 + alphax0 ** 2) / np.float64(betax0)
+        gamy0 = np.float64(1.0 + alphay0 ** 2) / np.float64(betay0)
+    z = pts[:, 4]
+    zmn, zmx = z.min(), z.max()
+    zmin = zmn - (zmx - zmn) * f32(0.5e-5)
+    zmax = zmx + (zmx - zmn) * f32(0.5e-5)
+    hz = (zmax - zmin) / (nslice - 1)
+    iz = np.trunc((z - zmin) / hz + 1).astype(np.int64)
+    iz = np.where(iz < 1, 1, iz)
+    iz = np.where(iz >= nslice, nslice - 1, iz)
+    ab = ((zmin - z) + iz * hz) / hz
+    # contributions in the reference's order: particle by particle, iz then iz+1
+    idx = np.stack([iz - 1, iz], axis=1).ravel()
+    wts = np.stack([ab, 1.0 - ab], axis=1).ravel()
+
+    def acc(v):
+        return np.bincount(idx, weights=np.repeat(v, 2) * wts, minlength=nslice)
+
+    x, px, y, py, pt = pts[:, 0], pts[:, 1], pts[:, 2], pts[:, 3], pts[:, 5]
+    count = np.bincount(idx, weights=wts, minlength=nslice)
+    sums = [acc(v) for v in (x, x ** 2, px, px ** 2, x * px, y, y ** 2, py, py ** 2, y * py, pt)]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        have = count > 0
+        xx, xx2, pxm, px2, xpx, yy, yy2, pym, py2, ypy, gam = (
+            np.where(have, sm / np.where(have, count, 1.0), 0.0) for sm in sums)
+        epx = np.sqrt((xx2 - xx ** 2) * (px2 - pxm ** 2) - (xpx - xx * pxm) ** 2)
+        epy = np.sqrt((yy2 - yy ** 2) * (py2 - pym ** 2) - (ypy - yy * pym) ** 2)
+        alphax = -xpx / epx
+        gambet = np.sqrt((gam0 - gam) ** 2 - 1.0)
+        betax = (xx2 - xx ** 2) * gambet / epx
+        gamx = (1.0 + alphax ** 2) / betax
+        bmx = betax * gamx0 - 2 * alphax * alphax0 + gamx * betax0
+        alphay = -ypy / epy
+        betay = (yy2 - yy ** 2) * gambet / epy
+        gamy = (1.0 + alphay ** 2) / betay
+        bmy = betay * gamy0 - 2 * alphay * alphay0 + gamy * betay0
+        epx, epy = np.where(have, epx, 0.0), np.where(have, epy, 0.0)
+        bmx, bmy = np.where(have, bmx, 0.0), np.where(have, bmy, 0.0)
+        gammaz = gam[iz - 1] * ab + gam[iz] * (1.0 - ab)
+        dg2 = (-(pt - gammaz)) ** 2
+        unc = np.sqrt(np.bincount(idx, weights=np.repeat(dg2, 2) * wts, minlength=nslice) / count)
+        zz = zmin + np.arange(nslice) * hz
+        return np.c_[-zz * scxl, count, count / (hz * scxl) * sclcur, epx * scxl, epy * scxl,
+                     -gam / gam0, unc * pmass, xx * scxl, yy * scxl, bmx, bmy]
+
+
+def slice_params(e):
+    """nslice and the matching Twiss values of a -8 element
+    (AccSimulator.f90:908-922), beta_y0's default as written there (it tests
+    beta_x0 a second time, so a zero beta_y0 stays zero)."""
+    nslice = int(e.vals[0] + 0.1)
+    alphax0, betax0, alphay0, betay0 = e.vals[1], e.vals[2], e.vals[3], e.vals[4]
+    if betax0 == 0.0:
+        betax0 = 1.0
+    if betax0 == 0.0:
+        betay0 = 1.0
+    return nslice, alphax0, betax0, alphay0, betay0
+
+
+def write_slices(path, rows):
+    """Appends a slice table (the reference writes to a unit it keeps open,
+    so repeated -8 elements of one file number accumulate)."""
+    with open(path, "a") as f:
+        for r in rows:
+            f.write(" ".join("%.17g" % v for v in r) + "\n")
+
+
 def checkpoint_file(deck):
     """nfileout: the file number of the deck's last -7 element, which a
     restart reads (Input.f90:260, AccSimulator.f90:558-561)."""
@@ -312,7 +395,8 @@ def lattice_segments(deck, workdir, skip=(), start=0):
     ("wake", {"on", "table", "scale", "transverse"}) for each type -41
     read-in wake control, ("checkpoint", {"element", "inb", "jstp", "nstep"})
     for each type -7 checkpoint, ("laser", {"rsig", "wavelength", "ez"}) for
-    each type -52 laser heater, and last ("skipped", [types]) for the
+    each type -52 laser heater, ("slices", Element) for each type -8 slice
+    output, and last ("skipped", [types]) for the
     control elements passed over because they are in `skip`.  -99 ends the
     lattice; any other control element is refused (ValueError).  `start`
     skips the first elements (a restart continues after element iend).
@@ -350,6 +434,8 @@ def lattice_segments(deck, workdir, skip=(), start=0):
             yield "dump", e
         elif e.type in skip:
             skipped.append(e.type)
+        elif e.type == -8:
+            yield "slices", e
         elif e.type == -52:
             # laser heater (AccSimulator.f90:982-1006): Param(2..4)
             yield "laser", {"rsig": e.vals[0], "wavelength": e.vals[1], "ez": e.vals[2]}
@@ -391,6 +477,7 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
     Returns {"rows": diag rows, "skipped": [types passed over], "pts": final
     Pts1}."""
     from . import FORM_FP64, Bunch, diag_row
+    from .beams import scxl
     outdir = outdir or workdir
     deck = read_deck(os.path.join(workdir, "ImpactZ.in"))
     check_supported(deck)
@@ -417,6 +504,14 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
                     b.wake_off()
             elif kind == "laser":
                 b.laser_heater(item["rsig"], item["wavelength"], item["ez"])
+            elif kind == "slices":
+                if write:
+                    info = b.info()
+                    nslice, ax, bx, ay, by = slice_params(item)
+                    rows_s = slice_output(b.download(), info["npt"], nslice,
+                                          info["current"] / deck.bfreq, deck.bmass, ax, bx, ay,
+                                          by, -info["refptcl"][5], scxl(deck.bfreq))
+                    write_slices(os.path.join(outdir, "fort.%d" % item.mapstp), rows_s)
             elif kind == "checkpoint":
                 if write:
                     rng, ms = b.geom()

@@ -39,16 +39,16 @@ def test_reads_the_reference_example_decks():
 
 
 @have_examples
-def test_example3_lattice_runs_on_the_path_with_its_wake_controls_skipped():
+def test_example3_lattice_runs_on_the_path_with_its_controls_skipped():
     """Example3 (map integrator, open BC, particle.in) maps onto the path's
-    elements once its wake (-41), laser-heater (-52) and slice-output (-8)
-    controls are passed over; the oracle runs it (138 steps)."""
+    elements, its controls all handled (wake -41, laser heater -52, slice
+    output -8); with them passed over the oracle runs its 138 steps."""
     orc = load_oracle()
     wd = os.path.join(EXAMPLES, "Example3")
     d = deck.read_deck(os.path.join(wd, "ImpactZ.in"))
     deck.check_supported(d)
-    with pytest.raises(ValueError):
-        list(deck.lattice_segments(d, wd))
+    kinds = {k for k, _ in deck.lattice_segments(d, wd)}
+    assert kinds == {"run", "dump", "wake", "laser", "slices", "skipped"}
     pts = deck.read_particles(os.path.join(wd, "particle.in"))
     ref, z, nrows, skipped = d.refptcl(), 0.0, 0, None
     for kind, item in deck.lattice_segments(d, wd, {-8, -41, -52}):
@@ -168,3 +168,64 @@ def test_checkpoint_controls_in_the_lattice(tmp_path):
     rest = list(deck.lattice_segments(d, str(tmp_path), start=2))
     assert [k for k, _ in rest] == ["run", "checkpoint", "skipped"]
     assert rest[0][1][0].length == 0.4
+
+
+def _slices_by_loop(pts, npt, nslice, qchg, pmass, ax0, bx0, ay0, by0, gam0, scxl):
+    """sliceprocdep_Output (Output.f90:3002-3215) as plain loops."""
+    import math
+    f32 = lambda v: float(np.float32(v))  # noqa: E731
+    sclcur = 2.99792e8 * qchg / npt
+    gx0, gy0 = (1 + ax0 ** 2) / bx0, (1 + ay0 ** 2) / by0
+    zmn, zmx = min(pts[:, 4]), max(pts[:, 4])
+    zmin, zmax = zmn - (zmx - zmn) * f32(0.5e-5), zmx + (zmx - zmn) * f32(0.5e-5)
+    hz = (zmax - zmin) / (nslice - 1)
+    acc = [[0.0] * nslice for _ in range(12)]
+    cells = []
+    for p in pts:
+        iz = min(max(int((p[4] - zmin) / hz + 1), 1), nslice - 1)
+        ab = ((zmin - p[4]) + iz * hz) / hz
+        cells.append((iz, ab))
+        vals = (1.0, p[0], p[0] ** 2, p[1], p[1] ** 2, p[0] * p[1], p[2], p[2] ** 2, p[3],
+                p[3] ** 2, p[2] * p[3], p[5])
+        for k, v in enumerate(vals):
+            acc[k][iz - 1] += v * ab
+            acc[k][iz] += v * (1.0 - ab)
+    out = []
+    mean = [[acc[k][i] / acc[0][i] if acc[0][i] > 0 else 0.0 for i in range(nslice)]
+            for k in range(12)]
+    unc = [0.0] * nslice
+    for p, (iz, ab) in zip(pts, cells):
+        gz = mean[11][iz - 1] * ab + mean[11][iz] * (1 - ab)
+        unc[iz - 1] += (p[5] - gz) ** 2 * ab
+        unc[iz] += (p[5] - gz) ** 2 * (1 - ab)
+    for i in range(nslice):
+        c = acc[0][i]
+        xx, xx2, px, px2, xpx, yy, yy2, py, py2, ypy, gam = (mean[k][i] for k in range(1, 12))
+        epx = math.sqrt((xx2 - xx ** 2) * (px2 - px ** 2) - (xpx - xx * px) ** 2)
+        epy = math.sqrt((yy2 - yy ** 2) * (py2 - py ** 2) - (ypy - yy * py) ** 2)
+        gb = math.sqrt((gam0 - gam) ** 2 - 1)
+        axx, bxx = -xpx / epx, (xx2 - xx ** 2) * gb / epx
+        ayy, byy = -ypy / epy, (yy2 - yy ** 2) * gb / epy
+        bmx = bxx * gx0 - 2 * axx * ax0 + (1 + axx ** 2) / bxx * bx0
+        bmy = byy * gy0 - 2 * ayy * ay0 + (1 + ayy ** 2) / byy * by0
+        out.append([-(zmin + i * hz) * scxl, c, c / (hz * scxl) * sclcur, epx * scxl,
+                    epy * scxl, -gam / gam0, math.sqrt(unc[i] / c) * pmass, xx * scxl,
+                    yy * scxl, bmx, bmy])
+    return np.array(out)
+
+
+def test_slice_output_matches_a_loop_restatement():
+    """-8 slice tables (sliceprocdep_Output): the vectorised form = plain
+    loops over a correlated bunch, every slice populated."""
+    rng = np.random.default_rng(21)
+    n = 3000
+    pts = np.zeros((n, 9))
+    pts[:, :6] = rng.standard_normal((n, 6)) * [1e-2, 1e-3, 1e-2, 1e-3, 0.05, 0.02]
+    pts[:, 1] += 0.3 * pts[:, 0] * 1e-1
+    pts[:, 5] += 0.5 * pts[:, 4]
+    args = (n, 7, 1e-9, 0.511e6, 0.5, 2.0, -0.3, 3.0, 200.0, 0.118)
+    got = deck.slice_output(pts, *args)
+    want = _slices_by_loop(pts, *args)
+    assert got.shape == (7, 11) and np.all(np.isfinite(got))
+    np.testing.assert_allclose(got, want, rtol=1e-10, atol=0)
+    assert abs(got[:, 1].sum() - n) < 1e-9 * n

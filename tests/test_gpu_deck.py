@@ -1,7 +1,7 @@
 """The standalone deck runner on the GPU against the oracle: a deck shaped
 like the reference's Example3 (98 MeV electrons, phase dumps, drifts,
 quadrupoles, ideal-RF cavities, 150-type dipoles, a slice-output control
-that is passed over), written with impz_b200.deck, run by run_deck (FP64)
+whose table is checked), written with impz_b200.deck, run by run_deck (FP64)
 and by the oracle over the same lattice_segments.  fort.24-30 rms columns
 within 1e-8, z exact, the phase dump holds every particle."""
 import os
@@ -55,10 +55,19 @@ def example_like_deck(workdir, n=4000):
 def test_deck_runner_matches_the_oracle(tmp_path):
     wd = str(tmp_path)
     d = example_like_deck(wd)
-    out = deck.run_deck(wd, skip={-8})
-    assert out["skipped"] == [-8]
-    # the oracle over the same segments
+    out = deck.run_deck(wd)
+    assert out["skipped"] == []
+    # the slice table of the -8 at the start: the initial bunch's
     pts = deck.read_particles(os.path.join(wd, "particle.in"))
+    nslice, ax, bx, ay, by = deck.slice_params(d.elements[0])
+    want = deck.slice_output(pts, pts.shape[0], nslice, d.bcurr / d.bfreq, d.bmass, ax, bx, ay,
+                             by, -d.refptcl()[5], beams.scxl(d.bfreq))
+    got = np.loadtxt(os.path.join(wd, "fort.201"))
+    assert got.shape == want.shape == (101, 11)
+    fin = np.isfinite(want)
+    assert np.array_equal(fin, np.isfinite(got))
+    np.testing.assert_allclose(got[fin], want[fin], rtol=1e-12, atol=0)
+    # the oracle over the same segments
     ref, z, rows_o = d.refptcl(), 0.0, []
     for kind, item in deck.lattice_segments(d, wd, {-8}):
         if kind == "run":
