@@ -1197,9 +1197,9 @@ int impz_maplinear(const impz_elem_t* e, double zedge, double t, double tau, dou
     maplinear_quad(P, t, tau, xm, refpt, e->val[0], e->mapstp, charge, mass);
     return IMPZ_OK;
   }
-  if (e->type == 103 && e->ndata > 1) {
+  if (e->type >= 101 && e->type <= 104 && e->ndata > 1) {
     if (e->mapstp < 1) return IMPZ_ERR_ARG;
-    maplinear_ccl(P, t, tau, xm, refpt, zedge, *e, charge, mass);
+    maplinear_rfgap(P, t, tau, xm, refpt, zedge, *e, charge, mass);
     return IMPZ_OK;
   }
   return IMPZ_ERR_UNSUPPORTED;

@@ -190,10 +190,14 @@ void ccl_field(const impz_elem_t& e, double zedge, double z, double& ez1, double
 }
 }  // namespace
 
-void maplinear_ccl(const Phys& P, double t, double tau, double xm[36], double refpt[6],
-                   double zedge, const impz_elem_t& e, double chg, double mass) {
-  // maplinear_CCL (CCL.f90:122-215), intfunc1_CCL (269-328)
+void maplinear_rfgap(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                     double zedge, const impz_elem_t& e, double chg, double mass) {
+  // maplinear_CCL (CCL.f90:122-215), intfunc1_CCL (269-328); CCDTL and SC
+  // (CCDTL.f90, SC.f90:122-328) are the same map, DTL (DTL.f90:136-347)
+  // adds its drift-tube quadrupoles (getBgradfld_DTL, DTL.f90:395-418:
+  // Param(7..10) = val[5..8])
   const double Scxl = P.Scxl;
+  const bool dtl = e.type == 101;
   const double ww = e.val[1] / P.Scfreq;
   // theta0 = Param(4)*asin(1.0)/90 with a default-real asin(1.0)
   const double theta0 = e.val[2] * (double)std::asin(1.0f) / 90;
@@ -234,7 +238,15 @@ void maplinear_ccl(const Phys& P, double t, double tau, double xm[36], double re
                      sinphi * ww / Scxl +
                  1.5 * (1.0 - 0.5 * (gamma0 * gamma0)) * (q * q);
     s55 = Scxl * s55;
-    lin_rhs(Scxl, yy, f, s11tmp * Scxl, s11tmp * Scxl, s55);
+    if (dtl) {
+      const double zz = tt - zedge;
+      const double bgrad = zz < e.val[5] ? e.val[6] : (zz < e.length - e.val[7] ? 0.0 : e.val[8]);
+      const double gbet = std::sqrt((gamma0 - 1.0) * (gamma0 + 1.0));
+      const double brho = gbet / P.Clight / qmcc;
+      lin_rhs(Scxl, yy, f, (s11tmp + bgrad / brho) * Scxl, (s11tmp - bgrad / brho) * Scxl, s55);
+    } else {
+      lin_rhs(Scxl, yy, f, s11tmp * Scxl, s11tmp * Scxl, s55);
+    }
   });
   refpt[4] = y[4];
   refpt[5] = y[5];
@@ -366,10 +378,10 @@ int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, do
       op.c[5] = gam0; op.c[6] = gambet; op.c[7] = gam0o; op.c[8] = std::cos(phi0lc);
       return push_op(prog, op);
     }
-    if (e.type == 103 && e.ndata > 1 && e.zdat && e.edat && e.epdat && e.eppdat) {
+    if (e.type <= 104 && e.ndata > 1 && e.zdat && e.edat && e.epdat && e.eppdat) {
       if (e.mapstp < 1) return IMPZ_ERR_ARG;
       double xm[36];
-      maplinear_ccl(P, z, tau, xm, refptcl, zedge, e, sp.charge, sp.mass);
+      maplinear_rfgap(P, z, tau, xm, refptcl, zedge, e, sp.charge, sp.mass);
       return push_op(prog, op_xm6(xm));
     }
     return IMPZ_ERR_UNSUPPORTED;

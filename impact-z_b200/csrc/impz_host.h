@@ -13,12 +13,14 @@ struct Phys {  // PhysConst (src/DataStruct/PhysConst.f90:25-35)
 };
 Phys make_phys(double freq);
 
-// maplinear_Quadrupole / maplinear_DriftTube / maplinear_CCL (RK6 of the
-// 18-variable linear ODE); refpt(5), refpt(6) advance like the reference.
+// maplinear_Quadrupole / maplinear_DriftTube and the RF gaps' linear maps
+// over an on-axis field table, maplinear_DTL / CCDTL / CCL / SC (types
+// 101..104; RK6 of the 18-variable linear ODE); refpt(5), refpt(6) advance
+// like the reference.
 void maplinear_quad(const Phys& P, double t, double tau, double xm[36], double refpt[6],
                     double gradient, int mapstp, double chg, double mass);
-void maplinear_ccl(const Phys& P, double t, double tau, double xm[36], double refpt[6],
-                   double zedge, const impz_elem_t& e, double chg, double mass);
+void maplinear_rfgap(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                     double zedge, const impz_elem_t& e, double chg, double mass);
 
 struct BendState {  // the bend constants AccSimulator.f90:1057-1093 keeps
   bool active;

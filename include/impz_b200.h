@@ -52,8 +52,10 @@ typedef struct impz_bunch_s* impz_bunch_t;
  * Supported types: 0 drift, 1 quadrupole (gradient, or K map when
  * v2 in (-10,-1e-6)), 4 dipole (file ID v3 <= 200: no CSR; above 200 CSR
  * inside the bend, above 500 also downstream: impz_run only), 101..106 RF gaps
- * as the ideal-RF model (v4 < 0) and 103 (CCL) as the RK6 linear map over
- * the on-axis table zdat/edat/epdat/eppdat (rfdataN.in, read1_Data). */
+ * as the ideal-RF model (v4 < 0), and 101 DTL (with its drift-tube
+ * quadrupoles, v6..v9), 102 CCDTL, 103 CCL and 104 SC as the RK6 linear
+ * map over the on-axis table zdat/edat/epdat/eppdat (rfdataN.in,
+ * read1_Data); 105 SolRF and 106 TWS only as ideal gaps. */
 typedef struct {
   int type;
   int nseg;
@@ -267,8 +269,9 @@ int impz_server_stats(impz_server_t s, double out[8]);
 int impz_server_destroy(impz_server_t s);
 
 /* Host-side maps (for checking and for callers that keep their own loop):
- * maplinear_Quadrupole (Quadrupole.f90:120-252) and maplinear_CCL
- * (CCL.f90:122-328) by the same RK6; refpt is updated like the reference. */
+ * maplinear_Quadrupole (Quadrupole.f90:120-252) and the RF gaps'
+ * maplinear_DTL / CCDTL / CCL / SC (DTL.f90:136-418, CCDTL.f90, CCL.f90,
+ * SC.f90:122-328) by the same RK6; refpt is updated like the reference. */
 int impz_maplinear(const impz_elem_t* e, double zedge, double t, double tau,
                    double refpt[6], double charge, double mass, double freq, double xm[36]);
 

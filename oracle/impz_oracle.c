@@ -260,6 +260,10 @@ typedef struct {
   double zedge, escale, ww, theta0, qmcc;
   int ndata;
   const double *zdat, *edat, *epdat, *eppdat;
+  /* DTL (type 101): the element length and its drift-tube quadrupoles,
+   * Param(7..10) (DTL.f90:26-29) */
+  int dtl;
+  double dlen, q1len, q1grad, q2len, q2grad;
 } ccl_ctx;
 
 /* getaxfldE_CCL (CCL.f90:331-365): bisection + linear interpolation */
@@ -301,8 +305,19 @@ static void ccl_rhs(double t, const double *y, double *f, const void *vctx) {
   s11tmp = 0.5 * (1.0 + 0.5 * (gamma0 * gamma0)) * (q * q) +
            c->qmcc * 0.5 / ((beta0 * beta0) * beta0) / ((gamma0 * gamma0) * gamma0) * ez1 *
                sinphi * c->ww / Scxl;
-  s11 = s11tmp * Scxl;
-  s33 = s11tmp * Scxl;
+  if (c->dtl) {
+    /* intfunc1_DTL (DTL.f90:286-347): the drift-tube quadrupole gradient of
+     * getBgradfld_DTL (DTL.f90:395-418) focuses x and defocuses y */
+    const double zz = t - c->zedge;
+    const double bgrad = zz < c->q1len ? c->q1grad : (zz < c->dlen - c->q2len ? 0.0 : c->q2grad);
+    const double gbet = sqrt((gamma0 - 1.0) * (gamma0 + 1.0));
+    const double brho = gbet / PC.Clight / c->qmcc;
+    s11 = (s11tmp + bgrad / brho) * Scxl;
+    s33 = (s11tmp - bgrad / brho) * Scxl;
+  } else {
+    s11 = s11tmp * Scxl;
+    s33 = s11tmp * Scxl;
+  }
   s55 = -(1.5 * c->qmcc / (beta0 * beta0) / gamma0 * ezp1 * cosphi) +
         ((beta0 * beta0) + 0.5) / ((beta0 * beta0) * beta0) / gamma0 * c->qmcc * ez1 * sinphi *
             c->ww / Scxl +
@@ -311,14 +326,22 @@ static void ccl_rhs(double t, const double *y, double *f, const void *vctx) {
   lin_rhs(y, f, s11, s33, s55);
 }
 
-/* maplinear_CCL (CCL.f90:122-215) */
-void orc_maplinear_ccl(double t, double tau, double xm[36], double refpt[6],
-                       double zedge, double escale, double freq, double phase_deg,
-                       int mapstp, double chg, double mass,
-                       int ndata, const double *zdat, const double *edat,
-                       const double *epdat, const double *eppdat) {
+/* maplinear_CCL (CCL.f90:122-215); maplinear_CCDTL and maplinear_SC
+ * (CCDTL.f90:122-215, SC.f90:122-215) are the same map; maplinear_DTL
+ * (DTL.f90:136-232) adds the drift-tube quadrupoles (dtlq = length,
+ * Param(7..10), NULL for the others) */
+static void maplinear_rf(double t, double tau, double xm[36], double refpt[6], double zedge,
+                         double escale, double freq, double phase_deg, int mapstp, double chg,
+                         double mass, int ndata, const double *zdat, const double *edat,
+                         const double *epdat, const double *eppdat, const double *dtlq) {
   const double Scxl = PC.Scxl;
   ccl_ctx c;
+  c.dtl = dtlq != NULL;
+  c.dlen = dtlq ? dtlq[0] : 0.0;
+  c.q1len = dtlq ? dtlq[1] : 0.0;
+  c.q1grad = dtlq ? dtlq[2] : 0.0;
+  c.q2len = dtlq ? dtlq[3] : 0.0;
+  c.q2grad = dtlq ? dtlq[4] : 0.0;
   double y[18], h, t0, gi, betai, ui, squi, sqi3, gf, betaf, uf, squf, sqf3, s;
   double ein, e1in, e2in, ef, e1f, e2f, sinthi, costhi, uprimi, qpwi, dlti, thli;
   double sinthf, costhf, uprimf, qpwf, dltf, thlf, tfin;
@@ -365,6 +388,26 @@ void orc_maplinear_ccl(double t, double tau, double xm[36], double refpt[6],
   dltf = Scxl * (0.5 * uprimf / uf - qpwf * e1f * sinthf);
   thlf = 1.5 * Scxl * (uprimf / uf);
   xm_assemble(xm, y, squi, squf, sqi3, sqf3, dlti, dltf, thli, thlf);
+}
+
+void orc_maplinear_ccl(double t, double tau, double xm[36], double refpt[6],
+                       double zedge, double escale, double freq, double phase_deg,
+                       int mapstp, double chg, double mass,
+                       int ndata, const double *zdat, const double *edat,
+                       const double *epdat, const double *eppdat) {
+  maplinear_rf(t, tau, xm, refpt, zedge, escale, freq, phase_deg, mapstp, chg, mass, ndata, zdat,
+               edat, epdat, eppdat, NULL);
+}
+
+void orc_maplinear_dtl(double t, double tau, double xm[36], double refpt[6],
+                       double zedge, double escale, double freq, double phase_deg,
+                       int mapstp, double chg, double mass,
+                       int ndata, const double *zdat, const double *edat,
+                       const double *epdat, const double *eppdat, double length,
+                       double q1len, double q1grad, double q2len, double q2grad) {
+  const double q[5] = {length, q1len, q1grad, q2len, q2grad};
+  maplinear_rf(t, tau, xm, refpt, zedge, escale, freq, phase_deg, mapstp, chg, mass, ndata, zdat,
+               edat, epdat, eppdat, q);
 }
 
 /* 6x6 loop of drift1_BeamBunch (BeamBunch.f90:310-320) */
@@ -1823,11 +1866,14 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
           if (e->val[3] < 0.0) {
             orc_ideal_rf(beam->pts, beam->nlocal, beam->refptcl, beam->mass, tau1,
                          e->val[0], e->val[1], e->val[2], j, bnseg, ihlf);
-          } else if (bitype == 103 && e->ndata > 1) {
+          } else if (bitype <= 104 && e->ndata > 1) {
+            /* DTL, CCDTL, CCL, SC linear maps (maplinear_BeamLineElem,
+             * BeamLineElem.f90:776-800) */
             double xm[36];
-            orc_maplinear_ccl(z, tau1, xm, beam->refptcl, zedge, e->val[0], e->val[1],
-                              e->val[2], e->mapstp, beam->charge, beam->mass, e->ndata,
-                              e->zdat, e->edat, e->epdat, e->eppdat);
+            const double dtlq[5] = {blength, e->val[5], e->val[6], e->val[7], e->val[8]};
+            maplinear_rf(z, tau1, xm, beam->refptcl, zedge, e->val[0], e->val[1], e->val[2],
+                         e->mapstp, beam->charge, beam->mass, e->ndata, e->zdat, e->edat,
+                         e->epdat, e->eppdat, bitype == 101 ? dtlq : NULL);
             orc_apply_xm(beam->pts, beam->nlocal, xm);
           } else {
             free(rho);

@@ -45,6 +45,12 @@ void orc_maplinear_quad(double t, double tau, double xm[36], double refpt[6],
 void orc_maplinear_drift(double t, double tau, double xm[36], double refpt[6],
                          int mapstp, double chg, double mass);
 /* maplinear_CCL with on-axis table (CCL.f90:122-365); zdat shifted to start at 0 */
+void orc_maplinear_dtl(double t, double tau, double xm[36], double refpt[6],
+                       double zedge, double escale, double freq, double phase_deg,
+                       int mapstp, double chg, double mass,
+                       int ndata, const double *zdat, const double *edat,
+                       const double *epdat, const double *eppdat, double length,
+                       double q1len, double q1grad, double q2len, double q2grad);
 void orc_maplinear_ccl(double t, double tau, double xm[36], double refpt[6],
                        double zedge, double escale, double freq, double phase_deg,
                        int mapstp, double chg, double mass,

@@ -109,3 +109,36 @@ def test_footprint_is_exact_arena_plus_tables():
     assert impz.footprint(4_000_000, grid, nsteps=1000) > f0
     assert impz.lib().impz_bunch_footprint(0, 64, 64, 128, 1, 0, 0) == -1
     assert impz.lib().impz_bunch_footprint(10, 64, 64, 128, 1, 0, -1) == -1
+
+
+@pytest.mark.parametrize("etype", [101, 102, 104])
+def test_dtl_ccdtl_sc_linear_maps_match_oracle_bitwise(etype):
+    """CCDTL and SC use CCL's map; DTL adds its drift-tube quadrupoles
+    (getBgradfld_DTL: 5 cm at +8 T/m, 4 cm at -6 T/m at the ends)."""
+    freq, mass, charge = 402.5e6, beams.PROTON_MASS_EV, 1.0
+    ref = beams.refptcl_for(2.5e6, mass)
+    zt = np.linspace(0.0, 0.2, 41)
+    ez = 1e6 * np.sin(np.pi * zt / 0.2)
+    ezp = 1e6 * np.pi / 0.2 * np.cos(np.pi * zt / 0.2)
+    ezpp = -1e6 * (np.pi / 0.2) ** 2 * np.sin(np.pi * zt / 0.2)
+    vals = [1.0, 402.5e6, -30.0, 1.0, 0.01, 0.05, 8.0, 0.04, -6.0]
+    e = impz.elem(etype, 0.2, 4, 5, vals, rf=(zt, ez, ezp, ezpp))
+    cols = [np.ascontiguousarray(c) for c in (zt, ez, ezp, ezpp)]
+    orc.physconst(freq)
+    for t in (0.01, 0.08, 0.17):  # in the first quadrupole, between, in the second
+        xm_p, ref_p = impz.maplinear(e, 0.0, t, 0.025, ref, charge, mass, freq)
+        xm_o, ref_o = np.zeros(36), ref.copy()
+        args = (t, 0.025, orc.dp(xm_o), orc.dp(ref_o), 0.0, 1.0, 402.5e6, -30.0, 5, charge,
+                mass, len(zt), *[orc.dp(c) for c in cols])
+        if etype == 101:
+            orc.lib().orc_maplinear_dtl(*args, 0.2, 0.05, 8.0, 0.04, -6.0)
+        else:
+            orc.lib().orc_maplinear_ccl(*args)
+        np.testing.assert_array_equal(xm_p, xm_o.reshape(6, 6, order="F"))
+        np.testing.assert_array_equal(ref_p, ref_o)
+    if etype == 101:  # the quadrupole shows in the transverse blocks
+        xm_d, _ = impz.maplinear(e, 0.0, 0.01, 0.025, ref, charge, mass, freq)
+        xm_c, _ = impz.maplinear(impz.elem(103, 0.2, 4, 5, vals, rf=(zt, ez, ezp, ezpp)), 0.0,
+                                 0.01, 0.025, ref, charge, mass, freq)
+        assert abs(xm_d[1, 0] - xm_c[1, 0]) > 1e-3 * abs(xm_c[1, 0]) + 1e-9
+        assert abs(xm_d[3, 2] - xm_c[3, 2]) > 1e-3 * abs(xm_c[3, 2]) + 1e-9

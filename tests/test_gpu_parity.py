@@ -333,3 +333,38 @@ def test_single_step_with_particle_loss(small, form):
         np.testing.assert_allclose(g["range"], o["range"], rtol=1e-12, atol=0)
         assert np.abs(g["counts"] - o["counts"]).sum() <= 8
         assert rel_l2(g["eg"], o["eg"]) <= 1e-5
+
+
+def rf_table(length=0.2, amp=1e6, n=41):
+    zt = np.linspace(0.0, length, n)
+    k = np.pi / length
+    return zt, amp * np.sin(k * zt), amp * k * np.cos(k * zt), -amp * k * k * np.sin(k * zt)
+
+
+def test_rf_linear_maps_lattice_fp64_moments():
+    """Drift, then a DTL (101, with its drift-tube quadrupoles), a CCDTL
+    (102), a CCL (103) and an SC cavity (104) as linear maps over an
+    on-axis table (maplinear_DTL/CCDTL/CCL/SC), FP64: rms columns of every
+    record within 1e-8 of the oracle, z exact."""
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 14)
+    tab = rf_table()
+    gap = lambda t, v: impz.elem(t, 0.2, 4, 5, v, rf=tab)  # noqa: E731
+    lat = [impz.elem(0, 0.1, 2, 1, [1.0]),
+           gap(101, [1.0, 402.5e6, -30.0, 1.0, 1.0, 0.05, 15.0, 0.05, -15.0]),
+           gap(102, [1.0, 402.5e6, -30.0, 1.0, 1.0]), gap(103, [1.0, 402.5e6, -30.0, 1.0, 1.0]),
+           gap(104, [1.0, 402.5e6, -30.0, 1.0, 1.0]), impz.elem(0, 0.1, 2, 1, [1.0])]
+    rows_o, p_o, beam = orc.run(lat, cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"],
+                                cfg["freq"], cfg["refptcl"], cfg["grid"])
+    b = impz.Bunch(cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=impz.FORM_FP64, track_ids=False)
+    recs, zs = b.run(lat)
+    refs = b.run_reference()
+    b.close()
+    assert recs.shape[0] == rows_o.shape[0] == 21
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    np.testing.assert_allclose(refs[:, 4:6], np.c_[rows_o[:, 1], -rows_o[:, 2]], rtol=1e-14,
+                               atol=0)
+    rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], cfg["mass"], cfg["freq"])
+                       for i in range(len(recs))])
+    _row_cmp(rows_g, rows_o, RMS_COLS, 1e-8)
+    assert rows_o[-1, 3] > rows_o[0, 3]  # the cavities accelerate
