@@ -179,7 +179,8 @@ def _dp(a):
 # ---------------------------------------------------------------------------
 def elem(etype, length, nseg, mapstp=1, vals=(), rf=None):
     """Build an impz_elem_t.  vals are the deck values v1..v24; rf is an
-    optional (z, Ez, Ez', Ez'') on-axis table for linear RF maps."""
+    optional (z, Ez, Ez', Ez'') on-axis table for linear RF maps, or for a
+    SolRF (105) the 1-D array of read3_Data's Fourier coefficients."""
     e = ElemStruct()
     e.type = int(etype)
     e.nseg = int(nseg)
@@ -188,7 +189,12 @@ def elem(etype, length, nseg, mapstp=1, vals=(), rf=None):
     for i, v in enumerate(vals):
         e.val[i] = float(v)
     e._keep = None
-    if rf is not None:
+    if rf is not None and np.ndim(rf) == 1:
+        coef = np.ascontiguousarray(rf, dtype=np.float64)
+        e.ndata = len(coef)
+        e.zdat = coef.ctypes.data_as(_D)
+        e._keep = [coef]
+    elif rf is not None:
         cols = [np.ascontiguousarray(c, dtype=np.float64) for c in rf]
         e.ndata = len(cols[0])
         e.zdat, e.edat, e.epdat, e.eppdat = [c.ctypes.data_as(_D) for c in cols]

@@ -1202,6 +1202,16 @@ int impz_maplinear(const impz_elem_t* e, double zedge, double t, double tau, dou
     maplinear_rfgap(P, t, tau, xm, refpt, zedge, *e, charge, mass);
     return IMPZ_OK;
   }
+  if (e->type == 105 && solrf_table_ok(*e)) {
+    if (e->mapstp < 1) return IMPZ_ERR_ARG;
+    maplinear_solrf(P, t, tau, xm, refpt, zedge, *e, charge, mass);
+    return IMPZ_OK;
+  }
+  if (e->type == 106 && tws_table_ok(*e)) {
+    if (e->mapstp < 1) return IMPZ_ERR_ARG;
+    maplinear_tws(P, t, tau, xm, refpt, zedge, *e, charge, mass);
+    return IMPZ_OK;
+  }
   return IMPZ_ERR_UNSUPPORTED;
 }
 

@@ -29,7 +29,7 @@ Phys make_phys(double freq) {
 namespace {
 const int NV = 18;
 
-template <typename RHS>
+template <int NV = 18, typename RHS>
 void rk6(double h, int ns, double t, double* y, RHS rhs) {
   double yt[NV], a[NV], b[NV], c[NV], d[NV], e[NV], f[NV], g[NV], o[NV], p[NV];
   const double tint = t;
@@ -189,6 +189,271 @@ void ccl_field(const impz_elem_t& e, double zedge, double z, double& ez1, double
   ezpp1 = ezpp1 * escale;
 }
 }  // namespace
+
+namespace {
+// getaxfldE_SolRF (SolRF.f90:355-466): the on-axis field as the Fourier
+// series of read3_Data's coefficients F (F(1) their count, F(2..4) the
+// series' start, end and period within the element, then the constant,
+// cosine and sine terms), zero outside the element and the series' range
+void solrf_field(const Phys& P, const impz_elem_t& e, double zedge, double z, double& ez1,
+                 double& ezp1) {
+  const double escale = e.val[0];
+  const double len = e.length;
+  const double epstol = (double)1.0e-10f;
+  const double* F = e.zdat - 1;  // F(1..ndata)
+  ez1 = 0.0;
+  ezp1 = 0.0;
+  if (!((z >= zedge && z <= zedge + len) || std::fabs(z - zedge) <= epstol ||
+        std::fabs(z - zedge - len) <= epstol))
+    return;
+  const double zlc = z - zedge;
+  const int numpar1 = (int)(F[1] + 0.1);
+  const double zstart1 = F[2], zend1 = F[3], zlength1 = F[4];
+  if (!((zlc >= zstart1 && zlc <= zend1) || std::fabs(zlc - zstart1) <= epstol ||
+        std::fabs(zlc - zend1) <= epstol))
+    return;
+  const double zmid = zlength1 / 2;
+  const double zz = z - zedge - zstart1 - zmid;
+  const double zlen = zlength1;
+  const int ntmp = 4;
+  ez1 = F[ntmp + 1] / 2;
+  for (int i = 2; i <= (numpar1 - 1) / 2 + 1; i++) {
+    const double arg = (i - 1) * 2 * P.Pi * zz / zlen;
+    const double c = std::cos(arg), s = std::sin(arg);
+    ez1 = ez1 + F[2 * i - 2 + ntmp] * c + F[2 * i - 1 + ntmp] * s;
+    ezp1 = ezp1 + (i - 1) * 2 * P.Pi / zlen * (-F[2 * i - 2 + ntmp] * s + F[2 * i - 1 + ntmp] * c);
+  }
+  ez1 = ez1 * escale;
+  ezp1 = ezp1 * escale;
+}
+}  // namespace
+
+bool solrf_table_ok(const impz_elem_t& e) {
+  if (e.ndata < 5 || !e.zdat) return false;
+  const int numpar1 = (int)(e.zdat[0] + 0.1);
+  // the series reads F(5 .. numpar1+4)
+  return numpar1 >= 1 && numpar1 + 4 <= e.ndata && e.zdat[3] != 0.0;
+}
+
+void maplinear_solrf(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                     double zedge, const impz_elem_t& e, double chg, double mass) {
+  // maplinear_SolRF (SolRF.f90:126-233), intfunc1_SolRF (287-353): the RF
+  // gap's map plus a constant solenoid b0 = Param(12) = val[10], its
+  // focusing in s11 = s33 and its rotation in four more variables
+  const double Scxl = P.Scxl;
+  const double ww = e.val[1] / P.Scfreq;
+  const double theta0 = e.val[2] * (double)std::asin(1.0f) / 90;
+  const double qmcc = chg / mass;
+  const double b0 = e.val[10];
+  double y[22];
+  y_start(y, refpt);
+  y[18] = 1.0; y[19] = 0.0; y[20] = 0.0; y[21] = 1.0;
+  const double h = tau / e.mapstp;
+  const double gi = -refpt[5];
+  const double betai = std::sqrt(gi * gi - 1.) / gi;
+  double ui, squi, sqi3;
+  uvals(gi, ui, squi, sqi3);
+  double ein, e1in;
+  solrf_field(P, e, zedge, t, ein, e1in);
+  const double sinthi = std::sin(ww * refpt[4] + theta0);
+  const double costhi = std::cos(ww * refpt[4] + theta0);
+  const double uprimi = qmcc * ein / betai * costhi;
+  const double qpwi = 0.5 * qmcc * Scxl / (ui * ww);
+  const double dlti = Scxl * (0.5 * uprimi / ui - qpwi * e1in * sinthi);
+  const double thli = 1.5 * Scxl * (uprimi / ui);
+  rk6<22>(h, e.mapstp, t, y, [&](double tt, const double* yy, double* f) {
+    double ez1, ezp1;
+    solrf_field(P, e, zedge, tt, ez1, ezp1);
+    f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+    const double gamma0 = -yy[5];
+    const double beta0 = std::sqrt(gamma0 * gamma0 - 1.) / gamma0;
+    const double gbet = std::sqrt((gamma0 - 1.0) * (gamma0 + 1.0));
+    const double sinphi = std::sin(ww * yy[4] + theta0);
+    const double cosphi = std::cos(ww * yy[4] + theta0);
+    const double rfdsgn = ez1 * cosphi;
+    f[4] = 1.0 / (beta0 * Scxl);
+    f[5] = -(qmcc * rfdsgn);
+    const double brho = gbet / P.Clight / qmcc;
+    const double q = qmcc * rfdsgn / (beta0 * beta0) / (gamma0 * gamma0);
+    const double s11tmp =
+        0.5 * (1.0 + 0.5 * (gamma0 * gamma0)) * (q * q) +
+        qmcc * 0.5 / ((beta0 * beta0) * beta0) / ((gamma0 * gamma0) * gamma0) * ez1 * sinphi *
+            ww / Scxl;
+    const double sol = 0.5 * b0 / brho;
+    const double s11 = (s11tmp + sol * sol / 2) * Scxl;
+    double s55 = -(1.5 * qmcc / (beta0 * beta0) / gamma0 * ezp1 * cosphi) +
+                 ((beta0 * beta0) + 0.5) / ((beta0 * beta0) * beta0) / gamma0 * qmcc * ez1 *
+                     sinphi * ww / Scxl +
+                 1.5 * (1.0 - 0.5 * (gamma0 * gamma0)) * (q * q);
+    s55 = Scxl * s55;
+    lin_rhs(Scxl, yy, f, s11, s11, s55);
+    const double c2alpha = -b0 / brho / 2;
+    f[18] = -c2alpha * yy[20];
+    f[19] = -c2alpha * yy[21];
+    f[20] = c2alpha * yy[18];
+    f[21] = c2alpha * yy[19];
+  });
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  const double gf = -refpt[5];
+  const double betaf = std::sqrt(gf * gf - 1.) / gf;
+  double uf, squf, sqf3;
+  uvals(gf, uf, squf, sqf3);
+  double ef, e1f;
+  solrf_field(P, e, zedge, t + tau, ef, e1f);
+  const double sinthf = std::sin(ww * refpt[4] + theta0);
+  const double costhf = std::cos(ww * refpt[4] + theta0);
+  const double uprimf = qmcc * ef / betaf * costhf;
+  const double qpwf = 0.5 * qmcc * Scxl / (uf * ww);
+  const double dltf = Scxl * (0.5 * uprimf / uf - qpwf * e1f * sinthf);
+  const double thlf = 1.5 * Scxl * (uprimf / uf);
+  xm_from_y(xm, y, squi, squf, sqi3, sqf3, dlti, dltf, thli, thlf);
+  // the transverse blocks with the solenoid's rotation (SolRF.f90:216-235),
+  // each written as the reference writes it
+  auto X = [&](int j, int k) -> double& { return xm[(j - 1) + 6 * (k - 1)]; };
+  const double* Y = y - 1;
+  for (int r = 0; r < 2; r++) {  // rows 1,2 from the x block, 3,4 from y
+    const int a = r == 0 ? 7 : 11;          // first y index of the block
+    const double ca = Y[r == 0 ? 19 : 21];  // factor for the x columns
+    const double cb = Y[r == 0 ? 20 : 22];  // factor for the y columns
+    const int j = 2 * r + 1;
+    const double m1 = Y[a] * squi / squf + Y[a + 2] * squi / squf * dlti;
+    const double m2 = (Y[a + 1] - Y[a] * dltf) * squi * squf +
+                      (Y[a + 3] - Y[a + 2] * dltf) * squi * squf * dlti;
+    X(j, 1) = ca * m1;
+    X(j + 1, 1) = ca * m2;
+    X(j, 2) = ca * Y[a + 2] / (squi * squf);
+    X(j + 1, 2) = ca * (Y[a + 3] - Y[a + 2] * dltf) * squf / squi;
+    X(j, 3) = cb * m1;
+    X(j + 1, 3) = cb * m2;
+    X(j, 4) = cb * Y[a + 2] / (squi * squf);
+    X(j + 1, 4) = cb * (Y[a + 3] - Y[a + 2] * dltf) * squf / squi;
+  }
+}
+
+namespace {
+// one Fourier series of getaxfldE_TWS (TWS.f90:350-466): count, start, end
+// and period at F(k0+1..k0+4), terms from F(k0+5); pi is the routine's own
+// default-real 2*asin(1.0)
+void tws_series(const double* F, int k0, double pi, double zedge, double z, double zlc,
+                double epstol, double& ez, double& ezp) {
+  const int numpar = (int)(F[k0 + 1] + 0.1);
+  const double zstart = F[k0 + 2], zend = F[k0 + 3], zlength = F[k0 + 4];
+  if (!((zlc >= zstart && zlc <= zend) || std::fabs(zlc - zstart) <= epstol ||
+        std::fabs(zlc - zend) <= epstol))
+    return;
+  const double zmid = zlength / 2;
+  const double zz = z - zedge - zstart - zmid;
+  const double zlen = zlength;
+  const int ntmp = k0 + 4;
+  ez = F[ntmp + 1] / 2;
+  for (int i = 2; i <= (numpar - 1) / 2 + 1; i++) {
+    const double arg = (i - 1) * 2 * pi * zz / zlen;
+    const double c = std::cos(arg), s = std::sin(arg);
+    ez = ez + F[2 * i - 2 + ntmp] * c + F[2 * i - 1 + ntmp] * s;
+    ezp = ezp + (i - 1) * 2 * pi / zlen * (-F[2 * i - 2 + ntmp] * s + F[2 * i - 1 + ntmp] * c);
+  }
+}
+
+void tws_field(const impz_elem_t& e, double zedge, double z, double& ez1, double& ezp1,
+               double& ez12, double& ezp12) {
+  const double pi = (double)(2 * std::asin(1.0f));
+  const double epstol = (double)1.0e-10f;
+  const double escale = e.val[0];
+  const double len = e.length;
+  const double* F = e.zdat - 1;
+  ez1 = ezp1 = ez12 = ezp12 = 0.0;
+  if (!((z >= zedge && z <= zedge + len) || std::fabs(z - zedge) <= epstol ||
+        std::fabs(z - zedge - len) <= epstol))
+    return;
+  const double zlc = z - zedge;
+  tws_series(F, 0, pi, zedge, z, zlc, epstol, ez1, ezp1);
+  ez1 = ez1 * escale;
+  ezp1 = ezp1 * escale;
+  const int numpar1 = (int)(F[1] + 0.1);
+  tws_series(F, numpar1 + 4, pi, zedge, z, zlc, epstol, ez12, ezp12);
+  ez12 = ez12 * escale;
+  ezp12 = ezp12 * escale;
+}
+}  // namespace
+
+bool tws_table_ok(const impz_elem_t& e) {
+  if (e.ndata < 9 || !e.zdat) return false;
+  const int n1 = (int)(e.zdat[0] + 0.1);
+  if (n1 < 1 || n1 + 8 > e.ndata || e.zdat[3] == 0.0) return false;
+  const int n2 = (int)(e.zdat[n1 + 4] + 0.1);
+  return n2 >= 1 && n1 + 8 + n2 <= e.ndata && e.zdat[n1 + 7] != 0.0;
+}
+
+void maplinear_tws(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                   double zedge, const impz_elem_t& e, double chg, double mass) {
+  // maplinear_TWS (TWS.f90:129-229), intfunc1_TWS (231-340): the gap's map
+  // over two standing waves, the second shifted by theta2 = Param(12)
+  const double Scxl = P.Scxl;
+  const double ww = e.val[1] / P.Scfreq;
+  const double theta0 = e.val[2] * (double)std::asin(1.0f) / 90;
+  const double theta2 = e.val[10] * (double)std::asin(1.0f) / 90;
+  const double qmcc = chg / mass;
+  double y[NV];
+  y_start(y, refpt);
+  const double h = tau / e.mapstp;
+  const double gi = -refpt[5];
+  const double betai = std::sqrt(gi * gi - 1.) / gi;
+  double ui, squi, sqi3;
+  uvals(gi, ui, squi, sqi3);
+  double ein, e1in, ein2, e1in2;
+  tws_field(e, zedge, t, ein, e1in, ein2, e1in2);
+  const double sinthi = std::sin(ww * refpt[4] + theta0);
+  const double costhi = std::cos(ww * refpt[4] + theta0);
+  const double sinthi2 = std::sin(ww * refpt[4] + theta0 + theta2);
+  const double costhi2 = std::cos(ww * refpt[4] + theta0 + theta2);
+  const double uprimi = qmcc * (ein * costhi + ein2 * costhi2) / betai;
+  const double qpwi = 0.5 * qmcc * Scxl / (ui * ww);
+  const double dlti = Scxl * (0.5 * uprimi / ui - qpwi * (e1in * sinthi + e1in2 * sinthi2));
+  const double thli = 1.5 * Scxl * (uprimi / ui);
+  rk6(h, e.mapstp, t, y, [&](double tt, const double* yy, double* f) {
+    double ez1, ezp1, ez12, ezp12;
+    tws_field(e, zedge, tt, ez1, ezp1, ez12, ezp12);
+    f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+    const double gamma0 = -yy[5];
+    const double beta0 = std::sqrt(gamma0 * gamma0 - 1.) / gamma0;
+    const double sinphi = std::sin(ww * yy[4] + theta0);
+    const double cosphi = std::cos(ww * yy[4] + theta0);
+    const double sinphi2 = std::sin(ww * yy[4] + theta0 + theta2);
+    const double cosphi2 = std::cos(ww * yy[4] + theta0 + theta2);
+    const double rfdsgn = ez1 * cosphi + ez12 * cosphi2;
+    f[4] = 1.0 / (beta0 * Scxl);
+    f[5] = -(qmcc * rfdsgn);
+    const double q = qmcc * rfdsgn / (beta0 * beta0) / (gamma0 * gamma0);
+    const double es = ez1 * sinphi + ez12 * sinphi2;
+    const double s11tmp =
+        0.5 * (1.0 + 0.5 * (gamma0 * gamma0)) * (q * q) +
+        qmcc * 0.5 / ((beta0 * beta0) * beta0) / ((gamma0 * gamma0) * gamma0) * es * ww / Scxl;
+    double s55 = -(1.5 * qmcc / (beta0 * beta0) / gamma0 * (ezp1 * cosphi + ezp12 * cosphi2)) +
+                 ((beta0 * beta0) + 0.5) / ((beta0 * beta0) * beta0) / gamma0 * qmcc * es * ww /
+                     Scxl +
+                 1.5 * (1.0 - 0.5 * (gamma0 * gamma0)) * (q * q);
+    s55 = Scxl * s55;
+    lin_rhs(Scxl, yy, f, s11tmp * Scxl, s11tmp * Scxl, s55);
+  });
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  const double gf = -refpt[5];
+  const double betaf = std::sqrt(gf * gf - 1.) / gf;
+  double uf, squf, sqf3;
+  uvals(gf, uf, squf, sqf3);
+  double ef, e1f, ef2, e1f2;
+  tws_field(e, zedge, t + tau, ef, e1f, ef2, e1f2);
+  const double sinthf = std::sin(ww * refpt[4] + theta0);
+  const double costhf = std::cos(ww * refpt[4] + theta0);
+  const double sinthf2 = std::sin(ww * refpt[4] + theta0 + theta2);
+  const double costhf2 = std::cos(ww * refpt[4] + theta0 + theta2);
+  const double uprimf = qmcc * (ef * costhf + ef2 * costhf2) / betaf;
+  const double qpwf = 0.5 * qmcc * Scxl / (uf * ww);
+  const double dltf = Scxl * (0.5 * uprimf / uf - qpwf * (e1f * sinthf + e1f2 * sinthf2));
+  const double thlf = 1.5 * Scxl * (uprimf / uf);
+  xm_from_y(xm, y, squi, squf, sqi3, sqf3, dlti, dltf, thli, thlf);
+}
 
 void maplinear_rfgap(const Phys& P, double t, double tau, double xm[36], double refpt[6],
                      double zedge, const impz_elem_t& e, double chg, double mass) {
@@ -382,6 +647,18 @@ int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, do
       if (e.mapstp < 1) return IMPZ_ERR_ARG;
       double xm[36];
       maplinear_rfgap(P, z, tau, xm, refptcl, zedge, e, sp.charge, sp.mass);
+      return push_op(prog, op_xm6(xm));
+    }
+    if (e.type == 105 && solrf_table_ok(e)) {
+      if (e.mapstp < 1) return IMPZ_ERR_ARG;
+      double xm[36];
+      maplinear_solrf(P, z, tau, xm, refptcl, zedge, e, sp.charge, sp.mass);
+      return push_op(prog, op_xm6(xm));
+    }
+    if (e.type == 106 && tws_table_ok(e)) {
+      if (e.mapstp < 1) return IMPZ_ERR_ARG;
+      double xm[36];
+      maplinear_tws(P, z, tau, xm, refptcl, zedge, e, sp.charge, sp.mass);
       return push_op(prog, op_xm6(xm));
     }
     return IMPZ_ERR_UNSUPPORTED;

@@ -21,6 +21,16 @@ void maplinear_quad(const Phys& P, double t, double tau, double xm[36], double r
                     double gradient, int mapstp, double chg, double mass);
 void maplinear_rfgap(const Phys& P, double t, double tau, double xm[36], double refpt[6],
                      double zedge, const impz_elem_t& e, double chg, double mass);
+// maplinear_SolRF (type 105): zdat holds read3_Data's Fourier coefficients
+// (ndata values), val[10] the solenoid field Param(12)
+void maplinear_solrf(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                     double zedge, const impz_elem_t& e, double chg, double mass);
+bool solrf_table_ok(const impz_elem_t& e);
+// maplinear_TWS (type 106): zdat holds the two series of read3_Data's
+// coefficients, val[10] the second wave's phase Param(12)
+void maplinear_tws(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                   double zedge, const impz_elem_t& e, double chg, double mass);
+bool tws_table_ok(const impz_elem_t& e);
 
 struct BendState {  // the bend constants AccSimulator.f90:1057-1093 keeps
   bool active;

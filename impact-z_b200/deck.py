@@ -211,6 +211,21 @@ def read_rfdata(path):
     return tab[:, 0].copy(), tab[:, 1].copy(), tab[:, 2].copy(), tab[:, 3].copy()
 
 
+def read_rfcoef(path):
+    """rfdataN.in as Fourier coefficients, read3_Data
+    (src/DataStruct/Data.f90:348-408) for SolRF and TWS: the first value of
+    each line, a zero appended to make the count odd."""
+    vals = []
+    with open(path) as f:
+        for ln in f:
+            v = _values(ln)
+            if v:
+                vals.append(float(v[0]))
+    if len(vals) % 2 == 0:
+        vals.append(0.0)
+    return np.array(vals)
+
+
 def read_wake(path):
     """rfdataN.in as a wake table, read1wk_Data (src/DataStruct/Data.f90:
     559-633): rows (z, longitudinal, x, y wake); z is shifted to start at 0
@@ -410,7 +425,9 @@ def lattice_segments(deck, workdir, skip=(), start=0):
 
     def to_elem(e):
         rf = None
-        if 101 <= e.type <= 106 and e.vals[3] >= 0.0:
+        if e.type in (105, 106) and e.vals[3] >= 0.0:
+            rf = read_rfcoef(os.path.join(workdir, "rfdata%d.in" % int(e.vals[3] + 0.1)))
+        elif 101 <= e.type <= 104 and e.vals[3] >= 0.0:
             rf = read_rfdata(os.path.join(workdir, "rfdata%d.in" % int(e.vals[3])))
         return elem(e.type, e.length, e.nseg, e.mapstp, list(e.vals), rf=rf)
 

@@ -52,10 +52,12 @@ typedef struct impz_bunch_s* impz_bunch_t;
  * Supported types: 0 drift, 1 quadrupole (gradient, or K map when
  * v2 in (-10,-1e-6)), 4 dipole (file ID v3 <= 200: no CSR; above 200 CSR
  * inside the bend, above 500 also downstream: impz_run only), 101..106 RF gaps
- * as the ideal-RF model (v4 < 0), and 101 DTL (with its drift-tube
- * quadrupoles, v6..v9), 102 CCDTL, 103 CCL and 104 SC as the RK6 linear
- * map over the on-axis table zdat/edat/epdat/eppdat (rfdataN.in,
- * read1_Data); 105 SolRF and 106 TWS only as ideal gaps. */
+ * as the ideal-RF model (v4 < 0), and otherwise as RK6 linear maps:
+ * 101 DTL (with its drift-tube quadrupoles, v6..v9), 102 CCDTL, 103 CCL and
+ * 104 SC over the on-axis table zdat/edat/epdat/eppdat (rfdataN.in,
+ * read1_Data); 105 SolRF (solenoid field v11) and 106 TWS (second wave's
+ * phase v11) over read3_Data's Fourier coefficients in zdat (ndata values,
+ * the other table pointers unused). */
 typedef struct {
   int type;
   int nseg;

@@ -74,9 +74,9 @@ void orc_drift_exact(double *pts, int n, double refptcl[6], double tau) {
 /* rk6i_* (Quadrupole.f90:202-252, identical in DriftTube/CCL): 8-stage RK6 */
 typedef void (*orc_rhs)(double t, const double *y, double *f, const void *ctx);
 
-static void rk6i(double h, int ns, double *t, double *y, orc_rhs fn, const void *ctx) {
-  enum { NV = 18 };
-  double yt[NV], a[NV], b[NV], c[NV], d[NV], e[NV], f[NV], g[NV], o[NV], p[NV];
+static void rk6in(double h, int ns, double *t, double *y, int NV, orc_rhs fn,
+                  const void *ctx) {
+  double yt[22], a[22], b[22], c[22], d[22], e[22], f[22], g[22], o[22], p[22];
   double tint = *t, tt;
   int v;
   for (int i = 1; i <= ns; i++) {
@@ -123,6 +123,10 @@ static void rk6i(double h, int ns, double *t, double *y, orc_rhs fn, const void 
                        27.0 * g[v]) + 216.0 * o[v]) + 41.0 * p[v]) / 840.0;
     *t = tint + i * h;
   }
+}
+
+static void rk6i(double h, int ns, double *t, double *y, orc_rhs fn, const void *ctx) {
+  rk6in(h, ns, t, y, 18, fn, ctx);
 }
 
 /* the 18 linear-ODE derivatives shared by intfunc1_* given s11,s33,s55 */
@@ -408,6 +412,286 @@ void orc_maplinear_dtl(double t, double tau, double xm[36], double refpt[6],
   const double q[5] = {length, q1len, q1grad, q2len, q2grad};
   maplinear_rf(t, tau, xm, refpt, zedge, escale, freq, phase_deg, mapstp, chg, mass, ndata, zdat,
                edat, epdat, eppdat, q);
+}
+
+/* ---- SolRF (type 105) linear map ------------------------------------ */
+typedef struct {
+  double zedge, escale, len, ww, theta0, qmcc, b0;
+  int ncoef;
+  const double *F; /* read3_Data's coefficients, 1-based through F[k-1] */
+} solrf_ctx;
+
+/* getaxfldE_SolRF (SolRF.f90:355-466) */
+static void solrf_field(double z, const solrf_ctx *c, double *ez1, double *ezp1) {
+  const double *F = c->F - 1;
+  const double epstol = (double)1.0e-10f;
+  *ez1 = 0.0;
+  *ezp1 = 0.0;
+  if (((z >= c->zedge) && (z <= (c->zedge + c->len))) || (fabs(z - c->zedge) <= epstol) ||
+      (fabs(z - c->zedge - c->len) <= epstol)) {
+    const double zlc = z - c->zedge;
+    const int numpar1 = (int)(F[1] + 0.1);
+    const double zstart1 = F[2], zend1 = F[3], zlength1 = F[4];
+    if (((zlc >= zstart1) && (zlc <= zend1)) || (fabs(zlc - zstart1) <= epstol) ||
+        (fabs(zlc - zend1) <= epstol)) {
+      const double zmid = zlength1 / 2;
+      const double zz = z - c->zedge - zstart1 - zmid;
+      const double zlen = zlength1;
+      const int ntmp = 4;
+      double e = F[ntmp + 1] / 2, ep = 0.0;
+      for (int i = 2; i <= (numpar1 - 1) / 2 + 1; i++) {
+        e = e + F[2 * i - 2 + ntmp] * cos((i - 1) * 2 * PC.Pi * zz / zlen) +
+            F[2 * i - 1 + ntmp] * sin((i - 1) * 2 * PC.Pi * zz / zlen);
+        ep = ep + (i - 1) * 2 * PC.Pi / zlen *
+                      (-F[2 * i - 2 + ntmp] * sin((i - 1) * 2 * PC.Pi * zz / zlen) +
+                       F[2 * i - 1 + ntmp] * cos((i - 1) * 2 * PC.Pi * zz / zlen));
+      }
+      *ez1 = e * c->escale;
+      *ezp1 = ep * c->escale;
+    }
+  }
+}
+
+/* intfunc1_SolRF (SolRF.f90:287-353) */
+static void solrf_rhs(double t, const double *y, double *f, const void *vctx) {
+  const solrf_ctx *c = (const solrf_ctx *)vctx;
+  const double Scxl = PC.Scxl;
+  double ez1, ezp1;
+  solrf_field(t, c, &ez1, &ezp1);
+  f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+  const double gamma0 = -y[5];
+  const double beta0 = sqrt(gamma0 * gamma0 - 1.) / gamma0;
+  const double gbet = sqrt((gamma0 - 1.0) * (gamma0 + 1.0));
+  const double sinphi = sin(c->ww * y[4] + c->theta0);
+  const double cosphi = cos(c->ww * y[4] + c->theta0);
+  const double rfdsgn = ez1 * cosphi;
+  f[4] = 1.0 / (beta0 * Scxl);
+  f[5] = -(c->qmcc * rfdsgn);
+  const double brho = gbet / PC.Clight / c->qmcc;
+  const double q = c->qmcc * rfdsgn / (beta0 * beta0) / (gamma0 * gamma0);
+  const double s11tmp = 0.5 * (1.0 + 0.5 * (gamma0 * gamma0)) * (q * q) +
+                        c->qmcc * 0.5 / ((beta0 * beta0) * beta0) / ((gamma0 * gamma0) * gamma0) *
+                            ez1 * sinphi * c->ww / Scxl;
+  const double sol = 0.5 * c->b0 / brho;
+  const double s11 = (s11tmp + sol * sol / 2) * Scxl;
+  const double s33 = (s11tmp + sol * sol / 2) * Scxl;
+  double s55 = -(1.5 * c->qmcc / (beta0 * beta0) / gamma0 * ezp1 * cosphi) +
+               ((beta0 * beta0) + 0.5) / ((beta0 * beta0) * beta0) / gamma0 * c->qmcc * ez1 *
+                   sinphi * c->ww / Scxl +
+               1.5 * (1.0 - 0.5 * (gamma0 * gamma0)) * (q * q);
+  s55 = Scxl * s55;
+  lin_rhs(y, f, s11, s33, s55);
+  const double c2alpha = -c->b0 / brho / 2;
+  f[18] = -c2alpha * y[20];
+  f[19] = -c2alpha * y[21];
+  f[20] = c2alpha * y[18];
+  f[21] = c2alpha * y[19];
+}
+
+/* maplinear_SolRF (SolRF.f90:126-233): coef = read3_Data's coefficients
+ * (ncoef values), b0 = the solenoid field Param(12) */
+void orc_maplinear_solrf(double t, double tau, double xm[36], double refpt[6], double zedge,
+                         double escale, double freq, double phase_deg, int mapstp, double chg,
+                         double mass, double length, double b0, int ncoef, const double *coef) {
+  const double Scxl = PC.Scxl;
+  solrf_ctx c;
+  double y[22];
+  c.zedge = zedge; c.escale = escale; c.len = length;
+  c.ww = freq / PC.Scfreq;
+  c.theta0 = phase_deg * (double)asinf(1.0f) / 90;
+  c.qmcc = chg / mass;
+  c.b0 = b0;
+  c.ncoef = ncoef;
+  c.F = coef;
+  memset(xm, 0, 36 * sizeof(double));
+  y_init(y, refpt);
+  y[18] = 1.0; y[19] = 0.0; y[20] = 0.0; y[21] = 1.0;
+  const double h = tau / mapstp;
+  double t0 = t;
+  const double gi = -refpt[5];
+  const double betai = sqrt(gi * gi - 1.) / gi;
+  const double ui = gi * betai;
+  const double squi = sqrt(ui);
+  double s = sqrt(ui);
+  const double sqi3 = s * s * s;
+  double ein, e1in;
+  solrf_field(t, &c, &ein, &e1in);
+  const double sinthi = sin(c.ww * refpt[4] + c.theta0);
+  const double costhi = cos(c.ww * refpt[4] + c.theta0);
+  const double uprimi = c.qmcc * ein / betai * costhi;
+  const double qpwi = 0.5 * c.qmcc * Scxl / (ui * c.ww);
+  const double dlti = Scxl * (0.5 * uprimi / ui - qpwi * e1in * sinthi);
+  const double thli = 1.5 * Scxl * (uprimi / ui);
+  rk6in(h, mapstp, &t0, y, 22, solrf_rhs, &c);
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  const double gf = -refpt[5];
+  const double betaf = sqrt(gf * gf - 1.) / gf;
+  const double uf = gf * betaf;
+  const double squf = sqrt(uf);
+  s = sqrt(uf);
+  const double sqf3 = s * s * s;
+  double ef, e1f;
+  solrf_field(t + tau, &c, &ef, &e1f);
+  const double sinthf = sin(c.ww * refpt[4] + c.theta0);
+  const double costhf = cos(c.ww * refpt[4] + c.theta0);
+  const double uprimf = c.qmcc * ef / betaf * costhf;
+  const double qpwf = 0.5 * c.qmcc * Scxl / (uf * c.ww);
+  const double dltf = Scxl * (0.5 * uprimf / uf - qpwf * e1f * sinthf);
+  const double thlf = 1.5 * Scxl * (uprimf / uf);
+  xm_assemble(xm, y, squi, squf, sqi3, sqf3, dlti, dltf, thli, thlf);
+  const double *Y = y - 1;
+#define XM(j, k) xm[((j)-1) + 6 * ((k)-1)]
+  XM(1, 1) = Y[19] * (Y[7] * squi / squf + Y[9] * squi / squf * dlti);
+  XM(2, 1) = Y[19] * ((Y[8] - Y[7] * dltf) * squi * squf + (Y[10] - Y[9] * dltf) * squi * squf *
+                                                                 dlti);
+  XM(1, 2) = Y[19] * Y[9] / (squi * squf);
+  XM(2, 2) = Y[19] * (Y[10] - Y[9] * dltf) * squf / squi;
+  XM(1, 3) = Y[20] * (Y[7] * squi / squf + Y[9] * squi / squf * dlti);
+  XM(2, 3) = Y[20] * ((Y[8] - Y[7] * dltf) * squi * squf + (Y[10] - Y[9] * dltf) * squi * squf *
+                                                                 dlti);
+  XM(1, 4) = Y[20] * Y[9] / (squi * squf);
+  XM(2, 4) = Y[20] * (Y[10] - Y[9] * dltf) * squf / squi;
+  XM(3, 1) = Y[21] * (Y[11] * squi / squf + Y[13] * squi / squf * dlti);
+  XM(4, 1) = Y[21] * ((Y[12] - Y[11] * dltf) * squi * squf +
+                      (Y[14] - Y[13] * dltf) * squi * squf * dlti);
+  XM(3, 2) = Y[21] * Y[13] / (squi * squf);
+  XM(4, 2) = Y[21] * (Y[14] - Y[13] * dltf) * squf / squi;
+  XM(3, 3) = Y[22] * (Y[11] * squi / squf + Y[13] * squi / squf * dlti);
+  XM(4, 3) = Y[22] * ((Y[12] - Y[11] * dltf) * squi * squf +
+                      (Y[14] - Y[13] * dltf) * squi * squf * dlti);
+  XM(3, 4) = Y[22] * Y[13] / (squi * squf);
+  XM(4, 4) = Y[22] * (Y[14] - Y[13] * dltf) * squf / squi;
+#undef XM
+}
+
+/* ---- TWS (type 106) linear map --------------------------------------- */
+typedef struct {
+  double zedge, escale, len, ww, theta0, theta2, qmcc;
+  const double *F;
+} tws_ctx;
+
+/* getaxfldE_TWS (TWS.f90:350-466); its pi is a default-real 2*asin(1.0) */
+static void tws_field(double z, const tws_ctx *c, double *ez1, double *ezp1, double *ez12,
+                      double *ezp12) {
+  const double *F = c->F - 1;
+  const double pi = (double)(2 * asinf(1.0f));
+  const double epstol = (double)1.0e-10f;
+  *ez1 = 0.0; *ezp1 = 0.0; *ez12 = 0.0; *ezp12 = 0.0;
+  if (!(((z >= c->zedge) && (z <= (c->zedge + c->len))) || (fabs(z - c->zedge) <= epstol) ||
+        (fabs(z - c->zedge - c->len) <= epstol)))
+    return;
+  const double zlc = z - c->zedge;
+  const int numpar1 = (int)(F[1] + 0.1);
+  for (int w = 0; w < 2; w++) {
+    const int k0 = w == 0 ? 0 : numpar1 + 4;
+    const int numpar = (int)(F[k0 + 1] + 0.1);
+    const double zstart = F[k0 + 2], zend = F[k0 + 3], zlength = F[k0 + 4];
+    if (!(((zlc >= zstart) && (zlc <= zend)) || (fabs(zlc - zstart) <= epstol) ||
+          (fabs(zlc - zend) <= epstol)))
+      continue;
+    const double zmid = zlength / 2;
+    const double zz = z - c->zedge - zstart - zmid;
+    const double zlen = zlength;
+    const int ntmp = k0 + 4;
+    double e = F[ntmp + 1] / 2, ep = 0.0;
+    for (int i = 2; i <= (numpar - 1) / 2 + 1; i++) {
+      e = e + F[2 * i - 2 + ntmp] * cos((i - 1) * 2 * pi * zz / zlen) +
+          F[2 * i - 1 + ntmp] * sin((i - 1) * 2 * pi * zz / zlen);
+      ep = ep + (i - 1) * 2 * pi / zlen *
+                    (-F[2 * i - 2 + ntmp] * sin((i - 1) * 2 * pi * zz / zlen) +
+                     F[2 * i - 1 + ntmp] * cos((i - 1) * 2 * pi * zz / zlen));
+    }
+    if (w == 0) { *ez1 = e * c->escale; *ezp1 = ep * c->escale; }
+    else { *ez12 = e * c->escale; *ezp12 = ep * c->escale; }
+  }
+}
+
+/* intfunc1_TWS (TWS.f90:231-340) */
+static void tws_rhs(double t, const double *y, double *f, const void *vctx) {
+  const tws_ctx *c = (const tws_ctx *)vctx;
+  const double Scxl = PC.Scxl;
+  double ez1, ezp1, ez12, ezp12;
+  tws_field(t, c, &ez1, &ezp1, &ez12, &ezp12);
+  f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+  const double gamma0 = -y[5];
+  const double beta0 = sqrt(gamma0 * gamma0 - 1.) / gamma0;
+  const double sinphi = sin(c->ww * y[4] + c->theta0);
+  const double cosphi = cos(c->ww * y[4] + c->theta0);
+  const double sinphi2 = sin(c->ww * y[4] + c->theta0 + c->theta2);
+  const double cosphi2 = cos(c->ww * y[4] + c->theta0 + c->theta2);
+  const double rfdsgn = ez1 * cosphi + ez12 * cosphi2;
+  f[4] = 1.0 / (beta0 * Scxl);
+  f[5] = -(c->qmcc * rfdsgn);
+  const double q = c->qmcc * rfdsgn / (beta0 * beta0) / (gamma0 * gamma0);
+  const double s11tmp = 0.5 * (1.0 + 0.5 * (gamma0 * gamma0)) * (q * q) +
+                        c->qmcc * 0.5 / ((beta0 * beta0) * beta0) / ((gamma0 * gamma0) * gamma0) *
+                            (ez1 * sinphi + ez12 * sinphi2) * c->ww / Scxl;
+  double s55 =
+      -(1.5 * c->qmcc / (beta0 * beta0) / gamma0 * (ezp1 * cosphi + ezp12 * cosphi2)) +
+      ((beta0 * beta0) + 0.5) / ((beta0 * beta0) * beta0) / gamma0 * c->qmcc *
+          (ez1 * sinphi + ez12 * sinphi2) * c->ww / Scxl +
+      1.5 * (1.0 - 0.5 * (gamma0 * gamma0)) * (q * q);
+  s55 = Scxl * s55;
+  lin_rhs(y, f, s11tmp * Scxl, s11tmp * Scxl, s55);
+}
+
+/* maplinear_TWS (TWS.f90:129-229): coef = read3_Data's two series,
+ * phase2_deg = Param(12) */
+void orc_maplinear_tws(double t, double tau, double xm[36], double refpt[6], double zedge,
+                       double escale, double freq, double phase_deg, int mapstp, double chg,
+                       double mass, double length, double phase2_deg, int ncoef,
+                       const double *coef) {
+  const double Scxl = PC.Scxl;
+  tws_ctx c;
+  double y[18];
+  (void)ncoef;
+  c.zedge = zedge; c.escale = escale; c.len = length;
+  c.ww = freq / PC.Scfreq;
+  c.theta0 = phase_deg * (double)asinf(1.0f) / 90;
+  c.theta2 = phase2_deg * (double)asinf(1.0f) / 90;
+  c.qmcc = chg / mass;
+  c.F = coef;
+  memset(xm, 0, 36 * sizeof(double));
+  y_init(y, refpt);
+  const double h = tau / mapstp;
+  double t0 = t;
+  const double gi = -refpt[5];
+  const double betai = sqrt(gi * gi - 1.) / gi;
+  const double ui = gi * betai;
+  const double squi = sqrt(ui);
+  double s = sqrt(ui);
+  const double sqi3 = s * s * s;
+  double ein, e1in, ein2, e1in2;
+  tws_field(t, &c, &ein, &e1in, &ein2, &e1in2);
+  const double sinthi = sin(c.ww * refpt[4] + c.theta0);
+  const double costhi = cos(c.ww * refpt[4] + c.theta0);
+  const double sinthi2 = sin(c.ww * refpt[4] + c.theta0 + c.theta2);
+  const double costhi2 = cos(c.ww * refpt[4] + c.theta0 + c.theta2);
+  const double uprimi = c.qmcc * (ein * costhi + ein2 * costhi2) / betai;
+  const double qpwi = 0.5 * c.qmcc * Scxl / (ui * c.ww);
+  const double dlti = Scxl * (0.5 * uprimi / ui - qpwi * (e1in * sinthi + e1in2 * sinthi2));
+  const double thli = 1.5 * Scxl * (uprimi / ui);
+  rk6i(h, mapstp, &t0, y, tws_rhs, &c);
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  const double gf = -refpt[5];
+  const double betaf = sqrt(gf * gf - 1.) / gf;
+  const double uf = gf * betaf;
+  const double squf = sqrt(uf);
+  s = sqrt(uf);
+  const double sqf3 = s * s * s;
+  double ef, e1f, ef2, e1f2;
+  tws_field(t + tau, &c, &ef, &e1f, &ef2, &e1f2);
+  const double sinthf = sin(c.ww * refpt[4] + c.theta0);
+  const double costhf = cos(c.ww * refpt[4] + c.theta0);
+  const double sinthf2 = sin(c.ww * refpt[4] + c.theta0 + c.theta2);
+  const double costhf2 = cos(c.ww * refpt[4] + c.theta0 + c.theta2);
+  const double uprimf = c.qmcc * (ef * costhf + ef2 * costhf2) / betaf;
+  const double qpwf = 0.5 * c.qmcc * Scxl / (uf * c.ww);
+  const double dltf = Scxl * (0.5 * uprimf / uf - qpwf * (e1f * sinthf + e1f2 * sinthf2));
+  const double thlf = 1.5 * Scxl * (uprimf / uf);
+  xm_assemble(xm, y, squi, squf, sqi3, sqf3, dlti, dltf, thli, thlf);
 }
 
 /* 6x6 loop of drift1_BeamBunch (BeamBunch.f90:310-320) */
@@ -1866,6 +2150,18 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
           if (e->val[3] < 0.0) {
             orc_ideal_rf(beam->pts, beam->nlocal, beam->refptcl, beam->mass, tau1,
                          e->val[0], e->val[1], e->val[2], j, bnseg, ihlf);
+          } else if (bitype == 105 && e->ndata >= 5) {
+            double xm[36];
+            orc_maplinear_solrf(z, tau1, xm, beam->refptcl, zedge, e->val[0], e->val[1],
+                                e->val[2], e->mapstp, beam->charge, beam->mass, blength,
+                                e->val[10], e->ndata, e->zdat);
+            orc_apply_xm(beam->pts, beam->nlocal, xm);
+          } else if (bitype == 106 && e->ndata >= 9) {
+            double xm[36];
+            orc_maplinear_tws(z, tau1, xm, beam->refptcl, zedge, e->val[0], e->val[1], e->val[2],
+                              e->mapstp, beam->charge, beam->mass, blength, e->val[10],
+                              e->ndata, e->zdat);
+            orc_apply_xm(beam->pts, beam->nlocal, xm);
           } else if (bitype <= 104 && e->ndata > 1) {
             /* DTL, CCDTL, CCL, SC linear maps (maplinear_BeamLineElem,
              * BeamLineElem.f90:776-800) */

@@ -45,6 +45,13 @@ void orc_maplinear_quad(double t, double tau, double xm[36], double refpt[6],
 void orc_maplinear_drift(double t, double tau, double xm[36], double refpt[6],
                          int mapstp, double chg, double mass);
 /* maplinear_CCL with on-axis table (CCL.f90:122-365); zdat shifted to start at 0 */
+void orc_maplinear_solrf(double t, double tau, double xm[36], double refpt[6], double zedge,
+                         double escale, double freq, double phase_deg, int mapstp, double chg,
+                         double mass, double length, double b0, int ncoef, const double *coef);
+void orc_maplinear_tws(double t, double tau, double xm[36], double refpt[6], double zedge,
+                       double escale, double freq, double phase_deg, int mapstp, double chg,
+                       double mass, double length, double phase2_deg, int ncoef,
+                       const double *coef);
 void orc_maplinear_dtl(double t, double tau, double xm[36], double refpt[6],
                        double zedge, double escale, double freq, double phase_deg,
                        int mapstp, double chg, double mass,

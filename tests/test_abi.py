@@ -142,3 +142,65 @@ def test_dtl_ccdtl_sc_linear_maps_match_oracle_bitwise(etype):
                                  0.01, 0.025, ref, charge, mass, freq)
         assert abs(xm_d[1, 0] - xm_c[1, 0]) > 1e-3 * abs(xm_c[1, 0]) + 1e-9
         assert abs(xm_d[3, 2] - xm_c[3, 2]) > 1e-3 * abs(xm_c[3, 2]) + 1e-9
+
+
+def solrf_coefficients(length=0.2):
+    """read3_Data's layout: count, start, end, period, then the constant,
+    cosine and sine terms of a cavity-like Ez."""
+    terms = [0.4, 0.8, 0.0, -0.3, 0.05, 0.1, 0.02]
+    return np.array([len(terms), 0.0, length, length] + terms)
+
+
+def test_solrf_linear_map_matches_oracle_bitwise():
+    """maplinear_SolRF (SolRF.f90:126-353): the Fourier on-axis field and a
+    0.2 T solenoid whose rotation couples x and y."""
+    freq, mass, charge = 402.5e6, beams.PROTON_MASS_EV, 1.0
+    ref = beams.refptcl_for(2.5e6, mass)
+    coef = solrf_coefficients()
+    vals = [1e6, 402.5e6, -30.0, 1.0, 0.01, 0, 0, 0, 0, 0, 0.2]
+    e = impz.elem(105, 0.2, 4, 5, vals, rf=coef)
+    orc.physconst(freq)
+    for t in (0.0, 0.07, 0.175):
+        xm_p, ref_p = impz.maplinear(e, 0.0, t, 0.025, ref, charge, mass, freq)
+        xm_o, ref_o = np.zeros(36), ref.copy()
+        orc.lib().orc_maplinear_solrf(t, 0.025, orc.dp(xm_o), orc.dp(ref_o), 0.0, 1e6, 402.5e6,
+                                      -30.0, 5, charge, mass, 0.2, 0.2, len(coef), orc.dp(coef))
+        np.testing.assert_array_equal(xm_p, xm_o.reshape(6, 6, order="F"))
+        np.testing.assert_array_equal(ref_p, ref_o)
+    assert abs(xm_p[0, 2]) > 1e-6 and abs(xm_p[2, 0]) > 1e-6  # the solenoid couples x, y
+    assert abs(ref_p[5] - ref[5]) > 1e-7  # and the gap changes the energy
+
+
+def tws_coefficients(length=0.2):
+    """Two series (read3_Data's layout for TWS): a standing wave over the
+    element and a second one over its middle."""
+    s1 = [0.3, 0.9, 0.1, -0.2, 0.05]
+    s2 = [0.2, 0.5, -0.4, 0.1, 0.0, 0.02, 0.03]
+    return np.array([len(s1), 0.0, length, length] + s1 +
+                    [len(s2), 0.05, 0.15, 0.1] + s2)
+
+
+def test_tws_linear_map_matches_oracle_bitwise():
+    """maplinear_TWS (TWS.f90:129-466): two standing waves, the second 90
+    degrees later and only over the middle of the element."""
+    freq, mass, charge = 402.5e6, beams.PROTON_MASS_EV, 1.0
+    ref = beams.refptcl_for(2.5e6, mass)
+    coef = tws_coefficients()
+    vals = [1e6, 402.5e6, -30.0, 1.0, 0.01, 0, 0, 0, 0, 0, 90.0]
+    e = impz.elem(106, 0.2, 4, 5, vals, rf=coef)
+    orc.physconst(freq)
+    outs = []
+    for t in (0.0, 0.06, 0.175):
+        xm_p, ref_p = impz.maplinear(e, 0.0, t, 0.025, ref, charge, mass, freq)
+        xm_o, ref_o = np.zeros(36), ref.copy()
+        orc.lib().orc_maplinear_tws(t, 0.025, orc.dp(xm_o), orc.dp(ref_o), 0.0, 1e6, 402.5e6,
+                                    -30.0, 5, charge, mass, 0.2, 90.0, len(coef), orc.dp(coef))
+        np.testing.assert_array_equal(xm_p, xm_o.reshape(6, 6, order="F"))
+        np.testing.assert_array_equal(ref_p, ref_o)
+        outs.append(xm_p)
+    # the second wave acts in the middle: a zero second series changes it there
+    c0 = coef.copy()
+    c0[14:] = 0.0
+    xm_1, _ = impz.maplinear(impz.elem(106, 0.2, 4, 5, vals, rf=c0), 0.0, 0.06, 0.025, ref,
+                             charge, mass, freq)
+    assert abs(xm_1[1, 0] - outs[1][1, 0]) > 1e-6 * abs(outs[1][1, 0])
