@@ -1194,7 +1194,10 @@ int impz_maplinear(const impz_elem_t* e, double zedge, double t, double tau, dou
   const Phys P = make_phys(freq);
   if (e->type == 1) {
     if (e->mapstp < 1) return IMPZ_ERR_ARG;
-    maplinear_quad(P, t, tau, xm, refpt, e->val[0], e->mapstp, charge, mass);
+    const bool fringe = e->val[1] > 1.0e-5;
+    if (fringe && !(e->ndata > 1 && e->zdat && e->edat)) return IMPZ_ERR_UNSUPPORTED;
+    maplinear_quad(P, t, tau, xm, refpt, e->val[0], e->mapstp, charge, mass,
+                   fringe ? e : nullptr, zedge);
     return IMPZ_OK;
   }
   if (e->type >= 101 && e->type <= 104 && e->ndata > 1) {

@@ -135,15 +135,35 @@ void uvals(double g, double& u, double& squ, double& sq3) {
 }  // namespace
 
 void maplinear_quad(const Phys& P, double t, double tau, double xm[36], double refpt[6],
-                    double gradient, int mapstp, double chg, double mass) {
-  // maplinear_Quadrupole (Quadrupole.f90:120-200), intfunc1 (254-305)
+                    double gradient, int mapstp, double chg, double mass,
+                    const impz_elem_t* fringe, double zedge) {
+  // maplinear_Quadrupole (Quadrupole.f90:120-200), intfunc1 (254-305); a
+  // fringe-field quadrupole takes its gradient from the profile table
+  // (getfldfrg_Quadrupole, Quadrupole.f90:404-430: bisection and linear
+  // interpolation at t - zedge)
+  auto grad_at = [&](double tt) {
+    if (!fringe) return gradient;
+    const double zz = tt - zedge;
+    const double* zd = fringe->zdat - 1;
+    const double* gd = fringe->edat - 1;
+    int klo = 1, khi = fringe->ndata;
+    while (khi - klo > 1) {
+      const int k = (khi + klo) / 2;
+      if (zd[k] > zz) khi = k;
+      else klo = k;
+    }
+    const double hstep = zd[khi] - zd[klo];
+    const double slope = (gd[khi] - gd[klo]) / hstep;
+    return gd[klo] + slope * (zz - zd[klo]);
+  };
   double y[NV];
   y_start(y, refpt);
   const double h = tau / mapstp;
   double ui, squi, sqi3, uf, squf, sqf3;
   uvals(-refpt[5], ui, squi, sqi3);
   const double qmcc = chg / mass;
-  rk6(h, mapstp, t, y, [&](double, const double* yy, double* f) {
+  rk6(h, mapstp, t, y, [&](double tt, const double* yy, double* f) {
+    const double bgrad = grad_at(tt);
     f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
     const double gamma0 = -yy[5];
     const double beta0 = std::sqrt(gamma0 * gamma0 - 1.) / gamma0;
@@ -151,8 +171,8 @@ void maplinear_quad(const Phys& P, double t, double tau, double xm[36], double r
     f[4] = 1.0 / (beta0 * P.Scxl);
     f[5] = 0.0;
     const double brho = gbet / P.Clight / qmcc;
-    const double s11 = gradient / brho * P.Scxl;
-    const double s33 = -(gradient / brho * P.Scxl);
+    const double s11 = bgrad / brho * P.Scxl;
+    const double s33 = -(bgrad / brho * P.Scxl);
     lin_rhs(P.Scxl, yy, f, s11, s33, 0.0);
   });
   refpt[4] = y[4];
@@ -614,10 +634,13 @@ int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, do
       refptcl[4] = refptcl[4] + tau / beta0 / Scxl;
       return push_op(prog, op);
     }
-    if (x3 > 1.0e-5) return IMPZ_ERR_UNSUPPORTED;  // fringe-field table
+    // a gradient profile (read1_Data, AccSimulator.f90:853-863) when v2 > 1e-5
+    const bool fringe = x3 > 1.0e-5;
+    if (fringe && !(e.ndata > 1 && e.zdat && e.edat)) return IMPZ_ERR_UNSUPPORTED;
     if (e.mapstp < 1) return IMPZ_ERR_ARG;
     double xm[36];
-    maplinear_quad(P, z, tau, xm, refptcl, e.val[0], e.mapstp, sp.charge, sp.mass);
+    maplinear_quad(P, z, tau, xm, refptcl, e.val[0], e.mapstp, sp.charge, sp.mass,
+                   fringe ? &e : nullptr, zedge);
     return push_op(prog, op_xm6(xm));
   }
   if (e.type >= 101 && e.type <= 106) {

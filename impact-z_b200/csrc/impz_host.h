@@ -18,7 +18,8 @@ Phys make_phys(double freq);
 // 101..104; RK6 of the 18-variable linear ODE); refpt(5), refpt(6) advance
 // like the reference.
 void maplinear_quad(const Phys& P, double t, double tau, double xm[36], double refpt[6],
-                    double gradient, int mapstp, double chg, double mass);
+                    double gradient, int mapstp, double chg, double mass,
+                    const impz_elem_t* fringe = nullptr, double zedge = 0.0);
 void maplinear_rfgap(const Phys& P, double t, double tau, double xm[36], double refpt[6],
                      double zedge, const impz_elem_t& e, double chg, double mass);
 // maplinear_SolRF (type 105): zdat holds read3_Data's Fourier coefficients

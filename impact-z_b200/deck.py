@@ -429,6 +429,9 @@ def lattice_segments(deck, workdir, skip=(), start=0):
             rf = read_rfcoef(os.path.join(workdir, "rfdata%d.in" % int(e.vals[3] + 0.1)))
         elif 101 <= e.type <= 104 and e.vals[3] >= 0.0:
             rf = read_rfdata(os.path.join(workdir, "rfdata%d.in" % int(e.vals[3])))
+        elif e.type == 1 and e.vals[1] > 1.0e-5:
+            # a quadrupole's gradient profile (AccSimulator.f90:853-863)
+            rf = read_rfdata(os.path.join(workdir, "rfdata%d.in" % int(e.vals[1] + 0.1)))
         return elem(e.type, e.length, e.nseg, e.mapstp, list(e.vals), rf=rf)
 
     seg, skipped = [], []

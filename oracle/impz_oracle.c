@@ -146,13 +146,34 @@ static void lin_rhs(const double *y, double *f, double s11, double s33, double s
   f[17] = -s55 * y[16];
 }
 
-typedef struct { double bgrad, qmcc; } quad_ctx;
+typedef struct {
+  double bgrad, qmcc;
+  /* fringe-field profile (Param(3) > 1e-5): the gradient table of
+   * read1_Data, looked up at t - zedge by getfldfrg_Quadrupole */
+  int ndata;
+  const double *zdat, *gdat;
+  double zedge;
+} quad_ctx;
 
-/* intfunc1_Quadrupole (Quadrupole.f90:254-305), constant gradient */
+/* getfldfrg_Quadrupole (Quadrupole.f90:404-430): bisection + linear
+ * interpolation of the gradient table */
+static double quad_fringe(double zz, const quad_ctx *q) {
+  const double *zd = q->zdat - 1, *gd = q->gdat - 1;
+  int klo = 1, khi = q->ndata;
+  while (khi - klo > 1) {
+    const int k = (khi + klo) / 2;
+    if (zd[k] > zz) khi = k; else klo = k;
+  }
+  const double hstep = zd[khi] - zd[klo];
+  const double slope = (gd[khi] - gd[klo]) / hstep;
+  return gd[klo] + slope * (zz - zd[klo]);
+}
+
+/* intfunc1_Quadrupole (Quadrupole.f90:254-305) */
 static void quad_rhs(double t, const double *y, double *f, const void *vctx) {
-  (void)t;
   const quad_ctx *q = (const quad_ctx *)vctx;
   double gamma0, beta0, gbet, brho, s11, s33, s55;
+  const double bgrad = q->ndata > 1 ? quad_fringe(t - q->zedge, q) : q->bgrad;
   f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
   gamma0 = -y[5];
   beta0 = sqrt(gamma0 * gamma0 - 1.) / gamma0;
@@ -160,8 +181,8 @@ static void quad_rhs(double t, const double *y, double *f, const void *vctx) {
   f[4] = 1.0 / (beta0 * PC.Scxl);
   f[5] = 0.0;
   brho = gbet / PC.Clight / q->qmcc;
-  s11 = q->bgrad / brho * PC.Scxl;
-  s33 = -(q->bgrad / brho * PC.Scxl);
+  s11 = bgrad / brho * PC.Scxl;
+  s33 = -(bgrad / brho * PC.Scxl);
   s55 = 0.0;
   lin_rhs(y, f, s11, s33, s55);
 }
@@ -206,10 +227,10 @@ static void xm_assemble(double xm[36], const double *y, double squi, double squf
 }
 
 /* maplinear_Quadrupole (Quadrupole.f90:120-200) */
-void orc_maplinear_quad(double t, double tau, double xm[36], double refpt[6],
-                        double gradient, int mapstp, double chg, double mass) {
+static void maplinear_quad(double t, double tau, double xm[36], double refpt[6],
+                           const quad_ctx *qc, int mapstp) {
   double y[18], h, t0, gi, betai, ui, squi, sqi3, gf, betaf, uf, squf, sqf3, s;
-  quad_ctx q = {gradient, chg / mass};
+  const quad_ctx q = *qc;
   memset(xm, 0, 36 * sizeof(double));
   y_init(y, refpt);
   h = tau / mapstp;
@@ -257,6 +278,20 @@ void orc_maplinear_drift(double t, double tau, double xm[36], double refpt[6],
   s = sqrt(uf);
   sqf3 = s * s * s;
   xm_assemble(xm, y, squi, squf, sqi3, sqf3, 0.0, 0.0, 0.0, 0.0);
+}
+
+void orc_maplinear_quad(double t, double tau, double xm[36], double refpt[6],
+                        double gradient, int mapstp, double chg, double mass) {
+  const quad_ctx q = {gradient, chg / mass, 0, NULL, NULL, 0.0};
+  maplinear_quad(t, tau, xm, refpt, &q, mapstp);
+}
+
+/* the fringe-field quadrupole: gradient profile (z from 0, G) at zedge */
+void orc_maplinear_quad_fringe(double t, double tau, double xm[36], double refpt[6],
+                               double zedge, int mapstp, double chg, double mass, int ndata,
+                               const double *zdat, const double *gdat) {
+  const quad_ctx q = {0.0, chg / mass, ndata, zdat, gdat, zedge};
+  maplinear_quad(t, tau, xm, refpt, &q, mapstp);
 }
 
 /* ---- CCL linear gap ---------------------------------------------------- */
@@ -2136,8 +2171,12 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
           if (x3 < -1.0e-6) {
             orc_transfmapK(tau1, e->val[0], beam->refptcl, beam->pts, beam->nlocal, qm0);
           } else if (x3 > 1.0e-5) {
-            free(rho);
-            return -7; /* fringe-field table: out of scope */
+            /* the gradient profile of read1_Data (AccSimulator.f90:853-863) */
+            if (e->ndata < 2) { free(rho); return -7; }
+            double xm[36];
+            orc_maplinear_quad_fringe(z, tau1, xm, beam->refptcl, zedge, e->mapstp,
+                                      beam->charge, beam->mass, e->ndata, e->zdat, e->edat);
+            orc_apply_xm(beam->pts, beam->nlocal, xm);
           } else {
             double xm[36];
             orc_maplinear_quad(z, tau1, xm, beam->refptcl, e->val[0], e->mapstp,

@@ -52,6 +52,9 @@ void orc_maplinear_tws(double t, double tau, double xm[36], double refpt[6], dou
                        double escale, double freq, double phase_deg, int mapstp, double chg,
                        double mass, double length, double phase2_deg, int ncoef,
                        const double *coef);
+void orc_maplinear_quad_fringe(double t, double tau, double xm[36], double refpt[6],
+                               double zedge, int mapstp, double chg, double mass, int ndata,
+                               const double *zdat, const double *gdat);
 void orc_maplinear_dtl(double t, double tau, double xm[36], double refpt[6],
                        double zedge, double escale, double freq, double phase_deg,
                        int mapstp, double chg, double mass,

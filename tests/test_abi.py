@@ -204,3 +204,34 @@ def test_tws_linear_map_matches_oracle_bitwise():
     xm_1, _ = impz.maplinear(impz.elem(106, 0.2, 4, 5, vals, rf=c0), 0.0, 0.06, 0.025, ref,
                              charge, mass, freq)
     assert abs(xm_1[1, 0] - outs[1][1, 0]) > 1e-6 * abs(outs[1][1, 0])
+
+
+def quad_profile(length=0.1, g=20.0, n=51):
+    """A gradient profile with soft edges (Enge-like tanh), z from 0."""
+    z = np.linspace(0.0, length, n)
+    prof = g * 0.25 * (1 + np.tanh((z - 0.015) / 0.005)) * (1 + np.tanh((length - 0.015 - z) /
+                                                                          0.005))
+    return z, prof, np.zeros(n), np.zeros(n)
+
+
+def test_fringe_field_quadrupole_map_matches_oracle_bitwise():
+    """maplinear_Quadrupole with a gradient profile (file ID v2 > 1e-5,
+    getfldfrg_Quadrupole): host = oracle bitwise, and the soft edges make
+    it weaker than the hard-edge quadrupole of the peak gradient."""
+    freq, mass, charge = 402.5e6, beams.PROTON_MASS_EV, 1.0
+    ref = beams.refptcl_for(2.5e6, mass)
+    z, g, z0, z1 = quad_profile()
+    e = impz.elem(1, 0.1, 4, 5, [20.0, 7.0, 1.0], rf=(z, g, z0, z1))
+    orc.physconst(freq)
+    for t in (0.0, 0.0125, 0.05):
+        xm_p, ref_p = impz.maplinear(e, 0.0, t, 0.0125, ref, charge, mass, freq)
+        xm_o, ref_o = np.zeros(36), ref.copy()
+        orc.lib().orc_maplinear_quad_fringe(t, 0.0125, orc.dp(xm_o), orc.dp(ref_o), 0.0, 5,
+                                            charge, mass, len(z), orc.dp(np.ascontiguousarray(z)),
+                                            orc.dp(np.ascontiguousarray(g)))
+        np.testing.assert_array_equal(xm_p, xm_o.reshape(6, 6, order="F"))
+        np.testing.assert_array_equal(ref_p, ref_o)
+    hard, _ = impz.maplinear(impz.elem(1, 0.1, 4, 5, [20.0, 0.0, 1.0]), 0.0, 0.0, 0.0125, ref,
+                             charge, mass, freq)
+    soft, _ = impz.maplinear(e, 0.0, 0.0, 0.0125, ref, charge, mass, freq)
+    assert abs(soft[1, 0]) < abs(hard[1, 0])
