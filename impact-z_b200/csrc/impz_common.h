@@ -27,6 +27,7 @@ enum MapKind : int {
   MAP_BPOL = 6,      // Bpol_Dipole (Dipole.f90:528-591)
   MAP_SECTOR = 7,    // Sector_Dipole (Dipole.f90:693-788)
   MAP_XM2 = 8,       // 6x6 map with only its three 2x2 diagonal blocks nonzero
+  MAP_UNDUL = 9,     // transfUndulator_Quadrupole (Quadrupole.f90:611-665)
 };
 
 struct MapOp {

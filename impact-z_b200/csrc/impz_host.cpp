@@ -622,7 +622,23 @@ int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, do
   }
   if (e.type == 1) {
     const double x3 = e.val[1];
-    if (x3 < -10.0) return IMPZ_ERR_UNSUPPORTED;  // undulator map
+    if (x3 < -10.0) {
+      // transfUndulator_Quadrupole (Quadrupole.f90:611-665); kqlh = Param(2)
+      const double beta0 = std::sqrt(1.0 - 1.0 / (refptcl[5] * refptcl[5]));
+      const double kqlh = e.val[0];
+      const double argh = tau * std::sqrt(kqlh);
+      const double argh2 = argh * argh, argh4 = argh2 * argh2, argh6 = argh4 * argh2;
+      const double sincargh = 1 - argh2 / 6 + argh4 / 120 - argh6 / 5040;
+      MapOp op = blank(MAP_UNDUL);
+      op.c[0] = refptcl[5]; op.c[1] = beta0; op.c[2] = tau; op.c[3] = Scxl;
+      op.c[4] = 1.0; op.c[5] = tau; op.c[6] = 0.0; op.c[7] = 1.0;
+      op.c[8] = std::cos(tau * std::sqrt(kqlh));
+      op.c[9] = tau * sincargh;
+      op.c[10] = -std::sin(tau * std::sqrt(kqlh)) * std::sqrt(kqlh);
+      op.c[11] = std::cos(tau * std::sqrt(kqlh));
+      refptcl[4] = refptcl[4] + tau / beta0 / Scxl;
+      return push_op(prog, op);
+    }
     if (x3 < -1.0e-6) {
       // transfmapK_Quadrupole (Quadrupole.f90:509-607)
       const double gambet0 = std::sqrt(refptcl[5] * refptcl[5] - 1.0);

@@ -137,6 +137,24 @@ __device__ __forceinline__ void map_kquad(Particle& p, const volatile double* c)
   p.x = t1; p.px = t2; p.y = t3; p.py = t4; p.ph = t5;
 }
 
+// transfUndulator_Quadrupole (Quadrupole.f90:611-665): free in x, the
+// undulator's natural focusing in y; c = {refpt6, beta0, tau, Scxl, xm11,
+// xm12, xm21, xm22, xm33, xm34, xm43, xm44}
+__device__ __forceinline__ void map_undul(Particle& p, const volatile double* c) {
+  const double refpt6 = c[0], beta0 = c[1], tau = c[2], Scxl = c[3];
+  const double xm11 = c[4], xm12 = c[5], xm21 = c[6], xm22 = c[7];
+  const double xm33 = c[8], xm34 = c[9], xm43 = c[10], xm44 = c[11];
+  const double gam = -refpt6 - p.pt;
+  const double gambetz = sqrt(((gam * gam - 1.0) - p.px * p.px) - p.py * p.py);
+  const double betaz = gambetz / gam;
+  const double t1 = xm11 * p.x + xm12 * p.px / gambetz / Scxl;
+  const double t2 = gambetz * Scxl * xm21 * p.x + xm22 * p.px;
+  const double t3 = xm33 * p.y + xm34 * p.py / gambetz / Scxl;
+  const double t4 = gambetz * Scxl * xm43 * p.y + xm44 * p.py;
+  const double t5 = p.ph + (1.0 / betaz - 1.0 / beta0) * tau / Scxl;
+  p.x = t1; p.px = t2; p.y = t3; p.py = t4; p.ph = t5;
+}
+
 __device__ __forceinline__ void map_idealrf(Particle& p, const volatile double* c, int flags,
                                             int twonseg) {
   // BeamBunch.f90:337-438; c = {vtmp, harm, phi0lc, Scxl, tau, gam0_in,
@@ -292,6 +310,7 @@ __device__ __forceinline__ void apply_program(Particle& p, const volatile MapPro
       case MAP_BPOL: map_pole<true>(p, op.c); break;
       case MAP_SECTOR: map_sector(p, op.c); break;
       case MAP_XM2: map_xm2(p, op.c); break;
+      case MAP_UNDUL: map_undul(p, op.c); break;
       default: break;
     }
   }

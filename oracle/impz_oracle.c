@@ -744,6 +744,33 @@ void orc_apply_xm(double *pts, int n, const double xm[36]) {
 }
 
 /* transfmapK_Quadrupole (Quadrupole.f90:509-607) */
+/* transfUndulator_Quadrupole (Quadrupole.f90:611-665), kqlh = Param(2) */
+void orc_undulator(double tau, double kqlh, double refpt[6], double *pts, int n) {
+  const double Scxl = PC.Scxl;
+  const double beta0 = sqrt(1.0 - 1.0 / (refpt[5] * refpt[5]));
+  const double argh = tau * sqrt(kqlh);
+  const double argh2 = argh * argh, argh4 = argh2 * argh2, argh6 = argh4 * argh2;
+  const double sincargh = 1 - argh2 / 6 + argh4 / 120 - argh6 / 5040;
+  const double r34h = tau * sincargh;
+  const double xm11 = 1.0, xm12 = tau, xm21 = 0.0, xm22 = 1.0;
+  const double xm33 = cos(tau * sqrt(kqlh));
+  const double xm34 = r34h;
+  const double xm43 = -sin(tau * sqrt(kqlh)) * sqrt(kqlh);
+  const double xm44 = cos(tau * sqrt(kqlh));
+  for (int i = 0; i < n; i++) {
+    const double gam = -refpt[5] - P(i, 5);
+    const double gambetz = sqrt(gam * gam - 1.0 - P(i, 1) * P(i, 1) - P(i, 3) * P(i, 3));
+    const double betaz = gambetz / gam;
+    const double t1 = xm11 * P(i, 0) + xm12 * P(i, 1) / gambetz / Scxl;
+    const double t2 = gambetz * Scxl * xm21 * P(i, 0) + xm22 * P(i, 1);
+    const double t3 = xm33 * P(i, 2) + xm34 * P(i, 3) / gambetz / Scxl;
+    const double t4 = gambetz * Scxl * xm43 * P(i, 2) + xm44 * P(i, 3);
+    const double t5 = P(i, 4) + (1.0 / betaz - 1.0 / beta0) * tau / Scxl;
+    P(i, 0) = t1; P(i, 1) = t2; P(i, 2) = t3; P(i, 3) = t4; P(i, 4) = t5;
+  }
+  refpt[4] = refpt[4] + tau / beta0 / Scxl;
+}
+
 void orc_transfmapK(double tau, double kquad, double refpt[6], double *pts, int n,
                     double qmass) {
   const double Scxl = PC.Scxl;
@@ -2167,8 +2194,9 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
           ihlf++;
         } else if (bitype == 1) {
           double x3 = e->val[1];
-          if (x3 < -10.0) { free(rho); return -6; } /* undulator: out of scope */
-          if (x3 < -1.0e-6) {
+          if (x3 < -10.0) {
+            orc_undulator(tau1, e->val[0], beam->refptcl, beam->pts, beam->nlocal);
+          } else if (x3 < -1.0e-6) {
             orc_transfmapK(tau1, e->val[0], beam->refptcl, beam->pts, beam->nlocal, qm0);
           } else if (x3 > 1.0e-5) {
             /* the gradient profile of read1_Data (AccSimulator.f90:853-863) */

@@ -87,6 +87,7 @@ def lib():
             "orc_maplinear_quad_fringe": (v, [ctypes.c_double, ctypes.c_double, _D, _D,
                                               ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                               ctypes.c_double, ctypes.c_int, _D, _D]),
+            "orc_undulator": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_int]),
             "orc_apply_xm": (v, [_D, ctypes.c_int, _D]),
             "orc_transfmapK": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_int,
                                    ctypes.c_double]),
