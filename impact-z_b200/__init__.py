@@ -79,6 +79,8 @@ _SIGS = {
     "impz_bunch_info": (ctypes.c_int, [_B, _D]),
     "impz_bunch_geom": (ctypes.c_int, [_B, _D, _D]),
     "impz_laser_heater": (ctypes.c_int, [_B, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+    "impz_autotune": (ctypes.c_int, [_B, ctypes.c_int, _D]),
+    "impz_step_params_size": (ctypes.c_int, []),
     "impz_bunch_set_z": (ctypes.c_int, [_B, ctypes.c_double]),
     "impz_bunch_stream": (ctypes.c_void_p, [_B]),
     "impz_map_half": (ctypes.c_int, [_B, _E, ctypes.c_double, _D, ctypes.c_double, ctypes.c_int,
@@ -315,6 +317,14 @@ class Bunch:
         rng, ms = np.zeros(6), np.zeros(3)
         _check(lib().impz_bunch_geom(self.h, _dp(rng), _dp(ms)), "impz_bunch_geom")
         return rng, ms
+
+    def autotune(self, nsteps=8):
+        """Picks deposit and push blocks and the z convolution's lines per
+        block by timing this bunch; the bunch is left as it was."""
+        out = np.zeros(4)
+        _check(lib().impz_autotune(self.h, int(nsteps), _dp(out)), "impz_autotune")
+        return {"deposit_blocks": int(out[0]), "push_blocks": int(out[1]),
+                "z_lines": int(out[2]), "ms_per_step": float(out[3])}
 
     def laser_heater(self, rsig, wavelength, ez):
         """The energy kick of a type -52 laser heater element."""

@@ -270,6 +270,7 @@ struct impz_bunch_s {
   double* mom_out = nullptr;
   double* mom_fine = nullptr;
   int grid_adv = 0, grid_dep = 0;
+  int ztile = 0;  // z lines per block of the z convolution (0: the largest that fits)
   BendState bend;
   int stage = ST_IDLE;
   double sc_gam = 0, sc_rad = 0;
@@ -353,6 +354,7 @@ PoissonBuffers poisson_of(impz_bunch_t b) {
   const bool wake = b->run_wake;
   pb.wake = wake ? b->wk_field : nullptr;
   pb.wake_line = wake ? b->wk_line : nullptr;
+  pb.ztile = b->ztile;
   return pb;
 }
 
@@ -1513,6 +1515,133 @@ int impz_run_reference(impz_bunch_t b, double* refrec, int maxrec, int* nrec) {
   if (refrec && ncopy > 0)
     std::memcpy(refrec, b->lat.refrec.data(), (size_t)6 * ncopy * sizeof(double));
   if (nrec) *nrec = rows;
+  return IMPZ_OK;
+}
+
+// ---- autotuner ------------------------------------------------------------
+// Times real runs of the bunch (nsteps space-charge steps of a short drift)
+// under candidate launch shapes: deposit and push blocks, and z lines per
+// block of the convolution; one parameter at a time, keeping the best.
+// The bunch is restored before each trial and at the end.
+int impz_step_params_size(void) { return (int)sizeof(StepParams); }
+
+static void drop_graphs(impz_bunch_t b) {
+  cudaStreamSynchronize(b->stream);
+  for (int p = 0; p < 2; p++)
+    if (b->gexec[p]) {
+      cudaGraphExecDestroy(b->gexec[p]);
+      b->gexec[p] = nullptr;
+    }
+}
+
+int impz_autotune(impz_bunch_t b, int nsteps, double out[4]) {
+  if (!b || nsteps < 2 || nsteps > 64 || !out) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  DevState hs;
+  CK(cudaMemcpy(&hs, b->st, sizeof(hs), cudaMemcpyDeviceToHost));
+  const long long n = hs.nlocal;
+  if (n < 1) return IMPZ_ERR_STATE;
+  // snapshot of the bunch
+  const int ncol = b->ids[0] ? 7 : 6;
+  char* snap = nullptr;
+  const size_t col_bytes = (size_t)n * sizeof(double);
+  cudaError_t ce = cudaMalloc(&snap, ncol * col_bytes);
+  if (ce != cudaSuccess) return ce == cudaErrorMemoryAllocation ? IMPZ_ERR_NOMEM : cuda_fail(ce, "cudaMalloc");
+  const int par0 = b->parity;
+  for (int c = 0; c < 6; c++)
+    CK(cudaMemcpy(snap + c * col_bytes, b->pbuf[par0][c], col_bytes, cudaMemcpyDeviceToDevice));
+  if (ncol == 7) CK(cudaMemcpy(snap + 6 * col_bytes, b->ids[par0], col_bytes, cudaMemcpyDeviceToDevice));
+  double ref0[6];
+  std::memcpy(ref0, b->refptcl, sizeof(ref0));
+  const double z0 = b->z;
+  const LoopState loop0 = b->csr;
+  auto restore = [&]() -> int {
+    drop_graphs(b);
+    b->parity = par0;
+    for (int c = 0; c < 6; c++)
+      CK(cudaMemcpy(b->pbuf[par0][c], snap + c * col_bytes, col_bytes, cudaMemcpyDeviceToDevice));
+    if (ncol == 7) CK(cudaMemcpy(b->ids[par0], snap + 6 * col_bytes, col_bytes, cudaMemcpyDeviceToDevice));
+    CK(cudaMemcpy(b->st, &hs, sizeof(hs), cudaMemcpyHostToDevice));
+    std::memcpy(b->refptcl, ref0, sizeof(ref0));
+    b->z = z0;
+    b->csr = loop0;
+    return IMPZ_OK;
+  };
+  // a short drift with a wide pipe: nsteps space-charge steps
+  impz_elem_t drift;
+  std::memset(&drift, 0, sizeof(drift));
+  drift.type = 0;
+  drift.nseg = nsteps;
+  drift.mapstp = 1;
+  drift.length = 1.0e-3 * nsteps;
+  drift.val[0] = 1.0e3;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto trial = [&](double* ms) -> int {
+    int r = restore();
+    if (r) return r;
+    for (int rep = 0; rep < 2; rep++) {  // the first run captures the step graphs
+      if (rep == 1 && (r = restore())) return r;
+      if ((r = run_begin(b, &drift, 1))) return r;
+      CK(cudaEventRecord(e0, b->stream));
+      if ((r = run_advance(b, b->lat.nsteps))) return r;
+      CK(cudaEventRecord(e1, b->stream));
+      run_end(b);
+      CK(cudaEventSynchronize(e1));
+      if ((r = check_err(b))) return r;
+    }
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    *ms = (double)t / b->lat.nsteps;
+    return IMPZ_OK;
+  };
+  int sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int dep0 = b->grid_dep, adv0 = b->grid_adv;
+  const int dep_need = (int)std::max<long long>(
+      1, (n + (long long)IMPZ_DEP_BLOCK * IMPZ_DEP_PPT - 1) / ((long long)IMPZ_DEP_BLOCK * IMPZ_DEP_PPT));
+  const int adv_need = (int)std::max<long long>(1, (n + IMPZ_ADV_BLOCK - 1) / IMPZ_ADV_BLOCK);
+  double best = 0.0;
+  int r = trial(&best);
+  auto sweep = [&](int* param, std::vector<int> cands) -> int {
+    const int keep = *param;
+    int bestv = keep;
+    for (int v : cands) {
+      if (v == keep) continue;
+      *param = v;
+      double ms = 0.0;
+      int rr = trial(&ms);
+      if (rr) return rr;
+      if (ms < best * 0.99) { best = ms; bestv = v; }
+    }
+    *param = bestv;
+    return IMPZ_OK;
+  };
+  if (!r) {
+    std::vector<int> dc, ac, zc;
+    for (int v : {dep0, dep0 / 2, 2 * sms, 4 * sms, 8 * sms})
+      if (v >= 1 && v <= std::min(dep0, dep_need)) dc.push_back(v);
+    for (int v : {adv0, adv0 / 2, sms, 2 * sms, 3 * sms})
+      if (v >= 1 && v <= std::min(std::min(adv0, adv_need), kMaxAdvGrid)) ac.push_back(v);
+    for (int v : {8, 4, 2}) zc.push_back(v);
+    r = sweep(&b->grid_dep, dc);
+    if (!r) r = sweep(&b->grid_adv, ac);
+    if (!r) r = sweep(&b->ztile, zc);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int r2 = restore();
+  b->run_pending = false;
+  cudaFree(snap);
+  if (r) return r;
+  if (r2) return r2;
+  out[0] = b->grid_dep;
+  out[1] = b->grid_adv;
+  out[2] = b->ztile;
+  out[3] = best;
   return IMPZ_OK;
 }
 

@@ -84,6 +84,7 @@ struct PoissonBuffers {
   DevState* st;
   const double* wake;       // per-plane {dEx, dEy, dEz}[nz] added to E, or null
   unsigned long long* wake_line;  // the wake's [3][nz] line sums, cleared with the charge
+  int ztile;                // z lines per block of the z convolution (0: the largest that fits)
 };
 
 template <typename T>

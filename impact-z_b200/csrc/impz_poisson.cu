@@ -178,7 +178,9 @@ cudaError_t launch_conv_rest(const PoissonBuffers& b, cudaStream_t s) {
   cudaError_t e;
   const size_t sxy = xy_smem<T>(b.nx, b.ny);
   if ((e = allow_smem(k_fft_xy_inv<T>, sxy)) != cudaSuccess) return e;
-  switch (ztile<T>(b.nz)) {
+  int zt = ztile<T>(b.nz);
+  if (b.ztile > 0 && b.ztile < zt && (b.ztile & (b.ztile - 1)) == 0) zt = b.ztile;
+  switch (zt) {
     case 16: e = zconv_t<T, 16>(b, d, s); break;
     case 8: e = zconv_t<T, 8>(b, d, s); break;
     case 4: e = zconv_t<T, 4>(b, d, s); break;

@@ -124,6 +124,17 @@ int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]);
  * carries from one impz_run to the next. */
 int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, int transverse);
 int impz_wake_off(impz_bunch_t b);
+/* sizeof(StepParams): the bytes per step of the step table a run uploads. */
+int impz_step_params_size(void);
+/* Autotuner: times nsteps (2..64) space-charge steps of a short drift on
+ * this bunch under candidate launch shapes (deposit blocks, push blocks, z
+ * lines per block of the convolution), one parameter at a time, keeps the
+ * fastest and restores the bunch (particles, state, z, refptcl) before each
+ * trial and at the end.  out = {deposit blocks, push blocks, z lines per
+ * block (0: the largest that fits), ms per step}.  Call between runs (the
+ * last run's records are overwritten); allocates a snapshot of the
+ * particles for its duration.  No reference counterpart. */
+int impz_autotune(impz_bunch_t b, int nsteps, double out[4]);
 /* Laser heater of a type -52 element (AccSimulator.f90:982-1006): the
  * energy kick pt -= A sin(-h phase) exp(-(x^2+y^2)/(4 rsig^2/Scxl^2)) with
  * A = sqrt(2 (sigx^2 + rsig^2) / rsig^2) ez / mass from the beam's rms x,
