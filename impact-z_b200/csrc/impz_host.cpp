@@ -211,6 +211,32 @@ void ccl_field(const impz_elem_t& e, double zedge, double z, double& ez1, double
 }  // namespace
 
 namespace {
+// the transverse blocks of a solenoid's map with its rotation
+// y(19..22) (SolRF.f90:216-235, Sol.f90:181-200), each entry written as the
+// reference writes it
+void rotate_blocks(double xm[36], const double* y, double squi, double squf, double dlti,
+                   double dltf) {
+  auto X = [&](int j, int k) -> double& { return xm[(j - 1) + 6 * (k - 1)]; };
+  const double* Y = y - 1;
+  for (int r = 0; r < 2; r++) {  // rows 1,2 from the x block, 3,4 from y
+    const int a = r == 0 ? 7 : 11;          // first y index of the block
+    const double ca = Y[r == 0 ? 19 : 21];  // factor for the x columns
+    const double cb = Y[r == 0 ? 20 : 22];  // factor for the y columns
+    const int j = 2 * r + 1;
+    const double m1 = Y[a] * squi / squf + Y[a + 2] * squi / squf * dlti;
+    const double m2 = (Y[a + 1] - Y[a] * dltf) * squi * squf +
+                      (Y[a + 3] - Y[a + 2] * dltf) * squi * squf * dlti;
+    X(j, 1) = ca * m1;
+    X(j + 1, 1) = ca * m2;
+    X(j, 2) = ca * Y[a + 2] / (squi * squf);
+    X(j + 1, 2) = ca * (Y[a + 3] - Y[a + 2] * dltf) * squf / squi;
+    X(j, 3) = cb * m1;
+    X(j + 1, 3) = cb * m2;
+    X(j, 4) = cb * Y[a + 2] / (squi * squf);
+    X(j + 1, 4) = cb * (Y[a + 3] - Y[a + 2] * dltf) * squf / squi;
+  }
+}
+
 // getaxfldE_SolRF (SolRF.f90:355-466): the on-axis field as the Fourier
 // series of read3_Data's coefficients F (F(1) their count, F(2..4) the
 // series' start, end and period within the element, then the constant,
@@ -247,6 +273,44 @@ void solrf_field(const Phys& P, const impz_elem_t& e, double zedge, double z, do
   ezp1 = ezp1 * escale;
 }
 }  // namespace
+
+void maplinear_sol(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                   double b0, int mapstp, double chg, double mass) {
+  // maplinear_Sol (Sol.f90:120-210), intfunc1_Sol (264-316): a constant
+  // solenoid field b0 = Param(2), its focusing s11 = s33 = (b0/2/brho)^2 and
+  // its rotation in four more variables
+  const double Scxl = P.Scxl;
+  const double qmcc = chg / mass;
+  double y[22];
+  y_start(y, refpt);
+  y[18] = 1.0; y[19] = 0.0; y[20] = 0.0; y[21] = 1.0;
+  const double h = tau / mapstp;
+  double ui, squi, sqi3;
+  uvals(-refpt[5], ui, squi, sqi3);
+  rk6<22>(h, mapstp, t, y, [&](double, const double* yy, double* f) {
+    f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+    const double gamma0 = -yy[5];
+    const double beta0 = std::sqrt(gamma0 * gamma0 - 1.) / gamma0;
+    const double gbet = std::sqrt((gamma0 - 1.0) * (gamma0 + 1.0));
+    f[4] = 1.0 / (beta0 * Scxl);
+    f[5] = 0.0;
+    const double brho = gbet / P.Clight / qmcc;
+    const double sol = 0.5 * b0 / brho;
+    const double s11 = (sol * sol) * Scxl;
+    lin_rhs(Scxl, yy, f, s11, s11, 0.0);
+    const double c2alpha = -b0 / brho / 2;
+    f[18] = -c2alpha * yy[20];
+    f[19] = -c2alpha * yy[21];
+    f[20] = c2alpha * yy[18];
+    f[21] = c2alpha * yy[19];
+  });
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  double uf, squf, sqf3;
+  uvals(-refpt[5], uf, squf, sqf3);
+  xm_from_y(xm, y, squi, squf, sqi3, sqf3, 0.0, 0.0, 0.0, 0.0);
+  rotate_blocks(xm, y, squi, squf, 0.0, 0.0);
+}
 
 bool solrf_table_ok(const impz_elem_t& e) {
   if (e.ndata < 5 || !e.zdat) return false;
@@ -328,27 +392,7 @@ void maplinear_solrf(const Phys& P, double t, double tau, double xm[36], double 
   const double dltf = Scxl * (0.5 * uprimf / uf - qpwf * e1f * sinthf);
   const double thlf = 1.5 * Scxl * (uprimf / uf);
   xm_from_y(xm, y, squi, squf, sqi3, sqf3, dlti, dltf, thli, thlf);
-  // the transverse blocks with the solenoid's rotation (SolRF.f90:216-235),
-  // each written as the reference writes it
-  auto X = [&](int j, int k) -> double& { return xm[(j - 1) + 6 * (k - 1)]; };
-  const double* Y = y - 1;
-  for (int r = 0; r < 2; r++) {  // rows 1,2 from the x block, 3,4 from y
-    const int a = r == 0 ? 7 : 11;          // first y index of the block
-    const double ca = Y[r == 0 ? 19 : 21];  // factor for the x columns
-    const double cb = Y[r == 0 ? 20 : 22];  // factor for the y columns
-    const int j = 2 * r + 1;
-    const double m1 = Y[a] * squi / squf + Y[a + 2] * squi / squf * dlti;
-    const double m2 = (Y[a + 1] - Y[a] * dltf) * squi * squf +
-                      (Y[a + 3] - Y[a + 2] * dltf) * squi * squf * dlti;
-    X(j, 1) = ca * m1;
-    X(j + 1, 1) = ca * m2;
-    X(j, 2) = ca * Y[a + 2] / (squi * squf);
-    X(j + 1, 2) = ca * (Y[a + 3] - Y[a + 2] * dltf) * squf / squi;
-    X(j, 3) = cb * m1;
-    X(j + 1, 3) = cb * m2;
-    X(j, 4) = cb * Y[a + 2] / (squi * squf);
-    X(j + 1, 4) = cb * (Y[a + 3] - Y[a + 2] * dltf) * squf / squi;
-  }
+  rotate_blocks(xm, y, squi, squf, dlti, dltf);
 }
 
 namespace {
@@ -601,6 +645,7 @@ double pipe_radius(const impz_elem_t& e) {
   switch (e.type) {
     case 0: return e.val[0];
     case 1: return e.val[2];
+    case 3: return e.val[2];  // Sol: Param(4)
     case 4: return e.val[3];
     default: return e.val[4];
   }
@@ -657,6 +702,16 @@ int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, do
     double xm[36];
     maplinear_quad(P, z, tau, xm, refptcl, e.val[0], e.mapstp, sp.charge, sp.mass,
                    fringe ? &e : nullptr, zedge);
+    return push_op(prog, op_xm6(xm));
+  }
+  if (e.type == 3) {
+    // drift1_BeamBunch's generic branch: maplinear_Sol unless Param(5) < 0
+    // (the ideal-gap test, which a solenoid only meets with a negative x
+    // misalignment; left out)
+    if (e.val[3] < 0.0) return IMPZ_ERR_UNSUPPORTED;
+    if (e.mapstp < 1) return IMPZ_ERR_ARG;
+    double xm[36];
+    maplinear_sol(P, z, tau, xm, refptcl, e.val[0], e.mapstp, sp.charge, sp.mass);
     return push_op(prog, op_xm6(xm));
   }
   if (e.type >= 101 && e.type <= 106) {

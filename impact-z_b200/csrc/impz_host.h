@@ -27,6 +27,9 @@ void maplinear_rfgap(const Phys& P, double t, double tau, double xm[36], double 
 void maplinear_solrf(const Phys& P, double t, double tau, double xm[36], double refpt[6],
                      double zedge, const impz_elem_t& e, double chg, double mass);
 bool solrf_table_ok(const impz_elem_t& e);
+// maplinear_Sol (type 3): constant field b0 = Param(2)
+void maplinear_sol(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                   double b0, int mapstp, double chg, double mass);
 // maplinear_TWS (type 106): zdat holds the two series of read3_Data's
 // coefficients, val[10] the second wave's phase Param(12)
 void maplinear_tws(const Phys& P, double t, double tau, double xm[36], double refpt[6],

@@ -600,6 +600,85 @@ void orc_maplinear_solrf(double t, double tau, double xm[36], double refpt[6], d
 #undef XM
 }
 
+/* ---- Sol (type 3) linear map ------------------------------------------ */
+typedef struct { double b0, qmcc; } sol_ctx;
+
+/* intfunc1_Sol (Sol.f90:264-316) */
+static void sol_rhs(double t, const double *y, double *f, const void *vctx) {
+  (void)t;
+  const sol_ctx *c = (const sol_ctx *)vctx;
+  const double Scxl = PC.Scxl;
+  f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+  const double gamma0 = -y[5];
+  const double beta0 = sqrt(gamma0 * gamma0 - 1.) / gamma0;
+  const double gbet = sqrt((gamma0 - 1.0) * (gamma0 + 1.0));
+  f[4] = 1.0 / (beta0 * Scxl);
+  f[5] = 0.0;
+  const double brho = gbet / PC.Clight / c->qmcc;
+  const double sol = 0.5 * c->b0 / brho;
+  const double s11 = (sol * sol) * Scxl;
+  const double s33 = (sol * sol) * Scxl;
+  lin_rhs(y, f, s11, s33, 0.0);
+  const double c2alpha = -c->b0 / brho / 2;
+  f[18] = -c2alpha * y[20];
+  f[19] = -c2alpha * y[21];
+  f[20] = c2alpha * y[18];
+  f[21] = c2alpha * y[19];
+}
+
+/* maplinear_Sol (Sol.f90:120-210) */
+void orc_maplinear_sol(double t, double tau, double xm[36], double refpt[6], double b0,
+                       int mapstp, double chg, double mass) {
+  sol_ctx c = {b0, chg / mass};
+  double y[22];
+  memset(xm, 0, 36 * sizeof(double));
+  y_init(y, refpt);
+  y[18] = 1.0; y[19] = 0.0; y[20] = 0.0; y[21] = 1.0;
+  const double h = tau / mapstp;
+  double t0 = t;
+  const double gi = -refpt[5];
+  const double betai = sqrt(gi * gi - 1.) / gi;
+  const double ui = gi * betai;
+  const double squi = sqrt(ui);
+  double s = sqrt(ui);
+  const double sqi3 = s * s * s;
+  const double dlti = 0.0, thli = 0.0;
+  rk6in(h, mapstp, &t0, y, 22, sol_rhs, &c);
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  const double gf = -refpt[5];
+  const double betaf = sqrt(gf * gf - 1.) / gf;
+  const double uf = gf * betaf;
+  const double squf = sqrt(uf);
+  s = sqrt(uf);
+  const double sqf3 = s * s * s;
+  const double dltf = 0.0, thlf = 0.0;
+  xm_assemble(xm, y, squi, squf, sqi3, sqf3, dlti, dltf, thli, thlf);
+  const double *Y = y - 1;
+#define XM(j, k) xm[((j)-1) + 6 * ((k)-1)]
+  XM(1, 1) = Y[19] * (Y[7] * squi / squf + Y[9] * squi / squf * dlti);
+  XM(2, 1) = Y[19] * ((Y[8] - Y[7] * dltf) * squi * squf + (Y[10] - Y[9] * dltf) * squi * squf *
+                                                                 dlti);
+  XM(1, 2) = Y[19] * Y[9] / (squi * squf);
+  XM(2, 2) = Y[19] * (Y[10] - Y[9] * dltf) * squf / squi;
+  XM(1, 3) = Y[20] * (Y[7] * squi / squf + Y[9] * squi / squf * dlti);
+  XM(2, 3) = Y[20] * ((Y[8] - Y[7] * dltf) * squi * squf + (Y[10] - Y[9] * dltf) * squi * squf *
+                                                                 dlti);
+  XM(1, 4) = Y[20] * Y[9] / (squi * squf);
+  XM(2, 4) = Y[20] * (Y[10] - Y[9] * dltf) * squf / squi;
+  XM(3, 1) = Y[21] * (Y[11] * squi / squf + Y[13] * squi / squf * dlti);
+  XM(4, 1) = Y[21] * ((Y[12] - Y[11] * dltf) * squi * squf +
+                      (Y[14] - Y[13] * dltf) * squi * squf * dlti);
+  XM(3, 2) = Y[21] * Y[13] / (squi * squf);
+  XM(4, 2) = Y[21] * (Y[14] - Y[13] * dltf) * squf / squi;
+  XM(3, 3) = Y[22] * (Y[11] * squi / squf + Y[13] * squi / squf * dlti);
+  XM(4, 3) = Y[22] * ((Y[12] - Y[11] * dltf) * squi * squf +
+                      (Y[14] - Y[13] * dltf) * squi * squf * dlti);
+  XM(3, 4) = Y[22] * Y[13] / (squi * squf);
+  XM(4, 4) = Y[22] * (Y[14] - Y[13] * dltf) * squf / squi;
+#undef XM
+}
+
 /* ---- TWS (type 106) linear map --------------------------------------- */
 typedef struct {
   double zedge, escale, len, ww, theta0, theta2, qmcc;
@@ -2057,6 +2136,7 @@ static double pipe_radius(const orc_elem *e) {
   switch (e->type) {
     case 0: return e->val[0];  /* DriftTube Param(2) */
     case 1: return e->val[2];  /* Quadrupole Param(4) */
+    case 3: return e->val[2];  /* Sol Param(4) */
     case 4: return e->val[3];  /* Dipole Param(5) */
     default: return e->val[4]; /* RF gaps Param(6) */
   }
@@ -2211,6 +2291,14 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
                                beam->charge, beam->mass);
             orc_apply_xm(beam->pts, beam->nlocal, xm);
           }
+          z = z + tau1;
+          ihlf++;
+        } else if (bitype == 3) {
+          if (e->val[3] < 0.0) { free(rho); return -8; } /* ideal-gap test: left out */
+          double xm[36];
+          orc_maplinear_sol(z, tau1, xm, beam->refptcl, e->val[0], e->mapstp, beam->charge,
+                            beam->mass);
+          orc_apply_xm(beam->pts, beam->nlocal, xm);
           z = z + tau1;
           ihlf++;
         } else if (bitype >= 101 && bitype <= 106) {

@@ -88,6 +88,9 @@ def lib():
                                               ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                               ctypes.c_double, ctypes.c_int, _D, _D]),
             "orc_undulator": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_int]),
+            "orc_maplinear_sol": (v, [ctypes.c_double, ctypes.c_double, _D, _D,
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_double]),
             "orc_apply_xm": (v, [_D, ctypes.c_int, _D]),
             "orc_transfmapK": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_int,
                                    ctypes.c_double]),

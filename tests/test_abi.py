@@ -235,3 +235,17 @@ def test_fringe_field_quadrupole_map_matches_oracle_bitwise():
                              charge, mass, freq)
     soft, _ = impz.maplinear(e, 0.0, 0.0, 0.0125, ref, charge, mass, freq)
     assert abs(soft[1, 0]) < abs(hard[1, 0])
+
+
+def test_solenoid_map_matches_oracle_bitwise():
+    """maplinear_Sol (Sol.f90:120-316): a 0.5 T solenoid rotates x into y."""
+    freq, mass, charge = 402.5e6, beams.PROTON_MASS_EV, 1.0
+    ref = beams.refptcl_for(2.5e6, mass)
+    e = impz.elem(3, 0.2, 4, 5, [0.5, 0.0, 1.0, 0.0])
+    orc.physconst(freq)
+    xm_p, ref_p = impz.maplinear(e, 0.0, 0.05, 0.025, ref, charge, mass, freq)
+    xm_o, ref_o = np.zeros(36), ref.copy()
+    orc.lib().orc_maplinear_sol(0.05, 0.025, orc.dp(xm_o), orc.dp(ref_o), 0.5, 5, charge, mass)
+    np.testing.assert_array_equal(xm_p, xm_o.reshape(6, 6, order="F"))
+    np.testing.assert_array_equal(ref_p, ref_o)
+    assert abs(xm_p[0, 2]) > 1e-6 and abs(xm_p[2, 0]) > 1e-6
