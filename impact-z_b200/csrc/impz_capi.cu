@@ -1207,6 +1207,11 @@ int impz_maplinear(const impz_elem_t* e, double zedge, double t, double tau, dou
     maplinear_rfgap(P, t, tau, xm, refpt, zedge, *e, charge, mass);
     return IMPZ_OK;
   }
+  if (e->type == 2 && e->val[3] >= 0.0) {
+    if (e->mapstp < 1) return IMPZ_ERR_ARG;
+    maplinear_constfoc(P, t, tau, xm, refpt, e->val, e->mapstp);
+    return IMPZ_OK;
+  }
   if (e->type == 3 && e->val[3] >= 0.0) {
     if (e->mapstp < 1) return IMPZ_ERR_ARG;
     maplinear_sol(P, t, tau, xm, refpt, e->val[0], e->mapstp, charge, mass);

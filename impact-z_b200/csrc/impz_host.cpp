@@ -274,6 +274,31 @@ void solrf_field(const Phys& P, const impz_elem_t& e, double zedge, double z, do
 }
 }  // namespace
 
+void maplinear_constfoc(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                        const double k2[3], int mapstp) {
+  // maplinear_ConstFoc / intfunc1_ConstFoc (ConstFoc.f90): constant
+  // focusing kx0^2, ky0^2, kz0^2 = Param(2..4)
+  const double Scxl = P.Scxl;
+  double y[NV];
+  y_start(y, refpt);
+  const double h = tau / mapstp;
+  double ui, squi, sqi3;
+  uvals(-refpt[5], ui, squi, sqi3);
+  rk6(h, mapstp, t, y, [&](double, const double* yy, double* f) {
+    f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+    const double gamma0 = -yy[5];
+    const double beta0 = std::sqrt(gamma0 * gamma0 - 1.) / gamma0;
+    f[4] = 1.0 / (beta0 * Scxl);
+    f[5] = 0.0;
+    lin_rhs(Scxl, yy, f, k2[0] * Scxl, k2[1] * Scxl, k2[2] * Scxl);
+  });
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  double uf, squf, sqf3;
+  uvals(-refpt[5], uf, squf, sqf3);
+  xm_from_y(xm, y, squi, squf, sqi3, sqf3, 0.0, 0.0, 0.0, 0.0);
+}
+
 void maplinear_sol(const Phys& P, double t, double tau, double xm[36], double refpt[6],
                    double b0, int mapstp, double chg, double mass) {
   // maplinear_Sol (Sol.f90:120-210), intfunc1_Sol (264-316): a constant
@@ -645,6 +670,7 @@ double pipe_radius(const impz_elem_t& e) {
   switch (e.type) {
     case 0: return e.val[0];
     case 1: return e.val[2];
+    case 2: return e.val[3];  // ConstFoc: Param(5)
     case 3: return e.val[2];  // Sol: Param(4)
     case 4: return e.val[3];
     default: return e.val[4];
@@ -702,6 +728,14 @@ int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, do
     double xm[36];
     maplinear_quad(P, z, tau, xm, refptcl, e.val[0], e.mapstp, sp.charge, sp.mass,
                    fringe ? &e : nullptr, zedge);
+    return push_op(prog, op_xm6(xm));
+  }
+  if (e.type == 2) {
+    // ConstFoc through drift1's generic branch (Param(5), its radius, >= 0)
+    if (e.val[3] < 0.0) return IMPZ_ERR_UNSUPPORTED;
+    if (e.mapstp < 1) return IMPZ_ERR_ARG;
+    double xm[36];
+    maplinear_constfoc(P, z, tau, xm, refptcl, e.val, e.mapstp);
     return push_op(prog, op_xm6(xm));
   }
   if (e.type == 3) {

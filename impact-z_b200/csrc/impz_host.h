@@ -27,6 +27,9 @@ void maplinear_rfgap(const Phys& P, double t, double tau, double xm[36], double 
 void maplinear_solrf(const Phys& P, double t, double tau, double xm[36], double refpt[6],
                      double zedge, const impz_elem_t& e, double chg, double mass);
 bool solrf_table_ok(const impz_elem_t& e);
+// maplinear_ConstFoc (type 2): k2 = kx0^2, ky0^2, kz0^2 (Param(2..4))
+void maplinear_constfoc(const Phys& P, double t, double tau, double xm[36], double refpt[6],
+                        const double k2[3], int mapstp);
 // maplinear_Sol (type 3): constant field b0 = Param(2)
 void maplinear_sol(const Phys& P, double t, double tau, double xm[36], double refpt[6],
                    double b0, int mapstp, double chg, double mass);

@@ -51,8 +51,9 @@ typedef struct impz_bunch_s* impz_bunch_t;
  * zedge, Param(k) = val[k-2] for k >= 2 (AccSimulator.f90:262-330).
  * Supported types: 0 drift, 1 quadrupole (gradient; K map when v2 in
  * (-10,-1e-6); the undulator map when v2 < -10; with v2 > 1e-5 the
- * gradient profile of its rfdataN.in in zdat/edat), 3 solenoid (constant
- * field v1, maplinear_Sol), 4 dipole (file ID v3 <= 200: no CSR; above 200 CSR
+ * gradient profile of its rfdataN.in in zdat/edat), 2 constant focusing
+ * (kx0^2, ky0^2, kz0^2 = v1..v3), 3 solenoid (constant field v1,
+ * maplinear_Sol), 4 dipole (file ID v3 <= 200: no CSR; above 200 CSR
  * inside the bend, above 500 also downstream: impz_run only), 101..106 RF gaps
  * as the ideal-RF model (v4 < 0), and otherwise as RK6 linear maps:
  * 101 DTL (with its drift-tube quadrupoles, v6..v9), 102 CCDTL, 103 CCL and

@@ -600,6 +600,46 @@ void orc_maplinear_solrf(double t, double tau, double xm[36], double refpt[6], d
 #undef XM
 }
 
+/* ---- ConstFoc (type 2) linear map ------------------------------------- */
+/* intfunc1_ConstFoc (ConstFoc.f90), k2 = kx0^2, ky0^2, kz0^2 */
+static void constfoc_rhs(double t, const double *y, double *f, const void *vctx) {
+  (void)t;
+  const double *k2 = (const double *)vctx;
+  const double Scxl = PC.Scxl;
+  f[0] = 0.0; f[1] = 0.0; f[2] = 0.0; f[3] = 0.0;
+  const double gamma0 = -y[5];
+  const double beta0 = sqrt(gamma0 * gamma0 - 1.) / gamma0;
+  f[4] = 1.0 / (beta0 * Scxl);
+  f[5] = 0.0;
+  lin_rhs(y, f, k2[0] * Scxl, k2[1] * Scxl, k2[2] * Scxl);
+}
+
+/* maplinear_ConstFoc (ConstFoc.f90) */
+void orc_maplinear_constfoc(double t, double tau, double xm[36], double refpt[6],
+                            const double k2[3], int mapstp) {
+  double y[18];
+  memset(xm, 0, 36 * sizeof(double));
+  y_init(y, refpt);
+  const double h = tau / mapstp;
+  double t0 = t;
+  const double gi = -refpt[5];
+  const double betai = sqrt(gi * gi - 1.) / gi;
+  const double ui = gi * betai;
+  const double squi = sqrt(ui);
+  double s = sqrt(ui);
+  const double sqi3 = s * s * s;
+  rk6i(h, mapstp, &t0, y, constfoc_rhs, k2);
+  refpt[4] = y[4];
+  refpt[5] = y[5];
+  const double gf = -refpt[5];
+  const double betaf = sqrt(gf * gf - 1.) / gf;
+  const double uf = gf * betaf;
+  const double squf = sqrt(uf);
+  s = sqrt(uf);
+  const double sqf3 = s * s * s;
+  xm_assemble(xm, y, squi, squf, sqi3, sqf3, 0.0, 0.0, 0.0, 0.0);
+}
+
 /* ---- Sol (type 3) linear map ------------------------------------------ */
 typedef struct { double b0, qmcc; } sol_ctx;
 
@@ -2136,6 +2176,7 @@ static double pipe_radius(const orc_elem *e) {
   switch (e->type) {
     case 0: return e->val[0];  /* DriftTube Param(2) */
     case 1: return e->val[2];  /* Quadrupole Param(4) */
+    case 2: return e->val[3];  /* ConstFoc Param(5) */
     case 3: return e->val[2];  /* Sol Param(4) */
     case 4: return e->val[3];  /* Dipole Param(5) */
     default: return e->val[4]; /* RF gaps Param(6) */
@@ -2291,6 +2332,13 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
                                beam->charge, beam->mass);
             orc_apply_xm(beam->pts, beam->nlocal, xm);
           }
+          z = z + tau1;
+          ihlf++;
+        } else if (bitype == 2) {
+          if (e->val[3] < 0.0) { free(rho); return -8; } /* ideal-gap test: left out */
+          double xm[36];
+          orc_maplinear_constfoc(z, tau1, xm, beam->refptcl, e->val, e->mapstp);
+          orc_apply_xm(beam->pts, beam->nlocal, xm);
           z = z + tau1;
           ihlf++;
         } else if (bitype == 3) {

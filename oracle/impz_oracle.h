@@ -56,6 +56,8 @@ void orc_maplinear_quad_fringe(double t, double tau, double xm[36], double refpt
                                double zedge, int mapstp, double chg, double mass, int ndata,
                                const double *zdat, const double *gdat);
 void orc_undulator(double tau, double kqlh, double refpt[6], double *pts, int n);
+void orc_maplinear_constfoc(double t, double tau, double xm[36], double refpt[6],
+                            const double k2[3], int mapstp);
 void orc_maplinear_sol(double t, double tau, double xm[36], double refpt[6], double b0,
                        int mapstp, double chg, double mass);
 void orc_maplinear_dtl(double t, double tau, double xm[36], double refpt[6],

@@ -91,6 +91,8 @@ def lib():
             "orc_maplinear_sol": (v, [ctypes.c_double, ctypes.c_double, _D, _D,
                                       ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                       ctypes.c_double]),
+            "orc_maplinear_constfoc": (v, [ctypes.c_double, ctypes.c_double, _D, _D, _D,
+                                           ctypes.c_int]),
             "orc_apply_xm": (v, [_D, ctypes.c_int, _D]),
             "orc_transfmapK": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_int,
                                    ctypes.c_double]),

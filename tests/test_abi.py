@@ -249,3 +249,18 @@ def test_solenoid_map_matches_oracle_bitwise():
     np.testing.assert_array_equal(xm_p, xm_o.reshape(6, 6, order="F"))
     np.testing.assert_array_equal(ref_p, ref_o)
     assert abs(xm_p[0, 2]) > 1e-6 and abs(xm_p[2, 0]) > 1e-6
+
+
+def test_constant_focusing_map_matches_oracle_bitwise():
+    """maplinear_ConstFoc (ConstFoc.f90): kx0^2, ky0^2, kz0^2."""
+    freq, mass, charge = 402.5e6, beams.PROTON_MASS_EV, 1.0
+    ref = beams.refptcl_for(2.5e6, mass)
+    k2 = np.array([30.0, 20.0, 5.0])
+    e = impz.elem(2, 0.2, 4, 5, list(k2) + [1.0])
+    orc.physconst(freq)
+    xm_p, ref_p = impz.maplinear(e, 0.0, 0.05, 0.025, ref, charge, mass, freq)
+    xm_o, ref_o = np.zeros(36), ref.copy()
+    orc.lib().orc_maplinear_constfoc(0.05, 0.025, orc.dp(xm_o), orc.dp(ref_o), orc.dp(k2), 5)
+    np.testing.assert_array_equal(xm_p, xm_o.reshape(6, 6, order="F"))
+    np.testing.assert_array_equal(ref_p, ref_o)
+    assert xm_p[1, 0] < 0 and xm_p[3, 2] < 0 and xm_p[5, 4] < 0  # focusing in all three

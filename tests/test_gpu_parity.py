@@ -347,7 +347,8 @@ def test_rf_linear_maps_lattice_fp64_moments():
     on-axis table (maplinear_DTL/CCDTL/CCL/SC), a SolRF (105, Fourier field
     and a 0.2 T solenoid) and a TWS (106, two standing waves), after a
     quadrupole with a soft-edged gradient profile, an undulator section
-    (a quadrupole with v2 < -10) and a 0.5 T solenoid (type 3), FP64: rms
+    (a quadrupole with v2 < -10), a 0.5 T solenoid (type 3) and a
+    constant-focusing channel (type 2), FP64: rms
     columns of every record within 1e-8 of the oracle, z exact."""
     from test_abi import quad_profile, solrf_coefficients, tws_coefficients
 
@@ -358,6 +359,7 @@ def test_rf_linear_maps_lattice_fp64_moments():
            impz.elem(1, 0.1, 4, 5, [20.0, 7.0, 1.0], rf=quad_profile()),
            impz.elem(1, 0.2, 4, 1, [40.0, -20.0, 1.0]),
            impz.elem(3, 0.2, 4, 5, [0.5, 0.0, 1.0, 0.0]),
+           impz.elem(2, 0.2, 4, 5, [30.0, 20.0, 5.0, 1.0]),
            gap(101, [1.0, 402.5e6, -30.0, 1.0, 1.0, 0.05, 15.0, 0.05, -15.0]),
            gap(102, [1.0, 402.5e6, -30.0, 1.0, 1.0]), gap(103, [1.0, 402.5e6, -30.0, 1.0, 1.0]),
            gap(104, [1.0, 402.5e6, -30.0, 1.0, 1.0]),
@@ -373,7 +375,7 @@ def test_rf_linear_maps_lattice_fp64_moments():
     recs, zs = b.run(lat)
     refs = b.run_reference()
     b.close()
-    assert recs.shape[0] == rows_o.shape[0] == 41
+    assert recs.shape[0] == rows_o.shape[0] == 45
     np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
     np.testing.assert_allclose(refs[:, 4:6], np.c_[rows_o[:, 1], -rows_o[:, 2]], rtol=1e-14,
                                atol=0)
