@@ -81,6 +81,7 @@ _SIGS = {
     "impz_laser_heater": (ctypes.c_int, [_B, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
     "impz_autotune": (ctypes.c_int, [_B, ctypes.c_int, _D]),
     "impz_step_params_size": (ctypes.c_int, []),
+    "impz_set_integrator": (ctypes.c_int, [_B, ctypes.c_int]),
     "impz_bunch_set_z": (ctypes.c_int, [_B, ctypes.c_double]),
     "impz_bunch_stream": (ctypes.c_void_p, [_B]),
     "impz_map_half": (ctypes.c_int, [_B, _E, ctypes.c_double, _D, ctypes.c_double, ctypes.c_int,
@@ -330,6 +331,10 @@ class Bunch:
         """The energy kick of a type -52 laser heater element."""
         _check(lib().impz_laser_heater(self.h, float(rsig), float(wavelength), float(ez)),
                "impz_laser_heater")
+
+    def set_integrator(self, flagmap):
+        """1: the linear map integrator; 2: the Lorentz integrator."""
+        _check(lib().impz_set_integrator(self.h, int(flagmap)), "impz_set_integrator")
 
     def set_z(self, z):
         _check(lib().impz_bunch_set_z(self.h, float(z)), "impz_bunch_set_z")

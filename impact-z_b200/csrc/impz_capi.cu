@@ -1287,8 +1287,10 @@ int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double cur
   b->z = 0.0;
   // a new beam at z = 0: the bend bookkeeping restarts; the wake switch is
   // the one impz_wake_set / impz_wake_off left
+  const int flagmap = b->csr.flagmap;
   b->csr = LoopState();
   b->csr.flagwake = b->csr.flagwakeread = b->wk_on ? 1 : 0;
+  b->csr.flagmap = flagmap;
   b->stage = ST_IDLE;
   b->bend.active = false;
   b->run_pending = false;
@@ -1534,6 +1536,12 @@ int impz_run_reference(impz_bunch_t b, double* refrec, int maxrec, int* nrec) {
 // block of the convolution; one parameter at a time, keeping the best.
 // The bunch is restored before each trial and at the end.
 int impz_step_params_size(void) { return (int)sizeof(StepParams); }
+
+int impz_set_integrator(impz_bunch_t b, int flagmap) {
+  if (!b || (flagmap != 1 && flagmap != 2)) return IMPZ_ERR_ARG;
+  b->csr.flagmap = b->csr_run.flagmap = flagmap;
+  return IMPZ_OK;
+}
 
 static void drop_graphs(impz_bunch_t b) {
   cudaStreamSynchronize(b->stream);

@@ -28,6 +28,7 @@ enum MapKind : int {
   MAP_SECTOR = 7,    // Sector_Dipole (Dipole.f90:693-788)
   MAP_XM2 = 8,       // 6x6 map with only its three 2x2 diagonal blocks nonzero
   MAP_UNDUL = 9,     // transfUndulator_Quadrupole (Quadrupole.f90:611-665)
+  MAP_DRIFT2 = 10,   // drift2_BeamBunch, the Lorentz integrator's drift (BeamBunch.f90:467-509)
 };
 
 struct MapOp {
@@ -64,6 +65,9 @@ struct StepParams {
   int wake;            // wake of this step's kick: 0 none, 1 read-in table, 2 analytic
   int pad3;
   double wk_aa, wk_gg, wk_len;  // analytic wake: iris radius, gap, period (Param(13..15))
+  int lorentz;         // the kick is the Lorentz integrator's (kick2/scatter2)
+  int pad4;
+  double lz_grad;      // its element's external field: quadrupole gradient (0: drift)
 };
 
 #define IMPZ_MOMREC 48   // per recorded step: 44 raw values, npt, nlocal, current, spare

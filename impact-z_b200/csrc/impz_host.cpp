@@ -908,10 +908,11 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
   };
   struct Step {
     MapProgram a, b;
-    int sc, csr, wake;
+    int sc, csr, wake, lorentz;
     double gam, tau, rad;
     double csr_r0, csr_s0, csr_blen;
     double wk_aa, wk_gg, wk_len;
+    double lz_grad;
     double z;
     double ref[6];
   };
@@ -928,6 +929,11 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     if (e.nseg < 1) return IMPZ_ERR_ARG;
     const int bnseg = e.nseg, bitype = e.type;
     double piperad = pipe_radius(e), piperad2 = piperad;
+    // the Lorentz integrator covers drifts and hard-edge quadrupoles, with
+    // space charge (kick2 carries the quadrupoles' focusing)
+    const bool lorentz = csr.flagmap == 2;
+    if (lorentz && (!(bitype == 0 || (bitype == 1 && e.val[1] <= 0.0)) || !sc_on))
+      return IMPZ_ERR_UNSUPPORTED;
     // the wake switch of each element (AccSimulator.f90:865-875)
     if (bitype == 105 || bitype == 106) {
       csr.aawk = e.val[11];
@@ -984,8 +990,22 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
             s.wk_gg = csr.ggwk;
             s.wk_len = csr.lengwk;
           }
+          if (lorentz) {
+            s.lorentz = 1;
+            s.lz_grad = bitype == 1 ? e.val[0] : 0.0;
+          }
         }
-        if (bitype == 4) {
+        if (lorentz) {
+          // map1_BeamBunch(Bpts,z,tau2): drift2 by tau2/2 (BeamBunch.f90:467-509)
+          MapOp op = blank(MAP_DRIFT2);
+          const double gamma0 = -refptcl[5];
+          const double beta0 = std::sqrt(1.0 - 1.0 / gamma0 / gamma0);
+          op.c[0] = gamma0; op.c[1] = beta0; op.c[2] = P.Scxl; op.c[3] = tau2;
+          refptcl[4] = refptcl[4] + 0.5 * tau2 / (P.Scxl * beta0);
+          int r = push_op(prog, op);
+          if (r) return r;
+          ihlf++;
+        } else if (bitype == 4) {
           bend_sector_op(P, bs, tau1, sp, prog);
         } else {
           int r = half_map_ops(P, e, zedge, z, tau1, j, ihlf, refptcl, sp, prog);
@@ -1031,6 +1051,8 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
       sp_.wk_aa = cur.wk_aa;
       sp_.wk_gg = cur.wk_gg;
       sp_.wk_len = cur.wk_len;
+      sp_.lorentz = cur.lorentz;
+      sp_.lz_grad = cur.lz_grad;
       if (cur.csr || cur.wake) out.has_wake = true;
       sp_.gam = cur.gam;
       sp_.tau = cur.tau;

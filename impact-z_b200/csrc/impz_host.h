@@ -81,6 +81,7 @@ struct LoopState {
   int flagwake = 0;         // the kicks include a wake
   int flagwakeread = 0;     // ... the read-in one (-41), else the analytic one
   double aawk = 0.0, ggwk = 0.0, lengwk = 0.0;  // the last 105/106's Param(13..15)
+  int flagmap = 1;          // 1 the linear map integrator, 2 the Lorentz integrator (-25)
 };
 // run_AccSimulator's element/segment loop (AccSimulator.f90:742-1504)
 // turned into a step table.  refptcl, z and the CSR state advance to the

@@ -66,6 +66,17 @@ __device__ __forceinline__ void map_drift(Particle& p, const volatile double* c)
 #endif
 }
 
+// drift2_BeamBunch (BeamBunch.f90:467-509): the Lorentz integrator's drift
+// by tau/2; c = {gamma0, beta0, Scxl, tau}
+__device__ __forceinline__ void map_drift2(Particle& p, const volatile double* c) {
+  const double gamma0 = c[0], beta0 = c[1], xl = c[2], tau = c[3];
+  const double g = gamma0 - p.pt;
+  const double pz = sqrt(((g * g - 1.0) - p.px * p.px) - p.py * p.py);
+  p.x = p.x + 0.5 * tau * p.px / (xl * pz);
+  p.y = p.y + 0.5 * tau * p.py / (xl * pz);
+  p.ph = p.ph + 0.5 * tau * (g / (xl * pz) - 1.0 / (beta0 * xl));
+}
+
 __device__ __forceinline__ void map_xm6(Particle& p, const volatile double* xm, int mask_lo,
                                         int mask_hi) {
   // BeamBunch.f90:310-320: temp(j) = sum_k Pts1(k)*xm(j,k) from 0.0; the
@@ -311,6 +322,7 @@ __device__ __forceinline__ void apply_program(Particle& p, const volatile MapPro
       case MAP_SECTOR: map_sector(p, op.c); break;
       case MAP_XM2: map_xm2(p, op.c); break;
       case MAP_UNDUL: map_undul(p, op.c); break;
+      case MAP_DRIFT2: map_drift2(p, op.c); break;
       default: break;
     }
   }
@@ -637,6 +649,61 @@ __device__ __forceinline__ double moment_tail(double acc1, int lane) {
   return t;
 }
 
+// The Lorentz integrator's kick of a drift or hard-edge quadrupole
+// (scatter2_BeamBunch, BeamBunch.f90:2975-3065, the generic-element branch):
+// the space-charge field exn = Ex*gam, eyn = Ey*gam, ezn = Ez of the grid
+// times 1/(4 pi eps0) = c^2 1e-7 (a default-real literal there), its
+// magnetic part -beta0/c Ey, beta0/c Ex, the quadrupole's B = G (y, x, 0)
+// at the particle [m] (getfld_Quadrupole, Quadrupole.f90:369-402), and the
+// implicit momentum update iterated twice.  The on-axis Ez of these
+// elements is zero, so gamma0 does not change.
+__device__ __forceinline__ void lorentz_kick(Particle& p, double exn, double eyn, double ezn,
+                                             double gam, double tau, double grad,
+                                             const Consts& k) {
+  const double xl = k.Scxl, Clight = k.Clight;
+  const double tmpscale = Clight * Clight * 1.00000001168609742e-07;
+  const double beta0 = sqrt(gam * gam - 1.0) / gam;
+  const double qmcc = k.charge / k.mass;
+  const double ez0 = 0.0;
+  const double tmpgamma0 = gam + 0.5 * tau * qmcc * ez0;
+  const double ext4 = grad * (p.y * xl), ext5 = grad * (p.x * xl);
+  const double ex = tmpscale * exn + 0.0;
+  const double ey = tmpscale * eyn + 0.0;
+  const double ez = tmpscale * ezn + 0.0;
+  const double bx = -(beta0 / Clight * tmpscale * eyn) + ext4;
+  const double by = beta0 / Clight * tmpscale * exn + ext5;
+  const double bz = 0.0;
+  const double r7 = k.qmi;
+  const double tmp12 = -tau * Clight * bz * r7 / 2;
+  const double tmp13 = tau * ex * r7 / 2;
+  const double tmp23 = tau * ey * r7 / 2;
+  const double tmp1 = tmpgamma0 * ex * tau * r7;
+  const double tmp2 = Clight * by * tau * r7;
+  const double tmp3 = tmpgamma0 * ey * tau * r7;
+  const double tmp4 = Clight * bx * tau * r7;
+  const double tmp5 = (ez0 * qmcc - ez * r7) * tau;
+  double pz = sqrt((gam - p.pt) * (gam - p.pt) - 1.0 - p.px * p.px - p.py * p.py);
+  const double p1 = p.px, p2 = p.py, p3 = p.pt;
+#pragma unroll
+  for (int ii = 1; ii <= 2; ii++) {
+    const double a12 = tmp12 / pz, a13 = tmp13 / pz, a23 = tmp23 / pz;
+    const double b1 = p1 - a12 * p2 - a13 * p3 + tmp1 / pz - tmp2;
+    const double b2 = a12 * p1 + p2 - a23 * p3 + tmp3 / pz + tmp4;
+    const double b3 = -(a13 * p1) - a23 * p2 + p3 + tmp5;
+    const double det = 1 + a12 * a12 - a13 * a13 - a23 * a23;
+    const double s11 = 1 - a23 * a23, s12 = -a12 + a13 * a23, s13 = a12 * a23 - a13;
+    const double s21 = a12 + a13 * a23, s22 = 1 - a13 * a13, s23 = -a23 - a13 * a12;
+    const double s31 = -(a12 * a23) - a13, s32 = -a23 + a12 * a13, s33 = 1 + a12 * a12;
+    p.px = (s11 * b1 + s12 * b2 + s13 * b3) / det;
+    p.py = (s21 * b1 + s22 * b2 + s23 * b3) / det;
+    p.pt = (s31 * b1 + s32 * b2 + s33 * b3) / det;
+    const double tmpgamma00 = gam + tau * qmcc * ez0;
+    const double tmpsq2 = (tmpgamma00 - p.pt) * (tmpgamma00 - p.pt) - 1.0 - p.px * p.px -
+                          p.py * p.py;
+    if (tmpsq2 > 0.0) pz = 0.5 * pz + 0.5 * sqrt(tmpsq2);
+  }
+}
+
 template <int BLOCK, bool F32, int U, bool LIGHT>
 __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a) {
   __shared__ double red[BLOCK / 32][IMPZ_RAW_LEN];
@@ -762,15 +829,21 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
           }
           const double exn = ex * gam, eyn = ey * gam, ezn = ez;
           p[u].x = xg * xk;
-          p[u].px = p[u].px + txy * exn;
           p[u].y = yg * xk;
-          p[u].py = p[u].py + txy * eyn;
 #if IMPZ_FASTMATH
           p[u].ph = zg * xkg * rb;
 #else
           p[u].ph = zg * xk / (-(gam * betai));
 #endif
-          p[u].pt = p[u].pt - tt * ezn;
+          if (!LIGHT && sp->lorentz) {
+            // scatter2_BeamBunch (BeamBunch.f90:2766-3065): the same way back
+            // to the z frame, then the implicit Lorentz update
+            lorentz_kick(p[u], exn, eyn, ezn, gam, sp->tau, sp->lz_grad, a.k);
+          } else {
+            p[u].px = p[u].px + txy * exn;
+            p[u].py = p[u].py + txy * eyn;
+            p[u].pt = p[u].pt - tt * ezn;
+          }
         }
       }
       if (keep[u] && post) apply_program<LIGHT>(p[u], progs[0]);

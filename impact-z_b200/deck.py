@@ -411,7 +411,7 @@ def lattice_segments(deck, workdir, skip=(), start=0):
     read-in wake control, ("checkpoint", {"element", "inb", "jstp", "nstep"})
     for each type -7 checkpoint, ("laser", {"rsig", "wavelength", "ez"}) for
     each type -52 laser heater, ("slices", Element) for each type -8 slice
-    output, and last ("skipped", [types]) for the
+    output, ("integrator", Flagmap) for each type -25 switch, and last ("skipped", [types]) for the
     control elements passed over because they are in `skip`.  -99 ends the
     lattice; any other control element is refused (ValueError).  `start`
     skips the first elements (a restart continues after element iend).
@@ -456,6 +456,9 @@ def lattice_segments(deck, workdir, skip=(), start=0):
             skipped.append(e.type)
         elif e.type == -8:
             yield "slices", e
+        elif e.type == -25:
+            # switch integrator: Flagmap = bmpstp (AccSimulator.f90:806-809)
+            yield "integrator", e.mapstp
         elif e.type == -52:
             # laser heater (AccSimulator.f90:982-1006): Param(2..4)
             yield "laser", {"rsig": e.vals[0], "wavelength": e.vals[1], "ez": e.vals[2]}
@@ -483,10 +486,11 @@ def lattice_segments(deck, workdir, skip=(), start=0):
 
 
 def check_supported(deck):
-    """The runner covers the map integrator with open boundaries, one charge
-    state and a particle.in distribution."""
-    if deck.flagmap != 1 or deck.flagbc != 1 or deck.flagdist != 19 or deck.nchrg != 1:
-        raise ValueError("this runner needs Flagmap=1, Flagbc=1, Flagdist=19 and one charge "
+    """The runner covers open boundaries, one charge state and a particle.in
+    distribution, with the map integrator (Flagmap=1) or the Lorentz
+    integrator (Flagmap=2, drifts and hard-edge quadrupoles)."""
+    if deck.flagmap not in (1, 2) or deck.flagbc != 1 or deck.flagdist != 19 or deck.nchrg != 1:
+        raise ValueError("this runner needs Flagmap=1 or 2, Flagbc=1, Flagdist=19 and one charge "
                          "state (deck has %d, %d, %d, %d)" % (deck.flagmap, deck.flagbc,
                                                              deck.flagdist, deck.nchrg))
 
@@ -512,6 +516,7 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
               (deck.nx, deck.ny, deck.nz), form=FORM_FP64 if form is None else form,
               track_ids=True)
     b.set_z(z0)
+    b.set_integrator(deck.flagmap)
     rows, skipped = [], []
     try:
         for kind, item in lattice_segments(deck, workdir, set(skip), start):
@@ -524,6 +529,8 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
                     b.wake_off()
             elif kind == "laser":
                 b.laser_heater(item["rsig"], item["wavelength"], item["ez"])
+            elif kind == "integrator":
+                b.set_integrator(item)
             elif kind == "slices":
                 if write:
                     info = b.info()

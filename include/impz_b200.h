@@ -126,6 +126,12 @@ int impz_bunching(impz_bunch_t b, double wavenumber, double out[2]);
  * carries from one impz_run to the next. */
 int impz_wake_set(impz_bunch_t b, const double* table, int ntab, double scale, int transverse);
 int impz_wake_off(impz_bunch_t b);
+/* The integrator of the runs that follow (Flagmap of the deck, or a -25
+ * element): 1 the linear map integrator, 2 the Lorentz integrator
+ * (drift2 half steps around kick2/scatter2, BeamBunch.f90:467-509,
+ * 2187-3071), here for drifts and hard-edge quadrupoles with space
+ * charge; a run with any other element under it is IMPZ_ERR_UNSUPPORTED. */
+int impz_set_integrator(impz_bunch_t b, int flagmap);
 /* sizeof(StepParams): the bytes per step of the step table a run uploads. */
 int impz_step_params_size(void);
 /* Autotuner: times nsteps (2..64) space-charge steps of a short drift on

@@ -53,6 +53,22 @@ void orc_get_physconst(double out[5]) {
 
 /* ------------------------------------------------------------------ */
 /* drift1_BeamBunch, bitype 0: exact drift (BeamBunch.f90:276-298) */
+/* drift2_BeamBunch (BeamBunch.f90:467-509): the Lorentz integrator's drift
+ * by 0.5*tau; returns nothing, advances refptcl(5) */
+void orc_drift2(double *pts, int n, double refptcl[6], double tau) {
+  const double xl = PC.Scxl;
+  const double gamma0 = -refptcl[5];
+  const double beta0 = sqrt(1.0 - 1.0 / gamma0 / gamma0);
+  for (int i = 0; i < n; i++) {
+    const double pz = sqrt((gamma0 - P(i, 5)) * (gamma0 - P(i, 5)) - 1.0 - P(i, 1) * P(i, 1) -
+                           P(i, 3) * P(i, 3));
+    P(i, 0) = P(i, 0) + 0.5 * tau * P(i, 1) / (xl * pz);
+    P(i, 2) = P(i, 2) + 0.5 * tau * P(i, 3) / (xl * pz);
+    P(i, 4) = P(i, 4) + 0.5 * tau * ((gamma0 - P(i, 5)) / (xl * pz) - 1.0 / (beta0 * xl));
+  }
+  refptcl[4] = refptcl[4] + 0.5 * tau / (xl * beta0);
+}
+
 void orc_drift_exact(double *pts, int n, double refptcl[6], double tau) {
   const double Scxl = PC.Scxl;
   double gam0 = -refptcl[5];
@@ -1448,10 +1464,37 @@ void orc_kick1(double *pts, int n, const double *phi, const int mesh[3],
  * field added to the node fields before the gather (BeamBunch.f90:5015-5033);
  * wfield = {dEx[nz], dEy[nz], dEz[nz]} in grid-field units (orc_wake_field),
  * NULL for none. */
+/* The Lorentz integrator's kick of a drift or hard-edge quadrupole
+ * (scatter2_BeamBunch, BeamBunch.f90:2510-3071, the generic-element
+ * branch): gradient = Param(2) of a quadrupole, 0 for a drift; qmi =
+ * Pts1(7) */
+typedef struct { double gradient, qmi; } lorentz_kick;
+
+static void kick_common(double *pts, int n, const double *phi, const int mesh[3],
+                        const double range[6], const double msize[3], double gam, double curr,
+                        double tau, double mass, double chrg, double *eg, const double *wfield,
+                        const lorentz_kick *lz);
+
 void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
                 const double range[6], const double msize[3], double gam,
                 double curr, double tau, double mass, double chrg, double *eg,
                 const double *wfield) {
+  kick_common(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, eg, wfield, NULL);
+}
+
+/* kick2_BeamBunch (BeamBunch.f90:2187-2508) with scatter2 for a drift or a
+ * hard-edge quadrupole of the given gradient, one rank, Flagbc=1 */
+void orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const double range[6],
+               const double msize[3], double gam, double curr, double tau, double mass,
+               double chrg, double gradient, double qmi) {
+  const lorentz_kick lz = {gradient, qmi};
+  kick_common(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, NULL, NULL, &lz);
+}
+
+static void kick_common(double *pts, int n, const double *phi, const int mesh[3],
+                        const double range[6], const double msize[3], double gam, double curr,
+                        double tau, double mass, double chrg, double *eg, const double *wfield,
+                        const lorentz_kick *lz) {
   if (curr < 1.0e-20) return;
   const int nx = mesh[0], ny = mesh[1], nz = mesh[2];
   const size_t G = (size_t)nx * ny * nz;
@@ -1533,6 +1576,58 @@ void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
     double rcpgammai = 1.0 / (-P(q, 5) + gam);
     double tmpsq = 1.0 - rcpgammai * rcpgammai * ((1 + P(q, 1) * P(q, 1)) + P(q, 3) * P(q, 3));
     double betai = sqrt(tmpsq);
+    if (lz) {
+      /* back from t to z (BeamBunch.f90:2766-2771), then the external field
+       * at (x, y) [m] (getfld_Quadrupole, Quadrupole.f90:369-402: B = G (y,
+       * x, 0); none in a drift) and the implicit Lorentz update iterated
+       * twice (BeamBunch.f90:3023-3065) */
+      P(q, 4) = P(q, 4) * xk / (-gam * betai);
+      P(q, 0) = P(q, 0) * xk;
+      P(q, 2) = P(q, 2) * xk;
+      const double xl = PC.Scxl, Clight = PC.Clight;
+      const double tmpscale2 = Clight * Clight * (double)1.0e-7f;
+      const double beta0 = sqrt(gam * gam - 1.0) / gam;
+      const double qmcc = chrg / mass;
+      const double ez0 = 0.0;
+      const double tmpgamma0 = gam + 0.5 * tau * qmcc * ez0;
+      const double ext4 = lz->gradient * (P(q, 2) * xl), ext5 = lz->gradient * (P(q, 0) * xl);
+      const double ex = tmpscale2 * exn + 0.0;
+      const double ey = tmpscale2 * eyn + 0.0;
+      const double ez = tmpscale2 * ezn + 0.0;
+      const double bx = -(beta0 / Clight * tmpscale2 * eyn) + ext4;
+      const double by = beta0 / Clight * tmpscale2 * exn + ext5;
+      const double bz = 0.0;
+      const double r7 = lz->qmi;
+      const double tmp12 = -tau * Clight * bz * r7 / 2;
+      const double tmp13 = tau * ex * r7 / 2;
+      const double tmp23 = tau * ey * r7 / 2;
+      const double tmp1 = tmpgamma0 * ex * tau * r7;
+      const double tmp2 = Clight * by * tau * r7;
+      const double tmp3 = tmpgamma0 * ey * tau * r7;
+      const double tmp4 = Clight * bx * tau * r7;
+      const double tmp5 = (ez0 * qmcc - ez * r7) * tau;
+      double pz = sqrt((gam - P(q, 5)) * (gam - P(q, 5)) - 1.0 - P(q, 1) * P(q, 1) -
+                       P(q, 3) * P(q, 3));
+      const double p1 = P(q, 1), p2 = P(q, 3), p3 = P(q, 5);
+      for (int ii = 1; ii <= 2; ii++) {
+        const double a12 = tmp12 / pz, a13 = tmp13 / pz, a23 = tmp23 / pz;
+        const double b1 = p1 - a12 * p2 - a13 * p3 + tmp1 / pz - tmp2;
+        const double b2 = a12 * p1 + p2 - a23 * p3 + tmp3 / pz + tmp4;
+        const double b3 = -(a13 * p1) - a23 * p2 + p3 + tmp5;
+        const double det = 1 + a12 * a12 - a13 * a13 - a23 * a23;
+        const double s11 = 1 - a23 * a23, s12 = -a12 + a13 * a23, s13 = a12 * a23 - a13;
+        const double s21 = a12 + a13 * a23, s22 = 1 - a13 * a13, s23 = -a23 - a13 * a12;
+        const double s31 = -(a12 * a23) - a13, s32 = -a23 + a12 * a13, s33 = 1 + a12 * a12;
+        P(q, 1) = (s11 * b1 + s12 * b2 + s13 * b3) / det;
+        P(q, 3) = (s21 * b1 + s22 * b2 + s23 * b3) / det;
+        P(q, 5) = (s31 * b1 + s32 * b2 + s33 * b3) / det;
+        const double tmpgamma00 = gam + tau * qmcc * ez0;
+        const double tmpsq2 = (tmpgamma00 - P(q, 5)) * (tmpgamma00 - P(q, 5)) - 1.0 -
+                              P(q, 1) * P(q, 1) - P(q, 3) * P(q, 3);
+        if (tmpsq2 > 0.0) pz = 0.5 * pz + 0.5 * sqrt(tmpsq2);
+      }
+      continue;
+    }
     P(q, 0) = P(q, 0) * xk;
     P(q, 1) = P(q, 1) + tau * xycon * exn;
     P(q, 2) = P(q, 2) * xk;
@@ -2214,6 +2309,11 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     const int bnseg = e->nseg, bitype = e->type;
     double piperad = pipe_radius(e), piperad2 = piperad;
     if (bitype < 0) { free(rho); return -3; }
+    const int lorentz = beam->flagmap == 2;
+    if (lorentz && (!(bitype == 0 || (bitype == 1 && e->val[1] <= 0.0)) || bcurr < 1.0e-10)) {
+      free(rho); /* Lorentz integrator: drifts and hard-edge quadrupoles, with space charge */
+      return -10;
+    }
     orc_wake_elem(bitype, e->val);
     if (bitype == 4) { piperad = 100.0; piperad2 = 100.0; }
     double tau1 = 0.0;
@@ -2301,12 +2401,21 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
                          beam->current, beam->npt, beam->mass, beam->charge, !WK.read, wf);
             }
             orc_cvbkforth1st(beam->pts, beam->nlocal, beam->refptcl);
-            orc_kick1w(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],
-                       beam->current, tau2, beam->mass, beam->charge, NULL, wf);
+            if (lorentz)
+              orc_kick2(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],
+                        beam->current, tau2, beam->mass, beam->charge,
+                        bitype == 1 ? e->val[0] : 0.0, beam->nlocal ? beam->pts[6] : 0.0);
+            else
+              orc_kick1w(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],
+                         beam->current, tau2, beam->mass, beam->charge, NULL, wf);
             free(wf);
           }
         }
-        if (bitype == 4) {
+        if (lorentz) {
+          /* map1_BeamBunch(Bpts,z,tau2): drift2 by tau2/2 (AccSimulator.f90:1109-1116) */
+          orc_drift2(beam->pts, beam->nlocal, beam->refptcl, tau2);
+          z = z + 0.5 * tau2;
+        } else if (bitype == 4) {
           orc_sector(tau1, beta0, hd0, hd1, beam->pts, beam->nlocal, qm0);
           z = z + tau1;
         } else if (bitype == 0) {

@@ -123,6 +123,10 @@ void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
                 const double range[6], const double msize[3], double gam,
                 double curr, double tau, double mass, double chrg, double *eg,
                 const double *wfield);
+void orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const double range[6],
+               const double msize[3], double gam, double curr, double tau, double mass,
+               double chrg, double gradient, double qmi);
+void orc_drift2(double *pts, int n, double refptcl[6], double tau);
 /* read-in wakefield of type -41 elements (Data.f90:559-633,
  * AccSimulator.f90:959-978, 1273-1340, Field.f90:783-1001) */
 int orc_wake_set(const double *z, const double *ew, const double *epw, const double *eppw,
@@ -173,6 +177,9 @@ typedef struct {
   /* CSR bend bookkeeping of run_AccSimulator (AccSimulator.f90:638-740) */
   double zbleng, sentr, bendlencsr, r0;
   int flagbendcsr;
+  /* Flagmap: 1 (0 too) the linear map integrator, 2 the Lorentz integrator
+   * (drifts and hard-edge quadrupoles, with space charge) */
+  int flagmap;
 } orc_beam;
 
 /* runs elements [0,nelem); writes one ORC_DIAG_LEN row per diagnostic

@@ -42,6 +42,7 @@ class OrcBeam(ctypes.Structure):
         ("zbleng", ctypes.c_double), ("sentr", ctypes.c_double),
         ("bendlencsr", ctypes.c_double), ("r0", ctypes.c_double),
         ("flagbendcsr", ctypes.c_int),
+        ("flagmap", ctypes.c_int),
     ]
 
 CSR_FIELDS = ("zbleng", "sentr", "bendlencsr", "r0", "flagbendcsr")
@@ -187,7 +188,7 @@ def elem_from(e):
     return o
 
 
-def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0, state=None):
+def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0, state=None, flagmap=1):
     """orc_run over a lattice: returns (rows, final pts, final beam).  `state`
     (a beam returned by an earlier call) carries the CSR bend bookkeeping
     across calls, as one element loop of the reference would."""
@@ -202,6 +203,7 @@ def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0, state=Non
     for i in range(6):
         beam.refptcl[i] = refptcl[i]
     beam.z = z
+    beam.flagmap = int(flagmap)
     if state is not None:
         for f in CSR_FIELDS:
             setattr(beam, f, getattr(state, f))
