@@ -932,7 +932,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     // the Lorentz integrator covers drifts and hard-edge quadrupoles, with
     // space charge (kick2 carries the quadrupoles' focusing)
     const bool lorentz = csr.flagmap == 2;
-    if (lorentz && (!(bitype == 0 || (bitype == 1 && e.val[1] <= 0.0)) || !sc_on))
+    if (lorentz && !(bitype == 0 || (bitype == 1 && e.val[1] <= 0.0)))
       return IMPZ_ERR_UNSUPPORTED;
     // the wake switch of each element (AccSimulator.f90:865-875)
     if (bitype == 105 || bitype == 106) {

@@ -846,6 +846,11 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
           }
         }
       }
+      // a Lorentz-integrator step without space charge: scatter20's kick by
+      // the element's field alone, on the stored coordinates
+      // (BeamBunch.f90:3075-3531)
+      if (!LIGHT && keep[u] && !kick && post && sp->lorentz)
+        lorentz_kick(p[u], 0.0, 0.0, 0.0, gam, sp->tau, sp->lz_grad, a.k);
       if (keep[u] && post) apply_program<LIGHT>(p[u], progs[0]);
       if (keep[u]) {
         c[u].x = p[u].x; c[u].px = p[u].px; c[u].y = p[u].y;

@@ -1491,6 +1491,60 @@ void orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const d
   kick_common(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, NULL, NULL, &lz);
 }
 
+/* the implicit Lorentz update of scatter2/scatter20 (BeamBunch.f90:3023-3065
+ * and 3491-3531) for a space-charge field (exn, eyn, ezn) [grid units] and a
+ * quadrupole's B = G (y, x, 0) at (x, y) [m]; p = one particle's Pts1 */
+static void lorentz_update(double *p, double exn, double eyn, double ezn, double gam, double tau,
+                           double mass, double chrg, const lorentz_kick *lz) {
+  const double xl = PC.Scxl, Clight = PC.Clight;
+  const double tmpscale2 = Clight * Clight * (double)1.0e-7f;
+  const double beta0 = sqrt(gam * gam - 1.0) / gam;
+  const double qmcc = chrg / mass;
+  const double ez0 = 0.0;
+  const double tmpgamma0 = gam + 0.5 * tau * qmcc * ez0;
+  const double ext4 = lz->gradient * (p[2] * xl), ext5 = lz->gradient * (p[0] * xl);
+  const double ex = tmpscale2 * exn + 0.0;
+  const double ey = tmpscale2 * eyn + 0.0;
+  const double ez = tmpscale2 * ezn + 0.0;
+  const double bx = -(beta0 / Clight * tmpscale2 * eyn) + ext4;
+  const double by = beta0 / Clight * tmpscale2 * exn + ext5;
+  const double bz = 0.0;
+  const double r7 = lz->qmi;
+  const double tmp12 = -tau * Clight * bz * r7 / 2;
+  const double tmp13 = tau * ex * r7 / 2;
+  const double tmp23 = tau * ey * r7 / 2;
+  const double tmp1 = tmpgamma0 * ex * tau * r7;
+  const double tmp2 = Clight * by * tau * r7;
+  const double tmp3 = tmpgamma0 * ey * tau * r7;
+  const double tmp4 = Clight * bx * tau * r7;
+  const double tmp5 = (ez0 * qmcc - ez * r7) * tau;
+  double pz = sqrt((gam - p[5]) * (gam - p[5]) - 1.0 - p[1] * p[1] - p[3] * p[3]);
+  const double p1 = p[1], p2 = p[3], p3 = p[5];
+  for (int ii = 1; ii <= 2; ii++) {
+    const double a12 = tmp12 / pz, a13 = tmp13 / pz, a23 = tmp23 / pz;
+    const double b1 = p1 - a12 * p2 - a13 * p3 + tmp1 / pz - tmp2;
+    const double b2 = a12 * p1 + p2 - a23 * p3 + tmp3 / pz + tmp4;
+    const double b3 = -(a13 * p1) - a23 * p2 + p3 + tmp5;
+    const double det = 1 + a12 * a12 - a13 * a13 - a23 * a23;
+    const double s11 = 1 - a23 * a23, s12 = -a12 + a13 * a23, s13 = a12 * a23 - a13;
+    const double s21 = a12 + a13 * a23, s22 = 1 - a13 * a13, s23 = -a23 - a13 * a12;
+    const double s31 = -(a12 * a23) - a13, s32 = -a23 + a12 * a13, s33 = 1 + a12 * a12;
+    p[1] = (s11 * b1 + s12 * b2 + s13 * b3) / det;
+    p[3] = (s21 * b1 + s22 * b2 + s23 * b3) / det;
+    p[5] = (s31 * b1 + s32 * b2 + s33 * b3) / det;
+    const double tmpgamma00 = gam + tau * qmcc * ez0;
+    const double tmpsq2 =
+        (tmpgamma00 - p[5]) * (tmpgamma00 - p[5]) - 1.0 - p[1] * p[1] - p[3] * p[3];
+    if (tmpsq2 > 0.0) pz = 0.5 * pz + 0.5 * sqrt(tmpsq2);
+  }
+}
+
+void orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass, double chrg,
+                      double gradient, double qmi) {
+  const lorentz_kick lz = {gradient, qmi};
+  for (int q = 0; q < n; q++) lorentz_update(&P(q, 0), 0.0, 0.0, 0.0, gam, tau, mass, chrg, &lz);
+}
+
 static void kick_common(double *pts, int n, const double *phi, const int mesh[3],
                         const double range[6], const double msize[3], double gam, double curr,
                         double tau, double mass, double chrg, double *eg, const double *wfield,
@@ -1584,48 +1638,7 @@ static void kick_common(double *pts, int n, const double *phi, const int mesh[3]
       P(q, 4) = P(q, 4) * xk / (-gam * betai);
       P(q, 0) = P(q, 0) * xk;
       P(q, 2) = P(q, 2) * xk;
-      const double xl = PC.Scxl, Clight = PC.Clight;
-      const double tmpscale2 = Clight * Clight * (double)1.0e-7f;
-      const double beta0 = sqrt(gam * gam - 1.0) / gam;
-      const double qmcc = chrg / mass;
-      const double ez0 = 0.0;
-      const double tmpgamma0 = gam + 0.5 * tau * qmcc * ez0;
-      const double ext4 = lz->gradient * (P(q, 2) * xl), ext5 = lz->gradient * (P(q, 0) * xl);
-      const double ex = tmpscale2 * exn + 0.0;
-      const double ey = tmpscale2 * eyn + 0.0;
-      const double ez = tmpscale2 * ezn + 0.0;
-      const double bx = -(beta0 / Clight * tmpscale2 * eyn) + ext4;
-      const double by = beta0 / Clight * tmpscale2 * exn + ext5;
-      const double bz = 0.0;
-      const double r7 = lz->qmi;
-      const double tmp12 = -tau * Clight * bz * r7 / 2;
-      const double tmp13 = tau * ex * r7 / 2;
-      const double tmp23 = tau * ey * r7 / 2;
-      const double tmp1 = tmpgamma0 * ex * tau * r7;
-      const double tmp2 = Clight * by * tau * r7;
-      const double tmp3 = tmpgamma0 * ey * tau * r7;
-      const double tmp4 = Clight * bx * tau * r7;
-      const double tmp5 = (ez0 * qmcc - ez * r7) * tau;
-      double pz = sqrt((gam - P(q, 5)) * (gam - P(q, 5)) - 1.0 - P(q, 1) * P(q, 1) -
-                       P(q, 3) * P(q, 3));
-      const double p1 = P(q, 1), p2 = P(q, 3), p3 = P(q, 5);
-      for (int ii = 1; ii <= 2; ii++) {
-        const double a12 = tmp12 / pz, a13 = tmp13 / pz, a23 = tmp23 / pz;
-        const double b1 = p1 - a12 * p2 - a13 * p3 + tmp1 / pz - tmp2;
-        const double b2 = a12 * p1 + p2 - a23 * p3 + tmp3 / pz + tmp4;
-        const double b3 = -(a13 * p1) - a23 * p2 + p3 + tmp5;
-        const double det = 1 + a12 * a12 - a13 * a13 - a23 * a23;
-        const double s11 = 1 - a23 * a23, s12 = -a12 + a13 * a23, s13 = a12 * a23 - a13;
-        const double s21 = a12 + a13 * a23, s22 = 1 - a13 * a13, s23 = -a23 - a13 * a12;
-        const double s31 = -(a12 * a23) - a13, s32 = -a23 + a12 * a13, s33 = 1 + a12 * a12;
-        P(q, 1) = (s11 * b1 + s12 * b2 + s13 * b3) / det;
-        P(q, 3) = (s21 * b1 + s22 * b2 + s23 * b3) / det;
-        P(q, 5) = (s31 * b1 + s32 * b2 + s33 * b3) / det;
-        const double tmpgamma00 = gam + tau * qmcc * ez0;
-        const double tmpsq2 = (tmpgamma00 - P(q, 5)) * (tmpgamma00 - P(q, 5)) - 1.0 -
-                              P(q, 1) * P(q, 1) - P(q, 3) * P(q, 3);
-        if (tmpsq2 > 0.0) pz = 0.5 * pz + 0.5 * sqrt(tmpsq2);
-      }
+      lorentz_update(&P(q, 0), exn, eyn, ezn, gam, tau, mass, chrg, lz);
       continue;
     }
     P(q, 0) = P(q, 0) * xk;
@@ -2310,8 +2323,8 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     double piperad = pipe_radius(e), piperad2 = piperad;
     if (bitype < 0) { free(rho); return -3; }
     const int lorentz = beam->flagmap == 2;
-    if (lorentz && (!(bitype == 0 || (bitype == 1 && e->val[1] <= 0.0)) || bcurr < 1.0e-10)) {
-      free(rho); /* Lorentz integrator: drifts and hard-edge quadrupoles, with space charge */
+    if (lorentz && !(bitype == 0 || (bitype == 1 && e->val[1] <= 0.0))) {
+      free(rho); /* Lorentz integrator: drifts and hard-edge quadrupoles */
       return -10;
     }
     orc_wake_elem(bitype, e->val);
@@ -2411,6 +2424,11 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
             free(wf);
           }
         }
+        if (lorentz && half == 1 && bcurr < 1.0e-10)
+          /* kick2 without current: scatter20 (BeamBunch.f90:3075-3531) */
+          orc_lorentz_nosc(beam->pts, beam->nlocal, -beam->refptcl[5], tau2, beam->mass,
+                           beam->charge, bitype == 1 ? e->val[0] : 0.0,
+                           beam->nlocal ? beam->pts[6] : 0.0);
         if (lorentz) {
           /* map1_BeamBunch(Bpts,z,tau2): drift2 by tau2/2 (AccSimulator.f90:1109-1116) */
           orc_drift2(beam->pts, beam->nlocal, beam->refptcl, tau2);

@@ -127,6 +127,8 @@ void orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const d
                const double msize[3], double gam, double curr, double tau, double mass,
                double chrg, double gradient, double qmi);
 void orc_drift2(double *pts, int n, double refptcl[6], double tau);
+void orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass, double chrg,
+                      double gradient, double qmi);
 /* read-in wakefield of type -41 elements (Data.f90:559-633,
  * AccSimulator.f90:959-978, 1273-1340, Field.f90:783-1001) */
 int orc_wake_set(const double *z, const double *ew, const double *epw, const double *eppw,

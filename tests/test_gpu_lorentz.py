@@ -53,3 +53,24 @@ def test_lorentz_fodo_matches_the_oracle(form, cols, tol):
     rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], cfg["mass"], cfg["freq"])
                        for i in range(len(recs))])
     assert worst(rows_g, rows_o, cols) <= tol
+
+
+def test_lorentz_without_current_matches_the_oracle():
+    """Zero current: the element's field alone (scatter20), FP64: rms
+    columns within 1e-10 of the oracle."""
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 74)
+    lat = beams.fodo(1)
+    rows_o = orc.run(lat, cfg["pts"], 0.0, cfg["mass"], cfg["charge"], cfg["freq"],
+                     cfg["refptcl"], cfg["grid"], flagmap=2)[0]
+    b = impz.Bunch(cfg["pts"], 0.0, cfg["mass"], cfg["charge"], cfg["freq"], cfg["refptcl"],
+                   cfg["grid"], form=impz.FORM_FP64, track_ids=False)
+    try:
+        b.set_integrator(2)
+        recs, zs = b.run(lat)
+        refs = b.run_reference()
+    finally:
+        b.close()
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], cfg["mass"], cfg["freq"])
+                       for i in range(len(recs))])
+    assert worst(rows_g, rows_o, RMS_COLS) <= 1e-10

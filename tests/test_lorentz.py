@@ -38,3 +38,17 @@ def test_lorentz_integrator_refuses_elements_outside_it():
         assert "-10" in str(e)
     else:
         raise AssertionError("a bend under the Lorentz integrator must be refused")
+
+
+def test_lorentz_integrator_without_current_converges_too():
+    """Zero current: kick2 is scatter20, the quadrupoles' field alone on the
+    stored coordinates (BeamBunch.f90:3075-3531)."""
+    cfg = beams.fodo_1e5(n=2000, seed=beams.SEED0 + 73)
+    gaps = []
+    for nseg in (4, 32):
+        lat = beams.fodo(1, nseg=nseg)
+        run = lambda fm: orc.run(lat, cfg["pts"], 0.0, cfg["mass"], cfg["charge"],  # noqa: E731
+                                 cfg["freq"], cfg["refptcl"], (16, 16, 32), flagmap=fm)[0]
+        r1, r2 = run(1), run(2)
+        gaps.append(max(abs(r2[-1, c] - r1[-1, c]) / abs(r1[-1, c]) for c in (7, 13)))
+    assert gaps[0] > 8 * gaps[1] and gaps[1] < 2e-3
