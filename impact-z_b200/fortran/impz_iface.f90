@@ -169,5 +169,201 @@
             import :: c_int, c_ptr
             type(c_ptr), value :: bunch
           end function
+
+          ! ---- library: the strings are NUL-terminated C strings
+          ! (c_f_pointer onto a character(kind=c_char) array to print them)
+          type(c_ptr) function impz_version() bind(C, name="impz_version")
+            import :: c_ptr
+          end function
+
+          type(c_ptr) function impz_error_string(code) bind(C, name="impz_error_string")
+            import :: c_int, c_ptr
+            integer(c_int), value :: code
+          end function
+
+          type(c_ptr) function impz_last_cuda_error() bind(C, name="impz_last_cuda_error")
+            import :: c_ptr
+          end function
+
+          ! ---- deck-level switches and bunch state between runs
+          ! Flagmap of the deck or of a -25 element (1 map, 2 Lorentz)
+          integer(c_int) function impz_set_integrator(bunch, flagmap) &
+              bind(C, name="impz_set_integrator")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: bunch
+            integer(c_int), value :: flagmap
+          end function
+
+          ! laser heater of a -52 element: Param(2), Param(3), Param(4)
+          integer(c_int) function impz_laser_heater(bunch, rsig, wavelength, ez) &
+              bind(C, name="impz_laser_heater")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), value :: rsig, wavelength, ez
+          end function
+
+          ! Current, Npt, Nptlocal, refptcl(1..6), z, device bytes
+          integer(c_int) function impz_bunch_info(bunch, info) bind(C, name="impz_bunch_info")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), intent(out) :: info(11)
+          end function
+
+          ! range and msize of the last space-charge step, as outpoint_Output writes
+          integer(c_int) function impz_bunch_geom(bunch, range, msize) &
+              bind(C, name="impz_bunch_geom")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), intent(out) :: range(6), msize(3)
+          end function
+
+          ! z of a restart from a checkpoint (inpoint_Output)
+          integer(c_int) function impz_bunch_set_z(bunch, z) bind(C, name="impz_bunch_set_z")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), value :: z
+          end function
+
+          integer(c_int) function impz_bunch_upload(bunch, pts, n, current, refptcl) &
+              bind(C, name="impz_bunch_upload")
+            import :: c_int, c_long_long, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), intent(in) :: pts(9, *)
+            integer(c_long_long), value :: n
+            real(c_double), value :: current
+            real(c_double), intent(in) :: refptcl(6)
+          end function
+
+          integer(c_long_long) function impz_bunch_footprint(n, nx, ny, nz, form, flags, &
+              nsteps) bind(C, name="impz_bunch_footprint")
+            import :: c_int, c_long_long
+            integer(c_long_long), value :: n
+            integer(c_int), value :: nx, ny, nz, form, flags, nsteps
+          end function
+
+          ! the bunch's cudaStream_t
+          type(c_ptr) function impz_bunch_stream(bunch) bind(C, name="impz_bunch_stream")
+            import :: c_ptr
+            type(c_ptr), value :: bunch
+          end function
+
+          integer(c_int) function impz_bunching(bunch, wavenumber, out) &
+              bind(C, name="impz_bunching")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), value :: wavenumber
+            real(c_double), intent(out) :: out(2)
+          end function
+
+          ! ---- whole-lattice runner: records and refptcl per record
+          integer(c_int) function impz_run_reference(bunch, refrec, maxrec, nrec) &
+              bind(C, name="impz_run_reference")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), intent(out) :: refrec(6, *)
+            integer(c_int), value :: maxrec
+            integer(c_int), intent(out) :: nrec
+          end function
+
+          integer(c_int) function impz_count_steps(elems, nelem) &
+              bind(C, name="impz_count_steps")
+            import :: c_int, impz_elem_t
+            type(impz_elem_t), intent(in) :: elems(*)
+            integer(c_int), value :: nelem
+          end function
+
+          integer(c_int) function impz_run_async(bunch, elems, nelem) &
+              bind(C, name="impz_run_async")
+            import :: c_int, c_ptr, impz_elem_t
+            type(c_ptr), value :: bunch
+            type(impz_elem_t), intent(in) :: elems(*)
+            integer(c_int), value :: nelem
+          end function
+
+          integer(c_int) function impz_run_fetch(bunch, recs, zs, maxrec, nrec) &
+              bind(C, name="impz_run_fetch")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), intent(out) :: recs(48, *), zs(*)
+            integer(c_int), value :: maxrec
+            integer(c_int), intent(out) :: nrec
+          end function
+
+          integer(c_int) function impz_run_begin(bunch, elems, nelem) &
+              bind(C, name="impz_run_begin")
+            import :: c_int, c_ptr, impz_elem_t
+            type(c_ptr), value :: bunch
+            type(impz_elem_t), intent(in) :: elems(*)
+            integer(c_int), value :: nelem
+          end function
+
+          integer(c_int) function impz_run_advance(bunch, budget, remaining) &
+              bind(C, name="impz_run_advance")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: bunch
+            integer(c_int), value :: budget
+            integer(c_int), intent(out) :: remaining
+          end function
+
+          ! launch shapes for this bunch: out = deposit blocks, push blocks,
+          ! z lines per block, ms per step
+          integer(c_int) function impz_autotune(bunch, nsteps, out) &
+              bind(C, name="impz_autotune")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            integer(c_int), value :: nsteps
+            real(c_double), intent(out) :: out(4)
+          end function
+
+          ! host RK6 linear map of one element (maplinear_*)
+          integer(c_int) function impz_maplinear(elem, zedge, t, tau, refpt, charge, mass, &
+              freq, xm) bind(C, name="impz_maplinear")
+            import :: c_int, c_double, impz_elem_t
+            type(impz_elem_t), intent(in) :: elem
+            real(c_double), value :: zedge, t, tau, charge, mass, freq
+            real(c_double), intent(inout) :: refpt(6)
+            real(c_double), intent(out) :: xm(6, 6)
+          end function
+
+          ! bytes per step of the step table a run uploads
+          integer(c_int) function impz_step_params_size() &
+              bind(C, name="impz_step_params_size")
+            import :: c_int
+          end function
+
+          ! ---- instrumentation
+          integer(c_int) function impz_profile_enable(bunch, on) &
+              bind(C, name="impz_profile_enable")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: bunch
+            integer(c_int), value :: on
+          end function
+
+          integer(c_int) function impz_profile_fetch(bunch, ms, launches) &
+              bind(C, name="impz_profile_fetch")
+            import :: c_int, c_long_long, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), intent(out) :: ms(7)
+            integer(c_long_long), intent(out) :: launches(7)
+          end function
+
+          integer(c_long_long) function impz_kernel_launches() &
+              bind(C, name="impz_kernel_launches")
+            import :: c_long_long
+          end function
+
+          ! ---- deposit into caller-owned device memory (no allocation):
+          ! x..pt and chgdens are device addresses, stream a cudaStream_t
+          integer(c_int) function impz_deposit_static(x, px, y, py, ph, pt, n, gam, piperad, &
+              piperad2, freq, weight, range, nx, ny, nz, chgdens, stream) &
+              bind(C, name="impz_deposit_static")
+            import :: c_int, c_long_long, c_double, c_ptr
+            type(c_ptr), value :: x, px, y, py, ph, pt
+            integer(c_long_long), value :: n
+            real(c_double), value :: gam, piperad, piperad2, freq, weight
+            real(c_double), intent(in) :: range(6)
+            integer(c_int), value :: nx, ny, nz
+            type(c_ptr), value :: chgdens, stream
+          end function
         end interface
       end module impz_iface
