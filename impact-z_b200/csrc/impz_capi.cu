@@ -388,6 +388,7 @@ AdvanceArgs advance_args(impz_bunch_t b, const StepParams* table, int fixed, int
   a.do_post = post;
   a.do_pre = pre;
   a.mom_index = mom_index;
+  a.wake_raw = b->run_wake ? b->wk_field + 3 * (size_t)b->nz : nullptr;
   return a;
 }
 
@@ -1318,7 +1319,9 @@ static int wake_alloc(impz_bunch_t b, int ntab) {
   CK(exact::prepare_wake());  // outside any stream capture
   const size_t tab_bytes = round_up((size_t)3 * (ntab > 0 ? ntab : 1) * sizeof(double), kAlign);
   const size_t line_bytes = round_up((size_t)3 * b->nz * sizeof(unsigned long long), kAlign);
-  const size_t bytes = tab_bytes + line_bytes + (size_t)3 * b->nz * sizeof(double);
+  // field: the kick1wake planes in grid units, then the raw planes that a
+  // Lorentz step's kick2wake interpolates
+  const size_t bytes = tab_bytes + line_bytes + (size_t)6 * b->nz * sizeof(double);
   // the stream may still read the previous buffers
   CK(cudaStreamSynchronize(b->stream));
   if (b->wk_mem && b->wk_ntab != ntab && ntab > 0) {

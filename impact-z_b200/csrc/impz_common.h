@@ -39,6 +39,27 @@ struct MapOp {
   double c[IMPZ_OPC];
 };
 
+// The external field (E, B) of a Lorentz-integrator step's element at the
+// kick's z (getfld_BeamLineElem, BeamLineElem.f90:827-867), as a function
+// of X, Y [m] and the particle's time T = phase + tg; E_x = E_y = 0 for all.
+//   LZ_NONE      drift (getfld_DriftTube): 0
+//   LZ_QUAD      hard-edge quadrupole, c0 = G: B = (G Y, G X, 0)
+//   LZ_QUAD_FRG  Enge fringe (getfldfrgAna2_Quadrupole), c = (G, G', G''):
+//                Bx = G Y - G''(Y^3 + 3 X^2 Y)/12, By = G X - G''(X^3 + 3 X Y^2)/12,
+//                Bz = G' X Y
+//   LZ_SOL       solenoid body or outside (getfld_Sol): B = (0, 0, c1)
+//   LZ_SOL_FRG   solenoid ramp, c0 = dBz/dz: B = (-c0/2 X, -c0/2 Y, c1)
+//   LZ_CONSTFOC  constant focusing (getfld_ConstFoc), c = (kx, ky, kz):
+//                Ez = kz T Scxl, Bx = -kx Y / c, By = ky X / c
+enum LzKind {
+  LZ_NONE = 0,
+  LZ_QUAD = 1,
+  LZ_QUAD_FRG = 2,
+  LZ_SOL = 3,
+  LZ_SOL_FRG = 4,
+  LZ_CONSTFOC = 5
+};
+
 struct MapProgram {
   int nops;
   int pad;
@@ -66,8 +87,10 @@ struct StepParams {
   int pad3;
   double wk_aa, wk_gg, wk_len;  // analytic wake: iris radius, gap, period (Param(13..15))
   int lorentz;         // the kick is the Lorentz integrator's (kick2/scatter2)
-  int pad4;
-  double lz_grad;      // its element's external field: quadrupole gradient (0: drift)
+  int lz_kind;         // LzKind of its element's external field
+  double lz_c[3];      // that field's coefficients at the kick's z (LzKind)
+  double lz_tg;        // refptcl(5) at the kick (scatter2's tg)
+  double lz_ez0;       // the field's Ez on axis at tg (scatter2's ez0)
 };
 
 #define IMPZ_MOMREC 48   // per recorded step: 44 raw values, npt, nlocal, current, spare
@@ -135,6 +158,7 @@ struct AdvanceArgs {
   int do_pre;               // apply steps[s].pre_next (+ conv1st of s+1 if range_next)
   int mom_index;            // record row for fixed_step launches
   int pad1;
+  const double* wake_raw;   // per-plane wake {Ex,Ey,Ez}[nz] of a Lorentz step (kick2wake), or null
 };
 
 struct DepositArgs {

@@ -899,6 +899,91 @@ void bend_exit_op(const Phys& P, const BendState& bs, const Species& sp, MapProg
                         bs.angB, bs.gamma0, sp, bs.qm0));
 }
 
+namespace {
+// getfldfrgAna2_Quadrupole (Quadrupole.f90:456-506): the Enge profile of a
+// quadrupole of gradient bb, effective length Param(3) and aperture Param(4)
+// at zz from its entrance, and its first two derivatives.
+void quad_enge(double bb, double efflen, double radius, double length, double zz, double& g,
+               double& gp, double& gpp) {
+  const double c1 = -0.00004, c2 = 4.518219;
+  const double dd = 2 * radius;
+  const double z10 = (length - efflen) / 2;
+  const double z20 = length - z10;
+  const double z3 = z10 + 1.5 * dd;
+  const double z4 = z20 - 1.5 * dd;
+  if (zz < z3 || zz > z4) {
+    const double tmpz = zz < z3 ? -(zz - z10) / dd : (zz - z20) / dd;
+    const double s1 = c1 + c2 * tmpz;
+    const double e1 = std::exp(s1);
+    const double one = 1.0 + e1;
+    g = bb / one;
+    const double s2 = zz < z3 ? -c2 / dd : c2 / dd;
+    const double tmp1 = e1 * s2;
+    gp = -bb * tmp1 / (one * one);
+    const double s3 = 0.0;
+    const double s4 = e1 * (s3 + s2 * s2);
+    gpp = bb * (-s4 / (one * one) + 2 * tmp1 * tmp1 / (one * one * one));
+  } else {
+    g = bb;
+    gp = 0.0;
+    gpp = 0.0;
+  }
+}
+
+// The external field of element e for a Lorentz kick at z (LzKind):
+// getfld_Quadrupole (Quadrupole.f90:369-402), getfld_ConstFoc
+// (ConstFoc.f90:297-322), getfld_Sol (Sol.f90:391-435) and no field for a
+// drift.  ez0 is its Ez on axis at time tg.  Returns false for an element
+// the Lorentz integrator does not carry here.
+bool lorentz_field(const Phys& P, const impz_elem_t& e, double zedge, double z, double tg,
+                   int& kind, double c[3], double& ez0) {
+  kind = LZ_NONE;
+  c[0] = c[1] = c[2] = 0.0;
+  ez0 = 0.0;
+  const double zz = z - zedge;
+  switch (e.type) {
+    case 0:
+      return true;
+    case 1:
+      if (e.val[1] <= 0.0) {
+        kind = LZ_QUAD;
+        c[0] = e.val[0];
+        return true;
+      }
+      // 0 < Param(3) <= 1e-5 reads G', G'' that nothing set
+      if (!(e.val[1] > 1.0e-5)) return false;
+      kind = LZ_QUAD_FRG;
+      quad_enge(e.val[0], e.val[1], e.val[2], e.length, zz, c[0], c[1], c[2]);
+      return true;
+    case 2:
+      kind = LZ_CONSTFOC;
+      c[0] = e.val[0];
+      c[1] = e.val[1];
+      c[2] = e.val[2];
+      ez0 = c[2] * tg * P.Scxl;
+      return true;
+    case 3: {
+      const double b0 = e.val[0], x02 = 2 * e.val[2];
+      kind = LZ_SOL;
+      if (zz >= 0.0 && zz < x02) {
+        kind = LZ_SOL_FRG;
+        c[0] = b0 / x02;
+        c[1] = c[0] * zz;
+      } else if (zz >= x02 && zz <= e.length - x02) {
+        c[1] = b0;
+      } else if (zz > e.length - x02 && zz <= e.length) {
+        kind = LZ_SOL_FRG;
+        c[0] = -b0 / x02;
+        c[1] = b0 + c[0] * (zz - (e.length - x02));
+      }
+      return true;
+    }
+    default:
+      return false;
+  }
+}
+}  // namespace
+
 // ---------------------------------------------------------------------
 int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double bcurr,
                     const Species& sp, double refptcl[6], double* zio, LoopState& csr,
@@ -912,7 +997,8 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     double gam, tau, rad;
     double csr_r0, csr_s0, csr_blen;
     double wk_aa, wk_gg, wk_len;
-    double lz_grad;
+    int lz_kind;
+    double lz_c[3], lz_tg, lz_ez0;
     double z;
     double ref[6];
   };
@@ -929,11 +1015,14 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     if (e.nseg < 1) return IMPZ_ERR_ARG;
     const int bnseg = e.nseg, bitype = e.type;
     double piperad = pipe_radius(e), piperad2 = piperad;
-    // the Lorentz integrator covers drifts and hard-edge quadrupoles, with
-    // space charge (kick2 carries the quadrupoles' focusing)
+    // the Lorentz integrator covers drifts, quadrupoles, constant focusing
+    // and solenoids, whose fields kick2 applies (lorentz_field)
     const bool lorentz = csr.flagmap == 2;
-    if (lorentz && !(bitype == 0 || (bitype == 1 && e.val[1] <= 0.0)))
-      return IMPZ_ERR_UNSUPPORTED;
+    if (lorentz) {
+      int kind;
+      double c[3], ez0;
+      if (!lorentz_field(P, e, z, z, 0.0, kind, c, ez0)) return IMPZ_ERR_UNSUPPORTED;
+    }
     // the wake switch of each element (AccSimulator.f90:865-875)
     if (bitype == 105 || bitype == 106) {
       csr.aawk = e.val[11];
@@ -991,8 +1080,13 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
             s.wk_len = csr.lengwk;
           }
           if (lorentz) {
+            // kick2_BeamBunch (BeamBunch.f90:2187-2508): the field at the
+            // kick's z and tg = refptcl(5); gamma0 += tau qmcc Ez0 after it
             s.lorentz = 1;
-            s.lz_grad = bitype == 1 ? e.val[0] : 0.0;
+            s.lz_tg = refptcl[4];
+            lorentz_field(P, e, zedge, z, s.lz_tg, s.lz_kind, s.lz_c, s.lz_ez0);
+            const double gam = -refptcl[5] + tau2 * (sp.charge / sp.mass) * s.lz_ez0;
+            refptcl[5] = -gam;
           }
         }
         if (lorentz) {
@@ -1052,7 +1146,10 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
       sp_.wk_gg = cur.wk_gg;
       sp_.wk_len = cur.wk_len;
       sp_.lorentz = cur.lorentz;
-      sp_.lz_grad = cur.lz_grad;
+      sp_.lz_kind = cur.lz_kind;
+      std::memcpy(sp_.lz_c, cur.lz_c, sizeof(sp_.lz_c));
+      sp_.lz_tg = cur.lz_tg;
+      sp_.lz_ez0 = cur.lz_ez0;
       if (cur.csr || cur.wake) out.has_wake = true;
       sp_.gam = cur.gam;
       sp_.tau = cur.tau;

@@ -649,30 +649,67 @@ __device__ __forceinline__ double moment_tail(double acc1, int lane) {
   return t;
 }
 
-// The Lorentz integrator's kick of a drift or hard-edge quadrupole
-// (scatter2_BeamBunch, BeamBunch.f90:2975-3065, the generic-element branch):
-// the space-charge field exn = Ex*gam, eyn = Ey*gam, ezn = Ez of the grid
-// times 1/(4 pi eps0) = c^2 1e-7 (a default-real literal there), its
-// magnetic part -beta0/c Ey, beta0/c Ex, the quadrupole's B = G (y, x, 0)
-// at the particle [m] (getfld_Quadrupole, Quadrupole.f90:369-402), and the
-// implicit momentum update iterated twice.  The on-axis Ez of these
-// elements is zero, so gamma0 does not change.
+// The Lorentz integrator's kick (scatter2_BeamBunch, BeamBunch.f90:
+// 2975-3065, the analytic-field branch): the space-charge field exn =
+// Ex*gam, eyn = Ey*gam, ezn = Ez of the grid times 1/(4 pi eps0) = c^2 1e-7
+// (a default-real literal there), its magnetic part -beta0/c Ey, beta0/c Ex,
+// the element's field at the particle, and the implicit momentum update
+// iterated twice.  The on-axis Ez0 at the reference time moves gamma0 by
+// tau qmcc Ez0 (the host carries that in the step table).
+//
+// The element's field at (X, Y) [m] and time T of one particle
+// (getfld_Quadrupole, Quadrupole.f90:369-402; getfld_Sol, Sol.f90:391-435;
+// getfld_ConstFoc, ConstFoc.f90:297-322; LzKind), in the reference's
+// expression forms; ez = E_z, b = B.
+__device__ __forceinline__ void lz_field(int kind, const double* __restrict__ c, double X,
+                                         double Y, double T, const Consts& k, double& ez,
+                                         double& bx, double& by, double& bz) {
+  ez = 0.0; bx = 0.0; by = 0.0; bz = 0.0;
+  if (kind == LZ_QUAD) {
+    bx = c[0] * Y;
+    by = c[0] * X;
+  } else if (kind == LZ_QUAD_FRG) {
+    bx = c[0] * Y - c[2] * (Y * Y * Y + 3 * (X * X) * Y) / 12;
+    by = c[0] * X - c[2] * (X * X * X + 3 * X * (Y * Y)) / 12;
+    bz = c[1] * X * Y;
+  } else if (kind == LZ_SOL) {
+    bz = c[1];
+  } else if (kind == LZ_SOL_FRG) {
+    bx = -(c[0] / 2 * X);
+    by = -(c[0] / 2 * Y);
+    bz = c[1];
+  } else if (kind == LZ_CONSTFOC) {
+    ez = c[2] * T * k.Scxl;
+    bx = -(c[0] * Y / k.Clight);
+    by = c[1] * X / k.Clight;
+  }
+}
+
+// scatter2's implicit Lorentz update (BeamBunch.f90:3019-3065) of one
+// particle in the z frame by the space-charge field (exn, eyn, ezn) [grid
+// units] plus the step's element field (lz_*) and scatter2wake's wake at
+// the particle (wx, wy, wz; BeamBunch.f90:5885-5887); with no current
+// (scatter20, BeamBunch.f90:3478-3531) the space-charge field is zero.
 __device__ __forceinline__ void lorentz_kick(Particle& p, double exn, double eyn, double ezn,
-                                             double gam, double tau, double grad,
-                                             const Consts& k) {
+                                             double gam, const StepParams* __restrict__ sp,
+                                             const Consts& k, double wx, double wy,
+                                             double wz) {
   const double xl = k.Scxl, Clight = k.Clight;
+  const double tau = sp->tau;
   const double tmpscale = Clight * Clight * 1.00000001168609742e-07;
   const double beta0 = sqrt(gam * gam - 1.0) / gam;
   const double qmcc = k.charge / k.mass;
-  const double ez0 = 0.0;
+  const double ez0 = sp->lz_ez0;
   const double tmpgamma0 = gam + 0.5 * tau * qmcc * ez0;
-  const double ext4 = grad * (p.y * xl), ext5 = grad * (p.x * xl);
-  const double ex = tmpscale * exn + 0.0;
-  const double ey = tmpscale * eyn + 0.0;
-  const double ez = tmpscale * ezn + 0.0;
+  double e3, ext4, ext5, ext6;
+  lz_field(sp->lz_kind, sp->lz_c, p.x * xl, p.y * xl, p.ph + sp->lz_tg, k, e3, ext4, ext5,
+           ext6);
+  const double ex = tmpscale * exn + 0.0 + wx;
+  const double ey = tmpscale * eyn + 0.0 + wy;
+  const double ez = tmpscale * ezn + e3 + wz;
   const double bx = -(beta0 / Clight * tmpscale * eyn) + ext4;
   const double by = beta0 / Clight * tmpscale * exn + ext5;
-  const double bz = 0.0;
+  const double bz = ext6;
   const double r7 = k.qmi;
   const double tmp12 = -tau * Clight * bz * r7 / 2;
   const double tmp13 = tau * ex * r7 / 2;
@@ -838,7 +875,16 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
           if (!LIGHT && sp->lorentz) {
             // scatter2_BeamBunch (BeamBunch.f90:2766-3065): the same way back
             // to the z frame, then the implicit Lorentz update
-            lorentz_kick(p[u], exn, eyn, ezn, gam, sp->tau, sp->lz_grad, a.k);
+            // scatter2wake: the wake's planes kx, kx+1 weighted by the
+            // gather cell's ef (BeamBunch.f90:5634-5636)
+            double wx = 0.0, wy = 0.0, wz = 0.0;
+            if ((sp->csr || sp->wake) && a.wake_raw) {
+              const double* w = a.wake_raw + (cg.kx - 1);
+              wx = w[0] * cg.ef + w[1] * (1.0 - cg.ef);
+              wy = w[nz] * cg.ef + w[nz + 1] * (1.0 - cg.ef);
+              wz = w[2 * nz] * cg.ef + w[2 * nz + 1] * (1.0 - cg.ef);
+            }
+            lorentz_kick(p[u], exn, eyn, ezn, gam, sp, a.k, wx, wy, wz);
           } else {
             p[u].px = p[u].px + txy * exn;
             p[u].py = p[u].py + txy * eyn;
@@ -850,7 +896,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
       // the element's field alone, on the stored coordinates
       // (BeamBunch.f90:3075-3531)
       if (!LIGHT && keep[u] && !kick && post && sp->lorentz)
-        lorentz_kick(p[u], 0.0, 0.0, 0.0, gam, sp->tau, sp->lz_grad, a.k);
+        lorentz_kick(p[u], 0.0, 0.0, 0.0, gam, sp, a.k, 0.0, 0.0, 0.0);
       if (keep[u] && post) apply_program<LIGHT>(p[u], progs[0]);
       if (keep[u]) {
         c[u].x = p[u].x; c[u].px = p[u].px; c[u].y = p[u].y;
@@ -1715,7 +1761,14 @@ __global__ void __launch_bounds__(256) k_wake_field(WakeArgs a) {
     const double ez = csr_node(k + 1, d, sp.csr_r0, zwkmin, hzw, sp.csr_blen, gam);
     a.wfield[k] = 0.0;
     a.wfield[nz + k] = 0.0;
-    a.wfield[2 * nz + k] = chrg * ez / tcon / mass / a.unit;
+    if (sp.lorentz) {  // kick2wake takes the wake as it is, per particle
+      a.wfield[2 * nz + k] = 0.0;
+      a.wfield[3 * nz + k] = 0.0;
+      a.wfield[4 * nz + k] = 0.0;
+      a.wfield[5 * nz + k] = ez;
+    } else {
+      a.wfield[2 * nz + k] = chrg * ez / tcon / mass / a.unit;
+    }
     return;
   }
   const double bet = sqrt(gam * gam - 1.0) / gam;
@@ -1735,6 +1788,15 @@ __global__ void __launch_bounds__(256) k_wake_field(WakeArgs a) {
   const double ezwake = scale * (-cz * hzw);
   const double exwake = scale * (cx * hzw);
   const double eywake = scale * (cy * hzw);
+  if (sp.lorentz) {  // kick2wake takes the wake as it is, per particle
+    a.wfield[k] = 0.0;
+    a.wfield[nz + k] = 0.0;
+    a.wfield[2 * nz + k] = 0.0;
+    a.wfield[3 * nz + k] = exwake;
+    a.wfield[4 * nz + k] = eywake;
+    a.wfield[5 * nz + k] = ezwake;
+    return;
+  }
   a.wfield[k] = chrg * exwake / xycon / mass / bet / gam / a.unit;
   a.wfield[nz + k] = chrg * eywake / xycon / mass / bet / gam / a.unit;
   a.wfield[2 * nz + k] = chrg * ezwake / tcon / mass / a.unit;

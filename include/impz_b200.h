@@ -129,8 +129,13 @@ int impz_wake_off(impz_bunch_t b);
 /* The integrator of the runs that follow (Flagmap of the deck, or a -25
  * element): 1 the linear map integrator, 2 the Lorentz integrator
  * (drift2 half steps around kick2/scatter2, BeamBunch.f90:467-509,
- * 2187-3071), here for drifts and hard-edge quadrupoles with space
- * charge; a run with any other element under it is IMPZ_ERR_UNSUPPORTED. */
+ * 2187-3071, or scatter20 without current), here for drifts, quadrupoles
+ * (hard edge, or the Enge fringe of getfldfrgAna2_Quadrupole when
+ * Param(3) > 1e-5), constant focusing and solenoids (getfld_Quadrupole,
+ * getfld_ConstFoc, getfld_Sol), with a read-in or CSR wake applied as
+ * kick2wake does (BeamBunch.f90:5048-5938); a run with any other element
+ * under it, or a quadrupole with 0 < Param(3) <= 1e-5 (whose field reads
+ * unset derivatives there), is IMPZ_ERR_UNSUPPORTED. */
 int impz_set_integrator(impz_bunch_t b, int flagmap);
 /* sizeof(StepParams): the bytes per step of the step table a run uploads. */
 int impz_step_params_size(void);

@@ -1464,11 +1464,18 @@ void orc_kick1(double *pts, int n, const double *phi, const int mesh[3],
  * field added to the node fields before the gather (BeamBunch.f90:5015-5033);
  * wfield = {dEx[nz], dEy[nz], dEz[nz]} in grid-field units (orc_wake_field),
  * NULL for none. */
-/* The Lorentz integrator's kick of a drift or hard-edge quadrupole
- * (scatter2_BeamBunch, BeamBunch.f90:2510-3071, the generic-element
- * branch): gradient = Param(2) of a quadrupole, 0 for a drift; qmi =
- * Pts1(7) */
-typedef struct { double gradient, qmi; } lorentz_kick;
+/* The Lorentz integrator's kick (kick2/scatter2_BeamBunch, BeamBunch.f90:
+ * 2187-3071, the analytic-field branch) in element elem = {type, Param(2),
+ * Param(3), Param(4), length, zedge}: 0 drift, 1 quadrupole, 2 constant
+ * focusing, 3 solenoid; z = the kick's position, tg = refptcl(5) there,
+ * qmi = Pts1(7) */
+typedef struct {
+  int type;
+  double val[3], length, zedge, z, tg, qmi;
+  /* kick2wake (BeamBunch.f90:5048-5410): the per-plane wake {Ex, Ey,
+   * Ez}[nz] as the wake routines return it, or NULL */
+  const double *wraw;
+} lorentz_kick;
 
 static void kick_common(double *pts, int n, const double *phi, const int mesh[3],
                         const double range[6], const double msize[3], double gam, double curr,
@@ -1482,33 +1489,132 @@ void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
   kick_common(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, eg, wfield, NULL);
 }
 
-/* kick2_BeamBunch (BeamBunch.f90:2187-2508) with scatter2 for a drift or a
- * hard-edge quadrupole of the given gradient, one rank, Flagbc=1 */
-void orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const double range[6],
-               const double msize[3], double gam, double curr, double tau, double mass,
-               double chrg, double gradient, double qmi) {
-  const lorentz_kick lz = {gradient, qmi};
-  kick_common(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, NULL, NULL, &lz);
+static lorentz_kick lz_make(const double elem[6], double z, double tg, double qmi) {
+  lorentz_kick lz;
+  lz.type = (int)elem[0];
+  lz.val[0] = elem[1];
+  lz.val[1] = elem[2];
+  lz.val[2] = elem[3];
+  lz.length = elem[4];
+  lz.zedge = elem[5];
+  lz.z = z;
+  lz.tg = tg;
+  lz.qmi = qmi;
+  lz.wraw = NULL;
+  return lz;
 }
 
-/* the implicit Lorentz update of scatter2/scatter20 (BeamBunch.f90:3023-3065
- * and 3491-3531) for a space-charge field (exn, eyn, ezn) [grid units] and a
- * quadrupole's B = G (y, x, 0) at (x, y) [m]; p = one particle's Pts1 */
+/* getfldfrgAna2_Quadrupole (Quadrupole.f90:456-506): the Enge profile of
+ * the gradient at zz from the quadrupole's entrance and its first two
+ * derivatives */
+static void quad_ana2(const lorentz_kick *lz, double zz, double *bgrad, double *bgradp,
+                      double *bgradpp) {
+  const double c1 = -0.00004, c2 = 4.518219;
+  const double bb = lz->val[0];
+  const double dd = 2 * lz->val[2];
+  const double z10 = (lz->length - lz->val[1]) / 2;
+  const double z20 = lz->length - z10;
+  const double z3 = z10 + 1.5 * dd;
+  const double z4 = z20 - 1.5 * dd;
+  double tmpz, s1, s2, s3, s4, tmp1, q;
+  if (zz < z3) {
+    tmpz = -(zz - z10) / dd;
+    s1 = c1 + c2 * tmpz;
+    *bgrad = bb / (1.0 + exp(s1));
+    s2 = -c2 / dd;
+  } else if (zz > z4) {
+    tmpz = (zz - z20) / dd;
+    s1 = c1 + c2 * tmpz;
+    *bgrad = bb / (1.0 + exp(s1));
+    s2 = c2 / dd;
+  } else {
+    *bgrad = bb;
+    *bgradp = 0.0;
+    *bgradpp = 0.0;
+    return;
+  }
+  tmp1 = exp(s1) * s2;
+  q = 1.0 + exp(s1);
+  *bgradp = -bb * tmp1 / (q * q);
+  s3 = 0.0;
+  s4 = exp(s1) * (s3 + s2 * s2);
+  *bgradpp = bb * (-s4 / (q * q) + 2 * tmp1 * tmp1 / (q * q * q));
+}
+
+/* getfld_BeamLineElem (BeamLineElem.f90:827-867) at pos = (x [m], y [m],
+ * z [m], t) for the elements above: getfld_DriftTube (DriftTube.f90:
+ * 290-305), getfld_Quadrupole (Quadrupole.f90:369-402), getfld_ConstFoc
+ * (ConstFoc.f90:297-322, with its placeholder qmcc = gambetz = 1) and
+ * getfld_Sol (Sol.f90:391-435); f = (Ex, Ey, Ez, Bx, By, Bz) */
+static void lz_getfld(const lorentz_kick *lz, const double pos[4], double f[6]) {
+  for (int i = 0; i < 6; i++) f[i] = 0.0;
+  const double zz = pos[2] - lz->zedge;
+  if (lz->type == 1) {
+    double bgrad = lz->val[0], bgradp = 0.0, bgradpp = 0.0;
+    if (lz->val[1] > 1.0e-5) quad_ana2(lz, zz, &bgrad, &bgradp, &bgradpp);
+    if (lz->val[1] > 0.0) {
+      f[3] = bgrad * pos[1] -
+             bgradpp * (pos[1] * pos[1] * pos[1] + 3 * (pos[0] * pos[0]) * pos[1]) / 12;
+      f[4] = bgrad * pos[0] -
+             bgradpp * (pos[0] * pos[0] * pos[0] + 3 * pos[0] * (pos[1] * pos[1])) / 12;
+      f[5] = bgradp * pos[0] * pos[1];
+    } else {
+      f[3] = bgrad * pos[1];
+      f[4] = bgrad * pos[0];
+    }
+  } else if (lz->type == 2) {
+    const double qmcc = 1.0, gambetz = 1.0, pz = gambetz;
+    f[2] = lz->val[2] * pos[3] * pz * pz * pz * PC.Scxl / qmcc;
+    f[3] = -(lz->val[0] * pos[1] * pz / qmcc / PC.Clight);
+    f[4] = lz->val[1] * pos[0] * pz / qmcc / PC.Clight;
+  } else if (lz->type == 3) {
+    const double x0 = lz->val[2], x02 = 2 * x0, b0 = lz->val[0];
+    if (zz >= 0.0 && zz < x02) {
+      const double bb = b0 / x02, bgrad = bb;
+      f[3] = -(bgrad / 2 * pos[0]);
+      f[4] = -(bgrad / 2 * pos[1]);
+      f[5] = bb * zz;
+    } else if (zz >= x02 && zz <= lz->length - x02) {
+      f[5] = b0;
+    } else if (zz > lz->length - x02 && zz <= lz->length) {
+      const double bb = -b0 / x02, bgrad = bb, zshift = lz->length - x02;
+      f[3] = -(bgrad / 2 * pos[0]);
+      f[4] = -(bgrad / 2 * pos[1]);
+      f[5] = b0 + bb * (zz - zshift);
+    }
+  }
+}
+
+/* scatter2's ez0: the element's Ez on axis at the reference time */
+static double lz_ez0(const lorentz_kick *lz) {
+  const double pos[4] = {0.0, 0.0, lz->z, lz->tg};
+  double f[6];
+  lz_getfld(lz, pos, f);
+  return f[2];
+}
+
+/* the implicit Lorentz update of scatter2/scatter20 (BeamBunch.f90:3019-3065
+ * and 3478-3531) for a space-charge field (exn, eyn, ezn) [grid units] and
+ * the element's field at the particle, plus scatter2wake's wake (wx, wy, wz)
+ * at the particle (BeamBunch.f90:5634-5636, 5885-5887); p = one particle's
+ * Pts1 */
 static void lorentz_update(double *p, double exn, double eyn, double ezn, double gam, double tau,
-                           double mass, double chrg, const lorentz_kick *lz) {
+                           double mass, double chrg, double ez0, const lorentz_kick *lz,
+                           double wx, double wy, double wz) {
   const double xl = PC.Scxl, Clight = PC.Clight;
   const double tmpscale2 = Clight * Clight * (double)1.0e-7f;
   const double beta0 = sqrt(gam * gam - 1.0) / gam;
   const double qmcc = chrg / mass;
-  const double ez0 = 0.0;
   const double tmpgamma0 = gam + 0.5 * tau * qmcc * ez0;
-  const double ext4 = lz->gradient * (p[2] * xl), ext5 = lz->gradient * (p[0] * xl);
-  const double ex = tmpscale2 * exn + 0.0;
-  const double ey = tmpscale2 * eyn + 0.0;
-  const double ez = tmpscale2 * ezn + 0.0;
-  const double bx = -(beta0 / Clight * tmpscale2 * eyn) + ext4;
-  const double by = beta0 / Clight * tmpscale2 * exn + ext5;
-  const double bz = 0.0;
+  const double pos[4] = {p[0] * xl, p[2] * xl, lz->z, p[4] + lz->tg};
+  double extfld[6];
+  lz_getfld(lz, pos, extfld);
+  const double ex = tmpscale2 * exn + extfld[0] + wx;
+  const double ey = tmpscale2 * eyn + extfld[1] + wy;
+  const double ez = tmpscale2 * ezn + extfld[2] + wz;
+  const double bx = -(beta0 / Clight * tmpscale2 * eyn) + extfld[3];
+  const double by = beta0 / Clight * tmpscale2 * exn + extfld[4];
+  const double bz = extfld[5];
   const double r7 = lz->qmi;
   const double tmp12 = -tau * Clight * bz * r7 / 2;
   const double tmp13 = tau * ex * r7 / 2;
@@ -1539,10 +1645,30 @@ static void lorentz_update(double *p, double exn, double eyn, double ezn, double
   }
 }
 
-void orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass, double chrg,
-                      double gradient, double qmi) {
-  const lorentz_kick lz = {gradient, qmi};
-  for (int q = 0; q < n; q++) lorentz_update(&P(q, 0), 0.0, 0.0, 0.0, gam, tau, mass, chrg, &lz);
+/* kick2_BeamBunch (BeamBunch.f90:2187-2508) with scatter2, one rank,
+ * Flagbc=1, or kick2wake with scatter2wake when wraw (the per-plane wake
+ * {Ex, Ey, Ez}[nz] of the wake routines) is given; returns the new
+ * gamma0 = gam + tau qmcc ez0 (refptcl(6) = -it) */
+double orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const double range[6],
+                 const double msize[3], double gam, double curr, double tau, double mass,
+                 double chrg, const double elem[6], double z, double tg, double qmi,
+                 const double *wraw) {
+  lorentz_kick lz = lz_make(elem, z, tg, qmi);
+  lz.wraw = wraw;
+  kick_common(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, NULL, NULL, &lz);
+  return gam + tau * (chrg / mass) * lz_ez0(&lz);
+}
+
+/* kick2_BeamBunch without current: scatter20 (BeamBunch.f90:3075-3531),
+ * the element's field alone on the stored coordinates; returns the new
+ * gamma0 */
+double orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass, double chrg,
+                        const double elem[6], double z, double tg, double qmi) {
+  const lorentz_kick lz = lz_make(elem, z, tg, qmi);
+  const double ez0 = lz_ez0(&lz);
+  for (int q = 0; q < n; q++)
+    lorentz_update(&P(q, 0), 0.0, 0.0, 0.0, gam, tau, mass, chrg, ez0, &lz, 0.0, 0.0, 0.0);
+  return gam + tau * (chrg / mass) * ez0;
 }
 
 static void kick_common(double *pts, int n, const double *phi, const int mesh[3],
@@ -1550,6 +1676,7 @@ static void kick_common(double *pts, int n, const double *phi, const int mesh[3]
                         double tau, double mass, double chrg, double *eg, const double *wfield,
                         const lorentz_kick *lz) {
   if (curr < 1.0e-20) return;
+  const double lz_ez0v = lz ? lz_ez0(lz) : 0.0;
   const int nx = mesh[0], ny = mesh[1], nz = mesh[2];
   const size_t G = (size_t)nx * ny * nz;
   double *egx = eg ? eg : (double *)malloc(3 * G * sizeof(double));
@@ -1631,14 +1758,22 @@ static void kick_common(double *pts, int n, const double *phi, const int mesh[3]
     double tmpsq = 1.0 - rcpgammai * rcpgammai * ((1 + P(q, 1) * P(q, 1)) + P(q, 3) * P(q, 3));
     double betai = sqrt(tmpsq);
     if (lz) {
-      /* back from t to z (BeamBunch.f90:2766-2771), then the external field
-       * at (x, y) [m] (getfld_Quadrupole, Quadrupole.f90:369-402: B = G (y,
-       * x, 0); none in a drift) and the implicit Lorentz update iterated
-       * twice (BeamBunch.f90:3023-3065) */
+      /* scatter2wake's wake at the particle: linear in z over the gather
+       * cell's planes (BeamBunch.f90:5634-5636) */
+      double wx = 0.0, wy = 0.0, wz = 0.0;
+      if (lz->wraw) {
+        const double *w = lz->wraw;
+        wx = w[kx - 1] * ef + w[kx1 - 1] * (1.0 - ef);
+        wy = w[nz + kx - 1] * ef + w[nz + kx1 - 1] * (1.0 - ef);
+        wz = w[2 * nz + kx - 1] * ef + w[2 * nz + kx1 - 1] * (1.0 - ef);
+      }
+      /* back from t to z (BeamBunch.f90:2766-2771), then the element's field
+       * at the particle and the implicit Lorentz update iterated twice
+       * (BeamBunch.f90:3019-3065) */
       P(q, 4) = P(q, 4) * xk / (-gam * betai);
       P(q, 0) = P(q, 0) * xk;
       P(q, 2) = P(q, 2) * xk;
-      lorentz_update(&P(q, 0), exn, eyn, ezn, gam, tau, mass, chrg, lz);
+      lorentz_update(&P(q, 0), exn, eyn, ezn, gam, tau, mass, chrg, lz_ez0v, lz, wx, wy, wz);
       continue;
     }
     P(q, 0) = P(q, 0) * xk;
@@ -1890,12 +2025,12 @@ void orc_wake_line(const double *pts, int n, int nz, const double range[6], doub
  * d is recvdensz (AccSimulator.f90:1297-1322).  out = {dEx, dEy, dEz}[nz]. */
 static void wake_field(int nz, const double *densz, const double *xsum, const double *ysum,
                        const double range[6], double gam, double curr, int npt, double mass,
-                       double chrg, int analytic, double *out);
+                       double chrg, int analytic, double *out, double *raw);
 
 void orc_wake_field(int nz, const double *densz, const double *xsum, const double *ysum,
                     const double range[6], double gam, double curr, int npt, double mass,
                     double chrg, double *out) {
-  wake_field(nz, densz, xsum, ysum, range, gam, curr, npt, mass, chrg, 0, out);
+  wake_field(nz, densz, xsum, ysum, range, gam, curr, npt, mass, chrg, 0, out, NULL);
 }
 
 /* The analytic wake of wakefield_FieldQuant (Field.f90:590-782), the short-
@@ -1913,7 +2048,7 @@ void orc_wake_field_analytic(int nz, const double *densz, const double *xsum,
   WK.aa = aa;
   WK.gg = gg;
   WK.leng = leng;
-  wake_field(nz, densz, xsum, ysum, range, gam, curr, npt, mass, chrg, 1, out);
+  wake_field(nz, densz, xsum, ysum, range, gam, curr, npt, mass, chrg, 1, out, NULL);
   WK.aa = s_aa;
   WK.gg = s_gg;
   WK.leng = s_leng;
@@ -1946,9 +2081,11 @@ static double analytic_wt(const analytic_wake *w, int j, double hz) {
   return w->coef1 * (1.0 - (1. + sqrt(zz / w->z0t)) * exp(-sqrt(zz / w->z0t)));
 }
 
+/* out: the per-plane field in grid-field units (kick1wake); raw (or NULL):
+ * the wake itself, {Ex, Ey, Ez}[nz], as kick2wake takes it */
 static void wake_field(int nz, const double *densz, const double *xsum, const double *ysum,
                        const double range[6], double gam, double curr, int npt, double mass,
-                       double chrg, int analytic, double *out) {
+                       double chrg, int analytic, double *out, double *raw) {
   const analytic_wake aw = analytic ? analytic_of(WK.aa, WK.gg, WK.leng) : (analytic_wake){0};
   const int tr = analytic || WK.transverse;
   const double scale = analytic ? 1.0 : WK.scale;
@@ -2005,6 +2142,11 @@ static void wake_field(int nz, const double *densz, const double *xsum, const do
     out[k] = chrg * exwake / xycon / mass / bet / gam;
     out[nz + k] = chrg * eywake / xycon / mass / bet / gam;
     out[2 * nz + k] = chrg * ezwake / tcon / mass;
+    if (raw) {
+      raw[k] = exwake;
+      raw[nz + k] = eywake;
+      raw[2 * nz + k] = ezwake;
+    }
   }
   free(d);
 }
@@ -2223,9 +2365,20 @@ void orc_csr_wake(int nx, double r0, double ptmin, double hx, double blength,
  * addition (BeamBunch.f90:5015-5033): densz from orc_wake_line, s0 the
  * distance of the step from the bend entrance, blen the bend length; out =
  * {0, 0, dEz}[nz]. */
+static void csr_field(int nz, const double *densz, const double range[6], double gam,
+                      double curr, int npt, double mass, double chrg, double r0, double s0,
+                      double blen, double *out, double *raw);
+
 void orc_csr_field(int nz, const double *densz, const double range[6], double gam,
                    double curr, int npt, double mass, double chrg, double r0, double s0,
                    double blen, double *out) {
+  csr_field(nz, densz, range, gam, curr, npt, mass, chrg, r0, s0, blen, out, NULL);
+}
+
+/* raw (or NULL): the wake itself, {0, 0, Ez}[nz], as kick2wake takes it */
+static void csr_field(int nz, const double *densz, const double range[6], double gam,
+                      double curr, int npt, double mass, double chrg, double r0, double s0,
+                      double blen, double *out, double *raw) {
   double *d = (double *)malloc(2 * (size_t)nz * sizeof(double));
   double *ez = d + nz;
   double hzwake = (range[5] - range[4]) / (nz - 1);
@@ -2251,6 +2404,11 @@ void orc_csr_field(int nz, const double *densz, const double range[6], double ga
     out[k] = 0.0;
     out[nz + k] = 0.0;
     out[2 * nz + k] = chrg * ez[k] / tcon / mass;
+    if (raw) {
+      raw[k] = 0.0;
+      raw[nz + k] = 0.0;
+      raw[2 * nz + k] = ez[k];
+    }
   }
   free(d);
 }
@@ -2323,10 +2481,15 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     double piperad = pipe_radius(e), piperad2 = piperad;
     if (bitype < 0) { free(rho); return -3; }
     const int lorentz = beam->flagmap == 2;
-    if (lorentz && !(bitype == 0 || (bitype == 1 && e->val[1] <= 0.0))) {
-      free(rho); /* Lorentz integrator: drifts and hard-edge quadrupoles */
+    /* Lorentz integrator: drifts, quadrupoles (not 0 < Param(3) <= 1e-5,
+     * where getfld_Quadrupole reads G', G'' it never set), constant
+     * focusing and solenoids */
+    if (lorentz && !(bitype == 0 || bitype == 2 || bitype == 3 ||
+                     (bitype == 1 && (e->val[1] <= 0.0 || e->val[1] > 1.0e-5)))) {
+      free(rho);
       return -10;
     }
+    const double lz_elem[6] = {(double)bitype, e->val[0], e->val[1], e->val[2], blength, z};
     orc_wake_elem(bitype, e->val);
     if (bitype == 4) { piperad = 100.0; piperad2 = 100.0; }
     double tau1 = 0.0;
@@ -2396,28 +2559,31 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
             }
             if (flagcsr) { /* AccSimulator.f90:1344-1390: replaces any read-in wake */
               const int nz = mesh[2];
-              wf = (double *)calloc(6 * (size_t)nz, sizeof(double));
+              wf = (double *)calloc(9 * (size_t)nz, sizeof(double));
               double *line = wf + 3 * (size_t)nz;
               orc_wake_line(beam->pts, beam->nlocal, nz, range, line, line + nz,
                             line + 2 * (size_t)nz);
               const double s0 = bitype == 4 ? z - beam->zbleng : z - beam->zbleng + beam->sentr;
-              orc_csr_field(nz, line, range, -beam->refptcl[5], beam->current, beam->npt,
-                            beam->mass, beam->charge, beam->r0, s0,
-                            bitype == 4 ? blength : beam->bendlencsr, wf);
+              csr_field(nz, line, range, -beam->refptcl[5], beam->current, beam->npt,
+                        beam->mass, beam->charge, beam->r0, s0,
+                        bitype == 4 ? blength : beam->bendlencsr, wf, wf + 6 * (size_t)nz);
             } else if (WK.flag) { /* AccSimulator.f90:1273-1340 */
               const int nz = mesh[2];
-              wf = (double *)malloc(6 * (size_t)nz * sizeof(double));
+              wf = (double *)malloc(9 * (size_t)nz * sizeof(double));
               double *line = wf + 3 * (size_t)nz;
               orc_wake_line(beam->pts, beam->nlocal, nz, range, line, line + nz,
                             line + 2 * (size_t)nz);
               wake_field(nz, line, line + nz, line + 2 * (size_t)nz, range, -beam->refptcl[5],
-                         beam->current, beam->npt, beam->mass, beam->charge, !WK.read, wf);
+                         beam->current, beam->npt, beam->mass, beam->charge, !WK.read, wf,
+                         wf + 6 * (size_t)nz);
             }
             orc_cvbkforth1st(beam->pts, beam->nlocal, beam->refptcl);
             if (lorentz)
-              orc_kick2(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],
-                        beam->current, tau2, beam->mass, beam->charge,
-                        bitype == 1 ? e->val[0] : 0.0, beam->nlocal ? beam->pts[6] : 0.0);
+              beam->refptcl[5] = -orc_kick2(beam->pts, beam->nlocal, rho, mesh, range, msize,
+                                            -beam->refptcl[5], beam->current, tau2, beam->mass,
+                                            beam->charge, lz_elem, z, beam->refptcl[4],
+                                            beam->nlocal ? beam->pts[6] : 0.0,
+                                            wf ? wf + 6 * (size_t)mesh[2] : NULL);
             else
               orc_kick1w(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],
                          beam->current, tau2, beam->mass, beam->charge, NULL, wf);
@@ -2426,9 +2592,10 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
         }
         if (lorentz && half == 1 && bcurr < 1.0e-10)
           /* kick2 without current: scatter20 (BeamBunch.f90:3075-3531) */
-          orc_lorentz_nosc(beam->pts, beam->nlocal, -beam->refptcl[5], tau2, beam->mass,
-                           beam->charge, bitype == 1 ? e->val[0] : 0.0,
-                           beam->nlocal ? beam->pts[6] : 0.0);
+          beam->refptcl[5] = -orc_lorentz_nosc(beam->pts, beam->nlocal, -beam->refptcl[5], tau2,
+                                               beam->mass, beam->charge, lz_elem, z,
+                                               beam->refptcl[4],
+                                               beam->nlocal ? beam->pts[6] : 0.0);
         if (lorentz) {
           /* map1_BeamBunch(Bpts,z,tau2): drift2 by tau2/2 (AccSimulator.f90:1109-1116) */
           orc_drift2(beam->pts, beam->nlocal, beam->refptcl, tau2);

@@ -123,12 +123,16 @@ void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
                 const double range[6], const double msize[3], double gam,
                 double curr, double tau, double mass, double chrg, double *eg,
                 const double *wfield);
-void orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const double range[6],
-               const double msize[3], double gam, double curr, double tau, double mass,
-               double chrg, double gradient, double qmi);
+/* elem = {type, Param(2), Param(3), Param(4), length, zedge}; z and tg =
+ * refptcl(5) at the kick; wraw = the per-plane wake {Ex, Ey, Ez}[nz] of
+ * kick2wake or NULL; both return the new gamma0 */
+double orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const double range[6],
+                 const double msize[3], double gam, double curr, double tau, double mass,
+                 double chrg, const double elem[6], double z, double tg, double qmi,
+                 const double *wraw);
 void orc_drift2(double *pts, int n, double refptcl[6], double tau);
-void orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass, double chrg,
-                      double gradient, double qmi);
+double orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass, double chrg,
+                        const double elem[6], double z, double tg, double qmi);
 /* read-in wakefield of type -41 elements (Data.f90:559-633,
  * AccSimulator.f90:959-978, 1273-1340, Field.f90:783-1001) */
 int orc_wake_set(const double *z, const double *ew, const double *epw, const double *eppw,

@@ -3,7 +3,9 @@ around the kick2/scatter2 Lorentz kick, BeamBunch.f90:467-509, 2187-3071)
 through the C ABI against the oracle, on the proton FODO lattice with
 space charge: rms columns of every record within 1e-8 (FP64) and 1e-5
 (FP32 form), z exact; the run differs from the map integrator's by far more
-than that."""
+than that.  A lattice of the other elements kick2 carries (Enge-fringe
+quadrupole, ramped solenoid, constant focusing) is held to the same bounds,
+with the reference particle exact."""
 import numpy as np
 import pytest
 
@@ -74,3 +76,88 @@ def test_lorentz_without_current_matches_the_oracle():
     rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], cfg["mass"], cfg["freq"])
                        for i in range(len(recs))])
     assert worst(rows_g, rows_o, RMS_COLS) <= 1e-10
+
+
+def element_lattice():
+    """Drift, Enge-fringe quadrupole, ramped solenoid, constant focusing with
+    Ez (which moves gamma0) and a hard-edge quadrupole under kick2."""
+    return [impz.elem(0, 0.1, 4, 1, [1.0]),
+            impz.elem(1, 0.2, 8, 1, [20.0, 0.1, 0.01]),
+            impz.elem(3, 0.3, 8, 1, [0.5, 0.0, 0.03]),
+            impz.elem(2, 0.2, 4, 1, [6e9, 9e9, 1e-3, 1.0]),
+            impz.elem(1, 0.1, 4, 1, [-20.0, 0.0, 1.0])]
+
+
+@pytest.mark.parametrize("current,form,cols,tol", [
+    (0.030, impz.FORM_FP64, RMS_COLS, 1e-8),
+    (0.030, impz.FORM_FP32CONV, [7, 9, 11, 13, 15, 17, 19, 21, 23], 1e-5),
+    (0.0, impz.FORM_FP64, RMS_COLS, 1e-10)])
+def test_lorentz_element_fields_match_the_oracle(current, form, cols, tol):
+    """The element fields of getfld_Quadrupole (Enge fringe), getfld_Sol
+    (ramps and body) and getfld_ConstFoc, and gamma0's change by Ez0, on the
+    GPU as in the oracle; the reference particle of every record equal."""
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 79)
+    lat = element_lattice()
+    rows_o, _, beam = orc.run(lat, cfg["pts"], current, cfg["mass"], cfg["charge"], cfg["freq"],
+                              cfg["refptcl"], cfg["grid"], flagmap=2)
+    b = impz.Bunch(cfg["pts"], current, cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=form, track_ids=False)
+    try:
+        b.set_integrator(2)
+        recs, zs = b.run(lat)
+        refs = b.run_reference()
+    finally:
+        b.close()
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    np.testing.assert_array_equal(refs[-1], np.array(beam.refptcl[:]))
+    assert refs[-1][5] != cfg["refptcl"][5]  # Ez0 of the constant focusing
+    rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], cfg["mass"], cfg["freq"])
+                       for i in range(len(recs))])
+    assert worst(rows_g, rows_o, cols) <= tol
+
+
+@pytest.mark.parametrize("form,cols,tol", [
+    (impz.FORM_FP64, RMS_COLS, 1e-8),
+    (impz.FORM_FP32CONV, [7, 9, 11, 13, 15, 17, 19, 21, 23], 1e-5)])
+def test_lorentz_read_in_wake_matches_the_oracle(form, cols, tol):
+    """kick2wake/scatter2wake (BeamBunch.f90:5048-5938): under the Lorentz
+    integrator the wake kernel leaves the node fields alone and hands the
+    raw per-plane wake to the push, which interpolates it at each particle
+    and adds it after the space-charge scaling."""
+    from test_wake import synthetic_table
+    cur = 1.3
+    pts, ref = beams.gaussian_bunch(20_000, seed=beams.SEED0 + 82, mass=beams.ELECTRON_MASS_EV,
+                                    charge=-1.0, ekin=98.169272e6, current=cur, freq=1.3e9,
+                                    sig_x=0.5e-3, sig_y=0.5e-3, sig_xp=0.05e-3,
+                                    sig_yp=0.05e-3, sig_phase_deg=1.0, sig_e=50e3)
+    scxl = 2.99792458e8 / (2 * np.pi * 1.3e9)
+    pts = pts.copy()
+    pts[:, 0] += 0.5e-3 / scxl
+    pts[:, 2] += 0.3e-3 / scxl
+    lat = [impz.elem(0, 0.5, 8, 1, [1.0]), impz.elem(1, 0.1, 4, 1, [10.0, 0.0, 1.0]),
+           impz.elem(0, 0.5, 8, 1, [1.0])]
+    table = synthetic_table()
+    mass, freq, grid = beams.ELECTRON_MASS_EV, 1.3e9, (16, 16, 32)
+
+    def oracle(wake):
+        try:
+            if wake:
+                orc.wake_set(table, 1.0, True)
+            return orc.run(lat, pts, cur, mass, -1.0, freq, ref, grid, flagmap=2)[0]
+        finally:
+            orc.wake_off()
+
+    rows_o, rows_nowake = oracle(True), oracle(False)
+    assert worst(rows_nowake, rows_o, [20, 21]) > 1e3 * tol
+    b = impz.Bunch(pts, cur, mass, -1.0, freq, ref, grid, form=form, track_ids=False)
+    try:
+        b.set_integrator(2)
+        b.wake(table, 1.0, True)
+        recs, zs = b.run(lat)
+        refs = b.run_reference()
+    finally:
+        b.close()
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], mass, freq)
+                       for i in range(len(recs))])
+    assert worst(rows_g, rows_o, cols) <= tol

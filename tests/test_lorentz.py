@@ -52,3 +52,133 @@ def test_lorentz_integrator_without_current_converges_too():
         r1, r2 = run(1), run(2)
         gaps.append(max(abs(r2[-1, c] - r1[-1, c]) / abs(r1[-1, c]) for c in (7, 13)))
     assert gaps[0] > 8 * gaps[1] and gaps[1] < 2e-3
+
+
+def _lz_run(lat, cfg, current=0.0, pts=None):
+    return orc.run(lat, cfg["pts"] if pts is None else pts, current, cfg["mass"], cfg["charge"],
+                   cfg["freq"], cfg["refptcl"], (16, 16, 32), flagmap=2)
+
+
+def test_uniform_solenoid_rotates_the_transverse_momentum():
+    """A solenoid with no ramp (Param(4) = 0, getfld_Sol's body over the
+    whole length) and no current: each kick is a Cayley rotation of
+    (px, py) about z, so |p_perp| and pt of every particle stay as they
+    were (to rounding) and a particle's momentum turns by nseg Cayley angles 2 atan(q Bz tau / 2pz),
+    close to q Bz L / pz."""
+    cfg = beams.fodo_1e5(n=2000, seed=beams.SEED0 + 75)
+    bz, length, nseg = 0.8, 0.5, 40
+    rows, p1, beam = _lz_run([impz.elem(3, length, nseg, 1, [bz, 0.0, 0.0])], cfg)
+    p0 = cfg["pts"]
+    np.testing.assert_allclose(np.hypot(p1[:, 1], p1[:, 3]), np.hypot(p0[:, 1], p0[:, 3]),
+                               rtol=1e-13, atol=1e-300)
+    # (1 + a12^2) pt / (1 + a12^2): pt to the last bit or two
+    np.testing.assert_allclose(p1[:, 5], p0[:, 5], rtol=1e-15, atol=0)
+    gam = -cfg["refptcl"][5]
+    pz = np.sqrt((gam - p0[:, 5]) ** 2 - 1.0 - p0[:, 1] ** 2 - p0[:, 3] ** 2)
+    # q B / (m c) [1/m] with Pts1(7) = q/m [1/eV]: 2.99792458e8 B q / m
+    want = -2.99792458e8 * bz * p0[:, 6] * length / pz
+    turned = np.angle((p1[:, 1] + 1j * p1[:, 3]) / (p0[:, 1] + 1j * p0[:, 3]))
+    np.testing.assert_allclose(turned, np.angle(np.exp(1j * want)), rtol=0, atol=1e-3)
+    # exactly: nseg Cayley rotations by 2 atan(a12), a12 = -tau c Bz q/m / (2 pz)
+    cay = nseg * 2 * np.arctan(-(length / nseg) * 2.99792458e8 * bz * p0[:, 6] / (2 * pz))
+    np.testing.assert_allclose(turned, np.angle(np.exp(1j * cay)), rtol=0, atol=1e-11)
+    np.testing.assert_array_equal(beam.refptcl[5], cfg["refptcl"][5])
+
+
+def test_enge_quadrupole_approaches_the_hard_edge_one():
+    """getfldfrgAna2_Quadrupole's Enge profile with a short fringe (aperture
+    2 mm) over a 0.2 m element of effective length 0.1 m focuses like a
+    hard-edge 0.1 m quadrupole between two 0.05 m drifts."""
+    cfg = beams.fodo_1e5(n=2000, seed=beams.SEED0 + 76)
+    g = 20.0
+    frg = [impz.elem(1, 0.2, 400, 1, [g, 0.1, 0.002])]
+    hard = [impz.elem(0, 0.05, 100, 1, [1.0]), impz.elem(1, 0.1, 200, 1, [g, 0.0, 1.0]),
+            impz.elem(0, 0.05, 100, 1, [1.0])]
+    drift = [impz.elem(0, 0.2, 400, 1, [1.0])]
+    rf, rh, rd = (_lz_run(lat, cfg)[0][-1] for lat in (frg, hard, drift))
+    for c in (7, 13):  # rms x, rms y
+        assert abs(rf[c] - rh[c]) < 0.02 * abs(rd[c] - rh[c])
+
+
+def _self_convergence(make, cfg, cols, current=0.0):
+    finals = [_lz_run(make(n), cfg, current)[0][-1] for n in (8, 32, 256)]
+    err = [max(abs(f[c] - finals[-1][c]) / abs(finals[-1][c]) for c in cols)
+           for f in finals[:2]]
+    return err
+
+
+def test_lorentz_element_fields_converge_at_second_order():
+    """Quadrupole with Enge fringe, ramped solenoid and constant focusing
+    under kick2: the splitting error falls about 16x from 8 to 32 steps."""
+    cfg = beams.fodo_1e5(n=1000, seed=beams.SEED0 + 77)
+    makers = [
+        lambda n: [impz.elem(1, 0.3, n, 1, [15.0, 0.2, 0.02])],
+        lambda n: [impz.elem(3, 0.4, n, 1, [0.6, 0.0, 0.05])],
+        # getfld_ConstFoc's B = k X / c (its qmcc is a placeholder 1): 20-30 T/m
+        lambda n: [impz.elem(2, 0.4, n, 1, [6e9, 9e9, 0.0, 1.0])],
+    ]
+    for make in makers:
+        err = _self_convergence(make, cfg, (7, 8, 13, 14))
+        assert err[0] > 8 * err[1] > 0, err
+
+
+def test_constant_focusing_ez_moves_the_reference_energy():
+    """getfld_ConstFoc's Ez = kz t Scxl on axis at the reference time
+    changes gamma0 by tau qmcc Ez0 at each kick (kick2_BeamBunch's
+    refptcl(6) = -gam); kz = 0 leaves it alone."""
+    cfg = beams.fodo_1e5(n=500, seed=beams.SEED0 + 78)
+    ref = cfg["refptcl"].copy()
+    ref[4] = 2.0  # a nonzero reference time tg
+    c2 = dict(cfg, refptcl=ref)
+    g0 = -ref[5]
+    kz, length, nseg = 1e-3, 0.4, 4
+    _, _, beam = _lz_run([impz.elem(2, length, nseg, 1, [40.0, 60.0, kz, 1.0])], c2)
+    _, _, beam0 = _lz_run([impz.elem(2, length, nseg, 1, [40.0, 60.0, 0.0, 1.0])], c2)
+    assert beam0.refptcl[5] == ref[5]
+    # the same recurrence by hand: tg advances by tau/(2 Scxl beta0) per drift2
+    scxl = 2.99792458e8 / (2 * np.pi * cfg["freq"])
+    qmcc = cfg["charge"] / cfg["mass"]
+    tau, tg, gam = length / nseg, ref[4], g0
+    for _ in range(nseg):
+        tg += 0.5 * tau / (scxl * np.sqrt(1.0 - 1.0 / gam / gam))
+        gam = gam + tau * qmcc * (kz * tg * scxl)
+        tg += 0.5 * tau / (scxl * np.sqrt(1.0 - 1.0 / gam / gam))
+    np.testing.assert_allclose(-beam.refptcl[5], gam, rtol=1e-14)
+    assert -beam.refptcl[5] != g0
+
+
+def test_lorentz_read_in_wake_acts_as_under_the_map_integrator():
+    """kick2wake/scatter2wake (BeamBunch.f90:5048-5938) adds the raw
+    per-plane wake at the particle, linear in z, after the space-charge
+    scaling; kick1wake adds it to the node fields in grid units.  Both give
+    a particle tau q/m Ez of energy (and tau q/m Ex / beta of px), so the
+    wake's own effect on the bunch (with minus without) is the same under
+    both integrators, longitudinal and transverse."""
+    from test_wake import synthetic_table
+    cur = 1.3
+    pts, ref = beams.gaussian_bunch(3000, seed=beams.SEED0 + 81, mass=beams.ELECTRON_MASS_EV,
+                                    charge=-1.0, ekin=98.169272e6, current=cur, freq=1.3e9,
+                                    sig_x=0.5e-3, sig_y=0.5e-3, sig_xp=0.05e-3,
+                                    sig_yp=0.05e-3, sig_phase_deg=1.0, sig_e=50e3)
+    scxl = 2.99792458e8 / (2 * np.pi * 1.3e9)
+    pts = pts.copy()
+    pts[:, 0] += 0.5e-3 / scxl  # offsets drive the dipole (transverse) wake
+    pts[:, 2] += 0.3e-3 / scxl
+    lat = [impz.elem(0, 1.0, 8, 1, [1.0])]
+
+    def final(fm, wake):
+        try:
+            if wake:
+                orc.wake_set(synthetic_table(), 1.0, True)
+            return orc.run(lat, pts, cur, beams.ELECTRON_MASS_EV, -1.0, 1.3e9, ref,
+                           (16, 16, 32), flagmap=fm)[0][-1]
+        finally:
+            orc.wake_off()
+
+    d1 = final(1, True) - final(1, False)
+    d2 = final(2, True) - final(2, False)
+    assert abs(d1[20]) > 10 * abs(final(1, False)[20])  # the wake dominates <dE>
+    for c in (20, 21):  # mean and rms energy
+        assert abs(d2[c] - d1[c]) < 1e-3 * abs(d1[c]), (c, d1[c], d2[c])
+    for c in (8, 14):  # mean px, py
+        assert abs(d1[c]) > 0 and abs(d2[c] - d1[c]) < 1e-3 * abs(d1[c]), (c, d1[c], d2[c])
