@@ -182,8 +182,9 @@ def _dp(a):
 # ---------------------------------------------------------------------------
 def elem(etype, length, nseg, mapstp=1, vals=(), rf=None):
     """Build an impz_elem_t.  vals are the deck values v1..v24; rf is an
-    optional (z, Ez, Ez', Ez'') on-axis table for linear RF maps, or for a
-    SolRF (105) the 1-D array of read3_Data's Fourier coefficients."""
+    optional (z, Ez, Ez', Ez'') on-axis table for linear RF maps, or the
+    1-D array of read3_Data's Fourier coefficients for SolRF and TWS (105,
+    106) and, under the Lorentz integrator, for types 101..104."""
     e = ElemStruct()
     e.type = int(etype)
     e.nseg = int(nseg)

@@ -51,13 +51,21 @@ struct MapOp {
 //   LZ_SOL_FRG   solenoid ramp, c0 = dBz/dz: B = (-c0/2 X, -c0/2 Y, c1)
 //   LZ_CONSTFOC  constant focusing (getfld_ConstFoc), c = (kx, ky, kz):
 //                Ez = kz T Scxl, Bx = -kx Y / c, By = ky X / c
+//   LZ_RF        RF cavity 101..104 (getfld_DTL / CCDTL / CCL / SC), c =
+//                (G, ez1, ez1', f1, f1', w, theta0, xl c) with the on-axis
+//                Fourier sums at z; per particle, phi = w T + theta0:
+//                E = (-X (ez1'/2 + f1' r^2/4) cos phi, same with Y,
+//                (ez1 + f1 r^2) cos phi), B = (G Y + Y/(xl c)(ez1/2 + f1 r^2/4)
+//                sin phi, G X - X/(xl c)(...) sin phi, 0); G the DTL's
+//                drift-tube quadrupole gradient, 0 for the others
 enum LzKind {
   LZ_NONE = 0,
   LZ_QUAD = 1,
   LZ_QUAD_FRG = 2,
   LZ_SOL = 3,
   LZ_SOL_FRG = 4,
-  LZ_CONSTFOC = 5
+  LZ_CONSTFOC = 5,
+  LZ_RF = 6
 };
 
 struct MapProgram {
@@ -88,7 +96,7 @@ struct StepParams {
   double wk_aa, wk_gg, wk_len;  // analytic wake: iris radius, gap, period (Param(13..15))
   int lorentz;         // the kick is the Lorentz integrator's (kick2/scatter2)
   int lz_kind;         // LzKind of its element's external field
-  double lz_c[3];      // that field's coefficients at the kick's z (LzKind)
+  double lz_c[8];      // that field's coefficients at the kick's z (LzKind)
   double lz_tg;        // refptcl(5) at the kick (scatter2's tg)
   double lz_ez0;       // the field's Ez on axis at tg (scatter2's ez0)
 };

@@ -930,15 +930,73 @@ void quad_enge(double bb, double efflen, double radius, double length, double zz
   }
 }
 
+// The on-axis part of getfld_DTL / CCDTL / CCL / SC under the Lorentz
+// integrator (DTL.f90:769-855, CCL.f90:525-606, CCDTL.f90, SC.f90): Ez and
+// its derivatives from read3_Data's Fourier coefficients (zdat, ndata
+// values, the count made odd by a trailing zero, Data.f90:348-409) at z
+// from the cell's middle, the radial-expansion factors f1, f1', and the
+// DTL's drift-tube quadrupole gradient; pi and c are default-real literals
+// there.  c = (G, ez1, ez1', f1, f1', w, theta0, xl c); ez0 = Ez on axis
+// at time tg.
+void rf_fourier_field(const Phys& P, const impz_elem_t& e, double zedge, double z, double tg,
+                      double c[8], double& ez0) {
+  const double clite = (double)299792458.0f;
+  const double pi = (double)(2 * std::asin(1.0f));
+  const double escale = e.val[0];
+  const double len = e.length;
+  const double zmid = zedge + len / 2;
+  const double ww = e.val[1] / P.Scfreq;
+  const double xl = P.Scxl / ww;
+  const double theta0 = e.val[2] * (double)std::asin(1.0f) / 90;
+  double bgrad = 0.0;
+  if (e.type == 101) {
+    const double zz = z - zedge;
+    if (zz < e.val[5])
+      bgrad = e.val[6];
+    else if (zz < len - e.val[7])
+      bgrad = 0.0;
+    else
+      bgrad = e.val[8];
+  }
+  const double zz = z - zmid;
+  const int nd = e.ndata % 2 == 0 ? e.ndata + 1 : e.ndata;
+  auto fc = [&](int i) { return i <= e.ndata ? e.zdat[i - 1] : 0.0; };
+  double ez1 = fc(1) / 2, ezp1 = 0.0, ezpp1 = 0.0, ezppp = 0.0;
+  for (int i = 2; i <= (nd - 1) / 2 + 1; i++) {
+    const double a = fc(2 * i - 2), b = fc(2 * i - 1);
+    const double arg = (i - 1) * 2 * pi * zz / len;
+    const double k = (i - 1) * 2 * pi / len;
+    const double sa = std::sin(arg), ca = std::cos(arg);
+    ez1 = ez1 + a * ca + b * sa;
+    ezp1 = ezp1 + k * (-(a * sa) + b * ca);
+    ezpp1 = ezpp1 + k * k * (-(a * ca) - b * sa);
+    ezppp = ezppp + k * k * k * (a * sa - b * ca);
+  }
+  ez1 = ez1 * escale;
+  ezp1 = ezp1 * escale;
+  ezpp1 = ezpp1 * escale;
+  ezppp = ezppp * escale;
+  c[0] = bgrad;
+  c[1] = ez1;
+  c[2] = ezp1;
+  c[3] = -((ezpp1 + ez1 / xl / xl) / 4);
+  c[4] = -((ezppp + ezp1 / xl / xl) / 4);
+  c[5] = ww;
+  c[6] = theta0;
+  c[7] = xl * clite;
+  // getfld at (0, 0, z, tg): (ez1 + f1 0) cos(w tg + theta0)
+  ez0 = (ez1 + c[3] * 0.0) * std::cos(ww * tg + theta0);
+}
+
 // The external field of element e for a Lorentz kick at z (LzKind):
 // getfld_Quadrupole (Quadrupole.f90:369-402), getfld_ConstFoc
 // (ConstFoc.f90:297-322), getfld_Sol (Sol.f90:391-435) and no field for a
 // drift.  ez0 is its Ez on axis at time tg.  Returns false for an element
 // the Lorentz integrator does not carry here.
 bool lorentz_field(const Phys& P, const impz_elem_t& e, double zedge, double z, double tg,
-                   int& kind, double c[3], double& ez0) {
+                   int& kind, double c[8], double& ez0) {
   kind = LZ_NONE;
-  c[0] = c[1] = c[2] = 0.0;
+  for (int i = 0; i < 8; i++) c[i] = 0.0;
   ez0 = 0.0;
   const double zz = z - zedge;
   switch (e.type) {
@@ -978,6 +1036,14 @@ bool lorentz_field(const Phys& P, const impz_elem_t& e, double zedge, double z, 
       }
       return true;
     }
+    case 101:
+    case 102:
+    case 103:
+    case 104:
+      if (!e.zdat || e.ndata < 1 || !(e.length > 0.0)) return false;
+      kind = LZ_RF;
+      rf_fourier_field(P, e, zedge, z, tg, c, ez0);
+      return true;
     default:
       return false;
   }
@@ -998,7 +1064,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     double csr_r0, csr_s0, csr_blen;
     double wk_aa, wk_gg, wk_len;
     int lz_kind;
-    double lz_c[3], lz_tg, lz_ez0;
+    double lz_c[8], lz_tg, lz_ez0;
     double z;
     double ref[6];
   };
@@ -1015,12 +1081,13 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     if (e.nseg < 1) return IMPZ_ERR_ARG;
     const int bnseg = e.nseg, bitype = e.type;
     double piperad = pipe_radius(e), piperad2 = piperad;
-    // the Lorentz integrator covers drifts, quadrupoles, constant focusing
-    // and solenoids, whose fields kick2 applies (lorentz_field)
+    // the Lorentz integrator covers drifts, quadrupoles, constant focusing,
+    // solenoids and the RF cavities 101..104, whose fields kick2 applies
+    // (lorentz_field)
     const bool lorentz = csr.flagmap == 2;
     if (lorentz) {
       int kind;
-      double c[3], ez0;
+      double c[8], ez0;
       if (!lorentz_field(P, e, z, z, 0.0, kind, c, ez0)) return IMPZ_ERR_UNSUPPORTED;
     }
     // the wake switch of each element (AccSimulator.f90:865-875)

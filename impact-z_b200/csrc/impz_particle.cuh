@@ -659,13 +659,27 @@ __device__ __forceinline__ double moment_tail(double acc1, int lane) {
 //
 // The element's field at (X, Y) [m] and time T of one particle
 // (getfld_Quadrupole, Quadrupole.f90:369-402; getfld_Sol, Sol.f90:391-435;
-// getfld_ConstFoc, ConstFoc.f90:297-322; LzKind), in the reference's
-// expression forms; ez = E_z, b = B.
+// getfld_ConstFoc, ConstFoc.f90:297-322; getfldpts_DTL, DTL.f90:858-958,
+// and the CCDTL, CCL, SC forms; LzKind), in the reference's expression
+// forms; e = E, b = B.
 __device__ __forceinline__ void lz_field(int kind, const double* __restrict__ c, double X,
-                                         double Y, double T, const Consts& k, double& ez,
-                                         double& bx, double& by, double& bz) {
-  ez = 0.0; bx = 0.0; by = 0.0; bz = 0.0;
-  if (kind == LZ_QUAD) {
+                                         double Y, double T, const Consts& k, double& ex,
+                                         double& ey, double& ez, double& bx, double& by,
+                                         double& bz) {
+  ex = 0.0; ey = 0.0; ez = 0.0; bx = 0.0; by = 0.0; bz = 0.0;
+  if (kind == LZ_RF) {
+    // getfldpts_DTL (DTL.f90:932-956) and its CCDTL, CCL, SC forms
+    double sn, cs;
+    sincos(c[5] * T + c[6], &sn, &cs);
+    const double r2 = X * X + Y * Y;
+    const double er = c[2] / 2 + c[4] * r2 / 4;
+    const double bt = c[1] / 2 + c[3] * r2 / 4;
+    ex = -(X * er * cs);
+    ey = -(Y * er * cs);
+    ez = (c[1] + c[3] * r2) * cs;
+    bx = c[0] * Y + Y / c[7] * bt * sn;
+    by = c[0] * X + -(X / c[7] * bt * sn);
+  } else if (kind == LZ_QUAD) {
     bx = c[0] * Y;
     by = c[0] * X;
   } else if (kind == LZ_QUAD_FRG) {
@@ -701,11 +715,11 @@ __device__ __forceinline__ void lorentz_kick(Particle& p, double exn, double eyn
   const double qmcc = k.charge / k.mass;
   const double ez0 = sp->lz_ez0;
   const double tmpgamma0 = gam + 0.5 * tau * qmcc * ez0;
-  double e3, ext4, ext5, ext6;
-  lz_field(sp->lz_kind, sp->lz_c, p.x * xl, p.y * xl, p.ph + sp->lz_tg, k, e3, ext4, ext5,
-           ext6);
-  const double ex = tmpscale * exn + 0.0 + wx;
-  const double ey = tmpscale * eyn + 0.0 + wy;
+  double e1, e2, e3, ext4, ext5, ext6;
+  lz_field(sp->lz_kind, sp->lz_c, p.x * xl, p.y * xl, p.ph + sp->lz_tg, k, e1, e2, e3, ext4,
+           ext5, ext6);
+  const double ex = tmpscale * exn + e1 + wx;
+  const double ey = tmpscale * eyn + e2 + wy;
   const double ez = tmpscale * ezn + e3 + wz;
   const double bx = -(beta0 / Clight * tmpscale * eyn) + ext4;
   const double by = beta0 / Clight * tmpscale * exn + ext5;

@@ -213,8 +213,9 @@ def read_rfdata(path):
 
 def read_rfcoef(path):
     """rfdataN.in as Fourier coefficients, read3_Data
-    (src/DataStruct/Data.f90:348-408) for SolRF and TWS: the first value of
-    each line, a zero appended to make the count odd."""
+    (src/DataStruct/Data.f90:348-408) for SolRF and TWS, and for every RF
+    cavity under the Lorentz integrator: the first value of each line, a
+    zero appended to make the count odd."""
     vals = []
     with open(path) as f:
         for ln in f:
@@ -423,9 +424,16 @@ def lattice_segments(deck, workdir, skip=(), start=0):
     reset)."""
     from . import elem
 
+    flagmap = deck.flagmap
+
     def to_elem(e):
+        # the RF data (AccSimulator.f90:820-848): under the map integrator
+        # read1_Data's table, Fourier coefficients (read3_Data) for SolRF and
+        # TWS; under the Lorentz integrator Fourier coefficients for all
         rf = None
         if e.type in (105, 106) and e.vals[3] >= 0.0:
+            rf = read_rfcoef(os.path.join(workdir, "rfdata%d.in" % int(e.vals[3] + 0.1)))
+        elif 101 <= e.type <= 104 and e.vals[3] >= 0.0 and flagmap == 2:
             rf = read_rfcoef(os.path.join(workdir, "rfdata%d.in" % int(e.vals[3] + 0.1)))
         elif 101 <= e.type <= 104 and e.vals[3] >= 0.0:
             rf = read_rfdata(os.path.join(workdir, "rfdata%d.in" % int(e.vals[3])))
@@ -458,6 +466,7 @@ def lattice_segments(deck, workdir, skip=(), start=0):
             yield "slices", e
         elif e.type == -25:
             # switch integrator: Flagmap = bmpstp (AccSimulator.f90:806-809)
+            flagmap = e.mapstp
             yield "integrator", e.mapstp
         elif e.type == -52:
             # laser heater (AccSimulator.f90:982-1006): Param(2..4)

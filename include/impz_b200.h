@@ -60,7 +60,10 @@ typedef struct impz_bunch_s* impz_bunch_t;
  * 104 SC over the on-axis table zdat/edat/epdat/eppdat (rfdataN.in,
  * read1_Data); 105 SolRF (solenoid field v11) and 106 TWS (second wave's
  * phase v11) over read3_Data's Fourier coefficients in zdat (ndata values,
- * the other table pointers unused). */
+ * the other table pointers unused).  Under the Lorentz integrator
+ * (impz_set_integrator(b, 2)) types 101..104 also take read3_Data's
+ * Fourier coefficients in zdat, as the reference reads them then
+ * (AccSimulator.f90:826-848). */
 typedef struct {
   int type;
   int nseg;
@@ -131,8 +134,9 @@ int impz_wake_off(impz_bunch_t b);
  * (drift2 half steps around kick2/scatter2, BeamBunch.f90:467-509,
  * 2187-3071, or scatter20 without current), here for drifts, quadrupoles
  * (hard edge, or the Enge fringe of getfldfrgAna2_Quadrupole when
- * Param(3) > 1e-5), constant focusing and solenoids (getfld_Quadrupole,
- * getfld_ConstFoc, getfld_Sol), with a read-in or CSR wake applied as
+ * Param(3) > 1e-5), constant focusing, solenoids and the RF cavities
+ * 101..104 over Fourier coefficients (getfld_Quadrupole, getfld_ConstFoc,
+ * getfld_Sol, getfld_DTL/CCDTL/CCL/SC), with a read-in or CSR wake applied as
  * kick2wake does (BeamBunch.f90:5048-5938); a run with any other element
  * under it, or a quadrupole with 0 < Param(3) <= 1e-5 (whose field reads
  * unset derivatives there), is IMPZ_ERR_UNSUPPORTED. */

@@ -1465,16 +1465,19 @@ void orc_kick1(double *pts, int n, const double *phi, const int mesh[3],
  * wfield = {dEx[nz], dEy[nz], dEz[nz]} in grid-field units (orc_wake_field),
  * NULL for none. */
 /* The Lorentz integrator's kick (kick2/scatter2_BeamBunch, BeamBunch.f90:
- * 2187-3071, the analytic-field branch) in element elem = {type, Param(2),
- * Param(3), Param(4), length, zedge}: 0 drift, 1 quadrupole, 2 constant
- * focusing, 3 solenoid; z = the kick's position, tg = refptcl(5) there,
- * qmi = Pts1(7) */
+ * 2187-3071, the analytic-field branch) in element e with zedge = Param(1):
+ * 0 drift, 1 quadrupole, 2 constant focusing, 3 solenoid, 101..104 the RF
+ * cavities over read3_Data's Fourier coefficients (e->zdat, e->ndata); z =
+ * the kick's position, tg = refptcl(5) there, qmi = Pts1(7) */
 typedef struct {
-  int type;
-  double val[3], length, zedge, z, tg, qmi;
+  const orc_elem *e;
+  double zedge, z, tg, qmi;
   /* kick2wake (BeamBunch.f90:5048-5410): the per-plane wake {Ex, Ey,
    * Ez}[nz] as the wake routines return it, or NULL */
   const double *wraw;
+  /* the RF cavities' terms at z that getfldpts_DTL / getfldpts_CCL
+   * compute once per call (DTL.f90:858-958, CCL.f90:722-809) */
+  double bgrad, ez1, ezp1, f1, f1p, ww, theta0, xl, clite;
 } lorentz_kick;
 
 static void kick_common(double *pts, int n, const double *phi, const int mesh[3],
@@ -1489,18 +1492,70 @@ void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
   kick_common(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, eg, wfield, NULL);
 }
 
-static lorentz_kick lz_make(const double elem[6], double z, double tg, double qmi) {
+/* read3_Data's coefficient Fcoef(i), i from 1, with the count made odd by
+ * a trailing zero (Data.f90:348-409) */
+static double fcoef(const orc_elem *e, int i) { return i <= e->ndata ? e->zdat[i - 1] : 0.0; }
+
+/* the on-axis part of getfld_DTL / CCDTL / CCL / SC (DTL.f90:769-855,
+ * CCDTL.f90, CCL.f90:525-606, SC.f90): the drift-tube quadrupoles'
+ * gradient (DTL only), Ez and its derivatives from the Fourier series at
+ * z - zmid, and the radial-expansion factors; pi and c are the reference's
+ * default-real literals there */
+static void lz_rf_axis(lorentz_kick *lz) {
+  const orc_elem *e = lz->e;
+  const double clite = (double)299792458.0f;
+  const double pi = (double)(2 * asinf(1.0f));
+  const double escale = e->val[0];
+  const double len = e->length;
+  const double zmid = lz->zedge + len / 2;
+  lz->ww = e->val[1] / PC.Scfreq;
+  lz->xl = PC.Scxl / lz->ww;
+  lz->theta0 = e->val[2] * (double)asinf(1.0f) / 90;
+  lz->clite = clite;
+  lz->bgrad = 0.0;
+  if (e->type == 101) {
+    const double zz = lz->z - lz->zedge;
+    const double len1 = e->val[5], bgrad1 = e->val[6];
+    const double len2 = len - e->val[7], bgrad2 = e->val[8];
+    if (zz < len1)
+      lz->bgrad = bgrad1;
+    else if (zz < len2)
+      lz->bgrad = 0.0;
+    else
+      lz->bgrad = bgrad2;
+  }
+  const double zz = lz->z - zmid;
+  const int nd = e->ndata % 2 == 0 ? e->ndata + 1 : e->ndata;
+  double ez1 = fcoef(e, 1) / 2, ezp1 = 0.0, ezpp1 = 0.0, ezppp = 0.0;
+  for (int i = 2; i <= (nd - 1) / 2 + 1; i++) {
+    const double a = fcoef(e, 2 * i - 2), b = fcoef(e, 2 * i - 1);
+    const double arg = (i - 1) * 2 * pi * zz / len;
+    const double k = (i - 1) * 2 * pi / len;
+    ez1 = ez1 + a * cos(arg) + b * sin(arg);
+    ezp1 = ezp1 + k * (-(a * sin(arg)) + b * cos(arg));
+    ezpp1 = ezpp1 + k * k * (-(a * cos(arg)) - b * sin(arg));
+    ezppp = ezppp + k * k * k * (a * sin(arg) - b * cos(arg));
+  }
+  ez1 = ez1 * escale;
+  ezp1 = ezp1 * escale;
+  ezpp1 = ezpp1 * escale;
+  ezppp = ezppp * escale;
+  lz->ez1 = ez1;
+  lz->ezp1 = ezp1;
+  lz->f1 = -((ezpp1 + ez1 / lz->xl / lz->xl) / 4);
+  lz->f1p = -((ezppp + ezp1 / lz->xl / lz->xl) / 4);
+}
+
+static lorentz_kick lz_make(const orc_elem *e, double zedge, double z, double tg, double qmi) {
   lorentz_kick lz;
-  lz.type = (int)elem[0];
-  lz.val[0] = elem[1];
-  lz.val[1] = elem[2];
-  lz.val[2] = elem[3];
-  lz.length = elem[4];
-  lz.zedge = elem[5];
+  memset(&lz, 0, sizeof(lz));
+  lz.e = e;
+  lz.zedge = zedge;
   lz.z = z;
   lz.tg = tg;
   lz.qmi = qmi;
   lz.wraw = NULL;
+  if (e->type >= 101 && e->type <= 104) lz_rf_axis(&lz);
   return lz;
 }
 
@@ -1510,10 +1565,10 @@ static lorentz_kick lz_make(const double elem[6], double z, double tg, double qm
 static void quad_ana2(const lorentz_kick *lz, double zz, double *bgrad, double *bgradp,
                       double *bgradpp) {
   const double c1 = -0.00004, c2 = 4.518219;
-  const double bb = lz->val[0];
-  const double dd = 2 * lz->val[2];
-  const double z10 = (lz->length - lz->val[1]) / 2;
-  const double z20 = lz->length - z10;
+  const double bb = lz->e->val[0];
+  const double dd = 2 * lz->e->val[2];
+  const double z10 = (lz->e->length - lz->e->val[1]) / 2;
+  const double z20 = lz->e->length - z10;
   const double z3 = z10 + 1.5 * dd;
   const double z4 = z20 - 1.5 * dd;
   double tmpz, s1, s2, s3, s4, tmp1, q;
@@ -1544,15 +1599,17 @@ static void quad_ana2(const lorentz_kick *lz, double zz, double *bgrad, double *
 /* getfld_BeamLineElem (BeamLineElem.f90:827-867) at pos = (x [m], y [m],
  * z [m], t) for the elements above: getfld_DriftTube (DriftTube.f90:
  * 290-305), getfld_Quadrupole (Quadrupole.f90:369-402), getfld_ConstFoc
- * (ConstFoc.f90:297-322, with its placeholder qmcc = gambetz = 1) and
- * getfld_Sol (Sol.f90:391-435); f = (Ex, Ey, Ez, Bx, By, Bz) */
+ * (ConstFoc.f90:297-322, with its placeholder qmcc = gambetz = 1),
+ * getfld_Sol (Sol.f90:391-435) and the RF cavities (scatter2 takes the
+ * DTL's and CCL's through getfldpts_*, the same values); f = (Ex, Ey, Ez,
+ * Bx, By, Bz) */
 static void lz_getfld(const lorentz_kick *lz, const double pos[4], double f[6]) {
   for (int i = 0; i < 6; i++) f[i] = 0.0;
   const double zz = pos[2] - lz->zedge;
-  if (lz->type == 1) {
-    double bgrad = lz->val[0], bgradp = 0.0, bgradpp = 0.0;
-    if (lz->val[1] > 1.0e-5) quad_ana2(lz, zz, &bgrad, &bgradp, &bgradpp);
-    if (lz->val[1] > 0.0) {
+  if (lz->e->type == 1) {
+    double bgrad = lz->e->val[0], bgradp = 0.0, bgradpp = 0.0;
+    if (lz->e->val[1] > 1.0e-5) quad_ana2(lz, zz, &bgrad, &bgradp, &bgradpp);
+    if (lz->e->val[1] > 0.0) {
       f[3] = bgrad * pos[1] -
              bgradpp * (pos[1] * pos[1] * pos[1] + 3 * (pos[0] * pos[0]) * pos[1]) / 12;
       f[4] = bgrad * pos[0] -
@@ -1562,26 +1619,49 @@ static void lz_getfld(const lorentz_kick *lz, const double pos[4], double f[6]) 
       f[3] = bgrad * pos[1];
       f[4] = bgrad * pos[0];
     }
-  } else if (lz->type == 2) {
+  } else if (lz->e->type == 2) {
     const double qmcc = 1.0, gambetz = 1.0, pz = gambetz;
-    f[2] = lz->val[2] * pos[3] * pz * pz * pz * PC.Scxl / qmcc;
-    f[3] = -(lz->val[0] * pos[1] * pz / qmcc / PC.Clight);
-    f[4] = lz->val[1] * pos[0] * pz / qmcc / PC.Clight;
-  } else if (lz->type == 3) {
-    const double x0 = lz->val[2], x02 = 2 * x0, b0 = lz->val[0];
+    f[2] = lz->e->val[2] * pos[3] * pz * pz * pz * PC.Scxl / qmcc;
+    f[3] = -(lz->e->val[0] * pos[1] * pz / qmcc / PC.Clight);
+    f[4] = lz->e->val[1] * pos[0] * pz / qmcc / PC.Clight;
+  } else if (lz->e->type == 3) {
+    const double x0 = lz->e->val[2], x02 = 2 * x0, b0 = lz->e->val[0];
     if (zz >= 0.0 && zz < x02) {
       const double bb = b0 / x02, bgrad = bb;
       f[3] = -(bgrad / 2 * pos[0]);
       f[4] = -(bgrad / 2 * pos[1]);
       f[5] = bb * zz;
-    } else if (zz >= x02 && zz <= lz->length - x02) {
+    } else if (zz >= x02 && zz <= lz->e->length - x02) {
       f[5] = b0;
-    } else if (zz > lz->length - x02 && zz <= lz->length) {
-      const double bb = -b0 / x02, bgrad = bb, zshift = lz->length - x02;
+    } else if (zz > lz->e->length - x02 && zz <= lz->e->length) {
+      const double bb = -b0 / x02, bgrad = bb, zshift = lz->e->length - x02;
       f[3] = -(bgrad / 2 * pos[0]);
       f[4] = -(bgrad / 2 * pos[1]);
       f[5] = b0 + bb * (zz - zshift);
     }
+  } else if (lz->e->type >= 101 && lz->e->type <= 104) {
+    /* the per-particle part of getfld_DTL / getfldpts_DTL (DTL.f90:
+     * 836-855, 932-956) and of CCDTL, CCL, SC, with the on-axis terms of
+     * lz_rf_axis; the DTL adds its drift-tube quadrupoles' B = G (y, x, 0) */
+    const double tt = pos[3];
+    const double tmpcos = cos(lz->ww * tt + lz->theta0);
+    const double tmpsin = sin(lz->ww * tt + lz->theta0);
+    const double r2 = pos[0] * pos[0] + pos[1] * pos[1];
+    const double xlc = lz->xl * lz->clite;
+    const double tmpex = -(pos[0] * (lz->ezp1 / 2 + lz->f1p * r2 / 4) * tmpcos);
+    const double tmpey = -(pos[1] * (lz->ezp1 / 2 + lz->f1p * r2 / 4) * tmpcos);
+    const double tmpez = (lz->ez1 + lz->f1 * r2) * tmpcos;
+    const double tmpbx = pos[1] / xlc * (lz->ez1 / 2 + lz->f1 * r2 / 4) * tmpsin;
+    const double tmpby = -(pos[0] / xlc * (lz->ez1 / 2 + lz->f1 * r2 / 4) * tmpsin);
+    if (lz->e->type == 101) {
+      f[3] = lz->bgrad * pos[1];
+      f[4] = lz->bgrad * pos[0];
+    }
+    f[0] = f[0] + tmpex;
+    f[1] = f[1] + tmpey;
+    f[2] = f[2] + tmpez;
+    f[3] = f[3] + tmpbx;
+    f[4] = f[4] + tmpby;
   }
 }
 
@@ -1651,9 +1731,9 @@ static void lorentz_update(double *p, double exn, double eyn, double ezn, double
  * gamma0 = gam + tau qmcc ez0 (refptcl(6) = -it) */
 double orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const double range[6],
                  const double msize[3], double gam, double curr, double tau, double mass,
-                 double chrg, const double elem[6], double z, double tg, double qmi,
+                 double chrg, const orc_elem *e, double zedge, double z, double tg, double qmi,
                  const double *wraw) {
-  lorentz_kick lz = lz_make(elem, z, tg, qmi);
+  lorentz_kick lz = lz_make(e, zedge, z, tg, qmi);
   lz.wraw = wraw;
   kick_common(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, NULL, NULL, &lz);
   return gam + tau * (chrg / mass) * lz_ez0(&lz);
@@ -1663,8 +1743,8 @@ double orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const
  * the element's field alone on the stored coordinates; returns the new
  * gamma0 */
 double orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass, double chrg,
-                        const double elem[6], double z, double tg, double qmi) {
-  const lorentz_kick lz = lz_make(elem, z, tg, qmi);
+                        const orc_elem *e, double zedge, double z, double tg, double qmi) {
+  const lorentz_kick lz = lz_make(e, zedge, z, tg, qmi);
   const double ez0 = lz_ez0(&lz);
   for (int q = 0; q < n; q++)
     lorentz_update(&P(q, 0), 0.0, 0.0, 0.0, gam, tau, mass, chrg, ez0, &lz, 0.0, 0.0, 0.0);
@@ -2483,13 +2563,15 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     const int lorentz = beam->flagmap == 2;
     /* Lorentz integrator: drifts, quadrupoles (not 0 < Param(3) <= 1e-5,
      * where getfld_Quadrupole reads G', G'' it never set), constant
-     * focusing and solenoids */
+     * focusing, solenoids and the RF cavities 101..104 over Fourier
+     * coefficients */
     if (lorentz && !(bitype == 0 || bitype == 2 || bitype == 3 ||
-                     (bitype == 1 && (e->val[1] <= 0.0 || e->val[1] > 1.0e-5)))) {
+                     (bitype == 1 && (e->val[1] <= 0.0 || e->val[1] > 1.0e-5)) ||
+                     (bitype >= 101 && bitype <= 104 && e->zdat && e->ndata >= 1))) {
       free(rho);
       return -10;
     }
-    const double lz_elem[6] = {(double)bitype, e->val[0], e->val[1], e->val[2], blength, z};
+    const double lz_zedge = z;
     orc_wake_elem(bitype, e->val);
     if (bitype == 4) { piperad = 100.0; piperad2 = 100.0; }
     double tau1 = 0.0;
@@ -2581,7 +2663,7 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
             if (lorentz)
               beam->refptcl[5] = -orc_kick2(beam->pts, beam->nlocal, rho, mesh, range, msize,
                                             -beam->refptcl[5], beam->current, tau2, beam->mass,
-                                            beam->charge, lz_elem, z, beam->refptcl[4],
+                                            beam->charge, e, lz_zedge, z, beam->refptcl[4],
                                             beam->nlocal ? beam->pts[6] : 0.0,
                                             wf ? wf + 6 * (size_t)mesh[2] : NULL);
             else
@@ -2593,7 +2675,7 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
         if (lorentz && half == 1 && bcurr < 1.0e-10)
           /* kick2 without current: scatter20 (BeamBunch.f90:3075-3531) */
           beam->refptcl[5] = -orc_lorentz_nosc(beam->pts, beam->nlocal, -beam->refptcl[5], tau2,
-                                               beam->mass, beam->charge, lz_elem, z,
+                                               beam->mass, beam->charge, e, lz_zedge, z,
                                                beam->refptcl[4],
                                                beam->nlocal ? beam->pts[6] : 0.0);
         if (lorentz) {

@@ -123,16 +123,8 @@ void orc_kick1w(double *pts, int n, const double *phi, const int mesh[3],
                 const double range[6], const double msize[3], double gam,
                 double curr, double tau, double mass, double chrg, double *eg,
                 const double *wfield);
-/* elem = {type, Param(2), Param(3), Param(4), length, zedge}; z and tg =
- * refptcl(5) at the kick; wraw = the per-plane wake {Ex, Ey, Ez}[nz] of
- * kick2wake or NULL; both return the new gamma0 */
-double orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const double range[6],
-                 const double msize[3], double gam, double curr, double tau, double mass,
-                 double chrg, const double elem[6], double z, double tg, double qmi,
-                 const double *wraw);
 void orc_drift2(double *pts, int n, double refptcl[6], double tau);
-double orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass, double chrg,
-                        const double elem[6], double z, double tg, double qmi);
+
 /* read-in wakefield of type -41 elements (Data.f90:559-633,
  * AccSimulator.f90:959-978, 1273-1340, Field.f90:783-1001) */
 int orc_wake_set(const double *z, const double *ew, const double *epw, const double *eppw,
@@ -168,10 +160,21 @@ typedef struct {
   int nseg, mapstp;
   double length;
   double val[24];  /* deck values v1..v24: Param(k) = val[k-2] for k >= 2 */
-  /* on-axis RF table for linear RF maps (type 103, val4 >= 0), else NULL */
+  /* on-axis RF table for linear RF maps (types 101..104), or, under the
+   * Lorentz integrator, read3_Data's Fourier coefficients in zdat */
   int ndata;
   const double *zdat, *edat, *epdat, *eppdat;
 } orc_elem;
+
+/* the Lorentz integrator's kick in element e with zedge = Param(1); z and
+ * tg = refptcl(5) at the kick; wraw = the per-plane wake {Ex, Ey, Ez}[nz]
+ * of kick2wake or NULL; both return the new gamma0 */
+double orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const double range[6],
+                 const double msize[3], double gam, double curr, double tau, double mass,
+                 double chrg, const orc_elem *e, double zedge, double z, double tg, double qmi,
+                 const double *wraw);
+double orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass, double chrg,
+                        const orc_elem *e, double zedge, double z, double tg, double qmi);
 
 typedef struct {
   double current, mass, charge, freq;  /* A, eV, e, Hz */
@@ -184,7 +187,8 @@ typedef struct {
   double zbleng, sentr, bendlencsr, r0;
   int flagbendcsr;
   /* Flagmap: 1 (0 too) the linear map integrator, 2 the Lorentz integrator
-   * (drifts and hard-edge quadrupoles, with space charge) */
+   * (drifts, quadrupoles, constant focusing, solenoids, RF cavities
+   * 101..104 over Fourier coefficients) */
   int flagmap;
 } orc_beam;
 

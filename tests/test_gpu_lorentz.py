@@ -161,3 +161,38 @@ def test_lorentz_read_in_wake_matches_the_oracle(form, cols, tol):
     rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], mass, freq)
                        for i in range(len(recs))])
     assert worst(rows_g, rows_o, cols) <= tol
+
+
+@pytest.mark.parametrize("current,form,cols,tol", [
+    (0.010, impz.FORM_FP64, RMS_COLS, 1e-8),
+    (0.010, impz.FORM_FP32CONV, [7, 9, 11, 13, 15, 17, 19, 21, 23], 1e-5),
+    (0.0, impz.FORM_FP64, RMS_COLS, 1e-10)])
+def test_lorentz_rf_cavities_match_the_oracle(current, form, cols, tol):
+    """A DTL cell (with its drift-tube quadrupoles), a drift and a CCL cell
+    over read3_Data Fourier coefficients under kick2 (getfldpts_DTL,
+    getfldpts_CCL): the cos/sin of each particle's RF phase on the GPU,
+    the reference particle's energy gain exact."""
+    from test_lorentz import rf_cell
+    coef, _ = rf_cell()
+    mass, freq = beams.PROTON_MASS_EV, 324e6
+    pts, ref = beams.gaussian_bunch(20_000, seed=beams.SEED0 + 84, mass=mass, charge=1.0,
+                                    ekin=3.35e6, current=current, freq=freq)
+    lat = [impz.elem(101, 0.08, 16, 20, [2.5e6, freq, 222.0, 1.0, 0.0065, 0.02, 68.0, 0.02,
+                                         -67.0], rf=coef),
+           impz.elem(0, 0.05, 4, 1, [0.0065]),
+           impz.elem(103, 0.08, 16, 20, [2.5e6, freq, 30.0, 1.0, 0.0065], rf=coef)]
+    grid = (32, 32, 64)
+    rows_o, _, beam = orc.run(lat, pts, current, mass, 1.0, freq, ref, grid, flagmap=2)
+    b = impz.Bunch(pts, current, mass, 1.0, freq, ref, grid, form=form, track_ids=False)
+    try:
+        b.set_integrator(2)
+        recs, zs = b.run(lat)
+        refs = b.run_reference()
+    finally:
+        b.close()
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    np.testing.assert_array_equal(refs[-1], np.array(beam.refptcl[:]))
+    assert -refs[-1][5] + ref[5] > 1e-4  # the cells accelerate
+    rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], mass, freq)
+                       for i in range(len(recs))])
+    assert worst(rows_g, rows_o, cols) <= tol

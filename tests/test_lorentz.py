@@ -3,7 +3,10 @@ drift2 half steps around kick2/scatter2 (BeamBunch.f90:467-509,
 2187-3071).  Through a FODO lattice its second-order splitting of the
 quadrupoles' focusing converges to the linear map integrator's result as
 the steps shrink."""
+import os
+
 import numpy as np
+import pytest
 
 from conftest import load_impz, load_oracle
 
@@ -182,3 +185,106 @@ def test_lorentz_read_in_wake_acts_as_under_the_map_integrator():
         assert abs(d2[c] - d1[c]) < 1e-3 * abs(d1[c]), (c, d1[c], d2[c])
     for c in (8, 14):  # mean px, py
         assert abs(d1[c]) > 0 and abs(d2[c] - d1[c]) < 1e-3 * abs(d1[c]), (c, d1[c], d2[c])
+
+
+def rf_cell(length=0.08, harmonics=18):
+    """A DTL-like cell's on-axis field as read3_Data's Fourier coefficients
+    (Fcoef(1)/2 + sum a_k cos + b_k sin of 2 pi k (z - zmid)/L) and the same
+    field sampled as read1_Data's (z, Ez, Ez', Ez'') table from the
+    entrance, for the map integrator."""
+    k = np.arange(1, harmonics + 1)
+    a = 2 * np.exp(-(k / 4.0) ** 2)
+    b = 0.01 * (-1.0) ** k / k
+    coef = np.empty(1 + 2 * harmonics)
+    coef[0], coef[1::2], coef[2::2] = 2.0, a, b
+    z = np.linspace(0, length, 4001)
+    w = 2 * np.pi * k[None, :] / length
+    c, s = np.cos(w * (z[:, None] - length / 2)), np.sin(w * (z[:, None] - length / 2))
+    ez = 1.0 + (a * c + b * s).sum(1)
+    ezp = (w * (-a * s + b * c)).sum(1)
+    ezpp = (w * w * (-a * c - b * s)).sum(1)
+    return coef, (z, ez, ezp, ezpp)
+
+
+@pytest.mark.parametrize("etype", [101, 103])
+def test_rf_cavity_under_kick2_gains_the_map_integrators_energy(etype):
+    """getfld_DTL / getfld_CCL over Fourier coefficients (DTL.f90:769-958,
+    CCL.f90:525-809): gamma0 moves by tau qmcc ez1 cos(w tg + theta0) at
+    each kick, so the reference particle's energy gain through a cell
+    converges, at second order, to the map integrator's RK6 of the same
+    field; the bunch's rms sizes agree to the linear map's own accuracy."""
+    coef, table = rf_cell()
+    mass, freq = beams.PROTON_MASS_EV, 324e6
+    pts, ref = beams.gaussian_bunch(2000, seed=beams.SEED0 + 83, mass=mass, charge=1.0,
+                                    ekin=3.35e6, current=0.0, freq=freq)
+    vals = [2.5e6, freq, 222.0, 1.0, 0.0065]
+    if etype == 101:
+        vals += [0.02, 68.0, 0.02, -67.0]  # the drift-tube quadrupoles
+    gaps = []
+    for nseg in (40, 160):
+        r1, _, b1 = orc.run([impz.elem(etype, 0.08, nseg, 20, vals, rf=table)], pts, 0.0, mass,
+                            1.0, freq, ref, (16, 16, 32), flagmap=1)
+        r2, _, b2 = orc.run([impz.elem(etype, 0.08, nseg, 20, vals, rf=coef)], pts, 0.0, mass,
+                            1.0, freq, ref, (16, 16, 32), flagmap=2)
+        gain1 = -b1.refptcl[5] + ref[5]
+        gaps.append(abs((-b2.refptcl[5] + ref[5]) / gain1 - 1))
+        assert gain1 > 1e-4
+    assert gaps[0] > 8 * gaps[1] and gaps[1] < 1e-5, gaps
+    for c in (7, 13, 21):
+        assert abs(r2[-1, c] / r1[-1, c] - 1) < 1e-2
+
+
+EXAMPLE1 = "/root/reference/examples/Example1"
+
+
+@pytest.mark.skipif(not os.path.isdir(EXAMPLE1), reason="the reference's examples are absent")
+def test_example1_dtl_cells_on_the_oracle():
+    """The reference's Example1 (Flagmap=2: nine DTL cells over rfdata
+    Fourier coefficients, quadrupoles and a drift) through the deck reader
+    and the oracle's Lorentz integrator, without current: the reference
+    particle's energy and phase at the end agree with an independent
+    integration of d gamma/dz = qmcc Ez(z) cos(w phi + theta0), d phi/dz =
+    1/(beta Scxl) over the same Fourier fields (the reference's
+    default-real pi in the series and in theta0)."""
+    from scipy.integrate import solve_ivp
+    from impz_b200 import deck
+    d = deck.read_deck(os.path.join(EXAMPLE1, "ImpactZ.in"))
+    assert d.flagmap == 2
+    pts = deck.read_particles(os.path.join(EXAMPLE1, "particle.in"))
+    ref, z = d.refptcl(), 0.0
+    for kind, item in deck.lattice_segments(d, EXAMPLE1):
+        if kind == "run":
+            rows, pts, beam = orc.run(item, pts, 0.0, d.bmass, d.bcharge, d.bfreq, ref,
+                                      (d.nx, d.ny, d.nz), z, flagmap=d.flagmap)
+            ref, z = np.array(beam.refptcl[:]), beam.z
+            assert np.isfinite(rows).all()
+    # the same reference particle by an adaptive RK45 at tight tolerance
+    pi32 = float(np.float32(2) * np.arcsin(np.float32(1.0)))
+    half_pi32 = float(np.arcsin(np.float32(1.0)))
+    scxl = 299792458.0 / (2 * np.pi * d.bfreq)
+    qmcc = d.bcharge / d.bmass
+    y = np.array([-d.refptcl()[5], d.refptcl()[4]])
+    for e in d.elements:
+        if e.type < 0:
+            continue
+        if 101 <= e.type <= 104:
+            coef = deck.read_rfcoef(os.path.join(EXAMPLE1, "rfdata%d.in" % int(e.vals[3] + 0.1)))
+            n = (len(coef) - 1) // 2
+            k = np.arange(1, n + 1)
+            a, b = coef[1::2][:n], coef[2::2][:n]
+            ww, th0 = e.vals[1] / d.bfreq, e.vals[2] * half_pi32 / 90
+            L = e.length
+
+            def rhs(s, yy):
+                arg = k * 2 * pi32 * (s - L / 2) / L
+                ez = e.vals[0] * (coef[0] / 2 + (a * np.cos(arg) + b * np.sin(arg)).sum())
+                beta = np.sqrt(1 - 1 / yy[0] ** 2)
+                return [qmcc * ez * np.cos(ww * yy[1] + th0), 1 / (beta * scxl)]
+        else:
+            def rhs(s, yy):
+                return [0.0, 1 / (np.sqrt(1 - 1 / yy[0] ** 2) * scxl)]
+        y = solve_ivp(rhs, (0.0, e.length), y, rtol=1e-12, atol=1e-14, method="DOP853").y[:, -1]
+    gain = y[0] + d.refptcl()[5]
+    assert gain > 1e-4  # the cells accelerate
+    assert abs(-ref[5] - y[0]) < 1e-5 * gain
+    assert abs(ref[4] - y[1]) < 1e-6 * y[1]
