@@ -58,6 +58,14 @@ struct MapOp {
 //                (ez1 + f1 r^2) cos phi), B = (G Y + Y/(xl c)(ez1/2 + f1 r^2/4)
 //                sin phi, G X - X/(xl c)(...) sin phi, 0); G the DTL's
 //                drift-tube quadrupole gradient, 0 for the others
+//   LZ_SOLRF     SolRF 105 (getfld_SolRF): t = T / (2 pi Scfreq),
+//   LZ_TWS       phi = w t + theta0, r = xlrep, the wave c[4..7] = (ez1,
+//                ez1', f1, f1') as LZ_RF but B = (Y r/c (...) sin phi, -X r/c
+//                (...) sin phi, 0); c = (w, xlrep, 2 pi Scfreq, theta0, wave,
+//                then SolRF's solenoid (bscale times bz, bz', bz'', bz''')
+//                B += (-bz'/2 X + bz''' X r^2/16, same with Y, bz - bz'' r^2/4),
+//                or TWS 106's second wave (ez1, ez1', f1, f1', theta2) at
+//                phi + theta2)
 enum LzKind {
   LZ_NONE = 0,
   LZ_QUAD = 1,
@@ -65,7 +73,9 @@ enum LzKind {
   LZ_SOL = 3,
   LZ_SOL_FRG = 4,
   LZ_CONSTFOC = 5,
-  LZ_RF = 6
+  LZ_RF = 6,
+  LZ_SOLRF = 7,
+  LZ_TWS = 8
 };
 
 struct MapProgram {
@@ -96,7 +106,7 @@ struct StepParams {
   double wk_aa, wk_gg, wk_len;  // analytic wake: iris radius, gap, period (Param(13..15))
   int lorentz;         // the kick is the Lorentz integrator's (kick2/scatter2)
   int lz_kind;         // LzKind of its element's external field
-  double lz_c[8];      // that field's coefficients at the kick's z (LzKind)
+  double lz_c[16];     // that field's coefficients at the kick's z (LzKind)
   double lz_tg;        // refptcl(5) at the kick (scatter2's tg)
   double lz_ez0;       // the field's Ez on axis at tg (scatter2's ez0)
 };

@@ -988,15 +988,113 @@ void rf_fourier_field(const Phys& P, const impz_elem_t& e, double zedge, double 
   ez0 = (ez1 + c[3] * 0.0) * std::cos(ww * tg + theta0);
 }
 
+bool solrf_table_ok(const impz_elem_t& e) {
+  if (e.ndata < 5 || !e.zdat) return false;
+  const int n1 = (int)(e.zdat[0] + 0.1);
+  if (n1 < 1 || n1 + 4 > e.ndata || e.zdat[3] == 0.0) return false;
+  if (e.ndata < n1 + 8) return true;
+  const int n2 = (int)(e.zdat[n1 + 4] + 0.1);
+  return n2 < 3 || (n1 + 8 + n2 <= e.ndata && e.zdat[n1 + 7] != 0.0);
+}
+
+// One Fourier series of getfld_SolRF / getfld_TWS (SolRF.f90:482-628,
+// TWS.f90): terms from F(ntmp+1), npar of them, at zz from the series'
+// middle over its period zlen; Ez and three derivatives.
+void fourier_axis(const impz_elem_t& e, int ntmp, int npar, double zz, double zlen,
+                  double pi, double& ez1, double& ezp1, double& ezpp1, double& ezppp) {
+  auto F = [&](int i) { return i >= 1 && i <= e.ndata ? e.zdat[i - 1] : 0.0; };
+  ez1 = F(ntmp + 1) / 2;
+  ezp1 = 0.0;
+  ezpp1 = 0.0;
+  ezppp = 0.0;
+  for (int i = 2; i <= (npar - 1) / 2 + 1; i++) {
+    const double a = F(2 * i - 2 + ntmp), b = F(2 * i - 1 + ntmp);
+    const double arg = (i - 1) * 2 * pi * zz / zlen;
+    const double k = (i - 1) * 2 * pi / zlen;
+    const double sa = std::sin(arg), ca = std::cos(arg);
+    ez1 = ez1 + a * ca + b * sa;
+    ezp1 = ezp1 + k * (-(a * sa) + b * ca);
+    ezpp1 = ezpp1 + k * k * (-(a * ca) - b * sa);
+    ezppp = ezppp + k * k * k * (a * sa - b * ca);
+  }
+}
+
+// getfld_SolRF / getfld_TWS's terms at z (c as LZ_SOLRF / LZ_TWS) and the
+// on-axis Ez at time tg.  The field is zero outside zedge < z < zedge+len
+// and each series outside its own [zstart, zend].
+void rfw_field(const Phys& P, const impz_elem_t& e, double zedge, double z, double tg,
+               double c[16], double& ez0) {
+  const double clite = (double)299792458.0f;
+  const double pi = (double)(2 * std::asin(1.0f));
+  const double escale = e.val[0];
+  const double len = e.length;
+  const bool tws = e.type == 106;
+  for (int i = 0; i < 16; i++) c[i] = 0.0;
+  ez0 = 0.0;
+  if (!(z > zedge && z < zedge + len)) return;
+  auto F = [&](int i) { return i >= 1 && i <= e.ndata ? e.zdat[i - 1] : 0.0; };
+  const double ww = e.val[1] * 2 * pi;
+  const double xlrep = ww / clite;
+  const double theta0 = e.val[2] * (double)std::asin(1.0f) / 90;
+  const double tsc = 2 * pi * P.Scfreq;
+  c[0] = ww;
+  c[1] = xlrep;
+  c[2] = tsc;
+  c[3] = theta0;
+  const double zlc = z - zedge;
+  const int numpar1 = (int)(F(1) + 0.1);
+  const double zstart1 = F(2), zend1 = F(3), zlength1 = F(4);
+  double ez1, ezp1, ezpp1, ezppp;
+  const double tt = tg / tsc;
+  if (zlc >= zstart1 && zlc <= zend1) {
+    fourier_axis(e, 4, numpar1, z - zedge - zstart1 - zlength1 / 2, zlength1, pi, ez1, ezp1,
+                 ezpp1, ezppp);
+    ez1 = ez1 * escale;
+    ezp1 = ezp1 * escale;
+    ezpp1 = ezpp1 * escale;
+    ezppp = ezppp * escale;
+    c[4] = ez1;
+    c[5] = ezp1;
+    c[6] = -((ezpp1 + ez1 * xlrep * xlrep) / 4);
+    c[7] = -((ezppp + ezp1 * xlrep * xlrep) / 4);
+    ez0 = 0.0 + (c[4] + c[6] * 0.0) * std::cos(ww * tt + theta0);
+  }
+  const int numpar2 = (int)(F(5 + numpar1) + 0.1);
+  const double zstart2 = F(6 + numpar1), zend2 = F(7 + numpar1), zlength2 = F(8 + numpar1);
+  if (zlc >= zstart2 && zlc <= zend2) {
+    fourier_axis(e, numpar1 + 8, numpar2, z - zedge - zstart2 - zlength2 / 2, zlength2, pi,
+                 ez1, ezp1, ezpp1, ezppp);
+    if (tws) {
+      ez1 = ez1 * escale;
+      ezp1 = ezp1 * escale;
+      ezpp1 = ezpp1 * escale;
+      ezppp = ezppp * escale;
+      c[8] = ez1;
+      c[9] = ezp1;
+      c[10] = -((ezpp1 + ez1 * xlrep * xlrep) / 4);
+      c[11] = -((ezppp + ezp1 * xlrep * xlrep) / 4);
+      c[12] = e.val[10] * pi / 180;
+      ez0 = ez0 + (c[8] + c[10] * 0.0) * std::cos(ww * tt + theta0 + c[12]);
+    } else {
+      const double bscale = e.val[10];
+      c[8] = bscale * ez1;
+      c[9] = bscale * ezp1;
+      c[10] = bscale * ezpp1;
+      c[11] = bscale * ezppp;
+    }
+  }
+  if (tws) c[12] = e.val[10] * pi / 180;
+}
+
 // The external field of element e for a Lorentz kick at z (LzKind):
 // getfld_Quadrupole (Quadrupole.f90:369-402), getfld_ConstFoc
 // (ConstFoc.f90:297-322), getfld_Sol (Sol.f90:391-435) and no field for a
 // drift.  ez0 is its Ez on axis at time tg.  Returns false for an element
 // the Lorentz integrator does not carry here.
 bool lorentz_field(const Phys& P, const impz_elem_t& e, double zedge, double z, double tg,
-                   int& kind, double c[8], double& ez0) {
+                   int& kind, double c[16], double& ez0) {
   kind = LZ_NONE;
-  for (int i = 0; i < 8; i++) c[i] = 0.0;
+  for (int i = 0; i < 16; i++) c[i] = 0.0;
   ez0 = 0.0;
   const double zz = z - zedge;
   switch (e.type) {
@@ -1044,6 +1142,15 @@ bool lorentz_field(const Phys& P, const impz_elem_t& e, double zedge, double z, 
       kind = LZ_RF;
       rf_fourier_field(P, e, zedge, z, tg, c, ez0);
       return true;
+    case 105:
+    case 106:
+      // TWS needs both series; SolRF's solenoid series may be absent (the
+      // reference then reads its zero-filled coefficient array: no field)
+      if (!(e.type == 106 ? tws_table_ok(e) : solrf_table_ok(e)) || !(e.length > 0.0))
+        return false;
+      kind = e.type == 105 ? LZ_SOLRF : LZ_TWS;
+      rfw_field(P, e, zedge, z, tg, c, ez0);
+      return true;
     default:
       return false;
   }
@@ -1064,7 +1171,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     double csr_r0, csr_s0, csr_blen;
     double wk_aa, wk_gg, wk_len;
     int lz_kind;
-    double lz_c[8], lz_tg, lz_ez0;
+    double lz_c[16], lz_tg, lz_ez0;
     double z;
     double ref[6];
   };
@@ -1082,12 +1189,12 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     const int bnseg = e.nseg, bitype = e.type;
     double piperad = pipe_radius(e), piperad2 = piperad;
     // the Lorentz integrator covers drifts, quadrupoles, constant focusing,
-    // solenoids and the RF cavities 101..104, whose fields kick2 applies
+    // solenoids and the RF cavities 101..106, whose fields kick2 applies
     // (lorentz_field)
     const bool lorentz = csr.flagmap == 2;
     if (lorentz) {
       int kind;
-      double c[8], ez0;
+      double c[16], ez0;
       if (!lorentz_field(P, e, z, z, 0.0, kind, c, ez0)) return IMPZ_ERR_UNSUPPORTED;
     }
     // the wake switch of each element (AccSimulator.f90:865-875)

@@ -660,8 +660,8 @@ __device__ __forceinline__ double moment_tail(double acc1, int lane) {
 // The element's field at (X, Y) [m] and time T of one particle
 // (getfld_Quadrupole, Quadrupole.f90:369-402; getfld_Sol, Sol.f90:391-435;
 // getfld_ConstFoc, ConstFoc.f90:297-322; getfldpts_DTL, DTL.f90:858-958,
-// and the CCDTL, CCL, SC forms; LzKind), in the reference's expression
-// forms; e = E, b = B.
+// and the CCDTL, CCL, SC forms; getfld_SolRF, getfld_TWS; LzKind), in the
+// reference's expression forms; e = E, b = B.
 __device__ __forceinline__ void lz_field(int kind, const double* __restrict__ c, double X,
                                          double Y, double T, const Consts& k, double& ex,
                                          double& ey, double& ez, double& bx, double& by,
@@ -679,6 +679,36 @@ __device__ __forceinline__ void lz_field(int kind, const double* __restrict__ c,
     ez = (c[1] + c[3] * r2) * cs;
     bx = c[0] * Y + Y / c[7] * bt * sn;
     by = c[0] * X + -(X / c[7] * bt * sn);
+  } else if (kind == LZ_SOLRF || kind == LZ_TWS) {
+    // getfld_SolRF (SolRF.f90:482-628), getfld_TWS (TWS.f90)
+    const double clite = (double)299792458.0f;
+    const double tt = T / c[2];
+    const double ph = c[0] * tt + c[3];
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    const double r2 = X * X + Y * Y;
+    const double er = c[5] / 2 + c[7] * r2 / 4;
+    const double bt = c[4] / 2 + c[6] * r2 / 4;
+    ex = 0.0 + -(X * er * cs);
+    ey = 0.0 + -(Y * er * cs);
+    ez = 0.0 + (c[4] + c[6] * r2) * cs;
+    bx = 0.0 + Y * c[1] / clite * bt * sn;
+    by = 0.0 + -(X * c[1] / clite * bt * sn);
+    if (kind == LZ_TWS) {
+      double sn2, cs2;
+      sincos(ph + c[12], &sn2, &cs2);
+      const double er2 = c[9] / 2 + c[11] * r2 / 4;
+      const double bt2 = c[8] / 2 + c[10] * r2 / 4;
+      ex = ex + -(X * er2 * cs2);
+      ey = ey + -(Y * er2 * cs2);
+      ez = ez + (c[8] + c[10] * r2) * cs2;
+      bx = bx + Y * c[1] / clite * bt2 * sn2;
+      by = by + -(X * c[1] / clite * bt2 * sn2);
+    } else {
+      bx = bx - c[9] / 2 * X + c[11] * X * r2 / 16;
+      by = by - c[9] / 2 * Y + c[11] * Y * r2 / 16;
+      bz = bz + c[8] - c[10] * r2 / 4;
+    }
   } else if (kind == LZ_QUAD) {
     bx = c[0] * Y;
     by = c[0] * X;

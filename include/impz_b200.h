@@ -135,8 +135,9 @@ int impz_wake_off(impz_bunch_t b);
  * 2187-3071, or scatter20 without current), here for drifts, quadrupoles
  * (hard edge, or the Enge fringe of getfldfrgAna2_Quadrupole when
  * Param(3) > 1e-5), constant focusing, solenoids and the RF cavities
- * 101..104 over Fourier coefficients (getfld_Quadrupole, getfld_ConstFoc,
- * getfld_Sol, getfld_DTL/CCDTL/CCL/SC), with a read-in or CSR wake applied as
+ * 101..106 over Fourier coefficients (getfld_Quadrupole, getfld_ConstFoc,
+ * getfld_Sol, getfld_DTL/CCDTL/CCL/SC, getfld_SolRF with its solenoid
+ * series scaled by Param(12), getfld_TWS), with a read-in or CSR wake applied as
  * kick2wake does (BeamBunch.f90:5048-5938); a run with any other element
  * under it, or a quadrupole with 0 < Param(3) <= 1e-5 (whose field reads
  * unset derivatives there), is IMPZ_ERR_UNSUPPORTED. */

@@ -1478,6 +1478,11 @@ typedef struct {
   /* the RF cavities' terms at z that getfldpts_DTL / getfldpts_CCL
    * compute once per call (DTL.f90:858-958, CCL.f90:722-809) */
   double bgrad, ez1, ezp1, f1, f1p, ww, theta0, xl, clite;
+  /* SolRF / TWS (SolRF.f90:482-628, TWS.f90): inside the element, the
+   * first series' terms (on1), and the second series' (on2): TWS's second
+   * wave at theta0 + theta2, or SolRF's solenoid (bscale times the sums) */
+  int inside, on1, on2;
+  double xlrep, tsc, w1[4], w2[4], sol[4], theta2;
 } lorentz_kick;
 
 static void kick_common(double *pts, int n, const double *phi, const int mesh[3],
@@ -1546,6 +1551,80 @@ static void lz_rf_axis(lorentz_kick *lz) {
   lz->f1p = -((ezppp + ezp1 / lz->xl / lz->xl) / 4);
 }
 
+/* one Fourier series of getfld_SolRF / getfld_TWS: npar terms from
+ * Fcoef(ntmp+1) at zz over the period zlen; Ez and three derivatives */
+static void lz_series(const orc_elem *e, int ntmp, int npar, double zz, double zlen, double pi,
+                      double out[4]) {
+  double ez1 = fcoef(e, ntmp + 1) / 2, ezp1 = 0.0, ezpp1 = 0.0, ezppp = 0.0;
+  for (int i = 2; i <= (npar - 1) / 2 + 1; i++) {
+    const double a = fcoef(e, 2 * i - 2 + ntmp), b = fcoef(e, 2 * i - 1 + ntmp);
+    ez1 = ez1 + a * cos((i - 1) * 2 * pi * zz / zlen) + b * sin((i - 1) * 2 * pi * zz / zlen);
+    ezp1 = ezp1 + (i - 1) * 2 * pi / zlen *
+                      (-(a * sin((i - 1) * 2 * pi * zz / zlen)) +
+                       b * cos((i - 1) * 2 * pi * zz / zlen));
+    const double k = (i - 1) * 2 * pi / zlen;
+    ezpp1 = ezpp1 + k * k *
+                        (-(a * cos((i - 1) * 2 * pi * zz / zlen)) -
+                         b * sin((i - 1) * 2 * pi * zz / zlen));
+    ezppp = ezppp + k * k * k *
+                        (a * sin((i - 1) * 2 * pi * zz / zlen) -
+                         b * cos((i - 1) * 2 * pi * zz / zlen));
+  }
+  out[0] = ez1;
+  out[1] = ezp1;
+  out[2] = ezpp1;
+  out[3] = ezppp;
+}
+
+/* the on-axis part of getfld_SolRF / getfld_TWS at z */
+static void lz_rfw_axis(lorentz_kick *lz) {
+  const orc_elem *e = lz->e;
+  const double clite = (double)299792458.0f;
+  const double pi = (double)(2 * asinf(1.0f));
+  const double zedge = lz->zedge, z = lz->z, escale = e->val[0], len = e->length;
+  lz->inside = z > zedge && z < zedge + len;
+  if (!lz->inside) return;
+  lz->ww = e->val[1] * 2 * pi;
+  lz->xlrep = lz->ww / clite;
+  lz->theta0 = e->val[2] * (double)asinf(1.0f) / 90;
+  lz->tsc = 2 * pi * PC.Scfreq;
+  lz->clite = clite;
+  const double zlc = z - zedge;
+  const int numpar1 = (int)(fcoef(e, 1) + 0.1);
+  const double zstart1 = fcoef(e, 2), zend1 = fcoef(e, 3), zlength1 = fcoef(e, 4);
+  double t[4];
+  lz->on1 = zlc >= zstart1 && zlc <= zend1;
+  if (lz->on1) {
+    const double zmid = zlength1 / 2;
+    lz_series(e, 4, numpar1, z - zedge - zstart1 - zmid, zlength1, pi, t);
+    const double ez1 = t[0] * escale, ezp1 = t[1] * escale;
+    const double ezpp1 = t[2] * escale, ezppp = t[3] * escale;
+    lz->w1[0] = ez1;
+    lz->w1[1] = ezp1;
+    lz->w1[2] = -((ezpp1 + ez1 * lz->xlrep * lz->xlrep) / 4);
+    lz->w1[3] = -((ezppp + ezp1 * lz->xlrep * lz->xlrep) / 4);
+  }
+  const int numpar2 = (int)(fcoef(e, 5 + numpar1) + 0.1);
+  const double zstart2 = fcoef(e, 6 + numpar1), zend2 = fcoef(e, 7 + numpar1);
+  const double zlength2 = fcoef(e, 8 + numpar1);
+  lz->theta2 = e->val[10] * pi / 180;
+  lz->on2 = zlc >= zstart2 && zlc <= zend2;
+  if (lz->on2) {
+    const double zmid = zlength2 / 2;
+    lz_series(e, numpar1 + 8, numpar2, z - zedge - zstart2 - zmid, zlength2, pi, t);
+    if (e->type == 106) {
+      const double ez1 = t[0] * escale, ezp1 = t[1] * escale;
+      const double ezpp1 = t[2] * escale, ezppp = t[3] * escale;
+      lz->w2[0] = ez1;
+      lz->w2[1] = ezp1;
+      lz->w2[2] = -((ezpp1 + ez1 * lz->xlrep * lz->xlrep) / 4);
+      lz->w2[3] = -((ezppp + ezp1 * lz->xlrep * lz->xlrep) / 4);
+    } else {
+      for (int i = 0; i < 4; i++) lz->sol[i] = t[i];
+    }
+  }
+}
+
 static lorentz_kick lz_make(const orc_elem *e, double zedge, double z, double tg, double qmi) {
   lorentz_kick lz;
   memset(&lz, 0, sizeof(lz));
@@ -1556,6 +1635,7 @@ static lorentz_kick lz_make(const orc_elem *e, double zedge, double z, double tg
   lz.qmi = qmi;
   lz.wraw = NULL;
   if (e->type >= 101 && e->type <= 104) lz_rf_axis(&lz);
+  if (e->type == 105 || e->type == 106) lz_rfw_axis(&lz);
   return lz;
 }
 
@@ -1662,6 +1742,35 @@ static void lz_getfld(const lorentz_kick *lz, const double pos[4], double f[6]) 
     f[2] = f[2] + tmpez;
     f[3] = f[3] + tmpbx;
     f[4] = f[4] + tmpby;
+  } else if ((lz->e->type == 105 || lz->e->type == 106) && lz->inside) {
+    /* the per-particle lines of getfld_SolRF (SolRF.f90:482-628) and
+     * getfld_TWS (TWS.f90) with the on-axis terms of lz_rfw_axis */
+    const double tt = pos[3] / lz->tsc;
+    const double r2 = pos[0] * pos[0] + pos[1] * pos[1];
+    for (int w = 0; w < 2; w++) {
+      const double *c = w == 0 ? lz->w1 : lz->w2;
+      if (w == 0 ? !lz->on1 : !(lz->on2 && lz->e->type == 106)) continue;
+      const double ph = w == 0 ? lz->ww * tt + lz->theta0 : lz->ww * tt + lz->theta0 + lz->theta2;
+      const double tmpcos = cos(ph), tmpsin = sin(ph);
+      const double tmpex = -(pos[0] * (c[1] / 2 + c[3] * r2 / 4) * tmpcos);
+      const double tmpey = -(pos[1] * (c[1] / 2 + c[3] * r2 / 4) * tmpcos);
+      const double tmpez = (c[0] + c[2] * r2) * tmpcos;
+      const double tmpbx = pos[1] * lz->xlrep / lz->clite * (c[0] / 2 + c[2] * r2 / 4) * tmpsin;
+      const double tmpby =
+          -(pos[0] * lz->xlrep / lz->clite * (c[0] / 2 + c[2] * r2 / 4) * tmpsin);
+      f[0] = f[0] + tmpex;
+      f[1] = f[1] + tmpey;
+      f[2] = f[2] + tmpez;
+      f[3] = f[3] + tmpbx;
+      f[4] = f[4] + tmpby;
+    }
+    if (lz->on2 && lz->e->type == 105) {
+      const double bscale = lz->e->val[10];
+      const double ez1 = lz->sol[0], ezp1 = lz->sol[1], ezpp1 = lz->sol[2], ezppp = lz->sol[3];
+      f[3] = f[3] - bscale * ezp1 / 2 * pos[0] + bscale * ezppp * pos[0] * r2 / 16;
+      f[4] = f[4] - bscale * ezp1 / 2 * pos[1] + bscale * ezppp * pos[1] * r2 / 16;
+      f[5] = f[5] + bscale * ez1 - bscale * ezpp1 * r2 / 4;
+    }
   }
 }
 
@@ -2563,11 +2672,12 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     const int lorentz = beam->flagmap == 2;
     /* Lorentz integrator: drifts, quadrupoles (not 0 < Param(3) <= 1e-5,
      * where getfld_Quadrupole reads G', G'' it never set), constant
-     * focusing, solenoids and the RF cavities 101..104 over Fourier
+     * focusing, solenoids and the RF cavities 101..106 over Fourier
      * coefficients */
     if (lorentz && !(bitype == 0 || bitype == 2 || bitype == 3 ||
                      (bitype == 1 && (e->val[1] <= 0.0 || e->val[1] > 1.0e-5)) ||
-                     (bitype >= 101 && bitype <= 104 && e->zdat && e->ndata >= 1))) {
+                     (bitype >= 101 && bitype <= 104 && e->zdat && e->ndata >= 1) ||
+                     ((bitype == 105 || bitype == 106) && e->zdat && e->ndata >= 5))) {
       free(rho);
       return -10;
     }

@@ -196,3 +196,36 @@ def test_lorentz_rf_cavities_match_the_oracle(current, form, cols, tol):
     rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], mass, freq)
                        for i in range(len(recs))])
     assert worst(rows_g, rows_o, cols) <= tol
+
+
+@pytest.mark.parametrize("current,form,cols,tol", [
+    (0.010, impz.FORM_FP64, RMS_COLS, 1e-8),
+    (0.0, impz.FORM_FP64, RMS_COLS, 1e-10)])
+def test_lorentz_solrf_and_tws_match_the_oracle(current, form, cols, tol):
+    """A SolRF (105: the cavity's series and the solenoid's Bz profile
+    scaled by Param(12)) and a TWS (106: two waves, the second 90 degrees
+    on over the middle) under kick2 (getfld_SolRF, getfld_TWS)."""
+    from test_abi import tws_coefficients
+    from test_lorentz import solrf_two_series
+    mass, freq = beams.PROTON_MASS_EV, 402.5e6
+    pts, ref = beams.gaussian_bunch(20_000, seed=beams.SEED0 + 86, mass=mass, charge=1.0,
+                                    ekin=2.5e6, current=current, freq=freq)
+    lat = [impz.elem(105, 0.2, 16, 20, [1e6, freq, 60.0, 1.0, 1.0, 0, 0, 0, 0, 0, 0.5],
+                     rf=solrf_two_series()),
+           impz.elem(0, 0.05, 4, 1, [1.0]),
+           impz.elem(106, 0.2, 16, 20, [1e6, freq, 60.0, 1.0, 1.0, 0, 0, 0, 0, 0, 90.0],
+                     rf=tws_coefficients())]
+    grid = (32, 32, 64)
+    rows_o, _, beam = orc.run(lat, pts, current, mass, 1.0, freq, ref, grid, flagmap=2)
+    b = impz.Bunch(pts, current, mass, 1.0, freq, ref, grid, form=form, track_ids=False)
+    try:
+        b.set_integrator(2)
+        recs, zs = b.run(lat)
+        refs = b.run_reference()
+    finally:
+        b.close()
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    np.testing.assert_array_equal(refs[-1], np.array(beam.refptcl[:]))
+    rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], mass, freq)
+                       for i in range(len(recs))])
+    assert worst(rows_g, rows_o, cols) <= tol

@@ -288,3 +288,35 @@ def test_example1_dtl_cells_on_the_oracle():
     assert gain > 1e-4  # the cells accelerate
     assert abs(-ref[5] - y[0]) < 1e-5 * gain
     assert abs(ref[4] - y[1]) < 1e-6 * y[1]
+
+
+def solrf_two_series(length=0.2):
+    """getfld_SolRF's two series: the cavity's Ez, then the solenoid's Bz
+    profile (a constant 1 over the element, scaled by Param(12))."""
+    from test_abi import solrf_coefficients
+    rf = list(solrf_coefficients(length))
+    return np.array(rf + [1, 0.0, length, length, 2.0])
+
+
+@pytest.mark.parametrize("etype", [105, 106])
+def test_solrf_and_tws_under_kick2_gain_the_map_integrators_energy(etype):
+    """getfld_SolRF / getfld_TWS (SolRF.f90:482-628, TWS.f90) under kick2:
+    the reference particle's energy gain converges, at second order, to
+    maplinear_SolRF / maplinear_TWS's RK6 over the same coefficients."""
+    from test_abi import tws_coefficients
+    mass, freq = beams.PROTON_MASS_EV, 402.5e6
+    pts, ref = beams.gaussian_bunch(2000, seed=beams.SEED0 + 85, mass=mass, charge=1.0,
+                                    ekin=2.5e6, current=0.0, freq=freq)
+    coef = solrf_two_series() if etype == 105 else tws_coefficients()
+    vals = [1e6, freq, 60.0, 1.0, 1.0, 0, 0, 0, 0, 0, 0.2 if etype == 105 else 90.0]
+    gaps = []
+    for nseg in (40, 160):
+        lat = [impz.elem(etype, 0.2, nseg, 20, vals, rf=coef)]
+        _, _, b1 = orc.run(lat, pts, 0.0, mass, 1.0, freq, ref, (16, 16, 32), flagmap=1)
+        _, _, b2 = orc.run(lat, pts, 0.0, mass, 1.0, freq, ref, (16, 16, 32), flagmap=2)
+        gain1 = -b1.refptcl[5] + ref[5]
+        assert abs(gain1) > 1e-5
+        gaps.append(abs((-b2.refptcl[5] + ref[5]) / gain1 - 1))
+    # the 0.2 m element spans about four beta-lambda, so the splitting error
+    # is larger than in one DTL cell: 1e-2 at 40 steps, 6e-4 at 160
+    assert gaps[0] > 8 * gaps[1] and gaps[1] < 1e-3, gaps
