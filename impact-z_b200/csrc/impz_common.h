@@ -66,6 +66,10 @@ struct MapOp {
 //                B += (-bz'/2 X + bz''' X r^2/16, same with Y, bz - bz'' r^2/4),
 //                or TWS 106's second wave (ez1, ez1', f1, f1', theta2) at
 //                phi + theta2)
+//   LZ_MULT      multipole 5 (getfld_Multipole, MAD notation), c = (G, id):
+//                sextupole (id 2) B = (G X Y, G (X^2 - Y^2)/2, 0), octupole
+//                (3) G (3 X^2 Y - Y^3)/6, G (X^3 - 3 X Y^2)/6, decapole (4)
+//                G (X^3 Y - X Y^3)/6, G (X^4 - 6 X^2 Y^2 + Y^4)/24
 enum LzKind {
   LZ_NONE = 0,
   LZ_QUAD = 1,
@@ -75,7 +79,8 @@ enum LzKind {
   LZ_CONSTFOC = 5,
   LZ_RF = 6,
   LZ_SOLRF = 7,
-  LZ_TWS = 8
+  LZ_TWS = 8,
+  LZ_MULT = 9
 };
 
 struct MapProgram {

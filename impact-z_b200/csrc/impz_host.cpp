@@ -673,6 +673,7 @@ double pipe_radius(const impz_elem_t& e) {
     case 2: return e.val[3];  // ConstFoc: Param(5)
     case 3: return e.val[2];  // Sol: Param(4)
     case 4: return e.val[3];
+    case 5: return e.val[3];  // Multipole: Param(5)
     default: return e.val[4];
   }
 }
@@ -1142,6 +1143,34 @@ bool lorentz_field(const Phys& P, const impz_elem_t& e, double zedge, double z, 
       kind = LZ_RF;
       rf_fourier_field(P, e, zedge, z, tg, c, ez0);
       return true;
+    case 5: {
+      // getfld_Multipole (Multipole.f90:403-452): Param(2) the order,
+      // Param(3) the strength, or with Param(4) > 0 the profile
+      // getfldfrg_Multipole interpolates (Multipole.f90:455-480) from the
+      // element's (z, G) table
+      const int idpole = (int)(e.val[0] + 0.1);
+      if (idpole < 2 || idpole > 4) return false;
+      kind = LZ_MULT;
+      c[1] = idpole;
+      if (e.val[2] > 0.0) {
+        if (!e.zdat || !e.edat || e.ndata < 2) return false;
+        const double zz = z - zedge;
+        int klo = 1, khi = e.ndata;
+        const double* zd = e.zdat - 1;
+        const double* ed = e.edat - 1;
+        while (khi - klo > 1) {
+          const int k = (khi + klo) / 2;
+          if (zd[k] > zz) khi = k;
+          else klo = k;
+        }
+        const double hstep = zd[khi] - zd[klo];
+        const double slope = (ed[khi] - ed[klo]) / hstep;
+        c[0] = ed[klo] + slope * (zz - zd[klo]);
+      } else {
+        c[0] = e.val[1];
+      }
+      return true;
+    }
     case 105:
     case 106:
       // TWS needs both series; SolRF's solenoid series may be absent (the
@@ -1189,8 +1218,8 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     const int bnseg = e.nseg, bitype = e.type;
     double piperad = pipe_radius(e), piperad2 = piperad;
     // the Lorentz integrator covers drifts, quadrupoles, constant focusing,
-    // solenoids and the RF cavities 101..106, whose fields kick2 applies
-    // (lorentz_field)
+    // solenoids, multipoles and the RF cavities 101..106, whose fields
+    // kick2 applies (lorentz_field)
     const bool lorentz = csr.flagmap == 2;
     if (lorentz) {
       int kind;

@@ -660,8 +660,8 @@ __device__ __forceinline__ double moment_tail(double acc1, int lane) {
 // The element's field at (X, Y) [m] and time T of one particle
 // (getfld_Quadrupole, Quadrupole.f90:369-402; getfld_Sol, Sol.f90:391-435;
 // getfld_ConstFoc, ConstFoc.f90:297-322; getfldpts_DTL, DTL.f90:858-958,
-// and the CCDTL, CCL, SC forms; getfld_SolRF, getfld_TWS; LzKind), in the
-// reference's expression forms; e = E, b = B.
+// and the CCDTL, CCL, SC forms; getfld_SolRF, getfld_TWS; getfld_Multipole;
+// LzKind), in the reference's expression forms; e = E, b = B.
 __device__ __forceinline__ void lz_field(int kind, const double* __restrict__ c, double X,
                                          double Y, double T, const Consts& k, double& ex,
                                          double& ey, double& ez, double& bx, double& by,
@@ -708,6 +708,19 @@ __device__ __forceinline__ void lz_field(int kind, const double* __restrict__ c,
       bx = bx - c[9] / 2 * X + c[11] * X * r2 / 16;
       by = by - c[9] / 2 * Y + c[11] * Y * r2 / 16;
       bz = bz + c[8] - c[10] * r2 / 4;
+    }
+  } else if (kind == LZ_MULT) {
+    // getfld_Multipole (Multipole.f90:403-452)
+    const double g = c[0];
+    if (c[1] == 2.0) {
+      bx = g * Y * X;
+      by = g * (X * X - Y * Y) / 2;
+    } else if (c[1] == 3.0) {
+      bx = g * (3 * (X * X) * Y - Y * Y * Y) / 6;
+      by = g * (X * X * X - 3 * X * (Y * Y)) / 6;
+    } else {
+      bx = g * (X * X * X * Y - X * (Y * Y * Y)) / 6;
+      by = g * ((X * X) * (X * X) - 6 * (X * X) * (Y * Y) + (Y * Y) * (Y * Y)) / 24;
     }
   } else if (kind == LZ_QUAD) {
     bx = c[0] * Y;

@@ -134,13 +134,17 @@ int impz_wake_off(impz_bunch_t b);
  * (drift2 half steps around kick2/scatter2, BeamBunch.f90:467-509,
  * 2187-3071, or scatter20 without current), here for drifts, quadrupoles
  * (hard edge, or the Enge fringe of getfldfrgAna2_Quadrupole when
- * Param(3) > 1e-5), constant focusing, solenoids and the RF cavities
+ * Param(3) > 1e-5), constant focusing, solenoids, multipoles (type 5:
+ * sextupole, octupole, decapole by Param(2); with Param(4) > 0 the
+ * gradient profile of the element's (zdat, edat) table), the RF cavities
  * 101..106 over Fourier coefficients (getfld_Quadrupole, getfld_ConstFoc,
  * getfld_Sol, getfld_DTL/CCDTL/CCL/SC, getfld_SolRF with its solenoid
  * series scaled by Param(12), getfld_TWS), with a read-in or CSR wake applied as
  * kick2wake does (BeamBunch.f90:5048-5938); a run with any other element
  * under it, or a quadrupole with 0 < Param(3) <= 1e-5 (whose field reads
- * unset derivatives there), is IMPZ_ERR_UNSUPPORTED. */
+ * unset derivatives there), is IMPZ_ERR_UNSUPPORTED.  Bends stay outside:
+ * getfld_Dipole takes pole-face coefficients from the last rfdata file read
+ * (nothing loads them for a bend) on top of the sector map's bending. */
 int impz_set_integrator(impz_bunch_t b, int flagmap);
 /* sizeof(StepParams): the bytes per step of the step table a run uploads. */
 int impz_step_params_size(void);

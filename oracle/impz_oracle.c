@@ -1742,6 +1742,38 @@ static void lz_getfld(const lorentz_kick *lz, const double pos[4], double f[6]) 
     f[2] = f[2] + tmpez;
     f[3] = f[3] + tmpbx;
     f[4] = f[4] + tmpby;
+  } else if (lz->e->type == 5) {
+    /* getfld_Multipole (Multipole.f90:403-452), MAD notation, with
+     * getfldfrg_Multipole's interpolation (455-480) for Param(4) > 0 */
+    const int idpole = (int)(lz->e->val[0] + 0.1);
+    double bgrad;
+    if (lz->e->val[2] > 0.0) {
+      int klo = 1, khi = lz->e->ndata;
+      const double *zd = lz->e->zdat - 1, *ed = lz->e->edat - 1;
+      while (khi - klo > 1) {
+        const int k = (khi + klo) / 2;
+        if (zd[k] > zz)
+          khi = k;
+        else
+          klo = k;
+      }
+      const double hstep = zd[khi] - zd[klo];
+      const double slope = (ed[khi] - ed[klo]) / hstep;
+      bgrad = ed[klo] + slope * (zz - zd[klo]);
+    } else {
+      bgrad = lz->e->val[1];
+    }
+    const double x = pos[0], y = pos[1];
+    if (idpole == 2) {
+      f[3] = bgrad * y * x;
+      f[4] = bgrad * (x * x - y * y) / 2;
+    } else if (idpole == 3) {
+      f[3] = bgrad * (3 * (x * x) * y - y * y * y) / 6;
+      f[4] = bgrad * (x * x * x - 3 * x * (y * y)) / 6;
+    } else {
+      f[3] = bgrad * (x * x * x * y - x * (y * y * y)) / 6;
+      f[4] = bgrad * ((x * x) * (x * x) - 6 * (x * x) * (y * y) + (y * y) * (y * y)) / 24;
+    }
   } else if ((lz->e->type == 105 || lz->e->type == 106) && lz->inside) {
     /* the per-particle lines of getfld_SolRF (SolRF.f90:482-628) and
      * getfld_TWS (TWS.f90) with the on-axis terms of lz_rfw_axis */
@@ -2634,6 +2666,7 @@ static double pipe_radius(const orc_elem *e) {
     case 2: return e->val[3];  /* ConstFoc Param(5) */
     case 3: return e->val[2];  /* Sol Param(4) */
     case 4: return e->val[3];  /* Dipole Param(5) */
+    case 5: return e->val[3];  /* Multipole Param(5) */
     default: return e->val[4]; /* RF gaps Param(6) */
   }
 }
@@ -2677,7 +2710,10 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     if (lorentz && !(bitype == 0 || bitype == 2 || bitype == 3 ||
                      (bitype == 1 && (e->val[1] <= 0.0 || e->val[1] > 1.0e-5)) ||
                      (bitype >= 101 && bitype <= 104 && e->zdat && e->ndata >= 1) ||
-                     ((bitype == 105 || bitype == 106) && e->zdat && e->ndata >= 5))) {
+                     ((bitype == 105 || bitype == 106) && e->zdat && e->ndata >= 5) ||
+                     (bitype == 5 && (int)(e->val[0] + 0.1) >= 2 &&
+                      (int)(e->val[0] + 0.1) <= 4 &&
+                      (e->val[2] <= 0.0 || (e->zdat && e->edat && e->ndata >= 2))))) {
       free(rho);
       return -10;
     }

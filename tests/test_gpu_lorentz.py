@@ -229,3 +229,32 @@ def test_lorentz_solrf_and_tws_match_the_oracle(current, form, cols, tol):
     rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], mass, freq)
                        for i in range(len(recs))])
     assert worst(rows_g, rows_o, cols) <= tol
+
+
+@pytest.mark.parametrize("form,cols,tol", [
+    (impz.FORM_FP64, RMS_COLS, 1e-8),
+    (impz.FORM_FP32CONV, [7, 9, 11, 13, 15, 17, 19, 21, 23], 1e-5)])
+def test_lorentz_multipoles_match_the_oracle(form, cols, tol):
+    """Sextupole, octupole and decapole (getfld_Multipole, MAD notation)
+    between drifts and a quadrupole, with space charge, under kick2."""
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 88)
+    lat = [impz.elem(0, 0.1, 4, 1, [1.0]),
+           impz.elem(5, 0.05, 4, 1, [2, 3.0e3, 0.0, 1.0]),
+           impz.elem(1, 0.1, 4, 1, [20.0, 0.0, 1.0]),
+           impz.elem(5, 0.05, 4, 1, [3, 2.0e6, 0.0, 1.0]),
+           impz.elem(5, 0.05, 4, 1, [4, 1.0e9, 0.0, 1.0]),
+           impz.elem(0, 0.1, 4, 1, [1.0])]
+    rows_o, _, beam = orc.run(lat, cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"],
+                              cfg["freq"], cfg["refptcl"], cfg["grid"], flagmap=2)
+    b = impz.Bunch(cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=form, track_ids=False)
+    try:
+        b.set_integrator(2)
+        recs, zs = b.run(lat)
+        refs = b.run_reference()
+    finally:
+        b.close()
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], cfg["mass"], cfg["freq"])
+                       for i in range(len(recs))])
+    assert worst(rows_g, rows_o, cols) <= tol

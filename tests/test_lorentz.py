@@ -320,3 +320,33 @@ def test_solrf_and_tws_under_kick2_gain_the_map_integrators_energy(etype):
     # the 0.2 m element spans about four beta-lambda, so the splitting error
     # is larger than in one DTL cell: 1e-2 at 40 steps, 6e-4 at 160
     assert gaps[0] > 8 * gaps[1] and gaps[1] < 1e-3, gaps
+
+
+@pytest.mark.parametrize("idpole,g", [(2, 3.0e3), (3, 2.0e6), (4, 1.0e9)])
+def test_multipole_kick_is_getfld_multipole(idpole, g):
+    """One kick2 step of a 2 cm multipole without current: with only Bx,
+    By the implicit update is exactly px -= c q/m tau By, py += c q/m tau
+    Bx at the position after the first drift2 (getfld_Multipole's MAD
+    fields, Multipole.f90:403-452); pt does not move."""
+    cfg = beams.fodo_1e5(n=500, seed=beams.SEED0 + 87)
+    p0, ref = cfg["pts"], cfg["refptcl"]
+    tau, clight = 0.02, 299792458.0
+    scxl = clight / (2 * np.pi * cfg["freq"])
+    _, p1, _ = _lz_run([impz.elem(5, tau, 1, 1, [idpole, g, 0.0, 1.0])], cfg)
+    g0 = -ref[5]
+    pz = np.sqrt((g0 - p0[:, 5]) * (g0 - p0[:, 5]) - 1.0 - p0[:, 1] * p0[:, 1] -
+                 p0[:, 3] * p0[:, 3])
+    x = (p0[:, 0] + 0.5 * tau * p0[:, 1] / (scxl * pz)) * scxl
+    y = (p0[:, 2] + 0.5 * tau * p0[:, 3] / (scxl * pz)) * scxl
+    if idpole == 2:
+        bx, by = g * y * x, g * (x * x - y * y) / 2
+    elif idpole == 3:
+        bx, by = g * (3 * (x * x) * y - y * y * y) / 6, g * (x * x * x - 3 * x * (y * y)) / 6
+    else:
+        bx = g * (x * x * x * y - x * (y * y * y)) / 6
+        by = g * ((x * x) * (x * x) - 6 * (x * x) * (y * y) + (y * y) * (y * y)) / 24
+    r7 = p0[:, 6]
+    np.testing.assert_allclose(p1[:, 1], p0[:, 1] - clight * by * tau * r7, rtol=1e-14, atol=0)
+    np.testing.assert_allclose(p1[:, 3], p0[:, 3] + clight * bx * tau * r7, rtol=1e-14, atol=0)
+    np.testing.assert_array_equal(p1[:, 5], p0[:, 5])
+    assert np.max(np.abs(p1[:, 1] - p0[:, 1])) > 0.05 * np.max(np.abs(p0[:, 1]))
