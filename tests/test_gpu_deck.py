@@ -121,3 +121,55 @@ def test_checkpoint_and_restart(tmp_path):
     for c in RMS_COLS:
         scale = np.max(np.abs(tail[:, c])) + 1e-300
         assert np.max(np.abs(rows_r[:, c] - tail[:, c])) / scale <= 1e-10, c
+
+
+def test_lorentz_dtl_deck_matches_the_oracle(tmp_path):
+    """A deck shaped like the reference's Example1: Flagmap=2 (the Lorentz
+    integrator) over DTL cells whose rfdataN.in hold Fourier coefficients
+    (read3_Data), a quadrupole and a drift, with space charge, then a -25
+    switch to the map integrator for a last drift and quadrupole; run_deck
+    on the GPU against the oracle over the same segments."""
+    from test_lorentz import rf_cell
+    wd = str(tmp_path)
+    n, mass, freq, cur = 4000, beams.PROTON_MASS_EV, 324e6, 0.03
+    pts, _ = beams.gaussian_bunch(n, seed=beams.SEED0 + 89, mass=mass, charge=1.0,
+                                  ekin=3.35e6, current=cur, freq=freq)
+    d = deck.Deck(np=n, flagmap=2, nx=32, ny=32, nz=64, xrad=0.02, yrad=0.02, perdlen=0.1,
+                  nptlist=[n], currlist=[cur], qmcclist=[float(pts[0, 6])], bcurr=cur,
+                  bkenergy=3.35e6, bmass=mass, bcharge=1.0, bfreq=freq, phsini=0.0)
+    z24 = lambda *v: list(v) + [0.0] * (24 - len(v))  # noqa: E731
+    coef, _ = rf_cell()
+    for fid, scale in ((852, 1.0), (868, 0.9)):
+        np.savetxt(os.path.join(wd, "rfdata%d.in" % fid), coef * scale)
+    cell = lambda fid, th: deck.Element(  # noqa: E731
+        0.08, 12, 20, 101, z24(2.5e6, freq, th, fid, 0.0065, 0.02, 68.0, 0.02, -67.0))
+    d.elements = [
+        cell(852, 222.0), cell(868, 218.0), cell(852, 214.0),
+        deck.Element(0.045, 4, 20, 1, z24(-19.15, 0.0, 0.009)),
+        deck.Element(0.09, 6, 20, 0, z24(0.009)),
+        deck.Element(0.0, 0, 1, -25, z24()),
+        deck.Element(0.05, 4, 1, 0, z24(0.009)),
+        deck.Element(0.045, 4, 1, 1, z24(18.9, 0.0, 0.011)),
+        deck.Element(0.0, 0, 0, -99, z24()),
+    ]
+    deck.write_deck(os.path.join(wd, "ImpactZ.in"), d)
+    deck.write_particles(os.path.join(wd, "particle.in"), pts)
+    out = deck.run_deck(wd)
+    ref, z, rows_o, fm = d.refptcl(), 0.0, [], d.flagmap
+    for kind, item in deck.lattice_segments(d, wd):
+        if kind == "run":
+            seg, pts, beam = orc.run(item, pts, d.bcurr, d.bmass, d.bcharge, d.bfreq, ref,
+                                     (d.nx, d.ny, d.nz), z, flagmap=fm)
+            ref, z = np.array(beam.refptcl[:]), beam.z
+            rows_o += list(seg[1:] if rows_o else seg)
+        elif kind == "integrator":
+            fm = item
+    assert fm == 1
+    rows_o = np.array(rows_o)
+    rows_g = out["rows"]
+    assert rows_g.shape == rows_o.shape == (1 + 3 * 12 + 4 + 6 + 4 + 4, 45)
+    np.testing.assert_allclose(rows_g[:, 0], rows_o[:, 0], rtol=0, atol=0)
+    assert rows_o[-1, 2] > rows_o[0, 2]  # the cells accelerate (fort.18 gamma)
+    for c in RMS_COLS:
+        scale = np.max(np.abs(rows_o[:, c])) + 1e-300
+        assert np.max(np.abs(rows_g[:, c] - rows_o[:, c])) / scale <= 1e-8, c
