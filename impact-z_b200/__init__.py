@@ -93,6 +93,9 @@ _SIGS = {
     "impz_deposit": (ctypes.c_int, [_B, _D, _I]),
     "impz_poisson_open": (ctypes.c_int, [_B, _D]),
     "impz_kick": (ctypes.c_int, [_B, ctypes.c_double, _D]),
+    "impz_drift2": (ctypes.c_int, [_B, _D, ctypes.c_double]),
+    "impz_kick2": (ctypes.c_int, [_B, _E, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                  _D]),
     "impz_moments": (ctypes.c_int, [_B, _D]),
     "impz_diag_row": (ctypes.c_int, [ctypes.c_double, _D, _D, ctypes.c_double, ctypes.c_double,
                                      _D]),
@@ -420,6 +423,20 @@ class Bunch:
     def kick(self, tau, want_e=False):
         eg = np.zeros(3 * int(np.prod(self.grid))) if want_e else None
         _check(lib().impz_kick(self.h, tau, _dp(eg)), "impz_kick")
+        return eg
+
+    def drift2(self, z, tau):
+        """drift2_BeamBunch by tau/2 (the Lorentz integrator's half step);
+        returns the new z."""
+        zc = ctypes.c_double(z)
+        _check(lib().impz_drift2(self.h, ctypes.byref(zc), tau), "impz_drift2")
+        return zc.value
+
+    def kick2(self, e, zedge, z, tau, want_e=False):
+        """kick2_BeamBunch in element e at z (scatter2 after a solve, or
+        scatter20 for a bunch without current)."""
+        eg = np.zeros(3 * int(np.prod(self.grid))) if want_e else None
+        _check(lib().impz_kick2(self.h, ctypes.byref(e), zedge, z, tau, _dp(eg)), "impz_kick2")
         return eg
 
     def moments(self):

@@ -410,6 +410,8 @@ bool program_is_light(const MapProgram& prog) {
 
 bool table_is_light(const std::vector<StepParams>& steps) {
   for (const StepParams& sp : steps)
+    if (sp.lorentz) return false;  // the Lorentz kick is in the full pass only
+  for (const StepParams& sp : steps)
     if (!program_is_light(sp.post) || !program_is_light(sp.pre_next)) return false;
   return true;
 }
@@ -1143,10 +1145,9 @@ int impz_poisson_open(impz_bunch_t b, double* phi) {
   return IMPZ_OK;
 }
 
-int impz_kick(impz_bunch_t b, double tau, double* egrid) {
-  if (!b) return IMPZ_ERR_ARG;
-  if (b->stage != ST_SOLVED) return IMPZ_ERR_STATE;
-  CK(cudaSetDevice(b->device));
+// The node field of the last solve, and optionally its copy to the host
+// as kick1's egx, egy, egz.
+static int kick_field(impz_bunch_t b, double* egrid) {
   int r = solve_efield(b);
   if (r) return r;
   if (egrid) {
@@ -1162,6 +1163,15 @@ int impz_kick(impz_bunch_t b, double tau, double* egrid) {
     if (b->f32())
       for (long long i = 0; i < 3 * b->G; i++) egrid[i] *= b->weight;
   }
+  return IMPZ_OK;
+}
+
+int impz_kick(impz_bunch_t b, double tau, double* egrid) {
+  if (!b) return IMPZ_ERR_ARG;
+  if (b->stage != ST_SOLVED) return IMPZ_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  int r = kick_field(b, egrid);
+  if (r) return r;
   StepParams h[2];
   blank_steps(h);
   h[0].sc = 1;
@@ -1170,6 +1180,58 @@ int impz_kick(impz_bunch_t b, double tau, double* egrid) {
   h[0].tau = tau;
   b->stage = ST_IDLE;
   return run_fine_advance(b, h, 1, 0, 0, nullptr);
+}
+
+int impz_drift2(impz_bunch_t b, double* z, double tau) {
+  if (!b || !z) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  StepParams h[2];
+  blank_steps(h);
+  double ref[6];
+  std::memcpy(ref, b->refptcl, sizeof(ref));
+  int r = drift2_op(b->P, tau, ref, h[0].post);
+  if (r) return r;
+  r = run_fine_advance(b, h, 0, 1, 0, nullptr);
+  if (r) return r;
+  std::memcpy(b->refptcl, ref, sizeof(ref));
+  *z = *z + 0.5 * tau;
+  b->z = *z;
+  return IMPZ_OK;
+}
+
+int impz_kick2(impz_bunch_t b, const impz_elem_t* e, double zedge, double z, double tau,
+               double* egrid) {
+  if (!b || !e) return IMPZ_ERR_ARG;
+  const bool sc = b->stage == ST_SOLVED;
+  // AccSimulator.f90:1122: no space charge below 1e-10 A
+  if (!sc && !(b->current0 < 1.0e-10)) return IMPZ_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  StepParams h[2];
+  blank_steps(h);
+  double ref[6];
+  std::memcpy(ref, b->refptcl, sizeof(ref));
+  h[0].lorentz = 1;
+  h[0].tau = tau;
+  if (!lorentz_kick_terms(b->P, *e, zedge, z, tau, b->sp, ref, h[0].lz_kind, h[0].lz_c,
+                          h[0].lz_tg, h[0].lz_ez0))
+    return IMPZ_ERR_UNSUPPORTED;
+  int r;
+  if (sc) {
+    r = kick_field(b, egrid);
+    if (r) return r;
+    h[0].sc = 1;
+    h[0].gam = b->sc_gam;
+    h[0].rad = b->sc_rad;
+    b->stage = ST_IDLE;
+    r = run_fine_advance(b, h, 1, 0, 0, nullptr);
+  } else {
+    // scatter20: the element's field alone, in the particle pass's post phase
+    h[0].gam = -b->refptcl[5];
+    r = run_fine_advance(b, h, 0, 1, 0, nullptr);
+  }
+  if (r) return r;
+  std::memcpy(b->refptcl, ref, sizeof(ref));
+  return IMPZ_OK;
 }
 
 int impz_moments(impz_bunch_t b, double rec[IMPZ_MOMREC]) {

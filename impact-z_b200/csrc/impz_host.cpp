@@ -1187,6 +1187,25 @@ bool lorentz_field(const Phys& P, const impz_elem_t& e, double zedge, double z, 
 }  // namespace
 
 // ---------------------------------------------------------------------
+int drift2_op(const Phys& P, double tau, double refptcl[6], MapProgram& prog) {
+  MapOp op = blank(MAP_DRIFT2);
+  const double gamma0 = -refptcl[5];
+  const double beta0 = std::sqrt(1.0 - 1.0 / gamma0 / gamma0);
+  op.c[0] = gamma0; op.c[1] = beta0; op.c[2] = P.Scxl; op.c[3] = tau;
+  refptcl[4] = refptcl[4] + 0.5 * tau / (P.Scxl * beta0);
+  return push_op(prog, op);
+}
+
+bool lorentz_kick_terms(const Phys& P, const impz_elem_t& e, double zedge, double z, double tau,
+                        const Species& sp, double refptcl[6], int& kind, double c[16],
+                        double& tg, double& ez0) {
+  tg = refptcl[4];
+  if (!lorentz_field(P, e, zedge, z, tg, kind, c, ez0)) return false;
+  const double gam = -refptcl[5] + tau * (sp.charge / sp.mass) * ez0;
+  refptcl[5] = -gam;
+  return true;
+}
+
 int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double bcurr,
                     const Species& sp, double refptcl[6], double* zio, LoopState& csr,
                     CompiledLattice& out) {
@@ -1286,20 +1305,13 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
             // kick2_BeamBunch (BeamBunch.f90:2187-2508): the field at the
             // kick's z and tg = refptcl(5); gamma0 += tau qmcc Ez0 after it
             s.lorentz = 1;
-            s.lz_tg = refptcl[4];
-            lorentz_field(P, e, zedge, z, s.lz_tg, s.lz_kind, s.lz_c, s.lz_ez0);
-            const double gam = -refptcl[5] + tau2 * (sp.charge / sp.mass) * s.lz_ez0;
-            refptcl[5] = -gam;
+            lorentz_kick_terms(P, e, zedge, z, tau2, sp, refptcl, s.lz_kind, s.lz_c, s.lz_tg,
+                               s.lz_ez0);
           }
         }
         if (lorentz) {
           // map1_BeamBunch(Bpts,z,tau2): drift2 by tau2/2 (BeamBunch.f90:467-509)
-          MapOp op = blank(MAP_DRIFT2);
-          const double gamma0 = -refptcl[5];
-          const double beta0 = std::sqrt(1.0 - 1.0 / gamma0 / gamma0);
-          op.c[0] = gamma0; op.c[1] = beta0; op.c[2] = P.Scxl; op.c[3] = tau2;
-          refptcl[4] = refptcl[4] + 0.5 * tau2 / (P.Scxl * beta0);
-          int r = push_op(prog, op);
+          int r = drift2_op(P, tau2, refptcl, prog);
           if (r) return r;
           ihlf++;
         } else if (bitype == 4) {

@@ -54,6 +54,15 @@ struct Species {
 // BeamBunch.f90:250-464); appends its map op to prog, updates refptcl.
 int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, double tau,
                  int nst, int ihlf, double refptcl[6], const Species& sp, MapProgram& prog);
+// The Lorentz integrator's pieces (Flagmap=2): drift2_BeamBunch's op by
+// tau/2 with refptcl(5) advanced (BeamBunch.f90:467-509), and kick2's
+// field terms for a step table entry at z (tg = refptcl(5); LzKind) with
+// gamma0 moved by tau qmcc Ez0 (BeamBunch.f90:2187-2508); false for an
+// element outside the integrator.
+int drift2_op(const Phys& P, double tau, double refptcl[6], MapProgram& prog);
+bool lorentz_kick_terms(const Phys& P, const impz_elem_t& e, double zedge, double z, double tau,
+                        const Species& sp, double refptcl[6], int& kind, double c[16],
+                        double& tg, double& ez0);
 // Bend entry (refptcl(5) update + Fpol op), Sector op, Bpol op.
 int bend_entry_ops(const Phys& P, const impz_elem_t& e, double refptcl[6], const Species& sp,
                    BendState& bs, MapProgram& prog);

@@ -130,6 +130,24 @@
             type(c_ptr), value :: egrid
           end function
 
+          ! the Lorentz integrator's half step (drift2_BeamBunch) and kick
+          ! (kick2_BeamBunch) for Flagmap=2 call sites
+          integer(c_int) function impz_drift2(bunch, z, tau) bind(C, name="impz_drift2")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), intent(inout) :: z
+            real(c_double), value :: tau
+          end function
+
+          integer(c_int) function impz_kick2(bunch, elem, zedge, z, tau, egrid) &
+              bind(C, name="impz_kick2")
+            import :: c_int, c_double, c_ptr, impz_elem_t
+            type(c_ptr), value :: bunch
+            type(impz_elem_t), intent(in) :: elem
+            real(c_double), value :: zedge, z, tau
+            type(c_ptr), value :: egrid
+          end function
+
           integer(c_int) function impz_moments(bunch, rec) bind(C, name="impz_moments")
             import :: c_int, c_double, c_ptr
             type(c_ptr), value :: bunch

@@ -208,6 +208,21 @@ int impz_poisson_open(impz_bunch_t b, double* phi);
  * and re-sorts the bunch by deposit cell.  egrid (3*nx*ny*nz, may be NULL)
  * receives Ex, Ey, Ez as kick1's egx/egy/egz. */
 int impz_kick(impz_bunch_t b, double tau, double* egrid);
+/* The Lorentz integrator's per-step calls (Flagmap=2, AccSimulator.f90:
+ * 1109-1116, 1446-1469).  impz_drift2 is map1_BeamBunch(Bpts,z,tau2) =
+ * drift2_BeamBunch (BeamBunch.f90:467-509): a drift by tau/2,
+ * refptcl(5) += tau/(2 Scxl beta0), *z += tau/2.  impz_kick2 is
+ * map2_BeamBunch = kick2_BeamBunch (BeamBunch.f90:2187-2508) in element e
+ * (zedge = Param(1)) at position z: after impz_sc_prepare, impz_deposit and
+ * impz_poisson_open, scatter2 with the space-charge field (as impz_kick it
+ * drops the particles conv1st lost and re-sorts; egrid likewise); for a
+ * bunch created with current below 1e-10 A, with no solve, scatter20 with
+ * the element's field alone.  refptcl(6) then moves by tau qmcc Ez0.
+ * IMPZ_ERR_UNSUPPORTED for an element outside impz_set_integrator's list,
+ * IMPZ_ERR_STATE for a bunch with current and no solve. */
+int impz_drift2(impz_bunch_t b, double* z, double tau);
+int impz_kick2(impz_bunch_t b, const impz_elem_t* e, double zedge, double z, double tau,
+               double* egrid);
 /* diagnostic1_Output sums (Output.f90:133-245) of the current state:
  * rec[IMPZ_MOMREC] = 37 sums, 6 |max|, max r^2, Npt, Nptlocal, Current, 0. */
 int impz_moments(impz_bunch_t b, double rec[IMPZ_MOMREC]);

@@ -258,3 +258,52 @@ def test_lorentz_multipoles_match_the_oracle(form, cols, tol):
     rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], cfg["mass"], cfg["freq"])
                        for i in range(len(recs))])
     assert worst(rows_g, rows_o, cols) <= tol
+
+
+@pytest.mark.parametrize("current", [0.030, 0.0])
+def test_per_step_lorentz_calls_reproduce_the_runner(current):
+    """The Fortran driver's Flagmap=2 step (AccSimulator.f90:1109-1116,
+    1122-1405, 1446-1469) through the per-step calls: drift2, conv1st /
+    deposit / Poisson, kick2 in the element at z, drift2; against impz_run
+    with the Lorentz integrator over the same FODO: every particle (by id)
+    and the reference particle agree to rounding."""
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 90)
+    lat = beams.fodo(1, nseg=3)
+    args = (cfg["pts"], current, cfg["mass"], cfg["charge"], cfg["freq"], cfg["refptcl"],
+            cfg["grid"])
+    b1 = impz.Bunch(*args, form=impz.FORM_FP64, track_ids=True)
+    b2 = impz.Bunch(*args, form=impz.FORM_FP64, track_ids=True)
+    try:
+        b1.set_integrator(2)
+        b1.run(lat)
+        p1, i1 = b1.download(), b1.info()
+        z = 0.0
+        for e in lat:
+            zedge, tau = z, e.length / e.nseg
+            rad = e.val[0] if e.type == 0 else e.val[2]
+            for _ in range(e.nseg):
+                z = b2.drift2(z, tau)
+                if current > 0:
+                    b2.sc_prepare(rad, rad)
+                    b2.deposit(want_rho=False, want_counts=False)
+                    b2.poisson(want_phi=False)
+                b2.kick2(e, zedge, z, tau)
+                z = b2.drift2(z, tau)
+        p2, i2 = b2.download(), b2.info()
+        if current == 0.0:  # without a solve, a bunch with current is refused
+            b3 = impz.Bunch(cfg["pts"], 0.03, cfg["mass"], cfg["charge"], cfg["freq"],
+                            cfg["refptcl"], cfg["grid"], form=impz.FORM_FP64)
+            try:
+                with pytest.raises(impz.ImpzError):
+                    b3.kick2(lat[1], 0.1, 0.15, 0.025)
+            finally:
+                b3.close()
+    finally:
+        b1.close()
+        b2.close()
+    assert p1.shape == p2.shape
+    p1 = p1[np.argsort(p1[:, 8])]
+    p2 = p2[np.argsort(p2[:, 8])]
+    np.testing.assert_allclose(p2[:, :6], p1[:, :6], rtol=1e-12, atol=1e-300)
+    np.testing.assert_allclose(i2["refptcl"], i1["refptcl"], rtol=1e-15, atol=0)
+    assert abs(z - i1["z"]) < 1e-12 and abs(i2["z"] - i1["z"]) < 1e-12
