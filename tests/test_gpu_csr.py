@@ -92,3 +92,31 @@ def test_csr_state_carries_across_runs():
     # without the carried state the last drift would have no CSR
     r2n, _, _ = oracle(cfg, lat[-1:], pts=p1, ref=np.array(beam1.refptcl[:]), z=beam1.z)
     assert worst(r2n[1:], r2[1:], [21, 23]) > 1e-4
+
+
+def test_csr_transient_under_the_lorentz_integrator():
+    """The chicane's bends under the map integrator, then (as after a -25
+    switch) the drift behind it under kick2: the downstream transient CSR
+    acts through kick2wake (BeamBunch.f90:5048-5938), the raw wake added per
+    particle, on the GPU as in the oracle."""
+    cfg = chicane_cfg(600.0)
+    lat = cfg["lattice"]
+    r1, p1, beam1 = oracle(cfg, lat[:-1])
+    ref1 = np.array(beam1.refptcl[:])
+
+    def second(state):
+        return orc.run(lat[-1:], p1, cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                       ref1, cfg["grid"], beam1.z, state, flagmap=2)[0]
+
+    r2, r2_plain = second(beam1), second(None)
+    assert worst(r2_plain[1:], r2[1:], [21, 23]) > 1e-4  # the transient acts
+    rows_o = np.r_[r1, r2[1:]]
+    b = impz.Bunch(cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=impz.FORM_FP64, track_ids=False)
+    try:
+        g1 = rows_of(b, cfg, lat[:-1], r1[:, 0])
+        b.set_integrator(2)
+        g2 = rows_of(b, cfg, lat[-1:], r2[:, 0])
+    finally:
+        b.close()
+    assert worst(np.r_[g1, g2[1:]], rows_o, RMS_COLS) <= 1e-7
