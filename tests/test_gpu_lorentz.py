@@ -307,3 +307,31 @@ def test_per_step_lorentz_calls_reproduce_the_runner(current):
     np.testing.assert_allclose(p2[:, :6], p1[:, :6], rtol=1e-12, atol=1e-300)
     np.testing.assert_allclose(i2["refptcl"], i1["refptcl"], rtol=1e-15, atol=0)
     assert abs(z - i1["z"]) < 1e-12 and abs(i2["z"] - i1["z"]) < 1e-12
+
+
+def test_batched_runs_keep_each_bunchs_integrator():
+    """impz_run_batch over a bunch under the map integrator and one under
+    the Lorentz integrator: each bunch's records equal its own run alone."""
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 91)
+    lat = beams.fodo(1)
+    args = (cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+            cfg["refptcl"], cfg["grid"])
+    solo = {}
+    for fm in (1, 2):
+        b = impz.Bunch(*args, form=impz.FORM_FP64, track_ids=False)
+        try:
+            b.set_integrator(fm)
+            solo[fm] = b.run(lat)[0]
+        finally:
+            b.close()
+    assert np.max(np.abs(solo[1] - solo[2])) > 0
+    b1 = impz.Bunch(*args, form=impz.FORM_FP64, track_ids=False)
+    b2 = impz.Bunch(*args, form=impz.FORM_FP64, track_ids=False)
+    try:
+        b2.set_integrator(2)
+        out = impz.run_batch([b1, b2], [lat, lat])
+    finally:
+        b1.close()
+        b2.close()
+    np.testing.assert_allclose(out[0][0], solo[1], rtol=1e-13, atol=0)
+    np.testing.assert_allclose(out[1][0], solo[2], rtol=1e-13, atol=0)
