@@ -34,6 +34,9 @@ N_PARTICLES = 4_000_000
 GRID = (64, 64, 128)
 METRIC = "particle-steps/s at <=1e-5 moment error vs plain FP64 GPU"
 UNIT = "particle-steps/s"
+# the FP32-convolution form: FP64 particles, maps, Green function and moments,
+# int64 fixed-point charge, FP32 convolution and field gather
+DTYPE = "f64+i64+f32conv"
 
 
 def load(name, path, pkg_dir=None):
@@ -190,14 +193,16 @@ def run_reference(args):
         return 0
     threads = os.cpu_count() or 1
     n = N_PARTICLES
-    # one warm-up step, then as many timed steps as fit in ~2 minutes
-    v0, t0, _ = cpu_baseline_port(n, threads, 1)
-    budget = max(1, min(args.steps, int(120.0 / max(t0, 1e-3))))
+    # W untimed warm-up steps (at least one), then as many of the K timed
+    # steps as fit in about two minutes
+    v0, t0, w = cpu_baseline_port(n, threads, max(1, args.warmup), max_seconds=60.0)
+    per_step = t0 / max(w, 1)
+    budget = max(1, min(args.steps, int(120.0 / max(per_step, 1e-3))))
     value, secs, done = cpu_baseline_port(n, threads, budget)
     sample = "%d of %d steps of the %d-particle %dx%dx%d workload (oracle port, %d threads)" % (
         done, args.steps, n, *GRID, threads)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
-            "n_gpus": args.gpus, "steps": done, "warmup": 1,
+            "n_gpus": args.gpus, "steps": done, "warmup": w,
             "ms_per_step": 1e3 * secs / done, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (Philox-seeded Gaussian)",
             "config": workload_config(done),
@@ -303,14 +308,29 @@ def main():
     prof = b.profile_fetch()
     b.profile_enable(False)
 
-    # ---- moment error of this run against the plain FP64 GPU form
-    moment_err = None
+    # ---- the plain FP64 GPU form on the same bunch and steps: its own
+    # device-timed throughput, and the reference for the moment errors
+    moment_err, plain = None, None
     if not args.no_check:
         b64 = impz.Bunch(pts, 0.030, beams.PROTON_MASS_EV, 1.0, 402.5e6, ref, GRID,
                          form=impz.FORM_FP64, track_ids=False)
-        recs64, _ = b64.run(lat)
+        b64.run(warm)
+        b64.upload(pts, 0.030, ref)
+        s64 = torch.cuda.ExternalStream(b64.stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(s64)
+        b64.run_async(lat)
+        e1.record(s64)
+        recs64, _ = b64.run_fetch()
+        torch.cuda.synchronize()
+        t64 = max_over_ranks(dist, e0.elapsed_time(e1) / 1e3, "cuda")
         b64.close()
+        plain = {"value": world * n * K / t64, "ms_per_step": 1e3 * t64 / K,
+                 "fp32conv_over_fp64": t64 / t}
         moment_err = moment_error(impz, recs32, recs64, zs, ref)
+        moment_err["per_step_fields"] = field_errors(impz, beams, pts, ref, min(K, 10))
 
     # ---- e2e through the C ABI with pinned host buffers
     hp = torch.empty((n, 9), dtype=torch.float64, pin_memory=True).numpy()
@@ -372,11 +392,13 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
                 "warmup": W, "ms_per_step": 1e3 * t / K, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "scaling": "weak", "vs_baseline": None, "dtype": DTYPE,
                 "data": "synthetic (Philox-seeded 6D Gaussian protons)",
                 "config": dict(workload_config(K, n), launch=tuned), "clocks": clk, "e2e": e2e,
                 "gpu_launches": int(l1 - l0), "roofline": roofline, "cpu_baseline": cpu,
-                "kernels": kernels, "moment_rel_err_vs_fp64": moment_err}
+                "kernels": kernels, "plain_fp64": plain,
+                "moment_rel_err_vs_fp64": moment_err["max"] if moment_err else None,
+                "errors_vs_fp64": moment_err}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -430,7 +452,7 @@ def run_chicane(args):
     b.close()
     line = {"metric": METRIC, "value": n * K / t, "unit": UNIT, "n_gpus": 1, "steps": K,
             "warmup": args.warmup, "ms_per_step": 1e3 * t / K, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE,
             "data": "synthetic (Philox-seeded flat-top electrons)",
             "config": {"workload": "electron chicane: %d electrons 250 MeV 100 A 1.3 GHz, "
                                    "1 mm flat top with 1%% modulation at 10 um, grid %dx%dx%d, "
@@ -484,7 +506,7 @@ def run_scan(args):
     line = {"metric": METRIC, "value": work / tb, "unit": UNIT, "n_gpus": 1,
             "steps": int(sum(impz.count_steps(l) for l in lats)), "warmup": args.warmup,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (Philox-seeded Gaussian)",
+            "vs_baseline": None, "dtype": DTYPE, "data": "synthetic (Philox-seeded Gaussian)",
             "config": {"workload": "batched scan: %d proton bunches, %d particles in all, "
                                    "400 steps each" % (len(jobs), sum(j["n"] for j in jobs)),
                        "form": "fp32-convolution", "timing": "wall clock, synchronous calls"},
@@ -542,7 +564,7 @@ def run_serve(args):
     line = {"metric": METRIC, "value": work / span, "unit": UNIT, "n_gpus": 1,
             "steps": int(sum(impz.count_steps(j["lattice"]) for j in jobs)),
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE,
             "data": "synthetic (Philox-seeded Gaussian)",
             "config": {"workload": "served stream: %d proton jobs, Poisson arrivals at %g/s, "
                                    "160 GB budget" % (len(jobs), args.rate),
@@ -555,18 +577,68 @@ def run_serve(args):
     return 0
 
 
+# fort.24/25/26 columns of a diagnostic row (impz_diag_row): rms sizes and
+# spreads, emittances; Twiss alpha; centroids, each against the rms of its
+# coordinate (a centroid near zero has no scale of its own)
+RMS_COLS = {7: "x_rms", 9: "px_rms", 11: "x_emit", 13: "y_rms", 15: "py_rms", 17: "y_emit",
+            19: "phase_rms", 21: "dE_rms", 23: "z_emit"}
+ALPHA_COLS = {10: "x_alpha", 16: "y_alpha", 22: "z_alpha"}
+CENTROID_COLS = {6: ("x_mean", 7), 8: ("px_mean", 9), 12: ("y_mean", 13), 14: ("py_mean", 15),
+                 18: ("phase_mean", 19), 20: ("dE_mean", 21)}
+
+
 def moment_error(impz, recs_a, recs_b, zs, ref):
-    """Max relative difference of rms sizes, emittances and centroid spreads."""
+    """Largest difference over all records of every reported moment column:
+    rms sizes and emittances relative to their value, Twiss alpha relative to
+    its largest magnitude, centroids relative to the rms of the coordinate."""
     from impz_b200 import beams
-    cols = [7, 9, 11, 13, 15, 17, 19, 21, 23]
-    worst = 0.0
-    for i in range(len(recs_a)):
-        ra = impz.diag_row(zs[i], recs_a[i], ref, beams.PROTON_MASS_EV, 402.5e6)
-        rb = impz.diag_row(zs[i], recs_b[i], ref, beams.PROTON_MASS_EV, 402.5e6)
-        for c in cols:
-            d = abs(ra[c] - rb[c]) / max(abs(rb[c]), 1e-300)
-            worst = max(worst, d)
-    return worst
+    ra = np.array([impz.diag_row(zs[i], recs_a[i], ref, beams.PROTON_MASS_EV, 402.5e6)
+                   for i in range(len(recs_a))])
+    rb = np.array([impz.diag_row(zs[i], recs_b[i], ref, beams.PROTON_MASS_EV, 402.5e6)
+                   for i in range(len(recs_b))])
+    cols = {}
+    for c, name in RMS_COLS.items():
+        cols[name] = float(np.max(np.abs(ra[:, c] - rb[:, c]) / np.maximum(np.abs(rb[:, c]),
+                                                                          1e-300)))
+    for c, name in ALPHA_COLS.items():
+        cols[name] = float(np.max(np.abs(ra[:, c] - rb[:, c])) / max(np.max(np.abs(rb[:, c])),
+                                                                     1e-300))
+    for c, (name, s) in CENTROID_COLS.items():
+        cols[name] = float(np.max(np.abs(ra[:, c] - rb[:, c])) / max(np.max(np.abs(rb[:, s])),
+                                                                     1e-300))
+    return {"max": max(cols.values()), "columns": cols, "records": int(len(ra))}
+
+
+def field_errors(impz, beams, pts, ref, nsteps):
+    """Per-step relative L2 of the potential and of the field (Ex, Ey, Ez)
+    of the FP32-convolution form against the plain FP64 form, both through
+    the per-step calls (drift1/quadrupole half map, conv1st, deposit,
+    openBC3D, kick1 + scatter1, half map) on the first `nsteps` steps."""
+    out = {"steps": nsteps, "phi_rel_l2": [], "e_rel_l2": []}
+    runs = []
+    for form in (impz.FORM_FP32CONV, impz.FORM_FP64):
+        b = impz.Bunch(pts, 0.030, beams.PROTON_MASS_EV, 1.0, 402.5e6, ref, GRID, form=form,
+                       track_ids=False)
+        phis, egs, z, done = [], [], 0.0, 0
+        try:
+            for e in beams.fodo_steps(nsteps):
+                zedge, tau, ih = z, e.length / e.nseg, 0
+                rad = e.val[0] if e.type == 0 else e.val[2]
+                for j in range(1, e.nseg + 1):
+                    z, ih = b.map_half(e, zedge, z, tau / 2, j, ih)
+                    b.sc_prepare(rad, rad)
+                    b.deposit(want_rho=False, want_counts=False)
+                    phis.append(b.poisson())
+                    egs.append(b.kick(tau, want_e=True))
+                    z, ih = b.map_half(e, zedge, z, tau / 2, j, ih)
+        finally:
+            b.close()
+        runs.append((phis, egs))
+    (p32, e32), (p64, e64) = runs
+    for s in range(len(p32)):
+        out["phi_rel_l2"].append(float(np.linalg.norm(p32[s] - p64[s]) / np.linalg.norm(p64[s])))
+        out["e_rel_l2"].append(float(np.linalg.norm(e32[s] - e64[s]) / np.linalg.norm(e64[s])))
+    return out
 
 
 if __name__ == "__main__":

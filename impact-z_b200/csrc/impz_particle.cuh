@@ -401,9 +401,11 @@ __device__ __forceinline__ Cell cic_cell(double x, double y, double z, const GT&
   return c;
 }
 
+// deposit_BeamBunch's test ix < 1 .or. ix+1 > nx (BeamBunch.f90:3746-3747),
+// written without the +1: a particle far outside the box converts to a
+// saturated INT_MAX, and INT_MAX + 1 would wrap to a negative index.
 __device__ __forceinline__ bool cell_inside(const Cell& c, int nx, int ny, int nz) {
-  return !(c.ix < 1 || c.ix + 1 > nx || c.jx < 1 || c.jx + 1 > ny || c.kx < 1 ||
-           c.kx + 1 > nz);
+  return !(c.ix < 1 || c.ix >= nx || c.jx < 1 || c.jx >= ny || c.kx < 1 || c.kx >= nz);
 }
 
 // ---------------------------------------------------------------------

@@ -13,7 +13,8 @@
 // The arithmetic is that of the bunch deposit (k_deposit): the z->t frame
 // conversion and loss test of conv1st, the CIC cell and weights of
 // deposit_BeamBunch, the same fixed-point quanta with the remainder on the
-// largest corner, so for the same particles and geometry the grid equals
+// largest corner, with the quantum chosen from this call's n; for a bunch
+// created with the same n and the same geometry the grid equals
 // impz_deposit's bit for bit.  Sums go straight to the accumulator with
 // 64-bit atomics (integer adds: the result does not depend on their order).
 //
@@ -54,7 +55,9 @@ __global__ void k_static_clear(unsigned long long* acc, long long G) {
 }
 
 // conv1st z->t frame and loss test, deposit_BeamBunch cell, weights and the
-// int64 quanta of k_deposit; 64-bit global reductions per corner.
+// int64 quanta of k_deposit; 64-bit global reductions per corner.  A
+// particle outside the caller's box (far outside included: cell_inside does
+// not overflow) is skipped, as deposit_BeamBunch skips it.
 __global__ void __launch_bounds__(256) k_static_deposit(StaticDepositArgs a,
                                                         unsigned long long* acc) {
   const int nx = a.nx, ny = a.ny, nz = a.nz;
@@ -114,26 +117,35 @@ __global__ void k_static_finish(const unsigned long long* acc, long long G, doub
     out[i] = (double)(long long)acc[i] * scale;
 }
 
-// Device address of g_static_rho, looked up once per device.  In host code
-// the name g_static_rho is only a host-side stand-in for the symbol, so the
-// kernels are always given this address, never the name.
+// Device address of g_static_rho and the device's SM count, looked up once
+// per device.  In host code the name g_static_rho is only a host-side
+// stand-in for the symbol, so the kernels are always given this address,
+// never the name.  The cached address belongs to the device's current
+// context: a cudaDeviceReset would invalidate it, so the library must not be
+// used across one.
 constexpr int kMaxDevices = 64;
 std::mutex g_addr_mu;
 unsigned long long* g_addr[kMaxDevices] = {nullptr};
+int g_sms[kMaxDevices] = {0};
 
-int scratch_address(unsigned long long** out) {
+int scratch_address(unsigned long long** out, int* sms) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return report_cuda_error(e, "impz_deposit_static: cudaGetDevice");
   if (dev < 0 || dev >= kMaxDevices) return IMPZ_ERR_UNSUPPORTED;
   std::lock_guard<std::mutex> g(g_addr_mu);
   if (!g_addr[dev]) {
+    int n_sm = 0;
+    e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return report_cuda_error(e, "impz_deposit_static: SM count");
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_static_rho);
     if (e != cudaSuccess) return report_cuda_error(e, "impz_deposit_static: cudaGetSymbolAddress");
     g_addr[dev] = (unsigned long long*)p;
+    g_sms[dev] = n_sm > 0 ? n_sm : 1;
   }
   *out = g_addr[dev];
+  *sms = g_sms[dev];
   return IMPZ_OK;
 }
 
@@ -152,7 +164,8 @@ extern "C" int impz_deposit_static(const double* x, const double* px, const doub
   if (G > IMPZ_STATIC_MAX_CELLS) return IMPZ_ERR_LIMIT;
   if (n > 0 && (!x || !px || !y || !py || !ph || !pt)) return IMPZ_ERR_ARG;
   unsigned long long* acc = nullptr;
-  int r = scratch_address(&acc);
+  int sms = 1;
+  int r = scratch_address(&acc, &sms);
   if (r) return r;
   StaticDepositArgs a;
   const double* cols[6] = {x, px, y, py, ph, pt};
@@ -177,10 +190,10 @@ extern "C" int impz_deposit_static(const double* x, const double* px, const doub
     if (!(a.g.h[k] > 0.0) || !std::isfinite(a.g.hi[k])) return IMPZ_ERR_ARG;
   }
   cudaStream_t s = (cudaStream_t)stream;
-  const int gclear = (int)std::min<long long>((G + 255) / 256, 148 * 8);
+  const int gclear = (int)std::min<long long>((G + 255) / 256, (long long)sms * 8);
   k_static_clear<<<gclear, 256, 0, s>>>(acc, G);
   if (n > 0) {
-    const int gdep = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    const int gdep = (int)std::min<long long>((n + 255) / 256, (long long)sms * 16);
     k_static_deposit<<<gdep, 256, 0, s>>>(a, acc);
   }
   k_static_finish<<<gclear, 256, 0, s>>>(acc, G, a.scale, chgdens);

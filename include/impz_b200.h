@@ -337,16 +337,21 @@ int impz_maplinear(const impz_elem_t* e, double zedge, double t, double tau,
  * device image, which every GPU that loads the library holds until exit.
  *
  * Deposits the charge density of deposit_BeamBunch (BeamBunch.f90:3678-3768)
- * after conv1st's z->t conversion and loss test, with the same fixed-point
- * sums as impz_deposit, so for the same particles and geometry chgdens
- * equals impz_deposit's chgdens bit for bit.  x..pt: device columns of
+ * after conv1st's z->t conversion and loss test, in int64 fixed point with
+ * 2^-f of the weight per particle, f = min(40, 62 - ceil(log2(n + 1))) from
+ * this call's n.  A bunch fixes its f from its particle count at creation,
+ * so chgdens equals impz_deposit's bit for bit when that bunch was created
+ * with this n (tested in the plain FP64 form).  Particles outside the box
+ * are skipped without a count, as deposit_BeamBunch skips them: a stale box
+ * loses their charge silently.  x..pt: device columns of
  * Pts1 rows 1..6 (n particles); gam = -refptcl(6); piperad, piperad2 as for
  * impz_sc_prepare; freq = Scfreq; weight = Pts1 row 8; range[6] (host) =
  * the mesh box (impz_sc_prepare's range); chgdens: device, nx*ny*nz doubles,
  * x fastest.  Launches on `stream` (a cudaStream_t, 0 = default) and returns
  * without synchronizing; IMPZ_ERR_LIMIT if nx*ny*nz > IMPZ_STATIC_MAX_CELLS.
  * The first call on each device (the current one) looks up the array's
- * device address; make that first call before any stream capture.  All
+ * device address and keeps it; make that first call before any stream
+ * capture, and do not use the library across a cudaDeviceReset.  All
  * calls share the array: calls whose kernels can overlap on the GPU (other
  * streams, other host threads) race and give wrong sums. */
 #define IMPZ_STATIC_MAX_CELLS (1 << 19)

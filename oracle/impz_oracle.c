@@ -32,6 +32,21 @@ static int g_threads = 1;
 
 void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
 
+/* Optional per-step field capture of orc_run (test infrastructure): the
+ * potential (G values) and kick1's Ex, Ey, Ez (3G) of space-charge steps
+ * 0..maxsteps-1 are copied to phi + s*G and eg + 3*s*G. */
+static struct {
+  double *phi, *eg;
+  int maxsteps, step;
+} g_probe;
+
+void orc_set_field_probe(double *phi, double *eg, int maxsteps) {
+  g_probe.phi = phi;
+  g_probe.eg = eg;
+  g_probe.maxsteps = (phi || eg) ? maxsteps : 0;
+  g_probe.step = 0;
+}
+
 /* PhysConst.f90:25-35 */
 void orc_physconst(double freq) {
   PC.Clight = 299792458.0;
@@ -2812,9 +2827,17 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
                                             beam->charge, e, lz_zedge, z, beam->refptcl[4],
                                             beam->nlocal ? beam->pts[6] : 0.0,
                                             wf ? wf + 6 * (size_t)mesh[2] : NULL);
-            else
+            else {
+              double *egp = NULL;
+              if (g_probe.step < g_probe.maxsteps) {
+                if (g_probe.phi)
+                  memcpy(g_probe.phi + G * (size_t)g_probe.step, rho, G * sizeof(double));
+                if (g_probe.eg) egp = g_probe.eg + 3 * G * (size_t)g_probe.step;
+                g_probe.step++;
+              }
               orc_kick1w(beam->pts, beam->nlocal, rho, mesh, range, msize, -beam->refptcl[5],
-                         beam->current, tau2, beam->mass, beam->charge, NULL, wf);
+                         beam->current, tau2, beam->mass, beam->charge, egp, wf);
+            }
             free(wf);
           }
         }

@@ -34,6 +34,10 @@ void orc_get_physconst(double out[5]); /* Pi, Clight, Scxl, Rad2deg, Scfreq */
 
 /* OpenMP threads used by the particle loops (1 = sequential, bit-exact order) */
 void orc_set_threads(int n);
+/* per-step capture of orc_run's map-integrator space-charge steps: the
+ * potential into phi[s*G..] and kick1's Ex,Ey,Ez into eg[3*s*G..] for
+ * s < maxsteps (either may be NULL); resets the step counter */
+void orc_set_field_probe(double *phi, double *eg, int maxsteps);
 
 /* ---- element maps ---------------------------------------------------- */
 /* drift1_BeamBunch bitype 0 (BeamBunch.f90:276-298) */

@@ -62,6 +62,7 @@ def lib():
             "orc_physconst": (v, [ctypes.c_double]),
             "orc_get_physconst": (v, [_D]),
             "orc_set_threads": (v, [ctypes.c_int]),
+            "orc_set_field_probe": (v, [_D, _D, ctypes.c_int]),
             "orc_drift_exact": (v, [_D, ctypes.c_int, _D, ctypes.c_double]),
             "orc_maplinear_quad": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_double,
                                        ctypes.c_int, ctypes.c_double, ctypes.c_double]),
@@ -188,11 +189,19 @@ def elem_from(e):
     return o
 
 
-def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0, state=None, flagmap=1):
+def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0, state=None, flagmap=1,
+        probe=None):
     """orc_run over a lattice: returns (rows, final pts, final beam).  `state`
     (a beam returned by an earlier call) carries the CSR bend bookkeeping
-    across calls, as one element loop of the reference would."""
+    across calls, as one element loop of the reference would.  `probe` =
+    (phi, eg) float64 arrays of shape (S, G) and (S, 3G) (either may be None)
+    receive the potential and kick1's field of the first S space-charge
+    steps of the map integrator."""
     physconst(freq)
+    if probe is not None:
+        phi, eg = probe
+        steps = (phi if phi is not None else eg).shape[0]
+        lib().orc_set_field_probe(dp(phi), dp(eg), steps)
     arr = (OrcElem * len(elems))(*[elem_from(e) for e in elems])
     keep = [getattr(e, "_keep", None) for e in elems]
     p = np.ascontiguousarray(pts, dtype=np.float64).copy()
@@ -210,8 +219,12 @@ def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0, state=Non
     mesh = np.array(grid, dtype=np.int32)
     nsteps = sum(e.nseg for e in elems)
     rows = np.zeros((nsteps + 1, DIAG_LEN))
-    n = lib().orc_run(arr, len(elems), ctypes.byref(beam), mesh.ctypes.data_as(_I), dp(rows),
-                      nsteps + 1)
+    try:
+        n = lib().orc_run(arr, len(elems), ctypes.byref(beam), mesh.ctypes.data_as(_I), dp(rows),
+                          nsteps + 1)
+    finally:
+        if probe is not None:
+            lib().orc_set_field_probe(None, None, 0)
     del keep
     if n < 0:
         raise RuntimeError("orc_run failed: %d" % n)

@@ -108,3 +108,44 @@ def test_server_admits_within_budget_and_refuses_oversize():
             srv.submit(big, 0.03, beams.PROTON_MASS_EV, 1.0, 402.5e6, r, (64, 64, 128),
                        beams.fodo(1), form=impz.FORM_FP64)
         assert ei.value.code == impz.ERR_BUDGET
+
+
+def test_server_admits_a_job_that_arrives_while_others_run():
+    """Continuous batching: two long jobs are on the GPU when a short job is
+    submitted; it is admitted at once (slots and budget are free), finishes
+    while both long jobs are still running, and its records equal its solo
+    run within the module tolerance."""
+    import time
+    long_jobs = [dict(n=2_000_000, seed=beams.SEED0 + 600 + k, current=0.03 + 0.01 * k,
+                      grid=(64, 64, 128), lattice=beams.fodo_steps(1200, nseg=4))
+                 for k in range(2)]
+    short = dict(n=20_000, seed=beams.SEED0 + 610, current=0.02, grid=(32, 32, 64),
+                 lattice=beams.fodo_steps(40, nseg=4))
+    pts_s, ref_s = beams.make_scan_bunch(short)
+    with impz.Server(budget_bytes=8e9, max_active=8) as srv:
+        solo = srv.wait(srv.submit(pts_s, short["current"], beams.PROTON_MASS_EV, 1.0, 402.5e6,
+                                   ref_s, short["grid"], short["lattice"]))[0]
+    with impz.Server(budget_bytes=8e9, max_active=8) as srv:
+        ids = []
+        for j in long_jobs:
+            p, r = beams.make_scan_bunch(j)
+            ids.append(srv.submit(p, j["current"], beams.PROTON_MASS_EV, 1.0, 402.5e6, r,
+                                  j["grid"], j["lattice"]))
+        t0 = time.perf_counter()
+        while srv.stats()["queued"] > 0 and time.perf_counter() - t0 < 30:
+            time.sleep(0.002)
+        st = srv.stats()
+        assert st["queued"] == 0 and st["completed"] == 0 and st["admitted_bytes"] > 0
+        time.sleep(0.05)  # both long jobs are stepping on the device
+        sid = srv.submit(pts_s, short["current"], beams.PROTON_MASS_EV, 1.0, 402.5e6, ref_s,
+                         short["grid"], short["lattice"])
+        recs, latency, queued, _ = srv.wait(sid)
+        during = srv.stats()
+        long_res = [srv.wait(i) for i in ids]
+        end = srv.stats()
+    assert during["completed"] == 1, during  # only the short job had finished
+    assert queued <= latency
+    assert end["completed"] == 3 and end["failed"] == 0
+    assert all(r[0].shape[0] == 1201 for r in long_res)
+    assert recs.shape == solo.shape
+    assert close(recs, solo) <= TOL
