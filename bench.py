@@ -275,9 +275,9 @@ def main():
 
     b = impz.Bunch(pts, 0.030, beams.PROTON_MASS_EV, 1.0, 402.5e6, ref, GRID,
                    form=impz.FORM_FP32CONV, track_ids=False)
-    b.run(warm)                          # warm-up steps (untimed)
     tuned = b.autotune(8)                # launch shapes picked by timing this bunch
-    b.upload(pts, 0.030, ref)
+    b.run(warm)                          # W warm-up steps (untimed): the step graphs of the
+    b.upload(pts, 0.030, ref)            # tuned launch shapes are captured here
     stream = torch.cuda.ExternalStream(b.stream())
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)

@@ -52,6 +52,124 @@ __global__ void k_aos_to_soa(const double* __restrict__ aos, long long n, double
   }
 }
 
+// ---- upload order -------------------------------------------------------
+// Freshly uploaded particles are ordered by their cell on a coarse box grid
+// over (x, y, phase) in the z frame, so that the first deposit and push of a
+// run see the locality that every later step's sort by deposit cell keeps.
+// The order only changes which particles share a block; no particle's
+// arithmetic depends on it.
+
+// per-block min/max of x, y, phase -> part[block][6] (min, max pairs)
+__global__ void k_upload_box(const double* __restrict__ x, const double* __restrict__ y,
+                             const double* __restrict__ ph, long long n, double* part) {
+  __shared__ double red[6][8];
+  double v[6] = {1e300, -1e300, 1e300, -1e300, 1e300, -1e300};
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double a = x[i], b = y[i], c = ph[i];
+    v[0] = fmin(v[0], a); v[1] = fmax(v[1], a);
+    v[2] = fmin(v[2], b); v[3] = fmax(v[3], b);
+    v[4] = fmin(v[4], c); v[5] = fmax(v[5], c);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < 6; d++) {
+    double t = v[d];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_xor_sync(0xffffffffu, t, o);
+      t = (d & 1) ? fmax(t, u) : fmin(t, u);
+    }
+    if (lane == 0) red[d][wid] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int d = threadIdx.x;
+    double t = red[d][0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++)
+      t = (d & 1) ? fmax(t, red[d][w]) : fmin(t, red[d][w]);
+    part[6 * blockIdx.x + d] = t;
+  }
+}
+
+// the coarse cell of a particle: nx x ny x nz bins over the box; non-finite
+// coordinates fall into bin 0 (fmax/fmin return the number for a NaN)
+__device__ __forceinline__ int upload_key(double x, double y, double ph, const double* box,
+                                          int nx, int ny, int nz) {
+  const double fx = fmin(fmax((x - box[0]) * box[6], 0.0), (double)(nx - 1));
+  const double fy = fmin(fmax((y - box[2]) * box[7], 0.0), (double)(ny - 1));
+  const double fz = fmin(fmax((ph - box[4]) * box[8], 0.0), (double)(nz - 1));
+  return (int)fx + nx * ((int)fy + ny * (int)fz);
+}
+
+// box[0..5] = min/max over the nb partials, box[6..8] = bins per unit length
+__global__ void k_upload_box_final(const double* part, int nb, int nx, int ny, int nz,
+                                   double* box) {
+  __shared__ double red[6];
+  if (threadIdx.x < 6) {
+    const int d = threadIdx.x;
+    double t = part[d];
+    for (int b = 1; b < nb; b++) t = (d & 1) ? fmax(t, part[6 * b + d]) : fmin(t, part[6 * b + d]);
+    red[d] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int m[3] = {nx, ny, nz};
+    for (int d = 0; d < 3; d++) {
+      box[2 * d] = red[2 * d];
+      box[2 * d + 1] = red[2 * d + 1];
+      const double w = red[2 * d + 1] - red[2 * d];
+      box[6 + d] = w > 0.0 ? (double)(m[d] - 1) / w : 0.0;
+    }
+  }
+}
+
+__global__ void k_upload_count(const double* __restrict__ x, const double* __restrict__ y,
+                               const double* __restrict__ ph, long long n, const double* box_g,
+                               int nx, int ny, int nz, int* counts) {
+  __shared__ double box[9];
+  if (threadIdx.x < 9) box[threadIdx.x] = box_g[threadIdx.x];
+  __syncthreads();
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    atomicAdd(counts + upload_key(x[i], y[i], ph[i], box, nx, ny, nz), 1);
+}
+
+// scatter to the slot of the key (cursor from the scan of the counts); lanes
+// of one key take consecutive slots with one atomic per group
+__global__ void k_upload_scatter(const double* const* in, double* const* out,
+                                 const long long* ids_in, long long* ids_out, long long n,
+                                 const double* box_g, int nx, int ny, int nz, int* cursor,
+                                 const int* bsum) {
+  __shared__ double box[9];
+  if (threadIdx.x < 9) box[threadIdx.x] = box_g[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long nround = (n + 31) / 32 * 32;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nround;
+       i += (long long)gridDim.x * blockDim.x) {
+    const bool live = i < n;
+    double v[6];
+    int key = 0;
+    if (live) {
+#pragma unroll
+      for (int c = 0; c < 6; c++) v[c] = in[c][i];
+      key = upload_key(v[0], v[2], v[4], box, nx, ny, nz);
+    }
+    const unsigned active = __ballot_sync(0xffffffffu, live);
+    if (!live) continue;
+    const unsigned grp = __match_any_sync(active, (unsigned)key);
+    const int leader = __ffs(grp) - 1;
+    const int rank = __popc(grp & ((1u << lane) - 1u));
+    int base = 0;
+    if (lane == leader) base = atomicAdd(cursor + key, __popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    const long long dst = (long long)base + rank + bsum[key >> IMPZ_SCAN_LOG];
+#pragma unroll
+    for (int c = 0; c < 6; c++) out[c][dst] = v[c];
+    if (ids_out) ids_out[dst] = ids_in[i];
+  }
+}
+
 __global__ void k_soa_to_aos(double* __restrict__ aos, long long n, long long i0, const double* x,
                              const double* px, const double* y, const double* py,
                              const double* ph, const double* pt, const long long* ids,
@@ -214,6 +332,14 @@ Layout plan_layout(long long n, int nx, int ny, int nz, int form, int flags) {
   L.flag = take(sizeof(unsigned int));
   L.total = off;
   return L;
+}
+
+// step-table entries allocated for a run that needs `entries`: the next
+// power of two, at least 256 (about 0.8 MB)
+int table_capacity(int entries) {
+  int c = 256;
+  while (c < entries) c <<= 1;
+  return c;
 }
 
 size_t tables_bytes(int entries, int rows) {
@@ -549,10 +675,12 @@ int check_err(impz_bunch_t b) {
 }
 
 // step table (entries) and moment records (rows) of a run, one allocation
+// with room for table_capacity(entries) steps, so that runs of similar
+// length reuse the buffers (and the CUDA graphs that point into them)
 int ensure_tables(impz_bunch_t b, int entries, int rows) {
   if (entries <= b->tables_entries && rows <= b->tables_rows) return IMPZ_OK;
-  entries = std::max(entries, b->tables_entries);
-  rows = std::max(rows, b->tables_rows);
+  entries = std::max(table_capacity(std::max(entries, rows)), b->tables_entries);
+  rows = entries;
   if (b->tables) {
     CK(cudaStreamSynchronize(b->stream));
     cudaFree(b->tables);
@@ -578,6 +706,41 @@ double* staging(impz_bunch_t b, long long* cap_particles) {
   return b->pbuf[q][0];
 }
 
+// Orders the n particles of parity 0 by their coarse cell (k_upload_box ..
+// k_upload_scatter) into parity 1.  The per-cell counts are zero afterwards
+// (the scan clears them), as the deposit expects.
+int upload_order(impz_bunch_t b, long long n) {
+  const int nb = (int)std::min<long long>((n + 255) / 256, kMaxAdvGrid);
+  double* box = b->mom_fine;  // 9 doubles; the per-call record is not in use here
+  CK(cudaMemsetAsync(b->counts, 0, (size_t)(b->G + 1) * sizeof(int), b->stream));
+  CK(cudaMemsetAsync(&b->st->done_scan, 0, sizeof(unsigned int), b->stream));
+  k_upload_box<<<nb, 256, 0, b->stream>>>(b->pbuf[0][0], b->pbuf[0][2], b->pbuf[0][4], n,
+                                          b->rng_part);
+  k_upload_box_final<<<1, 32, 0, b->stream>>>(b->rng_part, nb, b->nx, b->ny, b->nz, box);
+  k_upload_count<<<nb, 256, 0, b->stream>>>(b->pbuf[0][0], b->pbuf[0][2], b->pbuf[0][4], n, box,
+                                            b->nx, b->ny, b->nz, b->counts);
+  CK(cudaGetLastError());
+  g_launches += 3;
+  CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
+  g_launches += 1;
+  // the column pointer arrays reach the scatter through a small device copy
+  // in the per-call step-table slot, which is free at upload
+  double* cols[12];
+  for (int c = 0; c < 6; c++) {
+    cols[c] = b->pbuf[0][c];
+    cols[6 + c] = b->pbuf[1][c];
+  }
+  double** dcols = (double**)b->dfine;
+  CK(cudaMemcpyAsync(dcols, cols, sizeof(cols), cudaMemcpyHostToDevice, b->stream));
+  k_upload_scatter<<<nb, 256, 0, b->stream>>>(dcols, dcols + 6, b->ids[0], b->ids[1], n, box,
+                                              b->nx, b->ny, b->nz, b->cursor, b->bsum);
+  CK(cudaGetLastError());
+  g_launches += 1;
+  b->parity = 1;
+  CK(cudaStreamSynchronize(b->stream));
+  return IMPZ_OK;
+}
+
 // Pts1(9,n) host array -> SoA columns of parity 0, through the staging area
 // in chunks; returns IMPZ_ERR_NONUNIFORM when a particle's charge/mass or
 // weight differs from the bunch's.
@@ -600,7 +763,8 @@ int upload_pts(impz_bunch_t b, const double* pts, long long n) {
   unsigned int hbad = 0;
   CK(cudaMemcpyAsync(&hbad, b->flag, sizeof(hbad), cudaMemcpyDeviceToHost, b->stream));
   CK(cudaStreamSynchronize(b->stream));
-  return hbad ? IMPZ_ERR_NONUNIFORM : IMPZ_OK;
+  if (hbad) return IMPZ_ERR_NONUNIFORM;
+  return upload_order(b, n);
 }
 
 template <typename C>
@@ -812,7 +976,10 @@ long long impz_bunch_footprint(long long n, int nx, int ny, int nz, int form, in
   if (n < 1 || nx < 1 || ny < 1 || nz < 1 || nsteps < 0) return -1;
   const Layout L = plan_layout(n, nx, ny, nz, form, flags);
   long long total = (long long)round_up(L.total, kGranule);
-  if (nsteps > 0) total += (long long)round_up(tables_bytes(nsteps + 2, nsteps + 1), kGranule);
+  if (nsteps > 0) {
+    const int c = table_capacity(nsteps + 2);
+    total += (long long)round_up(tables_bytes(c, c), kGranule);
+  }
   // graph executables, events and streams of the bunch
   return total + (long long)kGranule;
 }
