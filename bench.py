@@ -235,6 +235,9 @@ def main():
     ap.add_argument("--particles", type=int, default=N_PARTICLES)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shapes (fewer launches before the timed run, "
+                         "for profiling a chosen launch)")
     ap.add_argument("--workload", default="fodo", choices=["fodo", "chicane", "scan", "serve"],
                     help="fodo: the headline 4e6-proton line; chicane: 5e7 electrons, "
                          "64x64x2048; scan: 256 bunches batched; serve: Poisson job stream")
@@ -275,7 +278,7 @@ def main():
 
     b = impz.Bunch(pts, 0.030, beams.PROTON_MASS_EV, 1.0, 402.5e6, ref, GRID,
                    form=impz.FORM_FP32CONV, track_ids=False)
-    tuned = b.autotune(8)                # launch shapes picked by timing this bunch
+    tuned = None if args.no_tune else b.autotune(8)  # launch shapes picked by timing
     b.run(warm)                          # W warm-up steps (untimed): the step graphs of the
     b.upload(pts, 0.030, ref)            # tuned launch shapes are captured here
     stream = torch.cuda.ExternalStream(b.stream())

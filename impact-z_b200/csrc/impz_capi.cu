@@ -515,6 +515,10 @@ AdvanceArgs advance_args(impz_bunch_t b, const StepParams* table, int fixed, int
   a.do_pre = pre;
   a.mom_index = mom_index;
   a.wake_raw = b->run_wake ? b->wk_field + 3 * (size_t)b->nz : nullptr;
+  // the whole-lattice runner (step index from the device) keeps the bunch in
+  // conv1st's frame between a pass and the next step's deposit and kick; the
+  // per-step surface keeps the z frame, which the caller may download
+  a.tframe = fixed < 0 ? 1 : 0;
   return a;
 }
 
@@ -554,6 +558,7 @@ DepositArgs deposit_args(impz_bunch_t b, const StepParams* table, int fixed) {
   d.rho = b->rho;
   d.counts = b->counts;
   d.xl = b->P.Scxl;
+  d.tframe = fixed < 0 ? 1 : 0;
   return d;
 }
 
@@ -576,7 +581,16 @@ WakeArgs wake_args(impz_bunch_t b, const StepParams* table, int fixed) {
   w.unit = b->f32() ? b->weight : 1.0;
   w.xl = b->P.Scxl;
   w.k = b->k;
+  w.tframe = fixed < 0 ? 1 : 0;
   return w;
+}
+
+// The FP32-convolution form deposits with the contracting build (its cells
+// are the same: cic_cell rounds explicitly; a corner's quanta may differ by
+// one from the plain form's); the plain FP64 form with the exact one.
+cudaError_t launch_deposit(impz_bunch_t b, const DepositArgs& d) {
+  if (b->f32()) return fast::launch_deposit(d, b->grid_dep, b->stream);
+  return exact::launch_deposit(d, b->grid_dep, b->stream);
 }
 
 int solve_green(impz_bunch_t b, cudaStream_t s) {
@@ -621,7 +635,7 @@ int field_step(impz_bunch_t b, const StepParams* table, int fixed) {
   DepositArgs d = deposit_args(b, table, fixed);
   {
     ProfScope ps(b, IMPZ_PROF_DEPOSIT, 1);
-    CK(exact::launch_deposit(d, b->grid_dep, b->stream));
+    CK(launch_deposit(b, d));
   }
   // the scan of the counts is needed only by the push: on the second stream
   // it runs beside the forward transform
@@ -878,10 +892,9 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
   b->k.charge = charge;
   b->k.qm0 = charge / mass;
   b->k.qmi = b->sp.qmi;
-  // fixed point: no cell can exceed n units, so n * 2^fixbits < 2^62.  The
-  // FP32-convolution form keeps 2^-21 of a macro charge (finer than the FP32
-  // transforms that follow), which lets the deposit sum a chunk in one word
-  b->fixbits = std::min(form == IMPZ_FORM_FP32CONV ? 21 : 40, 62 - ilog2i(n + 1));
+  // fixed point: 2^-40 of a macro charge in both forms, fewer bits when
+  // n * 2^fixbits would not stay below 2^62 (no cell can exceed n units)
+  b->fixbits = std::min(40, 62 - ilog2i(n + 1));
   int rc = IMPZ_OK;
 #define ALLOC(call)                                   \
   do {                                                \
@@ -1263,7 +1276,7 @@ int impz_deposit(impz_bunch_t b, double* chgdens, int* counts) {
   DepositArgs d = deposit_args(b, b->dfine, 0);
   {
     ProfScope ps(b, IMPZ_PROF_DEPOSIT, 1);
-    CK(exact::launch_deposit(d, b->grid_dep, b->stream));
+    CK(launch_deposit(b, d));
   }
   if (counts) {
     CK(cudaMemcpyAsync(counts, b->counts, b->G * sizeof(int), cudaMemcpyDeviceToHost, b->stream));

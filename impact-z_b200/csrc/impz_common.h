@@ -180,7 +180,8 @@ struct AdvanceArgs {
   int do_post;              // apply steps[s].post (+ moments if steps[s].moments)
   int do_pre;               // apply steps[s].pre_next (+ conv1st of s+1 if range_next)
   int mom_index;            // record row for fixed_step launches
-  int pad1;
+  int tframe;               // 1: conv1st's frame between passes (the whole-lattice runner):
+                            //    a kick reads it, a pass with range_next writes it
   const double* wake_raw;   // per-plane wake {Ex,Ey,Ez}[nz] of a Lorentz step (kick2wake), or null
 };
 
@@ -191,7 +192,7 @@ struct DepositArgs {
   int fixed_step;
   int nx, ny, nz;
   int fixbits;
-  int pad0;
+  int tframe;               // 1: the particles are stored in conv1st's frame (AdvanceArgs)
   unsigned long long* rho;  // G int64 (two's complement) accumulators
   int* counts;              // G+1 per-cell particle counts (slot G: live but outside)
   double xl;
@@ -209,7 +210,7 @@ struct WakeArgs {
   int fixbits;               // fixed-point resolution of the line sums
   int transverse;            // 1: x/y moments and the transverse wakes too
   int ntab;                  // wake table rows
-  int pad0;
+  int tframe;                // 1: the particles are stored in conv1st's frame (AdvanceArgs)
   unsigned long long* line;  // [3][nz] int64 sums (density, x, y), left cleared
   const double* table;       // [3][ntab]: longitudinal, x and y wake columns
   double* wfield;            // [3][nz] out: added to Ex, Ey, Ez of plane k

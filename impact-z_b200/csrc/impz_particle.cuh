@@ -383,6 +383,30 @@ __device__ __forceinline__ TFrame to_tframe(const Particle& p, double gam, doubl
   return t;
 }
 
+// The whole-lattice runner stores a particle between two passes as conv1st
+// leaves Pts1 (BeamBunch.f90:1296-1340): x_t and y_t [m] in columns 1 and 3,
+// z_t in column 5, the momenta unchanged, and a NaN in column 5 for a
+// particle conv1st lost.  cvbkforth1st recomputes 1/gamma_i and beta_i from
+// the momenta (BeamBunch.f90:1681-1690), so nothing else is needed; the
+// values are those to_tframe returned when the pass stored them.
+__device__ __forceinline__ double lost_mark() { return __longlong_as_double(0x7ff8000000000000ll); }
+
+__device__ __forceinline__ TFrame stored_tframe(const Particle& p, double gam) {
+  TFrame t;
+  t.ph = 0.0;
+  t.rcp = 1.0 / __dadd_rn(-p.pt, gam);
+  t.tmpbet = __dsub_rn(1.0, __dmul_rn(__dmul_rn(t.rcp, t.rcp),
+                                      __dadd_rn(__dadd_rn(1.0, __dmul_rn(p.px, p.px)),
+                                                __dmul_rn(p.py, p.py))));
+  t.xt = p.x;
+  t.yt = p.y;
+  t.zt = p.ph;
+  t.tmpx = 0.0;
+  t.tmpy = 0.0;
+  t.lost = isnan(p.ph);
+  return t;
+}
+
 // deposit_BeamBunch cell and weights (BeamBunch.f90:3737-3742)
 struct Cell {
   int ix, jx, kx;   // 1-based like the reference
@@ -886,7 +910,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
 #pragma unroll
     for (int u = 0; u < U; u++) {
       if (keep[u] && kick) {
-        TFrame t = to_tframe(p[u], gam, rad, xl);
+        const TFrame t = a.tframe ? stored_tframe(p[u], gam) : to_tframe(p[u], gam, rad, xl);
         if (t.lost) {
           keep[u] = false;
         } else {
@@ -967,10 +991,12 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
     if (mom) warp_moments<U>(mtile_dyn + wid * 32 * IMPZ_MSUMS, c, lane, macc0, macc1, mmax);
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      if (keep[u] && pre) {
-        apply_program<LIGHT>(p[u], progs[1]);
+      if (keep[u]) {
+        if (pre) apply_program<LIGHT>(p[u], progs[1]);
+        if (!finite6(p[u])) err |= DERR_NONFINITE;
+        nkept++;
         if (rng) {
-          TFrame t = to_tframe(p[u], gam_n, rad_n, xl);
+          const TFrame t = to_tframe(p[u], gam_n, rad_n, xl);
           rmn[0] = fmin(rmn[0], fmin(t.tmpx, t.xt));
           rmx[0] = fmax(rmx[0], fmax(t.tmpx, t.xt));
           rmn[1] = fmin(rmn[1], fmin(t.tmpy, t.yt));
@@ -978,11 +1004,12 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
           rmn[2] = fmin(rmn[2], t.zt);
           rmx[2] = fmax(rmx[2], t.zt);
           nlive += t.lost ? 0 : 1;
+          if (a.tframe) {  // stored as conv1st leaves Pts1 (stored_tframe)
+            p[u].x = t.xt;
+            p[u].y = t.yt;
+            p[u].ph = t.lost ? lost_mark() : t.zt;
+          }
         }
-      }
-      if (keep[u]) {
-        if (!finite6(p[u])) err |= DERR_NONFINITE;
-        nkept++;
       }
       // destination slot
       long long dst = i0 + (long long)u * BLOCK;
@@ -1203,12 +1230,23 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
       pk[u] = 0u;
       wab[u] = wcd[u] = wef[u] = 0.0;
       if (i < n) {
-        Particle p;
-        p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
-        p.py = a.in[3][i]; p.ph = a.in[4][i]; p.pt = a.in[5][i];
-        TFrame t = to_tframe(p, gam, rad, a.xl);
-        if (!t.lost) {
-          Cell c = cic_cell(t.xt, t.yt, t.zt, g);
+        double xt, yt, zt;
+        bool lost;
+        if (a.tframe) {  // stored in conv1st's frame: three columns suffice
+          xt = a.in[0][i];
+          yt = a.in[2][i];
+          zt = a.in[4][i];
+          lost = isnan(zt);
+        } else {
+          Particle p;
+          p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
+          p.py = a.in[3][i]; p.ph = a.in[4][i]; p.pt = a.in[5][i];
+          const TFrame t = to_tframe(p, gam, rad, a.xl);
+          xt = t.xt; yt = t.yt; zt = t.zt;
+          lost = t.lost;
+        }
+        if (!lost) {
+          Cell c = cic_cell(xt, yt, zt, g);
           if (cell_inside(c, nx, ny, nz)) {
             cell[u] = (int)lin_cell(c, nx, ny);
             pk[u] = (unsigned)(c.ix - 1) | ((unsigned)(c.jx - 1) << 10) |
@@ -1463,7 +1501,7 @@ __global__ void __launch_bounds__(BLOCK) k_wake_line(WakeArgs a) {
       Particle p;
       p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
       p.py = a.in[3][i]; p.ph = a.in[4][i]; p.pt = a.in[5][i];
-      const TFrame t = to_tframe(p, gam, rad, a.xl);
+      const TFrame t = a.tframe ? stored_tframe(p, gam) : to_tframe(p, gam, rad, a.xl);
       if (!t.lost) {
         const int iizz = (int)((t.zt - zmin) / hzw + 1);
         const double ab = ((zmin - t.zt) + iizz * hzw) / hzw;

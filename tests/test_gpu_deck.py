@@ -66,7 +66,9 @@ def test_deck_runner_matches_the_oracle(tmp_path):
     assert got.shape == want.shape == (101, 11)
     fin = np.isfinite(want)
     assert np.array_equal(fin, np.isfinite(got))
-    np.testing.assert_allclose(got[fin], want[fin], rtol=1e-12, atol=0)
+    # the table sums over the downloaded bunch, whose particle order the
+    # upload changed (sorted by cell): sums agree to rounding
+    np.testing.assert_allclose(got[fin], want[fin], rtol=1e-10, atol=0)
     # the oracle over the same segments
     ref, z, rows_o = d.refptcl(), 0.0, []
     for kind, item in deck.lattice_segments(d, wd, {-8}):
