@@ -102,23 +102,38 @@ __device__ __forceinline__ int upload_key(double x, double y, double ph, const d
 }
 
 // box[0..5] = min/max over the nb partials, box[6..8] = bins per unit length
-__global__ void k_upload_box_final(const double* part, int nb, int nx, int ny, int nz,
-                                   double* box) {
-  __shared__ double red[6];
-  if (threadIdx.x < 6) {
-    const int d = threadIdx.x;
-    double t = part[d];
-    for (int b = 1; b < nb; b++) t = (d & 1) ? fmax(t, part[6 * b + d]) : fmin(t, part[6 * b + d]);
-    red[d] = t;
+// (one block of 256 threads: each thread folds a strided share of the
+// partials, then the block combines the threads' values)
+__global__ void __launch_bounds__(256) k_upload_box_final(const double* part, int nb, int nx,
+                                                          int ny, int nz, double* box) {
+  __shared__ double red[6][8];
+  double v[6] = {1e300, -1e300, 1e300, -1e300, 1e300, -1e300};
+  for (int b = threadIdx.x; b < nb; b += blockDim.x)
+#pragma unroll
+    for (int d = 0; d < 6; d++) v[d] = (d & 1) ? fmax(v[d], part[6 * b + d]) : fmin(v[d], part[6 * b + d]);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < 6; d++) {
+    double t = v[d];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_xor_sync(0xffffffffu, t, o);
+      t = (d & 1) ? fmax(t, u) : fmin(t, u);
+    }
+    if (lane == 0) red[d][wid] = t;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     const int m[3] = {nx, ny, nz};
     for (int d = 0; d < 3; d++) {
-      box[2 * d] = red[2 * d];
-      box[2 * d + 1] = red[2 * d + 1];
-      const double w = red[2 * d + 1] - red[2 * d];
-      box[6 + d] = w > 0.0 ? (double)(m[d] - 1) / w : 0.0;
+      double lo = red[2 * d][0], hi = red[2 * d + 1][0];
+      for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+        lo = fmin(lo, red[2 * d][w]);
+        hi = fmax(hi, red[2 * d + 1][w]);
+      }
+      box[2 * d] = lo;
+      box[2 * d + 1] = hi;
+      const double wd = hi - lo;
+      box[6 + d] = wd > 0.0 ? (double)(m[d] - 1) / wd : 0.0;
     }
   }
 }
@@ -730,7 +745,7 @@ int upload_order(impz_bunch_t b, long long n) {
   CK(cudaMemsetAsync(&b->st->done_scan, 0, sizeof(unsigned int), b->stream));
   k_upload_box<<<nb, 256, 0, b->stream>>>(b->pbuf[0][0], b->pbuf[0][2], b->pbuf[0][4], n,
                                           b->rng_part);
-  k_upload_box_final<<<1, 32, 0, b->stream>>>(b->rng_part, nb, b->nx, b->ny, b->nz, box);
+  k_upload_box_final<<<1, 256, 0, b->stream>>>(b->rng_part, nb, b->nx, b->ny, b->nz, box);
   k_upload_count<<<nb, 256, 0, b->stream>>>(b->pbuf[0][0], b->pbuf[0][2], b->pbuf[0][4], n, box,
                                             b->nx, b->ny, b->nz, b->counts);
   CK(cudaGetLastError());

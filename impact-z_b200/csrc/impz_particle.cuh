@@ -842,7 +842,9 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   stage_programs(progs, sp);
   if (threadIdx.x == 0) sgeom = st->geom;
   __syncthreads();
-  const volatile Geom& g = sgeom;
+  // the geometry lives in registers for the whole pass (a volatile shared
+  // reference re-read it per particle: 5 % slower)
+  const Geom g = sgeom;
   const double xl = a.k.Scxl, xk = a.k.xk;
   const bool kick = a.kick != 0;
   const bool post = a.do_post != 0;

@@ -32,6 +32,15 @@ def load_oracle():
     return mod
 
 
+def reference_path(*parts):
+    """A path inside a checkout of the reference (IMPACT-Z) named by the
+    environment variable IMPZ_REFERENCE_TREE, or None when it is unset; the
+    tests that read the reference's example decks or its GUI deck reader skip
+    without it."""
+    root = os.environ.get("IMPZ_REFERENCE_TREE")
+    return os.path.join(root, *parts) if root else None
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
 

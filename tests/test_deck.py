@@ -7,14 +7,14 @@ import os
 import numpy as np
 import pytest
 
-from conftest import load_impz, load_oracle
+from conftest import load_impz, load_oracle, reference_path
 
 impz = load_impz()
 from impz_b200 import beams, deck  # noqa: E402
 
-EXAMPLES = "/root/reference/examples"
+EXAMPLES = reference_path("examples") or ""
 have_examples = pytest.mark.skipif(not os.path.isdir(EXAMPLES),
-                                   reason="reference examples not present")
+                                   reason="IMPZ_REFERENCE_TREE unset (the reference's examples)")
 
 
 @have_examples
@@ -96,10 +96,11 @@ def test_particles_and_diag_files_round_trip(tmp_path):
                                   np.c_[rows[:, 0], rows[:, 39:45]])
 
 
-GUI_READER = "/root/reference/GUI/src/ImpactFile.py"
+GUI_READER = reference_path("GUI", "src", "ImpactFile.py") or ""
 
 
-@pytest.mark.skipif(not os.path.exists(GUI_READER), reason="reference GUI not present")
+@pytest.mark.skipif(not os.path.exists(GUI_READER),
+                    reason="IMPZ_REFERENCE_TREE unset (the reference's GUI deck reader)")
 @pytest.mark.parametrize("example", ["Example1", "Example2", "Example3"])
 def test_deck_reader_agrees_with_the_reference_gui_reader(example):
     """The reference's own Python deck reader (GUI/src/ImpactFile.py,

@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import load_impz, load_oracle
+from conftest import load_impz, load_oracle, reference_path
 
 impz = load_impz()
 orc = load_oracle()
@@ -234,10 +234,11 @@ def test_rf_cavity_under_kick2_gains_the_map_integrators_energy(etype):
         assert abs(r2[-1, c] / r1[-1, c] - 1) < 1e-2
 
 
-EXAMPLE1 = "/root/reference/examples/Example1"
+EXAMPLE1 = reference_path("examples", "Example1") or ""
 
 
-@pytest.mark.skipif(not os.path.isdir(EXAMPLE1), reason="the reference's examples are absent")
+@pytest.mark.skipif(not os.path.isdir(EXAMPLE1),
+                    reason="IMPZ_REFERENCE_TREE unset (the reference's examples)")
 def test_example1_dtl_cells_on_the_oracle():
     """The reference's Example1 (Flagmap=2: nine DTL cells over rfdata
     Fourier coefficients, quadrupoles and a drift) through the deck reader

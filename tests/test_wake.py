@@ -12,13 +12,13 @@ import os
 import numpy as np
 import pytest
 
-from conftest import load_impz, load_oracle
+from conftest import load_impz, load_oracle, reference_path
 
 impz = load_impz()
 orc = load_oracle()
 from impz_b200 import deck  # noqa: E402
 
-EXAMPLES = "/root/reference/examples"
+EXAMPLES = reference_path("examples") or ""
 
 
 def synthetic_table(rows=5000, hwk=2.0e-6, seed=7):
@@ -266,7 +266,8 @@ def test_deck_wake_controls():
     assert w[3]["on"] and not w[3]["transverse"]  # flagbtw = 2 stays
 
 
-@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference examples not present")
+@pytest.mark.skipif(not os.path.isdir(EXAMPLES),
+                    reason="IMPZ_REFERENCE_TREE unset (the reference's examples)")
 def test_example3_runs_with_its_wake_on_the_oracle():
     """Example3's ten -41 controls switch the cavities' read-in wake
     (rfdata41.in) on and off around the 1.3 GHz cavities, and its -52 laser
