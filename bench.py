@@ -469,11 +469,14 @@ def run_chicane(args):
 
 
 def run_scan(args):
-    """The batched parameter scan: 256 independent proton bunches (N
-    log-uniform in [1e4, 2e6], grids 16^3 / 32x32x64 / 64x64x128, gradient and
-    current drawn per bunch, 25 FODO periods = 400 steps), all advanced
-    together by impz_run_batch, against the same bunches run one after the
-    other.  Wall clock around each (the calls are synchronous)."""
+    """The batched parameter scan: 256 independent proton bunches
+    (N log-uniform in [1e4, 2e6], grids 16^3 / 32x32x64 / 64x64x128, gradient
+    and current drawn per bunch, 25 FODO periods = 400 steps), all advanced
+    together by impz_run_batch in the FP32-convolution form (one packed launch
+    per particle kernel and one per field-solve kernel and grid size, each step
+    pair a CUDA graph), against the same 256 runs done one by one in the plain
+    FP64 form, and one by one in the FP32 form.  Wall clock around each (the
+    calls are synchronous), bunches uploaded before the clock starts."""
     import torch
     impz = impz_pkg()
     from impz_b200 import beams
@@ -482,29 +485,43 @@ def run_scan(args):
     impz.lib().impz_set_device(local)
     jobs = beams.scan_jobs(nbunch=args.jobs or 256)
     data = [beams.make_scan_bunch(j) for j in jobs]
-    bunches = [impz.Bunch(p, j["current"], beams.PROTON_MASS_EV, 1.0, 402.5e6, r, j["grid"],
-                          form=impz.FORM_FP32CONV, track_ids=False)
-               for j, (p, r) in zip(jobs, data)]
     lats = [j["lattice"] for j in jobs]
     work = sum(j["n"] * impz.count_steps(j["lattice"]) for j in jobs)
     warm = [beams.fodo_steps(args.warmup, nseg=4)] * len(jobs)
-    impz.run_batch(bunches, warm)
 
-    def reload():
+    def make(form):
+        return [impz.Bunch(p, j["current"], beams.PROTON_MASS_EV, 1.0, 402.5e6, r, j["grid"],
+                           form=form, track_ids=False) for j, (p, r) in zip(jobs, data)]
+
+    def reload(bunches):
         for b, j, (p, r) in zip(bunches, jobs, data):
             b.upload(p, j["current"], r)
         torch.cuda.synchronize()
 
-    reload()
+    def one_by_one(bunches):
+        for b in bunches:
+            b.run(beams.fodo_steps(args.warmup, nseg=4))
+        reload(bunches)
+        t0 = time.perf_counter()
+        for b, lat in zip(bunches, lats):
+            b.run(lat)
+        return time.perf_counter() - t0
+
+    bunches = make(impz.FORM_FP32CONV)
+    impz.run_batch(bunches, warm)
+    reload(bunches)
+    clocks = ClockSampler(local)
+    clocks.start()
     t0 = time.perf_counter()
     impz.run_batch(bunches, lats)
     tb = time.perf_counter() - t0
-    reload()
-    t0 = time.perf_counter()
-    for b, lat in zip(bunches, lats):
-        b.run(lat)
-    ts = time.perf_counter() - t0
+    clk = clocks.stop()
+    ts32 = one_by_one(bunches)
     for b in bunches:
+        b.close()
+    b64 = make(impz.FORM_FP64)
+    ts64 = one_by_one(b64)
+    for b in b64:
         b.close()
     line = {"metric": METRIC, "value": work / tb, "unit": UNIT, "n_gpus": 1,
             "steps": int(sum(impz.count_steps(l) for l in lats)), "warmup": args.warmup,
@@ -513,8 +530,10 @@ def run_scan(args):
             "config": {"workload": "batched scan: %d proton bunches, %d particles in all, "
                                    "400 steps each" % (len(jobs), sum(j["n"] for j in jobs)),
                        "form": "fp32-convolution", "timing": "wall clock, synchronous calls"},
-            "batched_s": tb, "one_by_one_s": ts, "one_by_one_value": work / ts,
-            "batch_speedup": ts / tb}
+            "clocks": clk, "batched_s": tb,
+            "one_by_one_fp64": {"seconds": ts64, "value": work / ts64},
+            "one_by_one_fp32conv": {"seconds": ts32, "value": work / ts32},
+            "batched_over_fp64_one_by_one": ts64 / tb}
     print(json.dumps(line), flush=True)
     return 0
 

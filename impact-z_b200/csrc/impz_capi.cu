@@ -1737,6 +1737,208 @@ int impz_run_advance(impz_bunch_t b, int budget, int* remaining) {
   return r;
 }
 
+// ---- packed batches -------------------------------------------------------
+// Bunches whose runs have the same steps (count and space-charge pattern),
+// form and device, and no wakes, advance together: each step is one launch
+// of the particle pass, the deposit and the count scan over a packed work
+// list of (bunch, block) items, and one launch per field-solve kernel for
+// each group of bunches with the same grid size.  Two steps are captured as
+// one CUDA graph and replayed.  Each bunch keeps its own step counter,
+// tables, geometry and last-block reductions, so its arithmetic is that of
+// its solo run.
+static bool batch_packable(impz_bunch_t* bs, int nb) {
+  if (nb < 2) return false;
+  const impz_bunch_t b0 = bs[0];
+  const int K = b0->lat.nsteps;
+  for (int i = 0; i < nb; i++) {
+    const impz_bunch_t b = bs[i];
+    if (b->device != b0->device || b->form != b0->form || b->lat.nsteps != K ||
+        b->parity != b0->parity || b->run_wake || b->prof_on || b->run_next != 1)
+      return false;
+    for (int s = 1; s <= K; s++)
+      if ((b->lat.steps[s].sc != 0) != (b0->lat.steps[s].sc != 0)) return false;
+  }
+  return true;
+}
+
+namespace {
+struct BatchGroup {
+  int nx, ny, nz;
+  int first, count;  // members [first, first+count) of the PoissonMember array
+};
+}  // namespace
+
+static int run_batch_packed(impz_bunch_t* bs, int nb) {
+  const impz_bunch_t b0 = bs[0];
+  cudaStream_t s = b0->stream;
+  const bool f32 = b0->f32();
+  bool light = true;
+  for (int i = 0; i < nb; i++) light = light && bs[i]->run_light;
+  // the prologues ran on the bunches' own streams
+  for (int i = 1; i < nb; i++) {
+    CK(cudaEventRecord(bs[i]->ev_dep, bs[i]->stream));
+    CK(cudaStreamWaitEvent(s, bs[i]->ev_dep, 0));
+  }
+  // host copies of the launch arguments: [parity][member] for the kicked
+  // and the kick-free passes and the deposit
+  const int p0 = b0->parity;
+  std::vector<AdvanceArgs> adv(4 * (size_t)nb);
+  std::vector<DepositArgs> dep(2 * (size_t)nb);
+  std::vector<ScanArgs> scn(nb);
+  std::vector<int> adv_offs(nb + 1, 0), dep_offs(nb + 1, 0), scan_offs(nb + 1, 0);
+  for (int i = 0; i < nb; i++) {
+    impz_bunch_t b = bs[i];
+    for (int p = 0; p < 2; p++) {
+      b->parity = p;
+      adv[(size_t)p * nb + i] = advance_args(b, b->dsteps, -1, 1, 1, 1, b->mom_out, 0);
+      adv[(size_t)(2 + p) * nb + i] = advance_args(b, b->dsteps, -1, 0, 1, 1, b->mom_out, 0);
+      dep[(size_t)p * nb + i] = deposit_args(b, b->dsteps, -1);
+    }
+    b->parity = p0;
+    scn[i] = ScanArgs{b->counts, b->cursor, b->bsum, b->G + 1, b->st};
+    adv_offs[i + 1] = adv_offs[i] + b->grid_adv;
+    dep_offs[i + 1] = dep_offs[i] + b->grid_dep;
+    scan_offs[i + 1] = scan_offs[i] + (int)((b->G + 1 + (1ll << IMPZ_SCAN_LOG) - 1) >> IMPZ_SCAN_LOG);
+  }
+  // groups of equal grid size for the field solve
+  std::vector<int> order(nb);
+  for (int i = 0; i < nb; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+    const impz_bunch_t x = bs[a], y = bs[c];
+    if (x->nx != y->nx) return x->nx < y->nx;
+    if (x->ny != y->ny) return x->ny < y->ny;
+    return x->nz < y->nz;
+  });
+  std::vector<PoissonMember> mem(nb);
+  std::vector<BatchGroup> groups;
+  for (int k = 0; k < nb; k++) {
+    const impz_bunch_t b = bs[order[k]];
+    PoissonBuffers pb = poisson_of(b);
+    PoissonMember& m = mem[k];
+    m.rho = pb.rho; m.qscale = pb.qscale; m.spec = pb.spec; m.ghat = pb.ghat; m.phi = pb.phi;
+    m.efield = pb.efield; m.twx = pb.twx; m.twy = pb.twy; m.twz = pb.twz; m.F = pb.F;
+    m.Gt = pb.Gt; m.st = pb.st;
+    if (groups.empty() || groups.back().nx != b->nx || groups.back().ny != b->ny ||
+        groups.back().nz != b->nz)
+      groups.push_back(BatchGroup{b->nx, b->ny, b->nz, k, 0});
+    groups.back().count++;
+  }
+  // one device allocation for all of it
+  size_t off = 0;
+  auto place = [&](size_t bytes) {
+    const size_t o = off;
+    off = round_up(off + bytes, kAlign);
+    return o;
+  };
+  const size_t o_adv = place(adv.size() * sizeof(AdvanceArgs));
+  const size_t o_dep = place(dep.size() * sizeof(DepositArgs));
+  const size_t o_scn = place(scn.size() * sizeof(ScanArgs));
+  const size_t o_mem = place(mem.size() * sizeof(PoissonMember));
+  const size_t o_ao = place(adv_offs.size() * sizeof(int));
+  const size_t o_do = place(dep_offs.size() * sizeof(int));
+  const size_t o_so = place(scan_offs.size() * sizeof(int));
+  char* dmem = nullptr;
+  CK(cudaMalloc((void**)&dmem, off));
+  CK(cudaMemcpyAsync(dmem + o_adv, adv.data(), adv.size() * sizeof(AdvanceArgs),
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dmem + o_dep, dep.data(), dep.size() * sizeof(DepositArgs),
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dmem + o_scn, scn.data(), scn.size() * sizeof(ScanArgs),
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dmem + o_mem, mem.data(), mem.size() * sizeof(PoissonMember),
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dmem + o_ao, adv_offs.data(), adv_offs.size() * sizeof(int),
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dmem + o_do, dep_offs.data(), dep_offs.size() * sizeof(int),
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dmem + o_so, scan_offs.data(), scan_offs.size() * sizeof(int),
+                     cudaMemcpyHostToDevice, s));
+  const AdvanceArgs* d_adv = (const AdvanceArgs*)(dmem + o_adv);
+  const DepositArgs* d_dep = (const DepositArgs*)(dmem + o_dep);
+  const ScanArgs* d_scn = (const ScanArgs*)(dmem + o_scn);
+  const PoissonMember* d_mem = (const PoissonMember*)(dmem + o_mem);
+  const int* d_ao = (const int*)(dmem + o_ao);
+  const int* d_do = (const int*)(dmem + o_do);
+  const int* d_so = (const int*)(dmem + o_so);
+  const int n_adv = adv_offs[nb], n_dep = dep_offs[nb], n_scan = scan_offs[nb];
+  const int nlaunch_sc = 3 + 9 * (int)groups.size();
+
+  // one step from parity p: the field solve and the kick (sc), or the pass alone
+  auto step = [&](int p, bool sc) -> cudaError_t {
+    cudaError_t e = cudaSuccess;
+    if (sc) {
+      for (const BatchGroup& g : groups) {
+        e = f32 ? launch_green_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+                : launch_green_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+        if (e != cudaSuccess) return e;
+      }
+      e = f32 ? fast::launch_deposit_packed(d_dep + (size_t)p * nb, d_do, nb, n_dep, s)
+              : exact::launch_deposit_packed(d_dep + (size_t)p * nb, d_do, nb, n_dep, s);
+      if (e != cudaSuccess) return e;
+      if ((e = exact::launch_scan_packed(d_scn, d_so, nb, n_scan, s)) != cudaSuccess) return e;
+      for (const BatchGroup& g : groups) {
+        e = f32 ? launch_conv_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+                : launch_conv_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+        if (e != cudaSuccess) return e;
+        e = f32 ? launch_efield_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+                : launch_efield_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+        if (e != cudaSuccess) return e;
+      }
+      g_launches += nlaunch_sc - 1;
+    }
+    const AdvanceArgs* a = d_adv + (size_t)(sc ? p : 2 + p) * nb;
+    e = f32 ? fast::launch_advance_packed(a, d_ao, nb, n_adv, true, light, s)
+            : exact::launch_advance_packed(a, d_ao, nb, n_adv, false, light, s);
+    g_launches += 1;
+    return e;
+  };
+
+  const int K = b0->lat.nsteps;
+  int p = p0;
+  cudaGraphExec_t gx[2] = {nullptr, nullptr};
+  int rc = IMPZ_OK;
+  for (int st = 1; st <= K && !rc;) {
+    const bool sc = b0->lat.steps[st].sc != 0;
+    if (sc && st + 1 <= K && b0->lat.steps[st + 1].sc) {
+      if (!gx[p]) {
+        cudaGraph_t g = nullptr;
+        const long long counted = g_launches.load();
+        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+          cudaError_t e1 = step(p, true);
+          cudaError_t e2 = e1 == cudaSuccess ? step(p ^ 1, true) : e1;
+          e = cudaStreamEndCapture(s, &g);
+          if (e2 != cudaSuccess) e = e2;
+        }
+        g_launches = counted;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&gx[p], g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "packed batch graph"); break; }
+      }
+      cudaError_t e = cudaGraphLaunch(gx[p], s);
+      if (e != cudaSuccess) { rc = cuda_fail(e, "cudaGraphLaunch"); break; }
+      g_launches += 2 * nlaunch_sc;
+      st += 2;  // two kicks: the parity is back where it was
+    } else {
+      cudaError_t e = step(p, sc);
+      if (e != cudaSuccess) { rc = cuda_fail(e, "packed batch step"); break; }
+      if (sc) p ^= 1;
+      st += 1;
+    }
+  }
+  const cudaError_t es = cudaStreamSynchronize(s);
+  for (int k = 0; k < 2; k++)
+    if (gx[k]) cudaGraphExecDestroy(gx[k]);
+  cudaFree(dmem);
+  if (!rc && es != cudaSuccess) rc = cuda_fail(es, "packed batch");
+  if (rc) return rc;
+  for (int i = 0; i < nb; i++) {
+    bs[i]->parity = p;
+    bs[i]->run_next = K + 1;
+  }
+  return IMPZ_OK;
+}
+
 int impz_run_batch(impz_bunch_t* bunches, const impz_elem_t* const* lattices,
                    const int* nelem, int nb) {
   if (!bunches || !lattices || !nelem || nb < 0) return IMPZ_ERR_ARG;
@@ -1745,6 +1947,13 @@ int impz_run_batch(impz_bunch_t* bunches, const impz_elem_t* const* lattices,
   for (int i = 0; i < nb; i++) {
     int r = run_begin(bunches[i], lattices[i], nelem[i]);
     if (r) return r;
+  }
+  if (batch_packable(bunches, nb)) {
+    CK(cudaSetDevice(bunches[0]->device));
+    int r = run_batch_packed(bunches, nb);
+    if (r) return r;
+    for (int i = 0; i < nb; i++) run_end(bunches[i]);
+    return IMPZ_OK;
   }
   // round robin, two steps per bunch per turn, so that every bunch's
   // stream holds work and small bunches fill the gaps of large ones

@@ -221,6 +221,33 @@ struct WakeArgs {
   Consts k;
 };
 
+// One bunch of a group of bunches with the same grid size and form, for the
+// field solve launched once for the whole group (the *_group kernels):
+// blockIdx.y or blockIdx.z selects the member.
+struct PoissonMember {
+  unsigned long long* rho;  // int64 charge (read by the forward pass, cleared by the field)
+  double qscale;            // grid value of one fixed-point quantum
+  void* spec;               // spectrum (complex T)
+  void* ghat;               // G-hat octant (T) / DCT work
+  void* phi;                // potential (T)
+  void* efield;             // {Ex,Ey,Ez,0} per node (T)
+  const void* twx;          // twiddles of length 2nx, 2ny, 2nz (complex T)
+  const void* twy;
+  const void* twz;
+  double* F;                // IGF corners
+  double* Gt;               // FP64 Green octant
+  DevState* st;
+};
+
+// the arguments of one bunch's count scan in a packed launch (k_scan)
+struct ScanArgs {
+  int* counts;
+  int* cursor;
+  int* bsum;
+  long long total;
+  DevState* st;
+};
+
 #define IMPZ_SCAN_LOG 12      // 4096 cells per scan block (1024 threads x 4)
 #ifndef IMPZ_DEP_TILE
 #define IMPZ_DEP_TILE 4096    // deposit tile entries: two int32 halves + an int32 count (48 KB)

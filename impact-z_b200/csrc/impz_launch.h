@@ -59,6 +59,12 @@ inline cudaError_t launch_pdl(void (*kernel)(KP...), dim3 grid, dim3 block, size
   cudaError_t launch_scan(int* counts, int* cursor, int* bsum, long long total,          \
                           DevState* st, cudaStream_t s);                                 \
   int max_blocks_advance(bool f32);                                                      \
+  cudaError_t launch_advance_packed(const AdvanceArgs* args, const int* offs, int nmem,  \
+                                    int blocks, bool f32, bool light, cudaStream_t s);   \
+  cudaError_t launch_deposit_packed(const DepositArgs* args, const int* offs, int nmem,  \
+                                    int blocks, cudaStream_t s);                          \
+  cudaError_t launch_scan_packed(const ScanArgs* args, const int* offs, int nmem, int blocks, \
+                                 cudaStream_t s);                                         \
   int max_blocks_deposit();                                                              \
   }
 IMPZ_DECLARE_PARTICLE_LAUNCHERS(exact)
@@ -98,6 +104,17 @@ template <typename T>
 cudaError_t launch_conv_rest(const PoissonBuffers& b, cudaStream_t s);
 template <typename T>
 cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s);
+// the same solve for nmem bunches of one grid size (PoissonMember array in
+// device memory), one launch per kernel for the whole group
+template <typename T>
+cudaError_t launch_green_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                               cudaStream_t s);
+template <typename T>
+cudaError_t launch_conv_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                              cudaStream_t s);
+template <typename T>
+cudaError_t launch_efield_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                                cudaStream_t s);
 // true when every Poisson kernel of the form fits the device's shared memory
 template <typename T>
 bool poisson_fits(int nx, int ny, int nz);

@@ -487,13 +487,13 @@ __device__ __forceinline__ void gather_e(const void* ef, const Cell& c, int nx, 
 template <>
 __device__ __forceinline__ void gather_e<false>(const void* ef, const Cell& c, int nx, int ny,
                                                 double& ex, double& ey, double& ez) {
-  const long long sy = nx, sz = (long long)nx * ny;
-  const long long b = (long long)(c.ix - 1) + sy * (c.jx - 1) + sz * (c.kx - 1);
+  const int sy = nx, sz = nx * ny;  // a grid holds at most 64 x 64 x 4096 nodes
+  const int b = (c.ix - 1) + sy * (c.jx - 1) + sz * (c.kx - 1);
   const double ab = c.ab, cd = c.cd, efw = c.ef;
   const double ab1 = 1.0 - ab, cd1 = 1.0 - cd, ef1 = 1.0 - efw;
   const double2* E = reinterpret_cast<const double2*>(ef);
-  const long long nodes[8] = {b, b + sy, b + sy + sz, b + sz, b + 1 + sz, b + 1 + sy + sz,
-                              b + 1 + sy, b + 1};
+  const int nodes[8] = {b, b + sy, b + sy + sz, b + sz, b + 1 + sz, b + 1 + sy + sz, b + 1 + sy,
+                        b + 1};
   double2 A[8], B[8];
 #pragma unroll
   for (int q = 0; q < 8; q++) {
@@ -519,13 +519,13 @@ __device__ __forceinline__ void gather_e<false>(const void* ef, const Cell& c, i
 template <>
 __device__ __forceinline__ void gather_e<true>(const void* ef, const Cell& c, int nx, int ny,
                                                double& ex, double& ey, double& ez) {
-  const long long sy = nx, sz = (long long)nx * ny;
-  const long long b = (long long)(c.ix - 1) + sy * (c.jx - 1) + sz * (c.kx - 1);
+  const int sy = nx, sz = nx * ny;
+  const int b = (c.ix - 1) + sy * (c.jx - 1) + sz * (c.kx - 1);
   const float ab = (float)c.ab, cd = (float)c.cd, efw = (float)c.ef;
   const float ab1 = 1.0f - ab, cd1 = 1.0f - cd, ef1 = 1.0f - efw;
   const float4* E = reinterpret_cast<const float4*>(ef);
-  const long long nodes[8] = {b, b + sy, b + sy + sz, b + sz, b + 1 + sz, b + 1 + sy + sz,
-                              b + 1 + sy, b + 1};
+  const int nodes[8] = {b, b + sy, b + sy + sz, b + sz, b + 1 + sz, b + 1 + sy + sz, b + 1 + sy,
+                        b + 1};
   const float w[8] = {ab * cd * efw, ab * cd1 * efw, ab * cd1 * ef1, ab * cd * ef1,
                       ab1 * cd * ef1, ab1 * cd1 * ef1, ab1 * cd1 * efw, ab1 * cd * efw};
   float sx = 0.f, sy_ = 0.f, sz_ = 0.f;
@@ -824,8 +824,11 @@ __device__ __forceinline__ void lorentz_kick(Particle& p, double exn, double eyn
   }
 }
 
+// The pass of one bunch as block vbx of a grid of vgx blocks: k_advance
+// runs it for one bunch (vbx = vbx), k_advance_packed for the bunch
+// that owns the block in a launch over many.
 template <int BLOCK, bool F32, int U, bool LIGHT>
-__global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a) {
+__device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx, const int vgx) {
   __shared__ double red[BLOCK / 32][IMPZ_RAW_LEN];
   __shared__ double redr[BLOCK / 32][8];
   __shared__ unsigned int s_last;
@@ -870,7 +873,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   long long nlive = 0, nkept = 0;
   unsigned int err = 0;
 
-  const long long stride = (long long)gridDim.x * BLOCK * U;
+  const long long stride = (long long)vgx * BLOCK * U;
   const long long nround = (n + stride - 1) / stride * stride;
   // the next pass's particles are loaded while this pass computes (each
   // thread reads its own slots only; in-place launches write slot i back)
@@ -888,13 +891,13 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
     }
   };
 #if IMPZ_ADV_PREFETCH
-  fetch((long long)blockIdx.x * BLOCK * U + threadIdx.x);
+  fetch((long long)vbx * BLOCK * U + threadIdx.x);
 #endif
-  for (long long i0 = (long long)blockIdx.x * BLOCK * U + threadIdx.x; i0 < nround;
+  for (long long i0 = (long long)vbx * BLOCK * U + threadIdx.x; i0 < nround;
        i0 += stride) {
     Particle p[U];
     bool keep[U];
-    long long key[U];
+    int key[U];  // deposit cell (a grid holds at most 64 x 64 x 4096 nodes)
 #if !IMPZ_ADV_PREFETCH
     fetch(i0);
 #endif
@@ -917,7 +920,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
           keep[u] = false;
         } else {
           Cell cd = cic_cell(t.xt, t.yt, t.zt, g);
-          key[u] = cell_inside(cd, nx, ny, nz) ? lin_cell(cd, nx, ny) : G;
+          key[u] = cell_inside(cd, nx, ny, nz) ? (int)lin_cell(cd, nx, ny) : (int)G;
           // cvbkforth1st (BeamBunch.f90:1681-1699); betai reuses conv1st's
           // tmpbet, the same expression of the same operands
           const double rcp = t.rcp;
@@ -1018,7 +1021,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
       if (kick) {
         const unsigned active = __ballot_sync(0xffffffffu, keep[u]);
         if (keep[u]) {
-          const unsigned grp = __match_any_sync(active, (unsigned long long)key[u]);
+          const unsigned grp = __match_any_sync(active, key[u]);
           const int leader = __ffs(grp) - 1;
           const int rank = __popc(grp & ((1u << lane) - 1u));
           int base = 0;
@@ -1071,7 +1074,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
     const int v = threadIdx.x;
     double x = red[0][v];
     for (int w = 1; w < nw; w++) x = v < 37 ? x + red[w][v] : fmax(x, red[w][v]);
-    a.mom_part[(size_t)blockIdx.x * IMPZ_RAW_LEN + v] = x;
+    a.mom_part[(size_t)vbx * IMPZ_RAW_LEN + v] = x;
   }
   if (threadIdx.x < 8) {
     const int v = threadIdx.x;
@@ -1080,11 +1083,11 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
       double y = redr[w][v];
       x = (v >= 6) ? x + y : ((v & 1) ? fmax(x, y) : fmin(x, y));
     }
-    a.rng_part[(size_t)blockIdx.x * 8 + v] = x;
+    a.rng_part[(size_t)vbx * 8 + v] = x;
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(&st->done_range, 1u) == gridDim.x - 1) ? 1u : 0u;
+  if (threadIdx.x == 0) s_last = (atomicAdd(&st->done_range, 1u) == vgx - 1) ? 1u : 0u;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
@@ -1093,7 +1096,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   // values l and l+32; 0..43 moments, 44..51 range), then thread v combines
   // the warps' partials in warp order: a fixed order, and the loads of one
   // lane are independent, so they overlap instead of chaining.
-  const int nb = gridDim.x;
+  const int nb = vgx;
   const int row = a.fixed_step >= 0 ? a.mom_index : s;
   const int b0 = wid * nb / nw, b1 = (wid + 1) * nb / nw;
   for (int v = lane; v < IMPZ_RAW_LEN + 8; v += 32) {
@@ -1156,6 +1159,46 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
   }
 }
 
+template <int BLOCK, bool F32, int U, bool LIGHT>
+__global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a) {
+  advance_pass<BLOCK, F32, U, LIGHT>(a, blockIdx.x, gridDim.x);
+}
+
+// The member of a packed launch that owns block `blk`: blocks
+// [offs[m], offs[m+1]) belong to member m (binary search, offs[0] = 0).
+__device__ __forceinline__ int packed_member(const int* __restrict__ offs, int nmem, int blk) {
+  int lo = 0, hi = nmem - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(offs + mid) <= blk) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Copies a launch-argument struct of `bytes` (a multiple of 8) to shared
+// memory (whole block).
+__device__ __forceinline__ void copy_args(void* dst, const void* src, int bytes) {
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(src);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(dst);
+  for (int e = threadIdx.x; e < bytes / 8; e += blockDim.x) d[e] = __ldg(s + e);
+}
+
+// Every member's pass in one launch: a packed work list of (bunch, block)
+// items, each bunch keeping its own block count and last-block reduction.
+template <int BLOCK, bool F32, int U, bool LIGHT>
+__global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB)
+    k_advance_packed(const AdvanceArgs* __restrict__ args, const int* __restrict__ offs,
+                     int nmem) {
+  __shared__ __align__(16) AdvanceArgs sa;
+  static_assert(sizeof(AdvanceArgs) % 8 == 0, "argument copy in 8-byte words");
+  const int m = packed_member(offs, nmem, blockIdx.x);
+  copy_args(&sa, args + m, (int)sizeof(AdvanceArgs));
+  __syncthreads();
+  advance_pass<BLOCK, F32, U, LIGHT>(sa, blockIdx.x - __ldg(offs + m),
+                                     __ldg(offs + m + 1) - __ldg(offs + m));
+}
+
 // ---------------------------------------------------------------------
 // Charge deposit.  Each block takes chunks of BLOCK*U consecutive particles.
 // Particles are kept sorted by the previous step's deposit cell, so after the
@@ -1185,7 +1228,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a)
 #define IMPZ_DEP_LOBITS 20
 #define IMPZ_DEP_FIXBITS_1WORD 21
 template <int BLOCK, int U>
-__global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a) {
+__device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx, const int vgx) {
   static_assert(BLOCK * U <= 1024, "one-word tile sums sized for chunks of at most 1024");
   extern __shared__ __align__(16) unsigned int tsm[];
   unsigned int* tlo = tsm;                       // [IMPZ_DEP_TILE]
@@ -1205,7 +1248,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
     tcnt[e] = 0u;
   }
   __syncthreads();
-  const volatile Geom& g = sg;
+  const Geom g = sg;  // in registers: a volatile shared reference measured 6 % slower
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const long long P = (long long)nx * ny;
   const long long G = P * nz;
@@ -1220,7 +1263,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
   const bool split = a.fixbits > IMPZ_DEP_FIXBITS_1WORD;
   const long long chunk = (long long)BLOCK * U;
   const int lane = threadIdx.x & 31;
-  for (long long c0 = (long long)blockIdx.x * chunk; c0 < n; c0 += (long long)gridDim.x * chunk) {
+  for (long long c0 = (long long)vbx * chunk; c0 < n; c0 += (long long)vgx * chunk) {
     int cell[U];
     unsigned pk[U];  // x | y << 10 | z << 20 (nx, ny <= 64, nz <= 4096)
     double wab[U], wcd[U], wef[U];
@@ -1373,6 +1416,23 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a)
   }
 }
 
+template <int BLOCK, int U>
+__global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a) {
+  deposit_pass<BLOCK, U>(a, blockIdx.x, gridDim.x);
+}
+
+template <int BLOCK, int U>
+__global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB)
+    k_deposit_packed(const DepositArgs* __restrict__ args, const int* __restrict__ offs,
+                     int nmem) {
+  __shared__ __align__(16) DepositArgs sa;
+  static_assert(sizeof(DepositArgs) % 8 == 0, "argument copy in 8-byte words");
+  const int m = packed_member(offs, nmem, blockIdx.x);
+  copy_args(&sa, args + m, (int)sizeof(DepositArgs));
+  __syncthreads();
+  deposit_pass<BLOCK, U>(sa, blockIdx.x - __ldg(offs + m), __ldg(offs + m + 1) - __ldg(offs + m));
+}
+
 // Exclusive scan over the block of one value per thread; *total gets the
 // block's sum.  wsum: BLOCK/32 ints of shared memory.
 template <int BLOCK>
@@ -1408,12 +1468,12 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int* wsum, int* total
 // block to finish turns bsum into exclusive block offsets.  Each thread
 // takes four consecutive cells (one 16-byte load and store).
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_scan(int* counts, int* cursor, int* bsum,
-                                                long long total, DevState* st) {
+__device__ __forceinline__ void scan_pass(int* counts, int* cursor, int* bsum, long long total,
+                                          DevState* st, const int vbx, const int vgx) {
   static_assert((BLOCK << 2) == (1 << IMPZ_SCAN_LOG), "four cells per thread");
   __shared__ int wsum[BLOCK / 32 + 1];
   __shared__ unsigned int s_last;
-  const long long i0 = ((long long)blockIdx.x << IMPZ_SCAN_LOG) + 4ll * threadIdx.x;
+  const long long i0 = ((long long)vbx << IMPZ_SCAN_LOG) + 4ll * threadIdx.x;
   int v[4];
   const bool full = i0 + 3 < total;
   if (full) {
@@ -1442,15 +1502,15 @@ __global__ void __launch_bounds__(BLOCK) k_scan(int* counts, int* cursor, int* b
     for (int j = 0; j < 4; j++)
       if (i0 + j < total) cursor[i0 + j] = o[j];
   }
-  if (threadIdx.x == 0) bsum[blockIdx.x] = btotal;
+  if (threadIdx.x == 0) bsum[vbx] = btotal;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(&st->done_scan, 1u) == gridDim.x - 1) ? 1u : 0u;
+  if (threadIdx.x == 0) s_last = (atomicAdd(&st->done_scan, 1u) == vgx - 1) ? 1u : 0u;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
   // block totals -> exclusive block offsets, BLOCK at a time with a carry
-  const int nb = (int)gridDim.x;
+  const int nb = (int)vgx;
   int carry = 0;
   for (int k0 = 0; k0 < nb; k0 += BLOCK) {
     const int k = k0 + threadIdx.x;
@@ -1461,6 +1521,21 @@ __global__ void __launch_bounds__(BLOCK) k_scan(int* counts, int* cursor, int* b
     carry += sum;
   }
   if (threadIdx.x == 0) st->done_scan = 0;
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scan(int* counts, int* cursor, int* bsum,
+                                                long long total, DevState* st) {
+  scan_pass<BLOCK>(counts, cursor, bsum, total, st, blockIdx.x, gridDim.x);
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_scan_packed(const ScanArgs* __restrict__ args,
+                                                       const int* __restrict__ offs, int nmem) {
+  const int m = packed_member(offs, nmem, blockIdx.x);
+  const ScanArgs a = args[m];
+  scan_pass<BLOCK>(a.counts, a.cursor, a.bsum, a.total, a.st, blockIdx.x - __ldg(offs + m),
+                   __ldg(offs + m + 1) - __ldg(offs + m));
 }
 
 // ---------------------------------------------------------------------

@@ -31,11 +31,46 @@ cudaError_t launch_advance(const AdvanceArgs& a, bool f32, bool light, int grid,
   return light ? launch_adv_t<false, true>(a, grid, s) : launch_adv_t<false, false>(a, grid, s);
 }
 
+template <bool F32, bool LIGHT>
+static cudaError_t launch_adv_packed_t(const AdvanceArgs* args, const int* offs, int nmem,
+                                       int blocks, cudaStream_t s) {
+  auto kern = k_advance_packed<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT>;
+  static cudaError_t once =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdvSmem);
+  if (once != cudaSuccess) return once;
+  return launch_pdl(kern, dim3(blocks), dim3(IMPZ_ADV_BLOCK), kAdvSmem, s, args, offs, nmem);
+}
+
+cudaError_t launch_advance_packed(const AdvanceArgs* args, const int* offs, int nmem, int blocks,
+                                  bool f32, bool light, cudaStream_t s) {
+  if (f32)
+    return light ? launch_adv_packed_t<true, true>(args, offs, nmem, blocks, s)
+                 : launch_adv_packed_t<true, false>(args, offs, nmem, blocks, s);
+  return light ? launch_adv_packed_t<false, true>(args, offs, nmem, blocks, s)
+               : launch_adv_packed_t<false, false>(args, offs, nmem, blocks, s);
+}
+
 static cudaError_t dep_attr() {
   static cudaError_t once = cudaFuncSetAttribute(
       k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
       (int)kDepSmem);
   return once;
+}
+
+cudaError_t launch_deposit_packed(const DepositArgs* args, const int* offs, int nmem, int blocks,
+                                  cudaStream_t s) {
+  auto kern = k_deposit_packed<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>;
+  static cudaError_t once =
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
+  if (once != cudaSuccess) return once;
+  return launch_pdl(kern, dim3(blocks), dim3(IMPZ_DEP_BLOCK), kDepSmem, s, args, offs, nmem);
+}
+
+cudaError_t launch_scan_packed(const ScanArgs* args, const int* offs, int nmem, int blocks,
+                               cudaStream_t s) {
+  k_scan_packed<IMPZ_SCAN_THREADS><<<blocks, IMPZ_SCAN_THREADS, 0, s>>>(
+      args, offs, nmem);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s) {

@@ -207,6 +207,115 @@ cudaError_t launch_efield(const PoissonBuffers& b, cudaStream_t s) {
                     b.wake_line);
 }
 
+// ---- groups: the same solve for several bunches of one grid size, one
+// launch per kernel (PoissonMember array `mem` in device memory)
+static int group_grid(long long work, int block, int nmem) {
+  long long g = (work + block - 1) / block;
+  const long long cap = (148 * 16 + nmem - 1) / nmem;
+  if (g > cap) g = cap;
+  return (int)(g < 1 ? 1 : g);
+}
+
+template <typename TI, typename T, int TL>
+static cudaError_t dct_group_t(int axis, int n, long long es, long long ls, int ninner,
+                               long long os, int nouter, double scale,
+                               const PoissonMember* mem, int nmem, cudaStream_t s) {
+  auto kern = k_dct1_group<TI, T, T, TL>;
+  const size_t sm = dct_smem<T>(n, TL);
+  cudaError_t e = allow_smem(kern, sm);
+  if (e != cudaSuccess) return e;
+  dim3 g((ninner + TL - 1) / TL, nouter, nmem);
+  kern<<<g, 256, sm, s>>>(axis, ilog2(2 * n), es, ls, ninner, os, scale, mem);
+  return cudaGetLastError();
+}
+template <typename TI, typename T>
+static cudaError_t dct_group(int axis, int n, long long es, long long ls, int ninner, long long os,
+                             int nouter, double scale, const PoissonMember* mem, int nmem,
+                             cudaStream_t s) {
+  switch (dct_lines<T>(n)) {
+    case 16: return dct_group_t<TI, T, 16>(axis, n, es, ls, ninner, os, nouter, scale, mem, nmem, s);
+    case 8: return dct_group_t<TI, T, 8>(axis, n, es, ls, ninner, os, nouter, scale, mem, nmem, s);
+    case 4: return dct_group_t<TI, T, 4>(axis, n, es, ls, ninner, os, nouter, scale, mem, nmem, s);
+    default: return dct_group_t<TI, T, 2>(axis, n, es, ls, ninner, os, nouter, scale, mem, nmem, s);
+  }
+}
+
+template <typename T>
+cudaError_t launch_green_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                               cudaStream_t s) {
+  const long long nc = (long long)(nx + 2) * (ny + 2) * (nz + 2);
+  const long long ng = (long long)(nx + 1) * (ny + 1) * (nz + 1);
+  k_igf_corners_group<<<dim3(group_grid(nc, 256, nmem), nmem), 256, 0, s>>>(nx, ny, nz, mem);
+  k_igf_green_group<<<dim3(group_grid(ng, 256, nmem), nmem), 256, 0, s>>>(nx, ny, nz, mem);
+  const long long gx = nx + 1, gxy = (long long)(nx + 1) * (ny + 1);
+  const double scale = 1.0 / ((double)(2 * nx) * (double)(2 * ny) * (double)(2 * nz));
+  cudaError_t e;
+  if ((e = dct_group<double, T>(0, nx, 1, gx, ny + 1, gxy, nz + 1, 1.0, mem, nmem, s)) !=
+      cudaSuccess)
+    return e;
+  if ((e = dct_group<T, T>(1, ny, gx, 1, nx + 1, gxy, nz + 1, 1.0, mem, nmem, s)) != cudaSuccess)
+    return e;
+  if ((e = dct_group<T, T>(2, nz, gxy, 1, nx + 1, gx, ny + 1, scale, mem, nmem, s)) !=
+      cudaSuccess)
+    return e;
+  return cudaGetLastError();
+}
+
+template <typename T, int TKX>
+static cudaError_t zconv_group_t(const PoissonDims& d, const PoissonMember* mem, int nmem,
+                                 cudaStream_t s) {
+  const size_t sz = z_smem<T>(d.nz, TKX);
+  cudaError_t e = allow_smem(k_fft_z_conv_group<T, TKX>, sz);
+  if (e != cudaSuccess) return e;
+  dim3 gz((d.nx + 1 + TKX - 1) / TKX, 2 * d.ny, nmem);
+  return launch_pdl(k_fft_z_conv_group<T, TKX>, gz, dim3(256), sz, s, d, mem);
+}
+
+template <typename T>
+cudaError_t launch_conv_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                              cudaStream_t s) {
+  PoissonBuffers pb;
+  pb.nx = nx; pb.ny = ny; pb.nz = nz;
+  const PoissonDims d = dims_of(pb);
+  cudaError_t e;
+  const size_t sm = xyf_smem<T>(nx, ny, IMPZ_XY_PARTS);
+  if ((e = allow_smem(k_fft_xy_fwd_group<T, IMPZ_XY_PARTS>, sm)) != cudaSuccess) return e;
+  if ((e = launch_pdl(k_fft_xy_fwd_group<T, IMPZ_XY_PARTS>, dim3(IMPZ_XY_PARTS, nz, nmem),
+                      dim3(IMPZ_XY_THREADS), sm, s, d, mem)) != cudaSuccess)
+    return e;
+  switch (ztile<T>(nz)) {
+    case 16: e = zconv_group_t<T, 16>(d, mem, nmem, s); break;
+    case 8: e = zconv_group_t<T, 8>(d, mem, nmem, s); break;
+    case 4: e = zconv_group_t<T, 4>(d, mem, nmem, s); break;
+    case 2: e = zconv_group_t<T, 2>(d, mem, nmem, s); break;
+    default: e = zconv_group_t<T, 1>(d, mem, nmem, s); break;
+  }
+  if (e != cudaSuccess) return e;
+  const size_t sxy = xy_smem<T>(nx, ny);
+  if ((e = allow_smem(k_fft_xy_inv_group<T>, sxy)) != cudaSuccess) return e;
+  return launch_pdl(k_fft_xy_inv_group<T>, dim3(nz, nmem), dim3(512), sxy, s, d, mem);
+}
+
+template <typename T>
+cudaError_t launch_efield_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                                cudaStream_t s) {
+  const long long G = (long long)nx * ny * nz;
+  return launch_pdl(k_efield_group<T>, dim3(group_grid(G, 256, nmem), nmem), dim3(256), 0, s, nx,
+                    ny, nz, mem);
+}
+
+template cudaError_t launch_green_group<double>(int, int, int, const PoissonMember*, int,
+                                                cudaStream_t);
+template cudaError_t launch_green_group<float>(int, int, int, const PoissonMember*, int,
+                                               cudaStream_t);
+template cudaError_t launch_conv_group<double>(int, int, int, const PoissonMember*, int,
+                                               cudaStream_t);
+template cudaError_t launch_conv_group<float>(int, int, int, const PoissonMember*, int,
+                                              cudaStream_t);
+template cudaError_t launch_efield_group<double>(int, int, int, const PoissonMember*, int,
+                                                 cudaStream_t);
+template cudaError_t launch_efield_group<float>(int, int, int, const PoissonMember*, int,
+                                               cudaStream_t);
 template cudaError_t launch_green<double>(const PoissonBuffers&, cudaStream_t);
 template cudaError_t launch_green<float>(const PoissonBuffers&, cudaStream_t);
 template cudaError_t launch_convolve<double>(const PoissonBuffers&, cudaStream_t);

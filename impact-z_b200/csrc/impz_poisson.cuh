@@ -204,17 +204,19 @@ struct PoissonDims {
 // stores interleaved with the transform's loads).
 // smem: Z[ny/2][2nx] (packed row pairs) and Tm[own kx][2ny] (y lines).
 template <typename T, int PARTS>
-__global__ void k_fft_xy_fwd(PoissonDims d, const unsigned long long* __restrict__ rho,
-                             double qscale, typename Cplx<T>::type* __restrict__ S,
-                             const typename Cplx<T>::type* __restrict__ twx,
-                             const typename Cplx<T>::type* __restrict__ twy) {
+__device__ __forceinline__ void fft_xy_fwd_body(const PoissonDims& d,
+                                                const unsigned long long* __restrict__ rho,
+                                                double qscale, typename Cplx<T>::type* __restrict__ S,
+                                                const typename Cplx<T>::type* __restrict__ twx,
+                                                const typename Cplx<T>::type* __restrict__ twy,
+                                                const int bx, const int by) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   griddep_wait();
   const int nx = d.nx, ny = d.ny, n1 = 2 * nx, n2 = 2 * ny, w = nx + 1;
   const int zp = line_pitch(n1), tp = line_pitch(n2);  // x-line and y-line pitches
   const int hy = ny / 2;
-  const int part = blockIdx.x, k = blockIdx.y;
+  const int part = bx, k = by;
   const int kx_lo = w * part / PARTS, nown = w * (part + 1) / PARTS - kx_lo;
   C* Z = reinterpret_cast<C*>(smem_raw);
   C* Tm = Z + hy * zp;
@@ -275,11 +277,30 @@ __global__ void k_fft_xy_fwd(PoissonDims d, const unsigned long long* __restrict
   }
 }
 
+template <typename T, int PARTS>
+__global__ void k_fft_xy_fwd(PoissonDims d, const unsigned long long* __restrict__ rho,
+                             double qscale, typename Cplx<T>::type* __restrict__ S,
+                             const typename Cplx<T>::type* __restrict__ twx,
+                             const typename Cplx<T>::type* __restrict__ twy) {
+  fft_xy_fwd_body<T, PARTS>(d, rho, qscale, S, twx, twy, blockIdx.x, blockIdx.y);
+}
+
+// the same for every bunch of a group of one grid size: blockIdx.z = member
+template <typename T, int PARTS>
+__global__ void k_fft_xy_fwd_group(PoissonDims d, const PoissonMember* __restrict__ mem) {
+  typedef typename Cplx<T>::type C;
+  const PoissonMember& m = mem[blockIdx.z];
+  fft_xy_fwd_body<T, PARTS>(d, m.rho, m.qscale, (C*)m.spec, (const C*)m.twx, (const C*)m.twy,
+                            blockIdx.x, blockIdx.y);
+}
+
 // z-convolve: block = (tile of TKX kx values, one ky).
 template <typename T, int TKX>
-__global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__ S,
-                             const T* __restrict__ ghat,
-                             const typename Cplx<T>::type* __restrict__ twz) {
+__device__ __forceinline__ void fft_z_conv_body(const PoissonDims& d,
+                                                typename Cplx<T>::type* __restrict__ S,
+                                                const T* __restrict__ ghat,
+                                                const typename Cplx<T>::type* __restrict__ twz,
+                                                const int bx, const int by) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   griddep_wait();
@@ -288,8 +309,8 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
   C* L = reinterpret_cast<C*>(smem_raw);
   C* twzs = L + TKX * lp;
   stage_tw(twzs, twz, n3);
-  const int kx0 = blockIdx.x * TKX;
-  const int ky = blockIdx.y;
+  const int kx0 = bx * TKX;
+  const int ky = by;
   const int ntk = min(TKX, nx + 1 - kx0);
   const size_t pstride = (size_t)n2 * (nx + 1);  // one z plane of S
   C* base = S + (size_t)ky * (nx + 1) + kx0;
@@ -323,12 +344,29 @@ __global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__
   }
 }
 
+template <typename T, int TKX>
+__global__ void k_fft_z_conv(PoissonDims d, typename Cplx<T>::type* __restrict__ S,
+                             const T* __restrict__ ghat,
+                             const typename Cplx<T>::type* __restrict__ twz) {
+  fft_z_conv_body<T, TKX>(d, S, ghat, twz, blockIdx.x, blockIdx.y);
+}
+
+template <typename T, int TKX>
+__global__ void k_fft_z_conv_group(PoissonDims d, const PoissonMember* __restrict__ mem) {
+  typedef typename Cplx<T>::type C;
+  const PoissonMember& m = mem[blockIdx.z];
+  fft_z_conv_body<T, TKX>(d, (C*)m.spec, (const T*)m.ghat, (const C*)m.twz, blockIdx.x,
+                          blockIdx.y);
+}
+
 // xy-inverse: one block per z plane k < nz; phi out (nx, ny, nz) real.
 template <typename T>
-__global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __restrict__ S,
-                             T* __restrict__ phi,
-                             const typename Cplx<T>::type* __restrict__ twx,
-                             const typename Cplx<T>::type* __restrict__ twy) {
+__device__ __forceinline__ void fft_xy_inv_body(const PoissonDims& d,
+                                                const typename Cplx<T>::type* __restrict__ S,
+                                                T* __restrict__ phi,
+                                                const typename Cplx<T>::type* __restrict__ twx,
+                                                const typename Cplx<T>::type* __restrict__ twy,
+                                                const int bx) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   griddep_wait();
@@ -341,7 +379,7 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
   C* twys = twxs + n1 / 2;
   stage_tw(twxs, twx, n1);
   stage_tw(twys, twy, n2);
-  const int k = blockIdx.x;
+  const int k = bx;
   const C* Sk = S + (size_t)k * n2 * (nx + 1);
   // y lines in bit-reversed order for the DIT inverse
   {
@@ -378,10 +416,27 @@ __global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __rest
   }
 }
 
+template <typename T>
+__global__ void k_fft_xy_inv(PoissonDims d, const typename Cplx<T>::type* __restrict__ S,
+                             T* __restrict__ phi,
+                             const typename Cplx<T>::type* __restrict__ twx,
+                             const typename Cplx<T>::type* __restrict__ twy) {
+  fft_xy_inv_body<T>(d, S, phi, twx, twy, blockIdx.x);
+}
+
+template <typename T>
+__global__ void k_fft_xy_inv_group(PoissonDims d, const PoissonMember* __restrict__ mem) {
+  typedef typename Cplx<T>::type C;
+  const PoissonMember& m = mem[blockIdx.y];
+  fft_xy_inv_body<T>(d, (const C*)m.spec, (T*)m.phi, (const C*)m.twx, (const C*)m.twy,
+                     blockIdx.x);
+}
+
 // ---------------------------------------------------------------------
 // greenf1tIntnew corner antiderivative (Field.f90:392-418), FP64, at the
 // (nx+2)(ny+2)(nz+2) corners v = (i-1)h - h/2.
-__global__ void k_igf_corners(int nx, int ny, int nz, const DevState* st, double* F) {
+__device__ __forceinline__ void igf_corners_body(int nx, int ny, int nz, const DevState* st,
+                                                 double* F) {
   const int ax = nx + 2, ay = ny + 2, az = nz + 2;
   const long long total = (long long)ax * ay * az;
   const double hx = st->geom.h[0], hy = st->geom.h[1], hz = st->geom.h[2];
@@ -406,9 +461,18 @@ __global__ void k_igf_corners(int nx, int ny, int nz, const DevState* st, double
   }
 }
 
+__global__ void k_igf_corners(int nx, int ny, int nz, const DevState* st, double* F) {
+  igf_corners_body(nx, ny, nz, st, F);
+}
+
+__global__ void k_igf_corners_group(int nx, int ny, int nz, const PoissonMember* __restrict__ mem) {
+  const PoissonMember& m = mem[blockIdx.y];
+  igf_corners_body(nx, ny, nz, m.st, m.F);
+}
+
 // 8-corner difference (Field.f90:420-428) into the octant (nx+1)(ny+1)(nz+1)
-__global__ void k_igf_green(int nx, int ny, int nz, const double* __restrict__ F,
-                            double* __restrict__ Gt) {
+__device__ __forceinline__ void igf_green_body(int nx, int ny, int nz, const double* __restrict__ F,
+                                               double* __restrict__ Gt) {
   const int ax = nx + 2, ay = ny + 2;
   const int gx = nx + 1, gy = ny + 1, gz = nz + 1;
   const long long total = (long long)gx * gy * gz;
@@ -425,6 +489,16 @@ __global__ void k_igf_green(int nx, int ny, int nz, const double* __restrict__ F
   }
 }
 
+__global__ void k_igf_green(int nx, int ny, int nz, const double* __restrict__ F,
+                            double* __restrict__ Gt) {
+  igf_green_body(nx, ny, nz, F, Gt);
+}
+
+__global__ void k_igf_green_group(int nx, int ny, int nz, const PoissonMember* __restrict__ mem) {
+  const PoissonMember& m = mem[blockIdx.y];
+  igf_green_body(nx, ny, nz, m.F, m.Gt);
+}
+
 // DCT-I (transform of the even extension) along one axis of the octant.
 // Lines have n+1 points spaced by `es`; TL lines spaced by `ls` are handled
 // by one block (consecutive inner lines for coalescing), outer lines are
@@ -432,9 +506,10 @@ __global__ void k_igf_green(int nx, int ny, int nz, const double* __restrict__ F
 // compute type CT.  Reads `in` (TI), writes `out` (TO, may alias `in`: each
 // block owns its lines) times `scale`.
 template <typename TI, typename TO, typename CT, int TL>
-__global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long ls, int ninner,
-                       long long os, double scale,
-                       const typename Cplx<CT>::type* __restrict__ tw) {
+__device__ __forceinline__ void dct1_body(const TI* in, TO* out, int logn, long long es,
+                                          long long ls, int ninner, long long os, double scale,
+                                          const typename Cplx<CT>::type* __restrict__ tw,
+                                          const int bx, const int by) {
   typedef typename Cplx<CT>::type C;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* L = reinterpret_cast<C*>(smem_raw);
@@ -443,9 +518,9 @@ __global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long 
   const int lp = line_pitch(n2);
   C* tws = L + (TL / 2) * lp;
   stage_tw(tws, tw, n2);
-  const int l0 = blockIdx.x * TL;
+  const int l0 = bx * TL;
   const int nl = min(TL, ninner - l0);
-  const long long off = (long long)blockIdx.y * os + (long long)l0 * ls;
+  const long long off = (long long)by * os + (long long)l0 * ls;
   const TI* ib = in + off;
   TO* ob = out + off;
   // pair line t with line t + TL/2 (real and imaginary parts)
@@ -468,6 +543,26 @@ __global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long 
   }
 }
 
+template <typename TI, typename TO, typename CT, int TL>
+__global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long ls, int ninner,
+                       long long os, double scale,
+                       const typename Cplx<CT>::type* __restrict__ tw) {
+  dct1_body<TI, TO, CT, TL>(in, out, logn, es, ls, ninner, os, scale, tw, blockIdx.x, blockIdx.y);
+}
+
+// pass `axis` (0: x from the FP64 octant Gt into G-hat, 1: y, 2: z in place
+// on G-hat) for every member of a group: blockIdx.z = member
+template <typename TI, typename TO, typename CT, int TL>
+__global__ void k_dct1_group(int axis, int logn, long long es, long long ls, int ninner,
+                             long long os, double scale, const PoissonMember* __restrict__ mem) {
+  typedef typename Cplx<CT>::type C;
+  const PoissonMember& m = mem[blockIdx.z];
+  const TI* in = axis == 0 ? (const TI*)m.Gt : (const TI*)m.ghat;
+  const C* tw = (const C*)(axis == 0 ? m.twx : axis == 1 ? m.twy : m.twz);
+  dct1_body<TI, TO, CT, TL>(in, (TO*)m.ghat, logn, es, ls, ninner, os, scale, tw, blockIdx.x,
+                            blockIdx.y);
+}
+
 // ---------------------------------------------------------------------
 // kick1_BeamBunch finite differences (BeamBunch.f90:1784-2005), one rank,
 // open BC: centred inside, one-sided on the faces.  Out: {Ex,Ey,Ez,0}.
@@ -476,11 +571,11 @@ __global__ void k_dct1(const TI* in, TO* out, int logn, long long es, long long 
 // per-plane field wake = {dEx, dEy, dEz}[nz] to every node of the plane
 // (kick1wake, BeamBunch.f90:5015-5033) and clears the wake's line sums.
 template <typename T>
-__global__ void k_efield(int nx, int ny, int nz, const T* __restrict__ phi,
-                         const DevState* st, T* __restrict__ E,
-                         unsigned long long* __restrict__ rho,
-                         const double* __restrict__ wake,
-                         unsigned long long* __restrict__ wake_line) {
+__device__ __forceinline__ void efield_body(int nx, int ny, int nz, const T* __restrict__ phi,
+                                            const DevState* st, T* __restrict__ E,
+                                            unsigned long long* __restrict__ rho,
+                                            const double* __restrict__ wake,
+                                            unsigned long long* __restrict__ wake_line) {
   griddep_wait();
   if (wake_line)
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 3 * nz; e += gridDim.x * blockDim.x)
@@ -516,6 +611,21 @@ __global__ void k_efield(int nx, int ny, int nz, const T* __restrict__ phi,
     o[2] = ez;
     o[3] = (T)0;
   }
+}
+
+template <typename T>
+__global__ void k_efield(int nx, int ny, int nz, const T* __restrict__ phi,
+                         const DevState* st, T* __restrict__ E,
+                         unsigned long long* __restrict__ rho,
+                         const double* __restrict__ wake,
+                         unsigned long long* __restrict__ wake_line) {
+  efield_body<T>(nx, ny, nz, phi, st, E, rho, wake, wake_line);
+}
+
+template <typename T>
+__global__ void k_efield_group(int nx, int ny, int nz, const PoissonMember* __restrict__ mem) {
+  const PoissonMember& m = mem[blockIdx.y];
+  efield_body<T>(nx, ny, nz, (const T*)m.phi, m.st, (T*)m.efield, m.rho, nullptr, nullptr);
 }
 
 }  // namespace impz
