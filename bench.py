@@ -238,15 +238,19 @@ def main():
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shapes (fewer launches before the timed run, "
                          "for profiling a chosen launch)")
-    ap.add_argument("--workload", default="fodo", choices=["fodo", "chicane", "scan", "serve"],
-                    help="fodo: the headline 4e6-proton line; chicane: 5e7 electrons, "
-                         "64x64x2048; scan: 256 bunches batched; serve: Poisson job stream")
+    ap.add_argument("--workload", default="fodo",
+                    choices=["fodo", "small", "chicane", "scan", "serve"],
+                    help="fodo: the headline 4e6-proton line; small: 1e5 protons, 32x32x64, "
+                         "160 steps, plain FP64; chicane: 5e7 electrons, 64x64x2048; scan: 256 "
+                         "bunches batched; serve: Poisson job stream")
     ap.add_argument("--jobs", type=int, default=0, help="scan/serve: number of bunches or jobs")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "small":
+        return run_small(args)
     if args.workload == "chicane":
         return run_chicane(args)
     if args.workload == "scan":
@@ -463,7 +467,59 @@ def run_chicane(args):
                        "particles": n, "grid": list(CHICANE_GRID), "steps": K,
                        "form": "fp32-convolution"},
             "clocks": clk, "bunching_10um": {"before": b0, "after": b1},
+            "spectral_gain_10um": b1 / b0 if b0 > 0 else None,
             "live_particles": info["nlocal"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_small(args):
+    """The CPU-runnable configuration: 1e5 protons, 32x32x64,
+    ten FODO periods with four steps per element (160 steps), plain FP64.
+    The GPU run is timed with CUDA events on the bunch's stream after W
+    warm-up runs; the oracle port runs the same 160 steps on all host cores
+    beside it.  A launch-bound size: reported, not the headline."""
+    import torch
+    impz = impz_pkg()
+    orc = oracle_pkg()
+    from impz_b200 import beams
+    torch.cuda.set_device(0)
+    impz.lib().impz_set_device(0)
+    cfg = beams.fodo_1e5()
+    lat = cfg["lattice"]
+    K = impz.count_steps(lat)
+    b = impz.Bunch(cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=impz.FORM_FP64, track_ids=False)
+    for _ in range(max(1, args.warmup // 3)):
+        b.run(lat)
+        b.upload(cfg["pts"], cfg["current"], cfg["refptcl"])
+    stream = torch.cuda.ExternalStream(b.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.run_async(lat)
+    e1.record(stream)
+    b.run_fetch()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    b.close()
+    n = cfg["pts"].shape[0]
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    t0 = time.perf_counter()
+    orc.run(lat, cfg["pts"], cfg["current"], cfg["mass"], cfg["charge"], cfg["freq"],
+            cfg["refptcl"], cfg["grid"])
+    tc = time.perf_counter() - t0
+    orc.set_threads(1)
+    line = {"metric": METRIC, "value": n * K / t, "unit": UNIT, "n_gpus": 1, "steps": K,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+i64",
+            "data": "synthetic (Philox-seeded 6D Gaussian protons)",
+            "config": {"workload": "proton FODO: 100000 protons, grid 32x32x64, 160 steps",
+                       "form": "fp64"},
+            "cpu_baseline": {"value": n * K / tc, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "the same 160 steps, oracle port (%.1f s)" % tc}}
     print(json.dumps(line), flush=True)
     return 0
 

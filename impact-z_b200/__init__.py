@@ -183,11 +183,15 @@ def _dp(a):
 
 
 # ---------------------------------------------------------------------------
-def elem(etype, length, nseg, mapstp=1, vals=(), rf=None):
+def elem(etype, length, nseg, mapstp=1, vals=(), rf=None, grid=None):
     """Build an impz_elem_t.  vals are the deck values v1..v24; rf is an
     optional (z, Ez, Ez', Ez'') on-axis table for linear RF maps, or the
     1-D array of read3_Data's Fourier coefficients for SolRF and TWS (105,
-    106) and, under the Lorentz integrator, for types 101..104."""
+    106) and, under the Lorentz integrator, for types 101..104.  grid is
+    EMfld 110's x-y-z field map as read4_Data reads it: (header, data) with
+    header = (xmin, xmax, NxIntv, ymin, ymax, NyIntv, zmin, zmax, NzIntv) and
+    data the complex (Ex, Ey, Ez, Bx, By, Bz) of every node, x fastest, as an
+    array of shape (nodes, 6) complex or (nodes, 12) real (re, im pairs)."""
     e = ElemStruct()
     e.type = int(etype)
     e.nseg = int(nseg)
@@ -206,6 +210,18 @@ def elem(etype, length, nseg, mapstp=1, vals=(), rf=None):
         e.ndata = len(cols[0])
         e.zdat, e.edat, e.epdat, e.eppdat = [c.ctypes.data_as(_D) for c in cols]
         e._keep = cols
+    if grid is not None:
+        header = np.ascontiguousarray(grid[0], dtype=np.float64)
+        data = np.asarray(grid[1])
+        if np.iscomplexobj(data):
+            data = np.stack([data.real, data.imag], axis=-1).reshape(data.shape[0], 12)
+        data = np.ascontiguousarray(data, dtype=np.float64).reshape(-1)
+        if header.shape != (9,) or data.size % 12:
+            raise ValueError("grid: a 9-value header and 12 values per node")
+        e.ndata = data.size // 12
+        e.zdat = header.ctypes.data_as(_D)
+        e.edat = data.ctypes.data_as(_D)
+        e._keep = [header, data]
     return e
 
 

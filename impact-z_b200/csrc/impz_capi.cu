@@ -440,6 +440,11 @@ struct impz_bunch_s {
   unsigned long long* wk_line = nullptr;
   double* wk_field = nullptr;
   int h_step0 = 0;
+  // field data of Lorentz kicks (EMfld planes) of the run in progress or of
+  // the last per-step kick, grown as needed
+  double* lzd = nullptr;
+  size_t lzd_cap = 0;
+  const double* g_lzd[2] = {nullptr, nullptr};  // the data the step graphs point to
   int run_next = 0;       // next step of the run in progress
   double run_z = 0;       // z and refptcl at the end of the run in progress
   double run_ref[6] = {0};
@@ -534,6 +539,7 @@ AdvanceArgs advance_args(impz_bunch_t b, const StepParams* table, int fixed, int
   // conv1st's frame between a pass and the next step's deposit and kick; the
   // per-step surface keeps the z frame, which the caller may download
   a.tframe = fixed < 0 ? 1 : 0;
+  a.lz_data = b->lzd;
   return a;
 }
 
@@ -726,6 +732,25 @@ int ensure_tables(impz_bunch_t b, int entries, int rows) {
   return IMPZ_OK;
 }
 
+// Copies the Lorentz kicks' field data to the device (bunch stream),
+// growing the buffer when needed.
+int upload_lz_data(impz_bunch_t b, const std::vector<double>& d) {
+  if (d.empty()) return IMPZ_OK;
+  const size_t bytes = d.size() * sizeof(double);
+  if (bytes > b->lzd_cap) {
+    CK(cudaStreamSynchronize(b->stream));
+    if (b->lzd) cudaFree(b->lzd);
+    b->lzd = nullptr;
+    b->lzd_cap = 0;
+    CK(cudaMalloc((void**)&b->lzd, bytes));
+    b->lzd_cap = bytes;
+  }
+  // pageable source: the copy is complete when the call returns
+  CK(cudaMemcpyAsync(b->lzd, d.data(), bytes, cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return IMPZ_OK;
+}
+
 // Pts1 staging: the parity set the next push overwrites, 6 adjacent columns
 double* staging(impz_bunch_t b, long long* cap_particles) {
   const int q = 1 - b->parity;
@@ -814,6 +839,7 @@ void free_bunch(impz_bunch_t b) {
   if (b->arena) cudaFree(b->arena);
   if (b->tables) cudaFree(b->tables);
   if (b->wk_mem) cudaFree(b->wk_mem);
+  if (b->lzd) cudaFree(b->lzd);
   for (cudaEvent_t e : b->ev_pool) cudaEventDestroy(e);
   for (int p = 0; p < 2; p++)
     if (b->gexec[p]) cudaGraphExecDestroy(b->gexec[p]);
@@ -1407,10 +1433,12 @@ int impz_kick2(impz_bunch_t b, const impz_elem_t* e, double zedge, double z, dou
   std::memcpy(ref, b->refptcl, sizeof(ref));
   h[0].lorentz = 1;
   h[0].tau = tau;
+  std::vector<double> lzd;
   if (!lorentz_kick_terms(b->P, *e, zedge, z, tau, b->sp, ref, h[0].lz_kind, h[0].lz_c,
-                          h[0].lz_tg, h[0].lz_ez0))
+                          h[0].lz_tg, h[0].lz_ez0, &lzd))
     return IMPZ_ERR_UNSUPPORTED;
-  int r;
+  int r = upload_lz_data(b, lzd);
+  if (r) return r;
   if (sc) {
     r = kick_field(b, egrid);
     if (r) return r;
@@ -1617,7 +1645,8 @@ static int wake_key(impz_bunch_t b) { return 2 * b->wk_gen + (b->run_wake ? 1 : 
 static int graph_pair(impz_bunch_t b) {
   const int p = b->parity;
   if (b->gexec[p] && (b->g_steps[p] != b->dsteps || b->g_mom[p] != b->mom_out ||
-                      b->g_light[p] != b->run_light || b->g_wake[p] != wake_key(b))) {
+                      b->g_light[p] != b->run_light || b->g_wake[p] != wake_key(b) ||
+                      b->g_lzd[p] != b->lzd)) {
     cudaGraphExecDestroy(b->gexec[p]);
     b->gexec[p] = nullptr;
   }
@@ -1641,6 +1670,7 @@ static int graph_pair(impz_bunch_t b) {
     b->g_mom[p] = b->mom_out;
     b->g_light[p] = b->run_light;
     b->g_wake[p] = wake_key(b);
+    b->g_lzd[p] = b->lzd;
     b->parity = p;  // capture did not execute anything
   }
   g_launches += 2 * (12 + (b->run_wake ? 2 : 0));
@@ -1668,6 +1698,7 @@ static int run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   const int K = L.nsteps;
   b->run_light = table_is_light(L.steps);
   if ((r = ensure_tables(b, K + 2, K + 1))) return r;
+  if ((r = upload_lz_data(b, L.lz_data))) return r;
   CK(cudaMemcpyAsync(b->dsteps, L.steps.data(), (K + 2) * sizeof(StepParams),
                      cudaMemcpyHostToDevice, b->stream));
   // the device step counter drives every launch: 0 is the prologue (initial

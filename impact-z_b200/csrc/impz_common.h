@@ -66,6 +66,12 @@ struct MapOp {
 //                B += (-bz'/2 X + bz''' X r^2/16, same with Y, bz - bz'' r^2/4),
 //                or TWS 106's second wave (ez1, ez1', f1, f1', theta2) at
 //                phi + theta2)
+//   LZ_EMFLD     EMfld 110 with discrete x-y-z data (scatter2, FlagDisc 1,
+//                FlagCart 2): c = (escale, ww, theta0, xmin, hx, 1/hx, ymin,
+//                hy, 1/hy, NxIntvRfg, NyIntvRfg, offset of the step's complex
+//                field plane in AdvanceArgs::lz_data); nine-point quadratic
+//                interpolation in x, y of each component times escale
+//                e^{i(ww T + theta0)}, real part
 //   LZ_MULT      multipole 5 (getfld_Multipole, MAD notation), c = (G, id):
 //                sextupole (id 2) B = (G X Y, G (X^2 - Y^2)/2, 0), octupole
 //                (3) G (3 X^2 Y - Y^3)/6, G (X^3 - 3 X Y^2)/6, decapole (4)
@@ -80,7 +86,8 @@ enum LzKind {
   LZ_RF = 6,
   LZ_SOLRF = 7,
   LZ_TWS = 8,
-  LZ_MULT = 9
+  LZ_MULT = 9,
+  LZ_EMFLD = 10
 };
 
 struct MapProgram {
@@ -183,6 +190,7 @@ struct AdvanceArgs {
   int tframe;               // 1: conv1st's frame between passes (the whole-lattice runner):
                             //    a kick reads it, a pass with range_next writes it
   const double* wake_raw;   // per-plane wake {Ex,Ey,Ez}[nz] of a Lorentz step (kick2wake), or null
+  const double* lz_data;    // field data of the Lorentz kicks (LZ_EMFLD planes), or null
 };
 
 struct DepositArgs {

@@ -1087,18 +1087,119 @@ void rfw_field(const Phys& P, const impz_elem_t& e, double zedge, double z, doub
   if (tws) c[12] = e.val[10] * pi / 180;
 }
 
+// EMfld 110 as the Lorentz integrator carries it: discrete data (Param(13)
+// = 1) on read4_Data's x-y-z grid (Param(14) = 2).  zdat: the three header
+// records (xmin, xmax, NxIntvRfg, ymin, ymax, NyIntvRfg, zmin, zmax,
+// NzIntvRfg), edat: complex Ex, Ey, Ez, Bx, By, Bz per node (twelve
+// doubles, x fastest, then y, then z), ndata: the node count
+// (Data.f90:415-554).  The reference's other forms of the element read
+// data its driver never loads for it under Flagmap=2 (read2_Data's r-z
+// tables, read3_Data's coefficients: AccSimulator.f90:836-846).
+bool emfld_ok(const impz_elem_t& e) {
+  if (e.type != 110 || !e.zdat || !e.edat) return false;
+  if ((int)(0.1 + e.val[11]) != 1 || (int)(0.1 + e.val[12]) != 2) return false;
+  const int nx = (int)(e.zdat[2] + 0.1), ny = (int)(e.zdat[5] + 0.1), nz = (int)(e.zdat[8] + 0.1);
+  return nx >= 2 && ny >= 2 && nz >= 2 && e.ndata == (nx + 1) * (ny + 1) * (nz + 1);
+}
+
+// getfld6xyz_EMfld (EMfld.f90:854-916): the field plane at zz = z - zedge,
+// linear between the two end planes of the grid, quadratic over three
+// planes elsewhere; appended to `out` (twelve doubles per node, x fastest)
+void emfld_plane(const impz_elem_t& e, double zz, std::vector<double>& out) {
+  const double* hd = e.zdat;
+  const int nxi = (int)(hd[2] + 0.1), nyi = (int)(hd[5] + 0.1), nzi = (int)(hd[8] + 0.1);
+  const size_t nxp = nxi + 1, nyp = nyi + 1;
+  const double hz = (hd[7] - hd[6]) / nzi;
+  int iz = (int)(zz / hz + 1);
+  if (iz == nzi + 1) iz = iz - 1;
+  auto g = [&](int c, size_t i, size_t j, int k) {
+    return e.edat[12 * (i + nxp * (j + nyp * (size_t)(k - 1))) + c];
+  };
+  const bool lin = iz == 1 || iz == nzi;
+  const int iz1 = iz + 1;
+  int iz2 = iz;
+  double w0 = 0, w1 = 0, w2 = 0;
+  if (lin) {
+    w0 = (iz * hz - zz) / hz;
+    w1 = 1.0 - w0;
+  } else {
+    const double ab = (zz - (iz - 1) * hz) / hz;
+    if (ab <= 0.5) {
+      iz2 = iz - 1;
+      w0 = 0.75 - ab * ab;
+      w1 = (0.5 + ab) * (0.5 + ab) / 2;
+      w2 = (0.5 - ab) * (0.5 - ab) / 2;
+    } else {
+      iz2 = iz + 2;
+      w0 = (1.5 - ab) * (1.5 - ab) / 2;
+      w1 = 0.75 - (1 - ab) * (1 - ab);
+      w2 = (ab - 0.5) * (ab - 0.5) / 2;
+    }
+  }
+  for (size_t j = 0; j < nyp; j++)
+    for (size_t i = 0; i < nxp; i++)
+      for (int c = 0; c < 12; c++)
+        out.push_back(lin ? g(c, i, j, iz) * w0 + g(c, i, j, iz1) * w1
+                          : g(c, i, j, iz) * w0 + g(c, i, j, iz1) * w1 + g(c, i, j, iz2) * w2);
+}
+
 // The external field of element e for a Lorentz kick at z (LzKind):
 // getfld_Quadrupole (Quadrupole.f90:369-402), getfld_ConstFoc
 // (ConstFoc.f90:297-322), getfld_Sol (Sol.f90:391-435) and no field for a
 // drift.  ez0 is its Ez on axis at time tg.  Returns false for an element
 // the Lorentz integrator does not carry here.
 bool lorentz_field(const Phys& P, const impz_elem_t& e, double zedge, double z, double tg,
-                   int& kind, double c[16], double& ez0) {
+                   int& kind, double c[16], double& ez0, std::vector<double>* data) {
   kind = LZ_NONE;
   for (int i = 0; i < 16; i++) c[i] = 0.0;
   ez0 = 0.0;
   const double zz = z - zedge;
   switch (e.type) {
+    case 110: {
+      if (!emfld_ok(e)) return false;
+      // scatter2 with FlagDisc = 1, FlagCart = 2 (BeamBunch.f90:2604-2632,
+      // 2794-2880): c = (escale, ww, theta0, xmin, hx, 1/hx, ymin, hy, 1/hy,
+      // NxIntvRfg, NyIntvRfg, offset of the plane in the run's field data)
+      kind = LZ_EMFLD;
+      const double* hd = e.zdat;
+      c[0] = e.val[0];
+      c[1] = e.val[1] / P.Scfreq;
+      c[2] = e.val[2] * (double)std::asin(1.0f) / 90;
+      c[3] = hd[0];
+      c[4] = (hd[1] - hd[0]) / (int)(hd[2] + 0.1);
+      c[5] = 1.0 / c[4];
+      c[6] = hd[3];
+      c[7] = (hd[4] - hd[3]) / (int)(hd[5] + 0.1);
+      c[8] = 1.0 / c[7];
+      c[9] = (int)(hd[2] + 0.1);
+      c[10] = (int)(hd[5] + 0.1);
+      std::vector<double> local;
+      std::vector<double>& pl = data ? *data : local;
+      c[11] = (double)pl.size();
+      emfld_plane(e, zz, pl);
+      // ez0: bilinear at x = y = 0 in the plane's Ez, times escale
+      // e^{i(ww tg + theta0)}, real part
+      const size_t nxp = (size_t)c[9] + 1;
+      const double* q = pl.data() + (size_t)c[11];
+      const int ix = (int)((0.0 - c[3]) / c[4] + 1), iy = (int)((0.0 - c[6]) / c[7] + 1);
+      const double efx = (c[3] - 0.0 + ix * c[4]) / c[4];
+      const double efy = (c[6] - 0.0 + iy * c[7]) / c[7];
+      auto ez = [&](int i, int j, int part) {
+        return q[12 * ((size_t)(i - 1) + nxp * (size_t)(j - 1)) + 4 + part];
+      };
+      double sr = 0.0, si = 0.0;
+      const int ii[4] = {ix, ix, ix + 1, ix + 1}, jj[4] = {iy, iy + 1, iy, iy + 1};
+      const double wa[4] = {efx, efx, 1.0 - efx, 1.0 - efx};
+      const double wb[4] = {efy, 1.0 - efy, efy, 1.0 - efy};
+      if (ix < 1 || ix > (int)c[9] || iy < 1 || iy > (int)c[10]) return false;
+      for (int k = 0; k < 4; k++) {
+        sr = k ? sr + ez(ii[k], jj[k], 0) * wa[k] * wb[k] : ez(ii[k], jj[k], 0) * wa[k] * wb[k];
+        si = k ? si + ez(ii[k], jj[k], 1) * wa[k] * wb[k] : ez(ii[k], jj[k], 1) * wa[k] * wb[k];
+      }
+      const double ph = c[1] * tg + c[2];
+      ez0 = sr * (c[0] * std::cos(ph)) - si * (c[0] * std::sin(ph));
+      return true;
+    }
     case 0:
       return true;
     case 1:
@@ -1198,9 +1299,9 @@ int drift2_op(const Phys& P, double tau, double refptcl[6], MapProgram& prog) {
 
 bool lorentz_kick_terms(const Phys& P, const impz_elem_t& e, double zedge, double z, double tau,
                         const Species& sp, double refptcl[6], int& kind, double c[16],
-                        double& tg, double& ez0) {
+                        double& tg, double& ez0, std::vector<double>* data) {
   tg = refptcl[4];
-  if (!lorentz_field(P, e, zedge, z, tg, kind, c, ez0)) return false;
+  if (!lorentz_field(P, e, zedge, z, tg, kind, c, ez0, data)) return false;
   const double gam = -refptcl[5] + tau * (sp.charge / sp.mass) * ez0;
   refptcl[5] = -gam;
   return true;
@@ -1224,6 +1325,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     double ref[6];
   };
   std::vector<Step> steps;
+  std::vector<double> lz_data;
   MapProgram pending;
   std::memset(&pending, 0, sizeof(pending));
   double z = *zio;
@@ -1236,6 +1338,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     if (e.nseg < 1) return IMPZ_ERR_ARG;
     const int bnseg = e.nseg, bitype = e.type;
     double piperad = pipe_radius(e), piperad2 = piperad;
+    if (bitype == 110) piperad2 = e.val[5];  // EMfld: Param(7) (BeamLineElem.f90:538-540)
     // the Lorentz integrator covers drifts, quadrupoles, constant focusing,
     // solenoids, multipoles and the RF cavities 101..106, whose fields
     // kick2 applies (lorentz_field)
@@ -1243,7 +1346,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
     if (lorentz) {
       int kind;
       double c[16], ez0;
-      if (!lorentz_field(P, e, z, z, 0.0, kind, c, ez0)) return IMPZ_ERR_UNSUPPORTED;
+      if (!lorentz_field(P, e, z, z, 0.0, kind, c, ez0, nullptr)) return IMPZ_ERR_UNSUPPORTED;
     }
     // the wake switch of each element (AccSimulator.f90:865-875)
     if (bitype == 105 || bitype == 106) {
@@ -1306,7 +1409,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
             // kick's z and tg = refptcl(5); gamma0 += tau qmcc Ez0 after it
             s.lorentz = 1;
             lorentz_kick_terms(P, e, zedge, z, tau2, sp, refptcl, s.lz_kind, s.lz_c, s.lz_tg,
-                               s.lz_ez0);
+                               s.lz_ez0, &lz_data);
           }
         }
         if (lorentz) {
@@ -1334,6 +1437,7 @@ int compile_lattice(const Phys& P, const impz_elem_t* elems, int nelem, double b
   const int K = (int)steps.size();
   out.nsteps = K;
   out.has_wake = false;
+  out.lz_data.swap(lz_data);
   out.steps.assign(K + 2, StepParams());
   for (auto& st : out.steps) std::memset(&st, 0, sizeof(st));
   out.zrec.assign(K + 1, 0.0);

@@ -60,9 +60,11 @@ int half_map_ops(const Phys& P, const impz_elem_t& e, double zedge, double z, do
 // gamma0 moved by tau qmcc Ez0 (BeamBunch.f90:2187-2508); false for an
 // element outside the integrator.
 int drift2_op(const Phys& P, double tau, double refptcl[6], MapProgram& prog);
+// `data`, when given, receives the per-step field data of the kick (EMfld
+// 110: the plane at z), whose offset the coefficients c carry.
 bool lorentz_kick_terms(const Phys& P, const impz_elem_t& e, double zedge, double z, double tau,
                         const Species& sp, double refptcl[6], int& kind, double c[16],
-                        double& tg, double& ez0);
+                        double& tg, double& ez0, std::vector<double>* data = nullptr);
 // Bend entry (refptcl(5) update + Fpol op), Sector op, Bpol op.
 int bend_entry_ops(const Phys& P, const impz_elem_t& e, double refptcl[6], const Species& sp,
                    BendState& bs, MapProgram& prog);
@@ -76,6 +78,7 @@ struct CompiledLattice {
   std::vector<double> refrec;     // refptcl of each record, 6 per record
   int nsteps;
   bool has_wake;                  // some step kicks with a wake (read-in, analytic or CSR)
+  std::vector<double> lz_data;    // field data of Lorentz kicks (EMfld planes), in device order
 };
 // The state of run_AccSimulator's element loop that decides where wakes
 // act: the bend bookkeeping of CSR (AccSimulator.f90:638-740, 1032-1051,

@@ -688,12 +688,84 @@ __device__ __forceinline__ double moment_tail(double acc1, int lane) {
 // getfld_ConstFoc, ConstFoc.f90:297-322; getfldpts_DTL, DTL.f90:858-958,
 // and the CCDTL, CCL, SC forms; getfld_SolRF, getfld_TWS; getfld_Multipole;
 // LzKind), in the reference's expression forms; e = E, b = B.
+// scatter2's quadratic weights along one axis of EMfld's x-y grid
+// (BeamBunch.f90:2804-2860): node i, i+1 and a third node i2, one-sided at
+// the first and the last interval
+__device__ __forceinline__ void emfld_weights(int i, double ab, int nint, int& i2, double w[3]) {
+  if (i == 1 && ab <= 0.5) {
+    i2 = i;
+    w[0] = 0.75 - ab * ab;
+    w[1] = (0.5 + ab) * (0.5 + ab) / 2;
+    w[2] = 0.0;
+  } else if (i == nint && ab > 0.5) {
+    i2 = i;
+    w[0] = (1.5 - ab) * (1.5 - ab) / 2;
+    w[1] = 0.75 - (1 - ab) * (1 - ab);
+    w[2] = 0.0;
+  } else if (ab <= 0.5) {
+    i2 = i - 1;
+    w[0] = 0.75 - ab * ab;
+    w[1] = (0.5 + ab) * (0.5 + ab) / 2;
+    w[2] = (0.5 - ab) * (0.5 - ab) / 2;
+  } else {
+    i2 = i + 2;
+    w[0] = (1.5 - ab) * (1.5 - ab) / 2;
+    w[1] = 0.75 - (1 - ab) * (1 - ab);
+    w[2] = (ab - 0.5) * (ab - 0.5) / 2;
+  }
+}
+
 __device__ __forceinline__ void lz_field(int kind, const double* __restrict__ c, double X,
-                                         double Y, double T, const Consts& k, double& ex,
+                                         double Y, double T, const Consts& k,
+                                         const double* __restrict__ data, double& ex,
                                          double& ey, double& ez, double& bx, double& by,
                                          double& bz) {
   ex = 0.0; ey = 0.0; ez = 0.0; bx = 0.0; by = 0.0; bz = 0.0;
-  if (kind == LZ_RF) {
+  if (kind == LZ_EMFLD) {
+    // scatter2, EMfld with discrete x-y-z data (BeamBunch.f90:2794-2880):
+    // nine-point quadratic interpolation of the step's complex field plane
+    // (data + c[11], twelve doubles per node, x fastest), times escale
+    // e^{i(ww T + theta0)}, real part.  Node indices are kept inside the
+    // grid (the reference reads outside its arrays there).
+    const int nxi = (int)c[9], nyi = (int)c[10];
+    int ix = (int)((X - c[3]) * c[5] + 1), iy = (int)((Y - c[6]) * c[8] + 1);
+    const double ab = (X - c[3] - (ix - 1) * c[4]) * c[5];
+    const double cd = (Y - c[6] - (iy - 1) * c[7]) * c[8];
+    int ix2, iy2;
+    double wx[3], wy[3];
+    emfld_weights(ix, ab, nxi, ix2, wx);
+    emfld_weights(iy, cd, nyi, iy2, wy);
+    int ii[3] = {ix, ix + 1, ix2}, jj[3] = {iy, iy + 1, iy2};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      ii[a] = min(max(ii[a], 1), nxi + 1);
+      jj[a] = min(max(jj[a], 1), nyi + 1);
+    }
+    double sn, cs;
+    sincos(c[1] * T + c[2], &sn, &cs);
+    const double tr = c[0] * cs, ti = c[0] * sn;
+    const double* q = data + (long long)c[11];
+    double f[6];
+#pragma unroll
+    for (int comp = 0; comp < 6; comp++) {
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          const double* v = q + 12 * ((ii[a] - 1) + (nxi + 1) * (jj[b] - 1)) + 2 * comp;
+          if (a == 0 && b == 0) {
+            sr = v[0] * wx[a] * wy[b];
+            si = v[1] * wx[a] * wy[b];
+          } else {
+            sr = sr + v[0] * wx[a] * wy[b];
+            si = si + v[1] * wx[a] * wy[b];
+          }
+        }
+      f[comp] = sr * tr - si * ti;
+    }
+    ex = f[0]; ey = f[1]; ez = f[2]; bx = f[3]; by = f[4]; bz = f[5];
+  } else if (kind == LZ_RF) {
     // getfldpts_DTL (DTL.f90:932-956) and its CCDTL, CCL, SC forms
     double sn, cs;
     sincos(c[5] * T + c[6], &sn, &cs);
@@ -776,7 +848,7 @@ __device__ __forceinline__ void lz_field(int kind, const double* __restrict__ c,
 __device__ __forceinline__ void lorentz_kick(Particle& p, double exn, double eyn, double ezn,
                                              double gam, const StepParams* __restrict__ sp,
                                              const Consts& k, double wx, double wy,
-                                             double wz) {
+                                             double wz, const double* __restrict__ lz_data) {
   const double xl = k.Scxl, Clight = k.Clight;
   const double tau = sp->tau;
   const double tmpscale = Clight * Clight * 1.00000001168609742e-07;
@@ -785,8 +857,8 @@ __device__ __forceinline__ void lorentz_kick(Particle& p, double exn, double eyn
   const double ez0 = sp->lz_ez0;
   const double tmpgamma0 = gam + 0.5 * tau * qmcc * ez0;
   double e1, e2, e3, ext4, ext5, ext6;
-  lz_field(sp->lz_kind, sp->lz_c, p.x * xl, p.y * xl, p.ph + sp->lz_tg, k, e1, e2, e3, ext4,
-           ext5, ext6);
+  lz_field(sp->lz_kind, sp->lz_c, p.x * xl, p.y * xl, p.ph + sp->lz_tg, k, lz_data, e1, e2, e3,
+           ext4, ext5, ext6);
   const double ex = tmpscale * exn + e1 + wx;
   const double ey = tmpscale * eyn + e2 + wy;
   const double ez = tmpscale * ezn + e3 + wz;
@@ -972,7 +1044,7 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
               wy = w[nz] * cg.ef + w[nz + 1] * (1.0 - cg.ef);
               wz = w[2 * nz] * cg.ef + w[2 * nz + 1] * (1.0 - cg.ef);
             }
-            lorentz_kick(p[u], exn, eyn, ezn, gam, sp, a.k, wx, wy, wz);
+            lorentz_kick(p[u], exn, eyn, ezn, gam, sp, a.k, wx, wy, wz, a.lz_data);
           } else {
             p[u].px = p[u].px + txy * exn;
             p[u].py = p[u].py + txy * eyn;
@@ -984,7 +1056,7 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
       // the element's field alone, on the stored coordinates
       // (BeamBunch.f90:3075-3531)
       if (!LIGHT && keep[u] && !kick && post && sp->lorentz)
-        lorentz_kick(p[u], 0.0, 0.0, 0.0, gam, sp, a.k, 0.0, 0.0, 0.0);
+        lorentz_kick(p[u], 0.0, 0.0, 0.0, gam, sp, a.k, 0.0, 0.0, 0.0, a.lz_data);
       if (keep[u] && post) apply_program<LIGHT>(p[u], progs[0]);
       if (keep[u]) {
         c[u].x = p[u].x; c[u].px = p[u].px; c[u].y = p[u].y;

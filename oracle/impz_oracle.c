@@ -1498,6 +1498,12 @@ typedef struct {
    * wave at theta0 + theta2, or SolRF's solenoid (bscale times the sums) */
   int inside, on1, on2;
   double xlrep, tsc, w1[4], w2[4], sol[4], theta2;
+  /* EMfld 110 with discrete x-y-z data (Param(13) = 1, Param(14) = 2):
+   * getfld6xyz_EMfld's field plane at z (complex Ex, Ey, Ez, Bx, By, Bz per
+   * node, x fastest), the grid and the RF constants */
+  double *plane;
+  int enx, eny;
+  double exmin, ehx, ehxi, eymin, ehy, ehyi, escale, eww, etheta0;
 } lorentz_kick;
 
 static void kick_common(double *pts, int n, const double *phi, const int mesh[3],
@@ -1640,6 +1646,160 @@ static void lz_rfw_axis(lorentz_kick *lz) {
   }
 }
 
+/* read4_Data's grid of element 110 (Data.f90:415-554): e->zdat holds the
+ * three header records (xmin, xmax, NxIntvRfg; ymin, ymax, NyIntvRfg; zmin,
+ * zmax, NzIntvRfg) as nine doubles, e->edat the complex Ex, Ey, Ez, Bx, By,
+ * Bz of each grid node (re, im pairs, twelve doubles per node) in file
+ * order (x fastest, then y, then z), e->ndata the node count.
+ * getfld6xyz_EMfld (EMfld.f90:854-916): the plane at z, linear between the
+ * first two and the last two planes, quadratic (three planes) elsewhere. */
+#define EMG(c, i, j, k) e->edat[12 * ((size_t)((i)-1) + (size_t)(nxp) * \
+                                      ((size_t)((j)-1) + (size_t)(nyp) * ((size_t)((k)-1)))) + (c)]
+static void lz_emfld_plane(lorentz_kick *lz) {
+  const orc_elem *e = lz->e;
+  const double *hd = e->zdat;
+  const int nxi = (int)(hd[2] + 0.1), nyi = (int)(hd[5] + 0.1), nzi = (int)(hd[8] + 0.1);
+  const int nxp = nxi + 1, nyp = nyi + 1;
+  lz->enx = nxi;
+  lz->eny = nyi;
+  lz->exmin = hd[0];
+  lz->ehx = (hd[1] - hd[0]) / nxi;
+  lz->ehxi = 1.0 / lz->ehx;
+  lz->eymin = hd[3];
+  lz->ehy = (hd[4] - hd[3]) / nyi;
+  lz->ehyi = 1.0 / lz->ehy;
+  lz->escale = e->val[0];
+  lz->eww = e->val[1] / PC.Scfreq;
+  lz->etheta0 = e->val[2] * (double)asinf(1.0f) / 90;
+  lz->plane = (double *)malloc((size_t)12 * nxp * nyp * sizeof(double));
+  const double hz = (hd[7] - hd[6]) / nzi;
+  const double zz = lz->z - lz->zedge;
+  int iz = (int)(zz / hz + 1);
+  if (iz == nzi + 1) iz = iz - 1;
+  for (int j = 1; j <= nyp; j++)
+    for (int i = 1; i <= nxp; i++)
+      for (int c = 0; c < 12; c++) {
+        double v;
+        if (iz == 1 || iz == nzi) {
+          const int iz1 = iz + 1;
+          const double ef = (iz * hz - zz) / hz;
+          v = EMG(c, i, j, iz) * ef + EMG(c, i, j, iz1) * (1.0 - ef);
+        } else {
+          const double ab = (zz - (iz - 1) * hz) / hz;
+          const int iz1 = iz + 1;
+          int iz2;
+          double wix, wix1, wix2;
+          if (ab <= 0.5) {
+            iz2 = iz - 1;
+            wix = 0.75 - ab * ab;
+            wix1 = (0.5 + ab) * (0.5 + ab) / 2;
+            wix2 = (0.5 - ab) * (0.5 - ab) / 2;
+          } else {
+            iz2 = iz + 2;
+            wix = (1.5 - ab) * (1.5 - ab) / 2;
+            wix1 = 0.75 - (1 - ab) * (1 - ab);
+            wix2 = (ab - 0.5) * (ab - 0.5) / 2;
+          }
+          v = EMG(c, i, j, iz) * wix + EMG(c, i, j, iz1) * wix1 + EMG(c, i, j, iz2) * wix2;
+        }
+        lz->plane[12 * ((size_t)(i - 1) + (size_t)nxp * (j - 1)) + c] = v;
+      }
+}
+#undef EMG
+
+/* one complex field component c (0..5) of the plane at node (i, j), 1-based */
+static void emp(const lorentz_kick *lz, int c, int i, int j, double *re, double *im) {
+  const double *q = lz->plane + 12 * ((size_t)(i - 1) + (size_t)(lz->enx + 1) * (j - 1));
+  *re = q[2 * c];
+  *im = q[2 * c + 1];
+}
+
+/* scatter2's quadratic weights along one axis of the x-y grid
+ * (BeamBunch.f90:2804-2860): node i, its neighbour i1 = i+1 and a third
+ * node i2, with the one-sided forms at the first and the last interval */
+static void emfld_w(int i, double ab, int nint, int *i2, double w[3]) {
+  if (i == 1 && ab <= 0.5) {
+    *i2 = i;
+    w[0] = 0.75 - ab * ab;
+    w[1] = (0.5 + ab) * (0.5 + ab) / 2;
+    w[2] = 0.0;
+  } else if (i == nint && ab > 0.5) {
+    *i2 = i;
+    w[0] = (1.5 - ab) * (1.5 - ab) / 2;
+    w[1] = 0.75 - (1 - ab) * (1 - ab);
+    w[2] = 0.0;
+  } else if (ab <= 0.5) {
+    *i2 = i - 1;
+    w[0] = 0.75 - ab * ab;
+    w[1] = (0.5 + ab) * (0.5 + ab) / 2;
+    w[2] = (0.5 - ab) * (0.5 - ab) / 2;
+  } else {
+    *i2 = i + 2;
+    w[0] = (1.5 - ab) * (1.5 - ab) / 2;
+    w[1] = 0.75 - (1 - ab) * (1 - ab);
+    w[2] = (ab - 0.5) * (ab - 0.5) / 2;
+  }
+}
+
+/* the field of element 110 at (x, y) [m] and time tt (scatter2 with
+ * FlagDisc = 1, FlagCart = 2, BeamBunch.f90:2794-2880): nine-point
+ * quadratic interpolation of the complex plane, times escale e^{i(ww tt +
+ * theta0)}, real part */
+static void lz_emfld(const lorentz_kick *lz, const double pos[4], double f[6]) {
+  const double xx = pos[0], yy = pos[1];
+  const int ix = (int)((xx - lz->exmin) * lz->ehxi + 1), ix1 = ix + 1;
+  const int iy = (int)((yy - lz->eymin) * lz->ehyi + 1), iy1 = iy + 1;
+  const double ab = (xx - lz->exmin - (ix - 1) * lz->ehx) * lz->ehxi;
+  const double cd = (yy - lz->eymin - (iy - 1) * lz->ehy) * lz->ehyi;
+  int ix2, iy2;
+  double wx[3], wy[3];
+  emfld_w(ix, ab, lz->enx, &ix2, wx);
+  emfld_w(iy, cd, lz->eny, &iy2, wy);
+  const double ph = lz->eww * pos[3] + lz->etheta0;
+  const double tr = lz->escale * cos(ph), ti = lz->escale * sin(ph);
+  const int ii[3] = {ix, ix1, ix2}, jj[3] = {iy, iy1, iy2};
+  for (int c = 0; c < 6; c++) {
+    double sr = 0.0, si = 0.0;
+    for (int a = 0; a < 3; a++)
+      for (int b = 0; b < 3; b++) {
+        double vr, vi;
+        emp(lz, c, ii[a], jj[b], &vr, &vi);
+        if (a == 0 && b == 0) {
+          sr = vr * wx[a] * wy[b];
+          si = vi * wx[a] * wy[b];
+        } else {
+          sr = sr + vr * wx[a] * wy[b];
+          si = si + vi * wx[a] * wy[b];
+        }
+      }
+    f[c] = sr * tr - si * ti;
+  }
+}
+
+/* scatter2's ez0 of element 110 (BeamBunch.f90:2612-2632): bilinear in
+ * the plane at x = y = 0 times escale e^{i(ww tg + theta0)}, real part */
+static double lz_emfld_ez0(const lorentz_kick *lz) {
+  const double xx = 0.0, yy = 0.0;
+  const int ix = (int)((xx - lz->exmin) / lz->ehx + 1), ix1 = ix + 1;
+  const double efx = (lz->exmin - xx + ix * lz->ehx) / lz->ehx;
+  const int iy = (int)((yy - lz->eymin) / lz->ehy + 1), iy1 = iy + 1;
+  const double efy = (lz->eymin - yy + iy * lz->ehy) / lz->ehy;
+  const double ph = lz->eww * lz->tg + lz->etheta0;
+  const double tr = lz->escale * cos(ph), ti = lz->escale * sin(ph);
+  double r[4], im[4];
+  emp(lz, 2, ix, iy, &r[0], &im[0]);
+  emp(lz, 2, ix, iy1, &r[1], &im[1]);
+  emp(lz, 2, ix1, iy, &r[2], &im[2]);
+  emp(lz, 2, ix1, iy1, &r[3], &im[3]);
+  const double wa[4] = {efx, efx, 1.0 - efx, 1.0 - efx}, wb[4] = {efy, 1.0 - efy, efy, 1.0 - efy};
+  double sr = 0.0, si = 0.0;
+  for (int k = 0; k < 4; k++) {
+    sr = k ? sr + r[k] * wa[k] * wb[k] : r[k] * wa[k] * wb[k];
+    si = k ? si + im[k] * wa[k] * wb[k] : im[k] * wa[k] * wb[k];
+  }
+  return sr * tr - si * ti;
+}
+
 static lorentz_kick lz_make(const orc_elem *e, double zedge, double z, double tg, double qmi) {
   lorentz_kick lz;
   memset(&lz, 0, sizeof(lz));
@@ -1651,6 +1811,7 @@ static lorentz_kick lz_make(const orc_elem *e, double zedge, double z, double tg
   lz.wraw = NULL;
   if (e->type >= 101 && e->type <= 104) lz_rf_axis(&lz);
   if (e->type == 105 || e->type == 106) lz_rfw_axis(&lz);
+  if (e->type == 110) lz_emfld_plane(&lz);
   return lz;
 }
 
@@ -1701,7 +1862,9 @@ static void quad_ana2(const lorentz_kick *lz, double zz, double *bgrad, double *
 static void lz_getfld(const lorentz_kick *lz, const double pos[4], double f[6]) {
   for (int i = 0; i < 6; i++) f[i] = 0.0;
   const double zz = pos[2] - lz->zedge;
-  if (lz->e->type == 1) {
+  if (lz->e->type == 110) {
+    lz_emfld(lz, pos, f);
+  } else if (lz->e->type == 1) {
     double bgrad = lz->e->val[0], bgradp = 0.0, bgradpp = 0.0;
     if (lz->e->val[1] > 1.0e-5) quad_ana2(lz, zz, &bgrad, &bgradp, &bgradpp);
     if (lz->e->val[1] > 0.0) {
@@ -1823,6 +1986,7 @@ static void lz_getfld(const lorentz_kick *lz, const double pos[4], double f[6]) 
 
 /* scatter2's ez0: the element's Ez on axis at the reference time */
 static double lz_ez0(const lorentz_kick *lz) {
+  if (lz->e->type == 110) return lz_emfld_ez0(lz);
   const double pos[4] = {0.0, 0.0, lz->z, lz->tg};
   double f[6];
   lz_getfld(lz, pos, f);
@@ -1892,7 +2056,9 @@ double orc_kick2(double *pts, int n, const double *phi, const int mesh[3], const
   lorentz_kick lz = lz_make(e, zedge, z, tg, qmi);
   lz.wraw = wraw;
   kick_common(pts, n, phi, mesh, range, msize, gam, curr, tau, mass, chrg, NULL, NULL, &lz);
-  return gam + tau * (chrg / mass) * lz_ez0(&lz);
+  const double g = gam + tau * (chrg / mass) * lz_ez0(&lz);
+  free(lz.plane);
+  return g;
 }
 
 /* kick2_BeamBunch without current: scatter20 (BeamBunch.f90:3075-3531),
@@ -1904,6 +2070,7 @@ double orc_lorentz_nosc(double *pts, int n, double gam, double tau, double mass,
   const double ez0 = lz_ez0(&lz);
   for (int q = 0; q < n; q++)
     lorentz_update(&P(q, 0), 0.0, 0.0, 0.0, gam, tau, mass, chrg, ez0, &lz, 0.0, 0.0, 0.0);
+  free(lz.plane);
   return gam + tau * (chrg / mass) * ez0;
 }
 
@@ -2673,6 +2840,18 @@ void orc_laser_heater(double *pts, int n, int npt, double rsig, double wavelengt
 }
 
 /* ------------------------------------------------------------------ */
+/* element 110 as the Lorentz integrator carries it: discrete data
+ * (Param(13) = 1) on the x-y-z grid (Param(14) = 2) of read4_Data.  Its
+ * other forms read data the driver never loads for it under Flagmap=2
+ * (the r-z tables of read2_Data and the Fourier coefficients of
+ * read3_Data, AccSimulator.f90:836-846). */
+static int emfld_ok(const orc_elem *e) {
+  if (e->type != 110 || !e->zdat || !e->edat) return 0;
+  if ((int)(0.1 + e->val[11]) != 1 || (int)(0.1 + e->val[12]) != 2) return 0;
+  const int nx = (int)(e->zdat[2] + 0.1), ny = (int)(e->zdat[5] + 0.1), nz = (int)(e->zdat[8] + 0.1);
+  return nx >= 2 && ny >= 2 && nz >= 2 && e->ndata == (nx + 1) * (ny + 1) * (nz + 1);
+}
+
 static double pipe_radius(const orc_elem *e) {
   /* getradius_BeamLineElem (BeamLineElem.f90:500-552): Param index per type */
   switch (e->type) {
@@ -2716,13 +2895,14 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
     const double blength = e->length;
     const int bnseg = e->nseg, bitype = e->type;
     double piperad = pipe_radius(e), piperad2 = piperad;
+    if (bitype == 110) piperad2 = e->val[5]; /* EMfld: Param(7) (BeamLineElem.f90:538-540) */
     if (bitype < 0) { free(rho); return -3; }
     const int lorentz = beam->flagmap == 2;
     /* Lorentz integrator: drifts, quadrupoles (not 0 < Param(3) <= 1e-5,
      * where getfld_Quadrupole reads G', G'' it never set), constant
      * focusing, solenoids and the RF cavities 101..106 over Fourier
      * coefficients */
-    if (lorentz && !(bitype == 0 || bitype == 2 || bitype == 3 ||
+    if (lorentz && !(bitype == 0 || bitype == 2 || bitype == 3 || emfld_ok(e) ||
                      (bitype == 1 && (e->val[1] <= 0.0 || e->val[1] > 1.0e-5)) ||
                      (bitype >= 101 && bitype <= 104 && e->zdat && e->ndata >= 1) ||
                      ((bitype == 105 || bitype == 106) && e->zdat && e->ndata >= 5) ||

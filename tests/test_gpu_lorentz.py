@@ -335,3 +335,47 @@ def test_batched_runs_keep_each_bunchs_integrator():
         b2.close()
     np.testing.assert_allclose(out[0][0], solo[1], rtol=1e-13, atol=0)
     np.testing.assert_allclose(out[1][0], solo[2], rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("current,form,cols,tol", [
+    (0.010, impz.FORM_FP64, RMS_COLS, 1e-8),
+    (0.010, impz.FORM_FP32CONV, [7, 9, 11, 13, 15, 17, 19, 21, 23], 1e-5),
+    (0.0, impz.FORM_FP64, RMS_COLS, 1e-10)])
+def test_lorentz_emfld_maps_match_the_oracle(current, form, cols, tol):
+    """EMfld 110 elements over read4_Data x-y-z maps (scatter2 with
+    FlagDisc 1, FlagCart 2): an RF map whose complex fields vary in x, y and
+    z (the plane at each kick quadratic in z, each particle's field
+    quadratic in x and y, times escale e^{i(ww t + theta0)}) and a static
+    quadrupole map: GPU = oracle, the reference particle exact."""
+    from test_lorentz import emfld, emfld_grid, quad_map
+    cfg = beams.fodo_1e5(n=20_000, seed=beams.SEED0 + 94)
+    length = 0.2
+
+    def rf(x, y, z):
+        k = np.pi / length
+        ez = 1.0e7 * np.sin(k * z) * (1 + 0.1j) * (1 - 200.0 * (x * x + y * y))
+        ex = -1.0e8 * x * np.cos(k * z) * (1 - 0.3j)
+        ey = -1.0e8 * y * np.cos(k * z) * (1 - 0.3j)
+        bx = 0.02 * y * np.sin(k * z) * 1j
+        by = -0.02 * x * np.sin(k * z) * 1j
+        return ex, ey, ez, bx, by, 0.001 * np.cos(k * z) + 0 * x
+    lat = [impz.elem(0, 0.05, 2, 1, [1.0]),
+           emfld(length, 8, emfld_grid(rf, length, nz=20), 1.2, 402.5e6, 20.0),
+           impz.elem(0, 0.05, 2, 1, [1.0]),
+           emfld(0.1, 4, emfld_grid(quad_map(15.0), 0.1))]
+    rows_o, _, beam = orc.run(lat, cfg["pts"], current, cfg["mass"], cfg["charge"], cfg["freq"],
+                              cfg["refptcl"], cfg["grid"], flagmap=2)
+    b = impz.Bunch(cfg["pts"], current, cfg["mass"], cfg["charge"], cfg["freq"],
+                   cfg["refptcl"], cfg["grid"], form=form, track_ids=False)
+    try:
+        b.set_integrator(2)
+        recs, zs = b.run(lat)
+        refs = b.run_reference()
+    finally:
+        b.close()
+    np.testing.assert_allclose(zs, rows_o[:, 0], rtol=0, atol=0)
+    np.testing.assert_array_equal(refs[-1], np.array(beam.refptcl[:]))
+    assert abs(-refs[-1][5] + cfg["refptcl"][5]) > 1e-6  # the RF map changes the energy
+    rows_g = np.array([impz.diag_row(zs[i], recs[i], refs[i], cfg["mass"], cfg["freq"])
+                       for i in range(len(recs))])
+    assert worst(rows_g, rows_o, cols) <= tol

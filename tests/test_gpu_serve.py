@@ -116,8 +116,10 @@ def test_server_admits_a_job_that_arrives_while_others_run():
     while both long jobs are still running, and its records equal its solo
     run within the module tolerance."""
     import time
-    long_jobs = [dict(n=2_000_000, seed=beams.SEED0 + 600 + k, current=0.03 + 0.01 * k,
-                      grid=(64, 64, 128), lattice=beams.fodo_steps(1200, nseg=4))
+    # each long job runs for about a second (4e6 particles, 2400 steps),
+    # the short one for milliseconds
+    long_jobs = [dict(n=4_000_000, seed=beams.SEED0 + 600 + k, current=0.03 + 0.01 * k,
+                      grid=(64, 64, 128), lattice=beams.fodo_steps(2400, nseg=4))
                  for k in range(2)]
     short = dict(n=20_000, seed=beams.SEED0 + 610, current=0.02, grid=(32, 32, 64),
                  lattice=beams.fodo_steps(40, nseg=4))
@@ -136,7 +138,6 @@ def test_server_admits_a_job_that_arrives_while_others_run():
             time.sleep(0.002)
         st = srv.stats()
         assert st["queued"] == 0 and st["completed"] == 0 and st["admitted_bytes"] > 0
-        time.sleep(0.05)  # both long jobs are stepping on the device
         sid = srv.submit(pts_s, short["current"], beams.PROTON_MASS_EV, 1.0, 402.5e6, ref_s,
                          short["grid"], short["lattice"])
         recs, latency, queued, _ = srv.wait(sid)
@@ -146,6 +147,6 @@ def test_server_admits_a_job_that_arrives_while_others_run():
     assert during["completed"] == 1, during  # only the short job had finished
     assert queued <= latency
     assert end["completed"] == 3 and end["failed"] == 0
-    assert all(r[0].shape[0] == 1201 for r in long_res)
+    assert all(r[0].shape[0] == 2401 for r in long_res)
     assert recs.shape == solo.shape
     assert close(recs, solo) <= TOL

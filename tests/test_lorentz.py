@@ -351,3 +351,95 @@ def test_multipole_kick_is_getfld_multipole(idpole, g):
     np.testing.assert_allclose(p1[:, 3], p0[:, 3] + clight * bx * tau * r7, rtol=1e-14, atol=0)
     np.testing.assert_array_equal(p1[:, 5], p0[:, 5])
     assert np.max(np.abs(p1[:, 1] - p0[:, 1])) > 0.05 * np.max(np.abs(p0[:, 1]))
+
+
+# ---------------------------------------------------------------------------
+# EMfld 110: discrete x-y-z field map (read4_Data, scatter2 FlagDisc 1, FlagCart 2)
+def emfld_grid(fields, length, xr=(-8e-3, 8e-3, 16), yr=(-8e-3, 8e-3, 16), nz=10):
+    """read4_Data's map of an element of `length`: nodes x fastest, then y,
+    then z; fields(x, y, z) -> six complex arrays (Ex, Ey, Ez, Bx, By, Bz)."""
+    xs = np.linspace(xr[0], xr[1], xr[2] + 1)
+    ys = np.linspace(yr[0], yr[1], yr[2] + 1)
+    zs = np.linspace(0.0, length, nz + 1)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    comps = [np.broadcast_to(np.asarray(f, dtype=complex), X.shape).reshape(-1)
+             for f in fields(X, Y, Z)]
+    header = np.array([xr[0], xr[1], xr[2], yr[0], yr[1], yr[2], 0.0, length, nz], dtype=float)
+    return header, np.stack(comps, axis=1)
+
+
+def emfld(length, nseg, grid, scale=1.0, freq=0.0, theta0=0.0, radius=1.0):
+    """A type 110 element: Param(2..14) = scale, frequency, theta0 [deg],
+    file ID, x and y radius, errors (0), FlagDisc 1, FlagCart 2."""
+    vals = [scale, freq, theta0, 1.0, radius, radius, 0, 0, 0, 0, 0, 1.0, 2.0]
+    return impz.elem(110, length, nseg, 1, vals, grid=grid)
+
+
+def quad_map(g):
+    def f(x, y, z):
+        zero = np.zeros_like(x)
+        return zero, zero, zero, g * y, g * x, zero
+    return f
+
+
+@pytest.mark.parametrize("current", [0.0, 0.030])
+def test_emfld_with_a_quadrupoles_field_tracks_like_the_quadrupole(current):
+    """An EMfld 110 whose x-y-z map holds a hard-edge quadrupole's static
+    field (B = G (y, x, 0), zero frequency) tracks like that quadrupole
+    under the Lorentz integrator: the map's quadratic interpolation is exact
+    for fields linear in x and y inside the grid, so the runs agree to
+    rounding (1e-12 of each column's rms), with and without space charge."""
+    cfg = beams.fodo_1e5(n=2000, seed=beams.SEED0 + 91)
+    g, length = 20.0, 0.1
+    drift = impz.elem(0, 0.1, 2, 1, [1.0])
+    lat_q = [drift, impz.elem(1, length, 4, 1, [g, 0.0, 1.0]), drift]
+    lat_e = [drift, emfld(length, 4, emfld_grid(quad_map(g), length)), drift]
+    _, pq, bq = _lz_run(lat_q, cfg, current)
+    _, pe, be = _lz_run(lat_e, cfg, current)
+    assert pq.shape == pe.shape
+    for c in range(6):
+        scale = np.sqrt(np.mean(pq[:, c] ** 2))
+        assert np.max(np.abs(pe[:, c] - pq[:, c])) / scale <= 1e-12, c
+    np.testing.assert_allclose(be.refptcl[:], bq.refptcl[:], rtol=1e-15)
+
+
+def test_emfld_rf_map_moves_the_reference_energy():
+    """A uniform complex Ez map (E0 (1 + 0.2 i), escale 1.5, 402.5 MHz,
+    theta0 30 deg): each kick changes gamma0 by tau qmcc ez0 with ez0 =
+    Re(Ez escale e^{i(ww tg + theta0)}) at the reference time tg (kick2's
+    refptcl(6) = -gam, scatter2's ez0 at x = y = 0), theta0 with the
+    reference's single-precision asin(1.0)."""
+    cfg = beams.fodo_1e5(n=500, seed=beams.SEED0 + 92)
+    length, nseg, e0, scale, freq, th = 0.2, 5, 2.0e6, 1.5, 402.5e6, 30.0
+
+    def uniform(x, y, z):
+        zero = np.zeros_like(x)
+        return zero, zero, e0 * (1 + 0.2j) + zero, zero, zero, zero
+    lat = [emfld(length, nseg, emfld_grid(uniform, length), scale, freq, th)]
+    _, _, beam = _lz_run(lat, cfg)
+    scxl = 2.99792458e8 / (2 * np.pi * cfg["freq"])
+    qmcc = cfg["charge"] / cfg["mass"]
+    ww = freq / cfg["freq"]
+    theta0 = th * float(np.arcsin(np.float32(1.0))) / 90
+    tau, tg, gam = length / nseg, cfg["refptcl"][4], -cfg["refptcl"][5]
+    for _ in range(nseg):
+        tg += 0.5 * tau / (scxl * np.sqrt(1.0 - 1.0 / gam / gam))
+        ph = ww * tg + theta0
+        ez0 = e0 * (scale * np.cos(ph)) - 0.2 * e0 * (scale * np.sin(ph))
+        gam = gam + tau * qmcc * ez0
+        tg += 0.5 * tau / (scxl * np.sqrt(1.0 - 1.0 / gam / gam))
+    np.testing.assert_allclose(-beam.refptcl[5], gam, rtol=1e-13)
+    assert abs(-beam.refptcl[5] + cfg["refptcl"][5]) > 1e-4
+
+
+def test_emfld_other_forms_are_refused():
+    """EMfld's analytical and r-z forms read data the reference's driver
+    never loads for type 110 under Flagmap=2: refused."""
+    cfg = beams.fodo_1e5(n=200, seed=beams.SEED0 + 93)
+    grid = emfld_grid(quad_map(1.0), 0.1)
+    vals = [1.0, 0.0, 0.0, 1.0, 1.0, 1.0, 0, 0, 0, 0, 0, 1.0, 1.0]  # FlagCart 1 (r-z)
+    with pytest.raises(RuntimeError):
+        _lz_run([impz.elem(110, 0.1, 2, 1, vals, grid=grid)], cfg)
+    vals[11], vals[12] = 3.0, 2.0  # analytical
+    with pytest.raises(RuntimeError):
+        _lz_run([impz.elem(110, 0.1, 2, 1, vals, grid=grid)], cfg)
