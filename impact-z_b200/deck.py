@@ -227,6 +227,69 @@ def read_rfcoef(path):
     return np.array(vals)
 
 
+_CPLX = None
+
+
+def _fortran_tokens(line):
+    """List-directed values of one line: "(re,im)" complex constants and
+    plain numbers (Fortran d exponents allowed)."""
+    import re
+    global _CPLX
+    if _CPLX is None:
+        _CPLX = re.compile(r"\(\s*([^,()\s]+)\s*,\s*([^,()\s]+)\s*\)|([^\s,()]+)")
+    out = []
+    for m in _CPLX.finditer(line.replace("d", "e").replace("D", "e")):
+        if m.group(1) is not None:
+            out.append(complex(float(m.group(1)), float(m.group(2))))
+        else:
+            try:
+                out.append(float(m.group(3)))
+            except ValueError:
+                break
+    return out
+
+
+def read_emfld(path):
+    """rfdataN.in of an EMfld 110 element as read4_Data reads it
+    (src/DataStruct/Data.f90:415-554): three records xmin, xmax, NxIntv /
+    y / z (the bounds as complex constants, their real parts kept), then
+    (Ex, Ey, Ez, Bx, By, Bz) complex per node, x fastest, nodes not given
+    left zero.  Returns (header[9], data (nodes, 12) re/im pairs) for
+    impz_b200.elem(..., grid=...)."""
+    with open(path) as f:
+        lines = [ln for ln in f if ln.strip() and not _is_comment(ln)]
+    header = []
+    for ln in lines[:3]:
+        v = _fortran_tokens(ln)
+        header += [complex(v[0]).real, complex(v[1]).real, float(complex(v[2]).real)]
+    nx, ny, nz = (int(header[k] + 0.1) for k in (2, 5, 8))
+    nodes = (nx + 1) * (ny + 1) * (nz + 1)
+    data = np.zeros((nodes, 12))
+    n = 0
+    for ln in lines[3:]:
+        v = _fortran_tokens(ln)
+        if len(v) < 6 or n >= nodes:
+            break
+        for c in range(6):
+            z = complex(v[c])
+            data[n, 2 * c] = z.real
+            data[n, 2 * c + 1] = z.imag
+        n += 1
+    return np.array(header), data
+
+
+def write_emfld(path, header, data):
+    """Writes an EMfld map in read4_Data's format (read_emfld's inverse)."""
+    data = np.asarray(data, dtype=float).reshape(-1, 12)
+    with open(path, "w") as f:
+        for k in range(3):
+            lo, hi, nint = header[3 * k], header[3 * k + 1], int(header[3 * k + 2] + 0.1)
+            f.write("(%.17g,0.0) (%.17g,0.0) %d\n" % (lo, hi, nint))
+        for row in data:
+            f.write(" ".join("(%.17g,%.17g)" % (row[2 * c], row[2 * c + 1]) for c in range(6))
+                    + "\n")
+
+
 def read_wake(path):
     """rfdataN.in as a wake table, read1wk_Data (src/DataStruct/Data.f90:
     559-633): rows (z, longitudinal, x, y wake); z is shifted to start at 0
@@ -440,6 +503,10 @@ def lattice_segments(deck, workdir, skip=(), start=0):
         elif e.type == 1 and e.vals[1] > 1.0e-5:
             # a quadrupole's gradient profile (AccSimulator.f90:853-863)
             rf = read_rfdata(os.path.join(workdir, "rfdata%d.in" % int(e.vals[1] + 0.1)))
+        elif e.type == 110 and flagmap == 2 and e.vals[3] >= 0.0:
+            # EMfld's x-y-z map (read4_Data, AccSimulator.f90:841-842)
+            grid = read_emfld(os.path.join(workdir, "rfdata%d.in" % int(e.vals[3] + 0.1)))
+            return elem(e.type, e.length, e.nseg, e.mapstp, list(e.vals), grid=grid)
         return elem(e.type, e.length, e.nseg, e.mapstp, list(e.vals), rf=rf)
 
     seg, skipped = [], []

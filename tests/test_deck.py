@@ -230,3 +230,35 @@ def test_slice_output_matches_a_loop_restatement():
     assert got.shape == (7, 11) and np.all(np.isfinite(got))
     np.testing.assert_allclose(got, want, rtol=1e-10, atol=0)
     assert abs(got[:, 1].sum() - n) < 1e-9 * n
+
+
+def test_emfld_map_file_round_trip_and_deck_element(tmp_path):
+    """An EMfld 110 map written in read4_Data's format (complex constants
+    "(re,im)") reads back exactly, and a Flagmap=2 deck's 110 element built
+    from it tracks on the oracle like the element built from the arrays."""
+    from test_lorentz import emfld, emfld_grid, quad_map
+    header, data = emfld_grid(quad_map(12.0), 0.1, nz=6)
+    data = np.stack([data.real, data.imag], axis=-1).reshape(data.shape[0], 12)
+    data[:, 4] += 1.0e5  # a uniform Ez as well
+    data[:, 5] -= 2.0e4
+    path = str(tmp_path / "rfdata7.in")
+    deck.write_emfld(path, header, data)
+    h2, d2 = deck.read_emfld(path)
+    np.testing.assert_array_equal(h2, header)
+    np.testing.assert_array_equal(d2, data)
+    d = deck.Deck()
+    d.flagmap = 2
+    vals = [1.0, 402.5e6, 15.0, 7.0, 1.0, 1.0, 0, 0, 0, 0, 0, 1.0, 2.0]
+    d.elements = [deck.Element(0.1, 4, 1, 110, vals + [0.0] * (24 - len(vals)))]
+    runs = [item for kind, item in deck.lattice_segments(d, str(tmp_path)) if kind == "run"]
+    cfg = beams.fodo_1e5(n=500, seed=beams.SEED0 + 95)
+    args = (cfg["pts"], 0.0, cfg["mass"], cfg["charge"], cfg["freq"], cfg["refptcl"],
+            (16, 16, 32))
+    orc = load_oracle()
+    _, p1, b1 = orc.run(runs[0], *args, flagmap=2)
+    direct = emfld(0.1, 4, (header, data), 1.0, 402.5e6, 15.0)
+    direct.val[3] = 7.0
+    _, p2, b2 = orc.run([direct], *args, flagmap=2)
+    np.testing.assert_array_equal(p1, p2)
+    np.testing.assert_array_equal(b1.refptcl[:], b2.refptcl[:])
+    assert b1.refptcl[5] != cfg["refptcl"][5]
