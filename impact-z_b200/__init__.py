@@ -115,6 +115,8 @@ _SIGS = {
     "impz_run_reference": (ctypes.c_int, [_B, _D, ctypes.c_int, _I]),
     "impz_run_batch": (ctypes.c_int, [ctypes.POINTER(_B), ctypes.POINTER(_E),
                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "impz_run_advance_packed": (ctypes.c_int, [ctypes.POINTER(_B), ctypes.c_int, ctypes.c_int,
+                                               ctypes.POINTER(ctypes.c_int)]),
     "impz_run_begin": (ctypes.c_int, [_B, _E, ctypes.c_int]),
     "impz_run_advance": (ctypes.c_int, [_B, ctypes.c_int, _I]),
     "impz_bunch_footprint": (ctypes.c_longlong, [ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
@@ -251,6 +253,24 @@ def run_batch(bunches, lattices):
     for b, l, a in zip(bunches, lattices, arrs):
         b._pending = (a, count_steps(l) + 1)
     _check(lib().impz_run_batch(hs, ptrs, ns, nb), "impz_run_batch")
+    return [b.run_fetch() for b in bunches]
+
+
+def run_packed(bunches, lattices, steps_per_call=8):
+    """Runs every bunch over its own lattice (any lengths and grid sizes)
+    with impz_run_advance_packed, `steps_per_call` steps per call; returns
+    [(records, zs)] in bunch order."""
+    arrs = [elem_array(l) for l in lattices]
+    for b, l, a in zip(bunches, lattices, arrs):
+        _check(lib().impz_run_begin(b.h, a, len(l)), "impz_run_begin")
+        b._pending = (a, count_steps(l) + 1)
+    left = list(bunches)
+    while left:
+        hs = (_B * len(left))(*[b.h for b in left])
+        rem = (ctypes.c_int * len(left))()
+        _check(lib().impz_run_advance_packed(hs, len(left), int(steps_per_call), rem),
+               "impz_run_advance_packed")
+        left = [b for b, r in zip(left, rem) if r > 0]
     return [b.run_fetch() for b in bunches]
 
 

@@ -1970,6 +1970,178 @@ static int run_batch_packed(impz_bunch_t* bs, int nb) {
   return IMPZ_OK;
 }
 
+// One step of every listed bunch, each at its own place in its own run
+// (run_begin done, steps left), with packed launches on stream s: the field
+// solve of the bunches whose step kicks (grouped by grid size), then one
+// pass over all of them.  The launch arguments are built on the host for the
+// bunches' current parities and copied to dscratch (stream ordered, so the
+// previous step's kernels have read theirs).
+static size_t packed_scratch_bytes(int nb) {
+  return round_up((size_t)nb * sizeof(AdvanceArgs), kAlign) +
+         round_up((size_t)nb * sizeof(DepositArgs), kAlign) +
+         round_up((size_t)nb * sizeof(ScanArgs), kAlign) +
+         round_up((size_t)nb * sizeof(PoissonMember), kAlign) +
+         3 * round_up((size_t)(nb + 1) * sizeof(int), kAlign);
+}
+
+static int packed_step(impz_bunch_t* bs, int nb, cudaStream_t s, char* dscratch, bool f32,
+                       bool light) {
+  std::vector<impz_bunch_t> mem_b, sc_b;
+  for (int i = 0; i < nb; i++) {
+    impz_bunch_t b = bs[i];
+    if (b->run_next > b->lat.nsteps) continue;
+    mem_b.push_back(b);
+    if (b->lat.steps[b->run_next].sc) sc_b.push_back(b);
+  }
+  const int nm = (int)mem_b.size(), ns = (int)sc_b.size();
+  if (nm == 0) return IMPZ_OK;
+  std::vector<AdvanceArgs> adv(nm);
+  std::vector<int> adv_offs(nm + 1, 0), dep_offs(ns + 1, 0), scan_offs(ns + 1, 0);
+  for (int i = 0; i < nm; i++) {
+    impz_bunch_t b = mem_b[i];
+    const int sc = b->lat.steps[b->run_next].sc ? 1 : 0;
+    adv[i] = advance_args(b, b->dsteps, -1, sc, 1, 1, b->mom_out, 0);
+    adv_offs[i + 1] = adv_offs[i] + b->grid_adv;
+  }
+  std::vector<DepositArgs> dep(ns);
+  std::vector<ScanArgs> scn(ns);
+  std::vector<int> order(ns);
+  for (int i = 0; i < ns; i++) {
+    impz_bunch_t b = sc_b[i];
+    dep[i] = deposit_args(b, b->dsteps, -1);
+    scn[i] = ScanArgs{b->counts, b->cursor, b->bsum, b->G + 1, b->st};
+    dep_offs[i + 1] = dep_offs[i] + b->grid_dep;
+    scan_offs[i + 1] =
+        scan_offs[i] + (int)((b->G + 1 + (1ll << IMPZ_SCAN_LOG) - 1) >> IMPZ_SCAN_LOG);
+    order[i] = i;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+    const impz_bunch_t x = sc_b[a], y = sc_b[c];
+    if (x->nx != y->nx) return x->nx < y->nx;
+    if (x->ny != y->ny) return x->ny < y->ny;
+    return x->nz < y->nz;
+  });
+  std::vector<PoissonMember> pm(ns);
+  std::vector<BatchGroup> groups;
+  for (int k = 0; k < ns; k++) {
+    const impz_bunch_t b = sc_b[order[k]];
+    const PoissonBuffers pb = poisson_of(b);
+    PoissonMember& m = pm[k];
+    m.rho = pb.rho; m.qscale = pb.qscale; m.spec = pb.spec; m.ghat = pb.ghat; m.phi = pb.phi;
+    m.efield = pb.efield; m.twx = pb.twx; m.twy = pb.twy; m.twz = pb.twz; m.F = pb.F;
+    m.Gt = pb.Gt; m.st = pb.st;
+    if (groups.empty() || groups.back().nx != b->nx || groups.back().ny != b->ny ||
+        groups.back().nz != b->nz)
+      groups.push_back(BatchGroup{b->nx, b->ny, b->nz, k, 0});
+    groups.back().count++;
+  }
+  size_t off = 0;
+  cudaError_t ecopy = cudaSuccess;
+  auto put = [&](const void* src, size_t bytes) {
+    if (bytes && ecopy == cudaSuccess)
+      ecopy = cudaMemcpyAsync(dscratch + off, src, bytes, cudaMemcpyHostToDevice, s);
+    off = round_up(off + bytes, kAlign);
+  };
+  const size_t o_adv = off; put(adv.data(), adv.size() * sizeof(AdvanceArgs));
+  const size_t o_dep = off; put(dep.data(), dep.size() * sizeof(DepositArgs));
+  const size_t o_scn = off; put(scn.data(), scn.size() * sizeof(ScanArgs));
+  const size_t o_mem = off; put(pm.data(), pm.size() * sizeof(PoissonMember));
+  const size_t o_ao = off; put(adv_offs.data(), adv_offs.size() * sizeof(int));
+  const size_t o_do = off; put(dep_offs.data(), dep_offs.size() * sizeof(int));
+  const size_t o_so = off; put(scan_offs.data(), scan_offs.size() * sizeof(int));
+  if (ecopy != cudaSuccess) return cuda_fail(ecopy, "packed step: arguments");
+  cudaError_t e = cudaSuccess;
+  if (ns > 0) {
+    const PoissonMember* d_mem = (const PoissonMember*)(dscratch + o_mem);
+    for (const BatchGroup& g : groups) {
+      e = f32 ? launch_green_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+              : launch_green_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+      if (e != cudaSuccess) return cuda_fail(e, "packed step: Green function");
+    }
+    const DepositArgs* d_dep = (const DepositArgs*)(dscratch + o_dep);
+    const int* d_do = (const int*)(dscratch + o_do);
+    e = f32 ? fast::launch_deposit_packed(d_dep, d_do, ns, dep_offs[ns], s)
+            : exact::launch_deposit_packed(d_dep, d_do, ns, dep_offs[ns], s);
+    if (e != cudaSuccess) return cuda_fail(e, "packed step: deposit");
+    e = exact::launch_scan_packed((const ScanArgs*)(dscratch + o_scn),
+                                  (const int*)(dscratch + o_so), ns, scan_offs[ns], s);
+    if (e != cudaSuccess) return cuda_fail(e, "packed step: scan");
+    for (const BatchGroup& g : groups) {
+      e = f32 ? launch_conv_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+              : launch_conv_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+      if (e == cudaSuccess)
+        e = f32 ? launch_efield_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+                : launch_efield_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+      if (e != cudaSuccess) return cuda_fail(e, "packed step: field solve");
+    }
+    g_launches += 2 + 9 * (int)groups.size();
+  }
+  e = f32 ? fast::launch_advance_packed((const AdvanceArgs*)(dscratch + o_adv),
+                                        (const int*)(dscratch + o_ao), nm, adv_offs[nm], true,
+                                        light, s)
+          : exact::launch_advance_packed((const AdvanceArgs*)(dscratch + o_adv),
+                                         (const int*)(dscratch + o_ao), nm, adv_offs[nm], false,
+                                         light, s);
+  if (e != cudaSuccess) return cuda_fail(e, "packed step: particle pass");
+  g_launches += 1;
+  for (impz_bunch_t b : mem_b) {
+    if (b->lat.steps[b->run_next].sc) b->parity ^= 1;
+    b->run_next++;
+  }
+  return IMPZ_OK;
+}
+
+int impz_run_advance_packed(impz_bunch_t* bunches, int nb, int steps, int* remaining) {
+  if (!bunches || nb < 1 || steps < 1) return IMPZ_ERR_ARG;
+  const impz_bunch_t b0 = bunches[0];
+  if (!b0) return IMPZ_ERR_ARG;
+  bool light = true;
+  std::vector<impz_bunch_t> pk;  // the packable ones; bunches with wakes step on their own
+  for (int i = 0; i < nb; i++) {
+    const impz_bunch_t b = bunches[i];
+    if (!b || b->device != b0->device || b->form != b0->form) return IMPZ_ERR_ARG;
+    if (b->run_next < 1 || b->run_pending) return IMPZ_ERR_STATE;  // no run in progress
+  }
+  CK(cudaSetDevice(b0->device));
+  for (int i = 0; i < nb; i++) {
+    impz_bunch_t b = bunches[i];
+    if (b->run_wake || b->prof_on) {
+      const int r = run_advance(b, steps);
+      if (r) return r;
+    } else {
+      pk.push_back(b);
+      light = light && b->run_light;
+    }
+  }
+  if (pk.empty()) {
+    for (int i = 0; i < nb; i++) {
+      impz_bunch_t b = bunches[i];
+      if (remaining) remaining[i] = std::max(0, b->lat.nsteps + 1 - b->run_next);
+      if (b->run_next > b->lat.nsteps && !b->run_pending) run_end(b);
+    }
+    return IMPZ_OK;
+  }
+  const int np = (int)pk.size();
+  cudaStream_t s = pk[0]->stream;
+  for (int i = 1; i < np; i++) {
+    CK(cudaEventRecord(pk[i]->ev_dep, pk[i]->stream));
+    CK(cudaStreamWaitEvent(s, pk[i]->ev_dep, 0));
+  }
+  char* dscratch = nullptr;
+  CK(cudaMallocAsync((void**)&dscratch, packed_scratch_bytes(np), s));
+  int r = IMPZ_OK;
+  for (int k = 0; k < steps && !r; k++) r = packed_step(pk.data(), np, s, dscratch, b0->f32(), light);
+  cudaFreeAsync(dscratch, s);
+  CK(cudaEventRecord(pk[0]->ev_dep, s));
+  for (int i = 1; i < np; i++) CK(cudaStreamWaitEvent(pk[i]->stream, pk[0]->ev_dep, 0));
+  for (int i = 0; i < nb; i++) {
+    impz_bunch_t b = bunches[i];
+    if (remaining) remaining[i] = std::max(0, b->lat.nsteps + 1 - b->run_next);
+    if (!r && b->run_next > b->lat.nsteps && !b->run_pending) run_end(b);
+  }
+  return r;
+}
+
 int impz_run_batch(impz_bunch_t* bunches, const impz_elem_t* const* lattices,
                    const int* nelem, int nb) {
   if (!bunches || !lattices || !nelem || nb < 0) return IMPZ_ERR_ARG;

@@ -4,11 +4,12 @@
 // A worker thread owns every device call.  Submitted jobs wait in a FIFO
 // queue; a job is admitted as soon as its footprint (impz_bunch_footprint)
 // fits the HBM budget next to the running jobs and a slot is free.  Each
-// admitted job gets its own bunch (and so its own streams) and its state
-// stays resident in HBM until it finishes.  The worker enqueues the running
-// jobs' steps in chunks, round robin, keeping at most two chunks in flight
-// per job, so kernels of different jobs overlap on the device and a job that
-// arrives while others run starts between their chunks.  The actual device
+// admitted job gets its own bunch and its state stays resident in HBM until
+// it finishes.  The worker advances all running jobs of a form together in
+// chunks of steps with packed launches (one launch per kernel for every job,
+// each job at its own step of its own lattice), keeping at most two chunks in
+// flight, so a job that arrives while others run joins them at the next
+// chunk.  The actual device
 // memory a job holds is measured at admission (cudaMemGetInfo before and
 // after its bunch is created) and reported with the statistics.
 #include <cuda_runtime.h>
@@ -115,27 +116,43 @@ void release(impz_server_t s, Job* j) {
 }
 
 // One pass over the running jobs; returns true if anything was launched or
-// finished (worker thread).
+// finished (worker thread).  The stepping jobs of each form advance
+// together, `chunk` steps per call, with packed launches
+// (impz_run_advance_packed: one launch per kernel for all of them), at most
+// two calls in flight; a job that arrives joins at the next call.
 bool service(impz_server_t s, std::vector<Job*>& running) {
   bool progress = false;
-  for (Job* j : running) {
-    if (j->fin != 0) continue;
-    cudaStream_t st = (cudaStream_t)impz_bunch_stream(j->bunch);
-    if (j->remaining > 0) {
-      // at most two chunks in flight: chunk k may go once chunk k-2 is done
-      cudaEvent_t slot = j->ev[j->chunks & 1];
-      if (j->chunks >= 2 && cudaEventQuery(slot) == cudaErrorNotReady) continue;
-      int left = 0;
-      int r = impz_run_advance(j->bunch, s->chunk, &left);
+  for (int form = 0; form < 2; form++) {
+    std::vector<Job*> step;
+    bool ready = true;
+    for (Job* j : running) {
+      if (j->fin != 0 || j->remaining <= 0 || j->form != form) continue;
+      // chunk k of a job may go once its chunk k-2 is done
+      if (j->chunks >= 2 && cudaEventQuery(j->ev[j->chunks & 1]) == cudaErrorNotReady)
+        ready = false;
+      step.push_back(j);
+    }
+    if (step.empty() || !ready) continue;
+    std::vector<impz_bunch_t> bs(step.size());
+    std::vector<int> left(step.size(), 0);
+    for (size_t k = 0; k < step.size(); k++) bs[k] = step[k]->bunch;
+    const int r = impz_run_advance_packed(bs.data(), (int)bs.size(), s->chunk, left.data());
+    for (size_t k = 0; k < step.size(); k++) {
+      Job* j = step[k];
       if (r) {
         j->fin = r;
         continue;
       }
-      j->remaining = left;
-      cudaEventRecord(slot, st);
+      j->remaining = left[k];
+      cudaEventRecord(j->ev[j->chunks & 1], (cudaStream_t)impz_bunch_stream(j->bunch));
       j->chunks++;
-      progress = true;
-    } else if (cudaEventQuery(j->ev[(j->chunks - 1) & 1]) == cudaSuccess) {
+    }
+    progress = true;
+  }
+  for (Job* j : running) {
+    if (j->fin != 0) continue;
+    if (j->remaining > 0) continue;
+    if (cudaEventQuery(j->ev[(j->chunks - 1) & 1]) == cudaSuccess) {
       const int cap = (int)j->steps + 1;
       j->recs.assign((size_t)cap * IMPZ_MOMREC, 0.0);
       j->zs.assign(cap, 0.0);

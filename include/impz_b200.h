@@ -257,6 +257,18 @@ int impz_run_fetch(impz_bunch_t b, double* recs, double* zs, int maxrec, int* nr
  * once none remain the records can be fetched with impz_run_fetch. */
 int impz_run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem);
 int impz_run_advance(impz_bunch_t b, int budget, int* remaining);
+/* Advances several bunches, each in its own run (impz_run_begin done; any
+ * step counts, grid sizes and lattices; one device and form; no wakes), by
+ * up to `steps` steps each, with packed launches: per step one launch of
+ * the particle pass, the deposit and the count scan for all of them over a
+ * (bunch, block) work list, and one launch per field-solve kernel for each
+ * group of equal grid size.  A bunch's arithmetic is that of its own run.
+ * remaining[i] (may be NULL) receives each bunch's steps left; a finished
+ * run is ready for impz_run_fetch.  The launches go to the first bunch's
+ * stream; the other bunches' streams are ordered after them.  The serving
+ * loop's multi-job counterpart of impz_run_advance (AccSimulator.f90's
+ * step loop for many independent runs at once: no reference counterpart). */
+int impz_run_advance_packed(impz_bunch_t* bunches, int nb, int steps, int* remaining);
 /* Runs nb bunches, each over its own lattice, with their steps interleaved
  * two at a time on the bunches' own streams so that their kernels overlap on
  * the device (batched scans).  Returns once everything is enqueued; fetch

@@ -61,6 +61,28 @@ def test_batch_equals_one_by_one(form):
         assert close(recs, r) <= TOL
 
 
+@pytest.mark.parametrize("form", [impz.FORM_FP64, impz.FORM_FP32CONV])
+def test_packed_runs_of_different_lengths_equal_solo_runs(form):
+    """impz_run_advance_packed over bunches of three grid sizes whose
+    lattices have different lengths (each bunch at its own step, runs ending
+    at different calls): each bunch's records equal its solo run."""
+    jobs = small_jobs()
+    for i, j in enumerate(jobs):
+        j["lattice"] = beams.fodo_steps(16 + 7 * i, nseg=4)
+    ref = [alone(j, form) for j in jobs]
+    bunches = []
+    for j in jobs:
+        pts, r = beams.make_scan_bunch(j)
+        bunches.append(impz.Bunch(pts, j["current"], beams.PROTON_MASS_EV, 1.0, 402.5e6, r,
+                                  j["grid"], form=form, track_ids=False))
+    out = impz.run_packed(bunches, [j["lattice"] for j in jobs], steps_per_call=5)
+    for b in bunches:
+        b.close()
+    for (recs, zs), r in zip(out, ref):
+        assert recs.shape == r.shape
+        assert close(recs, r) <= TOL
+
+
 def test_server_result_alone_equals_result_in_mix():
     jobs = small_jobs()
     target = jobs[2]
