@@ -1801,7 +1801,7 @@ struct BatchGroup {
 
 static int run_batch_packed(impz_bunch_t* bs, int nb) {
   const impz_bunch_t b0 = bs[0];
-  cudaStream_t s = b0->stream;
+  cudaStream_t s = b0->stream, s2 = b0->stream2;
   const bool f32 = b0->f32();
   bool light = true;
   for (int i = 0; i < nb; i++) light = light && bs[i]->run_light;
@@ -1898,18 +1898,30 @@ static int run_batch_packed(impz_bunch_t* bs, int nb) {
   auto step = [&](int p, bool sc) -> cudaError_t {
     cudaError_t e = cudaSuccess;
     if (sc) {
+      // the Green functions on the second stream, beside the deposit, the
+      // scan and the forward transforms
+      if ((e = cudaEventRecord(b0->ev_fork, s)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(s2, b0->ev_fork, 0)) != cudaSuccess) return e;
       for (const BatchGroup& g : groups) {
-        e = f32 ? launch_green_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
-                : launch_green_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+        e = f32 ? launch_green_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s2)
+                : launch_green_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s2);
         if (e != cudaSuccess) return e;
       }
+      if ((e = cudaEventRecord(b0->ev_join, s2)) != cudaSuccess) return e;
       e = f32 ? fast::launch_deposit_packed(d_dep + (size_t)p * nb, d_do, nb, n_dep, s)
               : exact::launch_deposit_packed(d_dep + (size_t)p * nb, d_do, nb, n_dep, s);
       if (e != cudaSuccess) return e;
       if ((e = exact::launch_scan_packed(d_scn, d_so, nb, n_scan, s)) != cudaSuccess) return e;
       for (const BatchGroup& g : groups) {
-        e = f32 ? launch_conv_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
-                : launch_conv_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+        e = f32 ? launch_conv_group_forward<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+                : launch_conv_group_forward<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count,
+                                                    s);
+        if (e != cudaSuccess) return e;
+      }
+      if ((e = cudaStreamWaitEvent(s, b0->ev_join, 0)) != cudaSuccess) return e;
+      for (const BatchGroup& g : groups) {
+        e = f32 ? launch_conv_group_rest<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+                : launch_conv_group_rest<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
         if (e != cudaSuccess) return e;
         e = f32 ? launch_efield_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
                 : launch_efield_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
@@ -1984,8 +1996,8 @@ static size_t packed_scratch_bytes(int nb) {
          3 * round_up((size_t)(nb + 1) * sizeof(int), kAlign);
 }
 
-static int packed_step(impz_bunch_t* bs, int nb, cudaStream_t s, char* dscratch, bool f32,
-                       bool light) {
+static int packed_step(impz_bunch_t* bs, int nb, cudaStream_t s, cudaStream_t s2,
+                       cudaEvent_t evf, cudaEvent_t evj, char* dscratch, bool f32, bool light) {
   std::vector<impz_bunch_t> mem_b, sc_b;
   for (int i = 0; i < nb; i++) {
     impz_bunch_t b = bs[i];
@@ -2052,12 +2064,17 @@ static int packed_step(impz_bunch_t* bs, int nb, cudaStream_t s, char* dscratch,
   if (ecopy != cudaSuccess) return cuda_fail(ecopy, "packed step: arguments");
   cudaError_t e = cudaSuccess;
   if (ns > 0) {
+    // the Green functions on the second stream, beside the deposit, the
+    // scan and the forward transforms
     const PoissonMember* d_mem = (const PoissonMember*)(dscratch + o_mem);
+    CK(cudaEventRecord(evf, s));
+    CK(cudaStreamWaitEvent(s2, evf, 0));
     for (const BatchGroup& g : groups) {
-      e = f32 ? launch_green_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
-              : launch_green_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+      e = f32 ? launch_green_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s2)
+              : launch_green_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s2);
       if (e != cudaSuccess) return cuda_fail(e, "packed step: Green function");
     }
+    CK(cudaEventRecord(evj, s2));
     const DepositArgs* d_dep = (const DepositArgs*)(dscratch + o_dep);
     const int* d_do = (const int*)(dscratch + o_do);
     e = f32 ? fast::launch_deposit_packed(d_dep, d_do, ns, dep_offs[ns], s)
@@ -2067,8 +2084,14 @@ static int packed_step(impz_bunch_t* bs, int nb, cudaStream_t s, char* dscratch,
                                   (const int*)(dscratch + o_so), ns, scan_offs[ns], s);
     if (e != cudaSuccess) return cuda_fail(e, "packed step: scan");
     for (const BatchGroup& g : groups) {
-      e = f32 ? launch_conv_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
-              : launch_conv_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+      e = f32 ? launch_conv_group_forward<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+              : launch_conv_group_forward<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
+      if (e != cudaSuccess) return cuda_fail(e, "packed step: forward transform");
+    }
+    CK(cudaStreamWaitEvent(s, evj, 0));
+    for (const BatchGroup& g : groups) {
+      e = f32 ? launch_conv_group_rest<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
+              : launch_conv_group_rest<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
       if (e == cudaSuccess)
         e = f32 ? launch_efield_group<float>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s)
                 : launch_efield_group<double>(g.nx, g.ny, g.nz, d_mem + g.first, g.count, s);
@@ -2130,7 +2153,9 @@ int impz_run_advance_packed(impz_bunch_t* bunches, int nb, int steps, int* remai
   char* dscratch = nullptr;
   CK(cudaMallocAsync((void**)&dscratch, packed_scratch_bytes(np), s));
   int r = IMPZ_OK;
-  for (int k = 0; k < steps && !r; k++) r = packed_step(pk.data(), np, s, dscratch, b0->f32(), light);
+  for (int k = 0; k < steps && !r; k++)
+    r = packed_step(pk.data(), np, s, pk[0]->stream2, pk[0]->ev_fork, pk[0]->ev_join, dscratch,
+                    b0->f32(), light);
   cudaFreeAsync(dscratch, s);
   CK(cudaEventRecord(pk[0]->ev_dep, s));
   for (int i = 1; i < np; i++) CK(cudaStreamWaitEvent(pk[i]->stream, pk[0]->ev_dep, 0));

@@ -115,6 +115,13 @@ cudaError_t launch_conv_group(int nx, int ny, int nz, const PoissonMember* mem, 
 template <typename T>
 cudaError_t launch_efield_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
                                 cudaStream_t s);
+// launch_conv_group split where G-hat is first needed
+template <typename T>
+cudaError_t launch_conv_group_forward(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                                      cudaStream_t s);
+template <typename T>
+cudaError_t launch_conv_group_rest(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                                   cudaStream_t s);
 // true when every Poisson kernel of the form fits the device's shared memory
 template <typename T>
 bool poisson_fits(int nx, int ny, int nz);

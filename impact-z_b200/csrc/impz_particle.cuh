@@ -29,9 +29,6 @@
 #ifndef IMPZ_FASTMATH
 #define IMPZ_FASTMATH 0
 #endif
-#ifndef IMPZ_DEP_RUNS
-#define IMPZ_DEP_RUNS 0
-#endif
 
 #ifndef IMPZ_NS
 #error "define IMPZ_NS (exact or fast) before including impz_particle.cuh"
@@ -1345,12 +1342,7 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
     int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {-1, -1, -1};
 #pragma unroll
     for (int u = 0; u < U; u++) {
-#if IMPZ_DEP_RUNS
-      // U consecutive particles per thread: runs of one cell add up in registers
-      const long long i = c0 + (long long)threadIdx.x * U + u;
-#else
       const long long i = c0 + (long long)u * BLOCK + threadIdx.x;
-#endif
       cell[u] = -1;
       pk[u] = 0u;
       wab[u] = wcd[u] = wef[u] = 0.0;
@@ -1412,27 +1404,6 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
     const int R = tiled ? min(IMPZ_DEP_RMAX, IMPZ_DEP_TILE / S) : 1;
     const int mycopy = (lane % R) * S;
     const int bxy = bx * by;
-#if IMPZ_DEP_RUNS
-    unsigned long long acc[8];
-    int run_cell = -1, run_t = 0;
-    unsigned run_cnt = 0u;
-    auto flush_run = [&]() {
-      const int t = run_t;
-      const int node[8] = {t, t + bx, t + bx + bxy, t + bxy, t + 1 + bxy, t + 1 + bx + bxy,
-                           t + 1 + bx, t + 1};
-      if (split) {
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          atomicAdd(tlo + node[k], (unsigned)(acc[k] & lomask));
-          atomicAdd(thi + node[k], (unsigned)(acc[k] >> IMPZ_DEP_LOBITS));
-        }
-      } else {
-#pragma unroll
-        for (int k = 0; k < 8; k++) atomicAdd(tlo + node[k], (unsigned)acc[k]);
-      }
-      atomicAdd(tcnt + t, run_cnt);
-    };
-#endif
 #pragma unroll
     for (int u = 0; u < U; u++) {
       if (cell[u] < 0) continue;
@@ -1472,21 +1443,6 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
       } else {
         const int t = mycopy + ((int)(pk[u] & 1023u) - x0) +
                       bx * (((int)((pk[u] >> 10) & 1023u) - y0) + by * ((int)(pk[u] >> 20) - z0));
-#if IMPZ_DEP_RUNS
-        if (run_cnt && cell[u] == run_cell) {
-#pragma unroll
-          for (int k = 0; k < 8; k++) acc[k] += qv[k];
-          run_cnt++;
-        } else {
-          if (run_cnt) flush_run();
-#pragma unroll
-          for (int k = 0; k < 8; k++) acc[k] = qv[k];
-          run_cell = cell[u];
-          run_t = t;
-          run_cnt = 1u;
-        }
-        continue;
-#endif
         const int node[8] = {t, t + bx, t + bx + bxy, t + bxy, t + 1 + bxy, t + 1 + bx + bxy,
                              t + 1 + bx, t + 1};
         if (split) {
@@ -1502,9 +1458,6 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
         atomicAdd(tcnt + t, 1u);
       }
     }
-#if IMPZ_DEP_RUNS
-    if (run_cnt) flush_run();
-#endif
     __syncthreads();
     if (tiled) {
       // add the copies, flush the box and clear it for the next chunk

@@ -272,17 +272,26 @@ static cudaError_t zconv_group_t(const PoissonDims& d, const PoissonMember* mem,
 }
 
 template <typename T>
-cudaError_t launch_conv_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
-                              cudaStream_t s) {
+cudaError_t launch_conv_group_forward(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                                      cudaStream_t s) {
   PoissonBuffers pb;
   pb.nx = nx; pb.ny = ny; pb.nz = nz;
   const PoissonDims d = dims_of(pb);
   cudaError_t e;
   const size_t sm = xyf_smem<T>(nx, ny, IMPZ_XY_PARTS);
   if ((e = allow_smem(k_fft_xy_fwd_group<T, IMPZ_XY_PARTS>, sm)) != cudaSuccess) return e;
-  if ((e = launch_pdl(k_fft_xy_fwd_group<T, IMPZ_XY_PARTS>, dim3(IMPZ_XY_PARTS, nz, nmem),
-                      dim3(IMPZ_XY_THREADS), sm, s, d, mem)) != cudaSuccess)
-    return e;
+  return launch_pdl(k_fft_xy_fwd_group<T, IMPZ_XY_PARTS>, dim3(IMPZ_XY_PARTS, nz, nmem),
+                    dim3(IMPZ_XY_THREADS), sm, s, d, mem);
+}
+
+// the z convolution (needs G-hat) and the inverse transform
+template <typename T>
+cudaError_t launch_conv_group_rest(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                                   cudaStream_t s) {
+  PoissonBuffers pb;
+  pb.nx = nx; pb.ny = ny; pb.nz = nz;
+  const PoissonDims d = dims_of(pb);
+  cudaError_t e;
   switch (ztile<T>(nz)) {
     case 16: e = zconv_group_t<T, 16>(d, mem, nmem, s); break;
     case 8: e = zconv_group_t<T, 8>(d, mem, nmem, s); break;
@@ -308,10 +317,26 @@ template cudaError_t launch_green_group<double>(int, int, int, const PoissonMemb
                                                 cudaStream_t);
 template cudaError_t launch_green_group<float>(int, int, int, const PoissonMember*, int,
                                                cudaStream_t);
+template <typename T>
+cudaError_t launch_conv_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
+                              cudaStream_t s) {
+  cudaError_t e = launch_conv_group_forward<T>(nx, ny, nz, mem, nmem, s);
+  if (e != cudaSuccess) return e;
+  return launch_conv_group_rest<T>(nx, ny, nz, mem, nmem, s);
+}
+
 template cudaError_t launch_conv_group<double>(int, int, int, const PoissonMember*, int,
                                                cudaStream_t);
 template cudaError_t launch_conv_group<float>(int, int, int, const PoissonMember*, int,
                                               cudaStream_t);
+template cudaError_t launch_conv_group_forward<double>(int, int, int, const PoissonMember*, int,
+                                                       cudaStream_t);
+template cudaError_t launch_conv_group_forward<float>(int, int, int, const PoissonMember*, int,
+                                                      cudaStream_t);
+template cudaError_t launch_conv_group_rest<double>(int, int, int, const PoissonMember*, int,
+                                                    cudaStream_t);
+template cudaError_t launch_conv_group_rest<float>(int, int, int, const PoissonMember*, int,
+                                                   cudaStream_t);
 template cudaError_t launch_efield_group<double>(int, int, int, const PoissonMember*, int,
                                                  cudaStream_t);
 template cudaError_t launch_efield_group<float>(int, int, int, const PoissonMember*, int,
