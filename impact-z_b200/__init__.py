@@ -27,6 +27,7 @@ STATIC_MAX_CELLS = 1 << 19
 FORM_FP64 = 0
 FORM_FP32CONV = 1
 FLAG_TRACK_IDS = 1
+FLAG_SPECIES = 2
 RAW_LEN = 44
 DIAG_LEN = 45
 MOMREC = 48
@@ -113,6 +114,9 @@ _SIGS = {
     "impz_wake_set": (ctypes.c_int, [_B, _D, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
     "impz_wake_off": (ctypes.c_int, [_B]),
     "impz_run_reference": (ctypes.c_int, [_B, _D, ctypes.c_int, _I]),
+    "impz_bunch_species": (ctypes.c_int, [_B, _D, _D, ctypes.c_int]),
+    "impz_chgupdate": (ctypes.c_int, [_B, ctypes.c_int, _D, _I]),
+    "impz_run_species": (ctypes.c_int, [_B, _I, ctypes.c_int, _I]),
     "impz_run_batch": (ctypes.c_int, [ctypes.POINTER(_B), ctypes.POINTER(_E),
                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
     "impz_run_advance_packed": (ctypes.c_int, [ctypes.POINTER(_B), ctypes.c_int, ctypes.c_int,
@@ -294,14 +298,16 @@ class Bunch:
     """A bunch resident on the GPU (BeamBunch + CompDom + FieldQuant of one rank)."""
 
     def __init__(self, pts, current, mass, charge, freq, refptcl, grid, form=FORM_FP64,
-                 track_ids=True):
+                 track_ids=True, species=False):
+        """species=True: Pts1 rows 7 (q/m) and 8 (charge weight) may differ
+        between particles (multiple charge states); otherwise they must not."""
         pts = np.ascontiguousarray(pts, dtype=np.float64)
         if pts.ndim != 2 or pts.shape[1] != 9:
             raise ValueError("pts must be (n, 9): Pts1 transposed")
         ref = np.ascontiguousarray(refptcl, dtype=np.float64)
         h = _B()
         nx, ny, nz = grid
-        flags = FLAG_TRACK_IDS if track_ids else 0
+        flags = (FLAG_TRACK_IDS if track_ids else 0) | (FLAG_SPECIES if species else 0)
         _check(lib().impz_bunch_create(_dp(pts), pts.shape[0], current, mass, charge, freq,
                                        _dp(ref), nx, ny, nz, form, flags, ctypes.byref(h)),
                "impz_bunch_create")
@@ -430,6 +436,37 @@ class Bunch:
                "impz_run_reference")
         return out[: nrec.value]
 
+    def species(self):
+        """(q/m, weight) arrays of the bunch's species (Pts1 rows 7 and 8), in
+        order of first appearance in the uploaded particles."""
+        ns = lib().impz_bunch_species(self.h, None, None, 0)
+        if ns < 0:
+            raise ImpzError(ns, "impz_bunch_species")
+        qm, w = np.zeros(ns), np.zeros(ns)
+        _check(min(0, lib().impz_bunch_species(self.h, _dp(qm), _dp(w), ns)),
+               "impz_bunch_species")
+        return qm, w
+
+    def chgupdate(self, qmcclist):
+        """chgupdate_BeamBunch: particles per charge state of qmcclist (q/m
+        within relative 1e-4) that the latest conv1st kept."""
+        q = np.ascontiguousarray(qmcclist, dtype=np.float64)
+        out = np.zeros(len(q), dtype=np.int32)
+        _check(lib().impz_chgupdate(self.h, len(q), _dp(q), out.ctypes.data_as(_I)),
+               "impz_chgupdate")
+        return out
+
+    def run_species(self):
+        """Per-species particle counts at each record of the last run,
+        shape (records, species); multi-species bunches only."""
+        ns = len(self.species()[0])
+        nrec = ctypes.c_int()
+        _check(lib().impz_run_species(self.h, None, 0, ctypes.byref(nrec)), "impz_run_species")
+        out = np.zeros((max(nrec.value, 1), ns), dtype=np.int32)
+        _check(lib().impz_run_species(self.h, out.ctypes.data_as(_I), nrec.value,
+                                      ctypes.byref(nrec)), "impz_run_species")
+        return out[: nrec.value]
+
     def bunching(self, wavenumber):
         """(1/N) sum exp(-i k z) of the live particles (complex); abs() is the
         bunching factor at wavenumber k [1/m]."""
@@ -507,11 +544,12 @@ class Bunch:
         return recs[: nrec.value], zs[: nrec.value]
 
 
-def footprint(n, grid, form=FORM_FP32CONV, track_ids=False, nsteps=0):
+def footprint(n, grid, form=FORM_FP32CONV, track_ids=False, nsteps=0, species=False):
     """Device bytes of a bunch running nsteps steps (the serving loop admits by it)."""
     nx, ny, nz = grid
     return int(lib().impz_bunch_footprint(n, nx, ny, nz, form,
-                                          FLAG_TRACK_IDS if track_ids else 0, nsteps))
+                                          (FLAG_TRACK_IDS if track_ids else 0)
+                                          | (FLAG_SPECIES if species else 0), nsteps))
 
 
 class Server:

@@ -65,6 +65,31 @@ def gaussian_bunch(n, seed=SEED0, mass=PROTON_MASS_EV, charge=1.0, ekin=2.5e6, c
     return pts, refptcl_for(ekin, mass)
 
 
+AMU_EV = 931.49410242e6
+
+
+def charge_state_bunch(nptlist, charge_states, currlist, seed=SEED0, mass_number=238,
+                       ekin_per_u=0.5e6, freq=80.5e6, **kw):
+    """An ion bunch of several charge states (Distribution.f90:1360-1367):
+    charge state j holds nptlist[j] particles with Pts1(7) = Q_j / mass and
+    Pts1(8) = currlist[j] / freq / nptlist[j] (signed like Q_j), interleaved
+    at random; the coordinates are one truncated 6D Gaussian (gaussian_bunch's
+    keywords).  The reference particle has the first charge state.  Returns
+    (pts, refptcl, mass, qmcclist)."""
+    mass = mass_number * AMU_EV
+    n = int(sum(nptlist))
+    pts, ref = gaussian_bunch(n, seed=seed, mass=mass, charge=charge_states[0],
+                              ekin=ekin_per_u * mass_number, current=1.0, freq=freq, **kw)
+    rng = np.random.Generator(np.random.Philox(key=seed + 1))
+    state = rng.permutation(np.repeat(np.arange(len(nptlist)), nptlist))
+    qmc = np.array([q / mass for q in charge_states])
+    w = np.array([c / freq / m * math.copysign(1.0, q)
+                  for c, m, q in zip(currlist, nptlist, charge_states)])
+    pts[:, 6] = qmc[state]
+    pts[:, 7] = w[state]
+    return pts, ref, mass, qmc
+
+
 def flat_top_bunch(n, seed=SEED0, mass=ELECTRON_MASS_EV, charge=-1.0, ekin=250e6 - ELECTRON_MASS_EV,
                    current=100.0, freq=1.3e9, length=1e-3, mod_amp=0.01, mod_lambda=10e-6,
                    sig_x=0.2e-3, sig_xp=0.02e-3, sig_e=5e3, trunc=4.0):

@@ -48,7 +48,32 @@ __global__ void k_aos_to_soa(const double* __restrict__ aos, long long n, double
     const double* r = aos + 9 * i;
     x[i] = r[0]; px[i] = r[1]; y[i] = r[2]; py[i] = r[3]; ph[i] = r[4]; pt[i] = r[5];
     if (ids) ids[i] = (long long)r[8];
-    if (r[6] != qm_ref || r[7] != w_ref) atomicOr(bad, 1u);
+    if (bad && (r[6] != qm_ref || r[7] != w_ref)) atomicOr(bad, 1u);
+  }
+}
+
+// multi-species upload: each particle's species index from its (q/m,
+// weight) against the table the host built from the same rows (tab: the
+// bunch's {q/m, relative weight, weight} table)
+__global__ void k_aos_species(const double* __restrict__ aos, long long n,
+                              const double* __restrict__ tab, int ns, unsigned char* spc,
+                              unsigned int* bad) {
+  __shared__ double t[2 * IMPZ_MAX_SPECIES];
+  for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+    t[k] = tab[k];
+    t[IMPZ_MAX_SPECIES + k] = tab[2 * IMPZ_MAX_SPECIES + k];
+  }
+  __syncthreads();
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double qm = aos[9 * i + 6], w = aos[9 * i + 7];
+    int k = 0;
+    while (k < ns && !(t[k] == qm && t[IMPZ_MAX_SPECIES + k] == w)) k++;
+    if (k == ns) {
+      atomicOr(bad, 1u);
+      k = 0;
+    }
+    spc[i] = (unsigned char)k;
   }
 }
 
@@ -152,7 +177,8 @@ __global__ void k_upload_count(const double* __restrict__ x, const double* __res
 // scatter to the slot of the key (cursor from the scan of the counts); lanes
 // of one key take consecutive slots with one atomic per group
 __global__ void k_upload_scatter(const double* const* in, double* const* out,
-                                 const long long* ids_in, long long* ids_out, long long n,
+                                 const long long* ids_in, long long* ids_out,
+                                 const unsigned char* spc_in, unsigned char* spc_out, long long n,
                                  const double* box_g, int nx, int ny, int nz, int* cursor,
                                  const int* bsum) {
   __shared__ double box[9];
@@ -182,18 +208,28 @@ __global__ void k_upload_scatter(const double* const* in, double* const* out,
 #pragma unroll
     for (int c = 0; c < 6; c++) out[c][dst] = v[c];
     if (ids_out) ids_out[dst] = ids_in[i];
+    if (spc_out) spc_out[dst] = spc_in[i];
   }
 }
 
+// rows 7 and 8: the bunch's (qm, w), or, with spc, the species table's
+// {q/m, Pts1(8)} of each particle (tab8: the weights in Pts1 units)
 __global__ void k_soa_to_aos(double* __restrict__ aos, long long n, long long i0, const double* x,
                              const double* px, const double* y, const double* py,
                              const double* ph, const double* pt, const long long* ids,
-                             double qm, double w) {
+                             double qm, double w, const unsigned char* spc,
+                             const double* tab7, const double* tab8) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     double* r = aos + 9 * i;
     r[0] = x[i]; r[1] = px[i]; r[2] = y[i]; r[3] = py[i]; r[4] = ph[i]; r[5] = pt[i];
-    r[6] = qm; r[7] = w;
+    if (spc) {
+      r[6] = tab7[spc[i]];
+      r[7] = tab8[spc[i]];
+    } else {
+      r[6] = qm;
+      r[7] = w;
+    }
     r[8] = ids ? (double)ids[i] : (double)(i0 + i + 1);
   }
 }
@@ -299,7 +335,8 @@ constexpr int kMaxAdvGrid = 2048;       // cap on push blocks (partial sums)
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
-  size_t pbuf[2][6], ids[2], rho, counts, cursor, bsum, spec, F, Gt, ghat, phi, efield;
+  size_t pbuf[2][6], ids[2], spc[2], sptab, rho, counts, cursor, bsum, spec, F, Gt, ghat, phi,
+      efield;
   size_t tw[3], tw64[3], st, dfine, mom_fine, mom_part, rng_part, flag;
   size_t total;
   int nscan;
@@ -322,6 +359,11 @@ Layout plan_layout(long long n, int nx, int ny, int nz, int form, int flags) {
     for (int c = 0; c < 6; c++) L.pbuf[p][c] = take(N * sizeof(double));
   for (int p = 0; p < 2; p++)
     L.ids[p] = (flags & IMPZ_FLAG_TRACK_IDS) ? take(N * sizeof(long long)) : (size_t)-1;
+  // multi-species bunches: a species index per particle and the table of
+  // each species' q/m and relative weight
+  for (int p = 0; p < 2; p++)
+    L.spc[p] = (flags & IMPZ_FLAG_SPECIES) ? take(N) : (size_t)-1;
+  L.sptab = (flags & IMPZ_FLAG_SPECIES) ? take(3 * IMPZ_MAX_SPECIES * sizeof(double)) : (size_t)-1;
   L.rho = take(G * sizeof(unsigned long long));
   L.counts = take((G + 1) * sizeof(int));
   L.cursor = take((G + 1) * sizeof(int));
@@ -357,9 +399,12 @@ int table_capacity(int entries) {
   return c;
 }
 
-size_t tables_bytes(int entries, int rows) {
+// step table, moment records and, for a multi-species bunch, the records'
+// per-species particle counts
+size_t tables_bytes(int entries, int rows, bool species) {
   return round_up((size_t)entries * sizeof(StepParams), kAlign) +
-         round_up((size_t)rows * IMPZ_MOMREC * sizeof(double), kAlign);
+         round_up((size_t)rows * IMPZ_MOMREC * sizeof(double), kAlign) +
+         (species ? round_up((size_t)rows * IMPZ_MAX_SPECIES * sizeof(int), kAlign) : 0);
 }
 
 enum Stage { ST_IDLE = 0, ST_PREPARED = 1, ST_DEPOSITED = 2, ST_SOLVED = 3 };
@@ -389,6 +434,14 @@ struct impz_bunch_s {
   unsigned int* flag = nullptr;  // scratch word for validity checks
   double* pbuf[2][6] = {{nullptr}};
   long long* ids[2] = {nullptr, nullptr};
+  // multi-species bunches (IMPZ_FLAG_SPECIES): species index per particle,
+  // the device table {q/m, weight / weight of the bunch, weight} (each
+  // IMPZ_MAX_SPECIES long), its host copy, and the per-record counts of a run
+  unsigned char* spc[2] = {nullptr, nullptr};
+  double* sptab = nullptr;
+  int nspecies = 1;
+  std::vector<double> sp_qm, sp_w;
+  int* sp_rec = nullptr;
   int parity = 0;
   unsigned long long* rho = nullptr;
   int* counts = nullptr;
@@ -517,6 +570,14 @@ AdvanceArgs advance_args(impz_bunch_t b, const StepParams* table, int fixed, int
     a.id_in = b->ids[in];
     a.id_out = kick ? b->ids[out] : nullptr;
   }
+  if (b->spc[0]) {
+    a.sp_in = b->spc[in];
+    a.sp_out = kick ? b->spc[out] : nullptr;
+    a.sp_qm = b->sptab;
+    a.nspecies = b->nspecies;
+    // the whole-lattice runner's records carry chgupdate's counts
+    a.sp_cnt = (mom_out && mom_out == b->mom_out) ? b->sp_rec : nullptr;
+  }
   a.steps = table;
   a.st = b->st;
   a.nx = b->nx; a.ny = b->ny; a.nz = b->nz;
@@ -580,6 +641,10 @@ DepositArgs deposit_args(impz_bunch_t b, const StepParams* table, int fixed) {
   d.counts = b->counts;
   d.xl = b->P.Scxl;
   d.tframe = fixed < 0 ? 1 : 0;
+  if (b->spc[0]) {
+    d.sp_in = b->spc[b->parity];
+    d.sp_w = b->sptab + IMPZ_MAX_SPECIES;
+  }
   return d;
 }
 
@@ -723,10 +788,16 @@ int ensure_tables(impz_bunch_t b, int entries, int rows) {
   b->tables = nullptr;
   b->dsteps = nullptr;
   b->mom_out = nullptr;
+  b->sp_rec = nullptr;
   b->tables_entries = b->tables_rows = 0;
-  CK(cudaMalloc((void**)&b->tables, tables_bytes(entries, rows)));
+  const bool species = (b->flags & IMPZ_FLAG_SPECIES) != 0;
+  CK(cudaMalloc((void**)&b->tables, tables_bytes(entries, rows, species)));
   b->dsteps = (StepParams*)b->tables;
-  b->mom_out = (double*)(b->tables + round_up((size_t)entries * sizeof(StepParams), kAlign));
+  const size_t moff = round_up((size_t)entries * sizeof(StepParams), kAlign);
+  b->mom_out = (double*)(b->tables + moff);
+  b->sp_rec = species ? (int*)(b->tables + moff +
+                               round_up((size_t)rows * IMPZ_MOMREC * sizeof(double), kAlign))
+                      : nullptr;
   b->tables_entries = entries;
   b->tables_rows = rows;
   return IMPZ_OK;
@@ -786,8 +857,9 @@ int upload_order(impz_bunch_t b, long long n) {
   }
   double** dcols = (double**)b->dfine;
   CK(cudaMemcpyAsync(dcols, cols, sizeof(cols), cudaMemcpyHostToDevice, b->stream));
-  k_upload_scatter<<<nb, 256, 0, b->stream>>>(dcols, dcols + 6, b->ids[0], b->ids[1], n, box,
-                                              b->nx, b->ny, b->nz, b->cursor, b->bsum);
+  k_upload_scatter<<<nb, 256, 0, b->stream>>>(dcols, dcols + 6, b->ids[0], b->ids[1], b->spc[0],
+                                              b->spc[1], n, box, b->nx, b->ny, b->nz, b->cursor,
+                                              b->bsum);
   CK(cudaGetLastError());
   g_launches += 1;
   b->parity = 1;
@@ -795,11 +867,68 @@ int upload_order(impz_bunch_t b, long long n) {
   return IMPZ_OK;
 }
 
+// The species of a multi-species bunch: the distinct (Pts1(7), Pts1(8))
+// pairs of the rows in order of first appearance (at most
+// IMPZ_MAX_SPECIES, else IMPZ_ERR_LIMIT).  The weight of largest magnitude
+// becomes the bunch's charge weight, so its species deposits whole units
+// and every other species a fraction (negative for the other sign).
+int build_species(impz_bunch_t b, const double* pts, long long n) {
+  std::vector<double> qm, w;
+  int last = -1;
+  for (long long i = 0; i < n; i++) {
+    const double q = pts[9 * i + 6], ww = pts[9 * i + 7];
+    if (last >= 0 && qm[last] == q && w[last] == ww) continue;
+    int k = 0;
+    while (k < (int)qm.size() && !(qm[k] == q && w[k] == ww)) k++;
+    if (k == (int)qm.size()) {
+      if (k == IMPZ_MAX_SPECIES) return IMPZ_ERR_LIMIT;
+      if (!std::isfinite(q) || !std::isfinite(ww)) return IMPZ_ERR_ARG;
+      qm.push_back(q);
+      w.push_back(ww);
+    }
+    last = k;
+  }
+  int kref = 0;
+  for (int k = 1; k < (int)w.size(); k++)
+    if (std::fabs(w[k]) > std::fabs(w[kref])) kref = k;
+  const double wref = w[kref];
+  if (wref == 0.0) return IMPZ_ERR_ARG;
+  std::vector<double> tab(3 * IMPZ_MAX_SPECIES, 0.0);
+  for (int k = 0; k < (int)qm.size(); k++) {
+    tab[k] = qm[k];
+    tab[IMPZ_MAX_SPECIES + k] = w[k] / wref;
+    tab[2 * IMPZ_MAX_SPECIES + k] = w[k];
+  }
+  CK(cudaMemcpyAsync(b->sptab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice,
+                     b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  // the step graphs hold the weight (field scale), q/m and the number of
+  // species by value
+  if (b->weight != wref || b->sp.qmi != qm[0] || b->nspecies != (int)qm.size())
+    for (int p = 0; p < 2; p++)
+      if (b->gexec[p]) {
+        cudaGraphExecDestroy(b->gexec[p]);
+        b->gexec[p] = nullptr;
+      }
+  b->nspecies = (int)qm.size();
+  b->sp_qm = qm;
+  b->sp_w = w;
+  b->weight = wref;
+  b->sp.qmi = qm[0];
+  b->k.qmi = qm[0];
+  return IMPZ_OK;
+}
+
 // Pts1(9,n) host array -> SoA columns of parity 0, through the staging area
 // in chunks; returns IMPZ_ERR_NONUNIFORM when a particle's charge/mass or
-// weight differs from the bunch's.
+// weight differs from the bunch's (single-species bunches).
 int upload_pts(impz_bunch_t b, const double* pts, long long n) {
   b->parity = 0;
+  const bool species = b->spc[0] != nullptr;
+  if (species) {
+    const int r = build_species(b, pts, n);
+    if (r) return r;
+  }
   long long chunk = 0;
   double* stg = staging(b, &chunk);
   CK(cudaMemsetAsync(b->flag, 0, sizeof(unsigned int), b->stream));
@@ -810,9 +939,15 @@ int upload_pts(impz_bunch_t b, const double* pts, long long n) {
     k_aos_to_soa<<<1184, 256, 0, b->stream>>>(
         stg, m, b->pbuf[0][0] + i0, b->pbuf[0][1] + i0, b->pbuf[0][2] + i0, b->pbuf[0][3] + i0,
         b->pbuf[0][4] + i0, b->pbuf[0][5] + i0, b->ids[0] ? b->ids[0] + i0 : nullptr,
-        b->sp.qmi, b->weight, b->flag);
+        b->sp.qmi, b->weight, species ? nullptr : b->flag);
     CK(cudaGetLastError());
     g_launches += 1;
+    if (species) {
+      k_aos_species<<<1184, 256, 0, b->stream>>>(stg, m, b->sptab, b->nspecies, b->spc[0] + i0,
+                                                 b->flag);
+      CK(cudaGetLastError());
+      g_launches += 1;
+    }
   }
   unsigned int hbad = 0;
   CK(cudaMemcpyAsync(&hbad, b->flag, sizeof(hbad), cudaMemcpyDeviceToHost, b->stream));
@@ -958,7 +1093,9 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
   for (int p = 0; p < 2; p++) {
     for (int c = 0; c < 6; c++) b->pbuf[p][c] = (double*)at(L.pbuf[p][c]);
     b->ids[p] = (long long*)at(L.ids[p]);
+    b->spc[p] = (unsigned char*)at(L.spc[p]);
   }
+  b->sptab = (double*)at(L.sptab);
   b->rho = (unsigned long long*)at(L.rho);
   b->counts = (int*)at(L.counts);
   b->cursor = (int*)at(L.cursor);
@@ -1032,7 +1169,7 @@ long long impz_bunch_footprint(long long n, int nx, int ny, int nz, int form, in
   long long total = (long long)round_up(L.total, kGranule);
   if (nsteps > 0) {
     const int c = table_capacity(nsteps + 2);
-    total += (long long)round_up(tables_bytes(c, c), kGranule);
+    total += (long long)round_up(tables_bytes(c, c, (flags & IMPZ_FLAG_SPECIES) != 0), kGranule);
   }
   // graph executables, events and streams of the bunch
   return total + (long long)kGranule;
@@ -1204,7 +1341,8 @@ int impz_bunch_download(impz_bunch_t b, double* pts, long long cap, long long* n
     k_soa_to_aos<<<1184, 256, 0, b->stream>>>(
         stg, m, i0, b->pbuf[p][0] + i0, b->pbuf[p][1] + i0, b->pbuf[p][2] + i0,
         b->pbuf[p][3] + i0, b->pbuf[p][4] + i0, b->pbuf[p][5] + i0,
-        b->ids[p] ? b->ids[p] + i0 : nullptr, b->sp.qmi, b->weight);
+        b->ids[p] ? b->ids[p] + i0 : nullptr, b->sp.qmi, b->weight,
+        b->spc[p] ? b->spc[p] + i0 : nullptr, b->sptab, b->sptab + 2 * IMPZ_MAX_SPECIES);
     CK(cudaGetLastError());
     g_launches += 1;
     CK(cudaMemcpyAsync(pts + 9 * i0, stg, (size_t)9 * m * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1556,7 +1694,7 @@ long long impz_kernel_launches(void) { return g_launches.load(); }
 int impz_bunch_upload(impz_bunch_t b, const double* pts, long long n, double current,
                       const double refptcl[6]) {
   if (!b || !pts || !refptcl || n < 1 || n > b->cap) return IMPZ_ERR_ARG;
-  if (pts[6] != b->sp.qmi || pts[7] != b->weight) return IMPZ_ERR_NONUNIFORM;
+  if (!b->spc[0] && (pts[6] != b->sp.qmi || pts[7] != b->weight)) return IMPZ_ERR_NONUNIFORM;
   CK(cudaSetDevice(b->device));
   const int rc = upload_pts(b, pts, n);
   DevState hs;
@@ -1699,6 +1837,8 @@ static int run_begin(impz_bunch_t b, const impz_elem_t* elems, int nelem) {
   b->run_light = table_is_light(L.steps);
   if ((r = ensure_tables(b, K + 2, K + 1))) return r;
   if ((r = upload_lz_data(b, L.lz_data))) return r;
+  if (b->sp_rec)  // every pass adds its blocks' counts to its record row
+    CK(cudaMemsetAsync(b->sp_rec, 0, (size_t)(K + 1) * b->nspecies * sizeof(int), b->stream));
   CK(cudaMemcpyAsync(b->dsteps, L.steps.data(), (K + 2) * sizeof(StepParams),
                      cudaMemcpyHostToDevice, b->stream));
   // the device step counter drives every launch: 0 is the prologue (initial
@@ -1803,8 +1943,11 @@ static int run_batch_packed(impz_bunch_t* bs, int nb) {
   const impz_bunch_t b0 = bs[0];
   cudaStream_t s = b0->stream, s2 = b0->stream2;
   const bool f32 = b0->f32();
-  bool light = true;
-  for (int i = 0; i < nb; i++) light = light && bs[i]->run_light;
+  bool light = true, species = false;  // species: a member carries the species column
+  for (int i = 0; i < nb; i++) {
+    light = light && bs[i]->run_light;
+    species = species || bs[i]->spc[0] != nullptr;
+  }
   // the prologues ran on the bunches' own streams
   for (int i = 1; i < nb; i++) {
     CK(cudaEventRecord(bs[i]->ev_dep, bs[i]->stream));
@@ -1908,8 +2051,9 @@ static int run_batch_packed(impz_bunch_t* bs, int nb) {
         if (e != cudaSuccess) return e;
       }
       if ((e = cudaEventRecord(b0->ev_join, s2)) != cudaSuccess) return e;
-      e = f32 ? fast::launch_deposit_packed(d_dep + (size_t)p * nb, d_do, nb, n_dep, s)
-              : exact::launch_deposit_packed(d_dep + (size_t)p * nb, d_do, nb, n_dep, s);
+      e = f32 ? fast::launch_deposit_packed(d_dep + (size_t)p * nb, d_do, nb, n_dep, species, s)
+              : exact::launch_deposit_packed(d_dep + (size_t)p * nb, d_do, nb, n_dep, species,
+                                             s);
       if (e != cudaSuccess) return e;
       if ((e = exact::launch_scan_packed(d_scn, d_so, nb, n_scan, s)) != cudaSuccess) return e;
       for (const BatchGroup& g : groups) {
@@ -1930,8 +2074,8 @@ static int run_batch_packed(impz_bunch_t* bs, int nb) {
       g_launches += nlaunch_sc - 1;
     }
     const AdvanceArgs* a = d_adv + (size_t)(sc ? p : 2 + p) * nb;
-    e = f32 ? fast::launch_advance_packed(a, d_ao, nb, n_adv, true, light, s)
-            : exact::launch_advance_packed(a, d_ao, nb, n_adv, false, light, s);
+    e = f32 ? fast::launch_advance_packed(a, d_ao, nb, n_adv, true, light, species, s)
+            : exact::launch_advance_packed(a, d_ao, nb, n_adv, false, light, species, s);
     g_launches += 1;
     return e;
   };
@@ -1999,9 +2143,11 @@ static size_t packed_scratch_bytes(int nb) {
 static int packed_step(impz_bunch_t* bs, int nb, cudaStream_t s, cudaStream_t s2,
                        cudaEvent_t evf, cudaEvent_t evj, char* dscratch, bool f32, bool light) {
   std::vector<impz_bunch_t> mem_b, sc_b;
+  bool species = false;  // a member carries the species column
   for (int i = 0; i < nb; i++) {
     impz_bunch_t b = bs[i];
     if (b->run_next > b->lat.nsteps) continue;
+    species = species || b->spc[0] != nullptr;
     mem_b.push_back(b);
     if (b->lat.steps[b->run_next].sc) sc_b.push_back(b);
   }
@@ -2077,8 +2223,8 @@ static int packed_step(impz_bunch_t* bs, int nb, cudaStream_t s, cudaStream_t s2
     CK(cudaEventRecord(evj, s2));
     const DepositArgs* d_dep = (const DepositArgs*)(dscratch + o_dep);
     const int* d_do = (const int*)(dscratch + o_do);
-    e = f32 ? fast::launch_deposit_packed(d_dep, d_do, ns, dep_offs[ns], s)
-            : exact::launch_deposit_packed(d_dep, d_do, ns, dep_offs[ns], s);
+    e = f32 ? fast::launch_deposit_packed(d_dep, d_do, ns, dep_offs[ns], species, s)
+            : exact::launch_deposit_packed(d_dep, d_do, ns, dep_offs[ns], species, s);
     if (e != cudaSuccess) return cuda_fail(e, "packed step: deposit");
     e = exact::launch_scan_packed((const ScanArgs*)(dscratch + o_scn),
                                   (const int*)(dscratch + o_so), ns, scan_offs[ns], s);
@@ -2101,10 +2247,10 @@ static int packed_step(impz_bunch_t* bs, int nb, cudaStream_t s, cudaStream_t s2
   }
   e = f32 ? fast::launch_advance_packed((const AdvanceArgs*)(dscratch + o_adv),
                                         (const int*)(dscratch + o_ao), nm, adv_offs[nm], true,
-                                        light, s)
+                                        light, species, s)
           : exact::launch_advance_packed((const AdvanceArgs*)(dscratch + o_adv),
                                          (const int*)(dscratch + o_ao), nm, adv_offs[nm], false,
-                                         light, s);
+                                         light, species, s);
   if (e != cudaSuccess) return cuda_fail(e, "packed step: particle pass");
   g_launches += 1;
   for (impz_bunch_t b : mem_b) {
@@ -2217,6 +2363,87 @@ int impz_run_fetch(impz_bunch_t b, double* recs, double* zs, int maxrec, int* nr
   return check_err(b);
 }
 
+int impz_bunch_species(impz_bunch_t b, double* qm, double* weight, int cap) {
+  if (!b || cap < 0 || (cap > 0 && (!qm || !weight))) return IMPZ_ERR_ARG;
+  if (!b->spc[0]) {
+    if (cap > 0) {
+      qm[0] = b->sp.qmi;
+      weight[0] = b->weight;
+    }
+    return 1;
+  }
+  for (int k = 0; k < std::min(cap, b->nspecies); k++) {
+    qm[k] = b->sp_qm[k];
+    weight[k] = b->sp_w[k];
+  }
+  return b->nspecies;
+}
+
+// chgupdate's matching rule (BeamBunch.f90:700-708): a species counts for
+// charge state j when |(q/m - qmcclist(j)) / qmcclist(j)| < eps, eps the
+// default-real literal 1.0e-4
+static void charge_states(impz_bunch_t b, const long long* per_species, int nchge,
+                          const double* qmcclist, int* idchg) {
+  const double eps = (double)1.0e-4f;
+  for (int j = 0; j < nchge; j++) {
+    long long c = 0;
+    for (int k = 0; k < b->nspecies; k++) {
+      const double q = b->spc[0] ? b->sp_qm[k] : b->sp.qmi;
+      const double dd = std::fabs((q - qmcclist[j]) / qmcclist[j]);
+      if (dd < eps) c += per_species[k];
+    }
+    idchg[j] = (int)c;
+  }
+}
+
+int impz_chgupdate(impz_bunch_t b, int nchge, const double* qmcclist, int* idchg) {
+  if (!b || nchge < 1 || !qmcclist || !idchg) return IMPZ_ERR_ARG;
+  for (int j = 0; j < nchge; j++)
+    if (qmcclist[j] == 0.0) return IMPZ_ERR_ARG;
+  CK(cudaSetDevice(b->device));
+  // the counts land in the idle particle buffer (free between calls: the
+  // next kick writes it)
+  int* dcnt = (int*)b->pbuf[b->parity ^ 1][0];
+  CK(cudaMemsetAsync(dcnt, 0, (size_t)b->nspecies * sizeof(int), b->stream));
+  // between impz_sc_prepare and the kick conv1st's losses are not yet
+  // removed: the loss test of the prepared step decides, as in the deposit
+  const bool prepared = b->stage != ST_IDLE;
+  if (prepared) {
+    StepParams h[2];
+    blank_steps(h);
+    h[0].gam = b->sc_gam;
+    h[0].rad = b->sc_rad;
+    const int r = upload_fine(b, h);
+    if (r) return r;
+  }
+  const DepositArgs d = deposit_args(b, b->dfine, 0);
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  CK(exact::launch_species_count(d, prepared ? 1 : 0, b->nspecies, dcnt, sms * 4, b->stream));
+  g_launches += 1;
+  std::vector<int> h(b->nspecies);
+  CK(cudaMemcpyAsync(h.data(), dcnt, h.size() * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  std::vector<long long> per(h.begin(), h.end());
+  charge_states(b, per.data(), nchge, qmcclist, idchg);
+  return IMPZ_OK;
+}
+
+int impz_run_species(impz_bunch_t b, int* counts, int maxrec, int* nrec) {
+  if (!b || maxrec < 0 || (maxrec > 0 && !counts)) return IMPZ_ERR_ARG;
+  if (!b->sp_rec) return IMPZ_ERR_STATE;
+  CK(cudaSetDevice(b->device));
+  const int rows = b->lat.nsteps + 1;
+  const int ncopy = std::min(rows, maxrec);
+  if (ncopy > 0)
+    CK(cudaMemcpyAsync(counts, b->sp_rec, (size_t)ncopy * b->nspecies * sizeof(int),
+                       cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  if (nrec) *nrec = rows;
+  return IMPZ_OK;
+}
+
 int impz_run_reference(impz_bunch_t b, double* refrec, int maxrec, int* nrec) {
   if (!b) return IMPZ_ERR_ARG;
   const int rows = (int)(b->lat.refrec.size() / 6);
@@ -2261,12 +2488,15 @@ int impz_autotune(impz_bunch_t b, int nsteps, double out[4]) {
   const int ncol = b->ids[0] ? 7 : 6;
   char* snap = nullptr;
   const size_t col_bytes = (size_t)n * sizeof(double);
-  cudaError_t ce = cudaMalloc(&snap, ncol * col_bytes);
+  const size_t sp_bytes = b->spc[0] ? (size_t)n : 0;  // species indices after the columns
+  cudaError_t ce = cudaMalloc(&snap, ncol * col_bytes + sp_bytes);
   if (ce != cudaSuccess) return ce == cudaErrorMemoryAllocation ? IMPZ_ERR_NOMEM : cuda_fail(ce, "cudaMalloc");
   const int par0 = b->parity;
   for (int c = 0; c < 6; c++)
     CK(cudaMemcpy(snap + c * col_bytes, b->pbuf[par0][c], col_bytes, cudaMemcpyDeviceToDevice));
   if (ncol == 7) CK(cudaMemcpy(snap + 6 * col_bytes, b->ids[par0], col_bytes, cudaMemcpyDeviceToDevice));
+  if (sp_bytes)
+    CK(cudaMemcpy(snap + ncol * col_bytes, b->spc[par0], sp_bytes, cudaMemcpyDeviceToDevice));
   double ref0[6];
   std::memcpy(ref0, b->refptcl, sizeof(ref0));
   const double z0 = b->z;
@@ -2277,6 +2507,8 @@ int impz_autotune(impz_bunch_t b, int nsteps, double out[4]) {
     for (int c = 0; c < 6; c++)
       CK(cudaMemcpy(b->pbuf[par0][c], snap + c * col_bytes, col_bytes, cudaMemcpyDeviceToDevice));
     if (ncol == 7) CK(cudaMemcpy(b->ids[par0], snap + 6 * col_bytes, col_bytes, cudaMemcpyDeviceToDevice));
+    if (sp_bytes)
+      CK(cudaMemcpy(b->spc[par0], snap + ncol * col_bytes, sp_bytes, cudaMemcpyDeviceToDevice));
     CK(cudaMemcpy(b->st, &hs, sizeof(hs), cudaMemcpyHostToDevice));
     std::memcpy(b->refptcl, ref0, sizeof(ref0));
     b->z = z0;

@@ -172,7 +172,7 @@ struct AdvanceArgs {
   const StepParams* steps;
   DevState* st;
   int nx, ny, nz;
-  int pad0;
+  int nspecies;             // species of a multi-species bunch (sp_in set), else 0
   long long cap;            // particle capacity of the output buffer
   const void* efield;       // per node {Ex,Ey,Ez,0}: double in the FP64 form, float otherwise
   double efield_scale;      // FP32 form: charge weight (field solved for unit charges)
@@ -191,6 +191,12 @@ struct AdvanceArgs {
                             //    a kick reads it, a pass with range_next writes it
   const double* wake_raw;   // per-plane wake {Ex,Ey,Ez}[nz] of a Lorentz step (kick2wake), or null
   const double* lz_data;    // field data of the Lorentz kicks (LZ_EMFLD planes), or null
+  // multi-species bunches (Pts1 rows 7 and 8 differ between particles):
+  // each particle's species index, permuted with the sort like the ids
+  const unsigned char* sp_in;  // null for a single-species bunch
+  unsigned char* sp_out;
+  const double* sp_qm;      // [IMPZ_MAX_SPECIES] Pts1(7) of each species
+  int* sp_cnt;              // [records][nspecies] particles kept per species (chgupdate), or null
 };
 
 struct DepositArgs {
@@ -204,6 +210,8 @@ struct DepositArgs {
   unsigned long long* rho;  // G int64 (two's complement) accumulators
   int* counts;              // G+1 per-cell particle counts (slot G: live but outside)
   double xl;
+  const unsigned char* sp_in;  // species index per particle (multi-species bunches), or null
+  const double* sp_w;       // [IMPZ_MAX_SPECIES] Pts1(8) of each species / the bunch's weight
 };
 
 // Read-in wakefield of type -41 elements: the line density (and, with the
@@ -256,6 +264,9 @@ struct ScanArgs {
   DevState* st;
 };
 
+#ifndef IMPZ_MAX_SPECIES
+#define IMPZ_MAX_SPECIES 128   // distinct (q/m, weight) pairs of a multi-species bunch
+#endif
 #define IMPZ_SCAN_LOG 12      // 4096 cells per scan block (1024 threads x 4)
 #ifndef IMPZ_DEP_TILE
 #define IMPZ_DEP_TILE 4096    // deposit tile entries: two int32 halves + an int32 count (48 KB)

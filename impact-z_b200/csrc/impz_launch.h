@@ -60,12 +60,15 @@ inline cudaError_t launch_pdl(void (*kernel)(KP...), dim3 grid, dim3 block, size
                           DevState* st, cudaStream_t s);                                 \
   int max_blocks_advance(bool f32);                                                      \
   cudaError_t launch_advance_packed(const AdvanceArgs* args, const int* offs, int nmem,  \
-                                    int blocks, bool f32, bool light, cudaStream_t s);   \
+                                    int blocks, bool f32, bool light, bool species,      \
+                                    cudaStream_t s);                                     \
   cudaError_t launch_deposit_packed(const DepositArgs* args, const int* offs, int nmem,  \
-                                    int blocks, cudaStream_t s);                          \
+                                    int blocks, bool species, cudaStream_t s);            \
   cudaError_t launch_scan_packed(const ScanArgs* args, const int* offs, int nmem, int blocks, \
                                  cudaStream_t s);                                         \
   int max_blocks_deposit();                                                              \
+  cudaError_t launch_species_count(const DepositArgs& a, int test_loss, int nspecies,    \
+                                   int* counts, int grid, cudaStream_t s);               \
   }
 IMPZ_DECLARE_PARTICLE_LAUNCHERS(exact)
 IMPZ_DECLARE_PARTICLE_LAUNCHERS(fast)

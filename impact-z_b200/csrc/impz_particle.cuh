@@ -110,10 +110,12 @@ __device__ __forceinline__ void map_xm2(Particle& p, const volatile double* c) {
   p.pt = (0.0 + z * c[10]) + pz * c[11];
 }
 
-__device__ __forceinline__ void map_kquad(Particle& p, const volatile double* c) {
+// qmi: the particle's Pts1(7) (pts(7,i) of the loop; c[7] holds the bunch's)
+__device__ __forceinline__ void map_kquad(Particle& p, const volatile double* c,
+                                          const double qmi) {
   // Quadrupole.f90:526-600; c = {refpt6, gambet0, beta0, qmass, K, tau, Scxl, qmi}
   const double refpt6 = c[0], gambet0 = c[1], beta0 = c[2], qmass = c[3], K = c[4];
-  const double tau = c[5], Scxl = c[6], qmi = c[7];
+  const double tau = c[5], Scxl = c[6];
   double gam = -refpt6 - p.pt;
   double gambetz = sqrt(((gam * gam - 1.0) - p.px * p.px) - p.py * p.py);
   double betaz = gambetz / gam;
@@ -211,12 +213,13 @@ __device__ __forceinline__ void map_idealrf(Particle& p, const volatile double* 
 
 // Fpol_Dipole / Bpol_Dipole (Dipole.f90:488-524, 551-589).
 // c = {h0, h1, tanphi, tanphib, k1, psi, tanphi2, secphi2, secphi3,
-//      secphib2, beta0, gambet, gam0, qm0, qmi, Scxl}
+//      secphib2, beta0, gambet, gam0, qm0, qmi, Scxl}; the particle's own
+// Pts1(7) is passed as qmi (c[14] holds the bunch's)
 template <bool EXIT>
-__device__ __forceinline__ void map_pole(Particle& p, const volatile double* c) {
+__device__ __forceinline__ void map_pole(Particle& p, const volatile double* c, const double qmi) {
   const double h0 = c[0], h1 = c[1], tanphi = c[2], tanphib = c[3], k1 = c[4], psi = c[5];
   const double tanphi2 = c[6], secphi2 = c[7], secphi3 = c[8], secphib2 = c[9];
-  const double beta0 = c[10], gambet = c[11], gam0 = c[12], qm0 = c[13], qmi = c[14];
+  const double beta0 = c[10], gambet = c[11], gam0 = c[12], qm0 = c[13];
   const double Scxl = c[15];
   double x = p.x * Scxl;
   double gamn = gam0 - p.pt;
@@ -261,15 +264,17 @@ __device__ __forceinline__ void map_pole(Particle& p, const volatile double* c) 
 // Sector_Dipole second-order map (Dipole.f90:745-786).
 // c = {R11,R12,R16,R21,R22,R26,R51,R52,R56, T111,T112,T116,T122,T126,T166,
 //      T144,T216,T222,T266,T244,T314,T324,T346,T522,T544,T526,
-//      len, beta0, gambet, gam0, qm0, qmi, Scxl}
-__device__ __forceinline__ void map_sector(Particle& p, const volatile double* c) {
+//      len, beta0, gambet, gam0, qm0, qmi, Scxl}; the particle's own Pts1(7)
+// is passed as qmi (c[31] holds the bunch's)
+__device__ __forceinline__ void map_sector(Particle& p, const volatile double* c,
+                                           const double qmi) {
   const double R11 = c[0], R12 = c[1], R16 = c[2], R21 = c[3], R22 = c[4], R26 = c[5];
   const double R51 = c[6], R52 = c[7], R56 = c[8];
   const double T111 = c[9], T112 = c[10], T116 = c[11], T122 = c[12], T126 = c[13];
   const double T166 = c[14], T144 = c[15], T216 = c[16], T222 = c[17], T266 = c[18];
   const double T244 = c[19], T314 = c[20], T324 = c[21], T346 = c[22], T522 = c[23];
   const double T544 = c[24], T526 = c[25], len = c[26], beta0 = c[27], gambet = c[28];
-  const double gam0 = c[29], qm0 = c[30], qmi = c[31], Scxl = c[32];
+  const double gam0 = c[29], qm0 = c[30], Scxl = c[32];
   double gami = -p.pt + gam0;
   double gambeti = sqrt(gami * gami - 1.0);
   double gambetz = sqrt((gambeti * gambeti - p.px * p.px) - p.py * p.py);
@@ -302,8 +307,10 @@ __device__ __forceinline__ void map_sector(Particle& p, const volatile double* c
 // drift/quadrupole lattices); the host picks that instantiation when every
 // step of a run qualifies, which keeps the other map kinds' code and
 // registers out of the particle pass.
+// qmi: the particle's Pts1(7), read by the K-map and the bend maps.
 template <bool LIGHT>
-__device__ __forceinline__ void apply_program(Particle& p, const volatile MapProgram& prog) {
+__device__ __forceinline__ void apply_program(Particle& p, const volatile MapProgram& prog,
+                                              const double qmi) {
   const int nops = prog.nops;
   for (int o = 0; o < nops; o++) {
     const volatile MapOp& op = prog.ops[o];
@@ -315,11 +322,11 @@ __device__ __forceinline__ void apply_program(Particle& p, const volatile MapPro
     switch (op.kind) {
       case MAP_DRIFT: map_drift(p, op.c); break;
       case MAP_XM6: map_xm6(p, op.c, op.flags, op.iparam); break;
-      case MAP_KQUAD: map_kquad(p, op.c); break;
+      case MAP_KQUAD: map_kquad(p, op.c, qmi); break;
       case MAP_IDEALRF: map_idealrf(p, op.c, op.flags, op.iparam); break;
-      case MAP_FPOL: map_pole<false>(p, op.c); break;
-      case MAP_BPOL: map_pole<true>(p, op.c); break;
-      case MAP_SECTOR: map_sector(p, op.c); break;
+      case MAP_FPOL: map_pole<false>(p, op.c, qmi); break;
+      case MAP_BPOL: map_pole<true>(p, op.c, qmi); break;
+      case MAP_SECTOR: map_sector(p, op.c, qmi); break;
       case MAP_XM2: map_xm2(p, op.c); break;
       case MAP_UNDUL: map_undul(p, op.c); break;
       case MAP_DRIFT2: map_drift2(p, op.c); break;
@@ -845,10 +852,12 @@ __device__ __forceinline__ void lz_field(int kind, const double* __restrict__ c,
 // units] plus the step's element field (lz_*) and scatter2wake's wake at
 // the particle (wx, wy, wz; BeamBunch.f90:5885-5887); with no current
 // (scatter20, BeamBunch.f90:3478-3531) the space-charge field is zero.
+// r7 is the particle's own Pts1(7) (rays(7,n)); qmcc stays the bunch's.
 __device__ __forceinline__ void lorentz_kick(Particle& p, double exn, double eyn, double ezn,
                                              double gam, const StepParams* __restrict__ sp,
                                              const Consts& k, double wx, double wy,
-                                             double wz, const double* __restrict__ lz_data) {
+                                             double wz, const double* __restrict__ lz_data,
+                                             const double r7) {
   const double xl = k.Scxl, Clight = k.Clight;
   const double tau = sp->tau;
   const double tmpscale = Clight * Clight * 1.00000001168609742e-07;
@@ -865,7 +874,6 @@ __device__ __forceinline__ void lorentz_kick(Particle& p, double exn, double eyn
   const double bx = -(beta0 / Clight * tmpscale * eyn) + ext4;
   const double by = beta0 / Clight * tmpscale * exn + ext5;
   const double bz = ext6;
-  const double r7 = k.qmi;
   const double tmp12 = -tau * Clight * bz * r7 / 2;
   const double tmp13 = tau * ex * r7 / 2;
   const double tmp23 = tau * ey * r7 / 2;
@@ -899,7 +907,9 @@ __device__ __forceinline__ void lorentz_kick(Particle& p, double exn, double eyn
 // The pass of one bunch as block vbx of a grid of vgx blocks: k_advance
 // runs it for one bunch (vbx = vbx), k_advance_packed for the bunch
 // that owns the block in a launch over many.
-template <int BLOCK, bool F32, int U, bool LIGHT>
+// SP: the instantiation for multi-species bunches (the species column, each
+// particle's q/m and the per-species counts); without it that code is absent.
+template <int BLOCK, bool F32, int U, bool LIGHT, bool SP>
 __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx, const int vgx) {
   __shared__ double red[BLOCK / 32][IMPZ_RAW_LEN];
   __shared__ double redr[BLOCK / 32][8];
@@ -908,6 +918,7 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
   __shared__ MapProgram progs[2];  // post, pre_next
   extern __shared__ __align__(16) double mtile_dyn[];  // [BLOCK/32][32*IMPZ_MSUMS]
   __shared__ Geom sgeom;
+  __shared__ int s_spc[IMPZ_MAX_SPECIES];  // particles kept per species (multi-species bunches)
   griddep_wait();  // step state, geometry and field come from earlier kernels
   DevState* st = a.st;
   const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
@@ -916,6 +927,9 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
   static_assert(offsetof(StepParams, pre_next) == sizeof(MapProgram), "program layout");
   stage_programs(progs, sp);
   if (threadIdx.x == 0) sgeom = st->geom;
+  const bool species = SP && a.sp_in != nullptr;
+  if (SP)
+    for (int t = threadIdx.x; t < a.nspecies; t += BLOCK) s_spc[t] = 0;
   __syncthreads();
   // the geometry lives in registers for the whole pass (a volatile shared
   // reference re-read it per particle: 5 % slower)
@@ -970,6 +984,7 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
     Particle p[U];
     bool keep[U];
     int key[U];  // deposit cell (a grid holds at most 64 x 64 x 4096 nodes)
+    int spi[U];  // species index (0 for a single-species bunch)
 #if !IMPZ_ADV_PREFETCH
     fetch(i0);
 #endif
@@ -979,6 +994,7 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
       keep[u] = i < n;
       key[u] = 0;
       p[u] = nxt[u];
+      spi[u] = (species && keep[u]) ? (int)a.sp_in[i] : 0;
     }
 #if IMPZ_ADV_PREFETCH
     if (i0 + stride < nround) fetch(i0 + stride);
@@ -1044,7 +1060,8 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
               wy = w[nz] * cg.ef + w[nz + 1] * (1.0 - cg.ef);
               wz = w[2 * nz] * cg.ef + w[2 * nz + 1] * (1.0 - cg.ef);
             }
-            lorentz_kick(p[u], exn, eyn, ezn, gam, sp, a.k, wx, wy, wz, a.lz_data);
+            lorentz_kick(p[u], exn, eyn, ezn, gam, sp, a.k, wx, wy, wz, a.lz_data,
+                         species ? __ldg(a.sp_qm + spi[u]) : a.k.qmi);
           } else {
             p[u].px = p[u].px + txy * exn;
             p[u].py = p[u].py + txy * eyn;
@@ -1056,8 +1073,10 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
       // the element's field alone, on the stored coordinates
       // (BeamBunch.f90:3075-3531)
       if (!LIGHT && keep[u] && !kick && post && sp->lorentz)
-        lorentz_kick(p[u], 0.0, 0.0, 0.0, gam, sp, a.k, 0.0, 0.0, 0.0, a.lz_data);
-      if (keep[u] && post) apply_program<LIGHT>(p[u], progs[0]);
+        lorentz_kick(p[u], 0.0, 0.0, 0.0, gam, sp, a.k, 0.0, 0.0, 0.0, a.lz_data,
+                     species ? __ldg(a.sp_qm + spi[u]) : a.k.qmi);
+      if (keep[u] && post)
+        apply_program<LIGHT>(p[u], progs[0], species ? __ldg(a.sp_qm + spi[u]) : a.k.qmi);
       if (keep[u]) {
         c[u].x = p[u].x; c[u].px = p[u].px; c[u].y = p[u].y;
         c[u].py = p[u].py; c[u].z = p[u].ph; c[u].pz = p[u].pt;
@@ -1069,9 +1088,11 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
 #pragma unroll
     for (int u = 0; u < U; u++) {
       if (keep[u]) {
-        if (pre) apply_program<LIGHT>(p[u], progs[1]);
+        if (pre)
+          apply_program<LIGHT>(p[u], progs[1], species ? __ldg(a.sp_qm + spi[u]) : a.k.qmi);
         if (!finite6(p[u])) err |= DERR_NONFINITE;
         nkept++;
+        if (SP && a.sp_cnt) atomicAdd(&s_spc[spi[u]], 1);
         if (rng) {
           const TFrame t = to_tframe(p[u], gam_n, rad_n, xl);
           rmn[0] = fmin(rmn[0], fmin(t.tmpx, t.xt));
@@ -1110,6 +1131,7 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
         a.out[0][dst] = p[u].x; a.out[1][dst] = p[u].px; a.out[2][dst] = p[u].y;
         a.out[3][dst] = p[u].py; a.out[4][dst] = p[u].ph; a.out[5][dst] = p[u].pt;
         if (a.id_out) a.id_out[dst] = a.id_in[i0 + (long long)u * BLOCK];
+        if (species && a.sp_out) a.sp_out[dst] = (unsigned char)spi[u];
       }
     }
   }
@@ -1141,6 +1163,13 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
     if (err) atomicOr(&st->err, err);
   }
   __syncthreads();
+  // chgupdate_BeamBunch's count of each charge state (BeamBunch.f90:688-728)
+  // after this step's conv1st: integer sums, so the block order is immaterial
+  if (SP && a.sp_cnt) {
+    int* cnt = a.sp_cnt + (size_t)(a.fixed_step >= 0 ? a.mom_index : s) * a.nspecies;
+    for (int t = threadIdx.x; t < a.nspecies; t += BLOCK)
+      if (s_spc[t]) atomicAdd(cnt + t, s_spc[t]);
+  }
   const int nw = BLOCK / 32;
   if (mom && threadIdx.x < IMPZ_RAW_LEN) {
     const int v = threadIdx.x;
@@ -1231,9 +1260,9 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
   }
 }
 
-template <int BLOCK, bool F32, int U, bool LIGHT>
+template <int BLOCK, bool F32, int U, bool LIGHT, bool SP>
 __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB) k_advance(AdvanceArgs a) {
-  advance_pass<BLOCK, F32, U, LIGHT>(a, blockIdx.x, gridDim.x);
+  advance_pass<BLOCK, F32, U, LIGHT, SP>(a, blockIdx.x, gridDim.x);
 }
 
 // The member of a packed launch that owns block `blk`: blocks
@@ -1258,7 +1287,7 @@ __device__ __forceinline__ void copy_args(void* dst, const void* src, int bytes)
 
 // Every member's pass in one launch: a packed work list of (bunch, block)
 // items, each bunch keeping its own block count and last-block reduction.
-template <int BLOCK, bool F32, int U, bool LIGHT>
+template <int BLOCK, bool F32, int U, bool LIGHT, bool SP>
 __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB)
     k_advance_packed(const AdvanceArgs* __restrict__ args, const int* __restrict__ offs,
                      int nmem) {
@@ -1267,7 +1296,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB)
   const int m = packed_member(offs, nmem, blockIdx.x);
   copy_args(&sa, args + m, (int)sizeof(AdvanceArgs));
   __syncthreads();
-  advance_pass<BLOCK, F32, U, LIGHT>(sa, blockIdx.x - __ldg(offs + m),
+  advance_pass<BLOCK, F32, U, LIGHT, SP>(sa, blockIdx.x - __ldg(offs + m),
                                      __ldg(offs + m + 1) - __ldg(offs + m));
 }
 
@@ -1299,7 +1328,7 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_ADV_MINB)
 #endif
 #define IMPZ_DEP_LOBITS 20
 #define IMPZ_DEP_FIXBITS_1WORD 21
-template <int BLOCK, int U>
+template <int BLOCK, int U, bool SP>
 __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx, const int vgx) {
   static_assert(BLOCK * U <= 1024, "one-word tile sums sized for chunks of at most 1024");
   extern __shared__ __align__(16) unsigned int tsm[];
@@ -1330,9 +1359,10 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
   const double magic = 6755399441055744.0;
   const long long magic_bits = 0x4338000000000000ll;
   const unsigned lomask = (1u << IMPZ_DEP_LOBITS) - 1u;
-  // quanta of at most 2^21 (the FP32-convolution form's resolution): a
-  // chunk's sum at one node stays below 2^31 in a single word
-  const bool split = a.fixbits > IMPZ_DEP_FIXBITS_1WORD;
+  // quanta of at most 2^21: a chunk's sum at one node stays below 2^31 in
+  // a single word (species of either sign take the two signed halves)
+  const bool species = SP && a.sp_in != nullptr;
+  const bool split = a.fixbits > IMPZ_DEP_FIXBITS_1WORD || species;
   const long long chunk = (long long)BLOCK * U;
   const int lane = threadIdx.x & 31;
   for (long long c0 = (long long)vbx * chunk; c0 < n; c0 += (long long)vgx * chunk) {
@@ -1422,17 +1452,27 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
 #pragma unroll
       for (int k = 1; k < 8; k++)
         if (w8[k] > wbig) { wbig = w8[k]; big = k; }
+      // a particle of relative weight ws deposits round(ws 2^f) quanta (one
+      // unit, 2^f, for the bunch's own species); two's complement for
+      // species of the other sign
+      double pscale = scale;
+      unsigned long long punit = unit;
+      if (species) {  // the particle's charge weight relative to the bunch's
+        const double ws = __ldg(a.sp_w + a.sp_in[c0 + (long long)u * BLOCK + threadIdx.x]);
+        pscale = __dmul_rn(ws, scale);
+        punit = (unsigned long long)(__double_as_longlong(__dadd_rn(pscale, magic)) - magic_bits);
+      }
       unsigned long long qv[8];
       unsigned long long sum7 = 0;
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        const double sh = __dadd_rn(__dmul_rn(w8[k], scale), magic);
+        const double sh = __dadd_rn(__dmul_rn(w8[k], pscale), magic);
         qv[k] = (k == big) ? 0ull : (unsigned long long)(__double_as_longlong(sh) - magic_bits);
         sum7 += qv[k];
       }
 #pragma unroll
       for (int k = 0; k < 8; k++)
-        if (k == big) qv[k] = unit - sum7;
+        if (k == big) qv[k] = punit - sum7;
       if (!tiled) {
         const long long c = cell[u];
         const long long node[8] = {c, c + nx, c + nx + P, c + P, c + 1 + P, c + 1 + nx + P,
@@ -1449,7 +1489,7 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
 #pragma unroll
           for (int k = 0; k < 8; k++) {
             atomicAdd(tlo + node[k], (unsigned)(qv[k] & lomask));
-            atomicAdd(thi + node[k], (unsigned)(qv[k] >> IMPZ_DEP_LOBITS));
+            atomicAdd(thi + node[k], (unsigned)((long long)qv[k] >> IMPZ_DEP_LOBITS));
           }
         } else {
 #pragma unroll
@@ -1467,7 +1507,9 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
         for (int r = 0, o = e; r < R; r++, o += S) {
           const unsigned lo = tlo[o], hi = split ? thi[o] : 0u, c = tcnt[o];
           if (lo | hi | c) {
-            q += ((unsigned long long)hi << IMPZ_DEP_LOBITS) + (unsigned long long)lo;
+            // the high half is signed (a negative quantum's arithmetic shift)
+            q += ((unsigned long long)(long long)(int)hi << IMPZ_DEP_LOBITS) +
+                 (unsigned long long)lo;
             k += c;
             tlo[o] = 0u;
             if (split) thi[o] = 0u;
@@ -1488,12 +1530,12 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
   }
 }
 
-template <int BLOCK, int U>
+template <int BLOCK, int U, bool SP>
 __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB) k_deposit(DepositArgs a) {
-  deposit_pass<BLOCK, U>(a, blockIdx.x, gridDim.x);
+  deposit_pass<BLOCK, U, SP>(a, blockIdx.x, gridDim.x);
 }
 
-template <int BLOCK, int U>
+template <int BLOCK, int U, bool SP>
 __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB)
     k_deposit_packed(const DepositArgs* __restrict__ args, const int* __restrict__ offs,
                      int nmem) {
@@ -1502,7 +1544,42 @@ __global__ void __launch_bounds__(BLOCK, IMPZ_DEP_MINB)
   const int m = packed_member(offs, nmem, blockIdx.x);
   copy_args(&sa, args + m, (int)sizeof(DepositArgs));
   __syncthreads();
-  deposit_pass<BLOCK, U>(sa, blockIdx.x - __ldg(offs + m), __ldg(offs + m + 1) - __ldg(offs + m));
+  deposit_pass<BLOCK, U, SP>(sa, blockIdx.x - __ldg(offs + m), __ldg(offs + m + 1) - __ldg(offs + m));
+}
+
+// chgupdate_BeamBunch (BeamBunch.f90:688-728) on the per-step surface: the
+// particles of each species that the latest conv1st kept.  test_loss = 1
+// between impz_sc_prepare and the kick (conv1st has run, its losses are
+// not yet removed: the deposit's loss test of the step decides), 0 when
+// every stored particle is live.  counts[nspecies] are added to.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_species_count(DepositArgs a, int test_loss,
+                                                         int nspecies, int* counts) {
+  __shared__ int hist[IMPZ_MAX_SPECIES];
+  for (int t = threadIdx.x; t < nspecies; t += BLOCK) hist[t] = 0;
+  __syncthreads();
+  const DevState* st = a.st;
+  const int s = a.fixed_step >= 0 ? a.fixed_step : st->step;
+  const double gam = a.steps[s].gam, rad = a.steps[s].rad;
+  const long long n = st->nlocal;
+  for (long long i = (long long)blockIdx.x * BLOCK + threadIdx.x; i < n;
+       i += (long long)gridDim.x * BLOCK) {
+    bool lost = false;
+    if (test_loss) {
+      if (a.tframe) {
+        lost = isnan(a.in[4][i]);
+      } else {
+        Particle p;
+        p.x = a.in[0][i]; p.px = a.in[1][i]; p.y = a.in[2][i];
+        p.py = a.in[3][i]; p.ph = a.in[4][i]; p.pt = a.in[5][i];
+        lost = to_tframe(p, gam, rad, a.xl).lost;
+      }
+    }
+    if (!lost) atomicAdd(&hist[a.sp_in ? (int)a.sp_in[i] : 0], 1);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nspecies; t += BLOCK)
+    if (hist[t]) atomicAdd(counts + t, hist[t]);
 }
 
 // Exclusive scan over the block of one value per thread; *total gets the

@@ -10,60 +10,81 @@ static const size_t kDepSmem = (size_t)3 * IMPZ_DEP_TILE * sizeof(unsigned int);
 
 static const size_t kAdvSmem = (size_t)(IMPZ_ADV_BLOCK / 32) * 32 * 37 * sizeof(double);
 
-template <bool F32, bool LIGHT>
+template <bool F32, bool LIGHT, bool SP>
 static cudaError_t adv_attr() {
   static cudaError_t once = cudaFuncSetAttribute(
-      k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT>,
+      k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT, SP>,
       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdvSmem);
   return once;
 }
 
-template <bool F32, bool LIGHT>
+template <bool F32, bool LIGHT, bool SP>
 static cudaError_t launch_adv_t(const AdvanceArgs& a, int grid, cudaStream_t s) {
-  cudaError_t e = adv_attr<F32, LIGHT>();
+  cudaError_t e = adv_attr<F32, LIGHT, SP>();
   if (e != cudaSuccess) return e;
-  return launch_pdl(k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT>, dim3(grid),
+  return launch_pdl(k_advance<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT, SP>, dim3(grid),
                     dim3(IMPZ_ADV_BLOCK), kAdvSmem, s, a);
 }
 
-cudaError_t launch_advance(const AdvanceArgs& a, bool f32, bool light, int grid, cudaStream_t s) {
-  if (f32) return light ? launch_adv_t<true, true>(a, grid, s) : launch_adv_t<true, false>(a, grid, s);
-  return light ? launch_adv_t<false, true>(a, grid, s) : launch_adv_t<false, false>(a, grid, s);
+template <bool F32, bool LIGHT>
+static cudaError_t launch_adv_sp(const AdvanceArgs& a, int grid, cudaStream_t s) {
+  return a.sp_in ? launch_adv_t<F32, LIGHT, true>(a, grid, s)
+                 : launch_adv_t<F32, LIGHT, false>(a, grid, s);
 }
 
-template <bool F32, bool LIGHT>
+cudaError_t launch_advance(const AdvanceArgs& a, bool f32, bool light, int grid, cudaStream_t s) {
+  if (f32) return light ? launch_adv_sp<true, true>(a, grid, s) : launch_adv_sp<true, false>(a, grid, s);
+  return light ? launch_adv_sp<false, true>(a, grid, s) : launch_adv_sp<false, false>(a, grid, s);
+}
+
+template <bool F32, bool LIGHT, bool SP>
 static cudaError_t launch_adv_packed_t(const AdvanceArgs* args, const int* offs, int nmem,
                                        int blocks, cudaStream_t s) {
-  auto kern = k_advance_packed<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT>;
+  auto kern = k_advance_packed<IMPZ_ADV_BLOCK, F32, IMPZ_ADV_U, LIGHT, SP>;
   static cudaError_t once =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdvSmem);
   if (once != cudaSuccess) return once;
   return launch_pdl(kern, dim3(blocks), dim3(IMPZ_ADV_BLOCK), kAdvSmem, s, args, offs, nmem);
 }
 
-cudaError_t launch_advance_packed(const AdvanceArgs* args, const int* offs, int nmem, int blocks,
-                                  bool f32, bool light, cudaStream_t s) {
-  if (f32)
-    return light ? launch_adv_packed_t<true, true>(args, offs, nmem, blocks, s)
-                 : launch_adv_packed_t<true, false>(args, offs, nmem, blocks, s);
-  return light ? launch_adv_packed_t<false, true>(args, offs, nmem, blocks, s)
-               : launch_adv_packed_t<false, false>(args, offs, nmem, blocks, s);
+template <bool F32, bool LIGHT>
+static cudaError_t launch_adv_packed_sp(const AdvanceArgs* args, const int* offs, int nmem,
+                                        int blocks, bool species, cudaStream_t s) {
+  return species ? launch_adv_packed_t<F32, LIGHT, true>(args, offs, nmem, blocks, s)
+                 : launch_adv_packed_t<F32, LIGHT, false>(args, offs, nmem, blocks, s);
 }
 
+cudaError_t launch_advance_packed(const AdvanceArgs* args, const int* offs, int nmem, int blocks,
+                                  bool f32, bool light, bool species, cudaStream_t s) {
+  if (f32)
+    return light ? launch_adv_packed_sp<true, true>(args, offs, nmem, blocks, species, s)
+                 : launch_adv_packed_sp<true, false>(args, offs, nmem, blocks, species, s);
+  return light ? launch_adv_packed_sp<false, true>(args, offs, nmem, blocks, species, s)
+               : launch_adv_packed_sp<false, false>(args, offs, nmem, blocks, species, s);
+}
+
+template <bool SP>
 static cudaError_t dep_attr() {
   static cudaError_t once = cudaFuncSetAttribute(
-      k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT, SP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
       (int)kDepSmem);
   return once;
 }
 
-cudaError_t launch_deposit_packed(const DepositArgs* args, const int* offs, int nmem, int blocks,
-                                  cudaStream_t s) {
-  auto kern = k_deposit_packed<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>;
+template <bool SP>
+static cudaError_t launch_dep_packed_t(const DepositArgs* args, const int* offs, int nmem,
+                                      int blocks, cudaStream_t s) {
+  auto kern = k_deposit_packed<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT, SP>;
   static cudaError_t once =
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
   if (once != cudaSuccess) return once;
   return launch_pdl(kern, dim3(blocks), dim3(IMPZ_DEP_BLOCK), kDepSmem, s, args, offs, nmem);
+}
+
+cudaError_t launch_deposit_packed(const DepositArgs* args, const int* offs, int nmem, int blocks,
+                                  bool species, cudaStream_t s) {
+  return species ? launch_dep_packed_t<true>(args, offs, nmem, blocks, s)
+                 : launch_dep_packed_t<false>(args, offs, nmem, blocks, s);
 }
 
 cudaError_t launch_scan_packed(const ScanArgs* args, const int* offs, int nmem, int blocks,
@@ -73,11 +94,16 @@ cudaError_t launch_scan_packed(const ScanArgs* args, const int* offs, int nmem, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s) {
-  cudaError_t e = dep_attr();
+template <bool SP>
+static cudaError_t launch_dep_t(const DepositArgs& a, int grid, cudaStream_t s) {
+  cudaError_t e = dep_attr<SP>();
   if (e != cudaSuccess) return e;
-  return launch_pdl(k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>, dim3(grid), dim3(IMPZ_DEP_BLOCK),
+  return launch_pdl(k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT, SP>, dim3(grid), dim3(IMPZ_DEP_BLOCK),
                     kDepSmem, s, a);
+}
+
+cudaError_t launch_deposit(const DepositArgs& a, int grid, cudaStream_t s) {
+  return a.sp_in ? launch_dep_t<true>(a, grid, s) : launch_dep_t<false>(a, grid, s);
 }
 
 #define IMPZ_WAKE_BLOCK 256
@@ -107,19 +133,25 @@ cudaError_t launch_scan(int* counts, int* cursor, int* bsum, long long total, De
   return cudaGetLastError();
 }
 
+cudaError_t launch_species_count(const DepositArgs& a, int test_loss, int nspecies, int* counts,
+                                 int grid, cudaStream_t s) {
+  k_species_count<256><<<grid, 256, 0, s>>>(a, test_loss, nspecies, counts);
+  return cudaGetLastError();
+}
+
 int max_blocks_advance(bool f32) {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // the full instantiation bounds the light one (at most its registers)
+  // the full multi-species instantiation bounds the others (at most its registers)
   if (f32) {
-    adv_attr<true, false>();
+    adv_attr<true, false, true>();
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per, k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U, false>, IMPZ_ADV_BLOCK, kAdvSmem);
+        &per, k_advance<IMPZ_ADV_BLOCK, true, IMPZ_ADV_U, false, true>, IMPZ_ADV_BLOCK, kAdvSmem);
   } else {
-    adv_attr<false, false>();
+    adv_attr<false, false, true>();
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per, k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U, false>, IMPZ_ADV_BLOCK, kAdvSmem);
+        &per, k_advance<IMPZ_ADV_BLOCK, false, IMPZ_ADV_U, false, true>, IMPZ_ADV_BLOCK, kAdvSmem);
   }
   return sms * (per > 0 ? per : 1);
 }
@@ -128,8 +160,8 @@ int max_blocks_deposit() {
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  dep_attr();
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT>,
+  dep_attr<true>();
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_deposit<IMPZ_DEP_BLOCK, IMPZ_DEP_PPT, true>,
                                                 IMPZ_DEP_BLOCK, kDepSmem);
   return sms * (per > 0 ? per : 1);
 }

@@ -449,8 +449,10 @@ _FILES = (("fort.18", 1, 6), ("fort.24", 6, 12), ("fort.25", 12, 18), ("fort.26"
           ("fort.27", 24, 30), ("fort.28", 30, 33), ("fort.29", 33, 39), ("fort.30", 39, 45))
 
 
-def write_diag(outdir, rows):
-    """fort.18 and fort.24-30 (diagnostic1_Output) from diag rows."""
+def write_diag(outdir, rows, charge_states=None):
+    """fort.18 and fort.24-30 (diagnostic1_Output) from diag rows, and with
+    `charge_states` (records x nchrg particle counts) fort.32: z and the
+    count of each charge state (Output.f90:352)."""
     rows = np.asarray(rows)
     for name, a, b in _FILES:
         with open(os.path.join(outdir, name), "w") as f:
@@ -459,6 +461,25 @@ def write_diag(outdir, rows):
                     f.write("%.17g %10d %10d %10d\n" % (r[0], int(r[30]), int(r[31]), int(r[32])))
                 else:
                     f.write(" ".join("%.17g" % x for x in [r[0]] + list(r[a:b])) + "\n")
+    if charge_states is not None:
+        with open(os.path.join(outdir, "fort.32"), "w") as f:
+            for r, c in zip(rows, np.asarray(charge_states)):
+                f.write("%.17g " % r[0] + " ".join("%d" % int(x) for x in c) + "\n")
+
+
+def charge_state_counts(species_qm, species_counts, qmcclist):
+    """chgupdate_BeamBunch's counts (BeamBunch.f90:700-708): for each entry
+    j of qmcclist, the particles of the species whose q/m lies within
+    relative 1e-4 (a default-real literal) of it.  species_counts has one
+    row per record and one column per species."""
+    eps = float(np.float32(1.0e-4))
+    qm = np.asarray(species_qm, dtype=np.float64)
+    cnt = np.asarray(species_counts)
+    out = np.zeros((cnt.shape[0], len(qmcclist)), dtype=np.int64)
+    for j, q in enumerate(qmcclist):
+        sel = np.abs((qm - q) / q) < eps
+        out[:, j] = cnt[:, sel].sum(axis=1)
+    return out
 
 
 def read_diag(outdir, name):
@@ -562,20 +583,21 @@ def lattice_segments(deck, workdir, skip=(), start=0):
 
 
 def check_supported(deck):
-    """The runner covers open boundaries, one charge state and a particle.in
-    distribution, with the map integrator (Flagmap=1) or the Lorentz
-    integrator (Flagmap=2, drifts and hard-edge quadrupoles)."""
-    if deck.flagmap not in (1, 2) or deck.flagbc != 1 or deck.flagdist != 19 or deck.nchrg != 1:
-        raise ValueError("this runner needs Flagmap=1 or 2, Flagbc=1, Flagdist=19 and one charge "
-                         "state (deck has %d, %d, %d, %d)" % (deck.flagmap, deck.flagbc,
-                                                             deck.flagdist, deck.nchrg))
+    """The runner covers open boundaries and a particle.in distribution
+    (any number of charge states, rows 7 and 8 per particle), with the map
+    integrator (Flagmap=1) or the Lorentz integrator (Flagmap=2)."""
+    if deck.flagmap not in (1, 2) or deck.flagbc != 1 or deck.flagdist != 19:
+        raise ValueError("this runner needs Flagmap=1 or 2, Flagbc=1 and Flagdist=19 (deck has "
+                         "%d, %d, %d)" % (deck.flagmap, deck.flagbc, deck.flagdist))
 
 
 def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
     """Runs ImpactZ.in + particle.in of `workdir` on the GPU and writes
-    fort.18/24-30 and the -2 phase dumps into `outdir` (default: workdir).
-    Returns {"rows": diag rows, "skipped": [types passed over], "pts": final
-    Pts1}."""
+    fort.18/24-30, fort.32 and the -2 phase dumps into `outdir` (default:
+    workdir).  A particle.in whose rows 7 and 8 differ between particles
+    (multiple charge states) runs as a multi-species bunch.  Returns {"rows":
+    diag rows, "charge_states": fort.32's counts, "skipped": [types passed
+    over], "pts": final Pts1}."""
     from . import FORM_FP64, Bunch, diag_row
     from .beams import scxl
     outdir = outdir or workdir
@@ -588,12 +610,18 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
         pts, ref, z0, start = ck["pts"], ck["refptcl"], ck["z"], ck["inb"]
     else:
         pts = read_particles(os.path.join(workdir, "particle.in"))
+    multi = bool(np.any(pts[:, 6] != pts[0, 6]) or np.any(pts[:, 7] != pts[0, 7]))
     b = Bunch(pts, deck.bcurr, deck.bmass, deck.bcharge, deck.bfreq, ref,
               (deck.nx, deck.ny, deck.nz), form=FORM_FP64 if form is None else form,
-              track_ids=True)
+              track_ids=True, species=multi)
     b.set_z(z0)
     b.set_integrator(deck.flagmap)
-    rows, skipped = [], []
+    rows, skipped, charges = [], [], []
+    qmcc = list(deck.qmcclist) or [float(pts[0, 6])]
+    # nptlist of the deck until the first space-charge step's chgupdate
+    # (AccSimulator.f90:155-161, 1130); every step of a run with current has one
+    npl0 = list(deck.nptlist)[: len(qmcc)] + [0] * max(0, len(qmcc) - len(deck.nptlist))
+    sc = deck.bcurr >= 1.0e-10
     try:
         for kind, item in lattice_segments(deck, workdir, set(skip), start):
             if kind == "skipped":
@@ -632,12 +660,23 @@ def run_deck(workdir, outdir=None, form=None, skip=(), write=True):
                 refs = b.run_reference()
                 seg = [diag_row(zs[i], recs[i], refs[i], deck.bmass, deck.bfreq)
                        for i in range(len(recs))]
+                if multi:
+                    per = b.run_species()
+                else:  # one species: every live particle
+                    per = np.array([[int(r[32])] for r in seg])
+                cs = charge_state_counts(b.species()[0], per, qmcc)
+                if not sc:
+                    cs[:] = npl0
+                if not rows:
+                    cs[0] = npl0
                 # a stretch's first record repeats the previous stretch's last
                 rows += seg[1:] if rows else seg
+                charges += list(cs[1:] if charges else cs)
         final = b.download()
     finally:
         b.close()
     rows = np.array(rows)
+    charges = np.array(charges)
     if write:
-        write_diag(outdir, rows)
-    return {"rows": rows, "skipped": skipped, "pts": final}
+        write_diag(outdir, rows, charges if len(charges) else None)
+    return {"rows": rows, "charge_states": charges, "skipped": skipped, "pts": final}

@@ -39,6 +39,10 @@ extern "C" {
 
 /* bunch creation flags */
 #define IMPZ_FLAG_TRACK_IDS 1 /* carry Pts1(9,:) through the per-step particle sort */
+#define IMPZ_FLAG_SPECIES 2   /* multi-species bunch: Pts1(7,:) and Pts1(8,:) per particle */
+#ifndef IMPZ_MAX_SPECIES
+#define IMPZ_MAX_SPECIES 128  /* distinct (Pts1(7), Pts1(8)) pairs of one bunch */
+#endif
 
 #define IMPZ_RAW_LEN 44   /* 37 moment sums, 6 |max|, max r^2 */
 #define IMPZ_DIAG_LEN 45  /* one row of fort.18/24-30, see impz_diag_row */
@@ -92,6 +96,16 @@ int impz_set_device(int device);
 int impz_bunch_create(const double* pts, long long n, double current, double mass,
                       double charge, double freq, const double refptcl[6], int nx, int ny,
                       int nz, int form, int flags, impz_bunch_t* out);
+/* Pts1 rows 7 (q/m) and 8 (charge weight) are per-bunch constants unless the
+ * bunch is created with IMPZ_FLAG_SPECIES; without it, rows that differ
+ * from the first particle's are IMPZ_ERR_NONUNIFORM.  With it, each
+ * distinct (row 7, row 8) pair is a species (at most IMPZ_MAX_SPECIES, else
+ * IMPZ_ERR_LIMIT) carried per particle through the sort: the deposit weights
+ * each particle by its row 8 (deposit_BeamBunch, BeamBunch.f90:3749-3763),
+ * and the K-map quadrupole, the bend maps and the Lorentz kick use its row 7
+ * (Quadrupole.f90:533, Dipole.f90:466-591 and 693-788, BeamBunch.f90:3026-3035), as the
+ * reference's multiple charge states do (BeamBunch.f90:13-14: the map
+ * integrator's space-charge kick keeps the bunch's charge/mass). */
 /* getpts_BeamBunch (BeamBunch.f90:3663-3675): copies the live particles back
  * into pts (capacity cap particles); *n receives the live count.  Without
  * IMPZ_FLAG_TRACK_IDS column 9 is filled with 1..n in the current order. */
@@ -280,6 +294,23 @@ int impz_run_batch(impz_bunch_t* bunches, const impz_elem_t* const* lattices,
  * BeamBunch%refptcl when diagnostic1_Output wrote that record), for
  * impz_diag_row; *nrec receives the record count (refrec may be NULL). */
 int impz_run_reference(impz_bunch_t b, double* refrec, int maxrec, int* nrec);
+/* The species of the bunch: (q/m, weight) = Pts1 rows 7 and 8 of each, in
+ * order of first appearance in the uploaded rows; returns their number
+ * (1 for a bunch without IMPZ_FLAG_SPECIES) and fills up to cap of them. */
+int impz_bunch_species(impz_bunch_t b, double* qm, double* weight, int cap);
+/* chgupdate_BeamBunch (BeamBunch.f90:688-728): idchg[j] = particles whose
+ * q/m is within relative 1e-4 of qmcclist[j], counting those the latest
+ * conv1st kept (between impz_sc_prepare and the kick, its loss test
+ * decides; otherwise every stored particle).  The rescale of Pts1(8) the
+ * reference keeps commented out is not done. */
+int impz_chgupdate(impz_bunch_t b, int nchge, const double* qmcclist, int* idchg);
+/* For a bunch with IMPZ_FLAG_SPECIES, chgupdate's count of each species at
+ * every record of the last whole-lattice run: counts[r * nspecies + k]
+ * (nspecies from impz_bunch_species), the particles each step's pass kept
+ * after that step's conv1st (a step without space charge loses none).
+ * diagnostic1 writes them per charge state to fort.32 (Output.f90:352).
+ * IMPZ_ERR_STATE without the flag. */
+int impz_run_species(impz_bunch_t b, int* counts, int maxrec, int* nrec);
 int impz_count_steps(const impz_elem_t* elems, int nelem);
 
 /* ---- instrumentation --------------------------------------------------- */

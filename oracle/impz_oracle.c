@@ -47,6 +47,39 @@ void orc_set_field_probe(double *phi, double *eg, int maxsteps) {
   g_probe.step = 0;
 }
 
+/* Optional charge-state bookkeeping of orc_run (test infrastructure):
+ * chgupdate_BeamBunch (BeamBunch.f90:688-728) after every conv1st updates
+ * nptlist (idchgold: the count of particles whose Pts1(7) is within
+ * relative eps of qmcclist(j)), and every record copies it to out + nchrg*r,
+ * as diagnostic1 writes it to fort.32 (Output.f90:352). */
+static struct {
+  const double *qmc;
+  int nchrg, maxrows;
+  int *cur, *out;
+} g_chg;
+
+void orc_set_charge_states(const double *qmcclist, int nchrg, int *nptlist, int *out,
+                           int maxrows) {
+  g_chg.qmc = qmcclist;
+  g_chg.nchrg = (qmcclist && nptlist) ? nchrg : 0;
+  g_chg.cur = nptlist;
+  g_chg.out = out;
+  g_chg.maxrows = out ? maxrows : 0;
+}
+
+/* chgupdate_BeamBunch (BeamBunch.f90:697-722); eps = 1.0e-4, a default-real
+ * literal */
+static void orc_chgupdate(const double *pts, int n) {
+  if (!g_chg.nchrg) return;
+  const double eps = (double)1.0e-4f;
+  for (int j = 0; j < g_chg.nchrg; j++) g_chg.cur[j] = 0;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < g_chg.nchrg; j++) {
+      const double dd = fabs((pts[9 * (size_t)i + 6] - g_chg.qmc[j]) / g_chg.qmc[j]);
+      if (dd < eps) g_chg.cur[j]++;
+    }
+}
+
 /* PhysConst.f90:25-35 */
 void orc_physconst(double freq) {
   PC.Clight = 299792458.0;
@@ -1483,7 +1516,8 @@ void orc_kick1(double *pts, int n, const double *phi, const int mesh[3],
  * 2187-3071, the analytic-field branch) in element e with zedge = Param(1):
  * 0 drift, 1 quadrupole, 2 constant focusing, 3 solenoid, 101..104 the RF
  * cavities over read3_Data's Fourier coefficients (e->zdat, e->ndata); z =
- * the kick's position, tg = refptcl(5) there, qmi = Pts1(7) */
+ * the kick's position, tg = refptcl(5) there, qmi = the bunch's Pts1(7)
+ * (each particle's own row 7 enters the update, as rays(7,n) does) */
 typedef struct {
   const orc_elem *e;
   double zedge, z, tg, qmi;
@@ -2015,7 +2049,7 @@ static void lorentz_update(double *p, double exn, double eyn, double ezn, double
   const double bx = -(beta0 / Clight * tmpscale2 * eyn) + extfld[3];
   const double by = beta0 / Clight * tmpscale2 * exn + extfld[4];
   const double bz = extfld[5];
-  const double r7 = lz->qmi;
+  const double r7 = p[6];  /* rays(7,n): the particle's q/m (multiple charge states) */
   const double tmp12 = -tau * Clight * bz * r7 / 2;
   const double tmp13 = tau * ex * r7 / 2;
   const double tmp23 = tau * ey * r7 / 2;
@@ -2887,6 +2921,9 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
       orc_diag_row(z, raw, beam->npt, beam->nlocal, beam->refptcl, beam->mass,    \
                    rows + (size_t)ORC_DIAG_LEN * nrows);                          \
     }                                                                             \
+    if (nrows < g_chg.maxrows)                                                    \
+      memcpy(g_chg.out + (size_t)g_chg.nchrg * nrows, g_chg.cur,                  \
+             (size_t)g_chg.nchrg * sizeof(int));                                  \
     nrows++;                                                                      \
   } while (0)
   DIAG();
@@ -2965,6 +3002,7 @@ int orc_run(const orc_elem *elems, int nelem, orc_beam *beam, const int mesh[3],
             double ptrange[6], range[6], msize[3];
             beam->nlocal = orc_conv1st(beam->pts, beam->nlocal, &beam->current, &beam->npt,
                                        beam->refptcl, piperad, piperad2, ptrange);
+            orc_chgupdate(beam->pts, beam->nlocal); /* AccSimulator.f90:1130 */
             orc_update_compdom(ptrange, mesh, range, msize);
             orc_deposit(beam->pts, beam->nlocal, mesh, range, msize, rho, NULL, NULL);
             if (orc_poisson_open(mesh[0], mesh[1], mesh[2], msize[0], msize[1], msize[2], rho)) {

@@ -38,6 +38,11 @@ void orc_set_threads(int n);
  * potential into phi[s*G..] and kick1's Ex,Ey,Ez into eg[3*s*G..] for
  * s < maxsteps (either may be NULL); resets the step counter */
 void orc_set_field_probe(double *phi, double *eg, int maxsteps);
+/* charge states of orc_run: nptlist[nchrg] (idchgold, updated by
+ * chgupdate_BeamBunch after every conv1st) is copied to out[nchrg*r..]
+ * at every record r < maxrows (fort.32); qmcclist NULL switches it off */
+void orc_set_charge_states(const double *qmcclist, int nchrg, int *nptlist, int *out,
+                           int maxrows);
 
 /* ---- element maps ---------------------------------------------------- */
 /* drift1_BeamBunch bitype 0 (BeamBunch.f90:276-298) */

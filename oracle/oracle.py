@@ -63,6 +63,7 @@ def lib():
             "orc_get_physconst": (v, [_D]),
             "orc_set_threads": (v, [ctypes.c_int]),
             "orc_set_field_probe": (v, [_D, _D, ctypes.c_int]),
+            "orc_set_charge_states": (v, [_D, ctypes.c_int, _I, _I, ctypes.c_int]),
             "orc_drift_exact": (v, [_D, ctypes.c_int, _D, ctypes.c_double]),
             "orc_maplinear_quad": (v, [ctypes.c_double, ctypes.c_double, _D, _D, ctypes.c_double,
                                        ctypes.c_int, ctypes.c_double, ctypes.c_double]),
@@ -190,18 +191,26 @@ def elem_from(e):
 
 
 def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0, state=None, flagmap=1,
-        probe=None):
+        probe=None, charge_states=None):
     """orc_run over a lattice: returns (rows, final pts, final beam).  `state`
     (a beam returned by an earlier call) carries the CSR bend bookkeeping
     across calls, as one element loop of the reference would.  `probe` =
     (phi, eg) float64 arrays of shape (S, G) and (S, 3G) (either may be None)
     receive the potential and kick1's field of the first S space-charge
-    steps of the map integrator."""
+    steps of the map integrator.  `charge_states` = (qmcclist, nptlist,
+    out): chgupdate's counts per charge state (nptlist, int32, updated in
+    place) copied to out[r] (int32, shape (records, nchrg)) at every record."""
     physconst(freq)
     if probe is not None:
         phi, eg = probe
         steps = (phi if phi is not None else eg).shape[0]
         lib().orc_set_field_probe(dp(phi), dp(eg), steps)
+    if charge_states is not None:
+        qmc, npl, cs_out = charge_states
+        qmc = np.ascontiguousarray(qmc, dtype=np.float64)
+        assert npl.dtype == np.int32 and cs_out.dtype == np.int32 and cs_out.flags.c_contiguous
+        lib().orc_set_charge_states(dp(qmc), len(qmc), npl.ctypes.data_as(_I),
+                                    cs_out.ctypes.data_as(_I), cs_out.shape[0])
     arr = (OrcElem * len(elems))(*[elem_from(e) for e in elems])
     keep = [getattr(e, "_keep", None) for e in elems]
     p = np.ascontiguousarray(pts, dtype=np.float64).copy()
@@ -225,6 +234,8 @@ def run(elems, pts, current, mass, charge, freq, refptcl, grid, z=0.0, state=Non
     finally:
         if probe is not None:
             lib().orc_set_field_probe(None, None, 0)
+        if charge_states is not None:
+            lib().orc_set_charge_states(None, 0, None, None, 0)
     del keep
     if n < 0:
         raise RuntimeError("orc_run failed: %d" % n)

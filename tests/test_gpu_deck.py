@@ -175,3 +175,55 @@ def test_lorentz_dtl_deck_matches_the_oracle(tmp_path):
     for c in RMS_COLS:
         scale = np.max(np.abs(rows_o[:, c])) + 1e-300
         assert np.max(np.abs(rows_g[:, c] - rows_o[:, c])) / scale <= 1e-8, c
+
+
+def test_two_charge_state_deck_writes_fort32(tmp_path):
+    """A deck of two charge states (Nchrg = 2; particle.in rows 7 and 8 per
+    particle) under the Lorentz integrator through DTL cells with space
+    charge and a narrow aperture: run_deck's rows against the oracle's, and
+    fort.32 (z and the count of each charge state, Output.f90:352) equal to
+    the oracle's chgupdate counts (the deck's nptlist at the first record)."""
+    from test_lorentz import rf_cell
+    wd = str(tmp_path)
+    npt, qs, cur, freq = [2500, 1500], (33.0, 34.0), [0.004, 0.003], 80.5e6
+    pts, _, mass, qmc = beams.charge_state_bunch(npt, qs, cur, seed=beams.SEED0 + 119,
+                                                 freq=freq)
+    n = sum(npt)
+    d = deck.Deck(np=n, flagmap=2, nx=16, ny=16, nz=32, xrad=0.02, yrad=0.02, perdlen=0.1,
+                  nchrg=2, nptlist=npt, currlist=cur, qmcclist=list(qmc), bcurr=sum(cur),
+                  bkenergy=0.5e6 * 238, bmass=mass, bcharge=qs[0], bfreq=freq, phsini=0.0)
+    z24 = lambda *v: list(v) + [0.0] * (24 - len(v))  # noqa: E731
+    coef, _ = rf_cell()
+    np.savetxt(os.path.join(wd, "rfdata852.in"), coef)
+    cell = lambda th: deck.Element(  # noqa: E731
+        0.08, 12, 20, 101, z24(2.5e6, freq, th, 852, 0.0035, 0.02, 68.0, 0.02, -67.0))
+    d.elements = [cell(222.0), cell(218.0), deck.Element(0.09, 6, 20, 0, z24(0.0035)),
+                  deck.Element(0.0, 0, 0, -99, z24())]
+    deck.write_deck(os.path.join(wd, "ImpactZ.in"), d)
+    deck.write_particles(os.path.join(wd, "particle.in"), pts)
+    out = deck.run_deck(wd)
+    ref, z, rows_o, cs_o = d.refptcl(), 0.0, [], []
+    npl = np.array(npt, dtype=np.int32)
+    p = pts
+    for kind, item in deck.lattice_segments(d, wd):
+        if kind == "run":
+            nrec = 1 + sum(e.nseg for e in item)
+            cs = np.zeros((nrec, 2), dtype=np.int32)
+            seg, p, beam = orc.run(item, p, d.bcurr, d.bmass, d.bcharge, d.bfreq, ref,
+                                   (d.nx, d.ny, d.nz), z, flagmap=2,
+                                   charge_states=(qmc, npl, cs))
+            ref, z = np.array(beam.refptcl[:]), beam.z
+            rows_o += list(seg[1:] if rows_o else seg)
+            cs_o += list(cs[1:] if cs_o else cs)
+    rows_o, cs_o = np.array(rows_o), np.array(cs_o)
+    rows_g = out["rows"]
+    assert rows_g.shape == rows_o.shape
+    assert rows_o[-1, 32] < n  # the aperture lost particles
+    np.testing.assert_allclose(rows_g[:, 0], rows_o[:, 0], rtol=0, atol=0)
+    for c in RMS_COLS:
+        scale = np.max(np.abs(rows_o[:, c])) + 1e-300
+        assert np.max(np.abs(rows_g[:, c] - rows_o[:, c])) / scale <= 1e-8, c
+    np.testing.assert_array_equal(out["charge_states"], cs_o)
+    f32 = np.loadtxt(os.path.join(wd, "fort.32"))
+    np.testing.assert_array_equal(f32[:, 0], rows_g[:, 0])
+    np.testing.assert_array_equal(f32[:, 1:], cs_o)
