@@ -69,14 +69,22 @@ static int dct_lines(int n) {
   return t;
 }
 
+// k_green_xy: the line pairs of the longer of its two transforms, both
+// twiddle sets and the (nx+1)(ny+1) plane
+template <typename T>
+static size_t green_xy_smem(int nx, int ny) {
+  const size_t lx = (size_t)((ny + 2) / 2) * line_pitch(2 * nx);
+  const size_t ly = (size_t)((nx + 2) / 2) * line_pitch(2 * ny);
+  return sizeof(typename Cplx<T>::type) * ((lx > ly ? lx : ly) + nx + ny) +
+         sizeof(T) * (size_t)(nx + 1) * (ny + 1);
+}
+
 // true when every Poisson kernel fits the device's shared memory
 template <typename T>
 bool poisson_fits(int nx, int ny, int nz) {
   const size_t lim = smem_optin();
-  int nmax = nx > ny ? nx : ny;
-  nmax = nmax > nz ? nmax : nz;
   return xy_smem<T>(nx, ny) <= lim && xyf_smem<T>(nx, ny, 1) <= lim && z_smem<T>(nz, 1) <= lim &&
-         dct_smem<T>(nmax, 2) <= lim;
+         dct_smem<T>(nz, 2) <= lim && green_xy_smem<T>(nx, ny) <= lim;
 }
 
 template <typename K>
@@ -128,30 +136,24 @@ static cudaError_t zconv_t(const PoissonBuffers& b, const PoissonDims& d, cudaSt
                     (const T*)b.ghat, (const C*)b.twz);
 }
 
-// The Green function: FP64 corners and 8-corner difference (the difference
-// cancels catastrophically, Field.f90:420-428), then three DCT-I passes in
-// the convolution's type T (FP64 in the plain form, FP32 in the
-// FP32-convolution form, whose first pass converts the FP64 octant).
+// The Green function: FP64 corners, then per z plane the FP64 8-corner
+// difference (it cancels catastrophically, Field.f90:420-428) and the DCT-I
+// along x and y in the convolution's type T (FP64 in the plain form, FP32 in
+// the FP32-convolution form), then the DCT-I along z.
 template <typename T>
 cudaError_t launch_green(const PoissonBuffers& b, cudaStream_t s) {
   typedef typename Cplx<T>::type C;
   const int nx = b.nx, ny = b.ny, nz = b.nz;
   const long long nc = (long long)(nx + 2) * (ny + 2) * (nz + 2);
-  const long long ng = (long long)(nx + 1) * (ny + 1) * (nz + 1);
   k_igf_corners<<<grid_for(nc, 256), 256, 0, s>>>(nx, ny, nz, b.st, b.F);
-  k_igf_green<<<grid_for(ng, 256), 256, 0, s>>>(nx, ny, nz, b.F, b.Gt);
+  const size_t sm = green_xy_smem<T>(nx, ny);
+  cudaError_t e = allow_smem(k_green_xy<T>, sm);
+  if (e != cudaSuccess) return e;
+  k_green_xy<T><<<nz + 1, 256, sm, s>>>(nx, ny, ilog2(2 * nx), ilog2(2 * ny), b.F, (T*)b.ghat,
+                                        (const C*)b.twx, (const C*)b.twy);
   const long long gx = nx + 1, gxy = (long long)(nx + 1) * (ny + 1);
   const double scale = 1.0 / ((double)(2 * nx) * (double)(2 * ny) * (double)(2 * nz));
   T* work = (T*)b.ghat;
-  cudaError_t e;
-  // along x: lines j (inner, stride gx) x k (outer); points contiguous
-  if ((e = dct_pass<double, T>(b.Gt, work, nx, 1, gx, ny + 1, gxy, nz + 1, 1.0, (const C*)b.twx,
-                               s)) != cudaSuccess)
-    return e;
-  // along y: lines i (inner, stride 1) x k (outer); points stride gx
-  if ((e = dct_pass<T, T>(work, work, ny, gx, 1, nx + 1, gxy, nz + 1, 1.0, (const C*)b.twy, s)) !=
-      cudaSuccess)
-    return e;
   // along z: lines i (inner) x j (outer, stride gx); points stride gxy
   if ((e = dct_pass<T, T>(work, work, nz, gxy, 1, nx + 1, gx, ny + 1, scale, (const C*)b.twz,
                           s)) != cudaSuccess)
@@ -244,17 +246,14 @@ template <typename T>
 cudaError_t launch_green_group(int nx, int ny, int nz, const PoissonMember* mem, int nmem,
                                cudaStream_t s) {
   const long long nc = (long long)(nx + 2) * (ny + 2) * (nz + 2);
-  const long long ng = (long long)(nx + 1) * (ny + 1) * (nz + 1);
   k_igf_corners_group<<<dim3(group_grid(nc, 256, nmem), nmem), 256, 0, s>>>(nx, ny, nz, mem);
-  k_igf_green_group<<<dim3(group_grid(ng, 256, nmem), nmem), 256, 0, s>>>(nx, ny, nz, mem);
+  const size_t sm = green_xy_smem<T>(nx, ny);
+  cudaError_t e = allow_smem(k_green_xy_group<T>, sm);
+  if (e != cudaSuccess) return e;
+  k_green_xy_group<T><<<dim3(nz + 1, nmem), 256, sm, s>>>(nx, ny, ilog2(2 * nx), ilog2(2 * ny),
+                                                          mem);
   const long long gx = nx + 1, gxy = (long long)(nx + 1) * (ny + 1);
   const double scale = 1.0 / ((double)(2 * nx) * (double)(2 * ny) * (double)(2 * nz));
-  cudaError_t e;
-  if ((e = dct_group<double, T>(0, nx, 1, gx, ny + 1, gxy, nz + 1, 1.0, mem, nmem, s)) !=
-      cudaSuccess)
-    return e;
-  if ((e = dct_group<T, T>(1, ny, gx, 1, nx + 1, gxy, nz + 1, 1.0, mem, nmem, s)) != cudaSuccess)
-    return e;
   if ((e = dct_group<T, T>(2, nz, gxy, 1, nx + 1, gx, ny + 1, scale, mem, nmem, s)) !=
       cudaSuccess)
     return e;

@@ -470,33 +470,99 @@ __global__ void k_igf_corners_group(int nx, int ny, int nz, const PoissonMember*
   igf_corners_body(nx, ny, nz, m.st, m.F);
 }
 
-// 8-corner difference (Field.f90:420-428) into the octant (nx+1)(ny+1)(nz+1)
-__device__ __forceinline__ void igf_green_body(int nx, int ny, int nz, const double* __restrict__ F,
-                                               double* __restrict__ Gt) {
-  const int ax = nx + 2, ay = ny + 2;
-  const int gx = nx + 1, gy = ny + 1, gz = nz + 1;
-  const long long total = (long long)gx * gy * gz;
-  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(e % gx);
-    const int j = (int)((e / gx) % gy);
-    const int k = (int)(e / ((long long)gx * gy));
-#define IMPZ_F(a, b, c) __ldg(F + (a) + (size_t)ax * ((b) + (size_t)ay * (c)))
-    Gt[e] = IMPZ_F(i + 1, j + 1, k + 1) - IMPZ_F(i, j + 1, k + 1) - IMPZ_F(i + 1, j, k + 1) +
-            IMPZ_F(i, j, k + 1) - IMPZ_F(i + 1, j + 1, k) + IMPZ_F(i, j + 1, k) +
-            IMPZ_F(i + 1, j, k) - IMPZ_F(i, j, k);
+// The Green octant one z plane per block: the 8-corner difference of plane
+// k (Field.f90:420-428, FP64: it cancels catastrophically), rounded to the
+// convolution's type T, then its DCT-I along x and along y in shared memory
+// (rows, then columns, two lines per complex FFT of length 2n), written to
+// plane k of G-hat; the z pass follows.  One pass over the corners and one
+// write of the plane instead of a difference kernel and two strided DCT
+// passes through global memory.  lx, ly: log2(2 nx), log2(2 ny).
+// smem: the line pairs of the longer transform, the twiddles of both, and
+// the plane P[(ny+1)][(nx+1)] (T).
+template <typename T>
+__device__ __forceinline__ void green_xy_body(int nx, int ny, int lx, int ly,
+                                              const double* __restrict__ F, T* __restrict__ ghat,
+                                              const typename Cplx<T>::type* __restrict__ twx,
+                                              const typename Cplx<T>::type* __restrict__ twy,
+                                              const int k) {
+  typedef typename Cplx<T>::type C;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int gx = nx + 1, gy = ny + 1, ax = nx + 2, ay = ny + 2;
+  const int lpx = line_pitch(2 * nx), lpy = line_pitch(2 * ny);
+  const int npx = (gy + 1) / 2;  // row pairs (j, j + npx) for the x transform
+  const int npy = (gx + 1) / 2;  // column pairs (i, i + npy) for the y transform
+  C* L = reinterpret_cast<C*>(smem_raw);
+  C* twxs = L + max(npx * lpx, npy * lpy);
+  C* twys = twxs + nx;
+  T* P = reinterpret_cast<T*>(twys + ny);
+  stage_tw(twxs, twx, 2 * nx);
+  stage_tw(twys, twy, 2 * ny);
+  const double* F0 = F + (size_t)ax * ay * k;  // corner planes k and k + 1
+  const double* F1 = F0 + (size_t)ax * ay;
+  for (int e = threadIdx.x; e < gx * gy; e += blockDim.x) {
+    const int j = e / gx, i = e - j * gx;
+#define IMPZ_F(p, a, b) __ldg(p + (a) + (size_t)ax * (b))
+    const double v = IMPZ_F(F1, i + 1, j + 1) - IMPZ_F(F1, i, j + 1) - IMPZ_F(F1, i + 1, j) +
+                     IMPZ_F(F1, i, j) - IMPZ_F(F0, i + 1, j + 1) + IMPZ_F(F0, i, j + 1) +
+                     IMPZ_F(F0, i + 1, j) - IMPZ_F(F0, i, j);
 #undef IMPZ_F
+    P[e] = (T)v;
+  }
+  __syncthreads();
+  // along x: row t with row t + npx (real and imaginary parts)
+  for (int e = threadIdx.x; e < npx * 2 * nx; e += blockDim.x) {
+    const int m = e / npx, t = e - m * npx;
+    const int mm = m <= nx ? m : 2 * nx - m;
+    C v;
+    v.x = P[t * gx + mm];
+    v.y = t + npx < gy ? P[(t + npx) * gx + mm] : (T)0;
+    L[t * lpx + sw(m)] = v;
+  }
+  __syncthreads();
+  fft_dif<C>(L, lx, npx, lpx, -1, twxs);
+  for (int e = threadIdx.x; e < npx * gx; e += blockDim.x) {
+    const int m = e / npx, t = e - m * npx;
+    const C v = L[t * lpx + sw(bitrev(m, lx))];
+    P[t * gx + m] = v.x;
+    if (t + npx < gy) P[(t + npx) * gx + m] = v.y;
+  }
+  __syncthreads();
+  // along y: column t with column t + npy
+  for (int e = threadIdx.x; e < npy * 2 * ny; e += blockDim.x) {
+    const int m = e / npy, t = e - m * npy;
+    const int mm = m <= ny ? m : 2 * ny - m;
+    C v;
+    v.x = P[mm * gx + t];
+    v.y = t + npy < gx ? P[mm * gx + t + npy] : (T)0;
+    L[t * lpy + sw(m)] = v;
+  }
+  __syncthreads();
+  fft_dif<C>(L, ly, npy, lpy, -1, twys);
+  T* out = ghat + (size_t)gx * gy * k;
+  for (int e = threadIdx.x; e < npy * gy; e += blockDim.x) {
+    const int m = e / npy, t = e - m * npy;
+    const C v = L[t * lpy + sw(bitrev(m, ly))];
+    out[(size_t)m * gx + t] = v.x;
+    if (t + npy < gx) out[(size_t)m * gx + t + npy] = v.y;
   }
 }
 
-__global__ void k_igf_green(int nx, int ny, int nz, const double* __restrict__ F,
-                            double* __restrict__ Gt) {
-  igf_green_body(nx, ny, nz, F, Gt);
+template <typename T>
+__global__ void __launch_bounds__(256) k_green_xy(int nx, int ny, int lx, int ly,
+                                                  const double* __restrict__ F,
+                                                  T* __restrict__ ghat,
+                                                  const typename Cplx<T>::type* __restrict__ twx,
+                                                  const typename Cplx<T>::type* __restrict__ twy) {
+  green_xy_body<T>(nx, ny, lx, ly, F, ghat, twx, twy, blockIdx.x);
 }
 
-__global__ void k_igf_green_group(int nx, int ny, int nz, const PoissonMember* __restrict__ mem) {
+template <typename T>
+__global__ void __launch_bounds__(256) k_green_xy_group(int nx, int ny, int lx, int ly,
+                                                        const PoissonMember* __restrict__ mem) {
+  typedef typename Cplx<T>::type C;
   const PoissonMember& m = mem[blockIdx.y];
-  igf_green_body(nx, ny, nz, m.F, m.Gt);
+  green_xy_body<T>(nx, ny, lx, ly, m.F, (T*)m.ghat, (const C*)m.twx, (const C*)m.twy,
+                   blockIdx.x);
 }
 
 // DCT-I (transform of the even extension) along one axis of the octant.
@@ -557,7 +623,7 @@ __global__ void k_dct1_group(int axis, int logn, long long es, long long ls, int
                              long long os, double scale, const PoissonMember* __restrict__ mem) {
   typedef typename Cplx<CT>::type C;
   const PoissonMember& m = mem[blockIdx.z];
-  const TI* in = axis == 0 ? (const TI*)m.Gt : (const TI*)m.ghat;
+  const TI* in = (const TI*)m.ghat;  // x and y are done by k_green_xy_group
   const C* tw = (const C*)(axis == 0 ? m.twx : axis == 1 ? m.twy : m.twz);
   dct1_body<TI, TO, CT, TL>(in, (TO*)m.ghat, logn, es, ls, ninner, os, scale, tw, blockIdx.x,
                             blockIdx.y);
