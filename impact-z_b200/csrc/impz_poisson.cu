@@ -149,8 +149,9 @@ cudaError_t launch_green(const PoissonBuffers& b, cudaStream_t s) {
   const size_t sm = green_xy_smem<T>(nx, ny);
   cudaError_t e = allow_smem(k_green_xy<T>, sm);
   if (e != cudaSuccess) return e;
-  k_green_xy<T><<<nz + 1, 256, sm, s>>>(nx, ny, ilog2(2 * nx), ilog2(2 * ny), b.F, (T*)b.ghat,
-                                        (const C*)b.twx, (const C*)b.twy);
+  k_green_xy<T><<<nz + 1, IMPZ_GREEN_THREADS, sm, s>>>(nx, ny, ilog2(2 * nx), ilog2(2 * ny), b.F,
+                                                       (T*)b.ghat, (const C*)b.twx,
+                                                       (const C*)b.twy);
   const long long gx = nx + 1, gxy = (long long)(nx + 1) * (ny + 1);
   const double scale = 1.0 / ((double)(2 * nx) * (double)(2 * ny) * (double)(2 * nz));
   T* work = (T*)b.ghat;
@@ -250,8 +251,8 @@ cudaError_t launch_green_group(int nx, int ny, int nz, const PoissonMember* mem,
   const size_t sm = green_xy_smem<T>(nx, ny);
   cudaError_t e = allow_smem(k_green_xy_group<T>, sm);
   if (e != cudaSuccess) return e;
-  k_green_xy_group<T><<<dim3(nz + 1, nmem), 256, sm, s>>>(nx, ny, ilog2(2 * nx), ilog2(2 * ny),
-                                                          mem);
+  k_green_xy_group<T><<<dim3(nz + 1, nmem), IMPZ_GREEN_THREADS, sm, s>>>(
+      nx, ny, ilog2(2 * nx), ilog2(2 * ny), mem);
   const long long gx = nx + 1, gxy = (long long)(nx + 1) * (ny + 1);
   const double scale = 1.0 / ((double)(2 * nx) * (double)(2 * ny) * (double)(2 * nz));
   if ((e = dct_group<T, T>(2, nz, gxy, 1, nx + 1, gx, ny + 1, scale, mem, nmem, s)) !=

@@ -499,6 +499,7 @@ __device__ __forceinline__ void green_xy_body(int nx, int ny, int lx, int ly,
   stage_tw(twys, twy, 2 * ny);
   const double* F0 = F + (size_t)ax * ay * k;  // corner planes k and k + 1
   const double* F1 = F0 + (size_t)ax * ay;
+#pragma unroll 4
   for (int e = threadIdx.x; e < gx * gy; e += blockDim.x) {
     const int j = e / gx, i = e - j * gx;
 #define IMPZ_F(p, a, b) __ldg(p + (a) + (size_t)ax * (b))
@@ -547,18 +548,20 @@ __device__ __forceinline__ void green_xy_body(int nx, int ny, int lx, int ly,
   }
 }
 
+#ifndef IMPZ_GREEN_THREADS
+#define IMPZ_GREEN_THREADS 512
+#endif
 template <typename T>
-__global__ void __launch_bounds__(256) k_green_xy(int nx, int ny, int lx, int ly,
-                                                  const double* __restrict__ F,
-                                                  T* __restrict__ ghat,
-                                                  const typename Cplx<T>::type* __restrict__ twx,
-                                                  const typename Cplx<T>::type* __restrict__ twy) {
+__global__ void __launch_bounds__(IMPZ_GREEN_THREADS)
+    k_green_xy(int nx, int ny, int lx, int ly, const double* __restrict__ F, T* __restrict__ ghat,
+               const typename Cplx<T>::type* __restrict__ twx,
+               const typename Cplx<T>::type* __restrict__ twy) {
   green_xy_body<T>(nx, ny, lx, ly, F, ghat, twx, twy, blockIdx.x);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_green_xy_group(int nx, int ny, int lx, int ly,
-                                                        const PoissonMember* __restrict__ mem) {
+__global__ void __launch_bounds__(IMPZ_GREEN_THREADS)
+    k_green_xy_group(int nx, int ny, int lx, int ly, const PoissonMember* __restrict__ mem) {
   typedef typename Cplx<T>::type C;
   const PoissonMember& m = mem[blockIdx.y];
   green_xy_body<T>(nx, ny, lx, ly, m.F, (T*)m.ghat, (const C*)m.twx, (const C*)m.twy,
