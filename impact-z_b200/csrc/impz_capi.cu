@@ -1457,8 +1457,11 @@ int impz_deposit(impz_bunch_t b, double* chgdens, int* counts) {
     ProfScope ps(b, IMPZ_PROF_DEPOSIT, 1);
     CK(launch_deposit(b, d));
   }
-  if (counts) {
-    CK(cudaMemcpyAsync(counts, b->counts, b->G * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  std::vector<int> keyed;
+  if (counts) {  // per-cell counts are kept in sort-key order (cell_key, impz_particle.cuh)
+    keyed.resize((size_t)b->G);
+    CK(cudaMemcpyAsync(keyed.data(), b->counts, b->G * sizeof(int), cudaMemcpyDeviceToHost,
+                       b->stream));
   }
   std::vector<long long> q;
   if (chgdens) {
@@ -1471,6 +1474,16 @@ int impz_deposit(impz_bunch_t b, double* chgdens, int* counts) {
     CK(exact::launch_scan(b->counts, b->cursor, b->bsum, b->G + 1, b->st, b->stream));
   }
   CK(cudaStreamSynchronize(b->stream));
+  if (counts) {
+    const int nx = b->nx, ny = b->ny, nz = b->nz;
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++) {
+          const int brick = ((k >> 2) * (ny >> 2) + (j >> 2)) * (nx >> 2) + (i >> 2);
+          const int key = (brick << 6) | ((k & 3) << 4) | ((j & 3) << 2) | (i & 3);
+          counts[i + (size_t)nx * (j + (size_t)ny * k)] = keyed[(size_t)key];
+        }
+  }
   if (chgdens) {
     const double qs = b->weight * std::ldexp(1.0, -b->fixbits);
     for (long long i = 0; i < b->G; i++) chgdens[i] = (double)q[(size_t)i] * qs;

@@ -208,7 +208,8 @@ struct DepositArgs {
   int fixbits;
   int tframe;               // 1: the particles are stored in conv1st's frame (AdvanceArgs)
   unsigned long long* rho;  // G int64 (two's complement) accumulators
-  int* counts;              // G+1 per-cell particle counts (slot G: live but outside)
+  int* counts;              // G+1 per-cell particle counts by sort key (cell_key; slot G:
+                            // live but outside)
   double xl;
   const unsigned char* sp_in;  // species index per particle (multi-species bunches), or null
   const double* sp_w;       // [IMPZ_MAX_SPECIES] Pts1(8) of each species / the bunch's weight

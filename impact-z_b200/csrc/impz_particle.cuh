@@ -587,6 +587,18 @@ __device__ __forceinline__ long long lin_cell(const Cell& c, int nx, int ny) {
   return (long long)(c.ix - 1) + (long long)nx * ((c.jx - 1) + (long long)ny * (c.kx - 1));
 }
 
+// Sort key of the cell with lower node (ix, jx, kx) (0-based; grid sides are
+// powers of two >= 4): bricks of 4x4x4 cells in x-fastest order, the cells
+// of a brick x-fastest.  The particles are kept in this order and the
+// per-cell counts indexed by it, so that a deposit chunk of consecutive
+// particles covers a compact box of nodes even where the beam is sparse (in
+// plain x-fastest order a chunk over a few thousand sparse cells spans whole
+// rows and tens of them, more than the shared tile holds).
+__device__ __forceinline__ int cell_key(int ix, int jx, int kx, int nx, int ny) {
+  const int brick = ((kx >> 2) * (ny >> 2) + (jx >> 2)) * (nx >> 2) + (ix >> 2);
+  return (brick << 6) | ((kx & 3) << 4) | ((jx & 3) << 2) | (ix & 3);
+}
+
 // ---------------------------------------------------------------------
 // The fused particle pass of step s.  Per particle, in the reference's order:
 //   [kick]  conv1st z->t, loss test, deposit cell (sort key),
@@ -1008,7 +1020,8 @@ __device__ __forceinline__ void advance_pass(const AdvanceArgs& a, const int vbx
           keep[u] = false;
         } else {
           Cell cd = cic_cell(t.xt, t.yt, t.zt, g);
-          key[u] = cell_inside(cd, nx, ny, nz) ? (int)lin_cell(cd, nx, ny) : (int)G;
+          key[u] = cell_inside(cd, nx, ny, nz) ? cell_key(cd.ix - 1, cd.jx - 1, cd.kx - 1, nx, ny)
+                                                : (int)G;
           // cvbkforth1st (BeamBunch.f90:1681-1699); betai reuses conv1st's
           // tmpbet, the same expression of the same operands
           const double rcp = t.rcp;
@@ -1479,7 +1492,8 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
                                    c + 1 + nx, c + 1};
 #pragma unroll
         for (int k = 0; k < 8; k++) atomicAdd(a.rho + node[k], qv[k]);
-        atomicAdd(a.counts + c, 1);
+        atomicAdd(a.counts + cell_key((int)(pk[u] & 1023u), (int)((pk[u] >> 10) & 1023u),
+                                      (int)(pk[u] >> 20), nx, ny), 1);
       } else {
         const int t = mycopy + ((int)(pk[u] & 1023u) - x0) +
                       bx * (((int)((pk[u] >> 10) & 1023u) - y0) + by * ((int)(pk[u] >> 20) - z0));
@@ -1522,7 +1536,7 @@ __device__ __forceinline__ void deposit_pass(const DepositArgs& a, const int vbx
           const long long gi = (long long)(x0 + lx) + nx * ((long long)(y0 + ly) +
                                                            (long long)ny * (z0 + lz));
           if (q) atomicAdd(a.rho + gi, q);
-          if (k) atomicAdd(a.counts + gi, (int)k);
+          if (k) atomicAdd(a.counts + cell_key(x0 + lx, y0 + ly, z0 + lz, nx, ny), (int)k);
         }
       }
     }

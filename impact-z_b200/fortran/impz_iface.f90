@@ -21,6 +21,8 @@
         integer(c_int), parameter :: IMPZ_FORM_FP64 = 0
         integer(c_int), parameter :: IMPZ_FORM_FP32CONV = 1
         integer(c_int), parameter :: IMPZ_FLAG_TRACK_IDS = 1
+        integer(c_int), parameter :: IMPZ_FLAG_SPECIES = 2
+        integer(c_int), parameter :: IMPZ_MAX_SPECIES = 128
         integer(c_int), parameter :: IMPZ_MOMREC = 48
         integer(c_int), parameter :: IMPZ_DIAG_LEN = 45
 
@@ -279,6 +281,35 @@
             import :: c_int, c_double, c_ptr
             type(c_ptr), value :: bunch
             real(c_double), intent(out) :: refrec(6, *)
+            integer(c_int), value :: maxrec
+            integer(c_int), intent(out) :: nrec
+          end function
+
+          ! the bunch's species (Pts1 rows 7 and 8 of each), their number returned
+          integer(c_int) function impz_bunch_species(bunch, qm, weight, cap) &
+              bind(C, name="impz_bunch_species")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            real(c_double), intent(out) :: qm(*), weight(*)
+            integer(c_int), value :: cap
+          end function
+
+          ! chgupdate_BeamBunch (BeamBunch.f90:688-728)
+          integer(c_int) function impz_chgupdate(bunch, nchge, qmcclist, idchg) &
+              bind(C, name="impz_chgupdate")
+            import :: c_int, c_double, c_ptr
+            type(c_ptr), value :: bunch
+            integer(c_int), value :: nchge
+            real(c_double), intent(in) :: qmcclist(*)
+            integer(c_int), intent(out) :: idchg(*)
+          end function
+
+          ! per-record counts of each species of the last impz_run
+          integer(c_int) function impz_run_species(bunch, counts, maxrec, nrec) &
+              bind(C, name="impz_run_species")
+            import :: c_int, c_ptr
+            type(c_ptr), value :: bunch
+            integer(c_int), intent(out) :: counts(*)
             integer(c_int), value :: maxrec
             integer(c_int), intent(out) :: nrec
           end function
