@@ -2539,11 +2539,14 @@ int impz_autotune(impz_bunch_t b, int nsteps, double out[4]) {
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  // the fastest of three timed runs (the first, untimed run captures the
+  // step graphs): a single run's noise exceeded the 2 % a change must gain
   auto trial = [&](double* ms) -> int {
     int r = restore();
     if (r) return r;
-    for (int rep = 0; rep < 2; rep++) {  // the first run captures the step graphs
-      if (rep == 1 && (r = restore())) return r;
+    double tmin = 0.0;
+    for (int rep = 0; rep < 4; rep++) {
+      if (rep > 0 && (r = restore())) return r;
       if ((r = run_begin(b, &drift, 1))) return r;
       CK(cudaEventRecord(e0, b->stream));
       if ((r = run_advance(b, b->lat.nsteps))) return r;
@@ -2551,10 +2554,11 @@ int impz_autotune(impz_bunch_t b, int nsteps, double out[4]) {
       run_end(b);
       CK(cudaEventSynchronize(e1));
       if ((r = check_err(b))) return r;
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, e0, e1));
+      if (rep == 1 || (rep > 1 && t < tmin)) tmin = t;
     }
-    float t = 0.f;
-    CK(cudaEventElapsedTime(&t, e0, e1));
-    *ms = (double)t / b->lat.nsteps;
+    *ms = tmin / b->lat.nsteps;
     return IMPZ_OK;
   };
   int sms = 0, dev = 0;
@@ -2575,7 +2579,7 @@ int impz_autotune(impz_bunch_t b, int nsteps, double out[4]) {
       double ms = 0.0;
       int rr = trial(&ms);
       if (rr) return rr;
-      if (ms < best * 0.99) { best = ms; bestv = v; }
+      if (ms < best * 0.98) { best = ms; bestv = v; }
     }
     *param = bestv;
     return IMPZ_OK;
