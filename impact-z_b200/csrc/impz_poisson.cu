@@ -49,11 +49,11 @@ template <typename T>
 static size_t z_smem(int nz, int tkx) {
   return sizeof(typename Cplx<T>::type) * ((size_t)tkx * line_pitch(2 * nz) + nz);
 }
-// z lines per block: 8 (FP64) or 16 (FP32) for 128-byte rows, fewer when
-// long lines do not fit
+// z lines per block: 8, fewer when long lines do not fit (FP32 at
+// 64x64x128: 31.5 us per launch with 8 lines, 40.3 with 16, 32.0 with 4)
 template <typename T>
 static int ztile(int nz) {
-  int t = sizeof(T) == 8 ? 8 : 16;
+  int t = 8;
   while (t > 1 && z_smem<T>(nz, t) > smem_optin()) t /= 2;
   return t;
 }
