@@ -335,7 +335,7 @@ constexpr int kMaxAdvGrid = 2048;       // cap on push blocks (partial sums)
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
-  size_t pbuf[2][6], ids[2], spc[2], sptab, rho, counts, cursor, bsum, spec, F, Gt, ghat, phi,
+  size_t pbuf[2][6], ids[2], spc[2], sptab, rho, counts, cursor, bsum, spec, F, ghat, phi,
       efield;
   size_t tw[3], tw64[3], st, dfine, mom_fine, mom_part, rng_part, flag;
   size_t total;
@@ -372,7 +372,6 @@ Layout plan_layout(long long n, int nx, int ny, int nz, int form, int flags) {
   L.spec = take((size_t)(nx + 1) * 2 * ny * nz * 2 * esz);
   L.F = take((size_t)(nx + 2) * (ny + 2) * (nz + 2) * sizeof(double));
   const size_t noct = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
-  L.Gt = take(noct * sizeof(double));
   L.ghat = take(noct * esz);
   L.phi = take(G * esz);
   L.efield = take(4 * G * esz);
@@ -450,7 +449,6 @@ struct impz_bunch_s {
   int nscan = 0;
   void* spec = nullptr;
   double* F = nullptr;
-  double* Gt = nullptr;
   void* ghat = nullptr;
   void* phi = nullptr;
   void* efield = nullptr;
@@ -545,7 +543,7 @@ PoissonBuffers poisson_of(impz_bunch_t b) {
   pb.nx = b->nx; pb.ny = b->ny; pb.nz = b->nz;
   pb.rho = b->rho;
   pb.qscale = b->f32() ? std::ldexp(1.0, -b->fixbits) : b->weight * std::ldexp(1.0, -b->fixbits);
-  pb.spec = b->spec; pb.F = b->F; pb.Gt = b->Gt; pb.ghat = b->ghat;
+  pb.spec = b->spec; pb.F = b->F; pb.ghat = b->ghat;
   pb.phi = b->phi; pb.efield = b->efield;
   pb.twx = b->tw[0]; pb.twy = b->tw[1]; pb.twz = b->tw[2];
   pb.tw64x = b->tw64[0]; pb.tw64y = b->tw64[1]; pb.tw64z = b->tw64[2];
@@ -1103,7 +1101,6 @@ int impz_bunch_create(const double* pts, long long n, double current, double mas
   b->nscan = L.nscan;
   b->spec = at(L.spec);
   b->F = (double*)at(L.F);
-  b->Gt = (double*)at(L.Gt);
   b->ghat = at(L.ghat);
   b->phi = at(L.phi);
   b->efield = at(L.efield);
@@ -2004,7 +2001,7 @@ static int run_batch_packed(impz_bunch_t* bs, int nb) {
     PoissonMember& m = mem[k];
     m.rho = pb.rho; m.qscale = pb.qscale; m.spec = pb.spec; m.ghat = pb.ghat; m.phi = pb.phi;
     m.efield = pb.efield; m.twx = pb.twx; m.twy = pb.twy; m.twz = pb.twz; m.F = pb.F;
-    m.Gt = pb.Gt; m.st = pb.st;
+    m.st = pb.st;
     if (groups.empty() || groups.back().nx != b->nx || groups.back().ny != b->ny ||
         groups.back().nz != b->nz)
       groups.push_back(BatchGroup{b->nx, b->ny, b->nz, k, 0});
@@ -2200,7 +2197,7 @@ static int packed_step(impz_bunch_t* bs, int nb, cudaStream_t s, cudaStream_t s2
     PoissonMember& m = pm[k];
     m.rho = pb.rho; m.qscale = pb.qscale; m.spec = pb.spec; m.ghat = pb.ghat; m.phi = pb.phi;
     m.efield = pb.efield; m.twx = pb.twx; m.twy = pb.twy; m.twz = pb.twz; m.F = pb.F;
-    m.Gt = pb.Gt; m.st = pb.st;
+    m.st = pb.st;
     if (groups.empty() || groups.back().nx != b->nx || groups.back().ny != b->ny ||
         groups.back().nz != b->nz)
       groups.push_back(BatchGroup{b->nx, b->ny, b->nz, k, 0});

@@ -252,7 +252,6 @@ struct PoissonMember {
   const void* twy;
   const void* twz;
   double* F;                // IGF corners
-  double* Gt;               // FP64 Green octant
   DevState* st;
 };
 

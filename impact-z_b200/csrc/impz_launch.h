@@ -80,7 +80,6 @@ struct PoissonBuffers {
   double qscale;            // grid value of one fixed-point quantum
   void* spec;               // (nx+1)*2ny*nz complex T
   double* F;                // (nx+2)(ny+2)(nz+2) IGF corners
-  double* Gt;               // (nx+1)(ny+1)(nz+1) FP64 green octant / DCT work
   void* ghat;               // (nx+1)(ny+1)(nz+1) T
   void* phi;                // nx*ny*nz T
   void* efield;             // 4*nx*ny*nz T
