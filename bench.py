@@ -369,7 +369,10 @@ def main():
     # ---- roofline of the dominant kernel group
     peak, peak_kind = measured_peak()
     G = GRID[0] * GRID[1] * GRID[2]
-    alg = {"deposit": 48 * n + 16 * G, "scan": 12 * G, "green": 48 * G, "convolve": 76 * G,
+    # algorithmic bytes per step: the deposit reads the three conv1st-frame
+    # columns the push stored; the Green build writes and reads the FP64
+    # corners and writes Ĝ (FP32) once per plane pass
+    alg = {"deposit": 24 * n + 16 * G, "scan": 12 * G, "green": 24 * G, "convolve": 76 * G,
            "efield": 4 * G + 16 * G, "push": 96 * n + 16 * G}
     kernels = {}
     total_ms = sum(v[0] for v in prof.values())
