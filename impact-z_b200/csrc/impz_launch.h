@@ -47,7 +47,7 @@ inline cudaError_t launch_pdl(void (*kernel)(KP...), dim3 grid, dim3 block, size
 #ifndef IMPZ_DEP_MINB
 #define IMPZ_DEP_MINB 4
 #endif
-#define IMPZ_SCAN_THREADS 1024
+#define IMPZ_SCAN_THREADS 256  // x 16 cells: 4096 cells (one scan block) per block
 
 #define IMPZ_DECLARE_PARTICLE_LAUNCHERS(NS)                                              \
   namespace NS {                                                                         \

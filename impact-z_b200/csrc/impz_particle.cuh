@@ -1633,42 +1633,55 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int* wsum, int* total
 template <int BLOCK>
 __device__ __forceinline__ void scan_pass(int* counts, int* cursor, int* bsum, long long total,
                                           DevState* st, const int vbx, const int vgx) {
-  static_assert((BLOCK << 2) == (1 << IMPZ_SCAN_LOG), "four cells per thread");
+  // each thread owns CPT consecutive cells (CPT/4 16-byte loads and stores)
+  constexpr int CPT = (1 << IMPZ_SCAN_LOG) / BLOCK;
+  static_assert(CPT % 4 == 0 && CPT * BLOCK == (1 << IMPZ_SCAN_LOG), "cells per thread");
   __shared__ int wsum[BLOCK / 32 + 1];
   __shared__ unsigned int s_last;
-  const long long i0 = ((long long)vbx << IMPZ_SCAN_LOG) + 4ll * threadIdx.x;
-  int v[4];
-  const bool full = i0 + 3 < total;
+  const long long i0 = ((long long)vbx << IMPZ_SCAN_LOG) + (long long)CPT * threadIdx.x;
+  int v[CPT];
+  const bool full = i0 + CPT - 1 < total;
   if (full) {
-    const int4 q = *reinterpret_cast<const int4*>(counts + i0);
-    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
-    *reinterpret_cast<int4*>(counts + i0) = make_int4(0, 0, 0, 0);
+#pragma unroll
+    for (int q = 0; q < CPT / 4; q++) {
+      const int4 c = *reinterpret_cast<const int4*>(counts + i0 + 4 * q);
+      v[4 * q] = c.x; v[4 * q + 1] = c.y; v[4 * q + 2] = c.z; v[4 * q + 3] = c.w;
+    }
+#pragma unroll
+    for (int q = 0; q < CPT / 4; q++)
+      *reinterpret_cast<int4*>(counts + i0 + 4 * q) = make_int4(0, 0, 0, 0);
   } else {
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int j = 0; j < CPT; j++) {
       v[j] = (i0 + j < total) ? counts[i0 + j] : 0;
       if (i0 + j < total) counts[i0 + j] = 0;
     }
   }
-  int btotal = 0;
-  int run = block_exclusive_scan<BLOCK>(v[0] + v[1] + v[2] + v[3], wsum, &btotal);
-  int o[4];
+  int mine = 0;
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
-    o[j] = run;
-    run += v[j];
+  for (int j = 0; j < CPT; j++) mine += v[j];
+  int btotal = 0;
+  int run = block_exclusive_scan<BLOCK>(mine, wsum, &btotal);
+#pragma unroll
+  for (int j = 0; j < CPT; j++) {
+    const int x = v[j];
+    v[j] = run;  // the exclusive offset of cell j within the block
+    run += x;
   }
   if (full) {
-    *reinterpret_cast<int4*>(cursor + i0) = make_int4(o[0], o[1], o[2], o[3]);
+#pragma unroll
+    for (int q = 0; q < CPT / 4; q++)
+      *reinterpret_cast<int4*>(cursor + i0 + 4 * q) =
+          make_int4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
   } else {
 #pragma unroll
-    for (int j = 0; j < 4; j++)
-      if (i0 + j < total) cursor[i0 + j] = o[j];
+    for (int j = 0; j < CPT; j++)
+      if (i0 + j < total) cursor[i0 + j] = v[j];
   }
   // the last block reads only the block totals, so only their writer
   // fences (the cursors and the cleared counts reach the next kernels at the
-  // launch boundary); a fence in every thread cost 23 of the 141 cycles per
-  // issued instruction, most of the kernel's time
+  // launch boundary); a fence in every thread was the kernel's third stall
+  // reason under ncu
   if (threadIdx.x == 0) {
     bsum[vbx] = btotal;
     __threadfence();
